@@ -1,0 +1,336 @@
+"""Benchmark of the Conditional ReSTIR PT frame loop (one step = one frame).
+
+Workload: the large configuration -- 1920x1080 on a room of 64 displaced
+icospheres (5 subdivisions, 20,480 triangles each, 1,310,988 triangles in
+total with the room and the 256 emissive triangles), max depth 8, prefix
+length 2, prefix-endpoint search k = 8, 1 temporal + 2 spatial suffix passes
+of 5 neighbours, FP32 reservoirs, a 60-frame camera orbit, seed 1.
+
+Metric: resampled paths per second (25 per pixel per frame: prefix temporal
+2 + suffix temporal 2 + suffix spatial 2 x (5 + 1) + final gather 8 + 1) and
+ms per frame.  `value` is measured with everything resident on the device;
+`e2e` goes through the C ABI with the frame's camera in and the image copied
+out to pinned host memory every step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl crisb|reference]
+
+Under torchrun each rank renders its own view of the orbit (weak scaling, no
+collective on the data path); the reported time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PATHS_PER_PIXEL_LARGE = 25  # 2 + 2 + 2 * (5 + 1) + (8 + 1)
+METRIC = "1080p ms/frame & paths/s at fixed relMSE; batched+adjoint vs plain, same GPU"
+UNIT = "resampled paths/s"
+
+
+def workload(name: str):
+    from crisoptix_b200 import scenes
+
+    if name == "large":
+        desc, cam = scenes.sphere_room(num_spheres=64, subdiv=5, num_emitters=256, seed=1)
+        return desc, cam, 1920, 1080, PATHS_PER_PIXEL_LARGE
+    if name == "small":
+        desc, cam = scenes.cornell_box()
+        return desc, cam, 256, 256, 2 + 2 + (3 + 1) + 1
+    raise ValueError(name)
+
+
+def params_for(name: str, scene_size: float):
+    from crisoptix_b200 import _abi
+    from crisoptix_b200.scenes import Camera  # noqa: F401
+
+    p = _abi.Params()
+    base = dict(renderer_type=_abi.CONDITIONAL_RESTIR, nee_prob=0.3, max_path_len=8, enable_accum=0,
+                recon_min_distance=0.01 * scene_size, recon_min_roughness=0.2, prefix_len=2, prefix_enable_temporal=1,
+                prefix_enable_spatial=0, prefix_spatial_count=1, prefix_spatial_rounds=1, suffix_enable_temporal=1,
+                suffix_enable_spatial=1, suffix_spatial_count=5, suffix_spatial_rounds=2, gather_n=1, gather_m=9,
+                gather_radius=0.01, gather_radius_type=_abi.RADIUS_PATH_LENGTH, window_radius=10,
+                storage=_abi.STORAGE_FP32, seed=1)
+    if name == "small":
+        base.update(max_path_len=4, prefix_len=1, suffix_spatial_count=3, suffix_spatial_rounds=1, gather_m=1,
+                    window_radius=30, seed=0)
+    for k, v in base.items():
+        setattr(p, k, v)
+    return p
+
+
+# algorithmic bytes per pixel per pass (FP32 records: prefix reservoir 144 B,
+# canonical prefix 128 B, suffix reservoir / canonical suffix 112 B, G-buffer
+# 16 B, neighbour entry 8 B); reads + writes of the records each pass must touch
+def pass_bytes(k: int, spatial_count: int, spatial_rounds: int, copy_prefix_back: bool):
+    prefix = 144 + 128 + 144 + 128 + 144 + 16 + (144 if copy_prefix_back else 0)
+    suffix_temp = 128 + 112 + 112 + 112 + 16 + 8
+    suffix_spatial = spatial_rounds * (112 + spatial_count * (16 + 112) + 112 + 16 + 8 + 16)
+    store = 128 + 112 + 16 + 8 + 16 + 16
+    gather = 16 + 24 + k * 112 + 8 * k + 4 + 12 + 8
+    return {"prefix_gen_temp": prefix, "suffix_gen_temp": suffix_temp, "suffix_spatial": suffix_spatial,
+            "prefix_store": store, "final_gather": gather}
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.dev), "-lms", "200", "-f", self.path],
+                                         stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(desc, cam, name: str, threads: int, frames: int, warm: int = 1, scale: int = 4):
+    """The oracle (a host port of the reference's device code) on a bounded
+    sample: the same scene and parameters at 1/scale of the resolution."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as op
+    from crisoptix_b200 import scenes
+
+    _, _, W, H, ppp = workload(name)
+    w, h = max(W // scale, 8), max(H // scale, 8)
+    op.set_threads(threads)
+    o = op.Oracle.from_scene(desc, w, h, params_for(name, 0.0))
+    p = params_for(name, o.scene_size)
+    o.set_params(p)
+    out = np.zeros((h, w, 3), np.float32)
+    for f in range(warm):
+        o.render_frame(scenes.orbit_camera(cam, f, 60), out)
+    t0 = time.perf_counter()
+    for f in range(frames):
+        o.render_frame(scenes.orbit_camera(cam, warm + f, 60), out)
+    dt = time.perf_counter() - t0
+    return {"value": ppp * w * h * frames / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{w}x{h} (1/{scale * scale} of the pixels) of the same scene and parameters, "
+                      f"{frames} frame(s) after {warm} warm-up frame(s), {threads} OpenMP threads",
+            "ms_per_frame": 1000.0 * dt / frames}
+
+
+def run_reference(args):
+    """--impl reference: the oracle port of the reference's device code on the
+    host cores (the reference itself needs OptiX and cannot run here)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    desc, cam, W, H, ppp = workload(args.workload)
+    threads = os.cpu_count() or 1
+    frames = max(1, min(args.steps, 3))
+    cb = cpu_baseline(desc, cam, args.workload, threads, frames, warm=min(args.warmup, 1), scale=args.cpu_scale)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": frames, "warmup": min(args.warmup, 1), "ms_per_step": cb["ms_per_frame"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {W}x{H} conditional ReSTIR PT frame (CPU sample {cb['sample']})"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "CrisOptix needs the OptiX SDK and an OpenGL window; its CPU-side stand-in is the oracle port "
+                    "of its device code"}
+    print(json.dumps(line), flush=True)
+
+
+def run_crisb(args):
+    import torch
+
+    from crisoptix_b200 import Renderer, Scene, _abi, scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    desc, cam, W, H, ppp = workload(args.workload)
+    sc = Scene(desc)
+    p = params_for(args.workload, sc.scene_size)
+    r = Renderer(W, H, sc, p)
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    out = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
+    offset = rank * 60 // max(world, 1)  # each rank renders its own view of the orbit
+    n_frames = args.warmup + args.steps
+    cams = [scenes.orbit_camera(cam, offset + f, 60) for f in range(2 * n_frames + 8)]
+
+    def frame(i):
+        r.launch_frame(cams[i % len(cams)], out.data_ptr(), sptr)
+
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            frame(i)
+    torch.cuda.synchronize()
+    r.check_device_errors()
+
+    # ---- device-resident timing ------------------------------------------------
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for i in range(args.steps):
+        frame(args.warmup + i)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if dist:
+        dist.barrier()
+    ms = t_start.elapsed_time(t_end)
+    launches_per_frame = r.stats()["kernel_launches"]
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_frame = ms / args.steps
+    value = ppp * W * H * args.steps * world / (ms / 1000.0)
+
+    # ---- per-pass breakdown (CUDA events on the launching stream) -------------
+    r.set_timing(True)
+    passes = {k: 0.0 for k in ("prefix_gen_temp_ms", "prefix_spatial_ms", "suffix_gen_temp_ms", "suffix_spatial_ms",
+                               "prefix_store_ms", "final_gather_ms", "total_ms")}
+    n_pass = 3
+    for i in range(n_pass):
+        frame(n_frames + i)
+        st = r.stats()
+        for k in passes:
+            passes[k] += st[k] / n_pass
+    r.set_timing(False)
+    r.check_device_errors()
+
+    # ---- end to end through the C ABI with host buffers ------------------------
+    host = torch.empty(W * H * 3, dtype=torch.float32, pin_memory=True)
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_steps = max(3, args.steps // 2)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e_start.record(stream)
+    with torch.cuda.stream(stream):
+        for i in range(e_steps):
+            frame(n_frames + n_pass + i)
+            host.copy_(out, non_blocking=True)
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    e_ms = e_start.elapsed_time(e_end)
+    if dist:
+        t = torch.tensor([e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_ms = float(t.item())
+    e2e_value = ppp * W * H * e_steps * world / (e_ms / 1000.0)
+    img_mean = float(host.mean())
+
+    # ---- roofline of the dominant pass ------------------------------------------
+    peak, peak_kind = measured_peaks()
+    pb = pass_bytes(p.gather_m - 1, p.suffix_spatial_count, p.suffix_spatial_rounds, bool(p.suffix_enable_spatial))
+    pass_ms = {"prefix_gen_temp": passes["prefix_gen_temp_ms"], "suffix_gen_temp": passes["suffix_gen_temp_ms"],
+               "suffix_spatial": passes["suffix_spatial_ms"], "prefix_store": passes["prefix_store_ms"],
+               "final_gather": passes["final_gather_ms"]}
+    dom = max(pass_ms, key=pass_ms.get)
+    dom_bytes = pb[dom] * W * H
+    achieved = dom_bytes / (pass_ms[dom] / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": dom, "peak_kind": f"{peak_kind} copy bandwidth",
+                "algorithmic_bytes_per_launch": dom_bytes, "pass_ms": pass_ms}
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    cb = None
+    if not args.no_cpu_baseline and world == 1:
+        cb = cpu_baseline(desc, cam, args.workload, os.cpu_count() or 1, 3, warm=1, scale=args.cpu_scale)
+        cb.pop("ms_per_frame", None)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_frame, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {W}x{H} conditional ReSTIR PT, {sc.num_triangles} triangles, "
+                                   f"k={p.gather_m - 1}, {p.suffix_spatial_rounds}x{p.suffix_spatial_count} spatial, "
+                                   f"max depth {p.max_path_len}, FP32 storage",
+                       "paths_per_pixel": ppp, "l2": "working set (reservoirs, BVH) larger than L2",
+                       "parallelism": f"view-sharded replicas x{world}"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 48, "d2h_bytes_per_step": W * H * 12},
+            "roofline": roofline, "cpu_baseline": cb, "clocks": clk,
+            "gpu_launches": launches_per_frame * args.steps, "image_mean": img_mean}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="crisb", choices=["crisb", "reference"])
+    ap.add_argument("--workload", default="large", choices=["large", "small"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-scale", type=int, default=2)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_crisb(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,212 @@
+"""crisoptix_b200 -- B200-native Conditional ReSTIR PT frame loop.
+
+Python view of the C ABI in include/crisb.h, shaped like the reference's host
+API: ``Scene`` (include/model/Scene.h:12-24), ``Renderer``
+(include/graph/Renderer.h:11-21) with ``launch_frame`` / ``get_frame_idx``,
+and a camera description (include/graph/Camera.h).  All compute runs in the
+in-tree CUDA library libcrisb.so; importing works without a GPU, creating a
+scene or renderer needs one.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import _abi
+from ._abi import CrisbError, check, load
+from .scenes import Camera as CameraDesc
+from .scenes import Scene as SceneDesc
+
+__all__ = ["Scene", "Renderer", "CameraDesc", "SceneDesc", "default_params", "camera_struct", "CrisbError", "load"]
+
+
+def camera_struct(cam: CameraDesc) -> _abi.Camera:
+    c = _abi.Camera()
+    c.pos[:] = cam.pos
+    c.view_dir[:] = cam.view_dir
+    c.up[:] = cam.up
+    c.aspect = cam.aspect
+    c.fov = cam.fov
+    c.changed = 1 if cam.changed else 0
+    return c
+
+
+def camera_data(cam: CameraDesc) -> np.ndarray:
+    """Camera::GetData -> (pos, U, V, W) as a (4, 3) float32 array."""
+    d = _abi.CameraData()
+    check(load().crisb_camera_get_data(ctypes.byref(camera_struct(cam)), ctypes.byref(d)))
+    return np.array([list(d.pos), list(d.u), list(d.v), list(d.w)], dtype=np.float32)
+
+
+def default_params(scene_size: float, **overrides) -> _abi.Params:
+    """Renderer defaults of src/Renderer.cpp:34-58, then `overrides`."""
+    p = _abi.Params()
+    check(load().crisb_params_default(ctypes.byref(p), ctypes.c_float(scene_size)))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+class Scene:
+    """Scene(instances, emitters): flattens instances and builds the device
+    BVH on the current CUDA device."""
+
+    def __init__(self, desc: SceneDesc):
+        lib = load()
+        self.desc = desc
+        self._keep = []
+
+        def arr(a, dtype):
+            a = np.ascontiguousarray(a, dtype=dtype)
+            self._keep.append(a)
+            return a.ctypes.data_as(ctypes.c_void_p)
+
+        d = _abi.SceneDesc()
+        d.positions = arr(desc.positions, np.float32)
+        d.normals = arr(desc.normals, np.float32)
+        d.num_vertices = len(desc.positions)
+        d.indices = arr(desc.indices, np.uint32)
+        d.triangle_material = arr(desc.triangle_material, np.uint32)
+        d.num_triangles = len(desc.indices)
+        mats = (_abi.Material * len(desc.materials))()
+        for i, m in enumerate(desc.materials):
+            mats[i].diffuse[:] = [float(v) for v in m["diffuse"]]
+            mats[i].specular[:] = [float(v) for v in m["specular"]]
+            mats[i].emission[:] = [float(v) for v in m["emission"]]
+            mats[i].roughness = float(m["roughness"])
+            mats[i].spec_usage = int(m["spec_usage"])
+        self._keep.append(mats)
+        d.materials = ctypes.cast(mats, ctypes.c_void_p)
+        d.num_materials = len(desc.materials)
+        if desc.instances:
+            meshes = (_abi.Mesh * len(desc.meshes))()
+            for i, (f, n) in enumerate(desc.meshes):
+                meshes[i].first_triangle = int(f)
+                meshes[i].num_triangles = int(n)
+            inst = (_abi.Instance * len(desc.instances))()
+            for i, (m, ov, xf) in enumerate(desc.instances):
+                inst[i].mesh = int(m)
+                inst[i].material_override = int(ov)
+                inst[i].transform[:] = [float(v) for v in xf]
+            self._keep += [meshes, inst]
+            d.meshes = ctypes.cast(meshes, ctypes.c_void_p)
+            d.num_meshes = len(desc.meshes)
+            d.instances = ctypes.cast(inst, ctypes.c_void_p)
+            d.num_instances = len(desc.instances)
+        ems = (_abi.Emitter * len(desc.emitters))()
+        for i, (color, first, count) in enumerate(desc.emitters):
+            ems[i].color[:] = [float(v) for v in color]
+            ems[i].first_face = int(first)
+            ems[i].num_faces = int(count)
+        self._keep.append(ems)
+        d.emitters = ctypes.cast(ems, ctypes.c_void_p)
+        d.num_emitters = len(desc.emitters)
+        d.emitter_faces = arr(desc.emitter_faces, np.float32)
+        d.num_emitter_faces = len(desc.emitter_faces)
+        h = ctypes.c_void_p()
+        check(lib.crisb_scene_create(ctypes.byref(d), ctypes.byref(h)))
+        self.handle = h
+        self._keep.clear()
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            load().crisb_scene_destroy(h)
+            self.handle = None
+
+    @property
+    def scene_size(self) -> float:
+        v = ctypes.c_float()
+        check(load().crisb_scene_size(self.handle, ctypes.byref(v)))
+        return v.value
+
+    @property
+    def num_triangles(self) -> int:
+        v = ctypes.c_uint32()
+        check(load().crisb_scene_num_triangles(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def read_triangles(self):
+        """World-space triangle soup: (T, 9) positions, (T, 9) normals, (T,)
+        materials, in scene order."""
+        n = self.num_triangles
+        pos = np.zeros((n, 9), np.float32)
+        nrm = np.zeros((n, 9), np.float32)
+        mat = np.zeros(n, np.uint32)
+        check(load().crisb_scene_read_triangles(self.handle, pos.ctypes.data_as(ctypes.c_void_p),
+                                                 nrm.ctypes.data_as(ctypes.c_void_p),
+                                                 mat.ctypes.data_as(ctypes.c_void_p)))
+        return pos, nrm, mat
+
+    def trace(self, rays_dev_ptr: int, hits_dev_ptr: int, n: int, any_hit: bool, stream: int = 0):
+        check(load().crisb_trace_rays(self.handle, ctypes.c_void_p(rays_dev_ptr), ctypes.c_void_p(hits_dev_ptr),
+                                      n, 1 if any_hit else 0, ctypes.c_void_p(stream)))
+
+
+class Renderer:
+    """Renderer(width, height, camera, scene): the Conditional ReSTIR PT
+    frame loop on the scene's device."""
+
+    def __init__(self, width: int, height: int, scene: Scene, params: Optional[_abi.Params] = None):
+        self.scene = scene
+        self.width = width
+        self.height = height
+        if params is None:
+            params = default_params(scene.scene_size)
+        h = ctypes.c_void_p()
+        check(load().crisb_renderer_create(scene.handle, width, height, ctypes.byref(params), ctypes.byref(h)))
+        self.handle = h
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            load().crisb_renderer_destroy(h)
+            self.handle = None
+
+    @property
+    def params(self) -> _abi.Params:
+        p = _abi.Params()
+        check(load().crisb_renderer_get_params(self.handle, ctypes.byref(p)))
+        return p
+
+    @params.setter
+    def params(self, p: _abi.Params):
+        check(load().crisb_renderer_set_params(self.handle, ctypes.byref(p)))
+
+    def launch_frame(self, camera: CameraDesc, out_dev_ptr: int, stream: int = 0):
+        """Renderer::LaunchFrame into a device buffer of width*height*3 floats."""
+        check(load().crisb_render_frame(self.handle, ctypes.byref(camera_struct(camera)), ctypes.c_void_p(out_dev_ptr),
+                                        ctypes.c_void_p(stream)))
+
+    def get_frame_idx(self) -> int:
+        v = ctypes.c_uint64()
+        check(load().crisb_frame_index(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def frame_random(self) -> int:
+        v = ctypes.c_uint32()
+        check(load().crisb_frame_random(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def set_timing(self, enable: bool):
+        check(load().crisb_set_timing(self.handle, 1 if enable else 0))
+
+    def stats(self) -> dict:
+        s = _abi.Stats()
+        check(load().crisb_get_stats(self.handle, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def check_device_errors(self):
+        check(load().crisb_check_device_errors(self.handle))
+
+    def debug_read(self, buffer_id: int) -> np.ndarray:
+        size = ctypes.c_size_t()
+        check(load().crisb_debug_size(self.handle, buffer_id, ctypes.byref(size)))
+        dt = _abi.BUFFER_DTYPES[buffer_id]
+        out = np.zeros(size.value // dt.itemsize, dtype=dt)
+        check(load().crisb_debug_read(self.handle, buffer_id, out.ctypes.data_as(ctypes.c_void_p), size.value))
+        return out

@@ -1,0 +1,910 @@
+// api.cu -- host side of the library: scene creation and device BVH build,
+// the renderer and its frame orchestration, and the C ABI of include/crisb.h.
+//
+// Mirrors Scene (src/Scene.cpp), Camera::GetData (src/Camera.cpp:20-32) and
+// Renderer (src/Renderer.cpp).  No call throws across the ABI; failures are
+// status codes with a per-thread message (crisb_last_error).
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "passes.cuh"
+
+namespace crisb {
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        const int code = (e == cudaErrorMemoryAllocation) ? CRISB_ERR_OUT_OF_MEMORY : CRISB_ERR_CUDA;
+        throw Error(code, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+void require(bool ok, const std::string& msg) {
+    if (!ok) throw Error(CRISB_ERR_INVALID_ARGUMENT, msg);
+}
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        return CRISB_OK;
+    } catch (const Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return CRISB_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return CRISB_ERR_CUDA;
+    }
+}
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count) {
+        release();
+        if (count == 0) count = 1;
+        check(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+        n = count;
+    }
+    void upload(const T* src, size_t count) {
+        alloc(count);
+        if (count) check(cudaMemcpy(p, src, count * sizeof(T), cudaMemcpyHostToDevice), "upload");
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// host PCG32 with an explicit stream (per-frame random of LaunchFrame)
+uint32_t frame_random(uint64_t seed, uint64_t counter) {
+    uint64_t state = 0;
+    const uint64_t inc = (counter << 1u) | 1u;
+    auto next = [&]() {
+        const uint64_t old = state;
+        state = old * kPcgMult + inc;
+        const uint32_t xs = static_cast<uint32_t>(((old >> 18u) ^ old) >> 27u);
+        const uint32_t rot = static_cast<uint32_t>(old >> 59u);
+        return (xs >> rot) | (xs << ((32u - rot) & 31u));
+    };
+    next();
+    state += seed;
+    next();
+    return next();
+}
+
+// Camera::GetData (src/Camera.cpp:20-32).  The rotation block of
+// inverse(lookAt) is the transpose of lookAt's, so its columns (s, u, -f)
+// are taken directly.
+crisb_camera_data camera_data(const crisb_camera& c) {
+    const V3 pos = ld3(c.pos), view = ld3(c.view_dir), up = ld3(c.up);
+    const V3 center = pos + view;
+    const V3 f = normalize(center - pos);
+    const V3 s = normalize(cross(f, up));
+    const V3 u = cross(s, f);
+    const float tan_half = std::tan(0.5f * c.fov);
+    crisb_camera_data d;
+    st3(d.pos, pos);
+    st3(d.u, normalize(s) * tan_half * c.aspect);
+    st3(d.v, -normalize(u) * tan_half);
+    st3(d.w, -normalize(-f));
+    return d;
+}
+
+}  // namespace
+
+__global__ void k_tri_keys(const float* pos, uint32_t n, float3 lo, float3 hi, uint64_t* keys) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* p = pos + 9 * static_cast<size_t>(i);
+    const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
+    const float cx = (p[0] + p[3] + p[6]) * (1.0f / 3.0f);
+    const float cy = (p[1] + p[4] + p[7]) * (1.0f / 3.0f);
+    const float cz = (p[2] + p[5] + p[8]) * (1.0f / 3.0f);
+    keys[i] = lbvh::morton_key(l, h, cx, cy, cz, i);
+}
+
+__global__ void k_tri_leaves(const float* pos, lbvh::Work w, float4* tris) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *w.n) return;
+    const uint32_t prim = static_cast<uint32_t>(w.keys[i] & 0xFFFFFFFFull);
+    w.order[i] = prim;
+    const float* p = pos + 9 * static_cast<size_t>(prim);
+    tris[3 * i + 0] = make_float4(p[0], p[1], p[2], 0.0f);
+    tris[3 * i + 1] = make_float4(p[3], p[4], p[5], 0.0f);
+    tris[3 * i + 2] = make_float4(p[6], p[7], p[8], __uint_as_float(prim));
+    lbvh::Box b;
+    for (int a = 0; a < 3; ++a) {
+        b.lo[a] = fminf(fminf(p[a], p[3 + a]), p[6 + a]);
+        b.hi[a] = fmaxf(fmaxf(p[a], p[3 + a]), p[6 + a]);
+    }
+    w.leaf_box[i] = b;
+}
+
+__global__ void k_trace_rays(SceneView s, const float* rays, crisb_trace_hit* hits, uint32_t n, int any_hit) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* r = rays + 8 * static_cast<size_t>(i);
+    const RayPre rp = make_ray(V3{r[0], r[1], r[2]}, V3{r[4], r[5], r[6]});
+    crisb_trace_hit h;
+    if (any_hit) {
+        const TraceResult t = traverse<true>(s, rp, r[3], r[7]);
+        h.prim = t.prim != CRISB_INVALID_PRIM ? 1u : 0u;
+        h.t = h.u = h.v = 0.0f;
+    } else {
+        const TraceResult t = traverse<false>(s, rp, r[3], r[7]);
+        h.prim = t.prim;
+        h.t = t.prim != CRISB_INVALID_PRIM ? t.t : 0.0f;
+        h.u = t.prim != CRISB_INVALID_PRIM ? t.u : 0.0f;
+        h.v = t.prim != CRISB_INVALID_PRIM ? t.v : 0.0f;
+    }
+    hits[i] = h;
+}
+
+// default (never written) records: every hit invalid, everything else zero
+__global__ void k_init_records(crisb_prefix_res_rec* pres0, crisb_prefix_res_rec* pres1, crisb_prefix_rec* cpre,
+                               crisb_suffix_res_rec* sres0, crisb_suffix_res_rec* sres1, crisb_suffix_res_rec* csuf,
+                               crisb_gbuffer_rec* gbuf, uint32_t P) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    crisb_prefix_res_rec pr;
+    memset(&pr, 0, sizeof(pr));
+    pr.sample.primary.prim = pr.sample.recon.prim = pr.sample.last.prim = CRISB_INVALID_PRIM;
+    pres0[i] = pr;
+    pres1[i] = pr;
+    cpre[i] = pr.sample;
+    crisb_suffix_res_rec sr;
+    memset(&sr, 0, sizeof(sr));
+    sr.sample.recon.prim = sr.sample.last_prefix.prim = CRISB_INVALID_PRIM;
+    sres0[i] = sr;
+    sres1[i] = sr;
+    csuf[i] = sr;
+    crisb_gbuffer_rec g;
+    memset(&g, 0, sizeof(g));
+    gbuf[i] = g;
+}
+
+// sort 64-bit keys [0, n) of keys_in into keys
+static void sort_keys(const uint64_t* in, uint64_t* out, uint32_t n, DevBuf<char>& temp, cudaStream_t st) {
+    size_t need = 0;
+    check(cub::DeviceRadixSort::SortKeys(nullptr, need, in, out, static_cast<int>(n), 0, 64, st), "sort size");
+    if (temp.bytes() < need) temp.alloc(need);
+    size_t have = temp.bytes();
+    check(cub::DeviceRadixSort::SortKeys(temp.p, have, in, out, static_cast<int>(n), 0, 64, st), "radix sort");
+}
+
+struct LbvhStorage {
+    DevBuf<uint64_t> keys_in, keys;
+    DevBuf<int> inner_parent, leaf_parent, inner_left, inner_right, range_lo, range_hi, flags;
+    DevBuf<lbvh::Box> inner_box, leaf_box;
+    DevBuf<uint32_t> n, order;
+    DevBuf<BvhNode> nodes;
+    void alloc(uint32_t cap) {
+        const size_t c = std::max<uint32_t>(cap, 2);
+        keys_in.alloc(c);
+        keys.alloc(c);
+        inner_parent.alloc(c);
+        leaf_parent.alloc(c);
+        inner_left.alloc(c);
+        inner_right.alloc(c);
+        range_lo.alloc(c);
+        range_hi.alloc(c);
+        flags.alloc(c);
+        inner_box.alloc(c);
+        leaf_box.alloc(c);
+        n.alloc(1);
+        order.alloc(c);
+        nodes.alloc(c);
+    }
+    lbvh::Work work(int* err) {
+        lbvh::Work w;
+        w.keys_in = keys_in.p;
+        w.keys = keys.p;
+        w.inner_parent = inner_parent.p;
+        w.leaf_parent = leaf_parent.p;
+        w.inner_left = inner_left.p;
+        w.inner_right = inner_right.p;
+        w.range_lo = range_lo.p;
+        w.range_hi = range_hi.p;
+        w.inner_box = inner_box.p;
+        w.leaf_box = leaf_box.p;
+        w.flags = flags.p;
+        w.n = n.p;
+        w.nodes = nodes.p;
+        w.order = order.p;
+        w.err = err;
+        return w;
+    }
+};
+
+}  // namespace crisb
+
+using namespace crisb;
+
+struct crisb_scene {
+    int device = 0;
+    uint32_t num_tris = 0;
+    float scene_size = 0.0f;
+    std::vector<float> h_pos, h_nrm;
+    std::vector<uint32_t> h_mat;
+    DevBuf<BvhNode> nodes;
+    DevBuf<float4> tris;
+    DevBuf<float4> shade;
+    DevBuf<crisb_material> mats;
+    DevBuf<crisb_emitter> emitters;
+    DevBuf<float> emitter_faces;
+    uint32_t num_emitters = 0;
+    DevBuf<int> err;
+
+    SceneView view(int* err_word) const {
+        SceneView v;
+        v.nodes = nodes.p;
+        v.tris = tris.p;
+        v.shade = shade.p;
+        v.mats = mats.p;
+        v.emitters = emitters.p;
+        v.emitter_faces = emitter_faces.p;
+        v.num_emitters = num_emitters;
+        v.num_tris = num_tris;
+        v.err = err_word;
+        return v;
+    }
+};
+
+namespace {
+
+void flatten(const crisb_scene_desc& d, crisb_scene& s) {
+    require(d.positions && d.indices && d.triangle_material && d.materials, "scene: null array");
+    require(d.num_materials > 0, "scene: no materials");
+    require(d.emitters && d.num_emitters > 0 && d.emitter_faces, "scene: at least one emitter is required");
+    for (uint32_t t = 0; t < d.num_triangles; ++t) {
+        for (int c = 0; c < 3; ++c) require(d.indices[3 * t + c] < d.num_vertices, "scene: index out of range");
+        require(d.triangle_material[t] < d.num_materials, "scene: material index out of range");
+    }
+    for (uint32_t e = 0; e < d.num_emitters; ++e) {
+        require(d.emitters[e].num_faces > 0, "scene: emitter without faces");
+        require(static_cast<uint64_t>(d.emitters[e].first_face) + d.emitters[e].num_faces <= d.num_emitter_faces,
+                "scene: emitter face range out of bounds");
+    }
+    auto corner = [&](uint32_t t, int c, const float* M, float* p, float* n) {
+        const uint32_t vi = d.indices[3 * t + c];
+        const float* v = d.positions + 3 * static_cast<size_t>(vi);
+        float nn[3];
+        if (d.normals) {
+            const float* q = d.normals + 3 * static_cast<size_t>(vi);
+            nn[0] = q[0];
+            nn[1] = q[1];
+            nn[2] = q[2];
+        } else {
+            const float* a = d.positions + 3 * static_cast<size_t>(d.indices[3 * t]);
+            const float* b = d.positions + 3 * static_cast<size_t>(d.indices[3 * t + 1]);
+            const float* cc = d.positions + 3 * static_cast<size_t>(d.indices[3 * t + 2]);
+            const V3 fn = normalize(cross(V3{b[0] - a[0], b[1] - a[1], b[2] - a[2]},
+                                          V3{cc[0] - a[0], cc[1] - a[1], cc[2] - a[2]}));
+            nn[0] = fn.x;
+            nn[1] = fn.y;
+            nn[2] = fn.z;
+        }
+        if (!M) {
+            std::memcpy(p, v, 12);
+            std::memcpy(n, nn, 12);
+            return;
+        }
+        double m[3][3];
+        for (int r = 0; r < 3; ++r) {
+            for (int cc2 = 0; cc2 < 3; ++cc2) m[r][cc2] = M[4 * r + cc2];
+            p[r] = static_cast<float>(M[4 * r] * static_cast<double>(v[0]) + M[4 * r + 1] * static_cast<double>(v[1]) +
+                                      M[4 * r + 2] * static_cast<double>(v[2]) + M[4 * r + 3]);
+        }
+        // normal transform: inverse transpose of the 3x3 block, renormalised
+        const double det = m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) -
+                           m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+                           m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+        require(det != 0.0, "scene: singular instance transform");
+        double cof[3][3];
+        cof[0][0] = m[1][1] * m[2][2] - m[1][2] * m[2][1];
+        cof[0][1] = m[1][2] * m[2][0] - m[1][0] * m[2][2];
+        cof[0][2] = m[1][0] * m[2][1] - m[1][1] * m[2][0];
+        cof[1][0] = m[0][2] * m[2][1] - m[0][1] * m[2][2];
+        cof[1][1] = m[0][0] * m[2][2] - m[0][2] * m[2][0];
+        cof[1][2] = m[0][1] * m[2][0] - m[0][0] * m[2][1];
+        cof[2][0] = m[0][1] * m[1][2] - m[0][2] * m[1][1];
+        cof[2][1] = m[0][2] * m[1][0] - m[0][0] * m[1][2];
+        cof[2][2] = m[0][0] * m[1][1] - m[0][1] * m[1][0];
+        double o[3];
+        for (int r = 0; r < 3; ++r) o[r] = (cof[r][0] * nn[0] + cof[r][1] * nn[1] + cof[r][2] * nn[2]) / det;
+        const double len = std::sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+        for (int r = 0; r < 3; ++r) n[r] = static_cast<float>(len > 0 ? o[r] / len : o[r]);
+    };
+    auto emit = [&](uint32_t first, uint32_t count, const float* M, int32_t override_mat) {
+        for (uint32_t t = first; t < first + count; ++t) {
+            float p[9], n[9];
+            for (int c = 0; c < 3; ++c) corner(t, c, M, p + 3 * c, n + 3 * c);
+            s.h_pos.insert(s.h_pos.end(), p, p + 9);
+            s.h_nrm.insert(s.h_nrm.end(), n, n + 9);
+            s.h_mat.push_back(override_mat >= 0 ? static_cast<uint32_t>(override_mat) : d.triangle_material[t]);
+        }
+    };
+    if (d.num_instances == 0) {
+        emit(0, d.num_triangles, nullptr, -1);
+    } else {
+        require(d.instances && d.meshes, "scene: instances need meshes");
+        for (uint32_t i = 0; i < d.num_instances; ++i) {
+            const crisb_instance& in = d.instances[i];
+            require(in.mesh < d.num_meshes, "scene: instance mesh out of range");
+            const crisb_mesh& m = d.meshes[in.mesh];
+            require(static_cast<uint64_t>(m.first_triangle) + m.num_triangles <= d.num_triangles,
+                    "scene: mesh triangle range out of bounds");
+            require(in.material_override < static_cast<int32_t>(d.num_materials),
+                    "scene: material override out of range");
+            emit(m.first_triangle, m.num_triangles, in.transform, in.material_override);
+        }
+    }
+    require(s.h_mat.size() < 0x7FFFFFFFu, "scene: too many triangles");
+    s.num_tris = static_cast<uint32_t>(s.h_mat.size());
+    // Scene::GetSceneSize (src/Scene.cpp:48-71): bounds start at the origin
+    float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    for (size_t k = 0; k < s.h_pos.size(); k += 3)
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = gmin(lo[a], s.h_pos[k + a]);
+            hi[a] = gmax(hi[a], s.h_pos[k + a]);
+        }
+    s.scene_size = distance(V3{lo[0], lo[1], lo[2]}, V3{hi[0], hi[1], hi[2]});
+}
+
+void build_scene(const crisb_scene_desc& d, crisb_scene& s) {
+    check(cudaGetDevice(&s.device), "cudaGetDevice");
+    flatten(d, s);
+    const uint32_t n = s.num_tris;
+    // shading records: p0 p1 p2 n0 n1 n2 material (5 float4 per triangle)
+    std::vector<float4> shade(5 * static_cast<size_t>(std::max<uint32_t>(n, 1)));
+    for (uint32_t t = 0; t < n; ++t) {
+        const float* p = &s.h_pos[9 * static_cast<size_t>(t)];
+        const float* q = &s.h_nrm[9 * static_cast<size_t>(t)];
+        float m;
+        std::memcpy(&m, &s.h_mat[t], 4);
+        shade[5 * t + 0] = make_float4(p[0], p[1], p[2], p[3]);
+        shade[5 * t + 1] = make_float4(p[4], p[5], p[6], p[7]);
+        shade[5 * t + 2] = make_float4(p[8], q[0], q[1], q[2]);
+        shade[5 * t + 3] = make_float4(q[3], q[4], q[5], q[6]);
+        shade[5 * t + 4] = make_float4(q[7], q[8], m, 0.0f);
+    }
+    s.shade.upload(shade.data(), shade.size());
+    s.mats.upload(d.materials, d.num_materials);
+    s.emitters.upload(d.emitters, d.num_emitters);
+    s.emitter_faces.upload(d.emitter_faces, 9 * static_cast<size_t>(d.num_emitter_faces));
+    s.num_emitters = d.num_emitters;
+    s.err.alloc(1);
+    check(cudaMemset(s.err.p, 0, sizeof(int)), "memset");
+    // LBVH over triangle centroids
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t t = 0; t < n; ++t) {
+        const float* p = &s.h_pos[9 * static_cast<size_t>(t)];
+        for (int a = 0; a < 3; ++a) {
+            const float c = (p[a] + p[3 + a] + p[6 + a]) * (1.0f / 3.0f);
+            lo[a] = std::min(lo[a], c);
+            hi[a] = std::max(hi[a], c);
+        }
+    }
+    DevBuf<float> dpos;
+    dpos.upload(s.h_pos.data(), s.h_pos.size());
+    LbvhStorage st;
+    st.alloc(n);
+    lbvh::Work w = st.work(s.err.p);
+    check(cudaMemcpy(st.n.p, &n, 4, cudaMemcpyHostToDevice), "upload n");
+    const unsigned g = (std::max<uint32_t>(n, 1) + kPassBlock - 1) / kPassBlock;
+    s.tris.alloc(3 * static_cast<size_t>(std::max<uint32_t>(n, 1)));
+    if (n > 0) {
+        k_tri_keys<<<g, kPassBlock>>>(dpos.p, n, make_float3(lo[0], lo[1], lo[2]), make_float3(hi[0], hi[1], hi[2]),
+                                      st.keys_in.p);
+        check(cudaGetLastError(), "k_tri_keys");
+        DevBuf<char> temp;
+        sort_keys(st.keys_in.p, st.keys.p, n, temp, nullptr);
+        k_tri_leaves<<<g, kPassBlock>>>(dpos.p, w, s.tris.p);
+        check(cudaGetLastError(), "k_tri_leaves");
+    }
+    launch_lbvh_hierarchy(w, std::max<uint32_t>(n, 1), kTriLeafMax, nullptr);
+    check(cudaGetLastError(), "lbvh");
+    check(cudaDeviceSynchronize(), "scene build");
+    s.nodes.alloc(std::max<size_t>(st.nodes.n, 1));
+    check(cudaMemcpy(s.nodes.p, st.nodes.p, st.nodes.bytes(), cudaMemcpyDeviceToDevice), "nodes");
+    int err = 0;
+    check(cudaMemcpy(&err, s.err.p, 4, cudaMemcpyDeviceToHost), "err");
+    if (err) throw Error(CRISB_ERR_DEVICE_FAULT, "scene build: device error " + std::to_string(err));
+}
+
+void validate_params(const crisb_params& p) {
+    require(p.renderer_type >= 0 && p.renderer_type <= 2, "params: renderer_type");
+    require(p.max_path_len >= 1 && p.max_path_len <= 255, "params: max_path_len must be in [1, 255]");
+    require(p.prefix_len >= 1 && p.prefix_len <= p.max_path_len, "params: prefix_len must be in [1, max_path_len]");
+    require(p.prefix_spatial_count >= 0 && p.prefix_spatial_count <= CRISB_MAX_SPATIAL_NEIGH,
+            "params: prefix_spatial_count must be in [0, 16]");
+    require(p.suffix_spatial_count >= 0 && p.suffix_spatial_count <= CRISB_MAX_SPATIAL_NEIGH,
+            "params: suffix_spatial_count must be in [0, 16]");
+    require(p.prefix_spatial_rounds >= 0 && p.suffix_spatial_rounds >= 0, "params: negative spatial rounds");
+    require(p.gather_n >= 1, "params: gather_n must be >= 1");
+    require(p.gather_m >= 1 && p.gather_m <= CRISB_MAX_GATHER_M, "params: gather_m must be in [1, 32]");
+    require(p.window_radius >= 0 && p.window_radius < 32768, "params: window_radius");
+    require(p.storage == CRISB_STORAGE_FP32, "params: only FP32 storage is available in this build");
+    require(p.nee_prob >= 0.0f && p.nee_prob <= 1.0f, "params: nee_prob must be in [0, 1]");
+}
+
+}  // namespace
+
+struct crisb_renderer {
+    const crisb_scene* scene = nullptr;
+    uint32_t width = 0, height = 0;
+    crisb_params params{};
+    uint64_t frame_idx = 0, frame_counter = 0;
+    uint32_t random = 0;
+    int front = 0, back = 0;
+    int scur = 0;
+    DevBuf<crisb_prefix_res_rec> pres[2];
+    DevBuf<crisb_prefix_rec> canon_prefix;
+    DevBuf<crisb_suffix_res_rec> sres[2];
+    DevBuf<crisb_suffix_res_rec> canon_suffix;
+    DevBuf<crisb_gbuffer_rec> gbuf;
+    DevBuf<crisb_neighbor_rec> neighbors;
+    DevBuf<uint32_t> neigh_count;
+    DevBuf<float4> entries, knn_leaf;
+    DevBuf<unsigned int> bounds;
+    DevBuf<char> sort_temp;
+    LbvhStorage knn;
+    DevBuf<int> err;
+    cudaStream_t last_stream = nullptr;
+    bool timing = false;
+    cudaEvent_t ev[7] = {};
+    uint32_t launches = 0;
+
+    uint32_t K() const { return static_cast<uint32_t>(params.gather_m - 1); }
+    uint32_t P() const { return width * height; }
+
+    Bufs bufs() const {
+        Bufs b;
+        b.pres[0] = pres[0].p;
+        b.pres[1] = pres[1].p;
+        b.canon_prefix = canon_prefix.p;
+        b.sres_cur = sres[scur].p;
+        b.sres_next = sres[scur ^ 1].p;
+        b.canon_suffix = canon_suffix.p;
+        b.gbuf = gbuf.p;
+        b.neighbors = neighbors.p;
+        b.neigh_count = neigh_count.p;
+        b.entries = entries.p;
+        b.knn_nodes = knn.nodes.p;
+        b.knn_leaf = knn_leaf.p;
+        b.knn_pixel = knn.order.p;
+        b.knn_n = knn.n.p;
+        return b;
+    }
+
+    ~crisb_renderer() {
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+
+    void allocate() {
+        const uint32_t p = P();
+        for (int i = 0; i < 2; ++i) {
+            pres[i].alloc(p);
+            sres[i].alloc(p);
+        }
+        canon_prefix.alloc(p);
+        canon_suffix.alloc(p);
+        gbuf.alloc(p);
+        neighbors.alloc(static_cast<size_t>(p) * std::max<uint32_t>(K(), 1));
+        neigh_count.alloc(p);
+        entries.alloc(p);
+        knn_leaf.alloc(p);
+        bounds.alloc(8);
+        knn.alloc(p);
+        err.alloc(1);
+        check(cudaMemset(err.p, 0, sizeof(int)), "memset");
+        check(cudaMemset(neighbors.p, 0, neighbors.bytes()), "memset");
+        check(cudaMemset(neigh_count.p, 0, neigh_count.bytes()), "memset");
+        k_init_records<<<(p + kPassBlock - 1) / kPassBlock, kPassBlock>>>(pres[0].p, pres[1].p, canon_prefix.p,
+                                                                         sres[0].p, sres[1].p, canon_suffix.p,
+                                                                         gbuf.p, p);
+        check(cudaGetLastError(), "init records");
+        size_t need = 0;
+        check(cub::DeviceRadixSort::SortKeys(nullptr, need, knn.keys_in.p, knn.keys.p, static_cast<int>(p), 0, 64),
+              "sort size");
+        sort_temp.alloc(need);
+        check(cudaDeviceSynchronize(), "renderer init");
+    }
+
+    void record(int slot, cudaStream_t st) {
+        if (timing) check(cudaEventRecord(ev[slot], st), "event");
+    }
+
+    void render(const crisb_camera& cam, float* out, cudaStream_t st) {
+        require(out != nullptr, "render_frame: null output");
+        launches = 0;
+        // Renderer::LaunchFrame (src/Renderer.cpp:211-232)
+        ++frame_idx;
+        if (cam.changed || !params.enable_accum) frame_idx = 0;
+        random = frame_random(params.seed, frame_counter);
+        ++frame_counter;
+        if (front == 0) {
+            front = 1;
+            back = 0;
+        } else {
+            front = 0;
+            back = 1;
+        }
+        FrameParams fp;
+        fp.p = params;
+        fp.cam = camera_data(cam);
+        fp.width = width;
+        fp.height = height;
+        fp.random = random;
+        fp.frame_idx = static_cast<uint32_t>(frame_idx);
+        fp.front = front;
+        fp.back = back;
+        fp.k = K();
+        const SceneView s = scene->view(err.p);
+        last_stream = st;
+        record(0, st);
+        launch_prefix_gen_temp(s, fp, bufs(), out, st);
+        ++launches;
+        record(1, st);
+        const int type = params.renderer_type;
+        if (type == CRISB_RENDERER_PATH_TRACER) {
+            for (int i = 2; i < 7; ++i) record(i, st);
+            check(cudaGetLastError(), "launch");
+            return;
+        }
+        if (params.prefix_enable_spatial) {
+            for (int r = 0; r < params.prefix_spatial_rounds; ++r) {
+                launch_prefix_spatial(s, fp, bufs(), out, r, st);
+                launch_prefix_copy_front_back(fp, bufs(), st);
+                launches += 2;
+            }
+        }
+        record(2, st);
+        if (type == CRISB_RENDERER_CONDITIONAL_RESTIR) {
+            launch_suffix_gen_temp(s, fp, bufs(), st);
+            ++launches;
+            record(3, st);
+            if (params.suffix_enable_spatial && params.suffix_spatial_count > 0) {
+                for (int r = 0; r < params.suffix_spatial_rounds; ++r) {
+                    launch_suffix_spatial(s, fp, bufs(), st);
+                    ++launches;
+                    scur ^= 1;
+                }
+            }
+            record(4, st);
+            lbvh::Work w = knn.work(err.p);
+            launch_store_entries(s, fp, bufs(), w, bounds.p, st);
+            size_t have = sort_temp.bytes();
+            check(cub::DeviceRadixSort::SortKeys(sort_temp.p, have, knn.keys_in.p, knn.keys.p, static_cast<int>(P()),
+                                                 0, 64, st),
+                  "radix sort");
+            launch_knn_finish(fp, bufs(), w, knn_leaf.p, st);
+            launches += 3 + 4;  // own kernels; the radix sort's library kernels are not counted
+            record(5, st);
+            launch_final_gather(s, fp, bufs(), out, st);
+            ++launches;
+        } else {
+            record(3, st);
+            record(4, st);
+            record(5, st);
+        }
+        record(6, st);
+        check(cudaGetLastError(), "launch");
+    }
+};
+
+extern "C" {
+
+const char* crisb_version(void) { return "crisb 0.1.0 (sm_100a)"; }
+
+int crisb_last_error(char* buf, size_t len) {
+    if (!buf || len == 0) return CRISB_ERR_INVALID_ARGUMENT;
+    std::strncpy(buf, g_last_error.c_str(), len - 1);
+    buf[len - 1] = 0;
+    return CRISB_OK;
+}
+
+int crisb_params_default(crisb_params* out, float scene_size) {
+    return guarded([&] {
+        require(out != nullptr, "null params");
+        std::memset(out, 0, sizeof(*out));
+        // Renderer::Renderer, src/Renderer.cpp:34-58
+        out->renderer_type = CRISB_RENDERER_PATH_TRACER;
+        out->nee_prob = 0.3f;
+        out->max_path_len = 8;
+        out->enable_accum = 0;
+        out->recon_min_distance = 0.01f * scene_size;
+        out->recon_min_roughness = 0.2f;
+        out->prefix_len = 2;
+        out->prefix_enable_temporal = 1;
+        out->prefix_enable_spatial = 0;
+        out->prefix_spatial_count = 1;
+        out->prefix_spatial_rounds = 1;
+        out->suffix_enable_temporal = 1;
+        out->suffix_enable_spatial = 1;
+        out->suffix_spatial_count = 1;
+        out->suffix_spatial_rounds = 1;
+        out->gather_n = 1;
+        out->gather_m = 1;
+        out->gather_radius = 0.01f;
+        out->gather_radius_type = CRISB_RADIUS_PATH_LENGTH;
+        out->window_radius = 10;
+        out->storage = CRISB_STORAGE_FP32;
+        out->seed = 0;
+    });
+}
+
+int crisb_camera_get_data(const crisb_camera* cam, crisb_camera_data* out) {
+    return guarded([&] {
+        require(cam && out, "null argument");
+        *out = camera_data(*cam);
+    });
+}
+
+int crisb_scene_create(const crisb_scene_desc* desc, crisb_scene** out) {
+    return guarded([&] {
+        require(desc && out, "null argument");
+        *out = nullptr;
+        auto s = std::make_unique<crisb_scene>();
+        build_scene(*desc, *s);
+        *out = s.release();
+    });
+}
+
+int crisb_scene_destroy(crisb_scene* scene) {
+    delete scene;
+    return CRISB_OK;
+}
+
+int crisb_scene_size(const crisb_scene* scene, float* out) {
+    return guarded([&] {
+        require(scene && out, "null argument");
+        *out = scene->scene_size;
+    });
+}
+
+int crisb_scene_num_triangles(const crisb_scene* scene, uint32_t* out) {
+    return guarded([&] {
+        require(scene && out, "null argument");
+        *out = scene->num_tris;
+    });
+}
+
+int crisb_scene_read_triangles(const crisb_scene* scene, float* positions, float* normals, uint32_t* materials) {
+    return guarded([&] {
+        require(scene != nullptr, "null scene");
+        if (positions) std::memcpy(positions, scene->h_pos.data(), scene->h_pos.size() * 4);
+        if (normals) std::memcpy(normals, scene->h_nrm.data(), scene->h_nrm.size() * 4);
+        if (materials) std::memcpy(materials, scene->h_mat.data(), scene->h_mat.size() * 4);
+    });
+}
+
+int crisb_trace_rays(const crisb_scene* scene, const float* rays_dev, crisb_trace_hit* hits_dev, uint32_t n,
+                     int any_hit, void* stream) {
+    return guarded([&] {
+        require(scene && rays_dev && hits_dev, "null argument");
+        if (n == 0) return;
+        const SceneView s = scene->view(scene->err.p);
+        k_trace_rays<<<(n + kPassBlock - 1) / kPassBlock, kPassBlock, 0, static_cast<cudaStream_t>(stream)>>>(
+            s, rays_dev, hits_dev, n, any_hit);
+        check(cudaGetLastError(), "k_trace_rays");
+    });
+}
+
+int crisb_renderer_create(const crisb_scene* scene, uint32_t width, uint32_t height, const crisb_params* params,
+                          crisb_renderer** out) {
+    return guarded([&] {
+        require(scene && params && out, "null argument");
+        *out = nullptr;
+        require(width > 0 && height > 0 && width < 65536 && height < 65536, "renderer: bad resolution");
+        require(static_cast<uint64_t>(width) * height < (1ull << 31), "renderer: too many pixels");
+        validate_params(*params);
+        int dev = 0;
+        check(cudaGetDevice(&dev), "cudaGetDevice");
+        require(dev == scene->device, "renderer: scene lives on another device");
+        auto r = std::make_unique<crisb_renderer>();
+        r->scene = scene;
+        r->width = width;
+        r->height = height;
+        r->params = *params;
+        r->allocate();
+        *out = r.release();
+    });
+}
+
+int crisb_renderer_destroy(crisb_renderer* r) {
+    delete r;
+    return CRISB_OK;
+}
+
+int crisb_renderer_set_params(crisb_renderer* r, const crisb_params* params) {
+    return guarded([&] {
+        require(r && params, "null argument");
+        validate_params(*params);
+        const bool realloc_neighbors = params->gather_m != r->params.gather_m;
+        r->params = *params;
+        if (realloc_neighbors) {
+            check(cudaDeviceSynchronize(), "sync");
+            r->neighbors.alloc(static_cast<size_t>(r->P()) * std::max<uint32_t>(r->K(), 1));
+            check(cudaMemset(r->neighbors.p, 0, r->neighbors.bytes()), "memset");
+        }
+    });
+}
+
+int crisb_renderer_get_params(const crisb_renderer* r, crisb_params* out) {
+    return guarded([&] {
+        require(r && out, "null argument");
+        *out = r->params;
+    });
+}
+
+int crisb_render_frame(crisb_renderer* r, const crisb_camera* cam, float* out_rgb_dev, void* stream) {
+    return guarded([&] {
+        require(r && cam, "null argument");
+        r->render(*cam, out_rgb_dev, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int crisb_frame_index(const crisb_renderer* r, uint64_t* out) {
+    return guarded([&] {
+        require(r && out, "null argument");
+        *out = r->frame_idx;
+    });
+}
+
+int crisb_frame_random(const crisb_renderer* r, uint32_t* out) {
+    return guarded([&] {
+        require(r && out, "null argument");
+        *out = r->random;
+    });
+}
+
+int crisb_set_timing(crisb_renderer* r, int enable) {
+    return guarded([&] {
+        require(r != nullptr, "null renderer");
+        if (enable && !r->ev[0])
+            for (auto& e : r->ev) check(cudaEventCreate(&e), "event create");
+        r->timing = enable != 0;
+    });
+}
+
+int crisb_get_stats(crisb_renderer* r, crisb_stats* out) {
+    return guarded([&] {
+        require(r && out, "null argument");
+        std::memset(out, 0, sizeof(*out));
+        out->kernel_launches = r->launches;
+        if (!r->timing) return;
+        check(cudaEventSynchronize(r->ev[6]), "event sync");
+        float ms[6];
+        for (int i = 0; i < 6; ++i) check(cudaEventElapsedTime(&ms[i], r->ev[i], r->ev[i + 1]), "elapsed");
+        out->prefix_gen_temp_ms = ms[0];
+        out->prefix_spatial_ms = ms[1];
+        out->suffix_gen_temp_ms = ms[2];
+        out->suffix_spatial_ms = ms[3];
+        out->prefix_store_ms = ms[4];
+        out->final_gather_ms = ms[5];
+        check(cudaEventElapsedTime(&out->total_ms, r->ev[0], r->ev[6]), "elapsed");
+    });
+}
+
+int crisb_check_device_errors(crisb_renderer* r) {
+    int code = CRISB_OK;
+    const int st = guarded([&] {
+        require(r != nullptr, "null renderer");
+        check(cudaStreamSynchronize(r->last_stream), "stream sync");
+        int e = 0;
+        check(cudaMemcpy(&e, r->err.p, 4, cudaMemcpyDeviceToHost), "read error word");
+        if (e) {
+            g_last_error = "device error word " + std::to_string(e) +
+                           ((e & kDevErrStack) ? " (traversal stack overflow)" : "") +
+                           ((e & kDevErrIterations) ? " (traversal iteration cap)" : "") +
+                           ((e & kDevErrKnn) ? " (endpoint search cap)" : "");
+            code = CRISB_ERR_DEVICE_FAULT;
+        }
+    });
+    return st != CRISB_OK ? st : code;
+}
+
+int crisb_debug_size(const crisb_renderer* r, int id, size_t* out) {
+    return guarded([&] {
+        require(r && out, "null argument");
+        const size_t P = r->P();
+        switch (id) {
+            case CRISB_BUF_PREFIX_RES_FRONT:
+            case CRISB_BUF_PREFIX_RES_BACK: *out = P * sizeof(crisb_prefix_res_rec); break;
+            case CRISB_BUF_CANON_PREFIX: *out = P * sizeof(crisb_prefix_rec); break;
+            case CRISB_BUF_SUFFIX_RES_FRONT:
+            case CRISB_BUF_SUFFIX_RES_BACK: *out = P * sizeof(crisb_suffix_res_rec); break;
+            case CRISB_BUF_CANON_SUFFIX: *out = P * sizeof(crisb_suffix_rec); break;
+            case CRISB_BUF_GBUFFER: *out = P * sizeof(crisb_gbuffer_rec); break;
+            case CRISB_BUF_NEIGHBORS: *out = P * r->K() * sizeof(crisb_neighbor_rec); break;
+            case CRISB_BUF_NEIGHBOR_COUNT: *out = P * sizeof(uint32_t); break;
+            default: require(false, "debug: unknown buffer id");
+        }
+    });
+}
+
+int crisb_debug_read(crisb_renderer* r, int id, void* dst, size_t bytes) {
+    return guarded([&] {
+        require(r && dst, "null argument");
+        size_t want = 0;
+        if (crisb_debug_size(r, id, &want) != CRISB_OK) throw Error(CRISB_ERR_INVALID_ARGUMENT, g_last_error);
+        require(bytes == want, "debug: size mismatch");
+        check(cudaDeviceSynchronize(), "sync");
+        const size_t P = r->P();
+        switch (id) {
+            case CRISB_BUF_PREFIX_RES_FRONT:
+                check(cudaMemcpy(dst, r->pres[r->front].p, bytes, cudaMemcpyDeviceToHost), "read");
+                break;
+            case CRISB_BUF_PREFIX_RES_BACK:
+                check(cudaMemcpy(dst, r->pres[r->back].p, bytes, cudaMemcpyDeviceToHost), "read");
+                break;
+            case CRISB_BUF_CANON_PREFIX:
+                check(cudaMemcpy(dst, r->canon_prefix.p, bytes, cudaMemcpyDeviceToHost), "read");
+                break;
+            case CRISB_BUF_SUFFIX_RES_FRONT:
+            case CRISB_BUF_SUFFIX_RES_BACK:
+                check(cudaMemcpy(dst, r->sres[r->scur].p, bytes, cudaMemcpyDeviceToHost), "read");
+                break;
+            case CRISB_BUF_CANON_SUFFIX: {
+                std::vector<crisb_suffix_res_rec> tmp(P);
+                check(cudaMemcpy(tmp.data(), r->canon_suffix.p, P * sizeof(crisb_suffix_res_rec),
+                                 cudaMemcpyDeviceToHost),
+                      "read");
+                auto* o = static_cast<crisb_suffix_rec*>(dst);
+                for (size_t i = 0; i < P; ++i) o[i] = tmp[i].sample;
+                break;
+            }
+            case CRISB_BUF_GBUFFER:
+                check(cudaMemcpy(dst, r->gbuf.p, bytes, cudaMemcpyDeviceToHost), "read");
+                break;
+            case CRISB_BUF_NEIGHBORS:
+                if (bytes) check(cudaMemcpy(dst, r->neighbors.p, bytes, cudaMemcpyDeviceToHost), "read");
+                break;
+            case CRISB_BUF_NEIGHBOR_COUNT:
+                check(cudaMemcpy(dst, r->neigh_count.p, bytes, cudaMemcpyDeviceToHost), "read");
+                break;
+            default: break;
+        }
+    });
+}
+
+int crisb_abi_sizes(uint32_t* out, uint32_t n) {
+    const uint32_t sizes[] = {
+        sizeof(crisb_material),    sizeof(crisb_mesh),         sizeof(crisb_instance),     sizeof(crisb_emitter),
+        sizeof(crisb_scene_desc),  sizeof(crisb_camera),       sizeof(crisb_camera_data),  sizeof(crisb_params),
+        sizeof(crisb_hit_rec),     sizeof(crisb_prefix_rec),   sizeof(crisb_prefix_res_rec), sizeof(crisb_suffix_rec),
+        sizeof(crisb_suffix_res_rec), sizeof(crisb_gbuffer_rec), sizeof(crisb_neighbor_rec), sizeof(crisb_trace_hit),
+        sizeof(crisb_stats)};
+    const uint32_t count = sizeof(sizes) / sizeof(sizes[0]);
+    if (!out) return static_cast<int>(count);
+    for (uint32_t i = 0; i < n && i < count; ++i) out[i] = sizes[i];
+    return static_cast<int>(count);
+}
+
+}  // extern "C"

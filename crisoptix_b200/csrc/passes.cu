@@ -1,0 +1,666 @@
+// passes.cu -- the per-frame pass kernels of Conditional ReSTIR PT.
+//
+// One kernel per reference raygen program (shader/*.cu), one thread per
+// pixel, records loaded whole, updated with the reference's in-place field
+// semantics, and stored whole.
+#define CRISB_LBVH_KERNELS 1
+#include "passes.cuh"
+
+namespace crisb {
+
+namespace {
+
+RT_D uint32_t pixel_count(const FrameParams& fp) { return fp.width * fp.height; }
+
+RT_D Res<Prefix> ld_pres(const crisb_prefix_res_rec* p, uint32_t i) {
+    const crisb_prefix_res_rec r = p[i];
+    return Res<Prefix>{ld_prefix(r.sample), r.w_sum, r.confidence};
+}
+RT_D void st_pres(crisb_prefix_res_rec* p, uint32_t i, const Res<Prefix>& r) {
+    crisb_prefix_res_rec o;
+    st_prefix(o.sample, r.s);
+    o.w_sum = r.w_sum;
+    o.confidence = r.conf;
+    o.pad[0] = 0;
+    o.pad[1] = 0;
+    p[i] = o;
+}
+RT_D Res<Suffix> ld_sres(const crisb_suffix_res_rec* p, uint32_t i) {
+    const crisb_suffix_res_rec r = p[i];
+    return Res<Suffix>{ld_suffix(r.sample), r.w_sum, r.confidence};
+}
+RT_D void st_sres(crisb_suffix_res_rec* p, uint32_t i, const Res<Suffix>& r) {
+    crisb_suffix_res_rec o;
+    st_suffix(o.sample, r.s);
+    o.w_sum = r.w_sum;
+    o.confidence = r.conf;
+    p[i] = o;
+}
+
+RT_D void store_output(const FrameParams& fp, float* out, uint32_t i, V3 radiance) {
+    V3 v = radiance;
+    if (fp.p.enable_accum) {
+        const V3 old = V3{out[3 * i], out[3 * i + 1], out[3 * i + 2]};
+        const float blend = 1.0f / static_cast<float>(fp.frame_idx + 1);
+        v = blend * radiance + (1.0f - blend) * old;
+    }
+    out[3 * i] = v.x;
+    out[3 * i + 1] = v.y;
+    out[3 * i + 2] = v.z;
+}
+
+// PrefixGenTempReuse, shader/prefix_gen_temp_reuse.cu:11-98
+RT_D bool prefix_gen_temp_reuse(const SceneView& s, const FrameParams& fp, const Bufs& b, uint32_t i, V3 origin,
+                                V3 dir, Rng& rng, Res<Prefix>& cur) {
+    Prefix canon = ld_prefix(b.canon_prefix[i]);
+    trace_prefix(s, fp, canon, origin, dir, rng);
+    st_prefix(b.canon_prefix[i], canon);
+    if (!fl_valid(canon.flags)) return false;
+    const float canon_phat = luminance(canon.f);
+    cur.w_sum = 0.0f;
+    cur.conf = 0.0f;
+    // prevPixelCoord == pixelCoord (no motion vectors), always inside the image
+    if (!fp.p.prefix_enable_temporal) {
+        res_update(cur, canon, canon_phat / canon.p, rng, 1.0f);
+        res_finalize(cur);
+        return true;
+    }
+    const Res<Prefix> prev = ld_pres(b.pres[fp.back], i);
+    const bool skip_nee = fp.p.renderer_type == CRISB_RENDERER_CONDITIONAL_RESTIR && fl_nee(prev.s.flags);
+    if (prev.w_sum <= 0.0f || !fl_valid(prev.s.flags) || skip_nee) {
+        res_update(cur, canon, canon_phat / canon.p, rng, 1.0f);
+        res_finalize(cur);
+        return true;
+    }
+    float jac_prev_to_canon = 0.0f, jac_canon_to_prev = 0.0f;
+    const V3 f_canon_of_prev = shift_prefix(s, prev.s, canon, jac_prev_to_canon);
+    const V3 f_prev_of_canon = shift_prefix(s, canon, prev.s, jac_canon_to_prev);
+    const float p_canon_of_prev = luminance(f_canon_of_prev) * jac_prev_to_canon;
+    const float K = 1.0f;
+    const float prev_mis = mis_neighbor(f_canon_of_prev, prev.s.f, jac_prev_to_canon, K, 1.0f, prev.conf);
+    const float canon_mis = 1.0f + mis_canonical(canon.f, f_prev_of_canon, jac_canon_to_prev, K, 1.0f, prev.conf);
+    res_update(cur, canon, canon_mis * canon_phat / canon.p, rng, 1.0f);
+    Prefix shifted = prev.s;  // PrefixPath(prev, f, canon.primaryInt)
+    shifted.f = f_canon_of_prev;
+    shifted.primary = canon.primary;
+    res_update(cur, shifted, prev_mis * p_canon_of_prev * prev.w_sum, rng, prev.conf);
+    if (cur.w_sum > 0.0f) {
+        cur.w_sum /= K + 1.0f;
+        res_finalize(cur);
+    }
+    return true;
+}
+
+// __raygen__prefix_gen_temp_reuse, shader/prefix_gen_temp_reuse.cu:100-193
+__global__ void __launch_bounds__(kPassBlock) k_prefix_gen_temp(SceneView s, FrameParams fp, Bufs b, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixel_count(fp)) return;
+    const uint32_t x = i % fp.width, y = i / fp.width;
+    Rng rng = rng_seeded(tea64(i, fp.random));
+    const V3 dir = camera_dir(fp, x, y, rng);
+    const V3 origin = ld3(fp.cam.pos);
+    const int type = fp.p.renderer_type;
+    if (type == CRISB_RENDERER_CONDITIONAL_RESTIR || type == CRISB_RENDERER_RESTIR_PT) {
+        Res<Prefix> cur = ld_pres(b.pres[fp.front], i);
+        const bool valid = prefix_gen_temp_reuse(s, fp, b, i, origin, dir, rng, cur);
+        st_pres(b.pres[fp.front], i, cur);
+        if (type == CRISB_RENDERER_RESTIR_PT && !fp.p.prefix_enable_spatial)
+            store_output(fp, out, i, valid ? cur.w_sum * cur.s.f : splat(0.0f));
+        if ((type == CRISB_RENDERER_RESTIR_PT && fp.p.prefix_enable_spatial) ||
+            (type == CRISB_RENDERER_CONDITIONAL_RESTIR && fp.p.suffix_enable_spatial))
+            st_pres(b.pres[fp.back], i, cur);
+        crisb_gbuffer_rec g;
+        g.rng = rng.state;
+        g.prev_xy = x | (y << 16);
+        g.flags = valid ? 1u : 0u;
+        b.gbuf[i] = g;
+    } else {
+        V3 L = trace_complete_path(s, fp, origin, dir, rng);
+        if (nonfinite(L)) L = splat(0.0f);
+        store_output(fp, out, i, L);
+    }
+}
+
+// PrefixSpatialReuse, shader/prefix_spatial_reuse.cu:11-134.  Neighbours come
+// from the back buffer, which equals the front buffer at pass start.
+__global__ void __launch_bounds__(kPassBlock)
+    k_prefix_spatial(SceneView s, FrameParams fp, Bufs b, float* out, int round) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixel_count(fp)) return;
+    const uint32_t x = i % fp.width, y = i / fp.width;
+    Res<Prefix> cur = ld_pres(b.pres[fp.front], i);
+    bool ok = false;
+    const Prefix cur_prefix = cur.s;
+    const crisb_prefix_rec& canon = b.canon_prefix[i];
+    if (fl_valid(cur_prefix.flags) && fl_valid(canon.flags) && canon.primary.prim != CRISB_INVALID_PRIM) {
+        ok = true;
+        Rng rng{b.gbuf[i].rng};
+        const float cur_wsum = cur.w_sum, cur_conf = cur.conf;
+        cur.w_sum = 0.0f;
+        cur.conf = 0.0f;
+        const int count = fp.p.prefix_spatial_count;
+        float canon_mis = 1.0f;
+        uint32_t nvalid = 0, vflags = 0;
+        uint32_t nx[CRISB_MAX_SPATIAL_NEIGH], ny[CRISB_MAX_SPATIAL_NEIGH];
+        for (int n = 0; n < count; ++n) {
+            select_spatial_neighbor(x, y, static_cast<uint32_t>(fp.p.window_radius), rng, nx[n], ny[n]);
+            if (!(nx[n] < fp.width && ny[n] < fp.height)) continue;
+            const uint32_t ni = ny[n] * fp.width + nx[n];
+            if (!(b.gbuf[ni].flags & 1u)) continue;
+            const uint32_t nflags = b.pres[fp.back][ni].sample.flags;
+            const bool skip_nee = fp.p.renderer_type == CRISB_RENDERER_CONDITIONAL_RESTIR && fl_nee(nflags);
+            if (!fl_valid(nflags) || skip_nee) continue;
+            ++nvalid;
+            vflags |= 1u << n;
+        }
+        const float K = static_cast<float>(nvalid);
+        for (int n = 0; n < count; ++n) {
+            if (!((vflags >> n) & 1u)) continue;
+            const uint32_t ni = ny[n] * fp.width + nx[n];
+            const Res<Prefix> nr = ld_pres(b.pres[fp.back], ni);
+            float jac_n2c = 0.0f, jac_c2n = 0.0f;
+            const V3 f_c_of_n = shift_prefix(s, nr.s, cur_prefix, jac_n2c);
+            const float p_c_of_n = luminance(f_c_of_n) * jac_n2c;
+            const V3 f_n_of_c = shift_prefix(s, cur_prefix, nr.s, jac_c2n);
+            float nmis = mis_neighbor(f_c_of_n, nr.s.f, jac_n2c, K, cur_conf, nr.conf);
+            if (nonfinite(nmis)) nmis = 0.0f;
+            Prefix shifted = nr.s;
+            shifted.f = f_c_of_n;
+            shifted.primary = cur_prefix.primary;
+            res_update(cur, shifted, nmis * p_c_of_n * nr.w_sum, rng, nr.conf);
+            canon_mis += mis_canonical(cur_prefix.f, f_n_of_c, jac_c2n, K, cur_conf, nr.conf);
+        }
+        if (nonfinite(canon_mis)) canon_mis = 0.0f;
+        res_update(cur, cur_prefix, canon_mis * cur_wsum * luminance(cur_prefix.f), rng, cur_conf);
+        if (cur.w_sum > 0.0f) {
+            cur.w_sum /= K + 1.0f;
+            res_finalize(cur);
+        }
+        b.gbuf[i].rng = rng.state;
+        st_pres(b.pres[fp.front], i, cur);
+    }
+    if (fp.p.renderer_type == CRISB_RENDERER_RESTIR_PT && round == fp.p.prefix_spatial_rounds - 1)
+        store_output(fp, out, i, ok ? cur.w_sum * cur.s.f : splat(0.0f));
+}
+
+__global__ void k_prefix_copy(FrameParams fp, Bufs b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixel_count(fp)) return;
+    b.pres[fp.back][i] = b.pres[fp.front][i];
+}
+
+RT_D void invalidate(Res<Suffix>& r) {
+    r.w_sum = 0.0f;
+    r.conf = 0.0f;
+    r.s.flags = fl_set_valid(r.s.flags, false);
+}
+
+// SuffixGenTempReuse + raygen, shader/suffix_gen_temp_reuse.cu:12-134.  The
+// suffix buffer is updated in place: front and back hold equal content at
+// pass start and the pass ends with front copied to back.
+__global__ void __launch_bounds__(kPassBlock) k_suffix_gen_temp(SceneView s, FrameParams fp, Bufs b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixel_count(fp)) return;
+    Res<Suffix> cur = ld_sres(b.sres_cur, i);
+    const Prefix prefix = ld_prefix(b.pres[fp.front][i].sample);
+    if (!fl_valid(prefix.flags) || fl_nee(prefix.flags)) {
+        invalidate(cur);
+        st_sres(b.sres_cur, i, cur);
+        return;
+    }
+    Rng rng{b.gbuf[i].rng};
+    Suffix canon = ld_suffix(b.canon_suffix[i].sample);
+    trace_suffix(s, fp, canon, prefix, rng);
+    {
+        crisb_suffix_res_rec o;
+        st_suffix(o.sample, canon);
+        o.w_sum = 0.0f;
+        o.confidence = 0.0f;
+        b.canon_suffix[i] = o;
+    }
+    if (!fl_valid(canon.flags)) {
+        invalidate(cur);
+        st_sres(b.sres_cur, i, cur);
+        b.gbuf[i].rng = rng.state;
+        return;
+    }
+    const float canon_phat = luminance(canon.f);
+    const Res<Suffix> prev = cur;  // back[prevPixelIdx] == front[i] content before this pass
+    cur.w_sum = 0.0f;
+    cur.conf = 0.0f;
+    if (!fp.p.suffix_enable_temporal || prev.w_sum <= 0.0f || !fl_valid(prev.s.flags)) {
+        res_update(cur, canon, canon_phat / canon.p, rng, 1.0f);
+        res_finalize(cur);
+    } else {
+        float jac_prev_to_canon = 0.0f, jac_canon_to_prev = 0.0f;
+        const V3 f_canon_of_prev = shift_suffix(s, prev.s, canon, jac_prev_to_canon);
+        const V3 f_prev_of_canon = shift_suffix(s, canon, prev.s, jac_canon_to_prev);
+        const float p_canon_of_prev = luminance(f_canon_of_prev) * jac_prev_to_canon;
+        const float K = 1.0f;
+        const float prev_mis = mis_neighbor(f_canon_of_prev, prev.s.f, jac_prev_to_canon, K, 1.0f, prev.conf);
+        const float canon_mis =
+            1.0f + mis_canonical(canon.f, f_prev_of_canon, jac_canon_to_prev, K, 1.0f, prev.conf);
+        res_update(cur, canon, canon_mis * canon_phat / canon.p, rng, 1.0f);
+        Suffix shifted = prev.s;  // SuffixPath(prev, canon.lastPrefixInt, f)
+        shifted.last_prefix = canon.last_prefix;
+        shifted.f = f_canon_of_prev;
+        res_update(cur, shifted, prev_mis * p_canon_of_prev * prev.w_sum, rng, prev.conf);
+        if (cur.w_sum > 0.0f) {
+            cur.w_sum /= K + 1.0f;
+            res_finalize(cur);
+        }
+    }
+    b.gbuf[i].rng = rng.state;
+    st_sres(b.sres_cur, i, cur);
+}
+
+// SuffixSpatialReuse + raygen, shader/suffix_spatial_reuse.cu:16-167: reads
+// the pass-start state `sres_cur` (own and neighbours), writes `sres_next`.
+__global__ void __launch_bounds__(kPassBlock) k_suffix_spatial(SceneView s, FrameParams fp, Bufs b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixel_count(fp)) return;
+    const uint32_t x = i % fp.width, y = i / fp.width;
+    Res<Suffix> cur = ld_sres(b.sres_cur, i);
+    const uint32_t prefix_flags = b.pres[fp.front][i].sample.flags;
+    const uint32_t canon_flags = b.canon_suffix[i].sample.flags;
+    if (!fl_valid(prefix_flags) || fl_nee(prefix_flags) || !fl_valid(cur.s.flags) || !fl_valid(canon_flags)) {
+        invalidate(cur);
+        st_sres(b.sres_next, i, cur);
+        return;
+    }
+    Rng rng{b.gbuf[i].rng};
+    const Suffix cur_suffix = cur.s;
+    const float cur_wsum = cur.w_sum, cur_conf = cur.conf;
+    cur.w_sum = 0.0f;
+    cur.conf = 0.0f;
+    const int count = fp.p.suffix_spatial_count;
+    float canon_mis = 1.0f;
+    uint32_t nvalid = 0, vflags = 0;
+    uint32_t nx[CRISB_MAX_SPATIAL_NEIGH], ny[CRISB_MAX_SPATIAL_NEIGH];
+    for (int n = 0; n < count; ++n) {
+        select_spatial_neighbor(x, y, static_cast<uint32_t>(fp.p.window_radius), rng, nx[n], ny[n]);
+        if (!(nx[n] < fp.width && ny[n] < fp.height)) continue;
+        const uint32_t ni = ny[n] * fp.width + nx[n];
+        if (!(b.gbuf[ni].flags & 1u)) continue;
+        if (!fl_valid(b.sres_cur[ni].sample.flags)) continue;
+        ++nvalid;
+        vflags |= 1u << n;
+    }
+    const float K = static_cast<float>(nvalid);
+    for (int n = 0; n < count; ++n) {
+        if (!((vflags >> n) & 1u)) continue;
+        const uint32_t ni = ny[n] * fp.width + nx[n];
+        const Res<Suffix> nr = ld_sres(b.sres_cur, ni);
+        float jac_n2c = 0.0f, jac_c2n = 0.0f;
+        const V3 f_c_of_n = shift_suffix(s, nr.s, cur_suffix, jac_n2c);
+        const float p_c_of_n = luminance(f_c_of_n) * jac_n2c;
+        const V3 f_n_of_c = shift_suffix(s, cur_suffix, nr.s, jac_c2n);
+        float nmis = mis_neighbor(f_c_of_n, nr.s.f, jac_n2c, K, cur_conf, nr.conf);
+        if (nonfinite(nmis)) nmis = 0.0f;
+        Suffix shifted = nr.s;
+        shifted.last_prefix = cur_suffix.last_prefix;
+        shifted.f = f_c_of_n;
+        res_update(cur, shifted, nmis * p_c_of_n * nr.w_sum, rng, nr.conf);
+        canon_mis += mis_canonical(cur_suffix.f, f_n_of_c, jac_c2n, K, cur_conf, nr.conf);
+    }
+    if (nonfinite(canon_mis)) canon_mis = 0.0f;
+    res_update(cur, cur_suffix, canon_mis * cur_wsum * luminance(cur_suffix.f), rng, cur_conf);
+    if (cur.w_sum > 0.0f) {
+        cur.w_sum /= K + 1.0f;
+        res_finalize(cur);
+    }
+    b.gbuf[i].rng = rng.state;
+    st_sres(b.sres_next, i, cur);
+}
+
+// ---- prefix entries and the endpoint search structure ---------------------------
+RT_D unsigned int float_to_ordered(float f) {
+    const unsigned int u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+RT_D float ordered_to_float(unsigned int u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
+}
+
+__global__ void k_bounds_init(unsigned int* ob, uint32_t* n) {
+    if (threadIdx.x < 3) ob[threadIdx.x] = float_to_ordered(INFINITY);
+    else if (threadIdx.x < 6) ob[threadIdx.x] = float_to_ordered(-INFINITY);
+    if (threadIdx.x == 0) *n = 0;
+}
+
+// __raygen__prefix_store_entries, shader/prefix_store_entries.cu:9-53: the
+// endpoint of the front prefix and the radius the search tests against,
+// (aabb.maxX - aabb.minX) / 2 (shader/prefix_search_hit.cu:42).
+__global__ void k_store_entries(FrameParams fp, Bufs b, const SceneView s, unsigned int* ob, uint32_t* count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t P = pixel_count(fp);
+    float4 e = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+    bool valid = false;
+    if (i < P) {
+        const crisb_prefix_rec& pr = b.pres[fp.front][i].sample;
+        const uint32_t sflags = b.sres_cur[i].sample.flags;
+        const Isect last = unpack(s, ld_hit(pr.last));
+        if (fl_valid(pr.flags) && fl_valid(sflags) && last.valid) {
+            float radius = fp.p.gather_radius;
+            if (fp.p.gather_radius_type == CRISB_RADIUS_PATH_LENGTH) radius *= pr.path_len / 4.5f;
+            const float minx = last.pos.x - radius, maxx = last.pos.x + radius;
+            e = make_float4(last.pos.x, last.pos.y, last.pos.z, (maxx - minx) / 2.0f);
+            valid = true;
+        }
+        b.entries[i] = e;
+    }
+    // block-level bounds of valid endpoints, then one atomic per block
+    __shared__ float smin[3][kPassBlock], smax[3][kPassBlock];
+    __shared__ uint32_t scount[kPassBlock];
+    smin[0][threadIdx.x] = valid ? e.x : INFINITY;
+    smin[1][threadIdx.x] = valid ? e.y : INFINITY;
+    smin[2][threadIdx.x] = valid ? e.z : INFINITY;
+    smax[0][threadIdx.x] = valid ? e.x : -INFINITY;
+    smax[1][threadIdx.x] = valid ? e.y : -INFINITY;
+    smax[2][threadIdx.x] = valid ? e.z : -INFINITY;
+    scount[threadIdx.x] = valid ? 1u : 0u;
+    __syncthreads();
+    for (int off = kPassBlock / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off) {
+            for (int a = 0; a < 3; ++a) {
+                smin[a][threadIdx.x] = fminf(smin[a][threadIdx.x], smin[a][threadIdx.x + off]);
+                smax[a][threadIdx.x] = fmaxf(smax[a][threadIdx.x], smax[a][threadIdx.x + off]);
+            }
+            scount[threadIdx.x] += scount[threadIdx.x + off];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && scount[0] > 0) {
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(&ob[a], float_to_ordered(smin[a][0]));
+            atomicMax(&ob[3 + a], float_to_ordered(smax[a][0]));
+        }
+        atomicAdd(count, scount[0]);
+    }
+}
+
+__global__ void k_knn_keys(FrameParams fp, Bufs b, lbvh::Work w, const unsigned int* ob) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixel_count(fp)) return;
+    const float4 e = b.entries[i];
+    uint64_t key = ~0ull;
+    if (e.w >= 0.0f) {
+        float lo[3], hi[3];
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = ordered_to_float(ob[a]);
+            hi[a] = ordered_to_float(ob[3 + a]);
+        }
+        key = lbvh::morton_key(lo, hi, e.x, e.y, e.z, i);
+    }
+    w.keys_in[i] = key;
+}
+
+// conservative box of an endpoint: a candidate passes dist <= radius only if
+// the query lies inside this box
+RT_D lbvh::Box entry_box(float4 e) {
+    const float h = e.w * 1.0001f + 4e-7f * (fabsf(e.x) + fabsf(e.y) + fabsf(e.z) + 1.0f);
+    lbvh::Box bx;
+    bx.lo[0] = e.x - h;
+    bx.lo[1] = e.y - h;
+    bx.lo[2] = e.z - h;
+    bx.hi[0] = e.x + h;
+    bx.hi[1] = e.y + h;
+    bx.hi[2] = e.z + h;
+    return bx;
+}
+
+__global__ void k_knn_leaves(FrameParams fp, Bufs b, lbvh::Work w, float4* leaf_entries) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *w.n) return;
+    const uint32_t pix = static_cast<uint32_t>(w.keys[i] & 0xFFFFFFFFull);
+    w.order[i] = pix;
+    const float4 e = b.entries[pix];
+    leaf_entries[i] = e;
+    w.leaf_box[i] = entry_box(e);
+}
+
+// ---- final gather -----------------------------------------------------------------------
+struct NeighborList {
+    float dist[CRISB_MAX_GATHER_M];
+    uint32_t pix[CRISB_MAX_GATHER_M];
+    uint32_t count;
+};
+
+RT_D bool knn_before(float d, uint32_t p, float d2, uint32_t p2) { return d < d2 || (d == d2 && p < p2); }
+
+// __intersection__prefix_entry (shader/prefix_search_hit.cu:9-73) over every
+// endpoint whose radius covers q; keeps the k nearest by (distance, pixel).
+RT_D void knn_query(const SceneView& s, const Bufs& b, V3 q, uint32_t k, NeighborList& nl) {
+    nl.count = 0;
+    const uint32_t n = *b.knn_n;
+    if (n == 0 || k == 0 || nonfinite(q)) return;
+    int stack[kTraversalStack];
+    int sp = 0;
+    int cur = 0;
+    uint32_t visits = 0;
+    while (true) {
+        if (++visits > kKnnMaxVisits) {
+            dev_error(s, kDevErrKnn);
+            return;
+        }
+        const BvhNode nd = b.knn_nodes[cur];
+        const bool in_l = q.x >= nd.a.x && q.y >= nd.a.y && q.z >= nd.a.z && q.x <= nd.a.w && q.y <= nd.b.x &&
+                          q.z <= nd.b.y;
+        const bool in_r = q.x >= nd.b.z && q.y >= nd.b.w && q.z >= nd.c.x && q.x <= nd.c.y && q.y <= nd.c.z &&
+                          q.z <= nd.c.w;
+        const int links[2] = {nd.d.x, nd.d.y};
+        const int counts[2] = {nd.d.z, nd.d.w};
+        bool go[2] = {in_l, in_r};
+        for (int c = 0; c < 2; ++c) {
+            if (!go[c] || links[c] >= 0) continue;
+            go[c] = false;
+            const int first = -1 - links[c];
+            for (int t = 0; t < counts[c]; ++t) {
+                const float4 e = b.knn_leaf[first + t];
+                const uint32_t j = b.knn_pixel[first + t];
+                const float d = distance(q, V3{e.x, e.y, e.z});
+                if (d > e.w) continue;
+                if (nl.count == k) {
+                    if (!knn_before(d, j, nl.dist[k - 1], nl.pix[k - 1])) continue;
+                    --nl.count;
+                }
+                uint32_t pos = nl.count;
+                while (pos > 0 && knn_before(d, j, nl.dist[pos - 1], nl.pix[pos - 1])) {
+                    nl.dist[pos] = nl.dist[pos - 1];
+                    nl.pix[pos] = nl.pix[pos - 1];
+                    --pos;
+                }
+                nl.dist[pos] = d;
+                nl.pix[pos] = j;
+                ++nl.count;
+            }
+        }
+        if (go[0] && go[1]) {
+            if (sp >= kTraversalStack) {
+                dev_error(s, kDevErrStack);
+                return;
+            }
+            stack[sp++] = links[1];
+            cur = links[0];
+        } else if (go[0]) {
+            cur = links[0];
+        } else if (go[1]) {
+            cur = links[1];
+        } else {
+            if (sp == 0) return;
+            cur = stack[--sp];
+        }
+    }
+}
+
+RT_D void write_neighbors(const FrameParams& fp, const Bufs& b, uint32_t i, const NeighborList& nl) {
+    const uint32_t k = fp.k;
+    for (uint32_t n = 0; n < k; ++n) {
+        crisb_neighbor_rec r;
+        r.pixel = n < nl.count ? nl.pix[n] : 0u;
+        r.dist = n < nl.count ? nl.dist[n] : 0.0f;
+        b.neighbors[static_cast<size_t>(i) * k + n] = r;
+    }
+    b.neigh_count[i] = nl.count;
+}
+
+// FinalGatherCanon, shader/final_gather.cu:69-188
+RT_D V3 final_gather_canon(const SceneView& s, const FrameParams& fp, const Bufs& b, uint32_t i, V3 origin, V3 dir,
+                           Rng& rng, NeighborList& nl, bool& queried) {
+    Prefix cp;
+    cp.rng = 0;
+    cp.primary = cp.recon = cp.last = Hit{CRISB_INVALID_PRIM, 0.0f, 0.0f, splat(0.0f)};
+    cp.flags = 0;
+    cp.f = cp.prf = cp.rod = splat(0.0f);
+    cp.p = cp.path_len = 0.0f;
+    trace_prefix(s, fp, cp, origin, dir, rng);
+    if (!fl_valid(cp.flags)) return splat(0.0f);
+    if (fl_nee(cp.flags)) return cp.f / cp.p;
+    Suffix cs;
+    cs.rng = 0;
+    cs.recon = cs.last_prefix = Hit{CRISB_INVALID_PRIM, 0.0f, 0.0f, splat(0.0f)};
+    cs.flags = 0;
+    cs.f = cs.prf = cs.rod = splat(0.0f);
+    cs.p = 0.0f;
+    trace_suffix(s, fp, cs, cp, rng);
+    if (!fl_valid(cs.flags)) return splat(0.0f);
+    const V3 canon_contrib = cp.f * cs.f / (cp.p * cs.p);
+    const uint32_t k = fp.k;
+    if (k == 0) return canon_contrib;
+    const Isect last = unpack(s, cs.last_prefix);
+    knn_query(s, b, last.pos, k, nl);
+    queried = true;
+    uint32_t nvalid = 0, vflags = 0;
+    for (uint32_t n = 0; n < nl.count; ++n) {
+        if (!fl_valid(b.sres_cur[nl.pix[n]].sample.flags)) continue;
+        ++nvalid;
+        vflags |= 1u << n;
+    }
+    V3 suffix_contrib = splat(0.0f);
+    const float K = static_cast<float>(nvalid);
+    float canon_mis = 1.0f;
+    for (uint32_t n = 0; n < nl.count; ++n) {
+        if (!(vflags & (1u << n))) continue;
+        const Res<Suffix> nr = ld_sres(b.sres_cur, nl.pix[n]);
+        float jac_n2c = 0.0f, jac_c2n = 0.0f;
+        const V3 f_c_of_n = shift_suffix(s, nr.s, cs, jac_n2c);
+        const V3 f_n_of_c = shift_suffix(s, cs, nr.s, jac_c2n);
+        float nmis = mis_neighbor(f_c_of_n, nr.s.f, jac_n2c, K, 1.0f, nr.conf);
+        if (nonfinite(nmis)) nmis = 0.0f;
+        const V3 contrib = nmis * f_c_of_n * nr.w_sum * jac_n2c;
+        if (!nonfinite(contrib)) suffix_contrib = suffix_contrib + contrib;
+        canon_mis += mis_canonical(cs.f, f_n_of_c, jac_c2n, K, 1.0f, nr.conf);
+    }
+    V3 gather = suffix_contrib * cp.f / cp.p;
+    gather = gather / static_cast<float>(nvalid + 1);
+    V3 result = gather + (canon_contrib * canon_mis);
+    result = result / (K + 1.0f);
+    if (nonfinite(result)) return splat(0.0f);
+    return result;
+}
+
+// FinalGatherNotCanon, shader/final_gather.cu:190-288
+RT_D V3 final_gather_not_canon(const SceneView& s, const FrameParams& fp, const Bufs& b, V3 origin, V3 dir, Rng& rng,
+                               NeighborList& nl, bool& queried) {
+    const uint32_t k = fp.k;
+    if (k == 0) return splat(0.0f);
+    Isect last;
+    last.valid = false;
+    V3 tp;
+    float pp;
+    if (!trace_prefix_for_gather(s, tp, pp, last, origin, dir, static_cast<uint32_t>(fp.p.prefix_len), rng))
+        return splat(0.0f);
+    knn_query(s, b, last.pos, k, nl);
+    queried = true;
+    uint32_t nvalid = 0, vflags = 0;
+    for (uint32_t n = 0; n < nl.count; ++n) {
+        if (!fl_valid(b.sres_cur[nl.pix[n]].sample.flags)) continue;
+        ++nvalid;
+        vflags |= 1u << n;
+    }
+    V3 suffix_contrib = splat(0.0f);
+    const float K = static_cast<float>(nvalid);
+    for (uint32_t n = 0; n < nl.count; ++n) {
+        if (!(vflags & (1u << n))) continue;
+        const Res<Suffix> nr = ld_sres(b.sres_cur, nl.pix[n]);
+        float jac_n2c = 0.0f;
+        const V3 f_c_of_n = shift_suffix(s, nr.s, last, jac_n2c);
+        float nmis = mis_neighbor(f_c_of_n, nr.s.f, jac_n2c, K, 1.0f, nr.conf);
+        if (nonfinite(nmis)) nmis = 0.0f;
+        const V3 contrib = nmis * f_c_of_n * nr.w_sum * jac_n2c;
+        if (!nonfinite(contrib)) suffix_contrib = suffix_contrib + contrib;
+    }
+    V3 result = suffix_contrib * tp / pp;
+    result = result / static_cast<float>(fp.p.gather_n);
+    result = result / (K + 1.0f);
+    if (nonfinite(result)) return splat(0.0f);
+    return result;
+}
+
+// GetRadiance + __raygen__final_gather, shader/final_gather.cu:290-356
+__global__ void __launch_bounds__(kPassBlock) k_final_gather(SceneView s, FrameParams fp, Bufs b, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixel_count(fp)) return;
+    const uint32_t x = i % fp.width, y = i / fp.width;
+    NeighborList nl;
+    nl.count = 0;
+    bool queried = false;
+    V3 L = splat(0.0f);
+    if (b.canon_prefix[i].primary.prim != CRISB_INVALID_PRIM) {
+        Rng rng{b.gbuf[i].rng};
+        const V3 dir = camera_dir(fp, x, y, rng);
+        const V3 origin = ld3(fp.cam.pos);
+        L = L + final_gather_canon(s, fp, b, i, origin, dir, rng, nl, queried);
+        for (int g = 1; g < fp.p.gather_n; ++g) L = L + final_gather_not_canon(s, fp, b, origin, dir, rng, nl, queried);
+        if (nonfinite(L)) L = splat(0.0f);
+        b.gbuf[i].rng = rng.state;
+    }
+    if (!queried) nl.count = 0;
+    if (fp.k > 0) write_neighbors(fp, b, i, nl);
+    else b.neigh_count[i] = 0;
+    store_output(fp, out, i, L);
+}
+
+inline unsigned grid_for(uint32_t n) { return (n + kPassBlock - 1) / kPassBlock; }
+
+}  // namespace
+
+void launch_prefix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, cudaStream_t st) {
+    k_prefix_gen_temp<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b, out);
+}
+void launch_prefix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, int round,
+                           cudaStream_t st) {
+    k_prefix_spatial<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b, out, round);
+}
+void launch_prefix_copy_front_back(const FrameParams& fp, const Bufs& b, cudaStream_t st) {
+    k_prefix_copy<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
+}
+void launch_suffix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st) {
+    k_suffix_gen_temp<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b);
+}
+void launch_suffix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st) {
+    k_suffix_spatial<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b);
+}
+void launch_store_entries(const SceneView& s, const FrameParams& fp, const Bufs& b, const lbvh::Work& w,
+                          unsigned int* bounds, cudaStream_t st) {
+    k_bounds_init<<<1, 32, 0, st>>>(bounds, w.n);
+    k_store_entries<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, s, bounds, w.n);
+    k_knn_keys<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, w, bounds);
+}
+void launch_knn_finish(const FrameParams& fp, const Bufs& b, const lbvh::Work& w, float4* leaf_entries,
+                       cudaStream_t st) {
+    const uint32_t P = fp.width * fp.height;
+    k_knn_leaves<<<grid_for(P), kPassBlock, 0, st>>>(fp, b, w, leaf_entries);
+    launch_lbvh_hierarchy(w, P, kKnnLeafMax, st);
+}
+void launch_lbvh_hierarchy(const lbvh::Work& w, uint32_t cap, int leaf_max, cudaStream_t st) {
+    const unsigned g = grid_for(cap > 1 ? cap : 1);
+    lbvh::k_karras<<<g, kPassBlock, 0, st>>>(w);
+    lbvh::k_refit<<<g, kPassBlock, 0, st>>>(w);
+    lbvh::k_emit<<<g, kPassBlock, 0, st>>>(w, leaf_max);
+}
+void launch_final_gather(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, cudaStream_t st) {
+    k_final_gather<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b, out);
+}
+
+}  // namespace crisb

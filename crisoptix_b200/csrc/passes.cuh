@@ -1,0 +1,52 @@
+// passes.cuh -- declarations shared by the pass kernels and the host side.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "lbvh.cuh"
+#include "rt_restir.cuh"
+
+namespace crisb {
+
+// Device buffers of one renderer.  Prefix reservoirs keep the reference's
+// front/back pair; suffix reservoirs live in two physical buffers where
+// `sres_cur` holds the state every logical copy front -> back has made equal
+// and spatial rounds write `sres_next` (then the roles swap).
+struct Bufs {
+    crisb_prefix_res_rec* pres[2];
+    crisb_prefix_rec* canon_prefix;
+    crisb_suffix_res_rec* sres_cur;
+    crisb_suffix_res_rec* sres_next;
+    crisb_suffix_res_rec* canon_suffix;  // 112-byte slots, w_sum/confidence unused
+    crisb_gbuffer_rec* gbuf;
+    crisb_neighbor_rec* neighbors;  // P * k
+    uint32_t* neigh_count;          // P
+    float4* entries;                // P: endpoint xyz + radius (w < 0: no entry)
+    // prefix-endpoint search structure (rebuilt every frame)
+    const BvhNode* knn_nodes;
+    const float4* knn_leaf;  // leaf order: endpoint xyz + radius
+    const uint32_t* knn_pixel;  // leaf order -> pixel index
+    const uint32_t* knn_n;
+};
+
+constexpr int kPassBlock = 128;
+constexpr int kKnnLeafMax = 8;
+constexpr int kTriLeafMax = 4;
+
+void launch_prefix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, cudaStream_t st);
+void launch_prefix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, int round,
+                           cudaStream_t st);
+void launch_prefix_copy_front_back(const FrameParams& fp, const Bufs& b, cudaStream_t st);
+void launch_suffix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st);
+void launch_suffix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st);
+// prefix entries, endpoint bounds/count and Morton keys (w.keys_in); the
+// caller then sorts w.keys_in into w.keys and calls launch_knn_finish
+void launch_store_entries(const SceneView& s, const FrameParams& fp, const Bufs& b, const lbvh::Work& w,
+                          unsigned int* bounds, cudaStream_t st);
+void launch_knn_finish(const FrameParams& fp, const Bufs& b, const lbvh::Work& w, float4* leaf_entries,
+                       cudaStream_t st);
+void launch_final_gather(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, cudaStream_t st);
+// generic LBVH stages over `cap` primitives (count in w.n)
+void launch_lbvh_hierarchy(const lbvh::Work& w, uint32_t cap, int leaf_max, cudaStream_t st);
+
+}  // namespace crisb

@@ -1,0 +1,263 @@
+// rt_common.cuh -- vector math, RNG and record access shared by all kernels.
+//
+// Floating-point contract: this code is compiled with -fmad=false and IEEE
+// division / square root, and every expression keeps the association order of
+// the reference's glm expressions (vec3 dot = (x + y) + z, scalar chains
+// left to right).  Together with a CPU restatement built the same way, that
+// makes discrete decisions (hits, selections, neighbours) reproducible bit
+// for bit.  Transcendentals the reference takes from glm are replaced by
+// deterministic definitions: sin/cos via Cody-Waite reduction plus Taylor
+// polynomials, pow(x, 5) via repeated squaring.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "crisb.h"
+
+#define RT_HD __host__ __device__ __forceinline__
+#define RT_D __device__ __forceinline__
+
+namespace crisb {
+
+// ---------------------------------------------------------------------------
+// float3 arithmetic in glm order
+// ---------------------------------------------------------------------------
+struct V3 {
+    float x, y, z;
+};
+
+RT_HD V3 mk(float x, float y, float z) { return V3{x, y, z}; }
+RT_HD V3 splat(float s) { return V3{s, s, s}; }
+RT_HD V3 operator+(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+RT_HD V3 operator-(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+RT_HD V3 operator*(V3 a, V3 b) { return V3{a.x * b.x, a.y * b.y, a.z * b.z}; }
+RT_HD V3 operator*(V3 a, float s) { return V3{a.x * s, a.y * s, a.z * s}; }
+RT_HD V3 operator*(float s, V3 a) { return V3{s * a.x, s * a.y, s * a.z}; }
+RT_HD V3 operator/(V3 a, float s) { return V3{a.x / s, a.y / s, a.z / s}; }
+RT_HD V3 operator-(V3 a) { return V3{-a.x, -a.y, -a.z}; }
+RT_HD float dot(V3 a, V3 b) {
+    const float x = a.x * b.x;
+    const float y = a.y * b.y;
+    const float z = a.z * b.z;
+    return (x + y) + z;
+}
+RT_HD float length(V3 v) { return sqrtf(dot(v, v)); }
+RT_HD V3 normalize(V3 v) { return v * (1.0f / sqrtf(dot(v, v))); }
+RT_HD float distance(V3 p0, V3 p1) { return length(p1 - p0); }
+RT_HD V3 reflect(V3 i, V3 n) { return i - n * dot(n, i) * 2.0f; }
+RT_HD V3 cross(V3 a, V3 b) {
+    return V3{a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y};
+}
+RT_HD float gmin(float x, float y) { return (y < x) ? y : x; }
+RT_HD float gmax(float x, float y) { return (x < y) ? y : x; }
+RT_HD V3 gmax(V3 a, V3 b) { return V3{gmax(a.x, b.x), gmax(a.y, b.y), gmax(a.z, b.z)}; }
+RT_HD float gclamp(float x, float lo, float hi) { return gmin(gmax(x, lo), hi); }
+RT_HD bool nonfinite(float v) { return isnan(v) || isinf(v); }
+RT_HD bool nonfinite(V3 v) { return nonfinite(v.x) || nonfinite(v.y) || nonfinite(v.z); }
+RT_HD bool is_zero(V3 v) { return v.x == 0.0f && v.y == 0.0f && v.z == 0.0f; }
+RT_HD float comp(V3 v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
+RT_HD V3 ld3(const float* p) { return V3{p[0], p[1], p[2]}; }
+RT_HD void st3(float* p, V3 v) {
+    p[0] = v.x;
+    p[1] = v.y;
+    p[2] = v.z;
+}
+
+// Rec.709 luminance (include/graph/luminance.h:6-9)
+RT_HD float luminance(V3 c) { return dot(c, V3{0.2126f, 0.7152f, 0.0722f}); }
+
+// sin and cos of an angle in [0, 2*pi): Cody-Waite reduction by pi/2 (two-term
+// split) and Taylor series of degree 9 (sin) and 10 (cos) on [-pi/4, pi/4],
+// each step a correctly rounded fma.  Error below 1e-7 absolute.
+RT_HD void sincos_reduced(float phi, float& s, float& c) {
+    const float q = rintf(phi * 0x1.45f306p-1f);
+    float r = fmaf(q, -0x1.921fb6p+0f, phi);
+    r = fmaf(q, 0x1.777a5cp-25f, r);
+    const float r2 = r * r;
+    float ps = fmaf(r2, 0x1.71de3ap-19f, -0x1.a01a02p-13f);
+    ps = fmaf(r2, ps, 0x1.111112p-7f);
+    ps = fmaf(r2, ps, -0x1.555556p-3f);
+    const float sn = fmaf(r * r2, ps, r);
+    float pc = fmaf(r2, -0x1.27e4fcp-22f, 0x1.a01a02p-16f);
+    pc = fmaf(r2, pc, -0x1.6c16c2p-10f);
+    pc = fmaf(r2, pc, 0x1.555556p-5f);
+    pc = fmaf(r2, pc, -0.5f);
+    const float cs = fmaf(r2, pc, 1.0f);
+    const int quadrant = static_cast<int>(q) & 3;
+    s = quadrant == 0 ? sn : (quadrant == 1 ? cs : (quadrant == 2 ? -sn : -cs));
+    c = quadrant == 0 ? cs : (quadrant == 1 ? -sn : (quadrant == 2 ? -cs : sn));
+}
+
+// ---------------------------------------------------------------------------
+// RNG: TEA-4 seeding and PCG32 on the default stream (include/util/random.h)
+// ---------------------------------------------------------------------------
+constexpr uint64_t kPcgMult = 0x5851f42d4c957f2dULL;
+constexpr uint64_t kPcgDefaultStream = 0xda3e39cb94b95bdbULL;
+constexpr uint64_t kPcgInc = (kPcgDefaultStream << 1u) | 1u;
+
+RT_HD uint64_t tea64(uint32_t v0, uint32_t v1) {
+    uint32_t s0 = 0;
+#pragma unroll
+    for (int n = 0; n < 4; n++) {
+        s0 += 0x9e3779b9u;
+        v0 += ((v1 << 4) + 0xa341316cu) ^ (v1 + s0) ^ ((v1 >> 5) + 0xc8013ea4u);
+        v1 += ((v0 << 4) + 0xad90777du) ^ (v0 + s0) ^ ((v0 >> 5) + 0x7e95761eu);
+    }
+    return static_cast<uint64_t>(v0) | (static_cast<uint64_t>(v1) << 32);
+}
+
+// PCG32 whose increment is fixed to the default stream: only the 64-bit state
+// is carried in records.
+struct Rng {
+    uint64_t state;
+
+    RT_HD uint32_t next_u32() {
+        const uint64_t old = state;
+        state = old * kPcgMult + kPcgInc;
+        const uint32_t xs = static_cast<uint32_t>(((old >> 18u) ^ old) >> 27u);
+        const uint32_t rot = static_cast<uint32_t>(old >> 59u);
+        return (xs >> rot) | (xs << ((32u - rot) & 31u));
+    }
+    RT_HD uint64_t next_u64() {
+        const uint64_t lo = next_u32();
+        const uint64_t hi = next_u32();
+        return lo | (hi << 32);
+    }
+    RT_HD float next_float() {
+        const uint32_t bits = (next_u32() >> 9) | 0x3f800000u;
+        return __uint_as_float_hd(bits) - 1.0f;
+    }
+    RT_HD static float __uint_as_float_hd(uint32_t b) {
+#ifdef __CUDA_ARCH__
+        return __uint_as_float(b);
+#else
+        float f;
+        __builtin_memcpy(&f, &b, 4);
+        return f;
+#endif
+    }
+};
+
+// PCG32(seed) with the default stream: Seed(initstate, initseq)
+RT_HD Rng rng_seeded(uint64_t initstate) {
+    Rng r{0};
+    r.next_u32();
+    r.state += initstate;
+    r.next_u32();
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// Path records in registers (FP32 layout of crisb_prefix_rec / crisb_suffix_rec)
+// ---------------------------------------------------------------------------
+struct Hit {  // PackedInteraction
+    uint32_t prim;  // CRISB_INVALID_PRIM when invalid
+    float bu, bv;
+    V3 dir;
+    RT_HD bool valid() const { return prim != CRISB_INVALID_PRIM; }
+};
+
+struct Isect {  // Interaction (position, normal and incoming direction)
+    bool valid;
+    uint32_t prim;
+    float bu, bv;
+    V3 pos, dir, nrm;
+    RT_HD Hit pack() const { return Hit{valid ? prim : CRISB_INVALID_PRIM, bu, bv, dir}; }
+};
+
+constexpr uint32_t kFlagValid = 1u << 16;
+constexpr uint32_t kFlagNee = 1u << 17;
+RT_HD uint32_t fl_len(uint32_t f) { return f & 0xFFu; }
+RT_HD uint32_t fl_recon(uint32_t f) { return (f >> 8) & 0xFFu; }
+RT_HD uint32_t fl_set_len(uint32_t f, uint32_t l) { return (f & ~0xFFu) | (l & 0xFFu); }
+RT_HD uint32_t fl_set_recon(uint32_t f, uint32_t r) { return (f & ~0xFF00u) | ((r & 0xFFu) << 8); }
+RT_HD bool fl_valid(uint32_t f) { return (f & kFlagValid) != 0; }
+RT_HD bool fl_nee(uint32_t f) { return (f & kFlagNee) != 0; }
+RT_HD uint32_t fl_set_valid(uint32_t f, bool v) { return v ? (f | kFlagValid) : (f & ~kFlagValid); }
+RT_HD uint32_t fl_set_nee(uint32_t f, bool v) { return v ? (f | kFlagNee) : (f & ~kFlagNee); }
+
+struct Prefix {
+    uint64_t rng;
+    Hit primary, recon, last;
+    uint32_t flags;
+    V3 f, prf;  // f, postReconF
+    float p, path_len;
+    V3 rod;  // reconOutDir
+};
+
+struct Suffix {
+    uint64_t rng;
+    Hit recon, last_prefix;
+    uint32_t flags;
+    V3 f, prf;
+    float p;
+    V3 rod;
+};
+
+template <typename T>
+struct Res {
+    T s;
+    float w_sum;
+    float conf;
+};
+
+// ---- record <-> register conversion -----------------------------------------
+RT_HD Hit ld_hit(const crisb_hit_rec& h) { return Hit{h.prim, h.bary[0], h.bary[1], ld3(h.in_dir)}; }
+RT_HD void st_hit(crisb_hit_rec& o, const Hit& h) {
+    o.prim = h.prim;
+    o.bary[0] = h.bu;
+    o.bary[1] = h.bv;
+    st3(o.in_dir, h.dir);
+}
+RT_HD Prefix ld_prefix(const crisb_prefix_rec& r) {
+    Prefix p;
+    p.rng = r.rng;
+    p.primary = ld_hit(r.primary);
+    p.recon = ld_hit(r.recon);
+    p.last = ld_hit(r.last);
+    p.flags = r.flags;
+    p.f = ld3(r.f);
+    p.prf = ld3(r.post_recon_f);
+    p.p = r.p;
+    p.path_len = r.path_len;
+    p.rod = ld3(r.recon_out_dir);
+    return p;
+}
+RT_HD void st_prefix(crisb_prefix_rec& r, const Prefix& p) {
+    r.rng = p.rng;
+    st_hit(r.primary, p.primary);
+    st_hit(r.recon, p.recon);
+    st_hit(r.last, p.last);
+    r.flags = p.flags;
+    st3(r.f, p.f);
+    st3(r.post_recon_f, p.prf);
+    r.p = p.p;
+    r.path_len = p.path_len;
+    st3(r.recon_out_dir, p.rod);
+}
+RT_HD Suffix ld_suffix(const crisb_suffix_rec& r) {
+    Suffix s;
+    s.rng = r.rng;
+    s.recon = ld_hit(r.recon);
+    s.last_prefix = ld_hit(r.last_prefix);
+    s.flags = r.flags;
+    s.f = ld3(r.f);
+    s.prf = ld3(r.post_recon_f);
+    s.p = r.p;
+    s.rod = ld3(r.recon_out_dir);
+    return s;
+}
+RT_HD void st_suffix(crisb_suffix_rec& r, const Suffix& s) {
+    r.rng = s.rng;
+    st_hit(r.recon, s.recon);
+    st_hit(r.last_prefix, s.last_prefix);
+    r.flags = s.flags;
+    st3(r.f, s.f);
+    st3(r.post_recon_f, s.prf);
+    r.p = s.p;
+    st3(r.recon_out_dir, s.rod);
+    r.pad = 0;
+}
+
+}  // namespace crisb

@@ -1,0 +1,489 @@
+// rt_scene.cuh -- device view of the scene: BVH traversal, surface
+// interactions, the reference BRDF and emitter sampling.
+//
+// Replaces OptiX's optixTrace + __closesthit__mesh / __miss__* programs
+// (include/graph/trace.h:25-88, shader/mesh_hit.cu:17-69, shader/miss.cu) and
+// the ggx direct callables (shader/brdf.cu:99-337).  Hit semantics: a
+// triangle is hit when tmin < t < tmax; the closest hit is the smallest t with
+// ties going to the lower triangle index, so the result does not depend on the
+// traversal order.
+#pragma once
+
+#include "rt_common.cuh"
+
+namespace crisb {
+
+// device error word bits
+constexpr int kDevErrStack = 1;
+constexpr int kDevErrIterations = 2;
+constexpr int kDevErrKnn = 4;
+
+constexpr int kTraversalStack = 64;
+// visit caps: a closest-hit query visits well under a thousand nodes; the
+// caps only bound the work of a malformed tree (the error word records it)
+constexpr uint32_t kMaxNodeVisits = 1u << 16;
+constexpr uint32_t kKnnMaxVisits = 1u << 21;
+// robust slab test: tfar *= 1 + 2*gamma(3) (Ize 2013, "Robust BVH Ray Traversal")
+constexpr float kSlabFarScale = 1.0000003576f;
+
+// BVH2 node: boxes of both children + child links.  A child link >= 0 is an
+// inner node; a negative link -1-first marks a leaf of `count` triangles
+// starting at `first` in the leaf-ordered triangle array.
+struct BvhNode {
+    float4 a;  // l.lo.xyz, l.hi.x
+    float4 b;  // l.hi.yz, r.lo.xy
+    float4 c;  // r.lo.z, r.hi.xyz
+    int4 d;    // left link, right link, left count, right count
+};
+
+struct SceneView {
+    const BvhNode* nodes;
+    const float4* tris;   // 3 per triangle in leaf order; tris[3i+2].w = triangle index bits
+    const float4* shade;  // 5 per triangle in scene order: p0 p1 p2 n0 n1 n2 material
+    const crisb_material* mats;
+    const crisb_emitter* emitters;
+    const float* emitter_faces;
+    uint32_t num_emitters;
+    uint32_t num_tris;
+    int* err;
+};
+
+struct RayPre {
+    V3 org, dir, inv;
+    int kx, ky, kz;
+    float sx, sy, sz;
+};
+
+RT_HD float rcp_box(float v) {
+    if (fabsf(v) < 1e-30f) v = copysignf(1e-30f, v);
+    return 1.0f / v;
+}
+
+RT_HD RayPre make_ray(V3 o, V3 d) {
+    RayPre r;
+    r.org = o;
+    r.dir = d;
+    const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    int kz = 0;
+    float m = ax;
+    if (ay > m) {
+        kz = 1;
+        m = ay;
+    }
+    if (az > m) kz = 2;
+    int kx = kz == 2 ? 0 : kz + 1;
+    int ky = kx == 2 ? 0 : kx + 1;
+    if (comp(d, kz) < 0.0f) {
+        const int t = kx;
+        kx = ky;
+        ky = t;
+    }
+    r.kx = kx;
+    r.ky = ky;
+    r.kz = kz;
+    const float dz = comp(d, kz);
+    r.sx = comp(d, kx) / dz;
+    r.sy = comp(d, ky) / dz;
+    r.sz = 1.0f / dz;
+    r.inv = V3{rcp_box(d.x), rcp_box(d.y), rcp_box(d.z)};
+    return r;
+}
+
+// Watertight ray/triangle test (Woop, Benthin & Wald, JCGT 2013).  u and v
+// are the barycentric weights of p1 and p2 (OptiX's convention).
+RT_HD bool intersect_tri(const RayPre& r, V3 p0, V3 p1, V3 p2, float tmin, float tmax, float& t_out,
+                         float& u_out, float& v_out) {
+    const V3 A = p0 - r.org, B = p1 - r.org, C = p2 - r.org;
+    const float akz = comp(A, r.kz), bkz = comp(B, r.kz), ckz = comp(C, r.kz);
+    const float Ax = comp(A, r.kx) - r.sx * akz;
+    const float Ay = comp(A, r.ky) - r.sy * akz;
+    const float Bx = comp(B, r.kx) - r.sx * bkz;
+    const float By = comp(B, r.ky) - r.sy * bkz;
+    const float Cx = comp(C, r.kx) - r.sx * ckz;
+    const float Cy = comp(C, r.ky) - r.sy * ckz;
+    float U = Cx * By - Cy * Bx;
+    float V = Ax * Cy - Ay * Cx;
+    float W = Bx * Ay - By * Ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = static_cast<float>(static_cast<double>(Cx) * static_cast<double>(By) -
+                               static_cast<double>(Cy) * static_cast<double>(Bx));
+        V = static_cast<float>(static_cast<double>(Ax) * static_cast<double>(Cy) -
+                               static_cast<double>(Ay) * static_cast<double>(Cx));
+        W = static_cast<float>(static_cast<double>(Bx) * static_cast<double>(Ay) -
+                               static_cast<double>(By) * static_cast<double>(Ax));
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    const float det = U + V + W;
+    if (det == 0.0f) return false;
+    const float Az = r.sz * akz;
+    const float Bz = r.sz * bkz;
+    const float Cz = r.sz * ckz;
+    const float T = U * Az + V * Bz + W * Cz;
+    const float rcp_det = 1.0f / det;
+    const float t = T * rcp_det;
+    if (!(t > tmin && t < tmax)) return false;
+    t_out = t;
+    u_out = V * rcp_det;
+    v_out = W * rcp_det;
+    return true;
+}
+
+RT_D bool slab(const RayPre& r, float lox, float loy, float loz, float hix, float hiy, float hiz, float tmin,
+               float tmax, float& tnear) {
+    float t0 = (lox - r.org.x) * r.inv.x, t1 = (hix - r.org.x) * r.inv.x;
+    float tn = fminf(t0, t1), tf = fmaxf(t0, t1);
+    t0 = (loy - r.org.y) * r.inv.y;
+    t1 = (hiy - r.org.y) * r.inv.y;
+    tn = fmaxf(tn, fminf(t0, t1));
+    tf = fminf(tf, fmaxf(t0, t1));
+    t0 = (loz - r.org.z) * r.inv.z;
+    t1 = (hiz - r.org.z) * r.inv.z;
+    tn = fmaxf(tn, fminf(t0, t1));
+    tf = fminf(tf, fmaxf(t0, t1));
+    tn = fmaxf(tn, tmin);
+    tf = fminf(tf, tmax);
+    tnear = tn;
+    return tn <= tf * kSlabFarScale;
+}
+
+struct TraceResult {
+    uint32_t prim;  // CRISB_INVALID_PRIM: miss
+    float t, u, v;
+};
+
+RT_D void dev_error(const SceneView& s, int code) {
+    if (s.err) atomicOr(s.err, code);
+}
+
+// Closest hit (any_hit == false) or first hit (any_hit == true) over the BVH.
+template <bool kAnyHit>
+RT_D TraceResult traverse(const SceneView& s, const RayPre& r, float tmin, float tmax) {
+    TraceResult best{CRISB_INVALID_PRIM, tmax, 0.0f, 0.0f};
+    if (s.num_tris == 0) return best;
+    int stack_node[kTraversalStack];
+    float stack_t[kTraversalStack];
+    int sp = 0;
+    int cur = 0;
+    uint32_t visits = 0;
+    while (true) {
+        if (++visits > kMaxNodeVisits) {
+            dev_error(s, kDevErrIterations);
+            break;
+        }
+        const BvhNode nd = s.nodes[cur];
+        const float bound = best.prim == CRISB_INVALID_PRIM ? tmax : best.t;
+        float tl, tr;
+        bool hl = slab(r, nd.a.x, nd.a.y, nd.a.z, nd.a.w, nd.b.x, nd.b.y, tmin, bound, tl);
+        bool hr = slab(r, nd.b.z, nd.b.w, nd.c.x, nd.c.y, nd.c.z, nd.c.w, tmin, bound, tr);
+        int links[2] = {nd.d.x, nd.d.y};
+        int counts[2] = {nd.d.z, nd.d.w};
+        bool hits[2] = {hl, hr};
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            if (!hits[c] || links[c] >= 0) continue;
+            hits[c] = false;
+            const int first = -1 - links[c];
+            for (int k = 0; k < counts[c]; ++k) {
+                const float4 q0 = s.tris[3 * (first + k) + 0];
+                const float4 q1 = s.tris[3 * (first + k) + 1];
+                const float4 q2 = s.tris[3 * (first + k) + 2];
+                const uint32_t prim = __float_as_uint(q2.w);
+                float t, u, v;
+                if (!intersect_tri(r, V3{q0.x, q0.y, q0.z}, V3{q1.x, q1.y, q1.z}, V3{q2.x, q2.y, q2.z}, tmin, tmax,
+                                   t, u, v))
+                    continue;
+                if (kAnyHit) {
+                    best.prim = prim;
+                    best.t = t;
+                    return best;
+                }
+                if (best.prim == CRISB_INVALID_PRIM || t < best.t || (t == best.t && prim < best.prim)) {
+                    best.prim = prim;
+                    best.t = t;
+                    best.u = u;
+                    best.v = v;
+                }
+            }
+        }
+        if (hits[0] && hits[1]) {
+            const bool left_first = tl <= tr;
+            const int near_c = left_first ? links[0] : links[1];
+            const int far_c = left_first ? links[1] : links[0];
+            if (sp >= kTraversalStack) {
+                dev_error(s, kDevErrStack);
+                break;
+            }
+            stack_node[sp] = far_c;
+            stack_t[sp] = left_first ? tr : tl;
+            ++sp;
+            cur = near_c;
+            continue;
+        }
+        if (hits[0]) {
+            cur = links[0];
+            continue;
+        }
+        if (hits[1]) {
+            cur = links[1];
+            continue;
+        }
+        // pop, skipping entries now beyond the closest hit
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            const float bnd = best.prim == CRISB_INVALID_PRIM ? tmax : best.t;
+            if (stack_t[sp] <= bnd * kSlabFarScale) {
+                cur = stack_node[sp];
+                found = true;
+                break;
+            }
+        }
+        if (!found) break;
+    }
+    return best;
+}
+
+// ---- interactions -------------------------------------------------------------
+struct ShadeTri {
+    V3 p0, p1, p2, n0, n1, n2;
+    uint32_t mat;
+};
+
+RT_D ShadeTri load_shade(const SceneView& s, uint32_t prim) {
+    const float4* q = s.shade + 5 * static_cast<size_t>(prim);
+    const float4 a = q[0], b = q[1], c = q[2], d = q[3], e = q[4];
+    ShadeTri t;
+    t.p0 = V3{a.x, a.y, a.z};
+    t.p1 = V3{a.w, b.x, b.y};
+    t.p2 = V3{b.z, b.w, c.x};
+    t.n0 = V3{c.y, c.z, c.w};
+    t.n1 = V3{d.x, d.y, d.z};
+    t.n2 = V3{d.w, e.x, e.y};
+    t.mat = __float_as_uint(e.z);
+    return t;
+}
+
+// InterpolateBary (include/graph/Interaction.h:18-25)
+RT_HD V3 interp(float bu, float bv, V3 v0, V3 v1, V3 v2) {
+    return ((1.0f - bu - bv) * v0) + (bu * v1) + (bv * v2);
+}
+
+// optixTrace + __closesthit__mesh / __miss__main: interaction with the
+// normalised interpolated normal.  On a miss only valid and dir change.
+RT_D void trace_closest(const SceneView& s, V3 o, V3 d, float tmin, float tmax, Isect& it) {
+    const RayPre r = make_ray(o, d);
+    const TraceResult h = traverse<false>(s, r, tmin, tmax);
+    it.dir = d;
+    if (h.prim == CRISB_INVALID_PRIM) {
+        it.valid = false;
+        return;
+    }
+    it.valid = true;
+    it.prim = h.prim;
+    it.bu = h.u;
+    it.bv = h.v;
+    const ShadeTri t = load_shade(s, h.prim);
+    it.pos = interp(it.bu, it.bv, t.p0, t.p1, t.p2);
+    it.nrm = normalize(interp(it.bu, it.bv, t.n0, t.n1, t.n2));
+}
+
+// TraceOcclusion (include/graph/trace.h:64-88)
+RT_D bool occluded(const SceneView& s, V3 o, V3 d, float tmin, float tmax) {
+    const RayPre r = make_ray(o, d);
+    return traverse<true>(s, r, tmin, tmax).prim != CRISB_INVALID_PRIM;
+}
+
+// Interaction(PackedInteraction, transforms) (include/graph/Interaction.h:115-172):
+// interpolated position and unnormalised normal.
+RT_D Isect unpack(const SceneView& s, const Hit& h) {
+    Isect it;
+    it.valid = h.valid() && h.prim < s.num_tris;
+    it.prim = h.prim;
+    it.bu = h.bu;
+    it.bv = h.bv;
+    it.dir = h.dir;
+    it.pos = splat(0.0f);
+    it.nrm = splat(0.0f);
+    if (!it.valid) return it;
+    const ShadeTri t = load_shade(s, h.prim);
+    it.pos = interp(it.bu, it.bv, t.p0, t.p1, t.p2);
+    it.nrm = interp(it.bu, it.bv, t.n0, t.n1, t.n2);
+    return it;
+}
+
+RT_D uint32_t material_of(const SceneView& s, uint32_t prim) {
+    return __float_as_uint(__ldg(&s.shade[5 * static_cast<size_t>(prim) + 4].z));
+}
+
+// ---- BRDF (shader/brdf.cu) ---------------------------------------------------------
+constexpr float kPi = 3.14159265358979323846264f;
+
+struct BrdfEval {
+    V3 brdf;
+    float pdf;
+    V3 emission;
+    float roughness;
+};
+struct BrdfSample {
+    V3 dir;
+    V3 brdf;
+    float pdf;
+    float roughness;
+};
+struct MatVals {
+    V3 diff, f0, emission;
+    float rough;
+};
+
+RT_D MatVals mat_vals(const crisb_material& m) {
+    MatVals v;
+    v.diff = V3{m.diffuse[0], m.diffuse[1], m.diffuse[2]};
+    V3 f0 = V3{m.specular[0], m.specular[1], m.specular[2]};
+    float rough = m.roughness;
+    float metal = 0.0f;
+    if (m.spec_usage == CRISB_SPEC_OCC_ROUGH_METAL) {
+        rough = f0.y;
+        metal = f0.z;
+        f0 = splat(1.0f);
+    }
+    v.f0 = v.diff * (1.0f - metal) + f0 * metal;  // glm::mix
+    v.emission = V3{m.emission[0], m.emission[1], m.emission[2]};
+    v.rough = rough;
+    return v;
+}
+
+RT_D float pow5(float x) {
+    const float x2 = x * x;
+    return x2 * x2 * x;
+}
+RT_D float d_ggx(float ndoth, float rough) {
+    const float a2 = rough * rough;
+    const float d = (ndoth * a2 - ndoth) * ndoth + 1.0f;
+    return a2 / (kPi * d * d);
+}
+RT_D float v_smith(float ndotl, float ndotv, float rough) {
+    const float a2 = rough * rough;
+    const float lv = ndotl * sqrtf(ndotv * ndotv * (1 - a2) + a2);
+    const float ll = ndotv * sqrtf(ndotl * ndotl * (1 - a2) + a2);
+    return 0.5f / (lv + ll);
+}
+RT_D V3 fresnel(V3 f0, float vdoth) { return f0 + (splat(1.0f) - f0) * pow5(gmax(0.0f, 1.0f - vdoth)); }
+RT_D float diff_prob(const MatVals& m) {
+    const float sd = dot(m.diff, splat(1.0f));
+    return sd / (dot(m.diff, splat(1.0f)) + dot(m.f0, splat(1.0f)));
+}
+
+// brdf * cos and the mixture pdf shared by eval and sample
+RT_D void brdf_value(const MatVals& m, V3 nrm, V3 view, V3 light, float ndotl, float ndotv, float dprob, V3& brdf,
+                     float& pdf) {
+    const V3 diff_brdf = m.diff / kPi;
+    V3 spec = splat(0.0f);
+    const V3 h = normalize(light + view);
+    const float ndoth = dot(h, nrm);
+    const float ldoth = dot(h, light);
+    if (static_cast<double>(dot(m.f0, m.f0)) > 1e-6) {
+        const float d = d_ggx(ndoth, m.rough);
+        const float v = v_smith(ndotl, ndotv, m.rough);
+        const V3 f = fresnel(m.f0, ldoth);
+        spec = d * v * f;
+    }
+    brdf = (diff_brdf + spec) * ndotl;
+    pdf = dprob * ndotl / kPi + (1.0f - dprob) * d_ggx(ndoth, m.rough) * ndoth / (4.0f * ldoth);
+}
+
+// __direct_callable__ggx_eval, shader/brdf.cu:115-190
+RT_D BrdfEval brdf_eval(const SceneView& s, const Isect& it, V3 out_dir) {
+    BrdfEval r;
+    r.brdf = splat(0.0f);
+    r.pdf = 0.0f;
+    r.emission = splat(0.0f);
+    r.roughness = 0.0f;
+    const MatVals m = mat_vals(s.mats[material_of(s, it.prim)]);
+    const V3 view = -it.dir;
+    const float ndotv = dot(it.nrm, view);
+    const float ndotl = dot(it.nrm, out_dir);
+    if (ndotv <= 0.0f || ndotl < 0.0f) return r;
+    brdf_value(m, it.nrm, view, out_dir, ndotl, ndotv, diff_prob(m), r.brdf, r.pdf);
+    r.emission = m.emission;
+    r.roughness = m.rough;
+    return r;
+}
+
+// ComputeLocalFrame (shader/brdf.cu:192-212) applied to a local vector
+RT_D V3 local_to_world(V3 z, V3 v) {
+    const float sz = (z.z >= 0) ? 1.0f : -1.0f;
+    const float a = 1 / (sz + z.z);
+    const float ya = z.y * a;
+    const float b = z.x * ya;
+    const float c = z.x * sz;
+    const V3 X = V3{c * z.x * a - 1, sz * b, c};
+    const V3 Y = V3{b, z.y * ya - sz, z.y};
+    return V3{X.x * v.x + Y.x * v.y + z.x * v.z, X.y * v.x + Y.y * v.y + z.y * v.z,
+              X.z * v.x + Y.z * v.y + z.z * v.z};
+}
+
+// __direct_callable__ggx_sample, shader/brdf.cu:214-337
+RT_D BrdfSample brdf_sample(const SceneView& s, const Isect& it, Rng& rng) {
+    const MatVals m = mat_vals(s.mats[material_of(s, it.prim)]);
+    BrdfSample r;
+    r.roughness = m.rough;
+    r.dir = splat(0.0f);
+    r.brdf = splat(0.0f);
+    r.pdf = 0.0f;
+    const V3 nrm = it.nrm;
+    const V3 view = -it.dir;
+    const float ndotv = dot(nrm, view);
+    if (ndotv <= 0) return r;
+    const float dprob = diff_prob(m);
+    V3 dir;
+    if (rng.next_float() < dprob) {
+        const float phi = rng.next_float() * 2.0f * kPi;
+        const float rr = sqrtf(rng.next_float());
+        float sp, cp;
+        sincos_reduced(phi, sp, cp);
+        const float x = rr * cp;
+        const float y = rr * sp;
+        const float z = sqrtf(gclamp(1.0f - x * x - y * y, 0.0f, 1.0f));
+        dir = local_to_world(nrm, V3{x, y, z});
+    } else {
+        const float u = rng.next_float();
+        const float mz = sqrtf(gclamp((1 - u) / (1 + (m.rough * m.rough - 1) * u), 0, 1));
+        const float mr = sqrtf(gclamp(1 - mz * mz, 0, 1));
+        const float phi = rng.next_float() * 2.0f * kPi;
+        float sp, cp;
+        sincos_reduced(phi, sp, cp);
+        dir = reflect(it.dir, local_to_world(nrm, V3{mr * cp, mr * sp, mz}));
+        if (dot(dir, nrm) < 0.0f) return r;
+    }
+    const float ndotl = dot(nrm, dir);
+    r.dir = dir;
+    brdf_value(m, nrm, view, dir, ndotl, ndotv, dprob, r.brdf, r.pdf);
+    return r;
+}
+
+// ---- emitters (include/graph/sample_emitter.h, include/model/Emitter.h:21-54) ----
+struct EmitterSample {
+    V3 pos;
+    V3 color;
+};
+
+RT_D EmitterSample sample_emitter(const SceneView& s, Rng& rng) {
+    const uint64_t ei = rng.next_u64() % static_cast<uint64_t>(s.num_emitters);
+    const crisb_emitter e = s.emitters[ei];
+    const uint64_t fi = rng.next_u64() % static_cast<uint64_t>(e.num_faces);
+    const float* f = s.emitter_faces + 9 * (static_cast<size_t>(e.first_face) + fi);
+    const V3 v0 = V3{f[0], f[1], f[2]}, v1 = V3{f[3], f[4], f[5]}, v2 = V3{f[6], f[7], f[8]};
+    float r0 = rng.next_float();
+    float r1 = rng.next_float();
+    float r2 = rng.next_float();
+    const float rsum = r0 + r1 + r2;
+    r0 /= rsum;
+    r1 /= rsum;
+    r2 /= rsum;
+    EmitterSample es;
+    es.pos = r0 * v0 + r1 * v1 + r2 * v2;
+    es.color = V3{e.color[0], e.color[1], e.color[2]};
+    return es;
+}
+
+}  // namespace crisb

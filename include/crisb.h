@@ -1,0 +1,348 @@
+/*
+ * crisb.h -- C ABI of the B200-native Conditional ReSTIR PT frame loop.
+ *
+ * This is the drop-in boundary for CrisOptix's per-frame render path.  The
+ * reference exposes it as C++ classes bound to OptiX:
+ *   Scene(OptixDeviceContext, instances, emitters)   include/model/Scene.h:12-24
+ *   Camera(pos, viewDir, up, aspect, fov)             include/graph/Camera.h:24-79
+ *   Renderer(w, h, ctx, Camera&, const Scene&)        include/graph/Renderer.h:11-21
+ *   Renderer::LaunchFrame(glm::vec3* outputBuffer)    src/Renderer.cpp:209-406
+ *   Renderer::GetFrameIdx()                           src/Renderer.cpp:408-411
+ *   LaunchParams / RestirParams                       include/graph/LaunchParams.h:11-36,
+ *                                                     include/graph/restir/RestirParams.h:11-59
+ * Here the same roles are plain C entry points with plain pointers and sizes:
+ * opaque handles own all device memory, every call returns a status code
+ * (0 = ok, negative = error; nothing throws across the ABI), and the frame is
+ * stream-ordered on the caller's CUDA stream with no host synchronisation.
+ *
+ * Record layouts (crisb_*_rec) are the FP32 storage layout of the device
+ * buffers; the debug read-back entry points return them in this layout for
+ * either storage mode.
+ */
+#ifndef CRISB_H
+#define CRISB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define CRISB_OK 0
+#define CRISB_ERR_INVALID_ARGUMENT (-1)
+#define CRISB_ERR_OUT_OF_MEMORY (-2)
+#define CRISB_ERR_CUDA (-3)
+#define CRISB_ERR_QUEUE_OVERFLOW (-4)
+#define CRISB_ERR_DEVICE_TIMEOUT (-5)
+#define CRISB_ERR_NOT_SUPPORTED (-6)
+#define CRISB_ERR_DEVICE_FAULT (-7)
+
+/* ---- enums (values match the reference's enums) ------------------------ */
+/* RendererType, include/graph/restir/settings.h:5-10 */
+#define CRISB_RENDERER_PATH_TRACER 0
+#define CRISB_RENDERER_RESTIR_PT 1
+#define CRISB_RENDERER_CONDITIONAL_RESTIR 2
+/* PrefixRadiusType, include/graph/restir/settings.h:15-19 */
+#define CRISB_RADIUS_CONSTANT 0
+#define CRISB_RADIUS_PATH_LENGTH 1
+/* SpecTexUsage, include/model/Material.h:9-13 */
+#define CRISB_SPEC_COLOR 0
+#define CRISB_SPEC_OCC_ROUGH_METAL 1
+/* reservoir / path-record storage (stands in for config.h USE_CUDA_F16) */
+#define CRISB_STORAGE_FP32 0
+#define CRISB_STORAGE_FP16 1
+
+/* MAX_SPATIAL_NEIGH_COUNT, include/graph/restir/settings.h:24 */
+#define CRISB_MAX_SPATIAL_NEIGH 16
+/* gatherM is clamped to [1, 32] by the reference UI (src/Renderer.cpp:462) */
+#define CRISB_MAX_GATHER_M 32
+/* CONFIDENCE_MAX, include/graph/restir/Reservoir.h:6 */
+#define CRISB_CONFIDENCE_MAX 50.0f
+/* invalid hit marker in crisb_hit_rec.prim */
+#define CRISB_INVALID_PRIM 0xFFFFFFFFu
+
+/* ---- scene description ------------------------------------------------- */
+/* MaterialSbtData without textures (include/model/Material.h:15-32).
+ * specular is the reference's specF0 input; with spec_usage == COLOR the
+ * reference replaces it by mix(diffuse, specular, 0) = diffuse
+ * (shader/brdf.cu:124-138), and this library does the same. */
+typedef struct crisb_material {
+    float diffuse[3];
+    float specular[3];
+    float emission[3];
+    float roughness;
+    int32_t spec_usage;
+    int32_t reserved;
+} crisb_material;
+
+/* A contiguous triangle range of the scene's triangle array. */
+typedef struct crisb_mesh {
+    uint32_t first_triangle;
+    uint32_t num_triangles;
+} crisb_mesh;
+
+/* ModelInstance(model, transform) (include/model/ModelInstance.h:9).
+ * transform is row-major 3x4 (object -> world).  material_override >= 0
+ * replaces the mesh material for this instance (-1: keep).  Instances are
+ * flattened into world-space triangles when the scene is created. */
+typedef struct crisb_instance {
+    uint32_t mesh;
+    int32_t material_override;
+    float transform[12];
+} crisb_instance;
+
+/* Emitter(mesh, transform, color) (include/model/Emitter.h:57-71): a colour
+ * and a run of world-space faces in crisb_scene_desc.emitter_faces. */
+typedef struct crisb_emitter {
+    float color[3];
+    uint32_t first_face;
+    uint32_t num_faces;
+} crisb_emitter;
+
+typedef struct crisb_scene_desc {
+    const float* positions;         /* num_vertices * 3 */
+    const float* normals;           /* num_vertices * 3, or NULL (face normals) */
+    uint32_t num_vertices;
+    const uint32_t* indices;        /* num_triangles * 3 */
+    const uint32_t* triangle_material; /* num_triangles */
+    uint32_t num_triangles;
+    const crisb_material* materials;
+    uint32_t num_materials;
+    const crisb_mesh* meshes;       /* may be NULL when num_instances == 0 */
+    uint32_t num_meshes;
+    const crisb_instance* instances; /* NULL/0: triangles are world space */
+    uint32_t num_instances;
+    const crisb_emitter* emitters;
+    uint32_t num_emitters;
+    const float* emitter_faces;     /* num_emitter_faces * 9 (v0,v1,v2) */
+    uint32_t num_emitter_faces;
+} crisb_scene_desc;
+
+/* ---- camera (Camera, include/graph/Camera.h:24-79) --------------------- */
+typedef struct crisb_camera {
+    float pos[3];
+    float view_dir[3];
+    float up[3];
+    float aspect;
+    float fov;      /* radians, full vertical field of view */
+    int32_t changed; /* Camera::HasChanged(): resets frameIdx */
+} crisb_camera;
+
+/* CameraData after Camera::GetData (src/Camera.cpp:20-32) */
+typedef struct crisb_camera_data {
+    float pos[3];
+    float u[3];
+    float v[3];
+    float w[3];
+} crisb_camera_data;
+
+/* ---- parameters (RestirParams + LaunchParams knobs) --------------------- */
+typedef struct crisb_params {
+    int32_t renderer_type;
+    float nee_prob;
+    int32_t max_path_len;
+    int32_t enable_accum;
+    float recon_min_roughness;
+    float recon_min_distance;
+    int32_t prefix_len;
+    int32_t prefix_enable_temporal;
+    int32_t prefix_enable_spatial;
+    int32_t prefix_spatial_count;
+    int32_t prefix_spatial_rounds;
+    int32_t suffix_enable_temporal;
+    int32_t suffix_enable_spatial;
+    int32_t suffix_spatial_count;
+    int32_t suffix_spatial_rounds;
+    int32_t gather_n;
+    int32_t gather_m;
+    float gather_radius;
+    int32_t gather_radius_type;
+    int32_t window_radius; /* WINDOW_RADIUS, include/graph/restir/path_gen.h:12 */
+    int32_t storage;       /* CRISB_STORAGE_* */
+    int32_t reserved;
+    uint64_t seed;         /* replaces std::random_device (src/Renderer.cpp:9-11) */
+} crisb_params;
+
+/* ---- FP32 record layouts (device storage and debug read-back) ----------- */
+/* PackedInteraction (include/graph/Interaction.h:59-86) with the mesh SBT
+ * pointer and instance id folded into a global triangle index. */
+typedef struct crisb_hit_rec {
+    uint32_t prim;      /* CRISB_INVALID_PRIM when !valid */
+    float bary[2];
+    float in_dir[3];
+} crisb_hit_rec;
+
+/* PrefixPath (include/graph/restir/PrefixPath.h:7-41); rng is PCG32::state
+ * (the stream increment is always the default stream). */
+typedef struct crisb_prefix_rec {
+    uint64_t rng;
+    crisb_hit_rec primary;
+    crisb_hit_rec recon;
+    crisb_hit_rec last;
+    uint32_t flags; /* 0:8 length, 8:16 reconIdx, bit16 valid, bit17 nee */
+    float f[3];
+    float post_recon_f[3];
+    float p;
+    float path_len;
+    float recon_out_dir[3];
+} crisb_prefix_rec;
+
+/* Reservoir<PrefixPath> (include/graph/restir/Reservoir.h:8-51) */
+typedef struct crisb_prefix_res_rec {
+    crisb_prefix_rec sample;
+    float w_sum;
+    float confidence;
+    uint32_t pad[2];
+} crisb_prefix_res_rec;
+
+/* SuffixPath (include/graph/restir/SuffixPath.h:9-36) */
+typedef struct crisb_suffix_rec {
+    uint64_t rng;
+    crisb_hit_rec recon;
+    crisb_hit_rec last_prefix;
+    uint32_t flags; /* 0:8 length, 8:16 reconIdx, bit16 valid */
+    float f[3];
+    float post_recon_f[3];
+    float p;
+    float recon_out_dir[3];
+    uint32_t pad;
+} crisb_suffix_rec;
+
+typedef struct crisb_suffix_res_rec {
+    crisb_suffix_rec sample;
+    float w_sum;
+    float confidence;
+} crisb_suffix_res_rec;
+
+/* RestirGBuffer (include/graph/restir/RestirGBuffer.h:5-28) */
+typedef struct crisb_gbuffer_rec {
+    uint64_t rng;
+    uint32_t prev_xy;  /* x | y << 16 */
+    uint32_t flags;    /* bit0 primaryIntValid */
+} crisb_gbuffer_rec;
+
+/* PrefixNeighbor (include/graph/restir/PrefixAccelStruct.h:8-27) */
+typedef struct crisb_neighbor_rec {
+    uint32_t pixel;
+    float dist;
+} crisb_neighbor_rec;
+
+/* closest-hit query result (debug / traversal tests) */
+typedef struct crisb_trace_hit {
+    uint32_t prim;
+    float t;
+    float u;
+    float v;
+} crisb_trace_hit;
+
+/* per-pass device time of the last frame (ImGui panel, src/Renderer.cpp:472-485) */
+typedef struct crisb_stats {
+    float prefix_gen_temp_ms;
+    float prefix_spatial_ms;
+    float suffix_gen_temp_ms;
+    float suffix_spatial_ms;
+    float prefix_store_ms;
+    float final_gather_ms;
+    float total_ms;
+    uint32_t kernel_launches;
+} crisb_stats;
+
+/* debug buffer ids for crisb_debug_read */
+#define CRISB_BUF_PREFIX_RES_FRONT 0
+#define CRISB_BUF_PREFIX_RES_BACK 1
+#define CRISB_BUF_CANON_PREFIX 2
+#define CRISB_BUF_SUFFIX_RES_FRONT 3
+#define CRISB_BUF_SUFFIX_RES_BACK 4
+#define CRISB_BUF_CANON_SUFFIX 5
+#define CRISB_BUF_GBUFFER 6
+#define CRISB_BUF_NEIGHBORS 7      /* W*H*k crisb_neighbor_rec */
+#define CRISB_BUF_NEIGHBOR_COUNT 8 /* W*H uint32 (final-gather canonical query) */
+
+typedef struct crisb_scene crisb_scene;
+typedef struct crisb_renderer crisb_renderer;
+
+/* ---- entry points -------------------------------------------------------- */
+/* Library version string. */
+const char* crisb_version(void);
+
+/* Message of the last failing call on this thread. */
+int crisb_last_error(char* buf, size_t len);
+
+/* Reference defaults of Renderer::Renderer (src/Renderer.cpp:34-58);
+ * reconMinDistance = 0.01 * scene_size. */
+int crisb_params_default(crisb_params* out, float scene_size);
+
+/* Camera::GetData (src/Camera.cpp:20-32). */
+int crisb_camera_get_data(const crisb_camera* cam, crisb_camera_data* out);
+
+/* Scene::Scene + BuildAccel + BuildEmitterTable (src/Scene.cpp:4-13,73-204):
+ * flattens instances, builds the device BVH on the current CUDA device. */
+int crisb_scene_create(const crisb_scene_desc* desc, crisb_scene** out);
+int crisb_scene_destroy(crisb_scene* scene);
+/* Scene::GetSceneSize (src/Scene.cpp:48-71). */
+int crisb_scene_size(const crisb_scene* scene, float* out);
+/* number of world-space triangles after flattening */
+int crisb_scene_num_triangles(const crisb_scene* scene, uint32_t* out);
+/* read back flattened world-space positions (ntri*9), normals (ntri*9) and
+ * materials (ntri) in original triangle order; any pointer may be NULL. */
+int crisb_scene_read_triangles(const crisb_scene* scene, float* positions,
+                               float* normals, uint32_t* materials);
+
+/* Closest-hit (any_hit == 0) or occlusion (any_hit != 0) query over the
+ * scene BVH for n rays given as device arrays; ray k is
+ * rays[8k..8k+7] = (ox, oy, oz, tmin, dx, dy, dz, tmax).  Hits are written
+ * to the device array hits (occlusion: prim = 1 occluded, 0 free). */
+int crisb_trace_rays(const crisb_scene* scene, const float* rays_dev,
+                     crisb_trace_hit* hits_dev, uint32_t n, int any_hit,
+                     void* stream);
+
+/* Renderer::Renderer (src/Renderer.cpp:13-200). */
+int crisb_renderer_create(const crisb_scene* scene, uint32_t width,
+                          uint32_t height, const crisb_params* params,
+                          crisb_renderer** out);
+int crisb_renderer_destroy(crisb_renderer* r);
+int crisb_renderer_set_params(crisb_renderer* r, const crisb_params* params);
+int crisb_renderer_get_params(const crisb_renderer* r, crisb_params* out);
+
+/* Renderer::LaunchFrame (src/Renderer.cpp:209-406): one frame of the pass
+ * chain on `stream` (a cudaStream_t, NULL = legacy default stream).
+ * out_rgb_dev is a caller-owned device buffer of width*height*3 floats,
+ * row-major, y down; written in place (blended when enable_accum). */
+int crisb_render_frame(crisb_renderer* r, const crisb_camera* cam,
+                       float* out_rgb_dev, void* stream);
+
+/* Renderer::GetFrameIdx (src/Renderer.cpp:408-411). */
+int crisb_frame_index(const crisb_renderer* r, uint64_t* out);
+/* per-frame random value the last frame used (params.random) */
+int crisb_frame_random(const crisb_renderer* r, uint32_t* out);
+
+/* Enable per-pass CUDA-event timing (adds events to the stream). */
+int crisb_set_timing(crisb_renderer* r, int enable);
+/* Per-pass times of the last frame; synchronises on its stop event. */
+int crisb_get_stats(crisb_renderer* r, crisb_stats* out);
+
+/* Device error word (traversal stack overflow, kNN overflow, ...); reading
+ * synchronises the renderer's last stream.  Returns CRISB_OK or the error. */
+int crisb_check_device_errors(crisb_renderer* r);
+
+/* Copy an internal buffer (CRISB_BUF_*) to host memory in the FP32 record
+ * layout.  bytes must equal the buffer size; synchronises the device. */
+int crisb_debug_read(crisb_renderer* r, int buffer_id, void* host_dst,
+                     size_t bytes);
+/* Size in bytes of an internal buffer in the FP32 record layout. */
+int crisb_debug_size(const crisb_renderer* r, int buffer_id, size_t* out);
+
+/* sizeof of every public struct, in declaration order (material, mesh,
+ * instance, emitter, scene_desc, camera, camera_data, params, hit_rec,
+ * prefix_rec, prefix_res_rec, suffix_rec, suffix_res_rec, gbuffer_rec,
+ * neighbor_rec, trace_hit, stats) -- lets bindings check their layouts.
+ * Writes up to n values; returns the number of structs. */
+int crisb_abi_sizes(uint32_t* out, uint32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CRISB_H */

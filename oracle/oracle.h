@@ -1,0 +1,70 @@
+/*
+ * oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * C API of the CPU restatement of CrisOptix's Conditional ReSTIR PT frame
+ * loop (oracle/restir_oracle.cpp).  It is the checker for the CUDA product:
+ * only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
+ * load it.  The product never links or calls it.
+ */
+#ifndef CRISB_ORACLE_H
+#define CRISB_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "crisb.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oracle_ctx oracle_ctx;
+
+/* Scene as world-space triangle soup: tri_pos / tri_nrm hold 9 floats per
+ * triangle (three corners), tri_mat one material index per triangle. */
+oracle_ctx* oracle_create(const float* tri_pos, const float* tri_nrm,
+                          const uint32_t* tri_mat, uint32_t num_tris,
+                          const crisb_material* mats, uint32_t num_mats,
+                          const crisb_emitter* emitters, uint32_t num_emitters,
+                          const float* emitter_faces, uint32_t num_faces,
+                          uint32_t width, uint32_t height,
+                          const crisb_params* params);
+void oracle_destroy(oracle_ctx* ctx);
+int oracle_set_params(oracle_ctx* ctx, const crisb_params* params);
+int oracle_set_threads(int n);
+float oracle_scene_size(const oracle_ctx* ctx);
+
+/* One Renderer::LaunchFrame; out_rgb is W*H*3 floats, read-modify-write. */
+int oracle_render_frame(oracle_ctx* ctx, const crisb_camera* cam, float* out_rgb);
+/* Same, with per-pass wall times (ms) written to pass_ms[6]. */
+int oracle_render_frame_timed(oracle_ctx* ctx, const crisb_camera* cam,
+                              float* out_rgb, double* pass_ms);
+uint64_t oracle_frame_index(const oracle_ctx* ctx);
+uint32_t oracle_frame_random(const oracle_ctx* ctx);
+/* Copy internal state in the crisb_*_rec layout (CRISB_BUF_* ids). */
+int oracle_dump(const oracle_ctx* ctx, int buffer_id, void* dst, size_t bytes);
+size_t oracle_dump_size(const oracle_ctx* ctx, int buffer_id);
+
+/* ray k = rays[8k..8k+7] = (ox, oy, oz, tmin, dx, dy, dz, tmax) */
+int oracle_trace(const oracle_ctx* ctx, const float* rays, crisb_trace_hit* hits,
+                 uint32_t n, int any_hit);
+int oracle_trace_bruteforce(const oracle_ctx* ctx, const float* rays,
+                            crisb_trace_hit* hits, uint32_t n, int any_hit);
+
+/* Plain path tracer (TraceCompletePath) accumulated in FP64: adds `spp`
+ * frames (frame randoms from `seed`) into accum (W*H*3 doubles). */
+int oracle_pt_accumulate(oracle_ctx* ctx, const crisb_camera* cam, uint32_t spp,
+                         uint64_t seed, double* accum);
+
+/* unit-level helpers for known-answer tests */
+void oracle_pcg32(uint64_t initstate, uint64_t initseq, uint32_t n, uint32_t* out);
+uint64_t oracle_tea64(uint32_t v0, uint32_t v1);
+void oracle_sincos(const float* phi, uint32_t n, float* s, float* c);
+int oracle_camera_data(const crisb_camera* cam, crisb_camera_data* out);
+uint32_t oracle_frame_random_for(uint64_t seed, uint64_t frame_counter);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,80 @@
+"""Frame-loop properties of the oracle (CPU): determinism, thread
+independence, reservoir invariants, and estimator sanity."""
+import numpy as np
+import pytest
+
+import oracle_py as op
+from crisoptix_b200 import _abi, scenes
+from helpers import large_config_params, make_params, orbit, scene_size_of, small_config_params, \
+    small_sphere_room, static
+
+BUFS = [_abi.BUF_PREFIX_RES_FRONT, _abi.BUF_PREFIX_RES_BACK, _abi.BUF_CANON_PREFIX, _abi.BUF_SUFFIX_RES_FRONT,
+        _abi.BUF_CANON_SUFFIX, _abi.BUF_GBUFFER, _abi.BUF_NEIGHBORS, _abi.BUF_NEIGHBOR_COUNT]
+
+
+def run(desc, cam, params, W, H, frames, cam_fn=static, threads=None):
+    if threads:
+        op.set_threads(threads)
+    o = op.Oracle.from_scene(desc, W, H, params)
+    out = np.zeros((H, W, 3), np.float32)
+    for f in range(frames):
+        o.render_frame(cam_fn(cam, f), out)
+    state = {b: o.dump(b) for b in BUFS}
+    return out, state
+
+
+def test_deterministic_and_thread_independent():
+    desc, cam = scenes.cornell_box()
+    p = small_config_params(scene_size_of(desc), gather_m=5, gather_radius=0.3)
+    a, sa = run(desc, cam, p, 40, 32, 3, threads=1)
+    b, sb = run(desc, cam, p, 40, 32, 3, threads=8)
+    assert a.tobytes() == b.tobytes()
+    for k in BUFS:
+        assert sa[k].tobytes() == sb[k].tobytes(), k
+
+
+def test_reservoir_invariants_large_config():
+    desc, cam = small_sphere_room()
+    p = large_config_params(scene_size_of(desc), gather_radius=0.3)
+    out, st = run(desc, cam, p, 48, 48, 3, cam_fn=lambda c, f: orbit(c, f, 240))
+    assert np.isfinite(out).all() and (out >= 0).all()
+    sr = st[_abi.BUF_SUFFIX_RES_FRONT]
+    assert (sr["confidence"] <= 50.0).all() and (sr["w_sum"] >= 0).all()
+    valid = (sr["sample"]["flags"] >> 16) & 1
+    assert valid.mean() > 0.1
+    nc = st[_abi.BUF_NEIGHBOR_COUNT]
+    assert nc.max() <= 8 and nc.mean() > 0.1
+    nb = st[_abi.BUF_NEIGHBORS].reshape(-1, 8)
+    for i in np.nonzero(nc > 1)[0][:200]:
+        d = nb[i, : nc[i]]["dist"]
+        assert (np.diff(d) >= 0).all()
+
+
+@pytest.mark.parametrize("rtype", [_abi.PATH_TRACER, _abi.RESTIR_PT, _abi.CONDITIONAL_RESTIR])
+def test_renderer_types_produce_finite_images(rtype):
+    desc, cam = scenes.cornell_box()
+    p = make_params(scene_size_of(desc), renderer_type=rtype, max_path_len=4, prefix_spatial_count=2,
+                    prefix_enable_spatial=1 if rtype == _abi.RESTIR_PT else 0, gather_m=3, gather_radius=0.2)
+    out, _ = run(desc, cam, p, 32, 32, 2)
+    assert np.isfinite(out).all() and out.mean() > 0.1
+
+
+def test_progressive_accumulation_matches_fp64_sum():
+    # PathTracer mode with enable_accum blends frame k with weight 1/(k+1)
+    # (final_gather.cu:346-355); its result must track an FP64 average of the
+    # same per-frame samples (same TEA/PCG streams, same frame randoms).
+    # (RestirPt is not compared with the path tracer: the reference's forced
+    # NEE at the last prefix vertex still multiplies p by neeProb,
+    # path_gen.h:145-149, so its target differs.)
+    desc, cam = scenes.cornell_box()
+    W = H = 24
+    p = make_params(scene_size_of(desc), renderer_type=_abi.PATH_TRACER, max_path_len=4, enable_accum=1, seed=9)
+    o = op.Oracle.from_scene(desc, W, H, p)
+    out = np.zeros((H, W, 3), np.float32)
+    for f in range(64):
+        o.render_frame(static(cam, f), out)
+    acc = np.zeros((H, W, 3), np.float64)
+    o.pt_accumulate(cam, 64, 9, acc)
+    # a fresh renderer starts at frameIdx 1 (blend 1/2 against the zero
+    # buffer), so after 64 frames the buffer holds (s_0 + ... + s_63) / 65
+    np.testing.assert_allclose(out, acc / 65.0, rtol=1e-4, atol=1e-5)

@@ -1,0 +1,116 @@
+"""GPU parity: the CUDA frame loop against the oracle, through the C ABI.
+
+Discrete state (hit triangle ids, reconnection indices, flags, reservoir
+selections, neighbour lists, RNG states) must match bit for bit; so do all
+floating-point record fields and the image, because both sides evaluate the
+same IEEE operations in the same order.  The image check also states the
+value tolerance the frame loop promises (1e-4 relative).
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle_py as op
+from crisoptix_b200 import Renderer, Scene, _abi, scenes
+from helpers import first_mismatch, large_config_params, make_params, orbit, random_rays, scene_size_of, \
+    small_config_params, small_sphere_room, static
+
+pytestmark = pytest.mark.gpu
+
+STATE_BUFS = [_abi.BUF_PREFIX_RES_FRONT, _abi.BUF_PREFIX_RES_BACK, _abi.BUF_CANON_PREFIX, _abi.BUF_SUFFIX_RES_FRONT,
+              _abi.BUF_CANON_SUFFIX, _abi.BUF_GBUFFER, _abi.BUF_NEIGHBORS, _abi.BUF_NEIGHBOR_COUNT]
+RTOL = 1e-4
+
+
+def gpu_trace(scene: Scene, rays: np.ndarray, any_hit: bool) -> np.ndarray:
+    r = torch.from_numpy(np.ascontiguousarray(rays, np.float32)).cuda()
+    h = torch.zeros((len(rays), 4), dtype=torch.int32, device="cuda")
+    scene.trace(r.data_ptr(), h.data_ptr(), len(rays), any_hit)
+    torch.cuda.synchronize()
+    return h.cpu().numpy().view(_abi.TRACE_HIT_DTYPE).reshape(-1)
+
+
+@pytest.mark.parametrize("which", ["cornell", "spheres"])
+def test_traversal_hits_bit_exact(cuda_device, which):
+    desc = scenes.cornell_box()[0] if which == "cornell" else small_sphere_room()[0]
+    sc = Scene(desc)
+    tri = sc.read_triangles()
+    o = op.Oracle.from_scene(desc, 4, 4, make_params(sc.scene_size), triangles=tri)
+    rays = random_rays(desc, 1 << 15, seed=3)
+    g, c = gpu_trace(sc, rays, False), o.trace(rays)
+    assert (g["prim"] != _abi.INVALID_PRIM).mean() > 0.5
+    assert first_mismatch(g, c) is None, first_mismatch(g, c)
+    rays[:, 7] = np.random.default_rng(4).uniform(0.01, 3.0, len(rays))
+    assert gpu_trace(sc, rays, True).tobytes() == o.trace(rays, any_hit=True).tobytes()
+
+
+def test_flattened_instances_match_float64_reference(cuda_device):
+    desc, _ = small_sphere_room()
+    pos, nrm, mat = Scene(desc).read_triangles()
+    rp, rn, rm = desc.flatten()
+    np.testing.assert_allclose(pos, rp, rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose(nrm, rn, rtol=1e-5, atol=1e-5)
+    assert (mat == rm).all()
+
+
+def run_parity(desc, cam, params, W, H, frames, cam_fn, change_params=None):
+    sc = Scene(desc)
+    tri = sc.read_triangles()
+    o = op.Oracle.from_scene(desc, W, H, params, triangles=tri)
+    r = Renderer(W, H, sc, params)
+    out_d = torch.zeros(H * W * 3, dtype=torch.float32, device="cuda")
+    out_h = np.zeros((H, W, 3), np.float32)
+    for f in range(frames):
+        if change_params and f in change_params:
+            params = change_params[f]
+            r.params = params
+            o.set_params(params)
+        c = cam_fn(cam, f)
+        r.launch_frame(c, out_d.data_ptr())
+        torch.cuda.synchronize()
+        o.render_frame(c, out_h)
+        r.check_device_errors()
+        assert r.get_frame_idx() == o.frame_index() and r.frame_random() == o.frame_random()
+        for b in STATE_BUFS:
+            g, c2 = r.debug_read(b), o.dump(b)
+            mm = first_mismatch(g, c2)
+            assert mm is None, f"frame {f} buffer {b}: first mismatch at {mm}"
+        img = out_d.cpu().numpy().reshape(H, W, 3)
+        np.testing.assert_allclose(img, out_h, rtol=RTOL, atol=1e-6)
+        assert img.tobytes() == out_h.tobytes()
+    return out_h
+
+
+def test_small_config_cornell_conditional_restir(cuda_device):
+    desc, cam = scenes.cornell_box()
+    p = small_config_params(scene_size_of(desc))
+    out = run_parity(desc, cam, p, 64, 64, 4, static)
+    assert out.mean() > 0.5
+
+
+def test_cornell_with_endpoint_search(cuda_device):
+    desc, cam = scenes.cornell_box()
+    p = small_config_params(scene_size_of(desc), gather_m=9, gather_radius=0.5, gather_n=2)
+    run_parity(desc, cam, p, 48, 40, 3, static)
+
+
+def test_large_config_reduced_scene_orbit(cuda_device):
+    desc, cam = small_sphere_room()
+    p = large_config_params(scene_size_of(desc), gather_radius=0.3)
+    run_parity(desc, cam, p, 64, 48, 4, lambda c, f: orbit(c, f, 120))
+
+
+@pytest.mark.parametrize("rtype", [_abi.PATH_TRACER, _abi.RESTIR_PT])
+def test_other_renderer_types(cuda_device, rtype):
+    desc, cam = scenes.cornell_box()
+    p = make_params(scene_size_of(desc), renderer_type=rtype, max_path_len=5, prefix_enable_spatial=1,
+                    prefix_spatial_count=3, prefix_spatial_rounds=2, enable_accum=1)
+    run_parity(desc, cam, p, 40, 40, 3, static)
+
+
+def test_param_change_between_frames(cuda_device):
+    desc, cam = scenes.cornell_box()
+    p0 = small_config_params(scene_size_of(desc))
+    p1 = small_config_params(scene_size_of(desc), gather_m=4, gather_radius=0.4, suffix_spatial_rounds=2,
+                             prefix_enable_spatial=1, prefix_spatial_count=2)
+    run_parity(desc, cam, p0, 32, 32, 4, static, change_params={2: p1})
