@@ -96,6 +96,8 @@ def first_mismatch(a: np.ndarray, b: np.ndarray):
     """Index and field name of the first bytewise difference of two record
     arrays, or None."""
     assert a.dtype == b.dtype and a.shape == b.shape
+    if a.size == 0:
+        return None
     ab = a.view(np.uint8).reshape(len(a), -1)
     bb = b.view(np.uint8).reshape(len(b), -1)
     bad = np.nonzero((ab != bb).any(axis=1))[0]
