@@ -83,6 +83,13 @@ def pass_bytes(k: int, spatial_count: int, spatial_rounds: int, copy_prefix_back
             "prefix_store": store, "final_gather": gather}
 
 
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
+# dominant kernel from one ncu capture, with the pixel count it was taken at;
+# scaled by pixels to the bench resolution.  Source:
+# profiles/k_final_gather_large_480x270.md
+PROFILED_TRAFFIC = {"final_gather": (97.639424e6 + 7.392e6, 480 * 270)}
+
+
 class ClockSampler:
     """nvidia-smi sampling of SM clocks and throttle reasons."""
 
@@ -204,6 +211,8 @@ def run_crisb(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     desc, cam, W, H, ppp = workload(args.workload)
+    if args.res:
+        W, H = (int(v) for v in args.res.lower().split("x"))
     sc = Scene(desc)
     p = params_for(args.workload, sc.scene_size)
     r = Renderer(W, H, sc, p)
@@ -291,8 +300,12 @@ def run_crisb(args):
     dom = max(pass_ms, key=pass_ms.get)
     dom_bytes = pb[dom] * W * H
     achieved = dom_bytes / (pass_ms[dom] / 1000.0) / 1e9
+    traffic = None
+    if dom in PROFILED_TRAFFIC:
+        tb, tpx = PROFILED_TRAFFIC[dom]
+        traffic = tb * (W * H) / tpx
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": dom, "peak_kind": f"{peak_kind} copy bandwidth",
+                "traffic": traffic, "kernel": dom, "peak_kind": f"{peak_kind} copy bandwidth",
                 "algorithmic_bytes_per_launch": dom_bytes, "pass_ms": pass_ms}
     if dist:
         dist.destroy_process_group()
@@ -325,6 +338,7 @@ def main():
     ap.add_argument("--workload", default="large", choices=["large", "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-scale", type=int, default=2)
+    ap.add_argument("--res", default=None, help="WxH override of the workload resolution (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
