@@ -116,6 +116,9 @@ crisb_camera_data camera_data(const crisb_camera& c) {
 
 }  // namespace
 
+// shared by the other translation units of the library
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
 __global__ void k_tri_keys(const float* pos, uint32_t n, float3 lo, float3 hi, uint64_t* keys) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;

@@ -313,15 +313,6 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_spatial(SceneView s, Fram
     st_sres(b.sres_next, i, cur);
 }
 
-// ---- prefix entries and the endpoint search structure ---------------------------
-RT_D unsigned int float_to_ordered(float f) {
-    const unsigned int u = __float_as_uint(f);
-    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
-RT_D float ordered_to_float(unsigned int u) {
-    return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
-}
-
 __global__ void k_bounds_init(unsigned int* ob, uint32_t* n) {
     if (threadIdx.x < 3) ob[threadIdx.x] = float_to_ordered(INFINITY);
     else if (threadIdx.x < 6) ob[threadIdx.x] = float_to_ordered(-INFINITY);
@@ -395,20 +386,6 @@ __global__ void k_knn_keys(FrameParams fp, Bufs b, lbvh::Work w, const unsigned 
     w.keys_in[i] = key;
 }
 
-// conservative box of an endpoint: a candidate passes dist <= radius only if
-// the query lies inside this box
-RT_D lbvh::Box entry_box(float4 e) {
-    const float h = e.w * 1.0001f + 4e-7f * (fabsf(e.x) + fabsf(e.y) + fabsf(e.z) + 1.0f);
-    lbvh::Box bx;
-    bx.lo[0] = e.x - h;
-    bx.lo[1] = e.y - h;
-    bx.lo[2] = e.z - h;
-    bx.hi[0] = e.x + h;
-    bx.hi[1] = e.y + h;
-    bx.hi[2] = e.z + h;
-    return bx;
-}
-
 __global__ void k_knn_leaves(FrameParams fp, Bufs b, lbvh::Work w, float4* leaf_entries) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= *w.n) return;
@@ -420,79 +397,6 @@ __global__ void k_knn_leaves(FrameParams fp, Bufs b, lbvh::Work w, float4* leaf_
 }
 
 // ---- final gather -----------------------------------------------------------------------
-struct NeighborList {
-    float dist[CRISB_MAX_GATHER_M];
-    uint32_t pix[CRISB_MAX_GATHER_M];
-    uint32_t count;
-};
-
-RT_D bool knn_before(float d, uint32_t p, float d2, uint32_t p2) { return d < d2 || (d == d2 && p < p2); }
-
-// __intersection__prefix_entry (shader/prefix_search_hit.cu:9-73) over every
-// endpoint whose radius covers q; keeps the k nearest by (distance, pixel).
-RT_D void knn_query(const SceneView& s, const Bufs& b, V3 q, uint32_t k, NeighborList& nl) {
-    nl.count = 0;
-    const uint32_t n = *b.knn_n;
-    if (n == 0 || k == 0 || nonfinite(q)) return;
-    int stack[kTraversalStack];
-    int sp = 0;
-    int cur = 0;
-    uint32_t visits = 0;
-    while (true) {
-        if (++visits > kKnnMaxVisits) {
-            dev_error(s, kDevErrKnn);
-            return;
-        }
-        const BvhNode nd = b.knn_nodes[cur];
-        const bool in_l = q.x >= nd.a.x && q.y >= nd.a.y && q.z >= nd.a.z && q.x <= nd.a.w && q.y <= nd.b.x &&
-                          q.z <= nd.b.y;
-        const bool in_r = q.x >= nd.b.z && q.y >= nd.b.w && q.z >= nd.c.x && q.x <= nd.c.y && q.y <= nd.c.z &&
-                          q.z <= nd.c.w;
-        const int links[2] = {nd.d.x, nd.d.y};
-        const int counts[2] = {nd.d.z, nd.d.w};
-        bool go[2] = {in_l, in_r};
-        for (int c = 0; c < 2; ++c) {
-            if (!go[c] || links[c] >= 0) continue;
-            go[c] = false;
-            const int first = -1 - links[c];
-            for (int t = 0; t < counts[c]; ++t) {
-                const float4 e = b.knn_leaf[first + t];
-                const uint32_t j = b.knn_pixel[first + t];
-                const float d = distance(q, V3{e.x, e.y, e.z});
-                if (d > e.w) continue;
-                if (nl.count == k) {
-                    if (!knn_before(d, j, nl.dist[k - 1], nl.pix[k - 1])) continue;
-                    --nl.count;
-                }
-                uint32_t pos = nl.count;
-                while (pos > 0 && knn_before(d, j, nl.dist[pos - 1], nl.pix[pos - 1])) {
-                    nl.dist[pos] = nl.dist[pos - 1];
-                    nl.pix[pos] = nl.pix[pos - 1];
-                    --pos;
-                }
-                nl.dist[pos] = d;
-                nl.pix[pos] = j;
-                ++nl.count;
-            }
-        }
-        if (go[0] && go[1]) {
-            if (sp >= kTraversalStack) {
-                dev_error(s, kDevErrStack);
-                return;
-            }
-            stack[sp++] = links[1];
-            cur = links[0];
-        } else if (go[0]) {
-            cur = links[0];
-        } else if (go[1]) {
-            cur = links[1];
-        } else {
-            if (sp == 0) return;
-            cur = stack[--sp];
-        }
-    }
-}
-
 RT_D void write_neighbors(const FrameParams& fp, const Bufs& b, uint32_t i, const NeighborList& nl) {
     const uint32_t k = fp.k;
     for (uint32_t n = 0; n < k; ++n) {
@@ -528,7 +432,7 @@ RT_D V3 final_gather_canon(const SceneView& s, const FrameParams& fp, const Bufs
     const uint32_t k = fp.k;
     if (k == 0) return canon_contrib;
     const Isect last = unpack(s, cs.last_prefix);
-    knn_query(s, b, last.pos, k, nl);
+    knn_query(b.knn(), s.err, last.pos, k, nl);
     queried = true;
     uint32_t nvalid = 0, vflags = 0;
     for (uint32_t n = 0; n < nl.count; ++n) {
@@ -570,7 +474,7 @@ RT_D V3 final_gather_not_canon(const SceneView& s, const FrameParams& fp, const 
     float pp;
     if (!trace_prefix_for_gather(s, tp, pp, last, origin, dir, static_cast<uint32_t>(fp.p.prefix_len), rng))
         return splat(0.0f);
-    knn_query(s, b, last.pos, k, nl);
+    knn_query(b.knn(), s.err, last.pos, k, nl);
     queried = true;
     uint32_t nvalid = 0, vflags = 0;
     for (uint32_t n = 0; n < nl.count; ++n) {

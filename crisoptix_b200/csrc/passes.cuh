@@ -3,7 +3,7 @@
 
 #include <cuda_runtime.h>
 
-#include "lbvh.cuh"
+#include "knn.cuh"
 #include "rt_restir.cuh"
 
 namespace crisb {
@@ -27,6 +27,8 @@ struct Bufs {
     const float4* knn_leaf;  // leaf order: endpoint xyz + radius
     const uint32_t* knn_pixel;  // leaf order -> pixel index
     const uint32_t* knn_n;
+
+    RT_HD KnnView knn() const { return KnnView{knn_nodes, knn_leaf, knn_pixel, knn_n}; }
 };
 
 constexpr int kPassBlock = 128;

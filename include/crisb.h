@@ -298,6 +298,22 @@ int crisb_trace_rays(const crisb_scene* scene, const float* rays_dev,
                      crisb_trace_hit* hits_dev, uint32_t n, int any_hit,
                      void* stream);
 
+/* Prefix-endpoint neighbour search as one operation: the rebuild of
+ * PrefixAccelStruct (src/PrefixAccelStruct.cpp:14-221) over caller-given
+ * entries plus the __intersection__prefix_entry query
+ * (shader/prefix_search_hit.cu:9-73) for a batch of points.
+ * entries_dev: n_entries float4 (x, y, z, radius) in device memory, 16-byte
+ * aligned; an entry with radius < 0 (or non-finite) is absent.
+ * queries_dev: n_queries float triples.  For query q, out_dev[q*k .. q*k+k)
+ * receives the k nearest entries j with |p_j - q| <= radius_j, ordered by
+ * (distance, entry index), unused slots zeroed; count_dev[q] their number.
+ * k in [1, 31].  Scratch comes from the stream-ordered allocator
+ * (cudaMallocAsync / cudaFreeAsync on `stream`); the call is asynchronous. */
+int crisb_endpoint_search(const float* entries_dev, uint32_t n_entries,
+                          const float* queries_dev, uint32_t n_queries,
+                          uint32_t k, crisb_neighbor_rec* out_dev,
+                          uint32_t* count_dev, void* stream);
+
 /* Renderer::Renderer (src/Renderer.cpp:13-200). */
 int crisb_renderer_create(const crisb_scene* scene, uint32_t width,
                           uint32_t height, const crisb_params* params,
