@@ -158,6 +158,7 @@ ENTRY_POINTS = {
     "crisb_debug_size": (c_i32, [c_vp, c_i32, ctypes.POINTER(ctypes.c_size_t)]),
     "crisb_abi_sizes": (c_i32, [ctypes.POINTER(c_u32), c_u32]),
     "crisb_endpoint_search": (c_i32, [c_vp, c_u32, c_vp, c_u32, c_u32, c_vp, c_vp, c_vp]),
+    "crisb_endpoint_search_noalloc": (c_i32, [c_vp, c_u32, c_vp, c_u32, c_u32, c_vp, c_vp, c_vp]),
 }
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libcrisb.so")

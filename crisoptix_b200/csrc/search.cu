@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "knn.cuh"
@@ -241,5 +242,70 @@ extern "C" int crisb_endpoint_search(const float* entries_dev, uint32_t n_entrie
     if (e != cudaSuccess || e2 != cudaSuccess)
         return search::fail(CRISB_ERR_CUDA, std::string("endpoint search: ") +
                                                 cudaGetErrorString(e != cudaSuccess ? e : e2));
+    return CRISB_OK;
+}
+
+// ---- allocation-free variant -------------------------------------------------------
+// Scratch for crisb_endpoint_search_noalloc: one static device array that
+// every GPU loading this library holds until the process exits.  Host code
+// only sees a stand-in symbol for it; its device address comes from
+// cudaGetSymbolAddress, looked up once per device.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 8u << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_base[kMaxDevices] = {};
+
+// device address of the scratch array on the current device (first call per
+// device does the lookup and checks that the largest accepted search fits)
+int noalloc_scratch(void** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return search::fail(CRISB_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return search::fail(CRISB_ERR_NOT_SUPPORTED, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_base[dev]) {
+        const size_t need = search::layout(CRISB_NOALLOC_MAX_ENTRIES,
+                                           search::sort_temp_bytes(CRISB_NOALLOC_MAX_ENTRIES), nullptr, nullptr);
+        if (need > kNoAllocScratchBytes)
+            return search::fail(CRISB_ERR_NOT_SUPPORTED, "endpoint search (no-alloc): scratch array too small");
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return search::fail(CRISB_ERR_CUDA,
+                                std::string("endpoint search (no-alloc): cudaGetSymbolAddress: ") +
+                                    cudaGetErrorString(e));
+        g_noalloc_base[dev] = p;
+    }
+    *out = g_noalloc_base[dev];
+    return CRISB_OK;
+}
+
+}  // namespace
+
+extern "C" int crisb_endpoint_search_noalloc(const float* entries_dev, uint32_t n_entries, const float* queries_dev,
+                                             uint32_t n_queries, uint32_t k, crisb_neighbor_rec* out_dev,
+                                             uint32_t* count_dev, void* stream) {
+    int rc = search::validate(entries_dev, n_entries, queries_dev, n_queries, k, out_dev, count_dev);
+    if (rc != CRISB_OK) return rc;
+    if (n_entries > CRISB_NOALLOC_MAX_ENTRIES)
+        return search::fail(CRISB_ERR_INVALID_ARGUMENT,
+                            "endpoint search (no-alloc): n_entries " + std::to_string(n_entries) +
+                                " exceeds the maximum " + std::to_string(CRISB_NOALLOC_MAX_ENTRIES));
+    void* base = nullptr;
+    rc = noalloc_scratch(&base);
+    if (rc != CRISB_OK) return rc;
+    const size_t sort_bytes = search::sort_temp_bytes(n_entries);
+    if (search::layout(n_entries, sort_bytes, nullptr, nullptr) > kNoAllocScratchBytes)
+        return search::fail(CRISB_ERR_NOT_SUPPORTED, "endpoint search (no-alloc): scratch does not fit");
+    search::Scratch s;
+    search::layout(n_entries, sort_bytes, static_cast<char*>(base), &s);
+    const cudaError_t e = search::run(s, reinterpret_cast<const float4*>(entries_dev), n_entries, queries_dev,
+                                      n_queries, k, out_dev, count_dev, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess)
+        return search::fail(CRISB_ERR_CUDA, std::string("endpoint search (no-alloc): ") + cudaGetErrorString(e));
     return CRISB_OK;
 }

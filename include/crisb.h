@@ -314,6 +314,29 @@ int crisb_endpoint_search(const float* entries_dev, uint32_t n_entries,
                           uint32_t k, crisb_neighbor_rec* out_dev,
                           uint32_t* count_dev, void* stream);
 
+/* Largest n_entries crisb_endpoint_search_noalloc accepts. */
+#define CRISB_NOALLOC_MAX_ENTRIES 32768u
+
+/* The same search as crisb_endpoint_search for callers that must not
+ * allocate device memory while they run -- for example an engine that
+ * reserves its whole device-memory budget at start-up and forbids allocation
+ * during a frame (an allocation can synchronise the device and its latency
+ * is unbounded), or a plugin host that gives its plugins no allocator.  It
+ * has no counterpart in the reference.  It calls no allocator: its scratch is
+ * one static 8 MiB device array in the library, held by every GPU that loads
+ * the library until the process exits.  n_entries above
+ * CRISB_NOALLOC_MAX_ENTRIES returns CRISB_ERR_INVALID_ARGUMENT.  All calls
+ * share that array (it keeps the last call's contents; each call clears what
+ * it needs), so calls that overlap on the GPU -- on different streams, or
+ * from different host threads -- race and corrupt each other's results:
+ * serialise them.  The first call on each device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture. */
+int crisb_endpoint_search_noalloc(const float* entries_dev, uint32_t n_entries,
+                                  const float* queries_dev, uint32_t n_queries,
+                                  uint32_t k, crisb_neighbor_rec* out_dev,
+                                  uint32_t* count_dev, void* stream);
+
 /* Renderer::Renderer (src/Renderer.cpp:13-200). */
 int crisb_renderer_create(const crisb_scene* scene, uint32_t width,
                           uint32_t height, const crisb_params* params,
