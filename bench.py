@@ -272,14 +272,14 @@ def run_crisb(args):
     # ---- end to end through the C ABI with host buffers ------------------------
     host = torch.empty(W * H * 3, dtype=torch.float32, pin_memory=True)
     e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e_steps = max(3, args.steps // 2)
+    e_steps = args.steps  # the same frames of the orbit as the device-resident loop
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     e_start.record(stream)
     with torch.cuda.stream(stream):
         for i in range(e_steps):
-            frame(n_frames + n_pass + i)
+            frame(args.warmup + i)
             host.copy_(out, non_blocking=True)
     e_end.record(stream)
     torch.cuda.synchronize()

@@ -473,6 +473,10 @@ struct crisb_renderer {
     DevBuf<crisb_neighbor_rec> neighbors;
     DevBuf<uint32_t> neigh_count;
     DevBuf<float4> entries, knn_leaf;
+    DevBuf<uint32_t> pass_status, pass_flags, spatial_nbr, job_items, job_count;
+    DevBuf<float4> shift_out, gather_state;
+    DevBuf<crisb_suffix_res_rec> gather_cs;
+    uint32_t slots = 0;
     DevBuf<unsigned int> bounds;
     DevBuf<char> sort_temp;
     LbvhStorage knn;
@@ -501,6 +505,15 @@ struct crisb_renderer {
         b.knn_leaf = knn_leaf.p;
         b.knn_pixel = knn.order.p;
         b.knn_n = knn.n.p;
+        b.pass_status = pass_status.p;
+        b.pass_flags = pass_flags.p;
+        b.spatial_nbr = spatial_nbr.p;
+        b.job_items = job_items.p;
+        b.job_count = job_count.p;
+        b.shift_out = shift_out.p;
+        b.gather_cs = gather_cs.p;
+        b.gather_state = gather_state.p;
+        b.slots = slots;
         return b;
     }
 
@@ -509,8 +522,28 @@ struct crisb_renderer {
             if (e) cudaEventDestroy(e);
     }
 
+    // job slots per pixel of the split suffix passes: two shifts per neighbour
+    static uint32_t slots_for(const crisb_params& q) {
+        const uint32_t m = static_cast<uint32_t>(std::max(std::max(q.gather_m - 1, q.suffix_spatial_count), 1));
+        return 2 * m;
+    }
+
+    void allocate_jobs() {
+        const size_t p = P();
+        slots = slots_for(params);
+        spatial_nbr.alloc(p * (slots / 2));
+        job_items.alloc(p * slots);
+        shift_out.alloc(p * slots);
+    }
+
     void allocate() {
         const uint32_t p = P();
+        pass_status.alloc(p);
+        pass_flags.alloc(p);
+        job_count.alloc(1);
+        gather_cs.alloc(p);
+        gather_state.alloc(2 * static_cast<size_t>(p));
+        allocate_jobs();
         for (int i = 0; i < 2; ++i) {
             pres[i].alloc(p);
             sres[i].alloc(p);
@@ -590,12 +623,12 @@ struct crisb_renderer {
         record(2, st);
         if (type == CRISB_RENDERER_CONDITIONAL_RESTIR) {
             launch_suffix_gen_temp(s, fp, bufs(), st);
-            ++launches;
+            launches += 3;
             record(3, st);
             if (params.suffix_enable_spatial && params.suffix_spatial_count > 0) {
                 for (int r = 0; r < params.suffix_spatial_rounds; ++r) {
                     launch_suffix_spatial(s, fp, bufs(), st);
-                    ++launches;
+                    launches += 3;
                     scur ^= 1;
                 }
             }
@@ -609,8 +642,13 @@ struct crisb_renderer {
             launch_knn_finish(fp, bufs(), w, knn_leaf.p, st);
             launches += 3 + 4;  // own kernels; the radix sort's library kernels are not counted
             record(5, st);
-            launch_final_gather(s, fp, bufs(), out, st);
-            ++launches;
+            if (params.gather_n == 1) {
+                launch_final_gather_split(s, fp, bufs(), out, st);
+                launches += 3;
+            } else {
+                launch_final_gather(s, fp, bufs(), out, st);
+                ++launches;
+            }
         } else {
             record(3, st);
             record(4, st);
@@ -725,7 +763,7 @@ int crisb_renderer_create(const crisb_scene* scene, uint32_t width, uint32_t hei
         require(scene && params && out, "null argument");
         *out = nullptr;
         require(width > 0 && height > 0 && width < 65536 && height < 65536, "renderer: bad resolution");
-        require(static_cast<uint64_t>(width) * height < (1ull << 31), "renderer: too many pixels");
+        require(static_cast<uint64_t>(width) * height < (1ull << 26), "renderer: too many pixels (max 2^26)");
         validate_params(*params);
         int dev = 0;
         check(cudaGetDevice(&dev), "cudaGetDevice");
@@ -750,12 +788,14 @@ int crisb_renderer_set_params(crisb_renderer* r, const crisb_params* params) {
         require(r && params, "null argument");
         validate_params(*params);
         const bool realloc_neighbors = params->gather_m != r->params.gather_m;
+        const bool realloc_jobs = crisb_renderer::slots_for(*params) != r->slots;
         r->params = *params;
+        if (realloc_neighbors || realloc_jobs) check(cudaDeviceSynchronize(), "sync");
         if (realloc_neighbors) {
-            check(cudaDeviceSynchronize(), "sync");
             r->neighbors.alloc(static_cast<size_t>(r->P()) * std::max<uint32_t>(r->K(), 1));
             check(cudaMemset(r->neighbors.p, 0, r->neighbors.bytes()), "memset");
         }
+        if (realloc_jobs) r->allocate_jobs();
     });
 }
 

@@ -4,50 +4,11 @@
 // pixel, records loaded whole, updated with the reference's in-place field
 // semantics, and stored whole.
 #define CRISB_LBVH_KERNELS 1
-#include "passes.cuh"
+#include "records.cuh"
 
 namespace crisb {
 
 namespace {
-
-RT_D uint32_t pixel_count(const FrameParams& fp) { return fp.width * fp.height; }
-
-RT_D Res<Prefix> ld_pres(const crisb_prefix_res_rec* p, uint32_t i) {
-    const crisb_prefix_res_rec r = p[i];
-    return Res<Prefix>{ld_prefix(r.sample), r.w_sum, r.confidence};
-}
-RT_D void st_pres(crisb_prefix_res_rec* p, uint32_t i, const Res<Prefix>& r) {
-    crisb_prefix_res_rec o;
-    st_prefix(o.sample, r.s);
-    o.w_sum = r.w_sum;
-    o.confidence = r.conf;
-    o.pad[0] = 0;
-    o.pad[1] = 0;
-    p[i] = o;
-}
-RT_D Res<Suffix> ld_sres(const crisb_suffix_res_rec* p, uint32_t i) {
-    const crisb_suffix_res_rec r = p[i];
-    return Res<Suffix>{ld_suffix(r.sample), r.w_sum, r.confidence};
-}
-RT_D void st_sres(crisb_suffix_res_rec* p, uint32_t i, const Res<Suffix>& r) {
-    crisb_suffix_res_rec o;
-    st_suffix(o.sample, r.s);
-    o.w_sum = r.w_sum;
-    o.confidence = r.conf;
-    p[i] = o;
-}
-
-RT_D void store_output(const FrameParams& fp, float* out, uint32_t i, V3 radiance) {
-    V3 v = radiance;
-    if (fp.p.enable_accum) {
-        const V3 old = V3{out[3 * i], out[3 * i + 1], out[3 * i + 2]};
-        const float blend = 1.0f / static_cast<float>(fp.frame_idx + 1);
-        v = blend * radiance + (1.0f - blend) * old;
-    }
-    out[3 * i] = v.x;
-    out[3 * i + 1] = v.y;
-    out[3 * i + 2] = v.z;
-}
 
 // PrefixGenTempReuse, shader/prefix_gen_temp_reuse.cu:11-98
 RT_D bool prefix_gen_temp_reuse(const SceneView& s, const FrameParams& fp, const Bufs& b, uint32_t i, V3 origin,
@@ -187,130 +148,6 @@ __global__ void k_prefix_copy(FrameParams fp, Bufs b) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pixel_count(fp)) return;
     b.pres[fp.back][i] = b.pres[fp.front][i];
-}
-
-RT_D void invalidate(Res<Suffix>& r) {
-    r.w_sum = 0.0f;
-    r.conf = 0.0f;
-    r.s.flags = fl_set_valid(r.s.flags, false);
-}
-
-// SuffixGenTempReuse + raygen, shader/suffix_gen_temp_reuse.cu:12-134.  The
-// suffix buffer is updated in place: front and back hold equal content at
-// pass start and the pass ends with front copied to back.
-__global__ void __launch_bounds__(kPassBlock) k_suffix_gen_temp(SceneView s, FrameParams fp, Bufs b) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= pixel_count(fp)) return;
-    Res<Suffix> cur = ld_sres(b.sres_cur, i);
-    const Prefix prefix = ld_prefix(b.pres[fp.front][i].sample);
-    if (!fl_valid(prefix.flags) || fl_nee(prefix.flags)) {
-        invalidate(cur);
-        st_sres(b.sres_cur, i, cur);
-        return;
-    }
-    Rng rng{b.gbuf[i].rng};
-    Suffix canon = ld_suffix(b.canon_suffix[i].sample);
-    trace_suffix(s, fp, canon, prefix, rng);
-    {
-        crisb_suffix_res_rec o;
-        st_suffix(o.sample, canon);
-        o.w_sum = 0.0f;
-        o.confidence = 0.0f;
-        b.canon_suffix[i] = o;
-    }
-    if (!fl_valid(canon.flags)) {
-        invalidate(cur);
-        st_sres(b.sres_cur, i, cur);
-        b.gbuf[i].rng = rng.state;
-        return;
-    }
-    const float canon_phat = luminance(canon.f);
-    const Res<Suffix> prev = cur;  // back[prevPixelIdx] == front[i] content before this pass
-    cur.w_sum = 0.0f;
-    cur.conf = 0.0f;
-    if (!fp.p.suffix_enable_temporal || prev.w_sum <= 0.0f || !fl_valid(prev.s.flags)) {
-        res_update(cur, canon, canon_phat / canon.p, rng, 1.0f);
-        res_finalize(cur);
-    } else {
-        float jac_prev_to_canon = 0.0f, jac_canon_to_prev = 0.0f;
-        const V3 f_canon_of_prev = shift_suffix(s, prev.s, canon, jac_prev_to_canon);
-        const V3 f_prev_of_canon = shift_suffix(s, canon, prev.s, jac_canon_to_prev);
-        const float p_canon_of_prev = luminance(f_canon_of_prev) * jac_prev_to_canon;
-        const float K = 1.0f;
-        const float prev_mis = mis_neighbor(f_canon_of_prev, prev.s.f, jac_prev_to_canon, K, 1.0f, prev.conf);
-        const float canon_mis =
-            1.0f + mis_canonical(canon.f, f_prev_of_canon, jac_canon_to_prev, K, 1.0f, prev.conf);
-        res_update(cur, canon, canon_mis * canon_phat / canon.p, rng, 1.0f);
-        Suffix shifted = prev.s;  // SuffixPath(prev, canon.lastPrefixInt, f)
-        shifted.last_prefix = canon.last_prefix;
-        shifted.f = f_canon_of_prev;
-        res_update(cur, shifted, prev_mis * p_canon_of_prev * prev.w_sum, rng, prev.conf);
-        if (cur.w_sum > 0.0f) {
-            cur.w_sum /= K + 1.0f;
-            res_finalize(cur);
-        }
-    }
-    b.gbuf[i].rng = rng.state;
-    st_sres(b.sres_cur, i, cur);
-}
-
-// SuffixSpatialReuse + raygen, shader/suffix_spatial_reuse.cu:16-167: reads
-// the pass-start state `sres_cur` (own and neighbours), writes `sres_next`.
-__global__ void __launch_bounds__(kPassBlock) k_suffix_spatial(SceneView s, FrameParams fp, Bufs b) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= pixel_count(fp)) return;
-    const uint32_t x = i % fp.width, y = i / fp.width;
-    Res<Suffix> cur = ld_sres(b.sres_cur, i);
-    const uint32_t prefix_flags = b.pres[fp.front][i].sample.flags;
-    const uint32_t canon_flags = b.canon_suffix[i].sample.flags;
-    if (!fl_valid(prefix_flags) || fl_nee(prefix_flags) || !fl_valid(cur.s.flags) || !fl_valid(canon_flags)) {
-        invalidate(cur);
-        st_sres(b.sres_next, i, cur);
-        return;
-    }
-    Rng rng{b.gbuf[i].rng};
-    const Suffix cur_suffix = cur.s;
-    const float cur_wsum = cur.w_sum, cur_conf = cur.conf;
-    cur.w_sum = 0.0f;
-    cur.conf = 0.0f;
-    const int count = fp.p.suffix_spatial_count;
-    float canon_mis = 1.0f;
-    uint32_t nvalid = 0, vflags = 0;
-    uint32_t nx[CRISB_MAX_SPATIAL_NEIGH], ny[CRISB_MAX_SPATIAL_NEIGH];
-    for (int n = 0; n < count; ++n) {
-        select_spatial_neighbor(x, y, static_cast<uint32_t>(fp.p.window_radius), rng, nx[n], ny[n]);
-        if (!(nx[n] < fp.width && ny[n] < fp.height)) continue;
-        const uint32_t ni = ny[n] * fp.width + nx[n];
-        if (!(b.gbuf[ni].flags & 1u)) continue;
-        if (!fl_valid(b.sres_cur[ni].sample.flags)) continue;
-        ++nvalid;
-        vflags |= 1u << n;
-    }
-    const float K = static_cast<float>(nvalid);
-    for (int n = 0; n < count; ++n) {
-        if (!((vflags >> n) & 1u)) continue;
-        const uint32_t ni = ny[n] * fp.width + nx[n];
-        const Res<Suffix> nr = ld_sres(b.sres_cur, ni);
-        float jac_n2c = 0.0f, jac_c2n = 0.0f;
-        const V3 f_c_of_n = shift_suffix(s, nr.s, cur_suffix, jac_n2c);
-        const float p_c_of_n = luminance(f_c_of_n) * jac_n2c;
-        const V3 f_n_of_c = shift_suffix(s, cur_suffix, nr.s, jac_c2n);
-        float nmis = mis_neighbor(f_c_of_n, nr.s.f, jac_n2c, K, cur_conf, nr.conf);
-        if (nonfinite(nmis)) nmis = 0.0f;
-        Suffix shifted = nr.s;
-        shifted.last_prefix = cur_suffix.last_prefix;
-        shifted.f = f_c_of_n;
-        res_update(cur, shifted, nmis * p_c_of_n * nr.w_sum, rng, nr.conf);
-        canon_mis += mis_canonical(cur_suffix.f, f_n_of_c, jac_c2n, K, cur_conf, nr.conf);
-    }
-    if (nonfinite(canon_mis)) canon_mis = 0.0f;
-    res_update(cur, cur_suffix, canon_mis * cur_wsum * luminance(cur_suffix.f), rng, cur_conf);
-    if (cur.w_sum > 0.0f) {
-        cur.w_sum /= K + 1.0f;
-        res_finalize(cur);
-    }
-    b.gbuf[i].rng = rng.state;
-    st_sres(b.sres_next, i, cur);
 }
 
 __global__ void k_bounds_init(unsigned int* ob, uint32_t* n) {
@@ -538,12 +375,6 @@ void launch_prefix_spatial(const SceneView& s, const FrameParams& fp, const Bufs
 }
 void launch_prefix_copy_front_back(const FrameParams& fp, const Bufs& b, cudaStream_t st) {
     k_prefix_copy<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
-}
-void launch_suffix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st) {
-    k_suffix_gen_temp<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b);
-}
-void launch_suffix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st) {
-    k_suffix_spatial<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b);
 }
 void launch_store_entries(const SceneView& s, const FrameParams& fp, const Bufs& b, const lbvh::Work& w,
                           unsigned int* bounds, cudaStream_t st) {

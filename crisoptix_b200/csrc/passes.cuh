@@ -27,6 +27,17 @@ struct Bufs {
     const float4* knn_leaf;  // leaf order: endpoint xyz + radius
     const uint32_t* knn_pixel;  // leaf order -> pixel index
     const uint32_t* knn_n;
+    // split suffix passes: per-pixel status / valid-neighbour flags, spatial
+    // neighbour pixels, the compacted shift-job list and the shift results
+    uint32_t* pass_status;  // P
+    uint32_t* pass_flags;   // P
+    uint32_t* spatial_nbr;  // P * slots / 2
+    uint32_t* job_items;    // P * slots
+    uint32_t* job_count;    // 1
+    float4* shift_out;      // P * slots: shifted f (xyz) and Jacobian (w)
+    crisb_suffix_res_rec* gather_cs;  // P: canonical suffix of the final gather
+    float4* gather_state;   // P * 3: prefix f / p, canonical contribution, direct result
+    uint32_t slots;         // job slots per pixel (>= 2 * max(k, spatial count, 1))
 
     RT_HD KnnView knn() const { return KnnView{knn_nodes, knn_leaf, knn_pixel, knn_n}; }
 };
@@ -39,8 +50,11 @@ void launch_prefix_gen_temp(const SceneView& s, const FrameParams& fp, const Buf
 void launch_prefix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, int round,
                            cudaStream_t st);
 void launch_prefix_copy_front_back(const FrameParams& fp, const Bufs& b, cudaStream_t st);
+// suffix passes as per-pixel kernel -> compacted shift jobs -> per-pixel combine
 void launch_suffix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st);
 void launch_suffix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st);
+void launch_final_gather_split(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out,
+                               cudaStream_t st);
 // prefix entries, endpoint bounds/count and Morton keys (w.keys_in); the
 // caller then sorts w.keys_in into w.keys and calls launch_knn_finish
 void launch_store_entries(const SceneView& s, const FrameParams& fp, const Bufs& b, const lbvh::Work& w,

@@ -1,0 +1,406 @@
+// suffix_passes.cu -- suffix temporal reuse, suffix spatial reuse and the
+// final gather, each split into three kernels:
+//
+//   1. a per-pixel kernel that does everything sequential in the pixel's RNG
+//      stream (canonical path tracing, neighbour selection, the endpoint
+//      query) and appends one job per needed shift to a compacted list;
+//   2. one kernel over that list evaluating the hybrid shifts (the expensive,
+//      traversal-heavy part) as independent, uniform work items;
+//   3. a per-pixel kernel that streams the shifted candidates through pairwise
+//      MIS and the reservoir in the reference's order.
+//
+// Shifts are pure functions of their two records, so the split evaluates the
+// same operations as the per-pixel formulation (shader/suffix_gen_temp_reuse.cu,
+// shader/suffix_spatial_reuse.cu, shader/final_gather.cu:69-188) and gives
+// the same bits; only the SIMD utilisation changes.
+#include <mutex>
+
+#include "records.cuh"
+
+namespace crisb {
+namespace {
+
+constexpr uint32_t kStFinal = 0;      // nothing left to do in the combine kernel
+constexpr uint32_t kStCanonOnly = 1;  // temporal: stream the canonical sample only
+constexpr uint32_t kStReuse = 2;      // reuse with the shift results
+
+enum ShiftMode : int { kModeTemporal = 0, kModeSpatial = 1, kModeGather = 2 };
+
+constexpr uint32_t kSlotBits = 6;  // job code = pixel << 6 | slot
+
+// Append the job slots set in `mask` for pixel i to the list.  Every thread of
+// the warp must call this (warp-aggregated reservation of list space).
+RT_D void push_jobs(const Bufs& b, uint32_t i, uint64_t mask) {
+    const uint32_t n = static_cast<uint32_t>(__popcll(mask));
+    const int lane = threadIdx.x & 31;
+    uint32_t incl = n;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += v;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    uint32_t base = 0;
+    if (lane == 31 && total) base = atomicAdd(b.job_count, total);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    uint32_t pos = base + incl - n;
+    while (mask) {
+        const int bit = __ffsll(static_cast<long long>(mask)) - 1;
+        mask &= mask - 1;
+        b.job_items[pos++] = (i << kSlotBits) | static_cast<uint32_t>(bit);
+    }
+}
+
+RT_D V3 xyz(float4 v) { return V3{v.x, v.y, v.z}; }
+
+// ---- 2. the shift jobs ------------------------------------------------------------
+// Slot 2n: neighbour / previous sample shifted onto the pixel's own path;
+// slot 2n+1: the pixel's own sample shifted onto the neighbour's.
+__global__ void __launch_bounds__(kPassBlock) k_shift_jobs(SceneView s, Bufs b, int mode, uint32_t k) {
+    const uint32_t total = *b.job_count;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const uint32_t code = b.job_items[t];
+        const uint32_t i = code >> kSlotBits, slot = code & ((1u << kSlotBits) - 1), n = slot >> 1;
+        const bool onto_own = (slot & 1u) == 0;
+        const crisb_suffix_rec* own;
+        const crisb_suffix_rec* other;
+        if (mode == kModeTemporal) {
+            own = &b.canon_suffix[i].sample;  // canonical; "other" is the previous sample
+            other = &b.sres_cur[i].sample;
+        } else if (mode == kModeSpatial) {
+            own = &b.sres_cur[i].sample;
+            other = &b.sres_cur[b.spatial_nbr[static_cast<size_t>(i) * (b.slots >> 1) + n]].sample;
+        } else {
+            own = &b.gather_cs[i].sample;
+            other = &b.sres_cur[b.neighbors[static_cast<size_t>(i) * k + n].pixel].sample;
+        }
+        const crisb_suffix_rec* src = onto_own ? other : own;
+        const crisb_hit_rec* dst = onto_own ? &own->last_prefix : &other->last_prefix;
+        const Suffix S = ld_suffix(*src);
+        const Isect d = unpack(s, ld_hit(*dst));
+        float jac = 0.0f;
+        V3 f = splat(0.0f);
+        if (d.valid) f = shift_suffix(s, S, d, jac);
+        b.shift_out[static_cast<size_t>(i) * b.slots + slot] = make_float4(f.x, f.y, f.z, jac);
+    }
+}
+
+// ---- suffix generation + temporal reuse (shader/suffix_gen_temp_reuse.cu) --------
+__global__ void __launch_bounds__(kPassBlock) k_suffix_temp_trace(SceneView s, FrameParams fp, Bufs b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t mask = 0;
+    if (i < pixel_count(fp)) {
+        uint32_t st = kStFinal;
+        Res<Suffix> cur = ld_sres(b.sres_cur, i);
+        const Prefix prefix = ld_prefix(b.pres[fp.front][i].sample);
+        if (!fl_valid(prefix.flags) || fl_nee(prefix.flags)) {
+            invalidate(cur);
+            st_sres(b.sres_cur, i, cur);
+        } else {
+            Rng rng{b.gbuf[i].rng};
+            Suffix canon = ld_suffix(b.canon_suffix[i].sample);
+            trace_suffix(s, fp, canon, prefix, rng);
+            crisb_suffix_res_rec o;
+            st_suffix(o.sample, canon);
+            o.w_sum = 0.0f;
+            o.confidence = 0.0f;
+            b.canon_suffix[i] = o;
+            b.gbuf[i].rng = rng.state;
+            if (!fl_valid(canon.flags)) {
+                invalidate(cur);
+                st_sres(b.sres_cur, i, cur);
+            } else if (!fp.p.suffix_enable_temporal || cur.w_sum <= 0.0f || !fl_valid(cur.s.flags)) {
+                st = kStCanonOnly;  // prevPixelCoord == pixelCoord is always inside the image
+            } else {
+                st = kStReuse;
+                mask = 3;
+            }
+        }
+        b.pass_status[i] = st;
+    }
+    push_jobs(b, i, mask);
+}
+
+__global__ void __launch_bounds__(kPassBlock) k_suffix_temp_combine(FrameParams fp, Bufs b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixel_count(fp)) return;
+    const uint32_t st = b.pass_status[i];
+    if (st == kStFinal) return;
+    Res<Suffix> cur = ld_sres(b.sres_cur, i);
+    const Suffix canon = ld_suffix(b.canon_suffix[i].sample);
+    Rng rng{b.gbuf[i].rng};
+    const float canon_phat = luminance(canon.f);
+    const Res<Suffix> prev = cur;  // back[prevPixelIdx] == front[i] content before the pass
+    cur.w_sum = 0.0f;
+    cur.conf = 0.0f;
+    if (st == kStCanonOnly) {
+        res_update(cur, canon, canon_phat / canon.p, rng, 1.0f);
+        res_finalize(cur);
+    } else {
+        const float4 o0 = b.shift_out[static_cast<size_t>(i) * b.slots];
+        const float4 o1 = b.shift_out[static_cast<size_t>(i) * b.slots + 1];
+        const V3 f_canon_of_prev = xyz(o0), f_prev_of_canon = xyz(o1);
+        const float jac_prev_to_canon = o0.w, jac_canon_to_prev = o1.w;
+        const float p_canon_of_prev = luminance(f_canon_of_prev) * jac_prev_to_canon;
+        const float K = 1.0f;
+        const float prev_mis = mis_neighbor(f_canon_of_prev, prev.s.f, jac_prev_to_canon, K, 1.0f, prev.conf);
+        const float canon_mis =
+            1.0f + mis_canonical(canon.f, f_prev_of_canon, jac_canon_to_prev, K, 1.0f, prev.conf);
+        res_update(cur, canon, canon_mis * canon_phat / canon.p, rng, 1.0f);
+        Suffix shifted = prev.s;  // SuffixPath(prev, canon.lastPrefixInt, f)
+        shifted.last_prefix = canon.last_prefix;
+        shifted.f = f_canon_of_prev;
+        res_update(cur, shifted, prev_mis * p_canon_of_prev * prev.w_sum, rng, prev.conf);
+        if (cur.w_sum > 0.0f) {
+            cur.w_sum /= K + 1.0f;
+            res_finalize(cur);
+        }
+    }
+    b.gbuf[i].rng = rng.state;
+    st_sres(b.sres_cur, i, cur);
+}
+
+// ---- suffix spatial reuse (shader/suffix_spatial_reuse.cu:16-167) -----------------
+// Reads the pass-start state sres_cur (own and neighbours), writes sres_next.
+__global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_select(FrameParams fp, Bufs b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t mask = 0;
+    if (i < pixel_count(fp)) {
+        const uint32_t x = i % fp.width, y = i / fp.width;
+        const uint32_t cur_flags = b.sres_cur[i].sample.flags;
+        const uint32_t prefix_flags = b.pres[fp.front][i].sample.flags;
+        const uint32_t canon_flags = b.canon_suffix[i].sample.flags;
+        uint32_t st = kStFinal;
+        if (fl_valid(prefix_flags) && !fl_nee(prefix_flags) && fl_valid(cur_flags) && fl_valid(canon_flags)) {
+            st = kStReuse;
+            Rng rng{b.gbuf[i].rng};
+            uint32_t vflags = 0;
+            uint32_t* nbr = b.spatial_nbr + static_cast<size_t>(i) * (b.slots >> 1);
+            for (int n = 0; n < fp.p.suffix_spatial_count; ++n) {
+                uint32_t nx, ny;
+                select_spatial_neighbor(x, y, static_cast<uint32_t>(fp.p.window_radius), rng, nx, ny);
+                if (!(nx < fp.width && ny < fp.height)) continue;
+                const uint32_t ni = ny * fp.width + nx;
+                if (!(b.gbuf[ni].flags & 1u)) continue;
+                if (!fl_valid(b.sres_cur[ni].sample.flags)) continue;
+                nbr[n] = ni;
+                vflags |= 1u << n;
+                mask |= 3ull << (2 * n);
+            }
+            b.gbuf[i].rng = rng.state;
+            b.pass_flags[i] = vflags;
+        }
+        b.pass_status[i] = st;
+    }
+    push_jobs(b, i, mask);
+}
+
+__global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_combine(FrameParams fp, Bufs b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixel_count(fp)) return;
+    Res<Suffix> cur = ld_sres(b.sres_cur, i);
+    if (b.pass_status[i] == kStFinal) {
+        invalidate(cur);
+        st_sres(b.sres_next, i, cur);
+        return;
+    }
+    Rng rng{b.gbuf[i].rng};
+    const Suffix cur_suffix = cur.s;
+    const float cur_wsum = cur.w_sum, cur_conf = cur.conf;
+    cur.w_sum = 0.0f;
+    cur.conf = 0.0f;
+    const uint32_t vflags = b.pass_flags[i];
+    const float K = static_cast<float>(__popc(vflags));
+    const uint32_t* nbr = b.spatial_nbr + static_cast<size_t>(i) * (b.slots >> 1);
+    const float4* sh = b.shift_out + static_cast<size_t>(i) * b.slots;
+    float canon_mis = 1.0f;
+    for (int n = 0; n < fp.p.suffix_spatial_count; ++n) {
+        if (!((vflags >> n) & 1u)) continue;
+        const Res<Suffix> nr = ld_sres(b.sres_cur, nbr[n]);
+        const float4 o0 = sh[2 * n], o1 = sh[2 * n + 1];
+        const V3 f_c_of_n = xyz(o0), f_n_of_c = xyz(o1);
+        const float jac_n2c = o0.w, jac_c2n = o1.w;
+        const float p_c_of_n = luminance(f_c_of_n) * jac_n2c;
+        float nmis = mis_neighbor(f_c_of_n, nr.s.f, jac_n2c, K, cur_conf, nr.conf);
+        if (nonfinite(nmis)) nmis = 0.0f;
+        Suffix shifted = nr.s;
+        shifted.last_prefix = cur_suffix.last_prefix;
+        shifted.f = f_c_of_n;
+        res_update(cur, shifted, nmis * p_c_of_n * nr.w_sum, rng, nr.conf);
+        canon_mis += mis_canonical(cur_suffix.f, f_n_of_c, jac_c2n, K, cur_conf, nr.conf);
+    }
+    if (nonfinite(canon_mis)) canon_mis = 0.0f;
+    res_update(cur, cur_suffix, canon_mis * cur_wsum * luminance(cur_suffix.f), rng, cur_conf);
+    if (cur.w_sum > 0.0f) {
+        cur.w_sum /= K + 1.0f;
+        res_finalize(cur);
+    }
+    b.gbuf[i].rng = rng.state;
+    st_sres(b.sres_next, i, cur);
+}
+
+// ---- final gather with gatherN == 1 (shader/final_gather.cu:69-188, 290-356) -----
+__global__ void __launch_bounds__(kPassBlock)
+    k_gather_canon(SceneView s, FrameParams fp, Bufs b, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t mask = 0;
+    if (i < pixel_count(fp)) {
+        const uint32_t x = i % fp.width, y = i / fp.width;
+        const uint32_t k = fp.k;
+        NeighborList nl;
+        nl.count = 0;
+        bool queried = false;
+        uint32_t st = kStFinal;
+        V3 direct = splat(0.0f);
+        if (b.canon_prefix[i].primary.prim != CRISB_INVALID_PRIM) {
+            Rng rng{b.gbuf[i].rng};
+            const V3 dir = camera_dir(fp, x, y, rng);
+            Prefix cp;
+            cp.rng = 0;
+            cp.primary = cp.recon = cp.last = Hit{CRISB_INVALID_PRIM, 0.0f, 0.0f, splat(0.0f)};
+            cp.flags = 0;
+            cp.f = cp.prf = cp.rod = splat(0.0f);
+            cp.p = cp.path_len = 0.0f;
+            trace_prefix(s, fp, cp, ld3(fp.cam.pos), dir, rng);
+            if (fl_valid(cp.flags)) {
+                if (fl_nee(cp.flags)) {
+                    direct = cp.f / cp.p;
+                } else {
+                    Suffix cs;
+                    cs.rng = 0;
+                    cs.recon = cs.last_prefix = Hit{CRISB_INVALID_PRIM, 0.0f, 0.0f, splat(0.0f)};
+                    cs.flags = 0;
+                    cs.f = cs.prf = cs.rod = splat(0.0f);
+                    cs.p = 0.0f;
+                    trace_suffix(s, fp, cs, cp, rng);
+                    if (fl_valid(cs.flags)) {
+                        const V3 canon_contrib = cp.f * cs.f / (cp.p * cs.p);
+                        if (k == 0) {
+                            direct = canon_contrib;
+                        } else {
+                            const Isect last = unpack(s, cs.last_prefix);
+                            knn_query(b.knn(), s.err, last.pos, k, nl);
+                            queried = true;
+                            uint32_t vflags = 0;
+                            for (uint32_t n = 0; n < nl.count; ++n) {
+                                if (!fl_valid(b.sres_cur[nl.pix[n]].sample.flags)) continue;
+                                vflags |= 1u << n;
+                                mask |= 3ull << (2 * n);
+                            }
+                            crisb_suffix_res_rec o;
+                            st_suffix(o.sample, cs);
+                            o.w_sum = 0.0f;
+                            o.confidence = 0.0f;
+                            b.gather_cs[i] = o;
+                            b.gather_state[2 * i] = make_float4(cp.f.x, cp.f.y, cp.f.z, cp.p);
+                            b.gather_state[2 * i + 1] =
+                                make_float4(canon_contrib.x, canon_contrib.y, canon_contrib.z, 0.0f);
+                            b.pass_flags[i] = vflags;
+                            st = kStReuse;
+                        }
+                    }
+                }
+            }
+            b.gbuf[i].rng = rng.state;
+        }
+        if (!queried) nl.count = 0;
+        if (k > 0) {
+            for (uint32_t n = 0; n < k; ++n) {
+                crisb_neighbor_rec r;
+                r.pixel = n < nl.count ? nl.pix[n] : 0u;
+                r.dist = n < nl.count ? nl.dist[n] : 0.0f;
+                b.neighbors[static_cast<size_t>(i) * k + n] = r;
+            }
+        }
+        b.neigh_count[i] = nl.count;
+        if (st == kStFinal) {
+            V3 L = splat(0.0f) + direct;
+            if (nonfinite(L)) L = splat(0.0f);
+            store_output(fp, out, i, L);
+        }
+        b.pass_status[i] = st;
+    }
+    push_jobs(b, i, mask);
+}
+
+__global__ void __launch_bounds__(kPassBlock) k_gather_combine(FrameParams fp, Bufs b, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixel_count(fp) || b.pass_status[i] != kStReuse) return;
+    const uint32_t k = fp.k;
+    const uint32_t count = b.neigh_count[i];
+    const uint32_t vflags = b.pass_flags[i];
+    const V3 cs_f = ld3(b.gather_cs[i].sample.f);
+    const float4 g0 = b.gather_state[2 * i], g1 = b.gather_state[2 * i + 1];
+    const V3 cp_f = xyz(g0), canon_contrib = xyz(g1);
+    const float cp_p = g0.w;
+    const uint32_t nvalid = __popc(vflags);
+    const float K = static_cast<float>(nvalid);
+    const float4* sh = b.shift_out + static_cast<size_t>(i) * b.slots;
+    V3 suffix_contrib = splat(0.0f);
+    float canon_mis = 1.0f;
+    for (uint32_t n = 0; n < count; ++n) {
+        if (!(vflags & (1u << n))) continue;
+        const crisb_suffix_res_rec& nrec = b.sres_cur[b.neighbors[static_cast<size_t>(i) * k + n].pixel];
+        const V3 nf = ld3(nrec.sample.f);
+        const float nconf = nrec.confidence, nwsum = nrec.w_sum;
+        const float4 o0 = sh[2 * n], o1 = sh[2 * n + 1];
+        const V3 f_c_of_n = xyz(o0), f_n_of_c = xyz(o1);
+        const float jac_n2c = o0.w, jac_c2n = o1.w;
+        float nmis = mis_neighbor(f_c_of_n, nf, jac_n2c, K, 1.0f, nconf);
+        if (nonfinite(nmis)) nmis = 0.0f;
+        const V3 contrib = nmis * f_c_of_n * nwsum * jac_n2c;
+        if (!nonfinite(contrib)) suffix_contrib = suffix_contrib + contrib;
+        canon_mis += mis_canonical(cs_f, f_n_of_c, jac_c2n, K, 1.0f, nconf);
+    }
+    V3 gather = suffix_contrib * cp_f / cp_p;
+    gather = gather / static_cast<float>(nvalid + 1);
+    V3 result = gather + (canon_contrib * canon_mis);
+    result = result / (K + 1.0f);
+    if (nonfinite(result)) result = splat(0.0f);
+    V3 L = splat(0.0f) + result;
+    if (nonfinite(L)) L = splat(0.0f);
+    store_output(fp, out, i, L);
+}
+
+inline unsigned grid_for(uint32_t n) { return (n + kPassBlock - 1) / kPassBlock; }
+
+// persistent grid of the job kernel: all blocks that fit on the device at once
+unsigned job_grid() {
+    static std::once_flag once;
+    static unsigned blocks = 148 * 4;
+    std::call_once(once, [] {
+        int dev = 0, sms = 0, per_sm = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_shift_jobs, kPassBlock, 0) == cudaSuccess &&
+            sms > 0 && per_sm > 0)
+            blocks = static_cast<unsigned>(sms * per_sm);
+    });
+    return blocks;
+}
+
+}  // namespace
+
+void launch_suffix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st) {
+    cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
+    k_suffix_temp_trace<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b);
+    k_shift_jobs<<<job_grid(), kPassBlock, 0, st>>>(s, b, kModeTemporal, fp.k);
+    k_suffix_temp_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
+}
+
+void launch_suffix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st) {
+    cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
+    k_suffix_spatial_select<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
+    k_shift_jobs<<<job_grid(), kPassBlock, 0, st>>>(s, b, kModeSpatial, fp.k);
+    k_suffix_spatial_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
+}
+
+void launch_final_gather_split(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out,
+                               cudaStream_t st) {
+    cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
+    k_gather_canon<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b, out);
+    k_shift_jobs<<<job_grid(), kPassBlock, 0, st>>>(s, b, kModeGather, fp.k);
+    k_gather_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, out);
+}
+
+}  // namespace crisb
