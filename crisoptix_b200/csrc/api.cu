@@ -604,8 +604,8 @@ struct crisb_renderer {
         const SceneView s = scene->view(err.p);
         last_stream = st;
         record(0, st);
-        launch_prefix_gen_temp(s, fp, bufs(), out, st);
-        ++launches;
+        launch_prefix_gen_temp_split(s, fp, bufs(), out, st);
+        launches += params.renderer_type == CRISB_RENDERER_PATH_TRACER ? 1 : 3;
         record(1, st);
         const int type = params.renderer_type;
         if (type == CRISB_RENDERER_PATH_TRACER) {

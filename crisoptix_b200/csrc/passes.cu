@@ -1,86 +1,16 @@
 // passes.cu -- the per-frame pass kernels of Conditional ReSTIR PT.
 //
-// One kernel per reference raygen program (shader/*.cu), one thread per
-// pixel, records loaded whole, updated with the reference's in-place field
-// semantics, and stored whole.
+// Prefix spatial reuse, the prefix-endpoint entries and search structure, and
+// the final gather for gatherN > 1: one thread per pixel, records loaded
+// whole, updated with the reference's in-place field semantics, stored whole.
+// (Prefix / suffix temporal, suffix spatial and the gatherN == 1 final gather
+// are split into shift jobs in reuse_passes.cu.)
 #define CRISB_LBVH_KERNELS 1
 #include "records.cuh"
 
 namespace crisb {
 
 namespace {
-
-// PrefixGenTempReuse, shader/prefix_gen_temp_reuse.cu:11-98
-RT_D bool prefix_gen_temp_reuse(const SceneView& s, const FrameParams& fp, const Bufs& b, uint32_t i, V3 origin,
-                                V3 dir, Rng& rng, Res<Prefix>& cur) {
-    Prefix canon = ld_prefix(b.canon_prefix[i]);
-    trace_prefix(s, fp, canon, origin, dir, rng);
-    st_prefix(b.canon_prefix[i], canon);
-    if (!fl_valid(canon.flags)) return false;
-    const float canon_phat = luminance(canon.f);
-    cur.w_sum = 0.0f;
-    cur.conf = 0.0f;
-    // prevPixelCoord == pixelCoord (no motion vectors), always inside the image
-    if (!fp.p.prefix_enable_temporal) {
-        res_update(cur, canon, canon_phat / canon.p, rng, 1.0f);
-        res_finalize(cur);
-        return true;
-    }
-    const Res<Prefix> prev = ld_pres(b.pres[fp.back], i);
-    const bool skip_nee = fp.p.renderer_type == CRISB_RENDERER_CONDITIONAL_RESTIR && fl_nee(prev.s.flags);
-    if (prev.w_sum <= 0.0f || !fl_valid(prev.s.flags) || skip_nee) {
-        res_update(cur, canon, canon_phat / canon.p, rng, 1.0f);
-        res_finalize(cur);
-        return true;
-    }
-    float jac_prev_to_canon = 0.0f, jac_canon_to_prev = 0.0f;
-    const V3 f_canon_of_prev = shift_prefix(s, prev.s, canon, jac_prev_to_canon);
-    const V3 f_prev_of_canon = shift_prefix(s, canon, prev.s, jac_canon_to_prev);
-    const float p_canon_of_prev = luminance(f_canon_of_prev) * jac_prev_to_canon;
-    const float K = 1.0f;
-    const float prev_mis = mis_neighbor(f_canon_of_prev, prev.s.f, jac_prev_to_canon, K, 1.0f, prev.conf);
-    const float canon_mis = 1.0f + mis_canonical(canon.f, f_prev_of_canon, jac_canon_to_prev, K, 1.0f, prev.conf);
-    res_update(cur, canon, canon_mis * canon_phat / canon.p, rng, 1.0f);
-    Prefix shifted = prev.s;  // PrefixPath(prev, f, canon.primaryInt)
-    shifted.f = f_canon_of_prev;
-    shifted.primary = canon.primary;
-    res_update(cur, shifted, prev_mis * p_canon_of_prev * prev.w_sum, rng, prev.conf);
-    if (cur.w_sum > 0.0f) {
-        cur.w_sum /= K + 1.0f;
-        res_finalize(cur);
-    }
-    return true;
-}
-
-// __raygen__prefix_gen_temp_reuse, shader/prefix_gen_temp_reuse.cu:100-193
-__global__ void __launch_bounds__(kPassBlock) k_prefix_gen_temp(SceneView s, FrameParams fp, Bufs b, float* out) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= pixel_count(fp)) return;
-    const uint32_t x = i % fp.width, y = i / fp.width;
-    Rng rng = rng_seeded(tea64(i, fp.random));
-    const V3 dir = camera_dir(fp, x, y, rng);
-    const V3 origin = ld3(fp.cam.pos);
-    const int type = fp.p.renderer_type;
-    if (type == CRISB_RENDERER_CONDITIONAL_RESTIR || type == CRISB_RENDERER_RESTIR_PT) {
-        Res<Prefix> cur = ld_pres(b.pres[fp.front], i);
-        const bool valid = prefix_gen_temp_reuse(s, fp, b, i, origin, dir, rng, cur);
-        st_pres(b.pres[fp.front], i, cur);
-        if (type == CRISB_RENDERER_RESTIR_PT && !fp.p.prefix_enable_spatial)
-            store_output(fp, out, i, valid ? cur.w_sum * cur.s.f : splat(0.0f));
-        if ((type == CRISB_RENDERER_RESTIR_PT && fp.p.prefix_enable_spatial) ||
-            (type == CRISB_RENDERER_CONDITIONAL_RESTIR && fp.p.suffix_enable_spatial))
-            st_pres(b.pres[fp.back], i, cur);
-        crisb_gbuffer_rec g;
-        g.rng = rng.state;
-        g.prev_xy = x | (y << 16);
-        g.flags = valid ? 1u : 0u;
-        b.gbuf[i] = g;
-    } else {
-        V3 L = trace_complete_path(s, fp, origin, dir, rng);
-        if (nonfinite(L)) L = splat(0.0f);
-        store_output(fp, out, i, L);
-    }
-}
 
 // PrefixSpatialReuse, shader/prefix_spatial_reuse.cu:11-134.  Neighbours come
 // from the back buffer, which equals the front buffer at pass start.
@@ -366,9 +296,6 @@ inline unsigned grid_for(uint32_t n) { return (n + kPassBlock - 1) / kPassBlock;
 
 }  // namespace
 
-void launch_prefix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, cudaStream_t st) {
-    k_prefix_gen_temp<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b, out);
-}
 void launch_prefix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, int round,
                            cudaStream_t st) {
     k_prefix_spatial<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b, out, round);

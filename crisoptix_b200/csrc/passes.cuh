@@ -46,11 +46,12 @@ constexpr int kPassBlock = 128;
 constexpr int kKnnLeafMax = 8;
 constexpr int kTriLeafMax = 4;
 
-void launch_prefix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, cudaStream_t st);
 void launch_prefix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, int round,
                            cudaStream_t st);
 void launch_prefix_copy_front_back(const FrameParams& fp, const Bufs& b, cudaStream_t st);
-// suffix passes as per-pixel kernel -> compacted shift jobs -> per-pixel combine
+// reuse passes as per-pixel kernel -> compacted shift jobs -> per-pixel combine
+void launch_prefix_gen_temp_split(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out,
+                                  cudaStream_t st);
 void launch_suffix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st);
 void launch_suffix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st);
 void launch_final_gather_split(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out,

@@ -1,5 +1,6 @@
-// suffix_passes.cu -- suffix temporal reuse, suffix spatial reuse and the
-// final gather, each split into three kernels:
+// reuse_passes.cu -- prefix generation + temporal reuse, suffix temporal
+// reuse, suffix spatial reuse and the final gather, each split into three
+// kernels:
 //
 //   1. a per-pixel kernel that does everything sequential in the pixel's RNG
 //      stream (canonical path tracing, neighbour selection, the endpoint
@@ -11,7 +12,8 @@
 //
 // Shifts are pure functions of their two records, so the split evaluates the
 // same operations as the per-pixel formulation (shader/suffix_gen_temp_reuse.cu,
-// shader/suffix_spatial_reuse.cu, shader/final_gather.cu:69-188) and gives
+// shader/suffix_spatial_reuse.cu, shader/final_gather.cu:69-188,
+// shader/prefix_gen_temp_reuse.cu) and gives
 // the same bits; only the SIMD utilisation changes.
 #include <mutex>
 
@@ -362,6 +364,116 @@ __global__ void __launch_bounds__(kPassBlock) k_gather_combine(FrameParams fp, B
     store_output(fp, out, i, L);
 }
 
+
+// ---- prefix generation + temporal reuse (shader/prefix_gen_temp_reuse.cu) -----------
+RT_D void prefix_tail(const FrameParams& fp, const Bufs& b, float* out, uint32_t i, const Res<Prefix>& cur,
+                      bool valid) {
+    const int type = fp.p.renderer_type;
+    if (type == CRISB_RENDERER_RESTIR_PT && !fp.p.prefix_enable_spatial)
+        store_output(fp, out, i, valid ? cur.w_sum * cur.s.f : splat(0.0f));
+    if ((type == CRISB_RENDERER_RESTIR_PT && fp.p.prefix_enable_spatial) ||
+        (type == CRISB_RENDERER_CONDITIONAL_RESTIR && fp.p.suffix_enable_spatial))
+        st_pres(b.pres[fp.back], i, cur);
+}
+
+__global__ void __launch_bounds__(kPassBlock) k_prefix_trace(SceneView s, FrameParams fp, Bufs b, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t mask = 0;
+    if (i < pixel_count(fp)) {
+        const uint32_t x = i % fp.width, y = i / fp.width;
+        Rng rng = rng_seeded(tea64(i, fp.random));
+        const V3 dir = camera_dir(fp, x, y, rng);
+        const V3 origin = ld3(fp.cam.pos);
+        if (fp.p.renderer_type == CRISB_RENDERER_PATH_TRACER) {
+            V3 L = trace_complete_path(s, fp, origin, dir, rng);
+            if (nonfinite(L)) L = splat(0.0f);
+            store_output(fp, out, i, L);
+        } else {
+            Prefix canon = ld_prefix(b.canon_prefix[i]);
+            trace_prefix(s, fp, canon, origin, dir, rng);
+            st_prefix(b.canon_prefix[i], canon);
+            const bool valid = fl_valid(canon.flags);
+            uint32_t st = kStFinal;
+            if (!valid) {
+                prefix_tail(fp, b, out, i, ld_pres(b.pres[fp.front], i), false);
+            } else if (!fp.p.prefix_enable_temporal) {
+                st = kStCanonOnly;
+            } else {
+                const crisb_prefix_res_rec& prev = b.pres[fp.back][i];
+                const uint32_t pf = prev.sample.flags;
+                const bool skip_nee = fp.p.renderer_type == CRISB_RENDERER_CONDITIONAL_RESTIR && fl_nee(pf);
+                if (prev.w_sum <= 0.0f || !fl_valid(pf) || skip_nee) {
+                    st = kStCanonOnly;
+                } else {
+                    st = kStReuse;
+                    mask = 3;
+                }
+            }
+            crisb_gbuffer_rec g;
+            g.rng = rng.state;
+            g.prev_xy = x | (y << 16);
+            g.flags = valid ? 1u : 0u;
+            b.gbuf[i] = g;
+            b.pass_status[i] = st;
+        }
+    }
+    push_jobs(b, i, mask);
+}
+
+// slot 0: previous prefix shifted onto the canonical one; slot 1: the reverse
+__global__ void __launch_bounds__(kPassBlock) k_prefix_shift_jobs(SceneView s, FrameParams fp, Bufs b) {
+    const uint32_t total = *b.job_count;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const uint32_t code = b.job_items[t];
+        const uint32_t i = code >> kSlotBits, slot = code & ((1u << kSlotBits) - 1);
+        const Prefix canon = ld_prefix(b.canon_prefix[i]);
+        const Prefix prev = ld_prefix(b.pres[fp.back][i].sample);
+        float jac = 0.0f;
+        const V3 f = slot == 0 ? shift_prefix(s, prev, canon, jac) : shift_prefix(s, canon, prev, jac);
+        b.shift_out[static_cast<size_t>(i) * b.slots + slot] = make_float4(f.x, f.y, f.z, jac);
+    }
+}
+
+__global__ void __launch_bounds__(kPassBlock) k_prefix_combine(FrameParams fp, Bufs b, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixel_count(fp) || fp.p.renderer_type == CRISB_RENDERER_PATH_TRACER) return;
+    const uint32_t st = b.pass_status[i];
+    if (st == kStFinal) return;
+    Res<Prefix> cur = ld_pres(b.pres[fp.front], i);
+    const Prefix canon = ld_prefix(b.canon_prefix[i]);
+    Rng rng{b.gbuf[i].rng};
+    const float canon_phat = luminance(canon.f);
+    cur.w_sum = 0.0f;
+    cur.conf = 0.0f;
+    if (st == kStCanonOnly) {
+        res_update(cur, canon, canon_phat / canon.p, rng, 1.0f);
+        res_finalize(cur);
+    } else {
+        const Res<Prefix> prev = ld_pres(b.pres[fp.back], i);
+        const float4 o0 = b.shift_out[static_cast<size_t>(i) * b.slots];
+        const float4 o1 = b.shift_out[static_cast<size_t>(i) * b.slots + 1];
+        const V3 f_canon_of_prev = xyz(o0), f_prev_of_canon = xyz(o1);
+        const float jac_prev_to_canon = o0.w, jac_canon_to_prev = o1.w;
+        const float p_canon_of_prev = luminance(f_canon_of_prev) * jac_prev_to_canon;
+        const float K = 1.0f;
+        const float prev_mis = mis_neighbor(f_canon_of_prev, prev.s.f, jac_prev_to_canon, K, 1.0f, prev.conf);
+        const float canon_mis =
+            1.0f + mis_canonical(canon.f, f_prev_of_canon, jac_canon_to_prev, K, 1.0f, prev.conf);
+        res_update(cur, canon, canon_mis * canon_phat / canon.p, rng, 1.0f);
+        Prefix shifted = prev.s;  // PrefixPath(prev, f, canon.primaryInt)
+        shifted.f = f_canon_of_prev;
+        shifted.primary = canon.primary;
+        res_update(cur, shifted, prev_mis * p_canon_of_prev * prev.w_sum, rng, prev.conf);
+        if (cur.w_sum > 0.0f) {
+            cur.w_sum /= K + 1.0f;
+            res_finalize(cur);
+        }
+    }
+    b.gbuf[i].rng = rng.state;
+    st_pres(b.pres[fp.front], i, cur);
+    prefix_tail(fp, b, out, i, cur, true);
+}
+
 inline unsigned grid_for(uint32_t n) { return (n + kPassBlock - 1) / kPassBlock; }
 
 // persistent grid of the job kernel: all blocks that fit on the device at once
@@ -380,6 +492,15 @@ unsigned job_grid() {
 }
 
 }  // namespace
+
+void launch_prefix_gen_temp_split(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out,
+                                  cudaStream_t st) {
+    cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
+    k_prefix_trace<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b, out);
+    if (fp.p.renderer_type == CRISB_RENDERER_PATH_TRACER) return;
+    k_prefix_shift_jobs<<<job_grid(), kPassBlock, 0, st>>>(s, fp, b);
+    k_prefix_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, out);
+}
 
 void launch_suffix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st) {
     cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
