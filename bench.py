@@ -70,24 +70,29 @@ def params_for(name: str, scene_size: float):
     return p
 
 
-# algorithmic bytes per pixel per pass (FP32 records: prefix reservoir 144 B,
-# canonical prefix 128 B, suffix reservoir / canonical suffix 112 B, G-buffer
-# 16 B, neighbour entry 8 B); reads + writes of the records each pass must touch
-def pass_bytes(k: int, spatial_count: int, spatial_rounds: int, copy_prefix_back: bool):
-    prefix = 144 + 128 + 144 + 128 + 144 + 16 + (144 if copy_prefix_back else 0)
-    suffix_temp = 128 + 112 + 112 + 112 + 16 + 8
-    suffix_spatial = spatial_rounds * (112 + spatial_count * (16 + 112) + 112 + 16 + 8 + 16)
-    store = 128 + 112 + 16 + 8 + 16 + 16
-    gather = 16 + 24 + k * 112 + 8 * k + 4 + 12 + 8
-    return {"prefix_gen_temp": prefix, "suffix_gen_temp": suffix_temp, "suffix_spatial": suffix_spatial,
-            "prefix_store": store, "final_gather": gather}
+# Compulsory bytes per pixel per frame of the resampling kernels (the
+# bandwidth-bound part of each reuse pass: MIS weights and reservoir
+# streaming over records and shift results).  Every record a kernel touches
+# is counted once per kernel (a neighbour's reservoir is another pixel's own
+# record), at nominal occupancy: all k / spatial neighbours present.
+# FP32 records: prefix reservoir 144 B, canonical prefix 128 B, suffix
+# reservoir / canonical suffix 112 B, G-buffer RNG 8 B, shift result 16 B.
+def resample_bytes(k: int, spatial_count: int, spatial_rounds: int, copy_prefix_back: bool) -> dict:
+    prefix_combine = 144 + 128 + 144 + 8 + 8 + 4 + 2 * 16 + 144 + (144 if copy_prefix_back else 0)
+    temporal_combine = 112 + 112 + 8 + 8 + 4 + 2 * 16 + 112
+    spatial_select = 3 * 4 + 8 + 8 + 4 * spatial_count + 8
+    spatial_combine = 112 + 8 + 8 + 8 + 4 * spatial_count + 2 * 16 * spatial_count + 112
+    gather_combine = 12 + 12 + 32 + 8 * k + 20 + 2 * 16 * k + 12
+    return {"prefix_combine": prefix_combine, "temporal_combine": temporal_combine,
+            "spatial_select": spatial_rounds * spatial_select, "spatial_combine": spatial_rounds * spatial_combine,
+            "gather_combine": gather_combine}
 
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
 # dominant kernel from one ncu capture, with the pixel count it was taken at;
 # scaled by pixels to the bench resolution.  Source:
 # profiles/k_final_gather_large_480x270.md
-PROFILED_TRAFFIC = {"final_gather": (97.639424e6 + 7.392e6, 480 * 270)}
+PROFILED_TRAFFIC = {}
 
 
 class ClockSampler:
@@ -256,17 +261,21 @@ def run_crisb(args):
     ms_per_frame = ms / args.steps
     value = ppp * W * H * args.steps * world / (ms / 1000.0)
 
-    # ---- per-pass breakdown (CUDA events on the launching stream) -------------
-    r.set_timing(True)
-    passes = {k: 0.0 for k in ("prefix_gen_temp_ms", "prefix_spatial_ms", "suffix_gen_temp_ms", "suffix_spatial_ms",
-                               "prefix_store_ms", "final_gather_ms", "total_ms")}
+    # ---- per-pass and per-kernel-class breakdown (CUDA events on the stream) ----
+    r.set_timing(1)
+    keys = ("prefix_gen_temp_ms", "prefix_spatial_ms", "suffix_gen_temp_ms", "suffix_spatial_ms", "prefix_store_ms",
+            "final_gather_ms", "total_ms", "trace_ms", "shift_ms", "resample_ms", "search_ms")
+    passes = {k: 0.0 for k in keys}
     n_pass = 3
     for i in range(n_pass):
-        frame(n_frames + i)
+        frame(args.warmup + i)
         st = r.stats()
-        for k in passes:
+        for k in keys:
             passes[k] += st[k] / n_pass
-    r.set_timing(False)
+    r.set_timing(2)  # ray counters (statistics only: adds atomics to the traversal)
+    frame(args.warmup)
+    rays = r.stats()
+    r.set_timing(0)
     r.check_device_errors()
 
     # ---- end to end through the C ABI with host buffers ------------------------
@@ -291,22 +300,26 @@ def run_crisb(args):
     e2e_value = ppp * W * H * e_steps * world / (e_ms / 1000.0)
     img_mean = float(host.mean())
 
-    # ---- roofline of the dominant pass ------------------------------------------
+    # ---- roofline of the resampling kernels; traversal in rays/s -----------------
     peak, peak_kind = measured_peaks()
-    pb = pass_bytes(p.gather_m - 1, p.suffix_spatial_count, p.suffix_spatial_rounds, bool(p.suffix_enable_spatial))
-    pass_ms = {"prefix_gen_temp": passes["prefix_gen_temp_ms"], "suffix_gen_temp": passes["suffix_gen_temp_ms"],
-               "suffix_spatial": passes["suffix_spatial_ms"], "prefix_store": passes["prefix_store_ms"],
-               "final_gather": passes["final_gather_ms"]}
-    dom = max(pass_ms, key=pass_ms.get)
-    dom_bytes = pb[dom] * W * H
-    achieved = dom_bytes / (pass_ms[dom] / 1000.0) / 1e9
+    rb = resample_bytes(p.gather_m - 1, p.suffix_spatial_count, p.suffix_spatial_rounds, bool(p.suffix_enable_spatial))
+    res_bytes = sum(rb.values()) * W * H
+    achieved = res_bytes / (passes["resample_ms"] / 1000.0) / 1e9
     traffic = None
-    if dom in PROFILED_TRAFFIC:
-        tb, tpx = PROFILED_TRAFFIC[dom]
+    if "resampling" in PROFILED_TRAFFIC:
+        tb, tpx = PROFILED_TRAFFIC["resampling"]
         traffic = tb * (W * H) / tpx
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": dom, "peak_kind": f"{peak_kind} copy bandwidth",
-                "algorithmic_bytes_per_launch": dom_bytes, "pass_ms": pass_ms}
+                "traffic": traffic, "kernel": "resampling kernels (reuse-pass combine / select)",
+                "peak_kind": f"{peak_kind} copy bandwidth", "algorithmic_bytes_per_launch": res_bytes,
+                "bytes_per_pixel": rb, "ms": passes["resample_ms"]}
+    n_rays = rays["closest_rays"] + rays["shadow_rays"]
+    trav_ms = passes["trace_ms"] + passes["shift_ms"]
+    traversal = {"closest_rays_per_frame": rays["closest_rays"], "shadow_rays_per_frame": rays["shadow_rays"],
+                 "ms": trav_ms, "rays_per_s": n_rays / (trav_ms / 1000.0) if trav_ms > 0 else None,
+                 "note": "path tracing + shift kernels: BVH traversal, latency bound"}
+    phases = {k: passes[k] for k in ("trace_ms", "shift_ms", "resample_ms", "search_ms")}
+    pass_ms = {k[:-3]: passes[k] for k in keys[:6]}
     if dist:
         dist.destroy_process_group()
     if rank != 0:
@@ -324,7 +337,8 @@ def run_crisb(args):
                        "paths_per_pixel": ppp, "l2": "working set (reservoirs, BVH) larger than L2",
                        "parallelism": f"view-sharded replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 48, "d2h_bytes_per_step": W * H * 12},
-            "roofline": roofline, "cpu_baseline": cb, "clocks": clk,
+            "roofline": roofline, "traversal": traversal, "phases_ms": phases, "pass_ms": pass_ms,
+            "cpu_baseline": cb, "clocks": clk,
             "gpu_launches": launches_per_frame * args.steps, "image_mean": img_mean}
     print(json.dumps(line), flush=True)
 

@@ -192,8 +192,9 @@ class Renderer:
         check(load().crisb_frame_random(self.handle, ctypes.byref(v)))
         return v.value
 
-    def set_timing(self, enable: bool):
-        check(load().crisb_set_timing(self.handle, 1 if enable else 0))
+    def set_timing(self, level: int):
+        """0 off, 1 per-pass / per-kernel-class CUDA events, 2 also ray counters."""
+        check(load().crisb_set_timing(self.handle, int(level)))
 
     def stats(self) -> dict:
         s = _abi.Stats()

@@ -273,6 +273,7 @@ struct crisb_scene {
         v.num_emitters = num_emitters;
         v.num_tris = num_tris;
         v.err = err_word;
+        v.ray_count = nullptr;
         return v;
     }
 };
@@ -482,9 +483,23 @@ struct crisb_renderer {
     LbvhStorage knn;
     DevBuf<int> err;
     cudaStream_t last_stream = nullptr;
-    bool timing = false;
+    int timing = 0;
     cudaEvent_t ev[7] = {};
     uint32_t launches = 0;
+    DevBuf<unsigned long long> ray_count;
+
+    // per-kernel timing: an event after each kernel, tagged with its class
+    struct KernelTimer : Marker {
+        static constexpr int kMax = 96;
+        cudaEvent_t ev[kMax] = {};
+        int cls[kMax] = {};
+        int n = 0;
+        void mark(int c, cudaStream_t st) override {
+            if (n >= kMax) return;
+            cudaEventRecord(ev[n], st);
+            cls[n++] = c;
+        }
+    } ktimer;
 
     uint32_t K() const { return static_cast<uint32_t>(params.gather_m - 1); }
     uint32_t P() const { return width * height; }
@@ -520,7 +535,11 @@ struct crisb_renderer {
     ~crisb_renderer() {
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
+        for (auto& e : ktimer.ev)
+            if (e) cudaEventDestroy(e);
     }
+
+    Marker* marker() { return timing ? &ktimer : nullptr; }
 
     // job slots per pixel of the split suffix passes: two shifts per neighbour
     static uint32_t slots_for(const crisb_params& q) {
@@ -601,10 +620,16 @@ struct crisb_renderer {
         fp.front = front;
         fp.back = back;
         fp.k = K();
-        const SceneView s = scene->view(err.p);
+        SceneView s = scene->view(err.p);
         last_stream = st;
+        ktimer.n = 0;
+        if (timing >= 2) {
+            check(cudaMemsetAsync(ray_count.p, 0, 2 * sizeof(unsigned long long), st), "memset");
+            s.ray_count = ray_count.p;
+        }
+        Marker* m = marker();
         record(0, st);
-        launch_prefix_gen_temp_split(s, fp, bufs(), out, st);
+        launch_prefix_gen_temp_split(s, fp, bufs(), out, st, m);
         launches += params.renderer_type == CRISB_RENDERER_PATH_TRACER ? 1 : 3;
         record(1, st);
         const int type = params.renderer_type;
@@ -617,17 +642,18 @@ struct crisb_renderer {
             for (int r = 0; r < params.prefix_spatial_rounds; ++r) {
                 launch_prefix_spatial(s, fp, bufs(), out, r, st);
                 launch_prefix_copy_front_back(fp, bufs(), st);
+                if (m) m->mark(kClsOther, st);
                 launches += 2;
             }
         }
         record(2, st);
         if (type == CRISB_RENDERER_CONDITIONAL_RESTIR) {
-            launch_suffix_gen_temp(s, fp, bufs(), st);
+            launch_suffix_gen_temp(s, fp, bufs(), st, m);
             launches += 3;
             record(3, st);
             if (params.suffix_enable_spatial && params.suffix_spatial_count > 0) {
                 for (int r = 0; r < params.suffix_spatial_rounds; ++r) {
-                    launch_suffix_spatial(s, fp, bufs(), st);
+                    launch_suffix_spatial(s, fp, bufs(), st, m);
                     launches += 3;
                     scur ^= 1;
                 }
@@ -640,13 +666,15 @@ struct crisb_renderer {
                                                  0, 64, st),
                   "radix sort");
             launch_knn_finish(fp, bufs(), w, knn_leaf.p, st);
+            if (m) m->mark(kClsSearch, st);
             launches += 3 + 4;  // own kernels; the radix sort's library kernels are not counted
             record(5, st);
             if (params.gather_n == 1) {
-                launch_final_gather_split(s, fp, bufs(), out, st);
-                launches += 3;
+                launch_final_gather_split(s, fp, bufs(), out, st, m);
+                launches += 4;
             } else {
                 launch_final_gather(s, fp, bufs(), out, st);
+                if (m) m->mark(kClsOther, st);
                 ++launches;
             }
         } else {
@@ -830,9 +858,13 @@ int crisb_frame_random(const crisb_renderer* r, uint32_t* out) {
 int crisb_set_timing(crisb_renderer* r, int enable) {
     return guarded([&] {
         require(r != nullptr, "null renderer");
-        if (enable && !r->ev[0])
+        require(enable >= 0 && enable <= 2, "timing level must be 0, 1 or 2");
+        if (enable && !r->ev[0]) {
             for (auto& e : r->ev) check(cudaEventCreate(&e), "event create");
-        r->timing = enable != 0;
+            for (auto& e : r->ktimer.ev) check(cudaEventCreate(&e), "event create");
+        }
+        if (enable >= 2 && !r->ray_count.p) r->ray_count.alloc(2);
+        r->timing = enable;
     });
 }
 
@@ -852,6 +884,24 @@ int crisb_get_stats(crisb_renderer* r, crisb_stats* out) {
         out->prefix_store_ms = ms[4];
         out->final_gather_ms = ms[5];
         check(cudaEventElapsedTime(&out->total_ms, r->ev[0], r->ev[6]), "elapsed");
+        float cls_ms[5] = {0, 0, 0, 0, 0};
+        cudaEvent_t prev = r->ev[0];
+        for (int j = 0; j < r->ktimer.n; ++j) {
+            float t = 0.0f;
+            check(cudaEventElapsedTime(&t, prev, r->ktimer.ev[j]), "elapsed");
+            cls_ms[r->ktimer.cls[j]] += t;
+            prev = r->ktimer.ev[j];
+        }
+        out->trace_ms = cls_ms[kClsTrace];
+        out->shift_ms = cls_ms[kClsShift];
+        out->resample_ms = cls_ms[kClsResample];
+        out->search_ms = cls_ms[kClsSearch];
+        if (r->timing >= 2) {
+            unsigned long long rc[2] = {0, 0};
+            check(cudaMemcpy(rc, r->ray_count.p, sizeof(rc), cudaMemcpyDeviceToHost), "ray counters");
+            out->closest_rays = rc[0];
+            out->shadow_rays = rc[1];
+        }
     });
 }
 

@@ -43,6 +43,14 @@ struct Bufs {
 };
 
 constexpr int kPassBlock = 128;
+
+// kernel classes of the per-kernel timing
+enum KernelClass : int { kClsTrace = 0, kClsShift = 1, kClsResample = 2, kClsSearch = 3, kClsOther = 4 };
+
+// called after each kernel launch when per-kernel timing is on
+struct Marker {
+    virtual void mark(int cls, cudaStream_t st) = 0;
+};
 constexpr int kKnnLeafMax = 8;
 constexpr int kTriLeafMax = 4;
 
@@ -51,11 +59,11 @@ void launch_prefix_spatial(const SceneView& s, const FrameParams& fp, const Bufs
 void launch_prefix_copy_front_back(const FrameParams& fp, const Bufs& b, cudaStream_t st);
 // reuse passes as per-pixel kernel -> compacted shift jobs -> per-pixel combine
 void launch_prefix_gen_temp_split(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out,
-                                  cudaStream_t st);
-void launch_suffix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st);
-void launch_suffix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st);
+                                  cudaStream_t st, Marker* m);
+void launch_suffix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m);
+void launch_suffix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m);
 void launch_final_gather_split(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out,
-                               cudaStream_t st);
+                               cudaStream_t st, Marker* m);
 // prefix entries, endpoint bounds/count and Morton keys (w.keys_in); the
 // caller then sorts w.keys_in into w.keys and calls launch_knn_finish
 void launch_store_entries(const SceneView& s, const FrameParams& fp, const Bufs& b, const lbvh::Work& w,

@@ -242,70 +242,85 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_combine(FramePara
 }
 
 // ---- final gather with gatherN == 1 (shader/final_gather.cu:69-188, 290-356) -----
+// k_gather_canon traces the canonical prefix + suffix; k_gather_query runs the
+// endpoint search for the pixels that need it and emits their shift jobs.
+constexpr uint32_t kStQuery = 3;
+
 __global__ void __launch_bounds__(kPassBlock)
     k_gather_canon(SceneView s, FrameParams fp, Bufs b, float* out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    uint64_t mask = 0;
-    if (i < pixel_count(fp)) {
-        const uint32_t x = i % fp.width, y = i / fp.width;
-        const uint32_t k = fp.k;
-        NeighborList nl;
-        nl.count = 0;
-        bool queried = false;
-        uint32_t st = kStFinal;
-        V3 direct = splat(0.0f);
-        if (b.canon_prefix[i].primary.prim != CRISB_INVALID_PRIM) {
-            Rng rng{b.gbuf[i].rng};
-            const V3 dir = camera_dir(fp, x, y, rng);
-            Prefix cp;
-            cp.rng = 0;
-            cp.primary = cp.recon = cp.last = Hit{CRISB_INVALID_PRIM, 0.0f, 0.0f, splat(0.0f)};
-            cp.flags = 0;
-            cp.f = cp.prf = cp.rod = splat(0.0f);
-            cp.p = cp.path_len = 0.0f;
-            trace_prefix(s, fp, cp, ld3(fp.cam.pos), dir, rng);
-            if (fl_valid(cp.flags)) {
-                if (fl_nee(cp.flags)) {
-                    direct = cp.f / cp.p;
-                } else {
-                    Suffix cs;
-                    cs.rng = 0;
-                    cs.recon = cs.last_prefix = Hit{CRISB_INVALID_PRIM, 0.0f, 0.0f, splat(0.0f)};
-                    cs.flags = 0;
-                    cs.f = cs.prf = cs.rod = splat(0.0f);
-                    cs.p = 0.0f;
-                    trace_suffix(s, fp, cs, cp, rng);
-                    if (fl_valid(cs.flags)) {
-                        const V3 canon_contrib = cp.f * cs.f / (cp.p * cs.p);
-                        if (k == 0) {
-                            direct = canon_contrib;
-                        } else {
-                            const Isect last = unpack(s, cs.last_prefix);
-                            knn_query(b.knn(), s.err, last.pos, k, nl);
-                            queried = true;
-                            uint32_t vflags = 0;
-                            for (uint32_t n = 0; n < nl.count; ++n) {
-                                if (!fl_valid(b.sres_cur[nl.pix[n]].sample.flags)) continue;
-                                vflags |= 1u << n;
-                                mask |= 3ull << (2 * n);
-                            }
-                            crisb_suffix_res_rec o;
-                            st_suffix(o.sample, cs);
-                            o.w_sum = 0.0f;
-                            o.confidence = 0.0f;
-                            b.gather_cs[i] = o;
-                            b.gather_state[2 * i] = make_float4(cp.f.x, cp.f.y, cp.f.z, cp.p);
-                            b.gather_state[2 * i + 1] =
-                                make_float4(canon_contrib.x, canon_contrib.y, canon_contrib.z, 0.0f);
-                            b.pass_flags[i] = vflags;
-                            st = kStReuse;
-                        }
+    if (i >= pixel_count(fp)) return;
+    const uint32_t x = i % fp.width, y = i / fp.width;
+    const uint32_t k = fp.k;
+    uint32_t st = kStFinal;
+    V3 direct = splat(0.0f);
+    if (b.canon_prefix[i].primary.prim != CRISB_INVALID_PRIM) {
+        Rng rng{b.gbuf[i].rng};
+        const V3 dir = camera_dir(fp, x, y, rng);
+        Prefix cp;
+        cp.rng = 0;
+        cp.primary = cp.recon = cp.last = Hit{CRISB_INVALID_PRIM, 0.0f, 0.0f, splat(0.0f)};
+        cp.flags = 0;
+        cp.f = cp.prf = cp.rod = splat(0.0f);
+        cp.p = cp.path_len = 0.0f;
+        trace_prefix(s, fp, cp, ld3(fp.cam.pos), dir, rng);
+        if (fl_valid(cp.flags)) {
+            if (fl_nee(cp.flags)) {
+                direct = cp.f / cp.p;
+            } else {
+                Suffix cs;
+                cs.rng = 0;
+                cs.recon = cs.last_prefix = Hit{CRISB_INVALID_PRIM, 0.0f, 0.0f, splat(0.0f)};
+                cs.flags = 0;
+                cs.f = cs.prf = cs.rod = splat(0.0f);
+                cs.p = 0.0f;
+                trace_suffix(s, fp, cs, cp, rng);
+                if (fl_valid(cs.flags)) {
+                    const V3 canon_contrib = cp.f * cs.f / (cp.p * cs.p);
+                    if (k == 0) {
+                        direct = canon_contrib;
+                    } else {
+                        crisb_suffix_res_rec o;
+                        st_suffix(o.sample, cs);
+                        o.w_sum = 0.0f;
+                        o.confidence = 0.0f;
+                        b.gather_cs[i] = o;
+                        b.gather_state[2 * i] = make_float4(cp.f.x, cp.f.y, cp.f.z, cp.p);
+                        b.gather_state[2 * i + 1] = make_float4(canon_contrib.x, canon_contrib.y, canon_contrib.z, 0.0f);
+                        st = kStQuery;
                     }
                 }
             }
-            b.gbuf[i].rng = rng.state;
         }
-        if (!queried) nl.count = 0;
+        b.gbuf[i].rng = rng.state;
+    }
+    if (st == kStFinal) {
+        V3 L = splat(0.0f) + direct;
+        if (nonfinite(L)) L = splat(0.0f);
+        store_output(fp, out, i, L);
+    }
+    b.pass_status[i] = st;
+}
+
+__global__ void __launch_bounds__(kPassBlock) k_gather_query(SceneView s, FrameParams fp, Bufs b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t mask = 0;
+    if (i < pixel_count(fp)) {
+        const uint32_t k = fp.k;
+        NeighborList nl;
+        nl.count = 0;
+        if (b.pass_status[i] == kStQuery) {
+            const Isect last = unpack(s, ld_hit(b.gather_cs[i].sample.last_prefix));
+            knn_query(b.knn(), s.err, last.pos, k, nl);
+            uint32_t vflags = 0;
+            for (uint32_t n = 0; n < nl.count; ++n) {
+                if (!fl_valid(b.sres_cur[nl.pix[n]].sample.flags)) continue;
+                vflags |= 1u << n;
+                mask |= 3ull << (2 * n);
+            }
+            b.pass_flags[i] = vflags;
+            b.pass_status[i] = kStReuse;
+        }
         if (k > 0) {
             for (uint32_t n = 0; n < k; ++n) {
                 crisb_neighbor_rec r;
@@ -315,12 +330,6 @@ __global__ void __launch_bounds__(kPassBlock)
             }
         }
         b.neigh_count[i] = nl.count;
-        if (st == kStFinal) {
-            V3 L = splat(0.0f) + direct;
-            if (nonfinite(L)) L = splat(0.0f);
-            store_output(fp, out, i, L);
-        }
-        b.pass_status[i] = st;
     }
     push_jobs(b, i, mask);
 }
@@ -493,35 +502,56 @@ unsigned job_grid() {
 
 }  // namespace
 
+#define MARK(cls)          \
+    do {                   \
+        if (m) m->mark(cls, st); \
+    } while (0)
+
 void launch_prefix_gen_temp_split(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out,
-                                  cudaStream_t st) {
+                                  cudaStream_t st, Marker* m) {
     cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
     k_prefix_trace<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b, out);
+    MARK(kClsTrace);
     if (fp.p.renderer_type == CRISB_RENDERER_PATH_TRACER) return;
     k_prefix_shift_jobs<<<job_grid(), kPassBlock, 0, st>>>(s, fp, b);
+    MARK(kClsShift);
     k_prefix_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, out);
+    MARK(kClsResample);
 }
 
-void launch_suffix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st) {
+void launch_suffix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m) {
     cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
     k_suffix_temp_trace<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b);
+    MARK(kClsTrace);
     k_shift_jobs<<<job_grid(), kPassBlock, 0, st>>>(s, b, kModeTemporal, fp.k);
+    MARK(kClsShift);
     k_suffix_temp_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
+    MARK(kClsResample);
 }
 
-void launch_suffix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st) {
+void launch_suffix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m) {
     cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
     k_suffix_spatial_select<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
+    MARK(kClsResample);
     k_shift_jobs<<<job_grid(), kPassBlock, 0, st>>>(s, b, kModeSpatial, fp.k);
+    MARK(kClsShift);
     k_suffix_spatial_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
+    MARK(kClsResample);
 }
 
 void launch_final_gather_split(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out,
-                               cudaStream_t st) {
+                               cudaStream_t st, Marker* m) {
     cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
     k_gather_canon<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b, out);
+    MARK(kClsTrace);
+    k_gather_query<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b);
+    MARK(kClsSearch);
     k_shift_jobs<<<job_grid(), kPassBlock, 0, st>>>(s, b, kModeGather, fp.k);
+    MARK(kClsShift);
     k_gather_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, out);
+    MARK(kClsResample);
 }
+
+#undef MARK
 
 }  // namespace crisb

@@ -46,6 +46,7 @@ struct SceneView {
     uint32_t num_emitters;
     uint32_t num_tris;
     int* err;
+    unsigned long long* ray_count;  // [closest, shadow] or null
 };
 
 struct RayPre {
@@ -153,6 +154,13 @@ struct TraceResult {
 
 RT_D void dev_error(const SceneView& s, int code) {
     if (s.err) atomicOr(s.err, code);
+}
+
+// statistics: one warp-aggregated atomic per call site
+RT_D void count_ray(const SceneView& s, int which) {
+    if (!s.ray_count) return;
+    const unsigned m = __activemask();
+    if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&s.ray_count[which], static_cast<unsigned long long>(__popc(m)));
 }
 
 // Closest hit (any_hit == false) or first hit (any_hit == true) over the BVH.
@@ -271,6 +279,7 @@ RT_HD V3 interp(float bu, float bv, V3 v0, V3 v1, V3 v2) {
 // optixTrace + __closesthit__mesh / __miss__main: interaction with the
 // normalised interpolated normal.  On a miss only valid and dir change.
 RT_D void trace_closest(const SceneView& s, V3 o, V3 d, float tmin, float tmax, Isect& it) {
+    count_ray(s, 0);
     const RayPre r = make_ray(o, d);
     const TraceResult h = traverse<false>(s, r, tmin, tmax);
     it.dir = d;
@@ -289,6 +298,7 @@ RT_D void trace_closest(const SceneView& s, V3 o, V3 d, float tmin, float tmax, 
 
 // TraceOcclusion (include/graph/trace.h:64-88)
 RT_D bool occluded(const SceneView& s, V3 o, V3 d, float tmin, float tmax) {
+    count_ray(s, 1);
     const RayPre r = make_ray(o, d);
     return traverse<true>(s, r, tmin, tmax).prim != CRISB_INVALID_PRIM;
 }

@@ -247,6 +247,16 @@ typedef struct crisb_stats {
     float final_gather_ms;
     float total_ms;
     uint32_t kernel_launches;
+    /* the same frame by kernel class: canonical path tracing, shift jobs,
+     * resampling (MIS / reservoir streaming, neighbour selection), and the
+     * prefix-endpoint search (entries, structure build, queries) */
+    float trace_ms;
+    float shift_ms;
+    float resample_ms;
+    float search_ms;
+    /* rays traced in the frame (crisb_set_timing level 2 only) */
+    uint64_t closest_rays;
+    uint64_t shadow_rays;
 } crisb_stats;
 
 /* debug buffer ids for crisb_debug_read */
@@ -357,7 +367,8 @@ int crisb_frame_index(const crisb_renderer* r, uint64_t* out);
 /* per-frame random value the last frame used (params.random) */
 int crisb_frame_random(const crisb_renderer* r, uint32_t* out);
 
-/* Enable per-pass CUDA-event timing (adds events to the stream). */
+/* Per-pass CUDA-event timing: 0 off, 1 events on the stream, 2 events plus
+ * ray counters (atomics in the traversal, for statistics runs). */
 int crisb_set_timing(crisb_renderer* r, int enable);
 /* Per-pass times of the last frame; synchronises on its stop event. */
 int crisb_get_stats(crisb_renderer* r, crisb_stats* out);

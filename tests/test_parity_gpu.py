@@ -53,11 +53,12 @@ def test_flattened_instances_match_float64_reference(cuda_device):
     assert (mat == rm).all()
 
 
-def run_parity(desc, cam, params, W, H, frames, cam_fn, change_params=None):
+def run_parity(desc, cam, params, W, H, frames, cam_fn, change_params=None, timing=0):
     sc = Scene(desc)
     tri = sc.read_triangles()
     o = op.Oracle.from_scene(desc, W, H, params, triangles=tri)
     r = Renderer(W, H, sc, params)
+    r.set_timing(timing)
     out_d = torch.zeros(H * W * 3, dtype=torch.float32, device="cuda")
     out_h = np.zeros((H, W, 3), np.float32)
     for f in range(frames):
@@ -78,6 +79,11 @@ def run_parity(desc, cam, params, W, H, frames, cam_fn, change_params=None):
         img = out_d.cpu().numpy().reshape(H, W, 3)
         np.testing.assert_allclose(img, out_h, rtol=RTOL, atol=1e-6)
         assert img.tobytes() == out_h.tobytes()
+        if timing:
+            st = r.stats()
+            assert st["total_ms"] > 0 and st["trace_ms"] > 0
+            if timing >= 2:
+                assert st["closest_rays"] >= W * H // 2 and st["shadow_rays"] > 0
     return out_h
 
 
@@ -114,3 +120,9 @@ def test_param_change_between_frames(cuda_device):
     p1 = small_config_params(scene_size_of(desc), gather_m=4, gather_radius=0.4, suffix_spatial_rounds=2,
                              prefix_enable_spatial=1, prefix_spatial_count=2)
     run_parity(desc, cam, p0, 32, 32, 4, static, change_params={2: p1})
+
+
+def test_timing_and_ray_counters_do_not_change_results(cuda_device):
+    desc, cam = small_sphere_room()
+    p = large_config_params(scene_size_of(desc), gather_radius=0.3)
+    run_parity(desc, cam, p, 48, 40, 3, lambda c, f: orbit(c, f, 120), timing=2)
