@@ -264,7 +264,7 @@ def run_crisb(args):
     # ---- per-pass and per-kernel-class breakdown (CUDA events on the stream) ----
     r.set_timing(1)
     keys = ("prefix_gen_temp_ms", "prefix_spatial_ms", "suffix_gen_temp_ms", "suffix_spatial_ms", "prefix_store_ms",
-            "final_gather_ms", "total_ms", "trace_ms", "shift_ms", "resample_ms", "search_ms")
+            "final_gather_ms", "total_ms", "trace_ms", "shift_ms", "resample_ms", "search_ms", "shade_ms", "other_ms")
     passes = {k: 0.0 for k in keys}
     n_pass = 3
     for i in range(n_pass):
@@ -314,11 +314,12 @@ def run_crisb(args):
                 "peak_kind": f"{peak_kind} copy bandwidth", "algorithmic_bytes_per_launch": res_bytes,
                 "bytes_per_pixel": rb, "ms": passes["resample_ms"]}
     n_rays = rays["closest_rays"] + rays["shadow_rays"]
-    trav_ms = passes["trace_ms"] + passes["shift_ms"]
     traversal = {"closest_rays_per_frame": rays["closest_rays"], "shadow_rays_per_frame": rays["shadow_rays"],
-                 "ms": trav_ms, "rays_per_s": n_rays / (trav_ms / 1000.0) if trav_ms > 0 else None,
-                 "note": "path tracing + shift kernels: BVH traversal, latency bound"}
-    phases = {k: passes[k] for k in ("trace_ms", "shift_ms", "resample_ms", "search_ms")}
+                 "trace_ms": passes["trace_ms"], "shift_ms": passes["shift_ms"],
+                 "rays_per_s": n_rays / ((passes["trace_ms"] + passes["shift_ms"]) / 1000.0)
+                 if passes["trace_ms"] + passes["shift_ms"] > 0 else None,
+                 "note": "wavefront closest/shadow traversal kernels + shift kernels (replay + reconnection rays)"}
+    phases = {k: passes[k] for k in ("trace_ms", "shade_ms", "shift_ms", "resample_ms", "search_ms", "other_ms")}
     pass_ms = {k[:-3]: passes[k] for k in keys[:6]}
     if dist:
         dist.destroy_process_group()

@@ -115,7 +115,10 @@ class Scene:
     def __del__(self):
         h = getattr(self, "handle", None)
         if h:
-            load().crisb_scene_destroy(h)
+            try:
+                load().crisb_scene_destroy(h)
+            except Exception:  # interpreter shutdown
+                pass
             self.handle = None
 
     @property
@@ -164,7 +167,10 @@ class Renderer:
     def __del__(self):
         h = getattr(self, "handle", None)
         if h:
-            load().crisb_renderer_destroy(h)
+            try:
+                load().crisb_renderer_destroy(h)
+            except Exception:  # interpreter shutdown
+                pass
             self.handle = None
 
     @property

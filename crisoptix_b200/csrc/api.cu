@@ -477,6 +477,9 @@ struct crisb_renderer {
     DevBuf<uint32_t> pass_status, pass_flags, spatial_nbr, job_items, job_count;
     DevBuf<float4> shift_out, gather_state;
     DevBuf<crisb_suffix_res_rec> gather_cs;
+    DevBuf<crisb_prefix_rec> gather_cp;
+    DevBuf<WfPath> wf;
+    DevBuf<uint32_t> wf_queue[4], wf_count;
     uint32_t slots = 0;
     DevBuf<unsigned int> bounds;
     DevBuf<char> sort_temp;
@@ -490,7 +493,7 @@ struct crisb_renderer {
 
     // per-kernel timing: an event after each kernel, tagged with its class
     struct KernelTimer : Marker {
-        static constexpr int kMax = 96;
+        static constexpr int kMax = 256;
         cudaEvent_t ev[kMax] = {};
         int cls[kMax] = {};
         int n = 0;
@@ -529,6 +532,10 @@ struct crisb_renderer {
         b.gather_cs = gather_cs.p;
         b.gather_state = gather_state.p;
         b.slots = slots;
+        b.wf = wf.p;
+        for (int q = 0; q < 4; ++q) b.wf_queue[q] = wf_queue[q].p;
+        b.wf_count = wf_count.p;
+        b.gather_cp = gather_cp.p;
         return b;
     }
 
@@ -562,6 +569,11 @@ struct crisb_renderer {
         job_count.alloc(1);
         gather_cs.alloc(p);
         gather_state.alloc(2 * static_cast<size_t>(p));
+        gather_cp.alloc(p);
+        wf.alloc(p);
+        for (int q = 0; q < 4; ++q) wf_queue[q].alloc(p);
+        wf_count.alloc(4);
+        check(cudaMemset(wf_count.p, 0, wf_count.bytes()), "memset");
         allocate_jobs();
         for (int i = 0; i < 2; ++i) {
             pres[i].alloc(p);
@@ -630,7 +642,7 @@ struct crisb_renderer {
         Marker* m = marker();
         record(0, st);
         launch_prefix_gen_temp_split(s, fp, bufs(), out, st, m);
-        launches += params.renderer_type == CRISB_RENDERER_PATH_TRACER ? 1 : 3;
+        launches += params.renderer_type == CRISB_RENDERER_PATH_TRACER ? 1 : 3 + wf_launches_per_pass(fp);
         record(1, st);
         const int type = params.renderer_type;
         if (type == CRISB_RENDERER_PATH_TRACER) {
@@ -649,7 +661,7 @@ struct crisb_renderer {
         record(2, st);
         if (type == CRISB_RENDERER_CONDITIONAL_RESTIR) {
             launch_suffix_gen_temp(s, fp, bufs(), st, m);
-            launches += 3;
+            launches += 3 + wf_launches_per_pass(fp);
             record(3, st);
             if (params.suffix_enable_spatial && params.suffix_spatial_count > 0) {
                 for (int r = 0; r < params.suffix_spatial_rounds; ++r) {
@@ -671,7 +683,7 @@ struct crisb_renderer {
             record(5, st);
             if (params.gather_n == 1) {
                 launch_final_gather_split(s, fp, bufs(), out, st, m);
-                launches += 4;
+                launches += 4 + wf_launches_per_pass(fp);
             } else {
                 launch_final_gather(s, fp, bufs(), out, st);
                 if (m) m->mark(kClsOther, st);
@@ -884,7 +896,7 @@ int crisb_get_stats(crisb_renderer* r, crisb_stats* out) {
         out->prefix_store_ms = ms[4];
         out->final_gather_ms = ms[5];
         check(cudaEventElapsedTime(&out->total_ms, r->ev[0], r->ev[6]), "elapsed");
-        float cls_ms[5] = {0, 0, 0, 0, 0};
+        float cls_ms[6] = {0, 0, 0, 0, 0, 0};
         cudaEvent_t prev = r->ev[0];
         for (int j = 0; j < r->ktimer.n; ++j) {
             float t = 0.0f;
@@ -896,6 +908,8 @@ int crisb_get_stats(crisb_renderer* r, crisb_stats* out) {
         out->shift_ms = cls_ms[kClsShift];
         out->resample_ms = cls_ms[kClsResample];
         out->search_ms = cls_ms[kClsSearch];
+        out->shade_ms = cls_ms[kClsShade];
+        out->other_ms = cls_ms[kClsOther];
         if (r->timing >= 2) {
             unsigned long long rc[2] = {0, 0};
             check(cudaMemcpy(rc, r->ray_count.p, sizeof(rc), cudaMemcpyDeviceToHost), "ray counters");

@@ -5,6 +5,7 @@
 
 #include "knn.cuh"
 #include "rt_restir.cuh"
+#include "wavefront.cuh"
 
 namespace crisb {
 
@@ -38,6 +39,12 @@ struct Bufs {
     crisb_suffix_res_rec* gather_cs;  // P: canonical suffix of the final gather
     float4* gather_state;   // P * 3: prefix f / p, canonical contribution, direct result
     uint32_t slots;         // job slots per pixel (>= 2 * max(k, spatial count, 1))
+    // wavefront path tracing: one path state per pixel, ray queues of two
+    // rounds (closest, shadow) x 2 and their counts
+    WfPath* wf;
+    uint32_t* wf_queue[4];
+    uint32_t* wf_count;          // 4
+    crisb_prefix_rec* gather_cp; // canonical prefix of the final gather
 
     RT_HD KnnView knn() const { return KnnView{knn_nodes, knn_leaf, knn_pixel, knn_n}; }
 };
@@ -45,7 +52,18 @@ struct Bufs {
 constexpr int kPassBlock = 128;
 
 // kernel classes of the per-kernel timing
-enum KernelClass : int { kClsTrace = 0, kClsShift = 1, kClsResample = 2, kClsSearch = 3, kClsOther = 4 };
+enum KernelClass : int {
+    kClsTrace = 0,     // closest-hit / shadow traversal of the path queues
+    kClsShift = 1,     // shift jobs
+    kClsResample = 2,  // MIS + reservoir streaming, neighbour selection
+    kClsSearch = 3,    // prefix-endpoint entries, structure build, queries
+    kClsOther = 4,
+    kClsShade = 5,     // path-machine shading steps and per-pass finish kernels
+};
+
+// pass_status of a pixel after a wavefront init kernel
+constexpr uint32_t kWfIdle = 0;  // no path ran for the pixel
+constexpr uint32_t kWfPath = 4;  // a path ran for the pixel
 
 // called after each kernel launch when per-kernel timing is on
 struct Marker {
@@ -64,6 +82,11 @@ void launch_suffix_gen_temp(const SceneView& s, const FrameParams& fp, const Buf
 void launch_suffix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m);
 void launch_final_gather_split(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out,
                                cudaStream_t st, Marker* m);
+// wavefront path tracing (wavefront.cu): init + rounds of trace / shade
+void launch_wf_prefix(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m);
+void launch_wf_suffix(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m);
+void launch_wf_gather(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m);
+uint32_t wf_launches_per_pass(const FrameParams& fp);
 // prefix entries, endpoint bounds/count and Morton keys (w.keys_in); the
 // caller then sorts w.keys_in into w.keys and calls launch_knn_finish
 void launch_store_entries(const SceneView& s, const FrameParams& fp, const Bufs& b, const lbvh::Work& w,

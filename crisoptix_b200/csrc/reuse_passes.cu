@@ -88,27 +88,17 @@ __global__ void __launch_bounds__(kPassBlock) k_shift_jobs(SceneView s, Bufs b, 
 }
 
 // ---- suffix generation + temporal reuse (shader/suffix_gen_temp_reuse.cu) --------
-__global__ void __launch_bounds__(kPassBlock) k_suffix_temp_trace(SceneView s, FrameParams fp, Bufs b) {
+// per pixel after the suffix paths (wavefront.cu, suffix flow) finished:
+// the temporal-reuse decision and its shift jobs
+__global__ void __launch_bounds__(kPassBlock) k_suffix_temp_finish(FrameParams fp, Bufs b) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     uint64_t mask = 0;
     if (i < pixel_count(fp)) {
         uint32_t st = kStFinal;
-        Res<Suffix> cur = ld_sres(b.sres_cur, i);
-        const Prefix prefix = ld_prefix(b.pres[fp.front][i].sample);
-        if (!fl_valid(prefix.flags) || fl_nee(prefix.flags)) {
-            invalidate(cur);
-            st_sres(b.sres_cur, i, cur);
-        } else {
-            Rng rng{b.gbuf[i].rng};
-            Suffix canon = ld_suffix(b.canon_suffix[i].sample);
-            trace_suffix(s, fp, canon, prefix, rng);
-            crisb_suffix_res_rec o;
-            st_suffix(o.sample, canon);
-            o.w_sum = 0.0f;
-            o.confidence = 0.0f;
-            b.canon_suffix[i] = o;
-            b.gbuf[i].rng = rng.state;
-            if (!fl_valid(canon.flags)) {
+        if (b.pass_status[i] == kWfPath) {  // else the init kernel invalidated the reservoir
+            b.gbuf[i].rng = b.wf[i].rng;
+            Res<Suffix> cur = ld_sres(b.sres_cur, i);
+            if (!fl_valid(b.canon_suffix[i].sample.flags)) {
                 invalidate(cur);
                 st_sres(b.sres_cur, i, cur);
             } else if (!fp.p.suffix_enable_temporal || cur.w_sum <= 0.0f || !fl_valid(cur.s.flags)) {
@@ -242,49 +232,31 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_combine(FramePara
 }
 
 // ---- final gather with gatherN == 1 (shader/final_gather.cu:69-188, 290-356) -----
-// k_gather_canon traces the canonical prefix + suffix; k_gather_query runs the
+// The gather flow of wavefront.cu traces the canonical prefix + suffix;
+// k_gather_finish forms the canonical contribution; k_gather_query runs the
 // endpoint search for the pixels that need it and emits their shift jobs.
 constexpr uint32_t kStQuery = 3;
 
-__global__ void __launch_bounds__(kPassBlock)
-    k_gather_canon(SceneView s, FrameParams fp, Bufs b, float* out) {
+// per pixel after the canonical paths (wavefront.cu, gather flow) finished
+__global__ void __launch_bounds__(kPassBlock) k_gather_finish(FrameParams fp, Bufs b, float* out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pixel_count(fp)) return;
-    const uint32_t x = i % fp.width, y = i / fp.width;
-    const uint32_t k = fp.k;
     uint32_t st = kStFinal;
     V3 direct = splat(0.0f);
-    if (b.canon_prefix[i].primary.prim != CRISB_INVALID_PRIM) {
-        Rng rng{b.gbuf[i].rng};
-        const V3 dir = camera_dir(fp, x, y, rng);
-        Prefix cp;
-        cp.rng = 0;
-        cp.primary = cp.recon = cp.last = Hit{CRISB_INVALID_PRIM, 0.0f, 0.0f, splat(0.0f)};
-        cp.flags = 0;
-        cp.f = cp.prf = cp.rod = splat(0.0f);
-        cp.p = cp.path_len = 0.0f;
-        trace_prefix(s, fp, cp, ld3(fp.cam.pos), dir, rng);
+    if (b.pass_status[i] == kWfPath) {
+        b.gbuf[i].rng = b.wf[i].rng;
+        const Prefix cp = ld_prefix(b.gather_cp[i]);
         if (fl_valid(cp.flags)) {
             if (fl_nee(cp.flags)) {
                 direct = cp.f / cp.p;
             } else {
-                Suffix cs;
-                cs.rng = 0;
-                cs.recon = cs.last_prefix = Hit{CRISB_INVALID_PRIM, 0.0f, 0.0f, splat(0.0f)};
-                cs.flags = 0;
-                cs.f = cs.prf = cs.rod = splat(0.0f);
-                cs.p = 0.0f;
-                trace_suffix(s, fp, cs, cp, rng);
-                if (fl_valid(cs.flags)) {
-                    const V3 canon_contrib = cp.f * cs.f / (cp.p * cs.p);
-                    if (k == 0) {
+                const crisb_suffix_rec& csr = b.gather_cs[i].sample;
+                if (fl_valid(csr.flags)) {
+                    const V3 cs_f = ld3(csr.f);
+                    const V3 canon_contrib = cp.f * cs_f / (cp.p * csr.p);
+                    if (fp.k == 0) {
                         direct = canon_contrib;
                     } else {
-                        crisb_suffix_res_rec o;
-                        st_suffix(o.sample, cs);
-                        o.w_sum = 0.0f;
-                        o.confidence = 0.0f;
-                        b.gather_cs[i] = o;
                         b.gather_state[2 * i] = make_float4(cp.f.x, cp.f.y, cp.f.z, cp.p);
                         b.gather_state[2 * i + 1] = make_float4(canon_contrib.x, canon_contrib.y, canon_contrib.z, 0.0f);
                         st = kStQuery;
@@ -292,7 +264,6 @@ __global__ void __launch_bounds__(kPassBlock)
                 }
             }
         }
-        b.gbuf[i].rng = rng.state;
     }
     if (st == kStFinal) {
         V3 L = splat(0.0f) + direct;
@@ -385,46 +356,47 @@ RT_D void prefix_tail(const FrameParams& fp, const Bufs& b, float* out, uint32_t
         st_pres(b.pres[fp.back], i, cur);
 }
 
-__global__ void __launch_bounds__(kPassBlock) k_prefix_trace(SceneView s, FrameParams fp, Bufs b, float* out) {
+// PathTracer mode: TraceCompletePath per pixel (prefix_gen_temp_reuse.cu:175-192)
+__global__ void __launch_bounds__(kPassBlock) k_path_tracer(SceneView s, FrameParams fp, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixel_count(fp)) return;
+    Rng rng = rng_seeded(tea64(i, fp.random));
+    const V3 dir = camera_dir(fp, i % fp.width, i / fp.width, rng);
+    V3 L = trace_complete_path(s, fp, ld3(fp.cam.pos), dir, rng);
+    if (nonfinite(L)) L = splat(0.0f);
+    store_output(fp, out, i, L);
+}
+
+// per pixel after the canonical prefixes (wavefront.cu, prefix flow) finished:
+// the temporal-reuse decision, its shift jobs and the G-buffer
+__global__ void __launch_bounds__(kPassBlock) k_prefix_finish(FrameParams fp, Bufs b, float* out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     uint64_t mask = 0;
     if (i < pixel_count(fp)) {
         const uint32_t x = i % fp.width, y = i / fp.width;
-        Rng rng = rng_seeded(tea64(i, fp.random));
-        const V3 dir = camera_dir(fp, x, y, rng);
-        const V3 origin = ld3(fp.cam.pos);
-        if (fp.p.renderer_type == CRISB_RENDERER_PATH_TRACER) {
-            V3 L = trace_complete_path(s, fp, origin, dir, rng);
-            if (nonfinite(L)) L = splat(0.0f);
-            store_output(fp, out, i, L);
+        const bool valid = fl_valid(b.canon_prefix[i].flags);
+        uint32_t st = kStFinal;
+        if (!valid) {
+            prefix_tail(fp, b, out, i, ld_pres(b.pres[fp.front], i), false);
+        } else if (!fp.p.prefix_enable_temporal) {
+            st = kStCanonOnly;
         } else {
-            Prefix canon = ld_prefix(b.canon_prefix[i]);
-            trace_prefix(s, fp, canon, origin, dir, rng);
-            st_prefix(b.canon_prefix[i], canon);
-            const bool valid = fl_valid(canon.flags);
-            uint32_t st = kStFinal;
-            if (!valid) {
-                prefix_tail(fp, b, out, i, ld_pres(b.pres[fp.front], i), false);
-            } else if (!fp.p.prefix_enable_temporal) {
+            const crisb_prefix_res_rec& prev = b.pres[fp.back][i];
+            const uint32_t pf = prev.sample.flags;
+            const bool skip_nee = fp.p.renderer_type == CRISB_RENDERER_CONDITIONAL_RESTIR && fl_nee(pf);
+            if (prev.w_sum <= 0.0f || !fl_valid(pf) || skip_nee) {
                 st = kStCanonOnly;
             } else {
-                const crisb_prefix_res_rec& prev = b.pres[fp.back][i];
-                const uint32_t pf = prev.sample.flags;
-                const bool skip_nee = fp.p.renderer_type == CRISB_RENDERER_CONDITIONAL_RESTIR && fl_nee(pf);
-                if (prev.w_sum <= 0.0f || !fl_valid(pf) || skip_nee) {
-                    st = kStCanonOnly;
-                } else {
-                    st = kStReuse;
-                    mask = 3;
-                }
+                st = kStReuse;
+                mask = 3;
             }
-            crisb_gbuffer_rec g;
-            g.rng = rng.state;
-            g.prev_xy = x | (y << 16);
-            g.flags = valid ? 1u : 0u;
-            b.gbuf[i] = g;
-            b.pass_status[i] = st;
         }
+        crisb_gbuffer_rec g;
+        g.rng = b.wf[i].rng;
+        g.prev_xy = x | (y << 16);
+        g.flags = valid ? 1u : 0u;
+        b.gbuf[i] = g;
+        b.pass_status[i] = st;
     }
     push_jobs(b, i, mask);
 }
@@ -509,10 +481,15 @@ unsigned job_grid() {
 
 void launch_prefix_gen_temp_split(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out,
                                   cudaStream_t st, Marker* m) {
+    if (fp.p.renderer_type == CRISB_RENDERER_PATH_TRACER) {
+        k_path_tracer<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, out);
+        MARK(kClsOther);
+        return;
+    }
+    launch_wf_prefix(s, fp, b, st, m);
     cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
-    k_prefix_trace<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b, out);
-    MARK(kClsTrace);
-    if (fp.p.renderer_type == CRISB_RENDERER_PATH_TRACER) return;
+    k_prefix_finish<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, out);
+    MARK(kClsShade);
     k_prefix_shift_jobs<<<job_grid(), kPassBlock, 0, st>>>(s, fp, b);
     MARK(kClsShift);
     k_prefix_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, out);
@@ -520,9 +497,10 @@ void launch_prefix_gen_temp_split(const SceneView& s, const FrameParams& fp, con
 }
 
 void launch_suffix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m) {
+    launch_wf_suffix(s, fp, b, st, m);
     cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
-    k_suffix_temp_trace<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b);
-    MARK(kClsTrace);
+    k_suffix_temp_finish<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
+    MARK(kClsShade);
     k_shift_jobs<<<job_grid(), kPassBlock, 0, st>>>(s, b, kModeTemporal, fp.k);
     MARK(kClsShift);
     k_suffix_temp_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
@@ -541,9 +519,10 @@ void launch_suffix_spatial(const SceneView& s, const FrameParams& fp, const Bufs
 
 void launch_final_gather_split(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out,
                                cudaStream_t st, Marker* m) {
+    launch_wf_gather(s, fp, b, st, m);
+    k_gather_finish<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, out);
+    MARK(kClsShade);
     cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
-    k_gather_canon<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b, out);
-    MARK(kClsTrace);
     k_gather_query<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b);
     MARK(kClsSearch);
     k_shift_jobs<<<job_grid(), kPassBlock, 0, st>>>(s, b, kModeGather, fp.k);

@@ -1,0 +1,284 @@
+// wavefront.cu -- the wavefront engine that runs the path machines of
+// wavefront.cuh for one pass: an init kernel starts one path per pixel, then
+// each round traces the queued closest-hit rays and shadow rays in two
+// dedicated traversal kernels and resumes every path whose ray finished in a
+// shading kernel, which queues the path's next ray for the following round.
+//
+// Flows (which records a path writes):
+//   prefix: TracePrefix into the canonical prefix record (prefix pass);
+//   suffix: TraceSuffix into the canonical suffix record from the pixel's
+//           reservoir prefix (suffix temporal pass);
+//   gather: TracePrefix, then TraceSuffix when the prefix ends without NEE,
+//           into fresh records (final gather, FinalGatherCanon).
+#include <mutex>
+
+#include "records.cuh"
+
+namespace crisb {
+
+namespace {
+
+// Warp-aggregated append of `val` to queue q (count cnt) for the lanes with
+// `take` set.  Every lane of the warp must call this.
+RT_D void wf_append(uint32_t* q, uint32_t* cnt, bool take, uint32_t val) {
+    const unsigned mask = __ballot_sync(0xffffffffu, take);
+    if (!mask) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(cnt, static_cast<uint32_t>(__popc(mask)));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (take) q[base + __popc(mask & ((1u << lane) - 1u))] = val;
+}
+
+RT_D void wf_push(const Bufs& b, int round, int req, uint32_t i) {
+    wf_append(b.wf_queue[2 * round], &b.wf_count[2 * round], req == kReqClosest, i);
+    wf_append(b.wf_queue[2 * round + 1], &b.wf_count[2 * round + 1], req == kReqShadow, i);
+}
+
+RT_D WfPath wf_blank() {
+    WfPath w;
+    w.rng = 0;
+    w.phase = kPhDone;
+    w.ctr = 0;
+    const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    w.ray_o = w.ray_d = w.it_pos = w.it_nrm = w.it_dir = w.nee_dir = w.nee_col = w.nee_brdf = w.hit = z;
+    w.occluded = 0;
+    w.pad[0] = w.pad[1] = w.pad[2] = 0;
+    return w;
+}
+
+RT_D Suffix fresh_suffix() {
+    Suffix cs;
+    cs.rng = 0;
+    cs.recon = cs.last_prefix = Hit{CRISB_INVALID_PRIM, 0.0f, 0.0f, splat(0.0f)};
+    cs.flags = 0;
+    cs.f = cs.prf = cs.rod = splat(0.0f);
+    cs.p = 0.0f;
+    return cs;
+}
+
+RT_D Prefix fresh_prefix() {
+    Prefix cp;
+    cp.rng = 0;
+    cp.primary = cp.recon = cp.last = Hit{CRISB_INVALID_PRIM, 0.0f, 0.0f, splat(0.0f)};
+    cp.flags = 0;
+    cp.f = cp.prf = cp.rod = splat(0.0f);
+    cp.p = cp.path_len = 0.0f;
+    return cp;
+}
+
+RT_D void st_suffix_slot(crisb_suffix_res_rec& slot, const Suffix& sfx) {
+    crisb_suffix_res_rec o;
+    st_suffix(o.sample, sfx);
+    o.w_sum = 0.0f;
+    o.confidence = 0.0f;
+    slot = o;
+}
+
+// ---- init kernels (round 0 requests) ----------------------------------------------
+__global__ void __launch_bounds__(kPassBlock) k_wf_init_prefix(FrameParams fp, Bufs b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    int req = kReqDone;
+    if (i < pixel_count(fp)) {
+        const uint32_t x = i % fp.width, y = i / fp.width;
+        Rng rng = rng_seeded(tea64(i, fp.random));
+        const V3 dir = camera_dir(fp, x, y, rng);
+        Prefix pre = ld_prefix(b.canon_prefix[i]);
+        WfPath w = wf_blank();
+        req = pre_begin(fp, pre, w, ld3(fp.cam.pos), dir, rng);
+        st_prefix(b.canon_prefix[i], pre);
+        w.rng = rng.state;
+        b.wf[i] = w;
+        b.pass_status[i] = kWfPath;
+    }
+    wf_push(b, 0, req, i);
+}
+
+__global__ void __launch_bounds__(kPassBlock) k_wf_init_suffix(SceneView s, FrameParams fp, Bufs b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    int req = kReqDone;
+    if (i < pixel_count(fp)) {
+        const crisb_prefix_rec& pr = b.pres[fp.front][i].sample;
+        const uint32_t pflags = pr.flags;
+        if (!fl_valid(pflags) || fl_nee(pflags)) {
+            Res<Suffix> cur = ld_sres(b.sres_cur, i);
+            invalidate(cur);
+            st_sres(b.sres_cur, i, cur);
+            b.pass_status[i] = kWfIdle;
+        } else {
+            Rng rng{b.gbuf[i].rng};
+            Suffix suf = ld_suffix(b.canon_suffix[i].sample);
+            WfPath w = wf_blank();
+            req = suf_begin(s, fp, suf, w, pflags, ld_hit(pr.last), rng);
+            st_suffix_slot(b.canon_suffix[i], suf);
+            w.rng = rng.state;
+            b.wf[i] = w;
+            b.pass_status[i] = kWfPath;
+        }
+    }
+    wf_push(b, 0, req, i);
+}
+
+__global__ void __launch_bounds__(kPassBlock) k_wf_init_gather(FrameParams fp, Bufs b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    int req = kReqDone;
+    if (i < pixel_count(fp)) {
+        if (b.canon_prefix[i].primary.prim == CRISB_INVALID_PRIM) {
+            b.pass_status[i] = kWfIdle;
+        } else {
+            const uint32_t x = i % fp.width, y = i / fp.width;
+            Rng rng{b.gbuf[i].rng};
+            const V3 dir = camera_dir(fp, x, y, rng);
+            Prefix cp = fresh_prefix();
+            WfPath w = wf_blank();
+            req = pre_begin(fp, cp, w, ld3(fp.cam.pos), dir, rng);
+            st_prefix(b.gather_cp[i], cp);
+            w.rng = rng.state;
+            b.wf[i] = w;
+            b.pass_status[i] = kWfPath;
+        }
+    }
+    wf_push(b, 0, req, i);
+}
+
+// ---- traversal kernels over the queues of round `cur` ------------------------------
+__global__ void __launch_bounds__(kPassBlock) k_wf_closest(SceneView s, Bufs b, int cur) {
+    const uint32_t n = b.wf_count[2 * cur];
+    const uint32_t* q = b.wf_queue[2 * cur];
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const uint32_t i = q[t];
+        const float4 o = b.wf[i].ray_o, d = b.wf[i].ray_d;
+        count_ray(s, 0);
+        const RayPre r = make_ray(f3(o), f3(d));
+        const TraceResult h = traverse<false>(s, r, 1e-3f, 1e16f);
+        b.wf[i].hit = make_float4(__uint_as_float(h.prim), h.t, h.u, h.v);
+    }
+}
+
+__global__ void __launch_bounds__(kPassBlock) k_wf_shadow(SceneView s, Bufs b, int cur) {
+    const uint32_t n = b.wf_count[2 * cur + 1];
+    const uint32_t* q = b.wf_queue[2 * cur + 1];
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const uint32_t i = q[t];
+        const float4 o = b.wf[i].it_pos, d = b.wf[i].nee_dir;
+        b.wf[i].occluded = occluded(s, f3(o), f3(d), 1e-3f, d.w) ? 1u : 0u;
+    }
+}
+
+// ---- shading: resume every path whose ray of round `cur` finished ---------------------
+RT_D int wf_step(const SceneView& s, const FrameParams& fp, const Bufs& b, int flow, uint32_t i, WfPath& w,
+                 Rng& rng) {
+    if (w.phase == kPhPreHit || w.phase == kPhPreShadow) {
+        crisb_prefix_rec& rec = flow == 0 ? b.canon_prefix[i] : b.gather_cp[i];
+        Prefix pre = ld_prefix(rec);
+        int req = w.phase == kPhPreHit ? pre_on_hit(s, fp, pre, w, rng) : pre_on_shadow(s, pre, w);
+        st_prefix(rec, pre);
+        if (req == kReqDone && flow == 2 && fl_valid(pre.flags) && !fl_nee(pre.flags)) {
+            // FinalGatherCanon: the canonical suffix continues the canonical prefix
+            Suffix cs = fresh_suffix();
+            req = suf_begin(s, fp, cs, w, pre.flags, pre.last, rng);
+            st_suffix_slot(b.gather_cs[i], cs);
+        }
+        return req;
+    }
+    crisb_suffix_res_rec& slot = flow == 1 ? b.canon_suffix[i] : b.gather_cs[i];
+    Suffix suf = ld_suffix(slot.sample);
+    int req = kReqDone;
+    if (w.phase == kPhSufHit) req = suf_on_hit(s, fp, suf, w, rng);
+    else if (w.phase == kPhSufShadow) req = suf_on_shadow(s, suf, w);
+    else if (w.phase == kPhSufRecon) req = suf_on_recon(s, suf, w);
+    st_suffix_slot(slot, suf);
+    return req;
+}
+
+__global__ void __launch_bounds__(kPassBlock) k_wf_shade(SceneView s, FrameParams fp, Bufs b, int flow, int cur) {
+    const uint32_t nc = b.wf_count[2 * cur], ns = b.wf_count[2 * cur + 1];
+    const uint32_t total = nc + ns;
+    const uint32_t* qc = b.wf_queue[2 * cur];
+    const uint32_t* qs = b.wf_queue[2 * cur + 1];
+    const int nxt = cur ^ 1;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
+        const uint32_t t = base + threadIdx.x;
+        int req = kReqDone;
+        uint32_t i = 0;
+        if (t < total) {
+            i = t < nc ? qc[t] : qs[t - nc];
+            WfPath w = b.wf[i];
+            Rng rng{w.rng};
+            req = wf_step(s, fp, b, flow, i, w, rng);
+            w.rng = rng.state;
+            b.wf[i] = w;
+        }
+        wf_push(b, nxt, req, i);
+    }
+}
+
+inline unsigned grid_for(uint32_t n) { return (n + kPassBlock - 1) / kPassBlock; }
+
+unsigned persistent_grid(const void* kernel) {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPassBlock, 0) == cudaSuccess && sms > 0 &&
+        per_sm > 0)
+        return static_cast<unsigned>(sms * per_sm);
+    return 148u * 4u;
+}
+
+struct WfGrids {
+    unsigned closest, shadow, shade;
+};
+
+const WfGrids& wf_grids() {
+    static std::once_flag once;
+    static WfGrids g{};
+    std::call_once(once, [] {
+        g.closest = persistent_grid(reinterpret_cast<const void*>(k_wf_closest));
+        g.shadow = persistent_grid(reinterpret_cast<const void*>(k_wf_shadow));
+        g.shade = persistent_grid(reinterpret_cast<const void*>(k_wf_shade));
+    });
+    return g;
+}
+
+// rounds after the init kernel: every path traces at most max_path_len + 1 rays
+void wf_rounds(const SceneView& s, const FrameParams& fp, const Bufs& b, int flow, cudaStream_t st, Marker* m) {
+    const WfGrids& g = wf_grids();
+    const int rounds = fp.p.max_path_len + 2;
+    for (int r = 0; r < rounds; ++r) {
+        const int cur = r & 1, nxt = cur ^ 1;
+        k_wf_closest<<<g.closest, kPassBlock, 0, st>>>(s, b, cur);
+        k_wf_shadow<<<g.shadow, kPassBlock, 0, st>>>(s, b, cur);
+        if (m) m->mark(kClsTrace, st);
+        cudaMemsetAsync(b.wf_count + 2 * nxt, 0, 2 * sizeof(uint32_t), st);
+        k_wf_shade<<<g.shade, kPassBlock, 0, st>>>(s, fp, b, flow, cur);
+        if (m) m->mark(kClsShade, st);
+    }
+}
+
+}  // namespace
+
+uint32_t wf_launches_per_pass(const FrameParams& fp) { return 1 + 3 * static_cast<uint32_t>(fp.p.max_path_len + 2); }
+
+void launch_wf_prefix(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m) {
+    cudaMemsetAsync(b.wf_count, 0, 2 * sizeof(uint32_t), st);
+    k_wf_init_prefix<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
+    if (m) m->mark(kClsShade, st);
+    wf_rounds(s, fp, b, 0, st, m);
+}
+
+void launch_wf_suffix(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m) {
+    cudaMemsetAsync(b.wf_count, 0, 2 * sizeof(uint32_t), st);
+    k_wf_init_suffix<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b);
+    if (m) m->mark(kClsShade, st);
+    wf_rounds(s, fp, b, 1, st, m);
+}
+
+void launch_wf_gather(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m) {
+    cudaMemsetAsync(b.wf_count, 0, 2 * sizeof(uint32_t), st);
+    k_wf_init_gather<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
+    if (m) m->mark(kClsShade, st);
+    wf_rounds(s, fp, b, 2, st, m);
+}
+
+}  // namespace crisb

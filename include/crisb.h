@@ -247,13 +247,15 @@ typedef struct crisb_stats {
     float final_gather_ms;
     float total_ms;
     uint32_t kernel_launches;
-    /* the same frame by kernel class: canonical path tracing, shift jobs,
+    /* the same frame by kernel class: path traversal, shift jobs,
      * resampling (MIS / reservoir streaming, neighbour selection), and the
      * prefix-endpoint search (entries, structure build, queries) */
     float trace_ms;
     float shift_ms;
     float resample_ms;
     float search_ms;
+    float shade_ms;   /* path-machine shading steps and per-pass finish kernels */
+    float other_ms;
     /* rays traced in the frame (crisb_set_timing level 2 only) */
     uint64_t closest_rays;
     uint64_t shadow_rays;
