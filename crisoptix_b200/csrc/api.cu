@@ -119,34 +119,6 @@ crisb_camera_data camera_data(const crisb_camera& c) {
 // shared by the other translation units of the library
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
-__global__ void k_tri_keys(const float* pos, uint32_t n, float3 lo, float3 hi, uint64_t* keys) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float* p = pos + 9 * static_cast<size_t>(i);
-    const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
-    const float cx = (p[0] + p[3] + p[6]) * (1.0f / 3.0f);
-    const float cy = (p[1] + p[4] + p[7]) * (1.0f / 3.0f);
-    const float cz = (p[2] + p[5] + p[8]) * (1.0f / 3.0f);
-    keys[i] = lbvh::morton_key(l, h, cx, cy, cz, i);
-}
-
-__global__ void k_tri_leaves(const float* pos, lbvh::Work w, float4* tris) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= *w.n) return;
-    const uint32_t prim = static_cast<uint32_t>(w.keys[i] & 0xFFFFFFFFull);
-    w.order[i] = prim;
-    const float* p = pos + 9 * static_cast<size_t>(prim);
-    tris[3 * i + 0] = make_float4(p[0], p[1], p[2], 0.0f);
-    tris[3 * i + 1] = make_float4(p[3], p[4], p[5], 0.0f);
-    tris[3 * i + 2] = make_float4(p[6], p[7], p[8], __uint_as_float(prim));
-    lbvh::Box b;
-    for (int a = 0; a < 3; ++a) {
-        b.lo[a] = fminf(fminf(p[a], p[3 + a]), p[6 + a]);
-        b.hi[a] = fmaxf(fmaxf(p[a], p[3 + a]), p[6 + a]);
-    }
-    w.leaf_box[i] = b;
-}
-
 __global__ void k_trace_rays(SceneView s, const float* rays, crisb_trace_hit* hits, uint32_t n, int any_hit) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -190,14 +162,6 @@ __global__ void k_init_records(crisb_prefix_res_rec* pres0, crisb_prefix_res_rec
     gbuf[i] = g;
 }
 
-// sort 64-bit keys [0, n) of keys_in into keys
-static void sort_keys(const uint64_t* in, uint64_t* out, uint32_t n, DevBuf<char>& temp, cudaStream_t st) {
-    size_t need = 0;
-    check(cub::DeviceRadixSort::SortKeys(nullptr, need, in, out, static_cast<int>(n), 0, 64, st), "sort size");
-    if (temp.bytes() < need) temp.alloc(need);
-    size_t have = temp.bytes();
-    check(cub::DeviceRadixSort::SortKeys(temp.p, have, in, out, static_cast<int>(n), 0, 64, st), "radix sort");
-}
 
 struct LbvhStorage {
     DevBuf<uint64_t> keys_in, keys;
@@ -253,7 +217,8 @@ struct crisb_scene {
     float scene_size = 0.0f;
     std::vector<float> h_pos, h_nrm;
     std::vector<uint32_t> h_mat;
-    DevBuf<BvhNode> nodes;
+    DevBuf<Bvh4Node> nodes;
+    int bvh_max_stack = 0, bvh_max_depth = 0;
     DevBuf<float4> tris;
     DevBuf<float4> shade;
     DevBuf<crisb_material> mats;
@@ -403,41 +368,34 @@ void build_scene(const crisb_scene_desc& d, crisb_scene& s) {
     s.num_emitters = d.num_emitters;
     s.err.alloc(1);
     check(cudaMemset(s.err.p, 0, sizeof(int)), "memset");
-    // LBVH over triangle centroids
-    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    for (uint32_t t = 0; t < n; ++t) {
-        const float* p = &s.h_pos[9 * static_cast<size_t>(t)];
-        for (int a = 0; a < 3; ++a) {
-            const float c = (p[a] + p[3 + a] + p[6 + a]) * (1.0f / 3.0f);
-            lo[a] = std::min(lo[a], c);
-            hi[a] = std::max(hi[a], c);
-        }
+    // 4-wide SAH BVH built on the host; triangles stored in leaf order
+    WideBvh bvh = build_wide_bvh(s.h_pos.data(), n, kTriLeafMax, kMedianDepth);
+    if (bvh.max_stack > kTraversalStack) {
+        // a pathological SAH tree: balanced median splits bound the depth
+        bvh = build_wide_bvh(s.h_pos.data(), n, kTriLeafMax, 0);
+        if (bvh.max_stack > kTraversalStack)
+            throw Error(CRISB_ERR_INVALID_ARGUMENT, "scene build: BVH deeper than the traversal stack");
     }
-    DevBuf<float> dpos;
-    dpos.upload(s.h_pos.data(), s.h_pos.size());
-    LbvhStorage st;
-    st.alloc(n);
-    lbvh::Work w = st.work(s.err.p);
-    check(cudaMemcpy(st.n.p, &n, 4, cudaMemcpyHostToDevice), "upload n");
-    const unsigned g = (std::max<uint32_t>(n, 1) + kPassBlock - 1) / kPassBlock;
-    s.tris.alloc(3 * static_cast<size_t>(std::max<uint32_t>(n, 1)));
-    if (n > 0) {
-        k_tri_keys<<<g, kPassBlock>>>(dpos.p, n, make_float3(lo[0], lo[1], lo[2]), make_float3(hi[0], hi[1], hi[2]),
-                                      st.keys_in.p);
-        check(cudaGetLastError(), "k_tri_keys");
-        DevBuf<char> temp;
-        sort_keys(st.keys_in.p, st.keys.p, n, temp, nullptr);
-        k_tri_leaves<<<g, kPassBlock>>>(dpos.p, w, s.tris.p);
-        check(cudaGetLastError(), "k_tri_leaves");
+    try {
+        validate_wide_bvh(bvh, s.h_pos.data(), n, kTriLeafMax);
+    } catch (const std::runtime_error& e) {
+        throw Error(CRISB_ERR_INVALID_ARGUMENT, std::string("scene build: ") + e.what());
     }
-    launch_lbvh_hierarchy(w, std::max<uint32_t>(n, 1), kTriLeafMax, nullptr);
-    check(cudaGetLastError(), "lbvh");
+    s.bvh_max_stack = bvh.max_stack;
+    s.bvh_max_depth = bvh.max_depth;
+    std::vector<float4> tris(3 * static_cast<size_t>(std::max<uint32_t>(n, 1)), make_float4(0, 0, 0, 0));
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t prim = bvh.order[i];
+        const float* p = &s.h_pos[9 * static_cast<size_t>(prim)];
+        float pb;
+        std::memcpy(&pb, &prim, 4);
+        tris[3 * i + 0] = make_float4(p[0], p[1], p[2], 0.0f);
+        tris[3 * i + 1] = make_float4(p[3], p[4], p[5], 0.0f);
+        tris[3 * i + 2] = make_float4(p[6], p[7], p[8], pb);
+    }
+    s.tris.upload(tris.data(), tris.size());
+    s.nodes.upload(bvh.nodes.data(), bvh.nodes.size());
     check(cudaDeviceSynchronize(), "scene build");
-    s.nodes.alloc(std::max<size_t>(st.nodes.n, 1));
-    check(cudaMemcpy(s.nodes.p, st.nodes.p, st.nodes.bytes(), cudaMemcpyDeviceToDevice), "nodes");
-    int err = 0;
-    check(cudaMemcpy(&err, s.err.p, 4, cudaMemcpyDeviceToHost), "err");
-    if (err) throw Error(CRISB_ERR_DEVICE_FAULT, "scene build: device error " + std::to_string(err));
 }
 
 void validate_params(const crisb_params& p) {

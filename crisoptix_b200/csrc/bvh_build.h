@@ -1,0 +1,45 @@
+// bvh_build.h -- host builder of the scene's 4-wide BVH.
+//
+// Stands in for the OptiX GAS/IAS build of the reference
+// (src/Scene.cpp:73-160, src/Mesh.cpp:54-120): a binned-SAH binary
+// tree over the flattened triangles, collapsed greedily (largest surface area
+// first) into 4-wide nodes.  Any conservative tree gives the same closest and
+// any hit, so the tree shape only changes speed.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+namespace crisb {
+
+// 4-wide node, one 128-byte line: child boxes as structure of arrays, child
+// links (>= 0 inner node, -1-first a leaf of `count` triangles starting at
+// `first` in leaf order, kNoChild an empty slot).
+struct alignas(128) Bvh4Node {
+    float lo_x[4], hi_x[4], lo_y[4], hi_y[4], lo_z[4], hi_z[4];
+    int link[4];
+    int count[4];
+};
+static_assert(sizeof(Bvh4Node) == 128, "Bvh4Node is one 128-byte line");
+
+constexpr int kNoChild = 0x7fffffff;
+
+struct WideBvh {
+    std::vector<Bvh4Node> nodes;  // root at 0
+    std::vector<uint32_t> order;  // leaf order -> triangle index
+    int max_stack = 0;            // worst-case traversal stack entries
+    int max_depth = 0;            // depth of the binary tree
+};
+
+// `pos`: 9 floats per triangle (three vertices).  Leaves hold at most
+// `leaf_max` triangles; below `median_depth` binary levels the SAH split is
+// replaced by object-median splits so the depth stays logarithmic.
+WideBvh build_wide_bvh(const float* pos, uint32_t num_tris, int leaf_max, int median_depth);
+
+// Structural check before the tree goes to the device: links in range, every
+// triangle in exactly one leaf, leaves of at most `leaf_max` triangles, child
+// boxes containing their subtrees, each inner node reached once, and the
+// traversal stack bound recomputed.  Throws std::runtime_error on a failure.
+void validate_wide_bvh(const WideBvh& bvh, const float* pos, uint32_t num_tris, int leaf_max);
+
+}  // namespace crisb

@@ -71,6 +71,8 @@ struct Marker {
 };
 constexpr int kKnnLeafMax = 8;
 constexpr int kTriLeafMax = 4;
+// binary levels of SAH splits before the scene builder switches to median splits
+constexpr int kMedianDepth = 40;
 
 void launch_prefix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, int round,
                            cudaStream_t st);

@@ -9,6 +9,7 @@
 // traversal order.
 #pragma once
 
+#include "bvh_build.h"
 #include "rt_common.cuh"
 
 namespace crisb {
@@ -26,9 +27,9 @@ constexpr uint32_t kKnnMaxVisits = 1u << 21;
 // robust slab test: tfar *= 1 + 2*gamma(3) (Ize 2013, "Robust BVH Ray Traversal")
 constexpr float kSlabFarScale = 1.0000003576f;
 
-// BVH2 node: boxes of both children + child links.  A child link >= 0 is an
-// inner node; a negative link -1-first marks a leaf of `count` triangles
-// starting at `first` in the leaf-ordered triangle array.
+// BVH2 node of the prefix-endpoint search structure: boxes of both children
+// + child links.  A child link >= 0 is an inner node; a negative link
+// -1-first marks a leaf of `count` entries starting at `first` in leaf order.
 struct BvhNode {
     float4 a;  // l.lo.xyz, l.hi.x
     float4 b;  // l.hi.yz, r.lo.xy
@@ -37,7 +38,7 @@ struct BvhNode {
 };
 
 struct SceneView {
-    const BvhNode* nodes;
+    const Bvh4Node* nodes;  // 4-wide scene BVH, root at 0
     const float4* tris;   // 3 per triangle in leaf order; tris[3i+2].w = triangle index bits
     const float4* shade;  // 5 per triangle in scene order: p0 p1 p2 n0 n1 n2 material
     const crisb_material* mats;
@@ -163,92 +164,152 @@ RT_D void count_ray(const SceneView& s, int which) {
     if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&s.ray_count[which], static_cast<unsigned long long>(__popc(m)));
 }
 
+// Traversal of one ray as a resumable state: step() visits one node (both
+// child boxes, leaf triangles) and reports whether the ray is finished.  The
+// stack is kept apart from the scalar state so the latter stays in registers.
+struct TravStack {
+    int node[kTraversalStack];
+    float t[kTraversalStack];
+};
+
+template <bool kAnyHit>
+struct Trav {
+    RayPre r;
+    float tmin, tmax;
+    TraceResult best;
+    int sp, cur;
+    uint32_t visits;
+
+    RT_D void init(const RayPre& ray, float t0, float t1) {
+        r = ray;
+        tmin = t0;
+        tmax = t1;
+        best = TraceResult{CRISB_INVALID_PRIM, t1, 0.0f, 0.0f};
+        sp = 0;
+        cur = 0;
+        visits = 0;
+    }
+
+    RT_D float bound() const { return best.prim == CRISB_INVALID_PRIM ? tmax : best.t; }
+
+    // triangles [first, first + count) of the leaf order; true when an
+    // any-hit query is answered
+    RT_D bool leaf(const SceneView& s, int first, int count) {
+        for (int k = 0; k < count; ++k) {
+            const float4 q0 = __ldg(&s.tris[3 * (first + k) + 0]);
+            const float4 q1 = __ldg(&s.tris[3 * (first + k) + 1]);
+            const float4 q2 = __ldg(&s.tris[3 * (first + k) + 2]);
+            const uint32_t prim = __float_as_uint(q2.w);
+            float t, u, v;
+            if (!intersect_tri(r, V3{q0.x, q0.y, q0.z}, V3{q1.x, q1.y, q1.z}, V3{q2.x, q2.y, q2.z}, tmin, tmax, t,
+                               u, v))
+                continue;
+            if (kAnyHit) {
+                best.prim = prim;
+                best.t = t;
+                return true;
+            }
+            if (best.prim == CRISB_INVALID_PRIM || t < best.t || (t == best.t && prim < best.prim)) {
+                best.prim = prim;
+                best.t = t;
+                best.u = u;
+                best.v = v;
+            }
+        }
+        return false;
+    }
+
+    // one wide node: the four child boxes, the triangles of every leaf child
+    // that is hit, then the nearest inner child next and the others pushed
+    // far to near
+    RT_D bool step(const SceneView& s, TravStack& st) {
+        if (s.num_tris == 0) return true;
+        if (++visits > kMaxNodeVisits) {
+            dev_error(s, kDevErrIterations);
+            return true;
+        }
+        const float4* np = reinterpret_cast<const float4*>(s.nodes + cur);
+        const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2);
+        const float4 hy = __ldg(np + 3), lz = __ldg(np + 4), hz = __ldg(np + 5);
+        const int4 lk = __ldg(reinterpret_cast<const int4*>(np + 6));
+        const int4 ct = __ldg(reinterpret_cast<const int4*>(np + 7));
+        const float bnd = bound();
+        int link[4] = {lk.x, lk.y, lk.z, lk.w};
+        const int cnt[4] = {ct.x, ct.y, ct.z, ct.w};
+        float tn[4];
+        bool hit[4];
+        hit[0] = link[0] != kNoChild && slab(r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, tmin, bnd, tn[0]);
+        hit[1] = link[1] != kNoChild && slab(r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, tmin, bnd, tn[1]);
+        hit[2] = link[2] != kNoChild && slab(r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, tmin, bnd, tn[2]);
+        hit[3] = link[3] != kNoChild && slab(r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, tmin, bnd, tn[3]);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            if (!hit[c] || link[c] >= 0) continue;
+            hit[c] = false;
+            if (leaf(s, -1 - link[c], cnt[c])) return true;
+        }
+        // inner children still in front of the closest hit, nearest first
+        const float cut = bound() * kSlabFarScale;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            if (!hit[c] || tn[c] > cut) tn[c] = INFINITY;
+        auto cswap = [&](int i, int j) {
+            if (tn[j] < tn[i]) {
+                const float t = tn[i];
+                tn[i] = tn[j];
+                tn[j] = t;
+                const int l = link[i];
+                link[i] = link[j];
+                link[j] = l;
+            }
+        };
+        cswap(0, 1);
+        cswap(2, 3);
+        cswap(0, 2);
+        cswap(1, 3);
+        cswap(1, 2);
+        const int nh = (tn[0] < INFINITY) + (tn[1] < INFINITY) + (tn[2] < INFINITY) + (tn[3] < INFINITY);
+        if (nh > 0) {
+            if (sp + nh - 1 > kTraversalStack) {
+                dev_error(s, kDevErrStack);
+                return true;
+            }
+            if (nh > 3) {
+                st.node[sp] = link[3];
+                st.t[sp++] = tn[3];
+            }
+            if (nh > 2) {
+                st.node[sp] = link[2];
+                st.t[sp++] = tn[2];
+            }
+            if (nh > 1) {
+                st.node[sp] = link[1];
+                st.t[sp++] = tn[1];
+            }
+            cur = link[0];
+            return false;
+        }
+        // pop, skipping entries now beyond the closest hit
+        while (sp > 0) {
+            --sp;
+            if (st.t[sp] <= bound() * kSlabFarScale) {
+                cur = st.node[sp];
+                return false;
+            }
+        }
+        return true;
+    }
+};
+
 // Closest hit (any_hit == false) or first hit (any_hit == true) over the BVH.
 template <bool kAnyHit>
 RT_D TraceResult traverse(const SceneView& s, const RayPre& r, float tmin, float tmax) {
-    TraceResult best{CRISB_INVALID_PRIM, tmax, 0.0f, 0.0f};
-    if (s.num_tris == 0) return best;
-    int stack_node[kTraversalStack];
-    float stack_t[kTraversalStack];
-    int sp = 0;
-    int cur = 0;
-    uint32_t visits = 0;
-    while (true) {
-        if (++visits > kMaxNodeVisits) {
-            dev_error(s, kDevErrIterations);
-            break;
-        }
-        const BvhNode nd = s.nodes[cur];
-        const float bound = best.prim == CRISB_INVALID_PRIM ? tmax : best.t;
-        float tl, tr;
-        bool hl = slab(r, nd.a.x, nd.a.y, nd.a.z, nd.a.w, nd.b.x, nd.b.y, tmin, bound, tl);
-        bool hr = slab(r, nd.b.z, nd.b.w, nd.c.x, nd.c.y, nd.c.z, nd.c.w, tmin, bound, tr);
-        int links[2] = {nd.d.x, nd.d.y};
-        int counts[2] = {nd.d.z, nd.d.w};
-        bool hits[2] = {hl, hr};
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            if (!hits[c] || links[c] >= 0) continue;
-            hits[c] = false;
-            const int first = -1 - links[c];
-            for (int k = 0; k < counts[c]; ++k) {
-                const float4 q0 = s.tris[3 * (first + k) + 0];
-                const float4 q1 = s.tris[3 * (first + k) + 1];
-                const float4 q2 = s.tris[3 * (first + k) + 2];
-                const uint32_t prim = __float_as_uint(q2.w);
-                float t, u, v;
-                if (!intersect_tri(r, V3{q0.x, q0.y, q0.z}, V3{q1.x, q1.y, q1.z}, V3{q2.x, q2.y, q2.z}, tmin, tmax,
-                                   t, u, v))
-                    continue;
-                if (kAnyHit) {
-                    best.prim = prim;
-                    best.t = t;
-                    return best;
-                }
-                if (best.prim == CRISB_INVALID_PRIM || t < best.t || (t == best.t && prim < best.prim)) {
-                    best.prim = prim;
-                    best.t = t;
-                    best.u = u;
-                    best.v = v;
-                }
-            }
-        }
-        if (hits[0] && hits[1]) {
-            const bool left_first = tl <= tr;
-            const int near_c = left_first ? links[0] : links[1];
-            const int far_c = left_first ? links[1] : links[0];
-            if (sp >= kTraversalStack) {
-                dev_error(s, kDevErrStack);
-                break;
-            }
-            stack_node[sp] = far_c;
-            stack_t[sp] = left_first ? tr : tl;
-            ++sp;
-            cur = near_c;
-            continue;
-        }
-        if (hits[0]) {
-            cur = links[0];
-            continue;
-        }
-        if (hits[1]) {
-            cur = links[1];
-            continue;
-        }
-        // pop, skipping entries now beyond the closest hit
-        bool found = false;
-        while (sp > 0) {
-            --sp;
-            const float bnd = best.prim == CRISB_INVALID_PRIM ? tmax : best.t;
-            if (stack_t[sp] <= bnd * kSlabFarScale) {
-                cur = stack_node[sp];
-                found = true;
-                break;
-            }
-        }
-        if (!found) break;
+    Trav<kAnyHit> t;
+    TravStack st;
+    t.init(r, tmin, tmax);
+    while (!t.step(s, st)) {
     }
-    return best;
+    return t.best;
 }
 
 // ---- interactions -------------------------------------------------------------
