@@ -315,10 +315,13 @@ def run_crisb(args):
                 "bytes_per_pixel": rb, "ms": passes["resample_ms"]}
     n_rays = rays["closest_rays"] + rays["shadow_rays"]
     traversal = {"closest_rays_per_frame": rays["closest_rays"], "shadow_rays_per_frame": rays["shadow_rays"],
-                 "trace_ms": passes["trace_ms"], "shift_ms": passes["shift_ms"],
-                 "rays_per_s": n_rays / ((passes["trace_ms"] + passes["shift_ms"]) / 1000.0)
-                 if passes["trace_ms"] + passes["shift_ms"] > 0 else None,
-                 "note": "wavefront closest/shadow traversal kernels + shift kernels (replay + reconnection rays)"}
+                 "shift_closest_rays_per_frame": rays["shift_closest_rays"],
+                 "shift_shadow_rays_per_frame": rays["shift_shadow_rays"],
+                 "shift_jobs_per_frame": rays["shift_jobs"],
+                 "trace_ms": passes["trace_ms"],
+                 "rays_per_s": n_rays / (passes["trace_ms"] / 1000.0) if passes["trace_ms"] > 0 else None,
+                 "note": "closest / shadow queue traversal kernels of the path and shift machines; rays of shift "
+                         "jobs left for the last shift round are traced inside the step kernel"}
     phases = {k: passes[k] for k in ("trace_ms", "shade_ms", "shift_ms", "resample_ms", "search_ms", "other_ms")}
     pass_ms = {k[:-3]: passes[k] for k in keys[:6]}
     if dist:

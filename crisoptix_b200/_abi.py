@@ -96,7 +96,8 @@ class Stats(ctypes.Structure):
     _fields_ = [("prefix_gen_temp_ms", c_f), ("prefix_spatial_ms", c_f), ("suffix_gen_temp_ms", c_f),
                 ("suffix_spatial_ms", c_f), ("prefix_store_ms", c_f), ("final_gather_ms", c_f), ("total_ms", c_f),
                 ("kernel_launches", c_u32), ("trace_ms", c_f), ("shift_ms", c_f), ("resample_ms", c_f),
-                ("search_ms", c_f), ("shade_ms", c_f), ("other_ms", c_f), ("closest_rays", c_u64), ("shadow_rays", c_u64)]
+                ("search_ms", c_f), ("shade_ms", c_f), ("other_ms", c_f), ("closest_rays", c_u64), ("shadow_rays", c_u64),
+                ("shift_closest_rays", c_u64), ("shift_shadow_rays", c_u64), ("shift_jobs", c_u64)]
 
 
 HIT_DTYPE = np.dtype([("prim", "<u4"), ("bary", "<f4", 2), ("in_dir", "<f4", 3)])

@@ -438,6 +438,8 @@ struct crisb_renderer {
     DevBuf<crisb_prefix_rec> gather_cp;
     DevBuf<WfPath> wf;
     DevBuf<uint32_t> wf_queue[4], wf_count;
+    DevBuf<ShiftJob> jobs;
+    DevBuf<uint32_t> job_queue[4], job_qcount;
     uint32_t slots = 0;
     DevBuf<unsigned int> bounds;
     DevBuf<char> sort_temp;
@@ -451,7 +453,7 @@ struct crisb_renderer {
 
     // per-kernel timing: an event after each kernel, tagged with its class
     struct KernelTimer : Marker {
-        static constexpr int kMax = 256;
+        static constexpr int kMax = 512;
         cudaEvent_t ev[kMax] = {};
         int cls[kMax] = {};
         int n = 0;
@@ -494,6 +496,9 @@ struct crisb_renderer {
         for (int q = 0; q < 4; ++q) b.wf_queue[q] = wf_queue[q].p;
         b.wf_count = wf_count.p;
         b.gather_cp = gather_cp.p;
+        b.jobs = jobs.p;
+        for (int q = 0; q < 4; ++q) b.job_queue[q] = job_queue[q].p;
+        b.job_qcount = job_qcount.p;
         return b;
     }
 
@@ -518,6 +523,8 @@ struct crisb_renderer {
         spatial_nbr.alloc(p * (slots / 2));
         job_items.alloc(p * slots);
         shift_out.alloc(p * slots);
+        jobs.alloc(p * slots);
+        for (int q = 0; q < 4; ++q) job_queue[q].alloc(p * slots);
     }
 
     void allocate() {
@@ -532,6 +539,8 @@ struct crisb_renderer {
         for (int q = 0; q < 4; ++q) wf_queue[q].alloc(p);
         wf_count.alloc(4);
         check(cudaMemset(wf_count.p, 0, wf_count.bytes()), "memset");
+        job_qcount.alloc(4);
+        check(cudaMemset(job_qcount.p, 0, job_qcount.bytes()), "memset");
         allocate_jobs();
         for (int i = 0; i < 2; ++i) {
             pres[i].alloc(p);
@@ -594,13 +603,14 @@ struct crisb_renderer {
         last_stream = st;
         ktimer.n = 0;
         if (timing >= 2) {
-            check(cudaMemsetAsync(ray_count.p, 0, 2 * sizeof(unsigned long long), st), "memset");
+            check(cudaMemsetAsync(ray_count.p, 0, 5 * sizeof(unsigned long long), st), "memset");
             s.ray_count = ray_count.p;
         }
         Marker* m = marker();
         record(0, st);
         launch_prefix_gen_temp_split(s, fp, bufs(), out, st, m);
-        launches += params.renderer_type == CRISB_RENDERER_PATH_TRACER ? 1 : 3 + wf_launches_per_pass(fp);
+        const uint32_t sj = shift_launches_per_phase();
+        launches += params.renderer_type == CRISB_RENDERER_PATH_TRACER ? 1 : 2 + sj + wf_launches_per_pass(fp);
         record(1, st);
         const int type = params.renderer_type;
         if (type == CRISB_RENDERER_PATH_TRACER) {
@@ -619,12 +629,12 @@ struct crisb_renderer {
         record(2, st);
         if (type == CRISB_RENDERER_CONDITIONAL_RESTIR) {
             launch_suffix_gen_temp(s, fp, bufs(), st, m);
-            launches += 3 + wf_launches_per_pass(fp);
+            launches += 2 + sj + wf_launches_per_pass(fp);
             record(3, st);
             if (params.suffix_enable_spatial && params.suffix_spatial_count > 0) {
                 for (int r = 0; r < params.suffix_spatial_rounds; ++r) {
                     launch_suffix_spatial(s, fp, bufs(), st, m);
-                    launches += 3;
+                    launches += 2 + sj;
                     scur ^= 1;
                 }
             }
@@ -641,7 +651,7 @@ struct crisb_renderer {
             record(5, st);
             if (params.gather_n == 1) {
                 launch_final_gather_split(s, fp, bufs(), out, st, m);
-                launches += 4 + wf_launches_per_pass(fp);
+                launches += 3 + sj + wf_launches_per_pass(fp);
             } else {
                 launch_final_gather(s, fp, bufs(), out, st);
                 if (m) m->mark(kClsOther, st);
@@ -833,7 +843,7 @@ int crisb_set_timing(crisb_renderer* r, int enable) {
             for (auto& e : r->ev) check(cudaEventCreate(&e), "event create");
             for (auto& e : r->ktimer.ev) check(cudaEventCreate(&e), "event create");
         }
-        if (enable >= 2 && !r->ray_count.p) r->ray_count.alloc(2);
+        if (enable >= 2 && !r->ray_count.p) r->ray_count.alloc(5);
         r->timing = enable;
     });
 }
@@ -869,10 +879,13 @@ int crisb_get_stats(crisb_renderer* r, crisb_stats* out) {
         out->shade_ms = cls_ms[kClsShade];
         out->other_ms = cls_ms[kClsOther];
         if (r->timing >= 2) {
-            unsigned long long rc[2] = {0, 0};
+            unsigned long long rc[5] = {0, 0, 0, 0, 0};
             check(cudaMemcpy(rc, r->ray_count.p, sizeof(rc), cudaMemcpyDeviceToHost), "ray counters");
-            out->closest_rays = rc[0];
-            out->shadow_rays = rc[1];
+            out->closest_rays = rc[0] + rc[2];
+            out->shadow_rays = rc[1] + rc[3];
+            out->shift_closest_rays = rc[2];
+            out->shift_shadow_rays = rc[3];
+            out->shift_jobs = rc[4];
         }
     });
 }

@@ -9,6 +9,20 @@
 
 namespace crisb {
 
+// State of one shift job between its rays (80 bytes).  A job replays the
+// source path's bounces from the destination vertex (closest-hit rays) and
+// then tests the reconnection edge (one shadow ray); everything that does not
+// depend on visibility is evaluated before that ray is queued.
+struct ShiftJob {
+    float4 o;      // ray origin xyz; w = shadow ray length
+    float4 d;      // ray direction xyz
+    float4 hit;    // closest-hit result (triangle bits, t, u, v); x = occluded flag after a shadow ray
+    float4 acc;    // during replays: throughput xyz; before the shadow ray: shifted f xyz, Jacobian w
+    uint64_t rng;  // replay RNG of the source path
+    uint32_t code; // job code: pixel << 6 | slot
+    uint32_t ctr;  // replays left after the ray in flight
+};
+
 // Device buffers of one renderer.  Prefix reservoirs keep the reference's
 // front/back pair; suffix reservoirs live in two physical buffers where
 // `sres_cur` holds the state every logical copy front -> back has made equal
@@ -45,6 +59,11 @@ struct Bufs {
     uint32_t* wf_queue[4];
     uint32_t* wf_count;          // 4
     crisb_prefix_rec* gather_cp; // canonical prefix of the final gather
+    // shift machines: one record per job of the list, ray queues of two
+    // rounds (closest, shadow) x 2 and their counts
+    ShiftJob* jobs;         // P * slots
+    uint32_t* job_queue[4]; // P * slots each
+    uint32_t* job_qcount;   // 4
 
     RT_HD KnnView knn() const { return KnnView{knn_nodes, knn_leaf, knn_pixel, knn_n}; }
 };
@@ -89,6 +108,8 @@ void launch_wf_prefix(const SceneView& s, const FrameParams& fp, const Bufs& b, 
 void launch_wf_suffix(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m);
 void launch_wf_gather(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m);
 uint32_t wf_launches_per_pass(const FrameParams& fp);
+// kernels of one shift-job phase (begin + rounds of closest / shadow / step)
+uint32_t shift_launches_per_phase();
 // prefix entries, endpoint bounds/count and Morton keys (w.keys_in); the
 // caller then sorts w.keys_in into w.keys and calls launch_knn_finish
 void launch_store_entries(const SceneView& s, const FrameParams& fp, const Bufs& b, const lbvh::Work& w,

@@ -17,6 +17,7 @@
 // the same bits; only the SIMD utilisation changes.
 #include <mutex>
 
+#include "queues.cuh"
 #include "records.cuh"
 
 namespace crisb {
@@ -58,32 +59,230 @@ RT_D V3 xyz(float4 v) { return V3{v.x, v.y, v.z}; }
 // ---- 2. the shift jobs ------------------------------------------------------------
 // Slot 2n: neighbour / previous sample shifted onto the pixel's own path;
 // slot 2n+1: the pixel's own sample shifted onto the neighbour's.
-__global__ void __launch_bounds__(kPassBlock) k_shift_jobs(SceneView s, Bufs b, int mode, uint32_t k) {
-    const uint32_t total = *b.job_count;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-        const uint32_t code = b.job_items[t];
-        const uint32_t i = code >> kSlotBits, slot = code & ((1u << kSlotBits) - 1), n = slot >> 1;
-        const bool onto_own = (slot & 1u) == 0;
-        const crisb_suffix_rec* own;
-        const crisb_suffix_rec* other;
-        if (mode == kModeTemporal) {
-            own = &b.canon_suffix[i].sample;  // canonical; "other" is the previous sample
-            other = &b.sres_cur[i].sample;
-        } else if (mode == kModeSpatial) {
-            own = &b.sres_cur[i].sample;
-            other = &b.sres_cur[b.spatial_nbr[static_cast<size_t>(i) * (b.slots >> 1) + n]].sample;
-        } else {
-            own = &b.gather_cs[i].sample;
-            other = &b.sres_cur[b.neighbors[static_cast<size_t>(i) * k + n].pixel].sample;
+// statistics view of the shift kernels: rays and jobs in their own counters
+SceneView shift_view(const SceneView& s) {
+    SceneView v = s;
+    if (v.ray_count) v.ray_count += 2;
+    return v;
+}
+
+RT_D void count_jobs(const SceneView& s, uint32_t total) {
+    if (s.ray_count && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&s.ray_count[2], static_cast<unsigned long long>(total));
+}
+
+// ---- shift machines ---------------------------------------------------------------
+// A shift job is CalcCurrContribInOtherDomain of the reference
+// (include/graph/restir/suffix_reuse.h:10-123 for suffixes,
+// include/graph/restir/prefix_reuse.h for prefixes) cut at its rays: the
+// replayed bounces are closest-hit rays traced by the queue kernels, and the
+// reconnection edge is one shadow ray.  The BRDF terms, the Jacobian and the
+// shifted contribution do not depend on the visibility result, so they are
+// evaluated before the shadow ray is queued and the ray only selects between
+// them and zero -- the value the per-job function returns when the edge is
+// occluded.  Jobs that still need a replay in the last round finish inline.
+constexpr int kShiftRounds = 3;
+constexpr int kModePrefix = 3;  // prefix temporal reuse (slot 0: previous onto canonical)
+
+// source path of a job
+struct ShiftSrc {
+    uint64_t rng;
+    uint32_t flags;
+    Hit anchor;  // suffix: the source's last prefix vertex; prefix: its primary hit
+    Hit recon;
+    V3 prf, rod;
+};
+
+RT_D ShiftSrc shift_src(const Suffix& S) { return ShiftSrc{S.rng, S.flags, S.last_prefix, S.recon, S.prf, S.rod}; }
+RT_D ShiftSrc shift_src(const Prefix& P) { return ShiftSrc{P.rng, P.flags, P.primary, P.recon, P.prf, P.rod}; }
+
+// the job's source path and, when `dst` is given, its destination vertex
+RT_D ShiftSrc resolve_job(const FrameParams& fp, const Bufs& b, int mode, uint32_t code, Hit* dst) {
+    const uint32_t i = code >> kSlotBits, slot = code & ((1u << kSlotBits) - 1), n = slot >> 1;
+    if (mode == kModePrefix) {
+        const crisb_prefix_rec& canon = b.canon_prefix[i];
+        const crisb_prefix_rec& prev = b.pres[fp.back][i].sample;
+        const crisb_prefix_rec& src = slot == 0 ? prev : canon;
+        const crisb_prefix_rec& dr = slot == 0 ? canon : prev;
+        if (dst) *dst = ld_hit(dr.primary);
+        return shift_src(ld_prefix(src));
+    }
+    const bool onto_own = (slot & 1u) == 0;
+    const crisb_suffix_rec* own;
+    const crisb_suffix_rec* other;
+    if (mode == kModeTemporal) {
+        own = &b.canon_suffix[i].sample;  // canonical; "other" is the previous sample
+        other = &b.sres_cur[i].sample;
+    } else if (mode == kModeSpatial) {
+        own = &b.sres_cur[i].sample;
+        other = &b.sres_cur[b.spatial_nbr[static_cast<size_t>(i) * (b.slots >> 1) + n]].sample;
+    } else {
+        own = &b.gather_cs[i].sample;
+        other = &b.sres_cur[b.neighbors[static_cast<size_t>(i) * fp.k + n].pixel].sample;
+    }
+    const crisb_suffix_rec* src = onto_own ? other : own;
+    if (dst) *dst = ld_hit(onto_own ? own->last_prefix : other->last_prefix);
+    return shift_src(ld_suffix(*src));
+}
+
+RT_D void job_out(const Bufs& b, uint32_t code, float4 v) {
+    const uint32_t i = code >> kSlotBits, slot = code & ((1u << kSlotBits) - 1);
+    b.shift_out[static_cast<size_t>(i) * b.slots + slot] = v;
+}
+
+// Runs the job from vertex `cur` with `left` replays to go: queues its next
+// ray (returned request) or, when `inline_rays`, traces the remaining rays in
+// place; a finished job writes its result.
+RT_D int shift_advance(const SceneView& s, const Bufs& b, bool prefix, const ShiftSrc& src, ShiftJob& j, Isect cur,
+                       Rng& srng, V3 tp, uint32_t left, bool inline_rays) {
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    while (left > 0) {
+        srng.next_float();
+        const BrdfSample bs = brdf_sample(s, cur, srng);
+        if (bs.pdf <= 0.0f) {
+            job_out(b, j.code, zero);
+            return kReqDone;
         }
-        const crisb_suffix_rec* src = onto_own ? other : own;
-        const crisb_hit_rec* dst = onto_own ? &own->last_prefix : &other->last_prefix;
-        const Suffix S = ld_suffix(*src);
-        const Isect d = unpack(s, ld_hit(*dst));
-        float jac = 0.0f;
-        V3 f = splat(0.0f);
-        if (d.valid) f = shift_suffix(s, S, d, jac);
-        b.shift_out[static_cast<size_t>(i) * b.slots + slot] = make_float4(f.x, f.y, f.z, jac);
+        tp = tp * bs.brdf;
+        --left;
+        if (!inline_rays) {
+            j.o = f4(cur.pos, 0.0f);
+            j.d = f4(bs.dir, 0.0f);
+            j.acc = f4(tp, 0.0f);
+            j.rng = srng.state;
+            j.ctr = left;
+            return kReqClosest;
+        }
+        const V3 pos = cur.pos;
+        trace_closest(s, pos, bs.dir, 1e-3f, 1e16f, cur);
+        if (!cur.valid) {
+            job_out(b, j.code, zero);
+            return kReqDone;
+        }
+    }
+    // the reconnection edge
+    const Isect src_anchor = unpack(s, src.anchor);
+    Isect src_recon = unpack(s, src.recon);
+    const V3 rv = src_recon.pos - cur.pos;
+    const float rlen = length(rv);
+    const V3 rdir = normalize(rv);
+    if ((prefix && isinf(rlen)) || nonfinite(rdir)) {
+        job_out(b, j.code, zero);
+        return kReqDone;
+    }
+    const BrdfEval b1 = brdf_eval(s, cur, rdir);
+    float4 res = zero;
+    if (b1.pdf > 0.0f) {
+        tp = tp * b1.brdf;
+        bool ok = true;
+        if (prefix || fl_recon(src.flags) < fl_len(src.flags)) {
+            src_recon.dir = rdir;
+            if (!prefix && is_zero(src.rod)) ok = false;
+            if (ok) {
+                const BrdfEval b2 = brdf_eval(s, src_recon, src.rod);
+                if (b2.pdf <= 0.0f) ok = false;
+                else tp = tp * b2.brdf;
+            }
+        }
+        if (ok) {
+            const float jac = recon_jacobian(src_anchor.pos, cur.pos, src_recon.pos, src_recon.nrm);
+            const V3 f = prefix ? gmax(splat(0.0f), tp * src.prf) : tp * src.prf;
+            res = f4(f, jac);
+        }
+    }
+    if ((__float_as_uint(res.x) | __float_as_uint(res.y) | __float_as_uint(res.z) | __float_as_uint(res.w)) == 0u) {
+        job_out(b, j.code, zero);  // +0 whether or not the edge is visible
+        return kReqDone;
+    }
+    if (inline_rays) {
+        job_out(b, j.code, occluded(s, cur.pos, rdir, 1e-3f, rlen) ? zero : res);
+        return kReqDone;
+    }
+    j.o = f4(cur.pos, rlen);
+    j.d = f4(rdir, 0.0f);
+    j.acc = res;
+    return kReqShadow;
+}
+
+RT_D void job_push(const Bufs& b, int round, int req, uint32_t t) {
+    q_append(b.job_queue[2 * round], &b.job_qcount[2 * round], req == kReqClosest, t);
+    q_append(b.job_queue[2 * round + 1], &b.job_qcount[2 * round + 1], req == kReqShadow, t);
+}
+
+// first step of every job of the list: the checks of the reference function,
+// then the first ray
+__global__ void __launch_bounds__(kPassBlock) k_shift_begin(SceneView s, FrameParams fp, Bufs b, int mode) {
+    const uint32_t total = *b.job_count;
+    count_jobs(s, total);
+    const bool prefix = mode == kModePrefix;
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
+        const uint32_t t = base + threadIdx.x;
+        int req = kReqDone;
+        if (t < total) {
+            ShiftJob j;
+            j.code = b.job_items[t];
+            Hit dh;
+            const ShiftSrc src = resolve_job(fp, b, mode, j.code, &dh);
+            const Isect cur = unpack(s, dh);
+            bool ok = fl_valid(src.flags) && cur.valid;
+            if (prefix) ok = ok && fl_recon(src.flags) >= 2;
+            ok = ok && unpack(s, src.anchor).valid && unpack(s, src.recon).valid;
+            if (!ok) {
+                job_out(b, j.code, zero);
+            } else {
+                const int skip = prefix ? 2 : 1;
+                const uint32_t left = static_cast<uint32_t>(max(static_cast<int>(fl_recon(src.flags)) - skip, 0));
+                Rng srng{src.rng};
+                req = shift_advance(s, b, prefix, src, j, cur, srng, splat(1.0f), left, false);
+                if (req != kReqDone) b.jobs[t] = j;
+            }
+        }
+        job_push(b, 0, req, t);
+    }
+}
+
+// resume every job whose ray of round `cur` finished; in the last round jobs
+// with replays left finish inline
+template <bool kLast>
+__global__ void __launch_bounds__(kPassBlock) k_shift_step(SceneView s, FrameParams fp, Bufs b, int mode, int cur) {
+    const uint32_t nc = b.job_qcount[2 * cur], ns = b.job_qcount[2 * cur + 1];
+    const uint32_t total = nc + ns;
+    const uint32_t* qc = b.job_queue[2 * cur];
+    const uint32_t* qs = b.job_queue[2 * cur + 1];
+    const bool prefix = mode == kModePrefix;
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
+        const uint32_t u = base + threadIdx.x;
+        int req = kReqDone;
+        uint32_t t = 0;
+        if (u < total) {
+            t = u < nc ? qc[u] : qs[u - nc];
+            ShiftJob j = b.jobs[t];
+            if (u >= nc) {
+                job_out(b, j.code, __float_as_uint(j.hit.x) ? zero : j.acc);
+            } else {
+                // trace_closest semantics: interpolated, normalised normal
+                Isect it;
+                const uint32_t prim = __float_as_uint(j.hit.x);
+                it.dir = f3(j.d);
+                it.valid = prim != CRISB_INVALID_PRIM;
+                if (!it.valid) {
+                    job_out(b, j.code, zero);
+                } else {
+                    it.prim = prim;
+                    it.bu = j.hit.z;
+                    it.bv = j.hit.w;
+                    const ShadeTri tri = load_shade(s, prim);
+                    it.pos = interp(it.bu, it.bv, tri.p0, tri.p1, tri.p2);
+                    it.nrm = normalize(interp(it.bu, it.bv, tri.n0, tri.n1, tri.n2));
+                    const ShiftSrc src = resolve_job(fp, b, mode, j.code, nullptr);
+                    Rng srng{j.rng};
+                    req = shift_advance(s, b, prefix, src, j, it, srng, f3(j.acc), j.ctr, kLast);
+                    if (req != kReqDone) b.jobs[t] = j;
+                }
+            }
+        }
+        if (!kLast) job_push(b, cur ^ 1, req, t);
     }
 }
 
@@ -402,19 +601,6 @@ __global__ void __launch_bounds__(kPassBlock) k_prefix_finish(FrameParams fp, Bu
 }
 
 // slot 0: previous prefix shifted onto the canonical one; slot 1: the reverse
-__global__ void __launch_bounds__(kPassBlock) k_prefix_shift_jobs(SceneView s, FrameParams fp, Bufs b) {
-    const uint32_t total = *b.job_count;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-        const uint32_t code = b.job_items[t];
-        const uint32_t i = code >> kSlotBits, slot = code & ((1u << kSlotBits) - 1);
-        const Prefix canon = ld_prefix(b.canon_prefix[i]);
-        const Prefix prev = ld_prefix(b.pres[fp.back][i].sample);
-        float jac = 0.0f;
-        const V3 f = slot == 0 ? shift_prefix(s, prev, canon, jac) : shift_prefix(s, canon, prev, jac);
-        b.shift_out[static_cast<size_t>(i) * b.slots + slot] = make_float4(f.x, f.y, f.z, jac);
-    }
-}
-
 __global__ void __launch_bounds__(kPassBlock) k_prefix_combine(FrameParams fp, Bufs b, float* out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pixel_count(fp) || fp.p.renderer_type == CRISB_RENDERER_PATH_TRACER) return;
@@ -455,29 +641,54 @@ __global__ void __launch_bounds__(kPassBlock) k_prefix_combine(FrameParams fp, B
     prefix_tail(fp, b, out, i, cur, true);
 }
 
-inline unsigned grid_for(uint32_t n) { return (n + kPassBlock - 1) / kPassBlock; }
+struct ShiftGrids {
+    unsigned begin, step, step_last, closest, shadow;
+};
 
-// persistent grid of the job kernel: all blocks that fit on the device at once
-unsigned job_grid() {
+const ShiftGrids& shift_grids() {
     static std::once_flag once;
-    static unsigned blocks = 148 * 4;
+    static ShiftGrids g{};
     std::call_once(once, [] {
-        int dev = 0, sms = 0, per_sm = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess &&
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_shift_jobs, kPassBlock, 0) == cudaSuccess &&
-            sms > 0 && per_sm > 0)
-            blocks = static_cast<unsigned>(sms * per_sm);
+        g.begin = persistent_grid(reinterpret_cast<const void*>(k_shift_begin));
+        g.step = persistent_grid(reinterpret_cast<const void*>(k_shift_step<false>));
+        g.step_last = persistent_grid(reinterpret_cast<const void*>(k_shift_step<true>));
+        g.closest = persistent_grid(reinterpret_cast<const void*>(k_q_closest<ShiftJob>));
+        g.shadow = persistent_grid(reinterpret_cast<const void*>(k_q_shadow<ShiftJob>));
     });
-    return blocks;
+    return g;
 }
-
-}  // namespace
 
 #define MARK(cls)          \
     do {                   \
         if (m) m->mark(cls, st); \
     } while (0)
+
+// the shift jobs of the list: begin, then rounds of trace / step
+void run_shift_jobs(const SceneView& s0, const FrameParams& fp, const Bufs& b, int mode, cudaStream_t st, Marker* m) {
+    const ShiftGrids& g = shift_grids();
+    const SceneView s = shift_view(s0);
+    cudaMemsetAsync(b.job_qcount, 0, 2 * sizeof(uint32_t), st);
+    k_shift_begin<<<g.begin, kPassBlock, 0, st>>>(s, fp, b, mode);
+    MARK(kClsShift);
+    for (int r = 0; r < kShiftRounds; ++r) {
+        const int cur = r & 1, nxt = cur ^ 1;
+        k_q_closest<ShiftJob><<<g.closest, kPassBlock, 0, st>>>(s, b.job_queue[2 * cur], b.job_qcount + 2 * cur, b.jobs);
+        k_q_shadow<ShiftJob><<<g.shadow, kPassBlock, 0, st>>>(s, b.job_queue[2 * cur + 1], b.job_qcount + 2 * cur + 1,
+                                                             b.jobs);
+        MARK(kClsTrace);
+        if (r + 1 < kShiftRounds) {
+            cudaMemsetAsync(b.job_qcount + 2 * nxt, 0, 2 * sizeof(uint32_t), st);
+            k_shift_step<false><<<g.step, kPassBlock, 0, st>>>(s, fp, b, mode, cur);
+        } else {
+            k_shift_step<true><<<g.step_last, kPassBlock, 0, st>>>(s, fp, b, mode, cur);
+        }
+        MARK(kClsShift);
+    }
+}
+
+}  // namespace
+
+uint32_t shift_launches_per_phase() { return 1 + 3 * kShiftRounds; }
 
 void launch_prefix_gen_temp_split(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out,
                                   cudaStream_t st, Marker* m) {
@@ -490,8 +701,7 @@ void launch_prefix_gen_temp_split(const SceneView& s, const FrameParams& fp, con
     cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
     k_prefix_finish<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, out);
     MARK(kClsShade);
-    k_prefix_shift_jobs<<<job_grid(), kPassBlock, 0, st>>>(s, fp, b);
-    MARK(kClsShift);
+    run_shift_jobs(s, fp, b, kModePrefix, st, m);
     k_prefix_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, out);
     MARK(kClsResample);
 }
@@ -501,8 +711,7 @@ void launch_suffix_gen_temp(const SceneView& s, const FrameParams& fp, const Buf
     cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
     k_suffix_temp_finish<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
     MARK(kClsShade);
-    k_shift_jobs<<<job_grid(), kPassBlock, 0, st>>>(s, b, kModeTemporal, fp.k);
-    MARK(kClsShift);
+    run_shift_jobs(s, fp, b, kModeTemporal, st, m);
     k_suffix_temp_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
     MARK(kClsResample);
 }
@@ -511,8 +720,7 @@ void launch_suffix_spatial(const SceneView& s, const FrameParams& fp, const Bufs
     cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
     k_suffix_spatial_select<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
     MARK(kClsResample);
-    k_shift_jobs<<<job_grid(), kPassBlock, 0, st>>>(s, b, kModeSpatial, fp.k);
-    MARK(kClsShift);
+    run_shift_jobs(s, fp, b, kModeSpatial, st, m);
     k_suffix_spatial_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
     MARK(kClsResample);
 }
@@ -525,8 +733,7 @@ void launch_final_gather_split(const SceneView& s, const FrameParams& fp, const 
     cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
     k_gather_query<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b);
     MARK(kClsSearch);
-    k_shift_jobs<<<job_grid(), kPassBlock, 0, st>>>(s, b, kModeGather, fp.k);
-    MARK(kClsShift);
+    run_shift_jobs(s, fp, b, kModeGather, st, m);
     k_gather_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, out);
     MARK(kClsResample);
 }

@@ -47,7 +47,9 @@ struct SceneView {
     uint32_t num_emitters;
     uint32_t num_tris;
     int* err;
-    unsigned long long* ray_count;  // [closest, shadow] or null
+    // [closest, shadow] or null; shift kernels get a view offset by 2 so
+    // their rays land in [2, 3] and their job count in [4]
+    unsigned long long* ray_count;
 };
 
 struct RayPre {

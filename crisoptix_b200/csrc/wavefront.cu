@@ -12,28 +12,16 @@
 //           into fresh records (final gather, FinalGatherCanon).
 #include <mutex>
 
+#include "queues.cuh"
 #include "records.cuh"
 
 namespace crisb {
 
 namespace {
 
-// Warp-aggregated append of `val` to queue q (count cnt) for the lanes with
-// `take` set.  Every lane of the warp must call this.
-RT_D void wf_append(uint32_t* q, uint32_t* cnt, bool take, uint32_t val) {
-    const unsigned mask = __ballot_sync(0xffffffffu, take);
-    if (!mask) return;
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(mask) - 1;
-    uint32_t base = 0;
-    if (lane == leader) base = atomicAdd(cnt, static_cast<uint32_t>(__popc(mask)));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (take) q[base + __popc(mask & ((1u << lane) - 1u))] = val;
-}
-
 RT_D void wf_push(const Bufs& b, int round, int req, uint32_t i) {
-    wf_append(b.wf_queue[2 * round], &b.wf_count[2 * round], req == kReqClosest, i);
-    wf_append(b.wf_queue[2 * round + 1], &b.wf_count[2 * round + 1], req == kReqShadow, i);
+    q_append(b.wf_queue[2 * round], &b.wf_count[2 * round], req == kReqClosest, i);
+    q_append(b.wf_queue[2 * round + 1], &b.wf_count[2 * round + 1], req == kReqShadow, i);
 }
 
 RT_D WfPath wf_blank() {
@@ -142,35 +130,6 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_gather(FrameParams fp, B
     wf_push(b, 0, req, i);
 }
 
-// ---- traversal kernels over the queues of round `cur` ------------------------------
-// Grid-stride loops over the queue.  A warp-synchronous variant with dynamic
-// ray fetching (refill idle lanes from per-warp batches) measured slower on
-// the 1080p workload (31 ms against 20 ms of trace per frame) at every refill
-// threshold: the per-step convergence removes the latency hiding between the
-// diverged inner-node and leaf lanes.
-__global__ void __launch_bounds__(kPassBlock) k_wf_closest(SceneView s, Bufs b, int cur) {
-    const uint32_t n = b.wf_count[2 * cur];
-    const uint32_t* q = b.wf_queue[2 * cur];
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const uint32_t i = q[t];
-        const float4 o = b.wf[i].ray_o, d = b.wf[i].ray_d;
-        count_ray(s, 0);
-        const RayPre r = make_ray(f3(o), f3(d));
-        const TraceResult h = traverse<false>(s, r, 1e-3f, 1e16f);
-        b.wf[i].hit = make_float4(__uint_as_float(h.prim), h.t, h.u, h.v);
-    }
-}
-
-__global__ void __launch_bounds__(kPassBlock) k_wf_shadow(SceneView s, Bufs b, int cur) {
-    const uint32_t n = b.wf_count[2 * cur + 1];
-    const uint32_t* q = b.wf_queue[2 * cur + 1];
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const uint32_t i = q[t];
-        const float4 o = b.wf[i].it_pos, d = b.wf[i].nee_dir;
-        b.wf[i].occluded = occluded(s, f3(o), f3(d), 1e-3f, d.w) ? 1u : 0u;
-    }
-}
-
 // ---- shading: resume every path whose ray of round `cur` finished ---------------------
 RT_D int wf_step(const SceneView& s, const FrameParams& fp, const Bufs& b, int flow, uint32_t i, WfPath& w,
                  Rng& rng) {
@@ -219,18 +178,6 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_shade(SceneView s, FrameParam
     }
 }
 
-inline unsigned grid_for(uint32_t n) { return (n + kPassBlock - 1) / kPassBlock; }
-
-unsigned persistent_grid(const void* kernel) {
-    int dev = 0, sms = 0, per_sm = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess &&
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPassBlock, 0) == cudaSuccess && sms > 0 &&
-        per_sm > 0)
-        return static_cast<unsigned>(sms * per_sm);
-    return 148u * 4u;
-}
-
 struct WfGrids {
     unsigned closest, shadow, shade;
 };
@@ -239,8 +186,8 @@ const WfGrids& wf_grids() {
     static std::once_flag once;
     static WfGrids g{};
     std::call_once(once, [] {
-        g.closest = persistent_grid(reinterpret_cast<const void*>(k_wf_closest));
-        g.shadow = persistent_grid(reinterpret_cast<const void*>(k_wf_shadow));
+        g.closest = persistent_grid(reinterpret_cast<const void*>(k_q_closest<WfPath>));
+        g.shadow = persistent_grid(reinterpret_cast<const void*>(k_q_shadow<WfPath>));
         g.shade = persistent_grid(reinterpret_cast<const void*>(k_wf_shade));
     });
     return g;
@@ -252,8 +199,9 @@ void wf_rounds(const SceneView& s, const FrameParams& fp, const Bufs& b, int flo
     const int rounds = fp.p.max_path_len + 2;
     for (int r = 0; r < rounds; ++r) {
         const int cur = r & 1, nxt = cur ^ 1;
-        k_wf_closest<<<g.closest, kPassBlock, 0, st>>>(s, b, cur);
-        k_wf_shadow<<<g.shadow, kPassBlock, 0, st>>>(s, b, cur);
+        k_q_closest<WfPath><<<g.closest, kPassBlock, 0, st>>>(s, b.wf_queue[2 * cur], b.wf_count + 2 * cur, b.wf);
+        k_q_shadow<WfPath><<<g.shadow, kPassBlock, 0, st>>>(s, b.wf_queue[2 * cur + 1], b.wf_count + 2 * cur + 1,
+                                                           b.wf);
         if (m) m->mark(kClsTrace, st);
         cudaMemsetAsync(b.wf_count + 2 * nxt, 0, 2 * sizeof(uint32_t), st);
         k_wf_shade<<<g.shade, kPassBlock, 0, st>>>(s, fp, b, flow, cur);

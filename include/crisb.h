@@ -256,9 +256,14 @@ typedef struct crisb_stats {
     float search_ms;
     float shade_ms;   /* path-machine shading steps and per-pass finish kernels */
     float other_ms;
-    /* rays traced in the frame (crisb_set_timing level 2 only) */
+    /* rays traced in the frame (crisb_set_timing level 2 only); the shift_*
+     * counts are the part traced inside shift jobs (path replays and
+     * reconnection visibility) and the number of shift jobs run */
     uint64_t closest_rays;
     uint64_t shadow_rays;
+    uint64_t shift_closest_rays;
+    uint64_t shift_shadow_rays;
+    uint64_t shift_jobs;
 } crisb_stats;
 
 /* debug buffer ids for crisb_debug_read */
