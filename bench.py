@@ -318,6 +318,8 @@ def run_crisb(args):
                  "shift_closest_rays_per_frame": rays["shift_closest_rays"],
                  "shift_shadow_rays_per_frame": rays["shift_shadow_rays"],
                  "shift_jobs_per_frame": rays["shift_jobs"],
+                 "node_visits_per_ray": rays["node_visits"] / max(n_rays, 1),
+                 "tri_tests_per_ray": rays["tri_tests"] / max(n_rays, 1),
                  "trace_ms": passes["trace_ms"],
                  "rays_per_s": n_rays / (passes["trace_ms"] / 1000.0) if passes["trace_ms"] > 0 else None,
                  "note": "closest / shadow queue traversal kernels of the path and shift machines; rays of shift "

@@ -239,6 +239,7 @@ struct crisb_scene {
         v.num_tris = num_tris;
         v.err = err_word;
         v.ray_count = nullptr;
+        v.trav_count = nullptr;
         return v;
     }
 };
@@ -603,8 +604,9 @@ struct crisb_renderer {
         last_stream = st;
         ktimer.n = 0;
         if (timing >= 2) {
-            check(cudaMemsetAsync(ray_count.p, 0, 5 * sizeof(unsigned long long), st), "memset");
+            check(cudaMemsetAsync(ray_count.p, 0, 7 * sizeof(unsigned long long), st), "memset");
             s.ray_count = ray_count.p;
+            s.trav_count = ray_count.p + 5;
         }
         Marker* m = marker();
         record(0, st);
@@ -843,7 +845,7 @@ int crisb_set_timing(crisb_renderer* r, int enable) {
             for (auto& e : r->ev) check(cudaEventCreate(&e), "event create");
             for (auto& e : r->ktimer.ev) check(cudaEventCreate(&e), "event create");
         }
-        if (enable >= 2 && !r->ray_count.p) r->ray_count.alloc(5);
+        if (enable >= 2 && !r->ray_count.p) r->ray_count.alloc(7);
         r->timing = enable;
     });
 }
@@ -879,13 +881,15 @@ int crisb_get_stats(crisb_renderer* r, crisb_stats* out) {
         out->shade_ms = cls_ms[kClsShade];
         out->other_ms = cls_ms[kClsOther];
         if (r->timing >= 2) {
-            unsigned long long rc[5] = {0, 0, 0, 0, 0};
+            unsigned long long rc[7] = {0, 0, 0, 0, 0, 0, 0};
             check(cudaMemcpy(rc, r->ray_count.p, sizeof(rc), cudaMemcpyDeviceToHost), "ray counters");
             out->closest_rays = rc[0] + rc[2];
             out->shadow_rays = rc[1] + rc[3];
             out->shift_closest_rays = rc[2];
             out->shift_shadow_rays = rc[3];
             out->shift_jobs = rc[4];
+            out->node_visits = rc[5];
+            out->tri_tests = rc[6];
         }
     });
 }

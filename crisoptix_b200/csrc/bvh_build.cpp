@@ -52,7 +52,7 @@ struct BinNode {
 
 constexpr int kBins = 32;
 constexpr float kCostNode = 1.0f;
-constexpr float kCostTri = 1.0f;
+constexpr float kCostTri = 2.0f;
 constexpr uint32_t kParallelMin = 1u << 15;
 
 struct Builder {

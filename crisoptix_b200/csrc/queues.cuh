@@ -61,28 +61,28 @@ RT_D void set_occluded(ShiftJob& j, uint32_t v) { j.hit.x = __uint_as_float(v); 
 // the 1080p workload (31 ms against 20 ms of trace per frame) at every refill
 // threshold: the per-step convergence removes the latency hiding between the
 // diverged inner-node and leaf lanes.
+// One launch per round over both queues: entries [0, nc) of the closest-hit
+// queue, then [nc, nc + ns) of the shadow queue, so the two queues' tails
+// (the last, slowest rays) overlap instead of running back to back.
 template <class R>
-__global__ void __launch_bounds__(kPassBlock) k_q_closest(SceneView s, const uint32_t* q, const uint32_t* cnt, R* rec) {
-    const uint32_t n = *cnt;
+__global__ void __launch_bounds__(kPassBlock) k_q_trace(SceneView s, const uint32_t* qc, const uint32_t* ccnt,
+                                                        const uint32_t* qs, const uint32_t* scnt, R* rec) {
+    const uint32_t nc = *ccnt, ns = *scnt;
+    const uint32_t n = nc + ns;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const uint32_t i = q[t];
         V3 o, d;
-        closest_ray(rec[i], o, d);
-        count_ray(s, 0);
-        const TraceResult h = traverse<false>(s, make_ray(o, d), 1e-3f, 1e16f);
-        set_hit(rec[i], make_float4(__uint_as_float(h.prim), h.t, h.u, h.v));
-    }
-}
-
-template <class R>
-__global__ void __launch_bounds__(kPassBlock) k_q_shadow(SceneView s, const uint32_t* q, const uint32_t* cnt, R* rec) {
-    const uint32_t n = *cnt;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const uint32_t i = q[t];
-        V3 o, d;
-        float tmax;
-        shadow_ray(rec[i], o, d, tmax);
-        set_occluded(rec[i], occluded(s, o, d, 1e-3f, tmax) ? 1u : 0u);
+        if (t < nc) {
+            const uint32_t i = qc[t];
+            closest_ray(rec[i], o, d);
+            count_ray(s, 0);
+            const TraceResult h = traverse<false>(s, make_ray(o, d), 1e-3f, 1e16f);
+            set_hit(rec[i], make_float4(__uint_as_float(h.prim), h.t, h.u, h.v));
+        } else {
+            const uint32_t i = qs[t - nc];
+            float tmax;
+            shadow_ray(rec[i], o, d, tmax);
+            set_occluded(rec[i], occluded(s, o, d, 1e-3f, tmax) ? 1u : 0u);
+        }
     }
 }
 

@@ -642,7 +642,7 @@ __global__ void __launch_bounds__(kPassBlock) k_prefix_combine(FrameParams fp, B
 }
 
 struct ShiftGrids {
-    unsigned begin, step, step_last, closest, shadow;
+    unsigned begin, step, step_last, trace;
 };
 
 const ShiftGrids& shift_grids() {
@@ -652,8 +652,7 @@ const ShiftGrids& shift_grids() {
         g.begin = persistent_grid(reinterpret_cast<const void*>(k_shift_begin));
         g.step = persistent_grid(reinterpret_cast<const void*>(k_shift_step<false>));
         g.step_last = persistent_grid(reinterpret_cast<const void*>(k_shift_step<true>));
-        g.closest = persistent_grid(reinterpret_cast<const void*>(k_q_closest<ShiftJob>));
-        g.shadow = persistent_grid(reinterpret_cast<const void*>(k_q_shadow<ShiftJob>));
+        g.trace = persistent_grid(reinterpret_cast<const void*>(k_q_trace<ShiftJob>));
     });
     return g;
 }
@@ -672,9 +671,9 @@ void run_shift_jobs(const SceneView& s0, const FrameParams& fp, const Bufs& b, i
     MARK(kClsShift);
     for (int r = 0; r < kShiftRounds; ++r) {
         const int cur = r & 1, nxt = cur ^ 1;
-        k_q_closest<ShiftJob><<<g.closest, kPassBlock, 0, st>>>(s, b.job_queue[2 * cur], b.job_qcount + 2 * cur, b.jobs);
-        k_q_shadow<ShiftJob><<<g.shadow, kPassBlock, 0, st>>>(s, b.job_queue[2 * cur + 1], b.job_qcount + 2 * cur + 1,
-                                                             b.jobs);
+        k_q_trace<ShiftJob><<<g.trace, kPassBlock, 0, st>>>(s, b.job_queue[2 * cur], b.job_qcount + 2 * cur,
+                                                            b.job_queue[2 * cur + 1], b.job_qcount + 2 * cur + 1,
+                                                            b.jobs);
         MARK(kClsTrace);
         if (r + 1 < kShiftRounds) {
             cudaMemsetAsync(b.job_qcount + 2 * nxt, 0, 2 * sizeof(uint32_t), st);
@@ -688,7 +687,7 @@ void run_shift_jobs(const SceneView& s0, const FrameParams& fp, const Bufs& b, i
 
 }  // namespace
 
-uint32_t shift_launches_per_phase() { return 1 + 3 * kShiftRounds; }
+uint32_t shift_launches_per_phase() { return 1 + 2 * kShiftRounds; }
 
 void launch_prefix_gen_temp_split(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out,
                                   cudaStream_t st, Marker* m) {

@@ -50,6 +50,7 @@ struct SceneView {
     // [closest, shadow] or null; shift kernels get a view offset by 2 so
     // their rays land in [2, 3] and their job count in [4]
     unsigned long long* ray_count;
+    unsigned long long* trav_count;  // [node visits, triangle tests] or null
 };
 
 struct RayPre {
@@ -180,7 +181,7 @@ struct Trav {
     float tmin, tmax;
     TraceResult best;
     int sp, cur;
-    uint32_t visits;
+    uint32_t visits, tris;
 
     RT_D void init(const RayPre& ray, float t0, float t1) {
         r = ray;
@@ -190,6 +191,7 @@ struct Trav {
         sp = 0;
         cur = 0;
         visits = 0;
+        tris = 0;
     }
 
     RT_D float bound() const { return best.prim == CRISB_INVALID_PRIM ? tmax : best.t; }
@@ -197,6 +199,7 @@ struct Trav {
     // triangles [first, first + count) of the leaf order; true when an
     // any-hit query is answered
     RT_D bool leaf(const SceneView& s, int first, int count) {
+        tris += static_cast<uint32_t>(count);
         for (int k = 0; k < count; ++k) {
             const float4 q0 = __ldg(&s.tris[3 * (first + k) + 0]);
             const float4 q1 = __ldg(&s.tris[3 * (first + k) + 1]);
@@ -303,6 +306,18 @@ struct Trav {
     }
 };
 
+// statistics: node visits and triangle tests of a finished ray (one
+// warp-aggregated atomic each)
+RT_D void count_trav(const SceneView& s, uint32_t visits, uint32_t tris) {
+    if (!s.trav_count) return;
+    const unsigned m = __activemask();
+    const uint32_t v = __reduce_add_sync(m, visits), t = __reduce_add_sync(m, tris);
+    if ((threadIdx.x & 31) == __ffs(m) - 1) {
+        atomicAdd(&s.trav_count[0], static_cast<unsigned long long>(v));
+        atomicAdd(&s.trav_count[1], static_cast<unsigned long long>(t));
+    }
+}
+
 // Closest hit (any_hit == false) or first hit (any_hit == true) over the BVH.
 template <bool kAnyHit>
 RT_D TraceResult traverse(const SceneView& s, const RayPre& r, float tmin, float tmax) {
@@ -311,6 +326,7 @@ RT_D TraceResult traverse(const SceneView& s, const RayPre& r, float tmin, float
     t.init(r, tmin, tmax);
     while (!t.step(s, st)) {
     }
+    count_trav(s, t.visits, t.tris);
     return t.best;
 }
 

@@ -179,15 +179,14 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_shade(SceneView s, FrameParam
 }
 
 struct WfGrids {
-    unsigned closest, shadow, shade;
+    unsigned trace, shade;
 };
 
 const WfGrids& wf_grids() {
     static std::once_flag once;
     static WfGrids g{};
     std::call_once(once, [] {
-        g.closest = persistent_grid(reinterpret_cast<const void*>(k_q_closest<WfPath>));
-        g.shadow = persistent_grid(reinterpret_cast<const void*>(k_q_shadow<WfPath>));
+        g.trace = persistent_grid(reinterpret_cast<const void*>(k_q_trace<WfPath>));
         g.shade = persistent_grid(reinterpret_cast<const void*>(k_wf_shade));
     });
     return g;
@@ -199,9 +198,8 @@ void wf_rounds(const SceneView& s, const FrameParams& fp, const Bufs& b, int flo
     const int rounds = fp.p.max_path_len + 2;
     for (int r = 0; r < rounds; ++r) {
         const int cur = r & 1, nxt = cur ^ 1;
-        k_q_closest<WfPath><<<g.closest, kPassBlock, 0, st>>>(s, b.wf_queue[2 * cur], b.wf_count + 2 * cur, b.wf);
-        k_q_shadow<WfPath><<<g.shadow, kPassBlock, 0, st>>>(s, b.wf_queue[2 * cur + 1], b.wf_count + 2 * cur + 1,
-                                                           b.wf);
+        k_q_trace<WfPath><<<g.trace, kPassBlock, 0, st>>>(s, b.wf_queue[2 * cur], b.wf_count + 2 * cur,
+                                                          b.wf_queue[2 * cur + 1], b.wf_count + 2 * cur + 1, b.wf);
         if (m) m->mark(kClsTrace, st);
         cudaMemsetAsync(b.wf_count + 2 * nxt, 0, 2 * sizeof(uint32_t), st);
         k_wf_shade<<<g.shade, kPassBlock, 0, st>>>(s, fp, b, flow, cur);
@@ -211,7 +209,7 @@ void wf_rounds(const SceneView& s, const FrameParams& fp, const Bufs& b, int flo
 
 }  // namespace
 
-uint32_t wf_launches_per_pass(const FrameParams& fp) { return 1 + 3 * static_cast<uint32_t>(fp.p.max_path_len + 2); }
+uint32_t wf_launches_per_pass(const FrameParams& fp) { return 1 + 2 * static_cast<uint32_t>(fp.p.max_path_len + 2); }
 
 void launch_wf_prefix(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m) {
     cudaMemsetAsync(b.wf_count, 0, 2 * sizeof(uint32_t), st);

@@ -264,6 +264,10 @@ typedef struct crisb_stats {
     uint64_t shift_closest_rays;
     uint64_t shift_shadow_rays;
     uint64_t shift_jobs;
+    /* traversal work of all rays of the frame: wide-node visits and
+     * ray/triangle tests (level 2 only) */
+    uint64_t node_visits;
+    uint64_t tri_tests;
 } crisb_stats;
 
 /* debug buffer ids for crisb_debug_read */
