@@ -196,6 +196,22 @@ struct Trav {
 
     RT_D float bound() const { return best.prim == CRISB_INVALID_PRIM ? tmax : best.t; }
 
+    // slab() with the near / far plane of each axis chosen by the sign of the
+    // inverse direction: the same values as the min / max form, since
+    // (lo - o) * inv <= (hi - o) * inv exactly when inv > 0 (rounding is
+    // monotonic) and the inverse direction is never zero or NaN
+    RT_D bool slab_nf(float nx, float fx, float ny, float fy, float nz, float fz, float tmax_, float& tnear) const {
+        float tn = (nx - r.org.x) * r.inv.x, tf = (fx - r.org.x) * r.inv.x;
+        tn = fmaxf(tn, (ny - r.org.y) * r.inv.y);
+        tf = fminf(tf, (fy - r.org.y) * r.inv.y);
+        tn = fmaxf(tn, (nz - r.org.z) * r.inv.z);
+        tf = fminf(tf, (fz - r.org.z) * r.inv.z);
+        tn = fmaxf(tn, tmin);
+        tf = fminf(tf, tmax_);
+        tnear = tn;
+        return tn <= tf * kSlabFarScale;
+    }
+
     // triangles [first, first + count) of the leaf order; true when an
     // any-hit query is answered
     RT_D bool leaf(const SceneView& s, int first, int count) {
@@ -233,9 +249,15 @@ struct Trav {
             dev_error(s, kDevErrIterations);
             return true;
         }
+        // rows of the node: lo_x hi_x lo_y hi_y lo_z hi_z (one float4 per
+        // plane over the four children), links, counts.  Per axis the near
+        // plane is lo for a positive inverse direction and hi otherwise, so
+        // min(t_lo, t_hi) of the slab test is the near plane's t.
         const float4* np = reinterpret_cast<const float4*>(s.nodes + cur);
-        const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2);
-        const float4 hy = __ldg(np + 3), lz = __ldg(np + 4), hz = __ldg(np + 5);
+        const int sx = signbit(r.inv.x) ? 1 : 0, sy = signbit(r.inv.y) ? 1 : 0, sz = signbit(r.inv.z) ? 1 : 0;
+        const float4 nx = __ldg(np + sx), fx = __ldg(np + (1 - sx));
+        const float4 ny = __ldg(np + 2 + sy), fy = __ldg(np + 3 - sy);
+        const float4 nz = __ldg(np + 4 + sz), fz = __ldg(np + 5 - sz);
         const int4 lk = __ldg(reinterpret_cast<const int4*>(np + 6));
         const int4 ct = __ldg(reinterpret_cast<const int4*>(np + 7));
         const float bnd = bound();
@@ -243,10 +265,10 @@ struct Trav {
         const int cnt[4] = {ct.x, ct.y, ct.z, ct.w};
         float tn[4];
         bool hit[4];
-        hit[0] = link[0] != kNoChild && slab(r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, tmin, bnd, tn[0]);
-        hit[1] = link[1] != kNoChild && slab(r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, tmin, bnd, tn[1]);
-        hit[2] = link[2] != kNoChild && slab(r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, tmin, bnd, tn[2]);
-        hit[3] = link[3] != kNoChild && slab(r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, tmin, bnd, tn[3]);
+        hit[0] = link[0] != kNoChild && slab_nf(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, bnd, tn[0]);
+        hit[1] = link[1] != kNoChild && slab_nf(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, bnd, tn[1]);
+        hit[2] = link[2] != kNoChild && slab_nf(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, bnd, tn[2]);
+        hit[3] = link[3] != kNoChild && slab_nf(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, bnd, tn[3]);
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             if (!hit[c] || link[c] >= 0) continue;

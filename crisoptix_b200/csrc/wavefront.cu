@@ -10,6 +10,7 @@
 //           reservoir prefix (suffix temporal pass);
 //   gather: TracePrefix, then TraceSuffix when the prefix ends without NEE,
 //           into fresh records (final gather, FinalGatherCanon).
+#include <algorithm>
 #include <mutex>
 
 #include "queues.cuh"
@@ -156,12 +157,34 @@ RT_D int wf_step(const SceneView& s, const FrameParams& fp, const Bufs& b, int f
     return req;
 }
 
+// the ray a path asked for, traced in place (the queue kernels' semantics)
+RT_D void wf_trace_inline(const SceneView& s, WfPath& w, int req) {
+    V3 o, d;
+    if (req == kReqClosest) {
+        closest_ray(w, o, d);
+        count_ray(s, 0);
+        const TraceResult h = traverse<false>(s, make_ray(o, d), 1e-3f, 1e16f);
+        set_hit(w, make_float4(__uint_as_float(h.prim), h.t, h.u, h.v));
+    } else {
+        float tmax;
+        shadow_ray(w, o, d, tmax);
+        set_occluded(w, occluded(s, o, d, 1e-3f, tmax) ? 1u : 0u);
+    }
+}
+
+// Resume every path whose ray of round `cur` finished and queue its next ray;
+// with kInline (the last wavefront round) trace the path's remaining rays in
+// place until it ends, so the few long paths left do not cost a trace and a
+// shade launch per bounce.
+template <bool kInline>
 __global__ void __launch_bounds__(kPassBlock) k_wf_shade(SceneView s, FrameParams fp, Bufs b, int flow, int cur) {
     const uint32_t nc = b.wf_count[2 * cur], ns = b.wf_count[2 * cur + 1];
     const uint32_t total = nc + ns;
     const uint32_t* qc = b.wf_queue[2 * cur];
     const uint32_t* qs = b.wf_queue[2 * cur + 1];
     const int nxt = cur ^ 1;
+    // a path traces at most a prefix, a suffix and one shadow ray per vertex
+    const int max_steps = 4 * (fp.p.max_path_len + 2);
     for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
         const uint32_t t = base + threadIdx.x;
         int req = kReqDone;
@@ -171,15 +194,26 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_shade(SceneView s, FrameParam
             WfPath w = b.wf[i];
             Rng rng{w.rng};
             req = wf_step(s, fp, b, flow, i, w, rng);
+            if (kInline) {
+                for (int k = 0; req != kReqDone; ++k) {
+                    if (k >= max_steps) {
+                        dev_error(s, kDevErrIterations);
+                        break;
+                    }
+                    wf_trace_inline(s, w, req);
+                    req = wf_step(s, fp, b, flow, i, w, rng);
+                }
+                req = kReqDone;
+            }
             w.rng = rng.state;
             b.wf[i] = w;
         }
-        wf_push(b, nxt, req, i);
+        if (!kInline) wf_push(b, nxt, req, i);
     }
 }
 
 struct WfGrids {
-    unsigned trace, shade;
+    unsigned trace, shade, shade_inline;
 };
 
 const WfGrids& wf_grids() {
@@ -187,29 +221,41 @@ const WfGrids& wf_grids() {
     static WfGrids g{};
     std::call_once(once, [] {
         g.trace = persistent_grid(reinterpret_cast<const void*>(k_q_trace<WfPath>));
-        g.shade = persistent_grid(reinterpret_cast<const void*>(k_wf_shade));
+        g.shade = persistent_grid(reinterpret_cast<const void*>(k_wf_shade<false>));
+        g.shade_inline = persistent_grid(reinterpret_cast<const void*>(k_wf_shade<true>));
     });
     return g;
 }
 
-// rounds after the init kernel: every path traces at most max_path_len + 1 rays
+// Wavefront rounds of a pass: a path traces at most max_path_len + 1 rays
+// after its first; the shading kernel of the last round finishes any path
+// still running in place.  Finishing in place from an earlier round (3 to 6)
+// saved traversal launches but cost as much in the in-place kernel on the
+// 1080p workload (24.2 ms/frame either way).
+int wf_round_count(const FrameParams& fp) { return fp.p.max_path_len + 2; }
+
+// rounds after the init kernel
 void wf_rounds(const SceneView& s, const FrameParams& fp, const Bufs& b, int flow, cudaStream_t st, Marker* m) {
     const WfGrids& g = wf_grids();
-    const int rounds = fp.p.max_path_len + 2;
+    const int rounds = wf_round_count(fp);
     for (int r = 0; r < rounds; ++r) {
         const int cur = r & 1, nxt = cur ^ 1;
         k_q_trace<WfPath><<<g.trace, kPassBlock, 0, st>>>(s, b.wf_queue[2 * cur], b.wf_count + 2 * cur,
                                                           b.wf_queue[2 * cur + 1], b.wf_count + 2 * cur + 1, b.wf);
         if (m) m->mark(kClsTrace, st);
-        cudaMemsetAsync(b.wf_count + 2 * nxt, 0, 2 * sizeof(uint32_t), st);
-        k_wf_shade<<<g.shade, kPassBlock, 0, st>>>(s, fp, b, flow, cur);
+        if (r + 1 < rounds) {
+            cudaMemsetAsync(b.wf_count + 2 * nxt, 0, 2 * sizeof(uint32_t), st);
+            k_wf_shade<false><<<g.shade, kPassBlock, 0, st>>>(s, fp, b, flow, cur);
+        } else {
+            k_wf_shade<true><<<g.shade_inline, kPassBlock, 0, st>>>(s, fp, b, flow, cur);
+        }
         if (m) m->mark(kClsShade, st);
     }
 }
 
 }  // namespace
 
-uint32_t wf_launches_per_pass(const FrameParams& fp) { return 1 + 2 * static_cast<uint32_t>(fp.p.max_path_len + 2); }
+uint32_t wf_launches_per_pass(const FrameParams& fp) { return 1 + 2 * static_cast<uint32_t>(wf_round_count(fp)); }
 
 void launch_wf_prefix(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m) {
     cudaMemsetAsync(b.wf_count, 0, 2 * sizeof(uint32_t), st);
