@@ -70,6 +70,15 @@ def params_for(name: str, scene_size: float):
     return p
 
 
+def config_for(name: str, W: int, H: int, n_tris: int, p, ppp: int, world: int) -> dict:
+    """The `config` object of both arms' JSON lines."""
+    return {"workload": f"{name}: {W}x{H} conditional ReSTIR PT, {n_tris} triangles, k={p.gather_m - 1}, "
+                        f"{p.suffix_spatial_rounds}x{p.suffix_spatial_count} spatial, max depth {p.max_path_len}, "
+                        f"FP32 storage",
+            "paths_per_pixel": ppp, "l2": "working set (reservoirs, BVH) larger than L2",
+            "parallelism": f"view-sharded replicas x{world}"}
+
+
 # Compulsory bytes per pixel per frame of the resampling kernels (the
 # bandwidth-bound part of each reuse pass: MIS weights and reservoir
 # streaming over records and shift results).  Every record a kernel touches
@@ -191,7 +200,8 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
             "steps": frames, "warmup": min(args.warmup, 1), "ms_per_step": cb["ms_per_frame"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: {W}x{H} conditional ReSTIR PT frame (CPU sample {cb['sample']})"},
+            "config": config_for(args.workload, W, H, desc.num_world_triangles, params_for(args.workload, 1.0), ppp,
+                                 args.gpus),
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "CrisOptix needs the OptiX SDK and an OpenGL window; its CPU-side stand-in is the oracle port "
@@ -202,7 +212,7 @@ def run_reference(args):
 def run_crisb(args):
     import torch
 
-    from crisoptix_b200 import Renderer, Scene, _abi, scenes
+    from crisoptix_b200 import Renderer, Scene, _abi, scenes, sharding
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -224,7 +234,7 @@ def run_crisb(args):
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
     out = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
-    offset = rank * 60 // max(world, 1)  # each rank renders its own view of the orbit
+    offset = sharding.orbit_offset(rank, world)  # each rank renders its own view of the orbit
     n_frames = args.warmup + args.steps
     cams = [scenes.orbit_camera(cam, offset + f, 60) for f in range(2 * n_frames + 8)]
 
@@ -252,14 +262,10 @@ def run_crisb(args):
     clk = clocks.stop()
     if dist:
         dist.barrier()
-    ms = t_start.elapsed_time(t_end)
     launches_per_frame = r.stats()["kernel_launches"]
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = sharding.max_over_ranks(t_start.elapsed_time(t_end), dist, "cuda")
     ms_per_frame = ms / args.steps
-    value = ppp * W * H * args.steps * world / (ms / 1000.0)
+    value = sharding.whole_job_rate(ppp * W * H, args.steps, world, ms)
 
     # ---- per-pass and per-kernel-class breakdown (CUDA events on the stream) ----
     r.set_timing(1)
@@ -292,12 +298,8 @@ def run_crisb(args):
             host.copy_(out, non_blocking=True)
     e_end.record(stream)
     torch.cuda.synchronize()
-    e_ms = e_start.elapsed_time(e_end)
-    if dist:
-        t = torch.tensor([e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e_ms = float(t.item())
-    e2e_value = ppp * W * H * e_steps * world / (e_ms / 1000.0)
+    e_ms = sharding.max_over_ranks(e_start.elapsed_time(e_end), dist, "cuda")
+    e2e_value = sharding.whole_job_rate(ppp * W * H, e_steps, world, e_ms)
     img_mean = float(host.mean())
 
     # ---- roofline of the resampling kernels; traversal in rays/s -----------------
@@ -337,11 +339,7 @@ def run_crisb(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_frame, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: {W}x{H} conditional ReSTIR PT, {sc.num_triangles} triangles, "
-                                   f"k={p.gather_m - 1}, {p.suffix_spatial_rounds}x{p.suffix_spatial_count} spatial, "
-                                   f"max depth {p.max_path_len}, FP32 storage",
-                       "paths_per_pixel": ppp, "l2": "working set (reservoirs, BVH) larger than L2",
-                       "parallelism": f"view-sharded replicas x{world}"},
+            "config": config_for(args.workload, W, H, sc.num_triangles, p, ppp, world),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 48, "d2h_bytes_per_step": W * H * 12},
             "roofline": roofline, "traversal": traversal, "phases_ms": phases, "pass_ms": pass_ms,
             "cpu_baseline": cb, "clocks": clk,
