@@ -97,11 +97,11 @@ def resample_bytes(k: int, spatial_count: int, spatial_rounds: int, copy_prefix_
             "gather_combine": gather_combine}
 
 
-# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
-# dominant kernel from one ncu capture, with the pixel count it was taken at;
-# scaled by pixels to the bench resolution.  Source:
-# profiles/k_final_gather_large_480x270.md
-PROFILED_TRAFFIC = {}
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the seven
+# resampling launches of one frame, from one ncu capture of the large workload
+# at 960x540 (518,400 px, caches flushed before each launch), with the pixel
+# count it was taken at; scaled by pixels to the bench resolution.
+PROFILED_TRAFFIC = {"resampling": (934.06e6, 960 * 540)}
 
 
 class ClockSampler:
