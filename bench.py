@@ -70,13 +70,13 @@ def params_for(name: str, scene_size: float):
     return p
 
 
-def config_for(name: str, W: int, H: int, n_tris: int, p, ppp: int, world: int) -> dict:
+def config_for(name: str, W: int, H: int, n_tris: int, p, ppp: int, world: int, graph: bool = True) -> dict:
     """The `config` object of both arms' JSON lines."""
     return {"workload": f"{name}: {W}x{H} conditional ReSTIR PT, {n_tris} triangles, k={p.gather_m - 1}, "
                         f"{p.suffix_spatial_rounds}x{p.suffix_spatial_count} spatial, max depth {p.max_path_len}, "
                         f"FP32 storage",
             "paths_per_pixel": ppp, "l2": "working set (reservoirs, BVH) larger than L2",
-            "parallelism": f"view-sharded replicas x{world}"}
+            "parallelism": f"view-sharded replicas x{world}", "frame_as_cuda_graph": graph}
 
 
 # Compulsory bytes per pixel per frame of the resampling kernels (the
@@ -231,6 +231,7 @@ def run_crisb(args):
     sc = Scene(desc)
     p = params_for(args.workload, sc.scene_size)
     r = Renderer(W, H, sc, p)
+    r.set_graph(not args.no_graph)
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
     out = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
@@ -339,7 +340,7 @@ def run_crisb(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_frame, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config_for(args.workload, W, H, sc.num_triangles, p, ppp, world),
+            "config": config_for(args.workload, W, H, sc.num_triangles, p, ppp, world, not args.no_graph),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 48, "d2h_bytes_per_step": W * H * 12},
             "roofline": roofline, "traversal": traversal, "phases_ms": phases, "pass_ms": pass_ms,
             "cpu_baseline": cb, "clocks": clk,
@@ -355,6 +356,7 @@ def main():
     ap.add_argument("--impl", default="crisb", choices=["crisb", "reference"])
     ap.add_argument("--workload", default="large", choices=["large", "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="launch kernels directly instead of one CUDA graph per frame")
     ap.add_argument("--cpu-scale", type=int, default=2)
     ap.add_argument("--res", default=None, help="WxH override of the workload resolution (profiling runs)")
     args = ap.parse_args()

@@ -198,6 +198,11 @@ class Renderer:
         check(load().crisb_frame_random(self.handle, ctypes.byref(v)))
         return v.value
 
+    def set_graph(self, enable: bool):
+        """Run frames as one CUDA graph of the pass chain (default) or launch
+        the kernels directly; the results are identical."""
+        check(load().crisb_set_graph(self.handle, 1 if enable else 0))
+
     def set_timing(self, level: int):
         """0 off, 1 per-pass / per-kernel-class CUDA events, 2 also ray counters."""
         check(load().crisb_set_timing(self.handle, int(level)))

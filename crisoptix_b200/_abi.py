@@ -152,6 +152,7 @@ ENTRY_POINTS = {
     "crisb_renderer_set_params": (c_i32, [c_vp, ctypes.POINTER(Params)]),
     "crisb_renderer_get_params": (c_i32, [c_vp, ctypes.POINTER(Params)]),
     "crisb_render_frame": (c_i32, [c_vp, ctypes.POINTER(Camera), c_vp, c_vp]),
+    "crisb_set_graph": (c_i32, [c_vp, c_i32]),
     "crisb_frame_index": (c_i32, [c_vp, ctypes.POINTER(c_u64)]),
     "crisb_frame_random": (c_i32, [c_vp, ctypes.POINTER(c_u32)]),
     "crisb_set_timing": (c_i32, [c_vp, c_i32]),

@@ -504,6 +504,8 @@ struct crisb_renderer {
     }
 
     ~crisb_renderer() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        if (cap_stream) cudaStreamDestroy(cap_stream);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         for (auto& e : ktimer.ev)
@@ -575,7 +577,55 @@ struct crisb_renderer {
         if (timing) check(cudaEventRecord(ev[slot], st), "event");
     }
 
+    // The frame's pass chain as one CUDA graph: the launches are captured on a
+    // private stream (nothing runs during capture), the executable graph is
+    // updated in place when only kernel parameters changed (camera, frame
+    // random, buffer roles) and re-instantiated otherwise, then launched on the
+    // caller's stream.  Per-kernel timing records events between launches, so
+    // timed frames launch directly.
+    bool graph_enabled = true;
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+
     void render(const crisb_camera& cam, float* out, cudaStream_t st) {
+        if (!graph_enabled || timing) {
+            enqueue(cam, out, st);
+            return;
+        }
+        if (!cap_stream) check(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking), "capture stream");
+        check(cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeRelaxed), "begin capture");
+        cudaGraph_t g = nullptr;
+        try {
+            enqueue(cam, out, cap_stream);
+        } catch (...) {
+            cudaStreamEndCapture(cap_stream, &g);
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            throw;
+        }
+        check(cudaStreamEndCapture(cap_stream, &g), "end capture");
+        if (graph_exec) {
+            cudaGraphExecUpdateResultInfo info;
+            if (cudaGraphExecUpdate(graph_exec, g, &info) != cudaSuccess) {
+                cudaGetLastError();
+                cudaGraphExecDestroy(graph_exec);
+                graph_exec = nullptr;
+            }
+        }
+        if (!graph_exec) {
+            const cudaError_t e = cudaGraphInstantiate(&graph_exec, g, 0);
+            if (e != cudaSuccess) {
+                cudaGraphDestroy(g);
+                graph_exec = nullptr;
+                check(e, "graph instantiate");
+            }
+        }
+        cudaGraphDestroy(g);
+        check(cudaGraphLaunch(graph_exec, st), "graph launch");
+        last_stream = st;
+    }
+
+    void enqueue(const crisb_camera& cam, float* out, cudaStream_t st) {
         require(out != nullptr, "render_frame: null output");
         launches = 0;
         // Renderer::LaunchFrame (src/Renderer.cpp:211-232)
@@ -820,6 +870,13 @@ int crisb_render_frame(crisb_renderer* r, const crisb_camera* cam, float* out_rg
     return guarded([&] {
         require(r && cam, "null argument");
         r->render(*cam, out_rgb_dev, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int crisb_set_graph(crisb_renderer* r, int enable) {
+    return guarded([&] {
+        require(r != nullptr, "null renderer");
+        r->graph_enabled = enable != 0;
     });
 }
 

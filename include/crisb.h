@@ -374,6 +374,13 @@ int crisb_render_frame(crisb_renderer* r, const crisb_camera* cam,
                        float* out_rgb_dev, void* stream);
 
 /* Renderer::GetFrameIdx (src/Renderer.cpp:408-411). */
+/* Frames run as one CUDA graph of the pass chain by default (captured, updated in
+ * place and launched on the caller's stream); 0 launches the kernels directly.
+ * Frames with per-kernel timing on (crisb_set_timing) always launch directly.
+ * Results are identical either way.  No counterpart in the reference, whose
+ * LaunchFrame synchronises the device between passes (src/Renderer.cpp:253-405). */
+int crisb_set_graph(crisb_renderer* r, int enable);
+
 int crisb_frame_index(const crisb_renderer* r, uint64_t* out);
 /* per-frame random value the last frame used (params.random) */
 int crisb_frame_random(const crisb_renderer* r, uint32_t* out);

@@ -53,7 +53,7 @@ def test_flattened_instances_match_float64_reference(cuda_device):
     assert (mat == rm).all()
 
 
-def run_parity(desc, cam, params, W, H, frames, cam_fn, change_params=None, timing=0):
+def run_parity(desc, cam, params, W, H, frames, cam_fn, change_params=None, timing=0, graph=lambda f: True):
     sc = Scene(desc)
     tri = sc.read_triangles()
     o = op.Oracle.from_scene(desc, W, H, params, triangles=tri)
@@ -67,6 +67,7 @@ def run_parity(desc, cam, params, W, H, frames, cam_fn, change_params=None, timi
             r.params = params
             o.set_params(params)
         c = cam_fn(cam, f)
+        r.set_graph(graph(f))
         r.launch_frame(c, out_d.data_ptr())
         torch.cuda.synchronize()
         o.render_frame(c, out_h)
@@ -126,3 +127,19 @@ def test_timing_and_ray_counters_do_not_change_results(cuda_device):
     desc, cam = small_sphere_room()
     p = large_config_params(scene_size_of(desc), gather_radius=0.3)
     run_parity(desc, cam, p, 48, 40, 3, lambda c, f: orbit(c, f, 120), timing=2)
+
+
+def test_direct_launches_match(cuda_device):
+    """Frames launched kernel by kernel instead of as one CUDA graph."""
+    desc, cam = small_sphere_room()
+    p = large_config_params(scene_size_of(desc), gather_radius=0.3)
+    run_parity(desc, cam, p, 48, 40, 3, lambda c, f: orbit(c, f, 120), graph=lambda f: False)
+
+
+def test_graph_and_direct_frames_interleaved(cuda_device):
+    """Graph frames, direct frames and a parameter change that alters the
+    graph's shape, in one sequence."""
+    desc, cam = scenes.cornell_box()
+    p0 = small_config_params(scene_size_of(desc))
+    p1 = small_config_params(scene_size_of(desc), gather_m=4, gather_radius=0.4, suffix_spatial_rounds=2)
+    run_parity(desc, cam, p0, 32, 32, 6, static, change_params={3: p1}, graph=lambda f: f % 3 != 1)
