@@ -333,6 +333,13 @@ def run_crisb(args):
         dist.destroy_process_group()
     if rank != 0:
         return
+    qual = None
+    if args.relmse > 0:
+        # relMSE of orbit frame 30 against an FP64-accumulated path-traced
+        # reference of that frame's camera
+        from crisoptix_b200 import quality
+
+        qual = quality.score(sc, W, H, lambda f: scenes.orbit_camera(cam, f, 60), p, 31, args.relmse)
     cb = None
     if not args.no_cpu_baseline and world == 1:
         cb = cpu_baseline(desc, cam, args.workload, os.cpu_count() or 1, 3, warm=1, scale=args.cpu_scale)
@@ -345,6 +352,8 @@ def run_crisb(args):
             "roofline": roofline, "traversal": traversal, "phases_ms": phases, "pass_ms": pass_ms,
             "cpu_baseline": cb, "clocks": clk,
             "gpu_launches": launches_per_frame * args.steps, "image_mean": img_mean}
+    if qual is not None:
+        line["quality"] = qual
     print(json.dumps(line), flush=True)
 
 
@@ -356,6 +365,8 @@ def main():
     ap.add_argument("--impl", default="crisb", choices=["crisb", "reference"])
     ap.add_argument("--workload", default="large", choices=["large", "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--relmse", type=int, default=0, metavar="SPP",
+                    help="also score orbit frame 30 by relMSE against a SPP-sample FP64 path-traced reference")
     ap.add_argument("--no-graph", action="store_true", help="launch kernels directly instead of one CUDA graph per frame")
     ap.add_argument("--cpu-scale", type=int, default=2)
     ap.add_argument("--res", default=None, help="WxH override of the workload resolution (profiling runs)")
