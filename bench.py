@@ -74,7 +74,7 @@ def config_for(name: str, W: int, H: int, n_tris: int, p, ppp: int, world: int, 
     """The `config` object of both arms' JSON lines."""
     return {"workload": f"{name}: {W}x{H} conditional ReSTIR PT, {n_tris} triangles, k={p.gather_m - 1}, "
                         f"{p.suffix_spatial_rounds}x{p.suffix_spatial_count} spatial, max depth {p.max_path_len}, "
-                        f"FP32 storage",
+                        f"{'FP16' if p.storage == 1 else 'FP32'} storage",
             "paths_per_pixel": ppp, "l2": "working set (reservoirs, BVH) larger than L2",
             "parallelism": f"view-sharded replicas x{world}", "frame_as_cuda_graph": graph}
 
@@ -84,13 +84,16 @@ def config_for(name: str, W: int, H: int, n_tris: int, p, ppp: int, world: int, 
 # streaming over records and shift results).  Every record a kernel touches
 # is counted once per kernel (a neighbour's reservoir is another pixel's own
 # record), at nominal occupancy: all k / spatial neighbours present.
-# FP32 records: prefix reservoir 144 B, canonical prefix 128 B, suffix
-# reservoir / canonical suffix 112 B, G-buffer RNG 8 B, shift result 16 B.
-def resample_bytes(k: int, spatial_count: int, spatial_rounds: int, copy_prefix_back: bool) -> dict:
-    prefix_combine = 144 + 128 + 144 + 8 + 8 + 4 + 2 * 16 + 144 + (144 if copy_prefix_back else 0)
-    temporal_combine = 112 + 112 + 8 + 8 + 4 + 2 * 16 + 112
+# Records: prefix reservoir 144 B (FP32) / 80 B (FP16 storage), canonical
+# prefix 128 B, suffix reservoir 112 B / 64 B, canonical suffix 112 B,
+# G-buffer RNG 8 B, shift result 16 B.
+def resample_bytes(k: int, spatial_count: int, spatial_rounds: int, copy_prefix_back: bool,
+                   fp16: bool = False) -> dict:
+    pr, sr = (80, 64) if fp16 else (144, 112)
+    prefix_combine = pr + 128 + pr + 8 + 8 + 4 + 2 * 16 + pr + (pr if copy_prefix_back else 0)
+    temporal_combine = sr + 112 + 8 + 8 + 4 + 2 * 16 + sr
     spatial_select = 3 * 4 + 8 + 8 + 4 * spatial_count + 8
-    spatial_combine = 112 + 8 + 8 + 8 + 4 * spatial_count + 2 * 16 * spatial_count + 112
+    spatial_combine = sr + 8 + 8 + 8 + 4 * spatial_count + 2 * 16 * spatial_count + sr
     gather_combine = 12 + 12 + 32 + 8 * k + 20 + 2 * 16 * k + 12
     return {"prefix_combine": prefix_combine, "temporal_combine": temporal_combine,
             "spatial_select": spatial_rounds * spatial_select, "spatial_combine": spatial_rounds * spatial_combine,
@@ -230,6 +233,7 @@ def run_crisb(args):
         W, H = (int(v) for v in args.res.lower().split("x"))
     sc = Scene(desc)
     p = params_for(args.workload, sc.scene_size)
+    p.storage = _abi.STORAGE_FP16 if args.storage == "fp16" else _abi.STORAGE_FP32
     r = Renderer(W, H, sc, p)
     r.set_graph(not args.no_graph)
     stream = torch.cuda.Stream()
@@ -305,11 +309,12 @@ def run_crisb(args):
 
     # ---- roofline of the resampling kernels; traversal in rays/s -----------------
     peak, peak_kind = measured_peaks()
-    rb = resample_bytes(p.gather_m - 1, p.suffix_spatial_count, p.suffix_spatial_rounds, bool(p.suffix_enable_spatial))
+    rb = resample_bytes(p.gather_m - 1, p.suffix_spatial_count, p.suffix_spatial_rounds, bool(p.suffix_enable_spatial),
+                        p.storage == _abi.STORAGE_FP16)
     res_bytes = sum(rb.values()) * W * H
     achieved = res_bytes / (passes["resample_ms"] / 1000.0) / 1e9
     traffic = None
-    if "resampling" in PROFILED_TRAFFIC:
+    if "resampling" in PROFILED_TRAFFIC and p.storage != _abi.STORAGE_FP16:
         tb, tpx = PROFILED_TRAFFIC["resampling"]
         traffic = tb * (W * H) / tpx
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -367,6 +372,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--relmse", type=int, default=0, metavar="SPP",
                     help="also score orbit frame 30 by relMSE against a SPP-sample FP64 path-traced reference")
+    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"],
+                    help="reservoir storage between passes and frames (fp16: packed binary16 / octahedral records)")
     ap.add_argument("--no-graph", action="store_true", help="launch kernels directly instead of one CUDA graph per frame")
     ap.add_argument("--cpu-scale", type=int, default=2)
     ap.add_argument("--res", default=None, help="WxH override of the workload resolution (profiling runs)")

@@ -218,7 +218,7 @@ class Renderer:
     def debug_read(self, buffer_id: int) -> np.ndarray:
         size = ctypes.c_size_t()
         check(load().crisb_debug_size(self.handle, buffer_id, ctypes.byref(size)))
-        dt = _abi.BUFFER_DTYPES[buffer_id]
+        dt = _abi.buffer_dtype(buffer_id, self.params.storage)
         out = np.zeros(size.value // dt.itemsize, dtype=dt)
         check(load().crisb_debug_read(self.handle, buffer_id, out.ctypes.data_as(ctypes.c_void_p), size.value))
         return out

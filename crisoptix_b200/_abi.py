@@ -110,6 +110,16 @@ SUFFIX_DTYPE = np.dtype([("rng", "<u8"), ("recon", HIT_DTYPE), ("last_prefix", H
                          ("f", "<f4", 3), ("post_recon_f", "<f4", 3), ("p", "<f4"), ("recon_out_dir", "<f4", 3),
                          ("pad", "<u4")])
 SUFFIX_RES_DTYPE = np.dtype([("sample", SUFFIX_DTYPE), ("w_sum", "<f4"), ("confidence", "<f4")])
+# FP16 reservoir storage (crisb_*_res16_rec)
+HIT16_DTYPE = np.dtype([("prim", "<u4"), ("bary", "<u2", 2), ("in_dir_oct", "<u4")])
+PREFIX_RES16_DTYPE = np.dtype([("rng", "<u8"), ("flags", "<u4"), ("p", "<f4"), ("path_len", "<f4"),
+                               ("primary", HIT16_DTYPE), ("recon", HIT16_DTYPE), ("last", HIT16_DTYPE),
+                               ("f", "<u2", 3), ("post_recon_f", "<u2", 3), ("recon_out_dir_oct", "<u4"),
+                               ("w_sum", "<f4"), ("confidence", "<f4")])
+SUFFIX_RES16_DTYPE = np.dtype([("rng", "<u8"), ("flags", "<u4"), ("p", "<f4"), ("recon", HIT16_DTYPE),
+                               ("last_prefix", HIT16_DTYPE), ("f", "<u2", 3), ("post_recon_f", "<u2", 3),
+                               ("recon_out_dir_oct", "<u4"), ("w_sum", "<f4"), ("confidence", "<f4")])
+OCT_ZERO = 0x80008000
 GBUFFER_DTYPE = np.dtype([("rng", "<u8"), ("prev_xy", "<u4"), ("flags", "<u4")])
 NEIGHBOR_DTYPE = np.dtype([("pixel", "<u4"), ("dist", "<f4")])
 TRACE_HIT_DTYPE = np.dtype([("prim", "<u4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")])
@@ -126,9 +136,21 @@ BUFFER_DTYPES = {
     BUF_NEIGHBOR_COUNT: np.dtype("<u4"),
 }
 
+
+def buffer_dtype(buffer_id: int, storage: int = STORAGE_FP32) -> np.dtype:
+    """Element type of a debug buffer; reservoirs follow the storage layout."""
+    if storage == STORAGE_FP16:
+        if buffer_id in (BUF_PREFIX_RES_FRONT, BUF_PREFIX_RES_BACK):
+            return PREFIX_RES16_DTYPE
+        if buffer_id in (BUF_SUFFIX_RES_FRONT, BUF_SUFFIX_RES_BACK):
+            return SUFFIX_RES16_DTYPE
+    return BUFFER_DTYPES[buffer_id]
+
+
 # sizeof order of crisb_abi_sizes
 ABI_STRUCTS = [Material, Mesh, Instance, Emitter, SceneDesc, Camera, CameraData, Params, HIT_DTYPE, PREFIX_DTYPE,
-               PREFIX_RES_DTYPE, SUFFIX_DTYPE, SUFFIX_RES_DTYPE, GBUFFER_DTYPE, NEIGHBOR_DTYPE, TraceHit, Stats]
+               PREFIX_RES_DTYPE, SUFFIX_DTYPE, SUFFIX_RES_DTYPE, GBUFFER_DTYPE, NEIGHBOR_DTYPE, TraceHit, Stats,
+               HIT16_DTYPE, PREFIX_RES16_DTYPE, SUFFIX_RES16_DTYPE]
 
 
 def abi_size(t) -> int:

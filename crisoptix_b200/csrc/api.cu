@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "passes.cuh"
+#include "records.cuh"
 
 namespace crisb {
 namespace {
@@ -140,22 +141,23 @@ __global__ void k_trace_rays(SceneView s, const float* rays, crisb_trace_hit* hi
 }
 
 // default (never written) records: every hit invalid, everything else zero
-__global__ void k_init_records(crisb_prefix_res_rec* pres0, crisb_prefix_res_rec* pres1, crisb_prefix_rec* cpre,
-                               crisb_suffix_res_rec* sres0, crisb_suffix_res_rec* sres1, crisb_suffix_res_rec* csuf,
-                               crisb_gbuffer_rec* gbuf, uint32_t P) {
+__global__ void k_init_records(PresBuf pres0, PresBuf pres1, crisb_prefix_rec* cpre, SresBuf sres0, SresBuf sres1,
+                               crisb_suffix_res_rec* csuf, crisb_gbuffer_rec* gbuf, uint32_t P) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
     crisb_prefix_res_rec pr;
     memset(&pr, 0, sizeof(pr));
     pr.sample.primary.prim = pr.sample.recon.prim = pr.sample.last.prim = CRISB_INVALID_PRIM;
-    pres0[i] = pr;
-    pres1[i] = pr;
+    const Res<Prefix> rp{ld_prefix(pr.sample), 0.0f, 0.0f};
+    st_pres(pres0, i, rp);
+    st_pres(pres1, i, rp);
     cpre[i] = pr.sample;
     crisb_suffix_res_rec sr;
     memset(&sr, 0, sizeof(sr));
     sr.sample.recon.prim = sr.sample.last_prefix.prim = CRISB_INVALID_PRIM;
-    sres0[i] = sr;
-    sres1[i] = sr;
+    const Res<Suffix> rs{ld_suffix(sr.sample), 0.0f, 0.0f};
+    st_sres(sres0, i, rs);
+    st_sres(sres1, i, rs);
     csuf[i] = sr;
     crisb_gbuffer_rec g;
     memset(&g, 0, sizeof(g));
@@ -411,7 +413,7 @@ void validate_params(const crisb_params& p) {
     require(p.gather_n >= 1, "params: gather_n must be >= 1");
     require(p.gather_m >= 1 && p.gather_m <= CRISB_MAX_GATHER_M, "params: gather_m must be in [1, 32]");
     require(p.window_radius >= 0 && p.window_radius < 32768, "params: window_radius");
-    require(p.storage == CRISB_STORAGE_FP32, "params: only FP32 storage is available in this build");
+    require(p.storage == CRISB_STORAGE_FP32 || p.storage == CRISB_STORAGE_FP16, "params: unknown storage");
     require(p.nee_prob >= 0.0f && p.nee_prob <= 1.0f, "params: nee_prob must be in [0, 1]");
 }
 
@@ -425,9 +427,10 @@ struct crisb_renderer {
     uint32_t random = 0;
     int front = 0, back = 0;
     int scur = 0;
-    DevBuf<crisb_prefix_res_rec> pres[2];
+    // reservoirs as raw 16-byte words in the layout of params.storage
+    DevBuf<uint4> pres[2];
     DevBuf<crisb_prefix_rec> canon_prefix;
-    DevBuf<crisb_suffix_res_rec> sres[2];
+    DevBuf<uint4> sres[2];
     DevBuf<crisb_suffix_res_rec> canon_suffix;
     DevBuf<crisb_gbuffer_rec> gbuf;
     DevBuf<crisb_neighbor_rec> neighbors;
@@ -466,15 +469,22 @@ struct crisb_renderer {
     } ktimer;
 
     uint32_t K() const { return static_cast<uint32_t>(params.gather_m - 1); }
+    size_t pres_bytes() const {
+        return params.storage == CRISB_STORAGE_FP16 ? sizeof(crisb_prefix_res16_rec) : sizeof(crisb_prefix_res_rec);
+    }
+    size_t sres_bytes() const {
+        return params.storage == CRISB_STORAGE_FP16 ? sizeof(crisb_suffix_res16_rec) : sizeof(crisb_suffix_res_rec);
+    }
     uint32_t P() const { return width * height; }
 
     Bufs bufs() const {
         Bufs b;
-        b.pres[0] = pres[0].p;
-        b.pres[1] = pres[1].p;
+        const uint32_t f16 = params.storage == CRISB_STORAGE_FP16 ? 1u : 0u;
+        b.pres[0] = PresBuf{pres[0].p, f16};
+        b.pres[1] = PresBuf{pres[1].p, f16};
         b.canon_prefix = canon_prefix.p;
-        b.sres_cur = sres[scur].p;
-        b.sres_next = sres[scur ^ 1].p;
+        b.sres_cur = SresBuf{sres[scur].p, f16};
+        b.sres_next = SresBuf{sres[scur ^ 1].p, f16};
         b.canon_suffix = canon_suffix.p;
         b.gbuf = gbuf.p;
         b.neighbors = neighbors.p;
@@ -546,8 +556,8 @@ struct crisb_renderer {
         check(cudaMemset(job_qcount.p, 0, job_qcount.bytes()), "memset");
         allocate_jobs();
         for (int i = 0; i < 2; ++i) {
-            pres[i].alloc(p);
-            sres[i].alloc(p);
+            pres[i].alloc(static_cast<size_t>(p) * (pres_bytes() / 16));
+            sres[i].alloc(static_cast<size_t>(p) * (sres_bytes() / 16));
         }
         canon_prefix.alloc(p);
         canon_suffix.alloc(p);
@@ -562,8 +572,9 @@ struct crisb_renderer {
         check(cudaMemset(err.p, 0, sizeof(int)), "memset");
         check(cudaMemset(neighbors.p, 0, neighbors.bytes()), "memset");
         check(cudaMemset(neigh_count.p, 0, neigh_count.bytes()), "memset");
-        k_init_records<<<(p + kPassBlock - 1) / kPassBlock, kPassBlock>>>(pres[0].p, pres[1].p, canon_prefix.p,
-                                                                         sres[0].p, sres[1].p, canon_suffix.p,
+        const Bufs b0 = bufs();
+        k_init_records<<<(p + kPassBlock - 1) / kPassBlock, kPassBlock>>>(b0.pres[0], b0.pres[1], canon_prefix.p,
+                                                                         b0.sres_cur, b0.sres_next, canon_suffix.p,
                                                                          gbuf.p, p);
         check(cudaGetLastError(), "init records");
         size_t need = 0;
@@ -847,6 +858,7 @@ int crisb_renderer_set_params(crisb_renderer* r, const crisb_params* params) {
     return guarded([&] {
         require(r && params, "null argument");
         validate_params(*params);
+        require(params->storage == r->params.storage, "params: storage is fixed when the renderer is created");
         const bool realloc_neighbors = params->gather_m != r->params.gather_m;
         const bool realloc_jobs = crisb_renderer::slots_for(*params) != r->slots;
         r->params = *params;
@@ -975,10 +987,10 @@ int crisb_debug_size(const crisb_renderer* r, int id, size_t* out) {
         const size_t P = r->P();
         switch (id) {
             case CRISB_BUF_PREFIX_RES_FRONT:
-            case CRISB_BUF_PREFIX_RES_BACK: *out = P * sizeof(crisb_prefix_res_rec); break;
+            case CRISB_BUF_PREFIX_RES_BACK: *out = P * r->pres_bytes(); break;
             case CRISB_BUF_CANON_PREFIX: *out = P * sizeof(crisb_prefix_rec); break;
             case CRISB_BUF_SUFFIX_RES_FRONT:
-            case CRISB_BUF_SUFFIX_RES_BACK: *out = P * sizeof(crisb_suffix_res_rec); break;
+            case CRISB_BUF_SUFFIX_RES_BACK: *out = P * r->sres_bytes(); break;
             case CRISB_BUF_CANON_SUFFIX: *out = P * sizeof(crisb_suffix_rec); break;
             case CRISB_BUF_GBUFFER: *out = P * sizeof(crisb_gbuffer_rec); break;
             case CRISB_BUF_NEIGHBORS: *out = P * r->K() * sizeof(crisb_neighbor_rec); break;
@@ -1039,7 +1051,7 @@ int crisb_abi_sizes(uint32_t* out, uint32_t n) {
         sizeof(crisb_scene_desc),  sizeof(crisb_camera),       sizeof(crisb_camera_data),  sizeof(crisb_params),
         sizeof(crisb_hit_rec),     sizeof(crisb_prefix_rec),   sizeof(crisb_prefix_res_rec), sizeof(crisb_suffix_rec),
         sizeof(crisb_suffix_res_rec), sizeof(crisb_gbuffer_rec), sizeof(crisb_neighbor_rec), sizeof(crisb_trace_hit),
-        sizeof(crisb_stats)};
+        sizeof(crisb_stats), sizeof(crisb_hit16_rec), sizeof(crisb_prefix_res16_rec), sizeof(crisb_suffix_res16_rec)};
     const uint32_t count = sizeof(sizes) / sizeof(sizes[0]);
     if (!out) return static_cast<int>(count);
     for (uint32_t i = 0; i < n && i < count; ++i) out[i] = sizes[i];

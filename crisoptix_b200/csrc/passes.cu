@@ -38,7 +38,7 @@ __global__ void __launch_bounds__(kPassBlock)
             if (!(nx[n] < fp.width && ny[n] < fp.height)) continue;
             const uint32_t ni = ny[n] * fp.width + nx[n];
             if (!(b.gbuf[ni].flags & 1u)) continue;
-            const uint32_t nflags = b.pres[fp.back][ni].sample.flags;
+            const uint32_t nflags = pres_flags(b.pres[fp.back], ni);
             const bool skip_nee = fp.p.renderer_type == CRISB_RENDERER_CONDITIONAL_RESTIR && fl_nee(nflags);
             if (!fl_valid(nflags) || skip_nee) continue;
             ++nvalid;
@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(kPassBlock)
 __global__ void k_prefix_copy(FrameParams fp, Bufs b) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pixel_count(fp)) return;
-    b.pres[fp.back][i] = b.pres[fp.front][i];
+    copy_pres(b.pres[fp.back], b.pres[fp.front], i);
 }
 
 __global__ void k_bounds_init(unsigned int* ob, uint32_t* n) {
@@ -95,12 +95,12 @@ __global__ void k_store_entries(FrameParams fp, Bufs b, const SceneView s, unsig
     float4 e = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
     bool valid = false;
     if (i < P) {
-        const crisb_prefix_rec& pr = b.pres[fp.front][i].sample;
-        const uint32_t sflags = b.sres_cur[i].sample.flags;
-        const Isect last = unpack(s, ld_hit(pr.last));
-        if (fl_valid(pr.flags) && fl_valid(sflags) && last.valid) {
+        const uint32_t pflags = pres_flags(b.pres[fp.front], i);
+        const uint32_t sflags = sres_flags(b.sres_cur, i);
+        const Isect last = unpack(s, pres_last(b.pres[fp.front], i));
+        if (fl_valid(pflags) && fl_valid(sflags) && last.valid) {
             float radius = fp.p.gather_radius;
-            if (fp.p.gather_radius_type == CRISB_RADIUS_PATH_LENGTH) radius *= pr.path_len / 4.5f;
+            if (fp.p.gather_radius_type == CRISB_RADIUS_PATH_LENGTH) radius *= pres_path_len(b.pres[fp.front], i) / 4.5f;
             const float minx = last.pos.x - radius, maxx = last.pos.x + radius;
             e = make_float4(last.pos.x, last.pos.y, last.pos.z, (maxx - minx) / 2.0f);
             valid = true;
@@ -203,7 +203,7 @@ RT_D V3 final_gather_canon(const SceneView& s, const FrameParams& fp, const Bufs
     queried = true;
     uint32_t nvalid = 0, vflags = 0;
     for (uint32_t n = 0; n < nl.count; ++n) {
-        if (!fl_valid(b.sres_cur[nl.pix[n]].sample.flags)) continue;
+        if (!fl_valid(sres_flags(b.sres_cur, nl.pix[n]))) continue;
         ++nvalid;
         vflags |= 1u << n;
     }
@@ -245,7 +245,7 @@ RT_D V3 final_gather_not_canon(const SceneView& s, const FrameParams& fp, const 
     queried = true;
     uint32_t nvalid = 0, vflags = 0;
     for (uint32_t n = 0; n < nl.count; ++n) {
-        if (!fl_valid(b.sres_cur[nl.pix[n]].sample.flags)) continue;
+        if (!fl_valid(sres_flags(b.sres_cur, nl.pix[n]))) continue;
         ++nvalid;
         vflags |= 1u << n;
     }

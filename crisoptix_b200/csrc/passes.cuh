@@ -23,15 +23,26 @@ struct ShiftJob {
     uint32_t ctr;  // replays left after the ray in flight
 };
 
+// A reservoir buffer in one of the two storage layouts: crisb_*_res_rec
+// (FP32) or crisb_*_res16_rec (FP16, f16 != 0).
+struct PresBuf {
+    void* p;
+    uint32_t f16;
+};
+struct SresBuf {
+    void* p;
+    uint32_t f16;
+};
+
 // Device buffers of one renderer.  Prefix reservoirs keep the reference's
 // front/back pair; suffix reservoirs live in two physical buffers where
 // `sres_cur` holds the state every logical copy front -> back has made equal
 // and spatial rounds write `sres_next` (then the roles swap).
 struct Bufs {
-    crisb_prefix_res_rec* pres[2];
+    PresBuf pres[2];
     crisb_prefix_rec* canon_prefix;
-    crisb_suffix_res_rec* sres_cur;
-    crisb_suffix_res_rec* sres_next;
+    SresBuf sres_cur;
+    SresBuf sres_next;
     crisb_suffix_res_rec* canon_suffix;  // 112-byte slots, w_sum/confidence unused
     crisb_gbuffer_rec* gbuf;
     crisb_neighbor_rec* neighbors;  // P * k

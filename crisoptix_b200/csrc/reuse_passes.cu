@@ -99,29 +99,28 @@ RT_D ShiftSrc shift_src(const Prefix& P) { return ShiftSrc{P.rng, P.flags, P.pri
 RT_D ShiftSrc resolve_job(const FrameParams& fp, const Bufs& b, int mode, uint32_t code, Hit* dst) {
     const uint32_t i = code >> kSlotBits, slot = code & ((1u << kSlotBits) - 1), n = slot >> 1;
     if (mode == kModePrefix) {
-        const crisb_prefix_rec& canon = b.canon_prefix[i];
-        const crisb_prefix_rec& prev = b.pres[fp.back][i].sample;
-        const crisb_prefix_rec& src = slot == 0 ? prev : canon;
-        const crisb_prefix_rec& dr = slot == 0 ? canon : prev;
-        if (dst) *dst = ld_hit(dr.primary);
-        return shift_src(ld_prefix(src));
+        // slot 0: the previous prefix onto the canonical one; slot 1: back
+        if (slot == 0) {
+            if (dst) *dst = ld_hit(b.canon_prefix[i].primary);
+            return shift_src(ld_pres(b.pres[fp.back], i).s);
+        }
+        if (dst) *dst = pres_primary(b.pres[fp.back], i);
+        return shift_src(ld_prefix(b.canon_prefix[i]));
     }
     const bool onto_own = (slot & 1u) == 0;
-    const crisb_suffix_rec* own;
-    const crisb_suffix_rec* other;
+    SufRef own, other;
     if (mode == kModeTemporal) {
-        own = &b.canon_suffix[i].sample;  // canonical; "other" is the previous sample
-        other = &b.sres_cur[i].sample;
+        own = SufRef{b.canon_suffix, b.sres_cur, i};  // canonical; "other" is the previous sample
+        other = SufRef{nullptr, b.sres_cur, i};
     } else if (mode == kModeSpatial) {
-        own = &b.sres_cur[i].sample;
-        other = &b.sres_cur[b.spatial_nbr[static_cast<size_t>(i) * (b.slots >> 1) + n]].sample;
+        own = SufRef{nullptr, b.sres_cur, i};
+        other = SufRef{nullptr, b.sres_cur, b.spatial_nbr[static_cast<size_t>(i) * (b.slots >> 1) + n]};
     } else {
-        own = &b.gather_cs[i].sample;
-        other = &b.sres_cur[b.neighbors[static_cast<size_t>(i) * fp.k + n].pixel].sample;
+        own = SufRef{b.gather_cs, b.sres_cur, i};
+        other = SufRef{nullptr, b.sres_cur, b.neighbors[static_cast<size_t>(i) * fp.k + n].pixel};
     }
-    const crisb_suffix_rec* src = onto_own ? other : own;
-    if (dst) *dst = ld_hit(onto_own ? own->last_prefix : other->last_prefix);
-    return shift_src(ld_suffix(*src));
+    if (dst) *dst = ld_suf_last(onto_own ? own : other);
+    return shift_src(ld_suf(onto_own ? other : own));
 }
 
 RT_D void job_out(const Bufs& b, uint32_t code, float4 v) {
@@ -358,8 +357,8 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_select(FrameParam
     uint64_t mask = 0;
     if (i < pixel_count(fp)) {
         const uint32_t x = i % fp.width, y = i / fp.width;
-        const uint32_t cur_flags = b.sres_cur[i].sample.flags;
-        const uint32_t prefix_flags = b.pres[fp.front][i].sample.flags;
+        const uint32_t cur_flags = sres_flags(b.sres_cur, i);
+        const uint32_t prefix_flags = pres_flags(b.pres[fp.front], i);
         const uint32_t canon_flags = b.canon_suffix[i].sample.flags;
         uint32_t st = kStFinal;
         if (fl_valid(prefix_flags) && !fl_nee(prefix_flags) && fl_valid(cur_flags) && fl_valid(canon_flags)) {
@@ -373,7 +372,7 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_select(FrameParam
                 if (!(nx < fp.width && ny < fp.height)) continue;
                 const uint32_t ni = ny * fp.width + nx;
                 if (!(b.gbuf[ni].flags & 1u)) continue;
-                if (!fl_valid(b.sres_cur[ni].sample.flags)) continue;
+                if (!fl_valid(sres_flags(b.sres_cur, ni))) continue;
                 nbr[n] = ni;
                 vflags |= 1u << n;
                 mask |= 3ull << (2 * n);
@@ -484,7 +483,7 @@ __global__ void __launch_bounds__(kPassBlock) k_gather_query(SceneView s, FrameP
             knn_query(b.knn(), s.err, last.pos, k, nl);
             uint32_t vflags = 0;
             for (uint32_t n = 0; n < nl.count; ++n) {
-                if (!fl_valid(b.sres_cur[nl.pix[n]].sample.flags)) continue;
+                if (!fl_valid(sres_flags(b.sres_cur, nl.pix[n]))) continue;
                 vflags |= 1u << n;
                 mask |= 3ull << (2 * n);
             }
@@ -521,9 +520,9 @@ __global__ void __launch_bounds__(kPassBlock) k_gather_combine(FrameParams fp, B
     float canon_mis = 1.0f;
     for (uint32_t n = 0; n < count; ++n) {
         if (!(vflags & (1u << n))) continue;
-        const crisb_suffix_res_rec& nrec = b.sres_cur[b.neighbors[static_cast<size_t>(i) * k + n].pixel];
-        const V3 nf = ld3(nrec.sample.f);
-        const float nconf = nrec.confidence, nwsum = nrec.w_sum;
+        const uint32_t np_ = b.neighbors[static_cast<size_t>(i) * k + n].pixel;
+        const V3 nf = sres_f(b.sres_cur, np_);
+        const float nconf = sres_conf(b.sres_cur, np_), nwsum = sres_wsum(b.sres_cur, np_);
         const float4 o0 = sh[2 * n], o1 = sh[2 * n + 1];
         const V3 f_c_of_n = xyz(o0), f_n_of_c = xyz(o1);
         const float jac_n2c = o0.w, jac_c2n = o1.w;
@@ -580,10 +579,9 @@ __global__ void __launch_bounds__(kPassBlock) k_prefix_finish(FrameParams fp, Bu
         } else if (!fp.p.prefix_enable_temporal) {
             st = kStCanonOnly;
         } else {
-            const crisb_prefix_res_rec& prev = b.pres[fp.back][i];
-            const uint32_t pf = prev.sample.flags;
+            const uint32_t pf = pres_flags(b.pres[fp.back], i);
             const bool skip_nee = fp.p.renderer_type == CRISB_RENDERER_CONDITIONAL_RESTIR && fl_nee(pf);
-            if (prev.w_sum <= 0.0f || !fl_valid(pf) || skip_nee) {
+            if (pres_wsum(b.pres[fp.back], i) <= 0.0f || !fl_valid(pf) || skip_nee) {
                 st = kStCanonOnly;
             } else {
                 st = kStReuse;

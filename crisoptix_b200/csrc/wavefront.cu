@@ -88,8 +88,7 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_suffix(SceneView s, Fram
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     int req = kReqDone;
     if (i < pixel_count(fp)) {
-        const crisb_prefix_rec& pr = b.pres[fp.front][i].sample;
-        const uint32_t pflags = pr.flags;
+        const uint32_t pflags = pres_flags(b.pres[fp.front], i);
         if (!fl_valid(pflags) || fl_nee(pflags)) {
             Res<Suffix> cur = ld_sres(b.sres_cur, i);
             invalidate(cur);
@@ -99,7 +98,7 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_suffix(SceneView s, Fram
             Rng rng{b.gbuf[i].rng};
             Suffix suf = ld_suffix(b.canon_suffix[i].sample);
             WfPath w = wf_blank();
-            req = suf_begin(s, fp, suf, w, pflags, ld_hit(pr.last), rng);
+            req = suf_begin(s, fp, suf, w, pflags, pres_last(b.pres[fp.front], i), rng);
             st_suffix_slot(b.canon_suffix[i], suf);
             w.rng = rng.state;
             b.wf[i] = w;

@@ -216,6 +216,51 @@ typedef struct crisb_suffix_res_rec {
     float confidence;
 } crisb_suffix_res_rec;
 
+/* ---- FP16 reservoir storage (crisb_params.storage == CRISB_STORAGE_FP16) --
+ * Reservoirs between passes and frames are packed: colours (f, post-recon f)
+ * as IEEE binary16 RGB (round to nearest even; NaN stored as 0, magnitudes
+ * saturate at 65504), barycentrics as binary16 (the reference's own F16
+ * switch, include/config.h + include/util/f16.h, stores them so), directions
+ * (incoming ray direction, reconOutDir) as 16+16-bit octahedral codes with
+ * CRISB_OCT_ZERO for the zero vector; random states, flags, pdfs, path length,
+ * weights and confidences stay 32-bit.  Canonical (per-frame working)
+ * records keep the FP32 layouts above. */
+typedef struct crisb_hit16_rec {
+    uint32_t prim;
+    uint16_t bary[2];
+    uint32_t in_dir_oct;
+} crisb_hit16_rec;
+
+typedef struct crisb_prefix_res16_rec { /* 80 bytes */
+    uint64_t rng;
+    uint32_t flags;
+    float p;
+    float path_len;
+    crisb_hit16_rec primary;
+    crisb_hit16_rec recon;
+    crisb_hit16_rec last;
+    uint16_t f[3];
+    uint16_t post_recon_f[3];
+    uint32_t recon_out_dir_oct;
+    float w_sum;
+    float confidence;
+} crisb_prefix_res16_rec;
+
+typedef struct crisb_suffix_res16_rec { /* 64 bytes */
+    uint64_t rng;
+    uint32_t flags;
+    float p;
+    crisb_hit16_rec recon;
+    crisb_hit16_rec last_prefix;
+    uint16_t f[3];
+    uint16_t post_recon_f[3];
+    uint32_t recon_out_dir_oct;
+    float w_sum;
+    float confidence;
+} crisb_suffix_res16_rec;
+
+#define CRISB_OCT_ZERO 0x80008000u
+
 /* RestirGBuffer (include/graph/restir/RestirGBuffer.h:5-28) */
 typedef struct crisb_gbuffer_rec {
     uint64_t rng;

@@ -59,6 +59,10 @@ int oracle_pt_accumulate(oracle_ctx* ctx, const crisb_camera* cam, uint32_t spp,
 /* unit-level helpers for known-answer tests */
 void oracle_pcg32(uint64_t initstate, uint64_t initseq, uint32_t n, uint32_t* out);
 uint64_t oracle_tea64(uint32_t v0, uint32_t v1);
+/* FP16 storage codecs (test hooks): binary16 bits and their value; octahedral
+ * codes and their decoded unit vectors (dirs: n x 3 floats). */
+void oracle_half(const float* in, uint32_t n, uint16_t* bits, float* back);
+void oracle_oct(const float* dirs, uint32_t n, uint32_t* codes, float* decoded);
 void oracle_sincos(const float* phi, uint32_t n, float* s, float* c);
 int oracle_camera_data(const crisb_camera* cam, crisb_camera_data* out);
 uint32_t oracle_frame_random_for(uint64_t seed, uint64_t frame_counter);

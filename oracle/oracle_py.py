@@ -56,6 +56,8 @@ def load():
         "oracle_pcg32": (None, [u64, u64, u32, vp]),
         "oracle_tea64": (u64, [u32, u32]),
         "oracle_sincos": (None, [vp, u32, vp, vp]),
+        "oracle_half": (None, [vp, u32, vp, vp]),
+        "oracle_oct": (None, [vp, u32, vp, vp]),
         "oracle_camera_data": (i32, [ctypes.POINTER(_abi.Camera), ctypes.POINTER(_abi.CameraData)]),
         "oracle_frame_random_for": (u32, [u64, u64]),
     }
@@ -105,6 +107,7 @@ class Oracle:
         if not h:
             raise RuntimeError("oracle_create rejected the scene or parameters")
         self.h = h
+        self.storage = int(params.storage)
 
     @classmethod
     def from_scene(cls, scene_desc, width, height, params, triangles=None):
@@ -122,6 +125,7 @@ class Oracle:
     def set_params(self, params):
         if load().oracle_set_params(self.h, ctypes.byref(params)) != 0:
             raise ValueError("oracle rejected parameters")
+        self.storage = int(params.storage)
 
     @property
     def scene_size(self) -> float:
@@ -146,7 +150,7 @@ class Oracle:
 
     def dump(self, buffer_id: int) -> np.ndarray:
         n = load().oracle_dump_size(self.h, buffer_id)
-        dt = _abi.BUFFER_DTYPES[buffer_id]
+        dt = _abi.buffer_dtype(buffer_id, self.storage)
         out = np.zeros(n // dt.itemsize, dtype=dt)
         if n and load().oracle_dump(self.h, buffer_id, _ptr(out), n) != 0:
             raise RuntimeError("oracle_dump failed")
@@ -181,6 +185,25 @@ def sincos(phi: np.ndarray):
     c = np.zeros_like(phi)
     load().oracle_sincos(_ptr(phi), len(phi), _ptr(s), _ptr(c))
     return s, c
+
+
+def half(x: np.ndarray):
+    """binary16 bits and values of the FP16 storage rule (NaN -> 0, clamp at
+    +-65504, round to nearest even)."""
+    x = np.ascontiguousarray(x, np.float32)
+    bits = np.zeros(x.shape, np.uint16)
+    back = np.zeros_like(x)
+    load().oracle_half(_ptr(x), x.size, _ptr(bits), _ptr(back))
+    return bits, back
+
+
+def oct(dirs: np.ndarray):
+    """Octahedral codes of (n, 3) directions and the decoded unit vectors."""
+    d = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
+    codes = np.zeros(len(d), np.uint32)
+    dec = np.zeros_like(d)
+    load().oracle_oct(_ptr(d), len(d), _ptr(codes), _ptr(dec))
+    return codes, dec
 
 
 def camera_data(cam) -> np.ndarray:

@@ -300,6 +300,115 @@ struct Reservoir {
     }
 };
 
+// ---- FP16 reservoir storage (crisb_params.storage == CRISB_STORAGE_FP16) ----
+// The library stores reservoirs between passes with binary16 colours and
+// barycentrics and octahedral directions (include/crisb.h); the oracle keeps
+// FP32 reservoirs and quantises them at the same points, so that every load
+// sees the value the library loads.  Rules: binary16 = NaN -> 0, clamp to
+// +-65504, round to nearest even (IEEE 754 binary32 -> binary16 conversion);
+// octahedral = zero vector -> a reserved code, else p = n.xy / |n|_1 folded
+// for n.z < 0, clamped to [-1, 1], rounded (nearest even) to int16 units of
+// 1/32767, decoded by the inverse fold and a normalisation.
+uint16_t HalfBits(float f) {
+    if (std::isnan(f)) f = 0.0f;
+    f = std::fmin(std::fmax(f, -65504.0f), 65504.0f);
+    uint32_t x;
+    std::memcpy(&x, &f, 4);
+    const uint32_t sign = (x >> 16) & 0x8000u;
+    const uint32_t ax = x & 0x7fffffffu;
+    if (ax >= 0x38800000u) {  // |f| >= 2^-14: a normal binary16
+        const uint32_t m = ax & 0x7fffffu;
+        uint32_t h = (((ax >> 23) - 112u) << 10) | (m >> 13);
+        const uint32_t rem = m & 0x1fffu;
+        if (rem > 0x1000u || (rem == 0x1000u && (h & 1u))) ++h;
+        return static_cast<uint16_t>(sign | h);
+    }
+    if (ax < 0x33000000u) return static_cast<uint16_t>(sign);  // below 2^-25
+    const uint32_t e = ax >> 23;
+    const uint32_t M = (ax & 0x7fffffu) | 0x800000u;
+    const uint32_t sh = 126u - e;  // 14 .. 24
+    uint32_t m = M >> sh;
+    const uint32_t rem = M & ((1u << sh) - 1u), half = 1u << (sh - 1u);
+    if (rem > half || (rem == half && (m & 1u))) ++m;
+    return static_cast<uint16_t>(sign | m);
+}
+
+float HalfValue(uint16_t h) {
+    const uint32_t sign = static_cast<uint32_t>(h & 0x8000u) << 16;
+    const uint32_t e = (h >> 10) & 0x1fu, m = h & 0x3ffu;
+    uint32_t bits;
+    if (e == 0) {
+        const float v = std::ldexp(static_cast<float>(m), -24);  // exact
+        std::memcpy(&bits, &v, 4);
+    } else if (e == 31) {
+        bits = m ? 0x7fc00000u : 0x7f800000u;
+    } else {
+        bits = ((e + 112u) << 23) | (m << 13);
+    }
+    bits |= sign;
+    float v;
+    std::memcpy(&v, &bits, 4);
+    return v;
+}
+
+float Quant16(float f) { return HalfValue(HalfBits(f)); }
+
+float OctSign(float v) { return v >= 0.0f ? 1.0f : -1.0f; }
+
+uint32_t OctEncode(vec3 n) {
+    if (n.x == 0.0f && n.y == 0.0f && n.z == 0.0f) return CRISB_OCT_ZERO;
+    const float l1 = (std::fabs(n.x) + std::fabs(n.y)) + std::fabs(n.z);
+    float px = n.x / l1, py = n.y / l1;
+    if (n.z < 0.0f) {
+        const float tx = (1.0f - std::fabs(py)) * OctSign(px);
+        const float ty = (1.0f - std::fabs(px)) * OctSign(py);
+        px = tx;
+        py = ty;
+    }
+    px = std::fmin(std::fmax(px, -1.0f), 1.0f);
+    py = std::fmin(std::fmax(py, -1.0f), 1.0f);
+    const int qx = static_cast<int>(std::rint(px * 32767.0f));
+    const int qy = static_cast<int>(std::rint(py * 32767.0f));
+    return (static_cast<uint32_t>(qx) & 0xFFFFu) | ((static_cast<uint32_t>(qy) & 0xFFFFu) << 16);
+}
+
+vec3 OctDecode(uint32_t c) {
+    if (c == CRISB_OCT_ZERO) return vec3(0.0f);
+    float x = static_cast<float>(static_cast<int16_t>(c & 0xFFFFu)) / 32767.0f;
+    float y = static_cast<float>(static_cast<int16_t>(c >> 16)) / 32767.0f;
+    const float z = (1.0f - std::fabs(x)) - std::fabs(y);
+    if (z < 0.0f) {
+        const float tx = (1.0f - std::fabs(y)) * OctSign(x);
+        const float ty = (1.0f - std::fabs(x)) * OctSign(y);
+        x = tx;
+        y = ty;
+    }
+    return normalize(vec3(x, y, z));
+}
+
+vec3 Quant16(vec3 v) { return vec3(Quant16(v.x), Quant16(v.y), Quant16(v.z)); }
+
+void QuantizeHit(PackedInteraction& p) {
+    p.bary.x = Quant16(p.bary.x);
+    p.bary.y = Quant16(p.bary.y);
+    p.inRayDir = OctDecode(OctEncode(p.inRayDir));
+}
+void Quantize(PrefixPath& s) {
+    QuantizeHit(s.primaryInt);
+    QuantizeHit(s.reconInt);
+    QuantizeHit(s.lastInt);
+    s.f = Quant16(s.f);
+    s.postReconF = Quant16(s.postReconF);
+    s.reconOutDir = OctDecode(OctEncode(s.reconOutDir));
+}
+void Quantize(SuffixPath& s) {
+    QuantizeHit(s.reconInt);
+    QuantizeHit(s.lastPrefixInt);
+    s.f = Quant16(s.f);
+    s.postReconF = Quant16(s.postReconF);
+    s.reconOutDir = OctDecode(OctEncode(s.reconOutDir));
+}
+
 // RestirGBuffer, include/graph/restir/RestirGBuffer.h:5-28
 struct GBuffer {
     PCG32 rng;
@@ -1777,6 +1886,20 @@ struct oracle_ctx {
     }
 
     // Renderer::LaunchFrame, src/Renderer.cpp:209-406
+    // the library stores every reservoir it writes at the end of a pass; in
+    // FP16 storage the stored values are the quantised ones
+    void QuantizeReservoirs() {
+        if (params.storage != CRISB_STORAGE_FP16) return;
+        const int64_t P = static_cast<int64_t>(width) * height;
+#pragma omp parallel for schedule(static)
+        for (int64_t pi = 0; pi < P; ++pi) {
+            for (int b = 0; b < 2; ++b) {
+                Quantize(prefixRes[b][pi].sample);
+                Quantize(suffixRes[b][pi].sample);
+            }
+        }
+    }
+
     void RenderFrame(const crisb_camera& c, float* out, double* passMs) {
         using clk = std::chrono::steady_clock;
         auto t0 = clk::now();
@@ -1801,17 +1924,25 @@ struct oracle_ctx {
             back = 1;
         }
         PassPrefixGenTempReuse(out);
+        QuantizeReservoirs();
         lap(0);
         const int type = params.renderer_type;
         if (type == CRISB_RENDERER_CONDITIONAL_RESTIR || type == CRISB_RENDERER_RESTIR_PT) {
             if (params.prefix_enable_spatial)
-                for (int r = 0; r < params.prefix_spatial_rounds; ++r) PassPrefixSpatialReuse(out, r);
+                for (int r = 0; r < params.prefix_spatial_rounds; ++r) {
+                    PassPrefixSpatialReuse(out, r);
+                    QuantizeReservoirs();
+                }
             lap(1);
             if (type == CRISB_RENDERER_CONDITIONAL_RESTIR) {
                 PassSuffixGenTempReuse();
+                QuantizeReservoirs();
                 lap(2);
                 if (params.suffix_enable_spatial && params.suffix_spatial_count > 0)
-                    for (int r = 0; r < params.suffix_spatial_rounds; ++r) PassSuffixSpatialReuse();
+                    for (int r = 0; r < params.suffix_spatial_rounds; ++r) {
+                        PassSuffixSpatialReuse();
+                        QuantizeReservoirs();
+                    }
                 lap(3);
                 PassPrefixStoreEntries();
                 lap(4);
@@ -1849,6 +1980,49 @@ void PackPrefix(const PrefixPath& s, crisb_prefix_rec& r) {
     r.p = s.p;
     r.path_len = s.pathLen;
     Put3(r.recon_out_dir, s.reconOutDir);
+}
+crisb_hit16_rec PackHit16(const PackedInteraction& p) {
+    crisb_hit16_rec h;
+    h.prim = p.valid ? p.prim : CRISB_INVALID_PRIM;
+    h.bary[0] = HalfBits(p.bary.x);
+    h.bary[1] = HalfBits(p.bary.y);
+    h.in_dir_oct = OctEncode(p.inRayDir);
+    return h;
+}
+void Put16(uint16_t* d, vec3 v) {
+    d[0] = HalfBits(v.x);
+    d[1] = HalfBits(v.y);
+    d[2] = HalfBits(v.z);
+}
+void PackPrefixRes16(const Reservoir<PrefixPath>& r, crisb_prefix_res16_rec& o) {
+    std::memset(&o, 0, sizeof(o));
+    const PrefixPath& s = r.sample;
+    o.rng = s.rng.state;
+    o.flags = s.flags;
+    o.p = s.p;
+    o.path_len = s.pathLen;
+    o.primary = PackHit16(s.primaryInt);
+    o.recon = PackHit16(s.reconInt);
+    o.last = PackHit16(s.lastInt);
+    Put16(o.f, s.f);
+    Put16(o.post_recon_f, s.postReconF);
+    o.recon_out_dir_oct = OctEncode(s.reconOutDir);
+    o.w_sum = r.wSum;
+    o.confidence = r.confidence;
+}
+void PackSuffixRes16(const Reservoir<SuffixPath>& r, crisb_suffix_res16_rec& o) {
+    std::memset(&o, 0, sizeof(o));
+    const SuffixPath& s = r.sample;
+    o.rng = s.rng.state;
+    o.flags = s.flags;
+    o.p = s.p;
+    o.recon = PackHit16(s.reconInt);
+    o.last_prefix = PackHit16(s.lastPrefixInt);
+    Put16(o.f, s.f);
+    Put16(o.post_recon_f, s.postReconF);
+    o.recon_out_dir_oct = OctEncode(s.reconOutDir);
+    o.w_sum = r.wSum;
+    o.confidence = r.confidence;
 }
 void PackSuffix(const SuffixPath& s, crisb_suffix_rec& r) {
     std::memset(&r, 0, sizeof(r));
@@ -1964,10 +2138,14 @@ size_t oracle_dump_size(const oracle_ctx* ctx, int id) {
     const size_t P = static_cast<size_t>(ctx->width) * ctx->height;
     switch (id) {
         case CRISB_BUF_PREFIX_RES_FRONT:
-        case CRISB_BUF_PREFIX_RES_BACK: return P * sizeof(crisb_prefix_res_rec);
+        case CRISB_BUF_PREFIX_RES_BACK:
+            return P * (ctx->params.storage == CRISB_STORAGE_FP16 ? sizeof(crisb_prefix_res16_rec)
+                                                                   : sizeof(crisb_prefix_res_rec));
         case CRISB_BUF_CANON_PREFIX: return P * sizeof(crisb_prefix_rec);
         case CRISB_BUF_SUFFIX_RES_FRONT:
-        case CRISB_BUF_SUFFIX_RES_BACK: return P * sizeof(crisb_suffix_res_rec);
+        case CRISB_BUF_SUFFIX_RES_BACK:
+            return P * (ctx->params.storage == CRISB_STORAGE_FP16 ? sizeof(crisb_suffix_res16_rec)
+                                                                   : sizeof(crisb_suffix_res_rec));
         case CRISB_BUF_CANON_SUFFIX: return P * sizeof(crisb_suffix_rec);
         case CRISB_BUF_GBUFFER: return P * sizeof(crisb_gbuffer_rec);
         case CRISB_BUF_NEIGHBORS: return P * ctx->K() * sizeof(crisb_neighbor_rec);
@@ -1983,6 +2161,11 @@ int oracle_dump(const oracle_ctx* ctx, int id, void* dst, size_t bytes) {
         case CRISB_BUF_PREFIX_RES_FRONT:
         case CRISB_BUF_PREFIX_RES_BACK: {
             const auto& v = ctx->prefixRes[id == CRISB_BUF_PREFIX_RES_FRONT ? ctx->front : ctx->back];
+            if (ctx->params.storage == CRISB_STORAGE_FP16) {
+                auto* o16 = static_cast<crisb_prefix_res16_rec*>(dst);
+                for (size_t i = 0; i < P; ++i) PackPrefixRes16(v[i], o16[i]);
+                return CRISB_OK;
+            }
             auto* o = static_cast<crisb_prefix_res_rec*>(dst);
             for (size_t i = 0; i < P; ++i) {
                 std::memset(&o[i], 0, sizeof(o[i]));
@@ -2000,6 +2183,11 @@ int oracle_dump(const oracle_ctx* ctx, int id, void* dst, size_t bytes) {
         case CRISB_BUF_SUFFIX_RES_FRONT:
         case CRISB_BUF_SUFFIX_RES_BACK: {
             const auto& v = ctx->suffixRes[id == CRISB_BUF_SUFFIX_RES_FRONT ? ctx->front : ctx->back];
+            if (ctx->params.storage == CRISB_STORAGE_FP16) {
+                auto* o16 = static_cast<crisb_suffix_res16_rec*>(dst);
+                for (size_t i = 0; i < P; ++i) PackSuffixRes16(v[i], o16[i]);
+                return CRISB_OK;
+            }
             auto* o = static_cast<crisb_suffix_res_rec*>(dst);
             for (size_t i = 0; i < P; ++i) {
                 std::memset(&o[i], 0, sizeof(o[i]));
@@ -2117,6 +2305,23 @@ void oracle_pcg32(uint64_t initstate, uint64_t initseq, uint32_t n, uint32_t* ou
 }
 
 uint64_t oracle_tea64(uint32_t v0, uint32_t v1) { return SampleTEA64(v0, v1); }
+
+void oracle_half(const float* in, uint32_t n, uint16_t* bits, float* back) {
+    for (uint32_t i = 0; i < n; ++i) {
+        bits[i] = HalfBits(in[i]);
+        back[i] = HalfValue(bits[i]);
+    }
+}
+
+void oracle_oct(const float* dirs, uint32_t n, uint32_t* codes, float* decoded) {
+    for (uint32_t i = 0; i < n; ++i) {
+        codes[i] = OctEncode(vec3(dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]));
+        const vec3 d = OctDecode(codes[i]);
+        decoded[3 * i] = d.x;
+        decoded[3 * i + 1] = d.y;
+        decoded[3 * i + 2] = d.z;
+    }
+}
 
 void oracle_sincos(const float* phi, uint32_t n, float* s, float* c) {
     for (uint32_t i = 0; i < n; ++i) SinCos(phi[i], s[i], c[i]);
