@@ -38,6 +38,14 @@ RT_D float pres_wsum(const PresBuf& b, uint32_t i) {
     return b.f16 ? static_cast<const crisb_prefix_res16_rec*>(b.p)[i].w_sum
                  : static_cast<const crisb_prefix_res_rec*>(b.p)[i].w_sum;
 }
+RT_D float pres_conf(const PresBuf& b, uint32_t i) {
+    return b.f16 ? static_cast<const crisb_prefix_res16_rec*>(b.p)[i].confidence
+                 : static_cast<const crisb_prefix_res_rec*>(b.p)[i].confidence;
+}
+RT_D V3 pres_f(const PresBuf& b, uint32_t i) {
+    return b.f16 ? unpack_rgb16(static_cast<const crisb_prefix_res16_rec*>(b.p)[i].f)
+                 : ld3(static_cast<const crisb_prefix_res_rec*>(b.p)[i].sample.f);
+}
 RT_D Hit pres_last(const PresBuf& b, uint32_t i) {
     return b.f16 ? unpack_hit16(static_cast<const crisb_prefix_res16_rec*>(b.p)[i].last)
                  : ld_hit(static_cast<const crisb_prefix_res_rec*>(b.p)[i].sample.last);

@@ -403,24 +403,44 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_combine(FramePara
     const float K = static_cast<float>(__popc(vflags));
     const uint32_t* nbr = b.spatial_nbr + static_cast<size_t>(i) * (b.slots >> 1);
     const float4* sh = b.shift_out + static_cast<size_t>(i) * b.slots;
+    // The reservoir's choices depend on the candidates' weights only, so the
+    // neighbours contribute f, confidence and weight here and the record of
+    // the chosen one is read once at the end (Reservoir::Update's arithmetic,
+    // with the chosen sample tracked by index: -1 is the pixel's own sample,
+    // which the reset reservoir also still holds).
+    int sel = -1;
+    V3 sel_f = cur_suffix.f;
     float canon_mis = 1.0f;
     for (int n = 0; n < fp.p.suffix_spatial_count; ++n) {
         if (!((vflags >> n) & 1u)) continue;
-        const Res<Suffix> nr = ld_sres(b.sres_cur, nbr[n]);
+        const uint32_t ni = nbr[n];
+        const V3 nf = sres_f(b.sres_cur, ni);
+        const float nconf = sres_conf(b.sres_cur, ni), nwsum = sres_wsum(b.sres_cur, ni);
         const float4 o0 = sh[2 * n], o1 = sh[2 * n + 1];
         const V3 f_c_of_n = xyz(o0), f_n_of_c = xyz(o1);
         const float jac_n2c = o0.w, jac_c2n = o1.w;
         const float p_c_of_n = luminance(f_c_of_n) * jac_n2c;
-        float nmis = mis_neighbor(f_c_of_n, nr.s.f, jac_n2c, K, cur_conf, nr.conf);
+        float nmis = mis_neighbor(f_c_of_n, nf, jac_n2c, K, cur_conf, nconf);
         if (nonfinite(nmis)) nmis = 0.0f;
-        Suffix shifted = nr.s;
-        shifted.last_prefix = cur_suffix.last_prefix;
-        shifted.f = f_c_of_n;
-        res_update(cur, shifted, nmis * p_c_of_n * nr.w_sum, rng, nr.conf);
-        canon_mis += mis_canonical(cur_suffix.f, f_n_of_c, jac_c2n, K, cur_conf, nr.conf);
+        if (res_choose(cur.w_sum, cur.conf, nmis * p_c_of_n * nwsum, rng, nconf)) {
+            sel = n;
+            sel_f = f_c_of_n;
+        }
+        canon_mis += mis_canonical(cur_suffix.f, f_n_of_c, jac_c2n, K, cur_conf, nconf);
     }
     if (nonfinite(canon_mis)) canon_mis = 0.0f;
-    res_update(cur, cur_suffix, canon_mis * cur_wsum * luminance(cur_suffix.f), rng, cur_conf);
+    if (res_choose(cur.w_sum, cur.conf, canon_mis * cur_wsum * luminance(cur_suffix.f), rng, cur_conf)) {
+        sel = -1;
+        sel_f = cur_suffix.f;
+    }
+    if (sel >= 0) {
+        // SuffixPath(neighbour, currSuffix.lastPrefixInt, fFromCanonOfNeigh)
+        cur.s = ld_sres(b.sres_cur, nbr[sel]).s;
+        cur.s.last_prefix = cur_suffix.last_prefix;
+        cur.s.f = sel_f;
+    } else {
+        cur.s = cur_suffix;
+    }
     if (cur.w_sum > 0.0f) {
         cur.w_sum /= K + 1.0f;
         res_finalize(cur);
@@ -604,35 +624,49 @@ __global__ void __launch_bounds__(kPassBlock) k_prefix_combine(FrameParams fp, B
     if (i >= pixel_count(fp) || fp.p.renderer_type == CRISB_RENDERER_PATH_TRACER) return;
     const uint32_t st = b.pass_status[i];
     if (st == kStFinal) return;
-    Res<Prefix> cur = ld_pres(b.pres[fp.front], i);
     const Prefix canon = ld_prefix(b.canon_prefix[i]);
     Rng rng{b.gbuf[i].rng};
     const float canon_phat = luminance(canon.f);
+    // Reservoir::Update's arithmetic with the chosen sample tracked by index
+    // (0: the sample the reset front reservoir still holds, 1: canonical,
+    // 2: the shifted previous sample); the chosen record is read at the end.
+    Res<Prefix> cur;
     cur.w_sum = 0.0f;
     cur.conf = 0.0f;
+    int sel = 0;
+    V3 f_canon_of_prev = splat(0.0f);
     if (st == kStCanonOnly) {
-        res_update(cur, canon, canon_phat / canon.p, rng, 1.0f);
-        res_finalize(cur);
+        if (res_choose(cur.w_sum, cur.conf, canon_phat / canon.p, rng, 1.0f)) sel = 1;
     } else {
-        const Res<Prefix> prev = ld_pres(b.pres[fp.back], i);
+        const V3 prev_f = pres_f(b.pres[fp.back], i);
+        const float prev_conf = pres_conf(b.pres[fp.back], i), prev_wsum = pres_wsum(b.pres[fp.back], i);
         const float4 o0 = b.shift_out[static_cast<size_t>(i) * b.slots];
         const float4 o1 = b.shift_out[static_cast<size_t>(i) * b.slots + 1];
-        const V3 f_canon_of_prev = xyz(o0), f_prev_of_canon = xyz(o1);
+        f_canon_of_prev = xyz(o0);
+        const V3 f_prev_of_canon = xyz(o1);
         const float jac_prev_to_canon = o0.w, jac_canon_to_prev = o1.w;
         const float p_canon_of_prev = luminance(f_canon_of_prev) * jac_prev_to_canon;
         const float K = 1.0f;
-        const float prev_mis = mis_neighbor(f_canon_of_prev, prev.s.f, jac_prev_to_canon, K, 1.0f, prev.conf);
+        const float prev_mis = mis_neighbor(f_canon_of_prev, prev_f, jac_prev_to_canon, K, 1.0f, prev_conf);
         const float canon_mis =
-            1.0f + mis_canonical(canon.f, f_prev_of_canon, jac_canon_to_prev, K, 1.0f, prev.conf);
-        res_update(cur, canon, canon_mis * canon_phat / canon.p, rng, 1.0f);
-        Prefix shifted = prev.s;  // PrefixPath(prev, f, canon.primaryInt)
-        shifted.f = f_canon_of_prev;
-        shifted.primary = canon.primary;
-        res_update(cur, shifted, prev_mis * p_canon_of_prev * prev.w_sum, rng, prev.conf);
-        if (cur.w_sum > 0.0f) {
-            cur.w_sum /= K + 1.0f;
-            res_finalize(cur);
-        }
+            1.0f + mis_canonical(canon.f, f_prev_of_canon, jac_canon_to_prev, K, 1.0f, prev_conf);
+        if (res_choose(cur.w_sum, cur.conf, canon_mis * canon_phat / canon.p, rng, 1.0f)) sel = 1;
+        if (res_choose(cur.w_sum, cur.conf, prev_mis * p_canon_of_prev * prev_wsum, rng, prev_conf)) sel = 2;
+    }
+    if (sel == 0) {
+        cur.s = ld_pres(b.pres[fp.front], i).s;
+    } else if (sel == 1) {
+        cur.s = canon;
+    } else {
+        cur.s = ld_pres(b.pres[fp.back], i).s;  // PrefixPath(prev, f, canon.primaryInt)
+        cur.s.f = f_canon_of_prev;
+        cur.s.primary = canon.primary;
+    }
+    if (st == kStCanonOnly) {
+        res_finalize(cur);
+    } else if (cur.w_sum > 0.0f) {
+        cur.w_sum /= 1.0f + 1.0f;
+        res_finalize(cur);
     }
     b.gbuf[i].rng = rng.state;
     st_pres(b.pres[fp.front], i, cur);

@@ -35,6 +35,16 @@ RT_D bool res_update(Res<T>& r, const T& s, float w, Rng& rng, float in_conf) {
     }
     return false;
 }
+// res_update without the sample: the same weight and confidence arithmetic and
+// the same random draw; true when the candidate replaces the current sample
+RT_D bool res_choose(float& w_sum, float& conf, float w, Rng& rng, float in_conf) {
+    if (isnan(w) || isinf(w)) w = 0.0f;
+    w_sum += w;
+    conf += in_conf;
+    conf = gmin(conf, CRISB_CONFIDENCE_MAX);
+    return rng.next_float() < w / w_sum;
+}
+
 template <typename T>
 RT_D void res_finalize(Res<T>& r) {
     const float phat = luminance(r.s.f);
