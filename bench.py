@@ -20,6 +20,7 @@ collective on the data path); the reported time is the max over ranks.
 from __future__ import annotations
 
 import argparse
+import copy
 import json
 import math
 import os
@@ -344,7 +345,13 @@ def run_crisb(args):
         # reference of that frame's camera
         from crisoptix_b200 import quality
 
-        qual = quality.score(sc, W, H, lambda f: scenes.orbit_camera(cam, f, 60), p, 31, args.relmse)
+        cam_of = lambda f: scenes.orbit_camera(cam, f, 60)  # noqa: E731
+        ref = quality.reference_image(sc, W, H, cam_of(30), p, args.relmse)
+        qual = {"reference_spp": args.relmse, "frame": 30}
+        for name, storage in (("fp32", _abi.STORAGE_FP32), ("fp16", _abi.STORAGE_FP16)):
+            q = copy.copy(p)
+            q.storage = storage
+            qual[name] = quality.score(sc, W, H, cam_of, q, 31, args.relmse, ref=ref)
     cb = None
     if not args.no_cpu_baseline and world == 1:
         cb = cpu_baseline(desc, cam, args.workload, os.cpu_count() or 1, 3, warm=1, scale=args.cpu_scale)
@@ -371,7 +378,8 @@ def main():
     ap.add_argument("--workload", default="large", choices=["large", "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--relmse", type=int, default=0, metavar="SPP",
-                    help="also score orbit frame 30 by relMSE against a SPP-sample FP64 path-traced reference")
+                    help="also score orbit frame 30, with FP32 and with FP16 storage, by relMSE against one "
+                         "SPP-sample FP64-accumulated path-traced reference")
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"],
                     help="reservoir storage between passes and frames (fp16: packed binary16 / octahedral records)")
     ap.add_argument("--no-graph", action="store_true", help="launch kernels directly instead of one CUDA graph per frame")
