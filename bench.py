@@ -369,13 +369,94 @@ def run_crisb(args):
     print(json.dumps(line), flush=True)
 
 
+def run_multiview(args):
+    """16 views of uneven resolution (8 x 512^2, 4 x 1280x720, 4 x 1920x1080)
+    of the large scene, 30-frame sequences; batched = one CUDA graph with a
+    branch per view each frame, plain (--no-batch) = the views one after
+    another on one stream.  One GPU (views shard across GPUs as replicas)."""
+    import torch
+
+    from crisoptix_b200 import Batch, Renderer, Scene, _abi, scenes
+
+    torch.cuda.set_device(0)
+    desc, cam0, _, _, ppp = workload("large")
+    sc = Scene(desc)
+    p = params_for("large", sc.scene_size)
+    p.seed = 2
+    p.storage = _abi.STORAGE_FP16 if args.storage == "fp16" else _abi.STORAGE_FP32
+    views = scenes.multiview_cameras(seed=2)
+    rs = [Renderer(w, h, sc, p) for _, w, h in views]
+    outs = [torch.zeros(w * h * 3, dtype=torch.float32, device="cuda") for _, w, h in views]
+    ptrs = [o.data_ptr() for o in outs]
+    px = sum(w * h for _, w, h in views)
+    stream = torch.cuda.Stream()
+    batch = None if args.no_batch else Batch(rs)
+
+    def cams(f):  # each view orbits about the room's vertical axis, 30 frames per sequence
+        return [scenes.orbit_camera(c, f % 30, 60) for c, _, _ in views]
+
+    def frame(f):
+        cs = cams(f)
+        if batch is not None:
+            batch.render(cs, ptrs, stream.cuda_stream)
+        else:
+            for r, c, o in zip(rs, cs, ptrs):
+                r.launch_frame(c, o, stream.cuda_stream)
+
+    with torch.cuda.stream(stream):
+        for f in range(args.warmup):
+            frame(f)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for f in range(args.steps):
+        frame(args.warmup + f)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = t0.elapsed_time(t1)
+    for r in rs:
+        r.check_device_errors()
+    value = ppp * px * args.steps / (ms / 1000.0)
+    launches = sum(r.stats()["kernel_launches"] for r in rs)
+    # end to end: every view's image into pinned host memory each frame
+    hosts = [torch.empty(o.numel(), dtype=torch.float32, pin_memory=True) for o in outs]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    with torch.cuda.stream(stream):
+        for f in range(args.steps):
+            frame(args.warmup + f)
+            for h, o in zip(hosts, outs):
+                h.copy_(o, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e_ms = e0.elapsed_time(e1)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"multiview: 16 views (8x512x512, 4x1280x720, 4x1920x1080) of the large scene, "
+                                   f"{sc.num_triangles} triangles, {px} pixels, "
+                                   f"{'FP16' if p.storage == _abi.STORAGE_FP16 else 'FP32'} storage",
+                       "batched": batch is not None, "paths_per_pixel": ppp,
+                       "l2": "working set larger than L2"},
+            "e2e": {"value": ppp * px * args.steps / (e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": 48 * 16,
+                    "d2h_bytes_per_step": px * 12},
+            "clocks": clk, "gpu_launches": launches * args.steps,
+            "image_mean": float(sum(float(o.mean()) for o in outs) / len(outs))}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="crisb", choices=["crisb", "reference"])
-    ap.add_argument("--workload", default="large", choices=["large", "small"])
+    ap.add_argument("--workload", default="large", choices=["large", "small", "multiview"])
+    ap.add_argument("--no-batch", action="store_true", help="multiview: render the views one after another")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--relmse", type=int, default=0, metavar="SPP",
                     help="also score orbit frame 30, with FP32 and with FP16 storage, by relMSE against one "
@@ -388,6 +469,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "multiview":
+        run_multiview(args)
     else:
         run_crisb(args)
 

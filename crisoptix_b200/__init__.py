@@ -19,7 +19,8 @@ from ._abi import CrisbError, check, load
 from .scenes import Camera as CameraDesc
 from .scenes import Scene as SceneDesc
 
-__all__ = ["Scene", "Renderer", "CameraDesc", "SceneDesc", "default_params", "camera_struct", "CrisbError", "load"]
+__all__ = ["Scene", "Renderer", "Batch", "CameraDesc", "SceneDesc", "default_params", "camera_struct", "CrisbError",
+           "load"]
 
 
 def camera_struct(cam: CameraDesc) -> _abi.Camera:
@@ -222,3 +223,34 @@ class Renderer:
         out = np.zeros(size.value // dt.itemsize, dtype=dt)
         check(load().crisb_debug_read(self.handle, buffer_id, out.ctypes.data_as(ctypes.c_void_p), size.value))
         return out
+
+
+class Batch:
+    """Several renderers (views) of one device whose frames run as parallel
+    branches of one CUDA graph (include/crisb.h, crisb_batch_render)."""
+
+    def __init__(self, renderers):
+        self.renderers = list(renderers)
+        arr = (ctypes.c_void_p * len(self.renderers))(*[r.handle.value for r in self.renderers])
+        h = ctypes.c_void_p()
+        check(load().crisb_batch_create(arr, len(self.renderers), ctypes.byref(h)))
+        self.handle = h
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            try:
+                load().crisb_batch_destroy(h)
+            except Exception:  # interpreter shutdown
+                pass
+            self.handle = None
+
+    def render(self, cameras, out_dev_ptrs, stream: int = 0):
+        """One frame of every view: cameras[k] into the device buffer
+        out_dev_ptrs[k] (W*H*3 floats of renderer k)."""
+        n = len(self.renderers)
+        if len(cameras) != n or len(out_dev_ptrs) != n:
+            raise ValueError("one camera and one output per view")
+        cams = (_abi.Camera * n)(*[camera_struct(c) for c in cameras])
+        outs = (ctypes.c_void_p * n)(*out_dev_ptrs)
+        check(load().crisb_batch_render(self.handle, ctypes.cast(cams, ctypes.c_void_p), outs, ctypes.c_void_p(stream)))

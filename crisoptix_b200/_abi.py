@@ -174,6 +174,9 @@ ENTRY_POINTS = {
     "crisb_renderer_set_params": (c_i32, [c_vp, ctypes.POINTER(Params)]),
     "crisb_renderer_get_params": (c_i32, [c_vp, ctypes.POINTER(Params)]),
     "crisb_render_frame": (c_i32, [c_vp, ctypes.POINTER(Camera), c_vp, c_vp]),
+    "crisb_batch_create": (c_i32, [ctypes.POINTER(c_vp), c_u32, ctypes.POINTER(c_vp)]),
+    "crisb_batch_destroy": (c_i32, [c_vp]),
+    "crisb_batch_render": (c_i32, [c_vp, c_vp, ctypes.POINTER(c_vp), c_vp]),
     "crisb_set_graph": (c_i32, [c_vp, c_i32]),
     "crisb_frame_index": (c_i32, [c_vp, ctypes.POINTER(c_u64)]),
     "crisb_frame_random": (c_i32, [c_vp, ctypes.POINTER(c_u32)]),

@@ -854,6 +854,113 @@ int crisb_renderer_destroy(crisb_renderer* r) {
     return CRISB_OK;
 }
 
+}  // extern "C"
+
+// Several renderers (views) whose frames run as parallel branches of one CUDA
+// graph: the captured launches of every view hang off one fork event and join
+// before the graph ends, so small views and the tails of large ones overlap
+// on the device instead of running one view after another.
+struct crisb_batch {
+    std::vector<crisb_renderer*> views;
+    cudaStream_t cap = nullptr;
+    std::vector<cudaStream_t> branch;
+    std::vector<cudaEvent_t> done;
+    cudaEvent_t fork = nullptr;
+    cudaGraphExec_t exec = nullptr;
+
+    ~crisb_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        for (auto& e : done)
+            if (e) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        for (auto& s : branch)
+            if (s) cudaStreamDestroy(s);
+        if (cap) cudaStreamDestroy(cap);
+    }
+
+    void render(const crisb_camera* cams, float* const* outs, cudaStream_t st) {
+        for (size_t k = 0; k < views.size(); ++k) {
+            require(outs[k] != nullptr, "batch: null output");
+            require(views[k]->timing == 0, "batch: per-kernel timing must be off for batched frames");
+        }
+        check(cudaStreamBeginCapture(cap, cudaStreamCaptureModeRelaxed), "begin capture");
+        cudaGraph_t g = nullptr;
+        try {
+            check(cudaEventRecord(fork, cap), "fork");
+            for (size_t k = 0; k < views.size(); ++k) {
+                check(cudaStreamWaitEvent(branch[k], fork, 0), "branch wait");
+                views[k]->enqueue(cams[k], outs[k], branch[k]);
+                check(cudaEventRecord(done[k], branch[k]), "join");
+                check(cudaStreamWaitEvent(cap, done[k], 0), "join wait");
+            }
+        } catch (...) {
+            cudaStreamEndCapture(cap, &g);
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            throw;
+        }
+        check(cudaStreamEndCapture(cap, &g), "end capture");
+        if (exec) {
+            cudaGraphExecUpdateResultInfo info;
+            if (cudaGraphExecUpdate(exec, g, &info) != cudaSuccess) {
+                cudaGetLastError();
+                cudaGraphExecDestroy(exec);
+                exec = nullptr;
+            }
+        }
+        if (!exec) {
+            const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+            if (e != cudaSuccess) {
+                cudaGraphDestroy(g);
+                exec = nullptr;
+                check(e, "graph instantiate");
+            }
+        }
+        cudaGraphDestroy(g);
+        check(cudaGraphLaunch(exec, st), "graph launch");
+        for (auto* v : views) v->last_stream = st;
+    }
+};
+
+extern "C" {
+
+int crisb_batch_create(crisb_renderer* const* renderers, uint32_t n, crisb_batch** out) {
+    return guarded([&] {
+        require(renderers && out && n > 0, "batch: null argument or no renderers");
+        *out = nullptr;
+        auto b = std::make_unique<crisb_batch>();
+        int dev = 0;
+        check(cudaGetDevice(&dev), "cudaGetDevice");
+        for (uint32_t k = 0; k < n; ++k) {
+            require(renderers[k] != nullptr, "batch: null renderer");
+            require(renderers[k]->scene->device == dev, "batch: renderer on another device");
+            for (uint32_t j = 0; j < k; ++j) require(renderers[j] != renderers[k], "batch: renderer listed twice");
+            b->views.push_back(renderers[k]);
+        }
+        check(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking), "stream");
+        b->branch.assign(n, nullptr);
+        b->done.assign(n, nullptr);
+        for (uint32_t k = 0; k < n; ++k) {
+            check(cudaStreamCreateWithFlags(&b->branch[k], cudaStreamNonBlocking), "stream");
+            check(cudaEventCreateWithFlags(&b->done[k], cudaEventDisableTiming), "event");
+        }
+        check(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "event");
+        *out = b.release();
+    });
+}
+
+int crisb_batch_destroy(crisb_batch* b) {
+    delete b;
+    return CRISB_OK;
+}
+
+int crisb_batch_render(crisb_batch* b, const crisb_camera* cams, float* const* outs, void* stream) {
+    return guarded([&] {
+        require(b && cams && outs, "null argument");
+        b->render(cams, outs, static_cast<cudaStream_t>(stream));
+    });
+}
+
 int crisb_renderer_set_params(crisb_renderer* r, const crisb_params* params) {
     return guarded([&] {
         require(r && params, "null argument");

@@ -355,3 +355,34 @@ def orbit_camera(cam: Camera, frame: int, frames_per_orbit: int = 60) -> Camera:
     for _ in range(frame):
         c = c.rotate_around_origin((0.0, 1.0, 0.0), 2.0 * math.pi / frames_per_orbit)
     return c
+
+
+# Multiview config: 8 views at 512x512, 4 at 1280x720, 4 at 1920x1080.
+MULTIVIEW_RESOLUTIONS = [(512, 512)] * 8 + [(1280, 720)] * 4 + [(1920, 1080)] * 4
+
+
+def multiview_cameras(resolutions=None, radius: float = 12.0, room=(20.0, 8.0, 20.0), seed: int = 2,
+                      fov: float = math.radians(60.0)):
+    """One camera per resolution on a sphere of `radius` about the room centre,
+    seeded jittered directions, each looking at the centre.  Positions are
+    scaled into the room's interior (80% of each half extent) when the sphere
+    reaches outside it, so every camera sees the scene from inside."""
+    res = list(resolutions or MULTIVIEW_RESOLUTIONS)
+    rng = np.random.default_rng(seed)
+    n = len(res)
+    out = []
+    for k, (w, h) in enumerate(res):
+        # stratified directions (golden-angle spiral) with a seeded jitter
+        z = 1.0 - 2.0 * (k + 0.5) / n + rng.uniform(-0.5, 0.5) / n
+        phi = k * math.pi * (3.0 - math.sqrt(5.0)) + rng.uniform(-0.2, 0.2)
+        r = math.sqrt(max(0.0, 1.0 - z * z))
+        d = np.array([r * math.cos(phi), 0.7 * z, r * math.sin(phi)])
+        d /= np.linalg.norm(d)
+        pos = d * radius
+        lim = 0.8 * np.array(room) / 2.0
+        scale = min(1.0, float(np.min(lim / np.maximum(np.abs(pos), 1e-9))))
+        pos = pos * scale
+        view = -pos / np.linalg.norm(pos)
+        out.append((Camera(pos=tuple(float(v) for v in pos), view_dir=tuple(float(v) for v in view),
+                           up=(0.0, 1.0, 0.0), aspect=w / h, fov=fov, changed=False), w, h))
+    return out

@@ -419,6 +419,21 @@ int crisb_render_frame(crisb_renderer* r, const crisb_camera* cam,
                        float* out_rgb_dev, void* stream);
 
 /* Renderer::GetFrameIdx (src/Renderer.cpp:408-411). */
+/* Batched views (survey config MV: many cameras of uneven resolution).  A
+ * batch holds renderers of one device -- one per view, each with its own
+ * resolution, parameters and storage -- and crisb_batch_render runs one frame
+ * of every view as parallel branches of a single CUDA graph launched on
+ * `stream`: cams[k] and outs[k] (W*H*3 floats on the device) belong to
+ * renderers[k].  Each view's results are those of crisb_render_frame on the
+ * same renderer.  The renderers must not be used on other streams while a
+ * batch frame runs, and per-kernel timing must be off.  No counterpart in the
+ * reference, which renders one view per Renderer::LaunchFrame
+ * (src/Renderer.cpp:209-406). */
+typedef struct crisb_batch crisb_batch;
+int crisb_batch_create(crisb_renderer* const* renderers, uint32_t n, crisb_batch** out);
+int crisb_batch_destroy(crisb_batch* b);
+int crisb_batch_render(crisb_batch* b, const crisb_camera* cams, float* const* outs, void* stream);
+
 /* Frames run as one CUDA graph of the pass chain by default (captured, updated in
  * place and launched on the caller's stream); 0 launches the kernels directly.
  * Frames with per-kernel timing on (crisb_set_timing) always launch directly.
