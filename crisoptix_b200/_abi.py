@@ -174,6 +174,14 @@ ENTRY_POINTS = {
     "crisb_renderer_set_params": (c_i32, [c_vp, ctypes.POINTER(Params)]),
     "crisb_renderer_get_params": (c_i32, [c_vp, ctypes.POINTER(Params)]),
     "crisb_render_frame": (c_i32, [c_vp, ctypes.POINTER(Camera), c_vp, c_vp]),
+    "crisb_scene_get_materials": (c_i32, [c_vp, c_vp, c_u32]),
+    "crisb_scene_set_materials": (c_i32, [c_vp, c_vp, c_u32]),
+    "crisb_scene_set_emitter_colors": (c_i32, [c_vp, c_vp, c_u32]),
+    "crisb_adjoint_create": (c_i32, [c_vp, c_u32, c_u32, ctypes.POINTER(Params), ctypes.POINTER(c_vp)]),
+    "crisb_adjoint_destroy": (c_i32, [c_vp]),
+    "crisb_adjoint_refreeze": (c_i32, [c_vp]),
+    "crisb_adjoint_forward": (c_i32, [c_vp, ctypes.POINTER(Camera), c_u64, c_vp, c_vp]),
+    "crisb_adjoint_backward": (c_i32, [c_vp, ctypes.POINTER(Camera), c_u64, c_vp, c_vp, c_vp, c_vp]),
     "crisb_batch_create": (c_i32, [ctypes.POINTER(c_vp), c_u32, ctypes.POINTER(c_vp)]),
     "crisb_batch_destroy": (c_i32, [c_vp]),
     "crisb_batch_render": (c_i32, [c_vp, c_vp, ctypes.POINTER(c_vp), c_vp]),

@@ -1,0 +1,319 @@
+"""Path-replay adjoint of the path tracer (include/crisb.h, crisb_adjoint_*).
+
+``PtAdjoint`` wraps the C ABI; ``PtImage`` is a ``torch.autograd.Function``
+over it, for checking only (the library itself needs no torch); ``fd_check``
+compares the adjoint's gradient of an L2 image loss with central differences
+of the same frozen-sampling estimator, summed in float64.
+
+Parameters as the inverse-rendering config names them: per material the
+diffuse albedo (3) and roughness (1); per emitter its radiance (3), which the
+library holds twice -- the emitter table colour used by next-event estimation
+and the emission of the emitter's material seen by camera rays -- so its
+gradient is the sum of both.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _abi
+from ._abi import check, load
+from .scenes import MATERIAL_DTYPE, Camera
+
+MAT_GRAD = 7  # diffuse rgb, roughness, emission rgb
+EM_GRAD = 3
+
+
+def get_materials(scene) -> np.ndarray:
+    n = len(scene.desc.materials)
+    out = np.zeros(n, MATERIAL_DTYPE)
+    check(load().crisb_scene_get_materials(scene.handle, out.ctypes.data_as(ctypes.c_void_p), n))
+    return out
+
+
+def set_materials(scene, mats: np.ndarray):
+    mats = np.ascontiguousarray(mats, MATERIAL_DTYPE)
+    check(load().crisb_scene_set_materials(scene.handle, mats.ctypes.data_as(ctypes.c_void_p), len(mats)))
+
+
+def set_emitter_colors(scene, rgb: np.ndarray):
+    rgb = np.ascontiguousarray(rgb, np.float32).reshape(-1, 3)
+    check(load().crisb_scene_set_emitter_colors(scene.handle, rgb.ctypes.data_as(ctypes.c_void_p), len(rgb)))
+
+
+class PtAdjoint:
+    """Frozen-sampling path tracer of `scene` at W x H and its adjoint."""
+
+    def __init__(self, scene, width: int, height: int, params: _abi.Params):
+        from . import camera_struct  # noqa: F401  (import check)
+
+        self.scene, self.width, self.height = scene, width, height
+        self.num_mats = len(scene.desc.materials)
+        self.num_emitters = len(scene.desc.emitters)
+        h = ctypes.c_void_p()
+        check(load().crisb_adjoint_create(scene.handle, width, height, ctypes.byref(params), ctypes.byref(h)))
+        self.handle = h
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            try:
+                load().crisb_adjoint_destroy(h)
+            except Exception:  # interpreter shutdown
+                pass
+            self.handle = None
+
+    def refreeze(self):
+        check(load().crisb_adjoint_refreeze(self.handle))
+
+    def forward(self, cam: Camera, frame: int, out_ptr: int, stream: int = 0):
+        from . import camera_struct
+
+        check(load().crisb_adjoint_forward(self.handle, ctypes.byref(camera_struct(cam)), frame,
+                                           ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream)))
+
+    def backward(self, cam: Camera, frame: int, d_img_ptr: int, d_mats_ptr: int, d_em_ptr: int, stream: int = 0):
+        from . import camera_struct
+
+        check(load().crisb_adjoint_backward(self.handle, ctypes.byref(camera_struct(cam)), frame,
+                                            ctypes.c_void_p(d_img_ptr), ctypes.c_void_p(d_mats_ptr),
+                                            ctypes.c_void_p(d_em_ptr), ctypes.c_void_p(stream)))
+
+    def render(self, cams: Sequence[Camera], frame: int = 0):
+        """(V, H, W, 3) float32 device tensor of every camera's image."""
+        import torch
+
+        out = torch.zeros(len(cams), self.height * self.width * 3, dtype=torch.float32, device="cuda")
+        for v, c in enumerate(cams):
+            self.forward(c, frame, out[v].data_ptr())
+        return out.view(len(cams), self.height, self.width, 3)
+
+    def gradient(self, cams: Sequence[Camera], d_img, frame: int = 0):
+        """(materials x 7, emitters x 3) float32 device tensors of dLoss/dparameter
+        for d_img = dLoss/dimage of shape (V, H, W, 3)."""
+        import torch
+
+        d_img = d_img.contiguous().view(len(cams), -1).float()
+        g_mat = torch.zeros(self.num_mats * MAT_GRAD, dtype=torch.float32, device="cuda")
+        g_em = torch.zeros(self.num_emitters * EM_GRAD, dtype=torch.float32, device="cuda")
+        for v, c in enumerate(cams):
+            self.backward(c, frame, d_img[v].data_ptr(), g_mat.data_ptr(), g_em.data_ptr())
+        return g_mat.view(self.num_mats, MAT_GRAD), g_em.view(self.num_emitters, EM_GRAD)
+
+
+def _apply(scene, base: np.ndarray, diffuse, roughness, emission, emitter_rgb):
+    mats = base.copy()
+    mats["diffuse"] = diffuse
+    mats["roughness"] = roughness
+    mats["emission"] = emission
+    set_materials(scene, mats)
+    set_emitter_colors(scene, emitter_rgb)
+
+
+def pt_image_function():
+    """The torch.autograd.Function class (built lazily so importing this module
+    needs no torch)."""
+    import torch
+
+    class PtImage(torch.autograd.Function):
+        """images = PtImage.apply(diffuse (M,3), roughness (M,), emission (M,3),
+        emitter_rgb (E,3), adjoint, base_materials, cameras, frame)"""
+
+        @staticmethod
+        def forward(ctx, diffuse, roughness, emission, emitter_rgb, adj, base, cams, frame):
+            _apply(adj.scene, base, diffuse.detach().cpu().numpy(), roughness.detach().cpu().numpy(),
+                   emission.detach().cpu().numpy(), emitter_rgb.detach().cpu().numpy())
+            ctx.adj, ctx.cams, ctx.frame = adj, cams, frame
+            ctx.like = (diffuse, roughness, emission, emitter_rgb)
+            return adj.render(cams, frame)
+
+        @staticmethod
+        def backward(ctx, grad_img):
+            g_mat, g_em = ctx.adj.gradient(ctx.cams, grad_img, ctx.frame)
+            grads = (g_mat[:, 0:3], g_mat[:, 3], g_mat[:, 4:7], g_em)
+            return tuple(g.to(device=t.device, dtype=t.dtype) for g, t in zip(grads, ctx.like)) + (None,) * 4
+
+    return PtImage
+
+
+@dataclass
+class Param:
+    kind: str   # "diffuse", "roughness" or "radiance"
+    index: int  # material (diffuse, roughness) or emitter (radiance)
+    channel: int = 0
+
+
+def emitter_materials(scene_desc) -> List[int]:
+    """Material of each emitter's faces (the emission camera rays see)."""
+    mats = scene_desc.triangle_material
+    faces = np.asarray(scene_desc.emitter_faces, np.float32).reshape(-1, 9)
+    P = np.asarray(scene_desc.positions, np.float32)[np.asarray(scene_desc.indices)].reshape(-1, 9)
+    out = []
+    for color, first, count in scene_desc.emitters:
+        hit = np.nonzero(np.all(np.abs(P - faces[first]) < 1e-6, axis=1))[0]
+        out.append(int(mats[hit[0]]) if len(hit) else -1)
+    return out
+
+
+def gather(g_mat: np.ndarray, g_em: np.ndarray, params: Sequence[Param], em_mats: Sequence[int]) -> np.ndarray:
+    out = np.zeros(len(params), np.float64)
+    for k, p in enumerate(params):
+        if p.kind == "diffuse":
+            out[k] = g_mat[p.index, p.channel]
+        elif p.kind == "roughness":
+            out[k] = g_mat[p.index, 3]
+        else:
+            out[k] = g_em[p.index, p.channel]
+            if em_mats[p.index] >= 0:
+                out[k] += g_mat[em_mats[p.index], 4 + p.channel]
+    return out
+
+
+def perturb(mats: np.ndarray, emitter_rgb: np.ndarray, p: Param, delta: float, em_mats: Sequence[int]):
+    mats, emitter_rgb = mats.copy(), emitter_rgb.copy()
+    if p.kind == "diffuse":
+        mats["diffuse"][p.index, p.channel] += delta
+    elif p.kind == "roughness":
+        mats["roughness"][p.index] += delta
+    else:
+        emitter_rgb[p.index, p.channel] += delta
+        if em_mats[p.index] >= 0:
+            mats["emission"][em_mats[p.index], p.channel] += delta
+    return mats, emitter_rgb
+
+
+def value_of(mats: np.ndarray, emitter_rgb: np.ndarray, p: Param) -> float:
+    if p.kind == "diffuse":
+        return float(mats["diffuse"][p.index, p.channel])
+    if p.kind == "roughness":
+        return float(mats["roughness"][p.index])
+    return float(emitter_rgb[p.index, p.channel])
+
+
+def fd_check(scene, desc, cams: Sequence[Camera], width: int, height: int, params: _abi.Params,
+             target_mats: np.ndarray, target_rgb: np.ndarray, start_mats: np.ndarray, start_rgb: np.ndarray,
+             check_params: Sequence[Param], eps: float = 1e-3, frame: int = 0) -> dict:
+    """Adjoint gradient of loss = sum over pixels of (image - target)^2 at the
+    start parameters against central differences (relative step `eps`, float64
+    loss sums) of the same frozen-sampling estimator, for `check_params`."""
+    import torch
+
+    em_mats = emitter_materials(desc)
+    set_materials(scene, start_mats)
+    set_emitter_colors(scene, start_rgb)
+    adj = PtAdjoint(scene, width, height, params)  # sampling frozen at the start parameters
+    set_materials(scene, target_mats)
+    set_emitter_colors(scene, target_rgb)
+    target = adj.render(cams, frame).double()
+    set_materials(scene, start_mats)
+    set_emitter_colors(scene, start_rgb)
+    img = adj.render(cams, frame)
+    d_img = 2.0 * (img.double() - target)
+    g_mat, g_em = adj.gradient(cams, d_img.float(), frame)
+    grad = gather(g_mat.cpu().numpy().astype(np.float64), g_em.cpu().numpy().astype(np.float64), check_params,
+                  em_mats)
+
+    def loss(mats, rgb):
+        set_materials(scene, mats)
+        set_emitter_colors(scene, rgb)
+        return float(((adj.render(cams, frame).double() - target) ** 2).sum())
+
+    fd = np.zeros(len(check_params))
+    for k, p in enumerate(check_params):
+        h = eps * max(abs(value_of(start_mats, start_rgb, p)), 1e-2)
+        mp, rp = perturb(start_mats, start_rgb, p, h, em_mats)
+        mm, rm = perturb(start_mats, start_rgb, p, -h, em_mats)
+        fd[k] = (loss(mp, rp) - loss(mm, rm)) / (2.0 * h)
+    set_materials(scene, start_mats)
+    set_emitter_colors(scene, start_rgb)
+    scale = np.maximum(np.abs(fd), 1e-12)
+    rel = np.abs(grad - fd) / scale
+    return {"adjoint": grad, "fd": fd, "rel_err": rel, "loss": loss(start_mats, start_rgb)}
+
+
+def inverse_config_params(desc, num_params: int = 20, seed: int = 3) -> List[Param]:
+    """`num_params` random parameters of the inverse-rendering config: sphere
+    albedos (materials 1..64, 3 channels), GGX roughnesses (odd spheres) and
+    emitter radiances."""
+    rng = np.random.default_rng(seed)
+    mats = desc.materials
+    em_mats = set(emitter_materials(desc))
+    sphere = [m for m in range(1, len(mats)) if m not in em_mats]
+    ggx = [m for m in sphere if float(mats["roughness"][m]) < 1.0]
+    pool: List[Param] = ([Param("diffuse", m, c) for m in sphere for c in range(3)] +
+                         [Param("roughness", m) for m in ggx] +
+                         [Param("radiance", e, c) for e in range(len(desc.emitters)) for c in range(3)])
+    pick = rng.choice(len(pool), size=min(num_params, len(pool)), replace=False)
+    return [pool[i] for i in pick]
+
+
+def perturbed_start(desc, seed: int = 3, sigma: float = 0.1):
+    """Target (ground-truth) parameters = the scene's; start = target * (1 + N(0,
+    sigma)) per parameter (albedos clamped to [0.01, 0.99], roughness to
+    [0.02, 1], radiance >= 0)."""
+    rng = np.random.default_rng(seed)
+    tm = np.array(desc.materials, MATERIAL_DTYPE)
+    trgb = np.array([c for c, _, _ in desc.emitters], np.float32).reshape(-1, 3)
+    sm, srgb = tm.copy(), trgb.copy()
+    em_mats = emitter_materials(desc)
+    sm["diffuse"] = np.clip(tm["diffuse"] * (1 + sigma * rng.standard_normal(tm["diffuse"].shape)), 0.01, 0.99)
+    ggx = tm["roughness"] < 1.0
+    sm["roughness"][ggx] = np.clip(tm["roughness"][ggx] * (1 + sigma * rng.standard_normal(ggx.sum())), 0.02, 1.0)
+    srgb = np.maximum(trgb * (1 + sigma * rng.standard_normal(trgb.shape)), 0.0).astype(np.float32)
+    for e, m in enumerate(em_mats):
+        if m >= 0:
+            sm["emission"][m] = srgb[e]
+            sm["diffuse"][m] = tm["diffuse"][m]
+    return tm, trgb, sm, srgb
+
+
+def main(argv=None):
+    """Central-difference check of the adjoint on the inverse-rendering config:
+    the large scene (64 sphere materials, 256 emitters), 8 views of 512 x 512,
+    L2 loss against images at the ground-truth parameters, start parameters
+    perturbed by N(0, 0.1) relative, 20 random parameters, eps 1e-3, seed 3.
+    Prints one JSON line."""
+    import argparse
+    import json
+    import time
+
+    import torch
+
+    from . import Scene, default_params, scenes
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--views", type=int, default=8)
+    ap.add_argument("--res", type=int, default=512)
+    ap.add_argument("--params", type=int, default=20)
+    ap.add_argument("--eps", type=float, default=1e-3)
+    ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--small", action="store_true", help="a 12-sphere room instead of the large scene")
+    a = ap.parse_args(argv)
+    if a.small:
+        desc, _ = scenes.sphere_room(num_spheres=12, subdiv=2, num_emitters=12, seed=4)
+    else:
+        desc, _ = scenes.sphere_room(num_spheres=64, subdiv=5, num_emitters=256, seed=1)
+    sc = Scene(desc)
+    p = default_params(sc.scene_size, max_path_len=8, nee_prob=0.3, seed=a.seed)
+    views = scenes.multiview_cameras([(a.res, a.res)] * a.views, seed=a.seed)
+    cams = [c for c, _, _ in views]
+    tm, trgb, sm, srgb = perturbed_start(desc, seed=a.seed)
+    chk = inverse_config_params(desc, a.params, a.seed)
+    t0 = time.time()
+    r = fd_check(sc, desc, cams, a.res, a.res, p, tm, trgb, sm, srgb, chk, eps=a.eps)
+    torch.cuda.synchronize()
+    big = np.abs(r["fd"]) > 1e-3 * np.abs(r["fd"]).max()
+    print(json.dumps({"config": f"inverse rendering: {a.views} views {a.res}x{a.res}, {len(desc.materials)} materials, "
+                                f"{len(desc.emitters)} emitters, {len(chk)} parameters, eps {a.eps}, seed {a.seed}",
+                      "max_rel_err": float(r["rel_err"][big].max()) if big.any() else None,
+                      "params_checked": int(big.sum()), "loss": r["loss"],
+                      "params": [f"{q.kind}[{q.index}].{q.channel}" for q in chk],
+                      "adjoint": [float(v) for v in r["adjoint"]], "fd": [float(v) for v in r["fd"]],
+                      "rel_err": [float(v) for v in r["rel_err"]], "seconds": time.time() - t0}))
+
+
+if __name__ == "__main__":
+    main()

@@ -924,6 +924,36 @@ struct crisb_batch {
 
 extern "C" {
 
+int crisb_scene_get_materials(const crisb_scene* scene, crisb_material* out, uint32_t n) {
+    return guarded([&] {
+        require(scene && out, "null argument");
+        require(n == scene->mats.n, "scene: material count mismatch");
+        check(cudaMemcpy(out, scene->mats.p, n * sizeof(crisb_material), cudaMemcpyDeviceToHost), "read");
+    });
+}
+
+int crisb_scene_set_materials(crisb_scene* scene, const crisb_material* mats, uint32_t n) {
+    return guarded([&] {
+        require(scene && mats, "null argument");
+        require(n == scene->mats.n, "scene: material count mismatch");
+        check(cudaDeviceSynchronize(), "sync");
+        check(cudaMemcpy(scene->mats.p, mats, n * sizeof(crisb_material), cudaMemcpyHostToDevice), "write");
+    });
+}
+
+int crisb_scene_set_emitter_colors(crisb_scene* scene, const float* rgb, uint32_t n) {
+    return guarded([&] {
+        require(scene && rgb, "null argument");
+        require(n == scene->num_emitters, "scene: emitter count mismatch");
+        std::vector<crisb_emitter> e(n);
+        check(cudaDeviceSynchronize(), "sync");
+        check(cudaMemcpy(e.data(), scene->emitters.p, n * sizeof(crisb_emitter), cudaMemcpyDeviceToHost), "read");
+        for (uint32_t k = 0; k < n; ++k)
+            for (int c = 0; c < 3; ++c) e[k].color[c] = rgb[3 * k + c];
+        check(cudaMemcpy(scene->emitters.p, e.data(), n * sizeof(crisb_emitter), cudaMemcpyHostToDevice), "write");
+    });
+}
+
 int crisb_batch_create(crisb_renderer* const* renderers, uint32_t n, crisb_batch** out) {
     return guarded([&] {
         require(renderers && out && n > 0, "batch: null argument or no renderers");
@@ -946,6 +976,89 @@ int crisb_batch_create(crisb_renderer* const* renderers, uint32_t n, crisb_batch
         }
         check(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "event");
         *out = b.release();
+    });
+}
+
+}  // extern "C"
+
+struct crisb_adjoint {
+    crisb_scene* scene = nullptr;
+    uint32_t width = 0, height = 0;
+    crisb_params params{};
+    DevBuf<crisb_material> sample_mats;  // theta0
+
+    FrameParams frame(const crisb_camera& cam, uint64_t index) const {
+        FrameParams fp;
+        std::memset(&fp, 0, sizeof(fp));
+        fp.p = params;
+        fp.cam = camera_data(cam);
+        fp.width = width;
+        fp.height = height;
+        fp.random = frame_random(params.seed, index);
+        fp.k = 0;
+        return fp;
+    }
+    void freeze() {
+        sample_mats.alloc(scene->mats.n);
+        check(cudaMemcpy(sample_mats.p, scene->mats.p, scene->mats.bytes(), cudaMemcpyDeviceToDevice), "freeze");
+        check(cudaDeviceSynchronize(), "freeze");
+    }
+};
+
+extern "C" {
+
+int crisb_adjoint_create(crisb_scene* scene, uint32_t width, uint32_t height, const crisb_params* params,
+                         crisb_adjoint** out) {
+    return guarded([&] {
+        require(scene && params && out, "null argument");
+        *out = nullptr;
+        require(width > 0 && height > 0 && static_cast<uint64_t>(width) * height < (1ull << 26), "adjoint: bad size");
+        validate_params(*params);
+        require(params->max_path_len <= 16, "adjoint: max_path_len must be <= 16");
+        require(scene->num_emitters > 0, "adjoint: the scene has no emitters");
+        auto a = std::make_unique<crisb_adjoint>();
+        a->scene = scene;
+        a->width = width;
+        a->height = height;
+        a->params = *params;
+        a->freeze();
+        *out = a.release();
+    });
+}
+
+int crisb_adjoint_destroy(crisb_adjoint* a) {
+    delete a;
+    return CRISB_OK;
+}
+
+int crisb_adjoint_refreeze(crisb_adjoint* a) {
+    return guarded([&] {
+        require(a != nullptr, "null argument");
+        a->freeze();
+    });
+}
+
+int crisb_adjoint_forward(crisb_adjoint* a, const crisb_camera* cam, uint64_t frame, float* out_rgb_dev,
+                          void* stream) {
+    return guarded([&] {
+        require(a && cam && out_rgb_dev, "null argument");
+        const FrameParams fp = a->frame(*cam, frame);
+        const SceneView s = a->scene->view(a->scene->err.p);
+        adjoint_forward(s, a->sample_mats.p, static_cast<uint32_t>(a->sample_mats.n), fp, out_rgb_dev,
+                        static_cast<cudaStream_t>(stream));
+        check(cudaGetLastError(), "adjoint forward");
+    });
+}
+
+int crisb_adjoint_backward(crisb_adjoint* a, const crisb_camera* cam, uint64_t frame, const float* d_image_dev,
+                           float* d_materials_dev, float* d_emitters_dev, void* stream) {
+    return guarded([&] {
+        require(a && cam && d_image_dev && d_materials_dev && d_emitters_dev, "null argument");
+        const FrameParams fp = a->frame(*cam, frame);
+        const SceneView s = a->scene->view(a->scene->err.p);
+        adjoint_backward(s, a->sample_mats.p, static_cast<uint32_t>(a->sample_mats.n), fp, d_image_dev,
+                         d_materials_dev, d_emitters_dev, static_cast<cudaStream_t>(stream));
+        check(cudaGetLastError(), "adjoint backward");
     });
 }
 

@@ -128,6 +128,11 @@ void launch_store_entries(const SceneView& s, const FrameParams& fp, const Bufs&
 void launch_knn_finish(const FrameParams& fp, const Bufs& b, const lbvh::Work& w, float4* leaf_entries,
                        cudaStream_t st);
 void launch_final_gather(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, cudaStream_t st);
+// path-replay adjoint of the frozen-sampling path tracer (adjoint.cu)
+void adjoint_forward(const SceneView& eval, const crisb_material* sample_mats, uint32_t num_mats,
+                     const FrameParams& fp, float* out, cudaStream_t st);
+void adjoint_backward(const SceneView& eval, const crisb_material* sample_mats, uint32_t num_mats,
+                      const FrameParams& fp, const float* d_img, float* g_mat, float* g_em, cudaStream_t st);
 // generic LBVH stages over `cap` primitives (count in w.n)
 void launch_lbvh_hierarchy(const lbvh::Work& w, uint32_t cap, int leaf_max, cudaStream_t st);
 

@@ -576,6 +576,7 @@ RT_D BrdfSample brdf_sample(const SceneView& s, const Isect& it, Rng& rng) {
 struct EmitterSample {
     V3 pos;
     V3 color;
+    uint32_t index;  // the emitter chosen
 };
 
 RT_D EmitterSample sample_emitter(const SceneView& s, Rng& rng) {
@@ -594,6 +595,7 @@ RT_D EmitterSample sample_emitter(const SceneView& s, Rng& rng) {
     EmitterSample es;
     es.pos = r0 * v0 + r1 * v1 + r2 * v2;
     es.color = V3{e.color[0], e.color[1], e.color[2]};
+    es.index = static_cast<uint32_t>(ei);
     return es;
 }
 

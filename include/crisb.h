@@ -419,6 +419,37 @@ int crisb_render_frame(crisb_renderer* r, const crisb_camera* cam,
                        float* out_rgb_dev, void* stream);
 
 /* Renderer::GetFrameIdx (src/Renderer.cpp:408-411). */
+/* Scene material and emitter tables after creation (for parameter updates of
+ * inverse rendering; counts must equal those given at creation).  Renderers
+ * and adjoint contexts of the scene see the new values from their next call. */
+int crisb_scene_get_materials(const crisb_scene* scene, crisb_material* out, uint32_t n);
+int crisb_scene_set_materials(crisb_scene* scene, const crisb_material* mats, uint32_t n);
+int crisb_scene_set_emitter_colors(crisb_scene* scene, const float* rgb, uint32_t n);
+
+/* Path-replay adjoint (survey config INV).  The estimator is the path tracer
+ * (TraceCompletePath, include/graph/restir/path_gen.h:389-472) with frozen
+ * sampling: random decisions, sampled directions and sampling pdfs use the
+ * material table copied when the context is made (or at
+ * crisb_adjoint_refreeze), BRDF values, emissions and emitter colours use the
+ * scene's current tables.  At the frozen parameters it equals the path tracer
+ * sample for sample, and it is smooth in the parameters.
+ * crisb_adjoint_forward writes one sample per pixel (seed from params.seed and
+ * `frame`) into out_rgb_dev (W*H*3 floats).  crisb_adjoint_backward replays the
+ * same paths and ADDS dLoss/dparameter, given d_image_dev = dLoss/dimage
+ * (W*H*3), into d_materials_dev (7 floats per material: diffuse rgb,
+ * roughness, emission rgb) and d_emitters_dev (3 floats per emitter: colour).
+ * max_path_len must be <= 16.  No counterpart in the reference, which has no
+ * differentiable renderer. */
+typedef struct crisb_adjoint crisb_adjoint;
+int crisb_adjoint_create(crisb_scene* scene, uint32_t width, uint32_t height, const crisb_params* params,
+                         crisb_adjoint** out);
+int crisb_adjoint_destroy(crisb_adjoint* a);
+int crisb_adjoint_refreeze(crisb_adjoint* a);
+int crisb_adjoint_forward(crisb_adjoint* a, const crisb_camera* cam, uint64_t frame, float* out_rgb_dev,
+                          void* stream);
+int crisb_adjoint_backward(crisb_adjoint* a, const crisb_camera* cam, uint64_t frame, const float* d_image_dev,
+                           float* d_materials_dev, float* d_emitters_dev, void* stream);
+
 /* Batched views (survey config MV: many cameras of uneven resolution).  A
  * batch holds renderers of one device -- one per view, each with its own
  * resolution, parameters and storage -- and crisb_batch_render runs one frame
