@@ -234,10 +234,10 @@ def fd_check(scene, desc, cams: Sequence[Camera], width: int, height: int, param
     return {"adjoint": grad, "fd": fd, "rel_err": rel, "loss": loss(start_mats, start_rgb)}
 
 
-def inverse_config_params(desc, num_params: int = 20, seed: int = 3) -> List[Param]:
+def inverse_config_params(desc, num_params: int = 20, seed: int = 3, min_roughness: int = 0) -> List[Param]:
     """`num_params` random parameters of the inverse-rendering config: sphere
     albedos (materials 1..64, 3 channels), GGX roughnesses (odd spheres) and
-    emitter radiances."""
+    emitter radiances; at least `min_roughness` of them roughnesses."""
     rng = np.random.default_rng(seed)
     mats = desc.materials
     em_mats = set(emitter_materials(desc))
@@ -246,7 +246,13 @@ def inverse_config_params(desc, num_params: int = 20, seed: int = 3) -> List[Par
     pool: List[Param] = ([Param("diffuse", m, c) for m in sphere for c in range(3)] +
                          [Param("roughness", m) for m in ggx] +
                          [Param("radiance", e, c) for e in range(len(desc.emitters)) for c in range(3)])
-    pick = rng.choice(len(pool), size=min(num_params, len(pool)), replace=False)
+    pick = list(rng.choice(len(pool), size=min(num_params, len(pool)), replace=False))
+    have = sum(1 for i in pick if pool[i].kind == "roughness")
+    if have < min_roughness:
+        first = len(sphere) * 3
+        extra = [first + j for j in rng.permutation(len(ggx)) if first + j not in pick][: min_roughness - have]
+        drop = [i for i in pick if pool[i].kind != "roughness"][: len(extra)]
+        pick = [i for i in pick if i not in drop] + extra
     return [pool[i] for i in pick]
 
 
@@ -290,6 +296,7 @@ def main(argv=None):
     ap.add_argument("--params", type=int, default=20)
     ap.add_argument("--eps", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--min-roughness", type=int, default=4, help="at least this many roughness parameters")
     ap.add_argument("--small", action="store_true", help="a 12-sphere room instead of the large scene")
     a = ap.parse_args(argv)
     if a.small:
@@ -301,7 +308,7 @@ def main(argv=None):
     views = scenes.multiview_cameras([(a.res, a.res)] * a.views, seed=a.seed)
     cams = [c for c, _, _ in views]
     tm, trgb, sm, srgb = perturbed_start(desc, seed=a.seed)
-    chk = inverse_config_params(desc, a.params, a.seed)
+    chk = inverse_config_params(desc, a.params, a.seed, a.min_roughness)
     t0 = time.time()
     r = fd_check(sc, desc, cams, a.res, a.res, p, tm, trgb, sm, srgb, chk, eps=a.eps)
     torch.cuda.synchronize()

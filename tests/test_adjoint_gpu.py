@@ -20,7 +20,8 @@ def test_adjoint_matches_central_differences(cuda_device):
     sc = Scene(desc)
     p = large_config_params(scene_size_of(desc), max_path_len=6)
     tm, trgb, sm, srgb = adjoint.perturbed_start(desc, seed=3)
-    params = adjoint.inverse_config_params(desc, num_params=20, seed=3)
+    params = adjoint.inverse_config_params(desc, num_params=20, seed=3, min_roughness=5)
+    assert sum(q.kind == "roughness" for q in params) >= 5
     cams = [cam, scenes.orbit_camera(cam, 15, 60)]
     r = adjoint.fd_check(sc, desc, cams, 96, 64, p, tm, trgb, sm, srgb, params, eps=1e-3)
     big = np.abs(r["fd"]) > 1e-3 * np.abs(r["fd"]).max()
