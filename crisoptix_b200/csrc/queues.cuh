@@ -65,7 +65,7 @@ RT_D void set_occluded(ShiftJob& j, uint32_t v) { j.hit.x = __uint_as_float(v); 
 // queue, then [nc, nc + ns) of the shadow queue, so the two queues' tails
 // (the last, slowest rays) overlap instead of running back to back.
 template <class R>
-__global__ void __launch_bounds__(kPassBlock) k_q_trace(SceneView s, const uint32_t* qc, const uint32_t* ccnt,
+__global__ void __launch_bounds__(kPassBlock, 8) k_q_trace(SceneView s, const uint32_t* qc, const uint32_t* ccnt,
                                                         const uint32_t* qs, const uint32_t* scnt, R* rec) {
     const uint32_t nc = *ccnt, ns = *scnt;
     const uint32_t n = nc + ns;
