@@ -102,10 +102,11 @@ def resample_bytes(k: int, spatial_count: int, spatial_rounds: int, copy_prefix_
 
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the seven
-# resampling launches of one frame, from one ncu capture of the large workload
-# at 960x540 (518,400 px, caches flushed before each launch), with the pixel
-# count it was taken at; scaled by pixels to the bench resolution.
-PROFILED_TRAFFIC = {"resampling": (934.06e6, 960 * 540)}
+# resampling launches of one frame, from ncu captures of the large workload
+# at 960x540 (518,400 px, caches flushed before each launch), per reservoir
+# storage, with the pixel count it was taken at; scaled by pixels to the bench
+# resolution.
+PROFILED_TRAFFIC = {"resampling": (867.04e6, 960 * 540), "resampling_fp16": (610.73e6, 960 * 540)}
 
 
 class ClockSampler:
@@ -315,8 +316,9 @@ def run_crisb(args):
     res_bytes = sum(rb.values()) * W * H
     achieved = res_bytes / (passes["resample_ms"] / 1000.0) / 1e9
     traffic = None
-    if "resampling" in PROFILED_TRAFFIC and p.storage != _abi.STORAGE_FP16:
-        tb, tpx = PROFILED_TRAFFIC["resampling"]
+    key = "resampling_fp16" if p.storage == _abi.STORAGE_FP16 else "resampling"
+    if key in PROFILED_TRAFFIC:
+        tb, tpx = PROFILED_TRAFFIC[key]
         traffic = tb * (W * H) / tpx
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "kernel": "resampling kernels (reuse-pass combine / select)",
