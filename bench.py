@@ -238,6 +238,7 @@ def run_crisb(args):
     p.storage = _abi.STORAGE_FP16 if args.storage == "fp16" else _abi.STORAGE_FP32
     r = Renderer(W, H, sc, p)
     r.set_graph(not args.no_graph)
+    tuned = r.autotune(cam, 3) if args.autotune else None
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
     out = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
@@ -361,7 +362,8 @@ def run_crisb(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_frame, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config_for(args.workload, W, H, sc.num_triangles, p, ppp, world, not args.no_graph),
+            "config": dict(config_for(args.workload, W, H, sc.num_triangles, p, ppp, world, not args.no_graph),
+                           trace_grid=tuned if tuned is not None else 8),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 48, "d2h_bytes_per_step": W * H * 12},
             "roofline": roofline, "traversal": traversal, "phases_ms": phases, "pass_ms": pass_ms,
             "cpu_baseline": cb, "clocks": clk,
@@ -465,6 +467,7 @@ def main():
                          "SPP-sample FP64-accumulated path-traced reference")
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"],
                     help="reservoir storage between passes and frames (fp16: packed binary16 / octahedral records)")
+    ap.add_argument("--autotune", action="store_true", help="pick the traversal launch shape by timing candidates")
     ap.add_argument("--no-graph", action="store_true", help="launch kernels directly instead of one CUDA graph per frame")
     ap.add_argument("--cpu-scale", type=int, default=2)
     ap.add_argument("--res", default=None, help="WxH override of the workload resolution (profiling runs)")

@@ -199,6 +199,16 @@ class Renderer:
         check(load().crisb_frame_random(self.handle, ctypes.byref(v)))
         return v.value
 
+    def set_trace_grid(self, blocks_per_resident_block: int):
+        check(load().crisb_set_trace_grid(self.handle, int(blocks_per_resident_block)))
+
+    def autotune(self, camera: CameraDesc, frames: int = 3) -> int:
+        """Pick the traversal launch shape by timing candidates on a scratch
+        renderer (this renderer's state is untouched); returns the choice."""
+        v = ctypes.c_uint32()
+        check(load().crisb_autotune(self.handle, ctypes.byref(camera_struct(camera)), int(frames), ctypes.byref(v)))
+        return v.value
+
     def set_graph(self, enable: bool):
         """Run frames as one CUDA graph of the pass chain (default) or launch
         the kernels directly; the results are identical."""

@@ -595,6 +595,11 @@ struct crisb_renderer {
     // caller's stream.  Per-kernel timing records events between launches, so
     // timed frames launch directly.
     bool graph_enabled = true;
+    // traversal grid = trace_grid x the blocks resident at once: the queue
+    // kernels give each thread a fixed share of rays, and a larger grid evens
+    // out the tail (8 measured best on the 1080p workload; crisb_autotune
+    // picks it per workload)
+    uint32_t trace_grid = 8;
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
 
@@ -661,6 +666,7 @@ struct crisb_renderer {
         fp.front = front;
         fp.back = back;
         fp.k = K();
+        fp.trace_grid = trace_grid;
         SceneView s = scene->view(err.p);
         last_stream = st;
         ktimer.n = 0;
@@ -1102,6 +1108,68 @@ int crisb_render_frame(crisb_renderer* r, const crisb_camera* cam, float* out_rg
     return guarded([&] {
         require(r && cam, "null argument");
         r->render(*cam, out_rgb_dev, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int crisb_set_trace_grid(crisb_renderer* r, uint32_t blocks_per_resident_block) {
+    return guarded([&] {
+        require(r != nullptr, "null renderer");
+        require(blocks_per_resident_block >= 1 && blocks_per_resident_block <= 64, "trace grid must be in [1, 64]");
+        r->trace_grid = blocks_per_resident_block;
+    });
+}
+
+int crisb_autotune(crisb_renderer* r, const crisb_camera* cam, uint32_t frames, uint32_t* chosen) {
+    return guarded([&] {
+        require(r && cam && frames > 0, "autotune: null argument or no frames");
+        // a scratch renderer of the same scene, size and parameters: the
+        // caller's renderer keeps its state
+        crisb_renderer* t = nullptr;
+        if (crisb_renderer_create(r->scene, r->width, r->height, &r->params, &t) != CRISB_OK)
+            throw Error(CRISB_ERR_CUDA, g_last_error);
+        std::unique_ptr<crisb_renderer> tmp(t);
+        DevBuf<float> out;
+        out.alloc(static_cast<size_t>(r->P()) * 3);
+        cudaStream_t st = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+        check(cudaEventCreate(&e0), "event");
+        check(cudaEventCreate(&e1), "event");
+        const uint32_t cand[] = {1, 2, 4, 8, 16};
+        constexpr int kCand = 5;
+        // warm up until the reservoirs carry history (the per-frame cost of a
+        // fresh renderer's first frames is lower), then time the candidates
+        // interleaved frame by frame so that drift hits all of them alike
+        for (int f = 0; f < 4; ++f) tmp->render(*cam, out.p, st);
+        for (int k = 0; k < kCand; ++k) {  // graph instantiation per shape
+            tmp->trace_grid = cand[k];
+            tmp->render(*cam, out.p, st);
+        }
+        float total[kCand] = {};
+        for (uint32_t f = 0; f < std::max<uint32_t>(frames, 3); ++f) {
+            for (int k = 0; k < kCand; ++k) {
+                tmp->trace_grid = cand[k];
+                check(cudaEventRecord(e0, st), "event");
+                tmp->render(*cam, out.p, st);
+                check(cudaEventRecord(e1, st), "event");
+                check(cudaEventSynchronize(e1), "sync");
+                float ms = 0.0f;
+                check(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+                total[k] += ms;
+            }
+        }
+        uint32_t best = r->trace_grid;
+        float best_ms = INFINITY;
+        for (int k = 0; k < kCand; ++k)
+            if (total[k] < best_ms) {
+                best_ms = total[k];
+                best = cand[k];
+            }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaStreamDestroy(st);
+        r->trace_grid = best;
+        if (chosen) *chosen = best;
     });
 }
 

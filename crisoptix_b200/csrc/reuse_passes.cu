@@ -15,6 +15,7 @@
 // shader/suffix_spatial_reuse.cu, shader/final_gather.cu:69-188,
 // shader/prefix_gen_temp_reuse.cu) and gives
 // the same bits; only the SIMD utilisation changes.
+#include <algorithm>
 #include <mutex>
 
 #include "queues.cuh"
@@ -703,7 +704,7 @@ void run_shift_jobs(const SceneView& s0, const FrameParams& fp, const Bufs& b, i
     MARK(kClsShift);
     for (int r = 0; r < kShiftRounds; ++r) {
         const int cur = r & 1, nxt = cur ^ 1;
-        k_q_trace<ShiftJob><<<g.trace, kPassBlock, 0, st>>>(s, b.job_queue[2 * cur], b.job_qcount + 2 * cur,
+        k_q_trace<ShiftJob><<<g.trace * std::max(fp.trace_grid, 1u), kPassBlock, 0, st>>>(s, b.job_queue[2 * cur], b.job_qcount + 2 * cur,
                                                             b.job_queue[2 * cur + 1], b.job_qcount + 2 * cur + 1,
                                                             b.jobs);
         MARK(kClsTrace);

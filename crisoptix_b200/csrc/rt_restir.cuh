@@ -20,6 +20,7 @@ struct FrameParams {
     uint32_t frame_idx;  // for the accumulation blend factor
     int front, back;     // 0/1 buffer selection
     uint32_t k;          // gatherM - 1
+    uint32_t trace_grid; // traversal launches: blocks per resident block (host side only)
 };
 
 // ---- reservoir (include/graph/restir/Reservoir.h:28-50) ------------------------

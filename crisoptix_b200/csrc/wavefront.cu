@@ -239,7 +239,7 @@ void wf_rounds(const SceneView& s, const FrameParams& fp, const Bufs& b, int flo
     const int rounds = wf_round_count(fp);
     for (int r = 0; r < rounds; ++r) {
         const int cur = r & 1, nxt = cur ^ 1;
-        k_q_trace<WfPath><<<g.trace, kPassBlock, 0, st>>>(s, b.wf_queue[2 * cur], b.wf_count + 2 * cur,
+        k_q_trace<WfPath><<<g.trace * std::max(fp.trace_grid, 1u), kPassBlock, 0, st>>>(s, b.wf_queue[2 * cur], b.wf_count + 2 * cur,
                                                           b.wf_queue[2 * cur + 1], b.wf_count + 2 * cur + 1, b.wf);
         if (m) m->mark(kClsTrace, st);
         if (r + 1 < rounds) {

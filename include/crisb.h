@@ -465,6 +465,15 @@ int crisb_batch_create(crisb_renderer* const* renderers, uint32_t n, crisb_batch
 int crisb_batch_destroy(crisb_batch* b);
 int crisb_batch_render(crisb_batch* b, const crisb_camera* cams, float* const* outs, void* stream);
 
+/* Launch shape of the traversal kernels: blocks per block resident at once
+ * (default 8; results do not depend on it).  crisb_autotune renders `frames`
+ * frames of `cam` for each candidate (1, 2, 4, 8, 16) on a scratch renderer of
+ * the same scene, size and parameters -- the given renderer's state is left
+ * alone -- and keeps the fastest, returned in *chosen.  No counterpart in the
+ * reference. */
+int crisb_set_trace_grid(crisb_renderer* r, uint32_t blocks_per_resident_block);
+int crisb_autotune(crisb_renderer* r, const crisb_camera* cam, uint32_t frames, uint32_t* chosen);
+
 /* Frames run as one CUDA graph of the pass chain by default (captured, updated in
  * place and launched on the caller's stream); 0 launches the kernels directly.
  * Frames with per-kernel timing on (crisb_set_timing) always launch directly.

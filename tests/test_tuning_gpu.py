@@ -1,0 +1,32 @@
+"""Launch-shape tuning: the traversal grid changes no result, and autotuning
+leaves the renderer's own frame sequence untouched."""
+import pytest
+import torch
+
+from crisoptix_b200 import Renderer, Scene, _abi
+from helpers import large_config_params, orbit, scene_size_of, small_sphere_room
+
+BUFS = [_abi.BUF_PREFIX_RES_FRONT, _abi.BUF_SUFFIX_RES_FRONT, _abi.BUF_GBUFFER]
+
+
+@pytest.mark.gpu
+def test_trace_grid_and_autotune_do_not_change_results(cuda_device):
+    desc, cam = small_sphere_room()
+    sc = Scene(desc)
+    p = large_config_params(scene_size_of(desc), gather_radius=0.3)
+    ref = Renderer(48, 40, sc, p)
+    ref.set_trace_grid(1)
+    tuned = Renderer(48, 40, sc, p)
+    out_r = torch.zeros(48 * 40 * 3, device="cuda")
+    out_t = torch.zeros(48 * 40 * 3, device="cuda")
+    for f in range(4):
+        c = orbit(cam, f, 120)
+        if f == 1:
+            chosen = tuned.autotune(c, frames=1)
+            assert chosen in (1, 2, 4, 8, 16)
+        ref.launch_frame(c, out_r.data_ptr())
+        tuned.launch_frame(c, out_t.data_ptr())
+        torch.cuda.synchronize()
+        assert out_r.cpu().numpy().tobytes() == out_t.cpu().numpy().tobytes(), f
+        for b in BUFS:
+            assert ref.debug_read(b).tobytes() == tuned.debug_read(b).tobytes(), (f, b)
