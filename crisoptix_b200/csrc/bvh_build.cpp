@@ -217,11 +217,11 @@ struct Collapser {
     bool is_leaf(int i) const { return bin[i].left < 0; }
 
     // children of the wide node standing for binary inner node `i`
-    void gather(int i, int ch[4], int& k) const {
+    void gather(int i, int ch[kBvhWidth], int& k) const {
         ch[0] = bin[i].left;
         ch[1] = bin[i].right;
         k = 2;
-        while (k < 4) {
+        while (k < kBvhWidth) {
             int pick = -1;
             float best = -1.0f;
             for (int c = 0; c < k; ++c) {
@@ -242,11 +242,11 @@ struct Collapser {
     // lays out the subtree of binary inner node `i` at wide index `w`;
     // returns the worst-case stack entries below it
     int emit(int i, uint32_t w) {
-        int ch[4], k;
+        int ch[kBvhWidth], k;
         gather(i, ch, k);
         Bvh4Node nd;
         int inner = 0;
-        for (int c = 0; c < 4; ++c) {
+        for (int c = 0; c < kBvhWidth; ++c) {
             nd.link[c] = kNoChild;
             nd.count[c] = 0;
             nd.lo_x[c] = nd.lo_y[c] = nd.lo_z[c] = 0.0f;
@@ -291,7 +291,7 @@ WideBvh build_wide_bvh(const float* pos, uint32_t n, int leaf_max, int median_de
     if (n == 0) {
         Bvh4Node nd;
         std::memset(&nd, 0, sizeof(nd));
-        for (int c = 0; c < 4; ++c) nd.link[c] = kNoChild;
+        for (int c = 0; c < kBvhWidth; ++c) nd.link[c] = kNoChild;
         r.nodes.push_back(nd);
         return r;
     }
@@ -318,7 +318,7 @@ WideBvh build_wide_bvh(const float* pos, uint32_t n, int leaf_max, int median_de
         // a single leaf: one wide node with one leaf child
         Bvh4Node nd;
         std::memset(&nd, 0, sizeof(nd));
-        for (int c = 0; c < 4; ++c) nd.link[c] = kNoChild;
+        for (int c = 0; c < kBvhWidth; ++c) nd.link[c] = kNoChild;
         const Box& bx = bin[root].box;
         nd.lo_x[0] = bx.lo[0];
         nd.lo_y[0] = bx.lo[1];
@@ -358,7 +358,7 @@ void validate_wide_bvh(const WideBvh& bvh, const float* pos, uint32_t n, int lea
         max_stack = std::max(max_stack, it.stack);
         const Bvh4Node& nd = bvh.nodes[it.node];
         int inner = 0;
-        for (int c = 0; c < 4; ++c) {
+        for (int c = 0; c < kBvhWidth; ++c) {
             const int l = nd.link[c];
             if (l == kNoChild) continue;
             if (l >= 0) {
@@ -382,14 +382,14 @@ void validate_wide_bvh(const WideBvh& bvh, const float* pos, uint32_t n, int lea
             }
         }
         const int pushed = std::max(inner - 1, 0);
-        for (int c = 0; c < 4; ++c) {
+        for (int c = 0; c < kBvhWidth; ++c) {
             const int l = nd.link[c];
             if (l == kNoChild || l < 0) continue;
             if (static_cast<size_t>(l) >= nn || l == 0) fail("inner link out of range");
             if (seen_node[l]) fail("inner node reached twice");
             seen_node[l] = 1;
             const Bvh4Node& ch = bvh.nodes[l];
-            for (int g = 0; g < 4; ++g) {
+            for (int g = 0; g < kBvhWidth; ++g) {
                 if (ch.link[g] == kNoChild) continue;
                 if (ch.lo_x[g] < nd.lo_x[c] || ch.hi_x[g] > nd.hi_x[c] || ch.lo_y[g] < nd.lo_y[c] ||
                     ch.hi_y[g] > nd.hi_y[c] || ch.lo_z[g] < nd.lo_z[c] || ch.hi_z[g] > nd.hi_z[c])

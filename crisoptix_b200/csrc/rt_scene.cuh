@@ -249,28 +249,40 @@ struct Trav {
             dev_error(s, kDevErrIterations);
             return true;
         }
-        // rows of the node: lo_x hi_x lo_y hi_y lo_z hi_z (one float4 per
-        // plane over the four children), links, counts.  Per axis the near
-        // plane is lo for a positive inverse direction and hi otherwise, so
-        // min(t_lo, t_hi) of the slab test is the near plane's t.
+        // rows of the node: lo_x hi_x lo_y hi_y lo_z hi_z (kBvhWidth / 4
+        // float4 per plane over the children), links, counts.  Per axis the
+        // near plane is lo for a positive inverse direction and hi otherwise,
+        // so min(t_lo, t_hi) of the slab test is the near plane's t.
+        constexpr int kQ = kBvhWidth / 4;
         const float4* np = reinterpret_cast<const float4*>(s.nodes + cur);
         const int sx = signbit(r.inv.x) ? 1 : 0, sy = signbit(r.inv.y) ? 1 : 0, sz = signbit(r.inv.z) ? 1 : 0;
-        const float4 nx = __ldg(np + sx), fx = __ldg(np + (1 - sx));
-        const float4 ny = __ldg(np + 2 + sy), fy = __ldg(np + 3 - sy);
-        const float4 nz = __ldg(np + 4 + sz), fz = __ldg(np + 5 - sz);
-        const int4 lk = __ldg(reinterpret_cast<const int4*>(np + 6));
-        const int4 ct = __ldg(reinterpret_cast<const int4*>(np + 7));
         const float bnd = bound();
-        int link[4] = {lk.x, lk.y, lk.z, lk.w};
-        const int cnt[4] = {ct.x, ct.y, ct.z, ct.w};
-        float tn[4];
-        bool hit[4];
-        hit[0] = link[0] != kNoChild && slab_nf(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, bnd, tn[0]);
-        hit[1] = link[1] != kNoChild && slab_nf(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, bnd, tn[1]);
-        hit[2] = link[2] != kNoChild && slab_nf(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, bnd, tn[2]);
-        hit[3] = link[3] != kNoChild && slab_nf(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, bnd, tn[3]);
+        int link[kBvhWidth];
+        int cnt[kBvhWidth];
+        float tn[kBvhWidth];
+        bool hit[kBvhWidth];
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
+        for (int j = 0; j < kQ; ++j) {
+            const float4 nx = __ldg(np + sx * kQ + j), fx = __ldg(np + (1 - sx) * kQ + j);
+            const float4 ny = __ldg(np + (2 + sy) * kQ + j), fy = __ldg(np + (3 - sy) * kQ + j);
+            const float4 nz = __ldg(np + (4 + sz) * kQ + j), fz = __ldg(np + (5 - sz) * kQ + j);
+            const int4 lk = __ldg(reinterpret_cast<const int4*>(np + 6 * kQ + j));
+            const int4 ct = __ldg(reinterpret_cast<const int4*>(np + 7 * kQ + j));
+            link[4 * j + 0] = lk.x;
+            link[4 * j + 1] = lk.y;
+            link[4 * j + 2] = lk.z;
+            link[4 * j + 3] = lk.w;
+            cnt[4 * j + 0] = ct.x;
+            cnt[4 * j + 1] = ct.y;
+            cnt[4 * j + 2] = ct.z;
+            cnt[4 * j + 3] = ct.w;
+            hit[4 * j + 0] = lk.x != kNoChild && slab_nf(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, bnd, tn[4 * j + 0]);
+            hit[4 * j + 1] = lk.y != kNoChild && slab_nf(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, bnd, tn[4 * j + 1]);
+            hit[4 * j + 2] = lk.z != kNoChild && slab_nf(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, bnd, tn[4 * j + 2]);
+            hit[4 * j + 3] = lk.w != kNoChild && slab_nf(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, bnd, tn[4 * j + 3]);
+        }
+#pragma unroll
+        for (int c = 0; c < kBvhWidth; ++c) {
             if (!hit[c] || link[c] >= 0) continue;
             hit[c] = false;
             if (leaf(s, -1 - link[c], cnt[c])) return true;
@@ -278,7 +290,7 @@ struct Trav {
         // inner children still in front of the closest hit, nearest first
         const float cut = bound() * kSlabFarScale;
 #pragma unroll
-        for (int c = 0; c < 4; ++c)
+        for (int c = 0; c < kBvhWidth; ++c)
             if (!hit[c] || tn[c] > cut) tn[c] = INFINITY;
         auto cswap = [&](int i, int j) {
             if (tn[j] < tn[i]) {
@@ -290,28 +302,48 @@ struct Trav {
                 link[j] = l;
             }
         };
-        cswap(0, 1);
-        cswap(2, 3);
-        cswap(0, 2);
-        cswap(1, 3);
-        cswap(1, 2);
-        const int nh = (tn[0] < INFINITY) + (tn[1] < INFINITY) + (tn[2] < INFINITY) + (tn[3] < INFINITY);
+        if (kBvhWidth == 4) {
+            cswap(0, 1);
+            cswap(2, 3);
+            cswap(0, 2);
+            cswap(1, 3);
+            cswap(1, 2);
+        } else {
+            // Batcher's odd-even merge network for 8 keys (19 comparators)
+            cswap(0, 1);
+            cswap(2, 3);
+            cswap(4, 5);
+            cswap(6, 7);
+            cswap(0, 2);
+            cswap(1, 3);
+            cswap(4, 6);
+            cswap(5, 7);
+            cswap(1, 2);
+            cswap(5, 6);
+            cswap(0, 4);
+            cswap(1, 5);
+            cswap(2, 6);
+            cswap(3, 7);
+            cswap(2, 4);
+            cswap(3, 5);
+            cswap(1, 2);
+            cswap(3, 4);
+            cswap(5, 6);
+        }
+        int nh = 0;
+#pragma unroll
+        for (int c = 0; c < kBvhWidth; ++c) nh += tn[c] < INFINITY ? 1 : 0;
         if (nh > 0) {
             if (sp + nh - 1 > kTraversalStack) {
                 dev_error(s, kDevErrStack);
                 return true;
             }
-            if (nh > 3) {
-                st.node[sp] = link[3];
-                st.t[sp++] = tn[3];
-            }
-            if (nh > 2) {
-                st.node[sp] = link[2];
-                st.t[sp++] = tn[2];
-            }
-            if (nh > 1) {
-                st.node[sp] = link[1];
-                st.t[sp++] = tn[1];
+#pragma unroll
+            for (int j = kBvhWidth - 1; j >= 1; --j) {
+                if (j < nh) {
+                    st.node[sp] = link[j];
+                    st.t[sp++] = tn[j];
+                }
             }
             cur = link[0];
             return false;
