@@ -302,7 +302,33 @@ struct Trav {
                 link[j] = l;
             }
         };
-        if (kBvhWidth == 4) {
+        if (kAnyHit) {
+            // any hit ends the ray: the visiting order only moves work
+            // around, so the first child hit goes next and the rest are pushed
+            // as they come
+            int nh = 0;
+#pragma unroll
+            for (int c = 0; c < kBvhWidth; ++c) nh += tn[c] < INFINITY ? 1 : 0;
+            if (nh > 0) {
+                if (sp + nh - 1 > kTraversalStack) {
+                    dev_error(s, kDevErrStack);
+                    return true;
+                }
+                bool first = true;
+#pragma unroll
+                for (int c = 0; c < kBvhWidth; ++c) {
+                    if (!(tn[c] < INFINITY)) continue;
+                    if (first) {
+                        cur = link[c];
+                        first = false;
+                    } else {
+                        st.node[sp] = link[c];
+                        st.t[sp++] = tn[c];
+                    }
+                }
+                return false;
+            }
+        } else if (kBvhWidth == 4) {
             cswap(0, 1);
             cswap(2, 3);
             cswap(0, 2);
