@@ -679,7 +679,7 @@ struct crisb_renderer {
         record(0, st);
         launch_prefix_gen_temp_split(s, fp, bufs(), out, st, m);
         const uint32_t sj = shift_launches_per_phase();
-        launches += params.renderer_type == CRISB_RENDERER_PATH_TRACER ? 1 : 2 + sj + wf_launches_per_pass(fp);
+        launches += params.renderer_type == CRISB_RENDERER_PATH_TRACER ? 1 : 2 + sj + wf_launches_per_pass(fp, 0);
         record(1, st);
         const int type = params.renderer_type;
         if (type == CRISB_RENDERER_PATH_TRACER) {
@@ -698,7 +698,7 @@ struct crisb_renderer {
         record(2, st);
         if (type == CRISB_RENDERER_CONDITIONAL_RESTIR) {
             launch_suffix_gen_temp(s, fp, bufs(), st, m);
-            launches += 2 + sj + wf_launches_per_pass(fp);
+            launches += 2 + sj + wf_launches_per_pass(fp, 1);
             record(3, st);
             if (params.suffix_enable_spatial && params.suffix_spatial_count > 0) {
                 for (int r = 0; r < params.suffix_spatial_rounds; ++r) {
@@ -720,7 +720,7 @@ struct crisb_renderer {
             record(5, st);
             if (params.gather_n == 1) {
                 launch_final_gather_split(s, fp, bufs(), out, st, m);
-                launches += 3 + sj + wf_launches_per_pass(fp);
+                launches += 3 + sj + wf_launches_per_pass(fp, 2);
             } else {
                 launch_final_gather(s, fp, bufs(), out, st);
                 if (m) m->mark(kClsOther, st);

@@ -118,7 +118,8 @@ void launch_final_gather_split(const SceneView& s, const FrameParams& fp, const 
 void launch_wf_prefix(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m);
 void launch_wf_suffix(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m);
 void launch_wf_gather(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m);
-uint32_t wf_launches_per_pass(const FrameParams& fp);
+// kernels of one wavefront pass of `flow` (0 prefix, 1 suffix, 2 gather)
+uint32_t wf_launches_per_pass(const FrameParams& fp, int flow);
 // kernels of one shift-job phase (begin + rounds of closest / shadow / step)
 uint32_t shift_launches_per_phase();
 // prefix entries, endpoint bounds/count and Morton keys (w.keys_in); the

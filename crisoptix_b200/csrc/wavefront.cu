@@ -231,12 +231,18 @@ const WfGrids& wf_grids() {
 // still running in place.  Finishing in place from an earlier round (3 to 6)
 // saved traversal launches but cost as much in the in-place kernel on the
 // 1080p workload (24.2 ms/frame either way).
-int wf_round_count(const FrameParams& fp) { return fp.p.max_path_len + 2; }
+// (the ConditionalRestir prefix flow stops after prefix_len vertices: at most
+// prefix_len closest-hit rays and one shadow ray per path)
+int wf_round_count(const FrameParams& fp, int flow) {
+    if (flow == 0 && fp.p.renderer_type == CRISB_RENDERER_CONDITIONAL_RESTIR)
+        return std::min(fp.p.prefix_len + 2, fp.p.max_path_len + 2);
+    return fp.p.max_path_len + 2;
+}
 
 // rounds after the init kernel
 void wf_rounds(const SceneView& s, const FrameParams& fp, const Bufs& b, int flow, cudaStream_t st, Marker* m) {
     const WfGrids& g = wf_grids();
-    const int rounds = wf_round_count(fp);
+    const int rounds = wf_round_count(fp, flow);
     for (int r = 0; r < rounds; ++r) {
         const int cur = r & 1, nxt = cur ^ 1;
         k_q_trace<WfPath><<<g.trace * std::max(fp.trace_grid, 1u), kPassBlock, 0, st>>>(s, b.wf_queue[2 * cur], b.wf_count + 2 * cur,
@@ -254,7 +260,9 @@ void wf_rounds(const SceneView& s, const FrameParams& fp, const Bufs& b, int flo
 
 }  // namespace
 
-uint32_t wf_launches_per_pass(const FrameParams& fp) { return 1 + 2 * static_cast<uint32_t>(wf_round_count(fp)); }
+uint32_t wf_launches_per_pass(const FrameParams& fp, int flow) {
+    return 1 + 2 * static_cast<uint32_t>(wf_round_count(fp, flow));
+}
 
 void launch_wf_prefix(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m) {
     cudaMemsetAsync(b.wf_count, 0, 2 * sizeof(uint32_t), st);
