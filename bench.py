@@ -166,6 +166,34 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+def tonemap_timing(frame, W: int, H: int, stream, stack: int = 16, reps: int = 10) -> dict:
+    """crisb_tonemap_srgb8 on `stack` copies of the rendered frame (inputs
+    larger than L2), 12 bytes read and 3 written per pixel."""
+    import torch
+
+    from crisoptix_b200 import image
+
+    src = frame.view(1, H * W * 3).repeat(stack, 1).contiguous()
+    dst = torch.empty(src.shape, dtype=torch.uint8, device=src.device)
+    sptr = stream.cuda_stream
+    for _ in range(3):
+        image.tonemap(src.view(-1, 3), dst.view(-1, 3), sptr)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(reps):
+        image.tonemap(src.view(-1, 3), dst.view(-1, 3), sptr)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    px = stack * W * H
+    peak, kind = measured_peaks()
+    gbs = 15.0 * px / (ms / 1000.0) / 1e9
+    return {"kernel": "k_tonemap_srgb8", "pixels_per_launch": px, "frames_per_launch": stack,
+            "bytes_per_pixel": 15, "ms_per_launch": ms, "ms_per_frame": ms / stack, "achieved_gbs": gbs,
+            "frac": gbs / peak, "peak_kind": f"{kind} copy bandwidth"}
+
+
 def cpu_baseline(desc, cam, name: str, threads: int, frames: int, warm: int = 1, scale: int = 4):
     """The oracle (a host port of the reference's device code) on a bounded
     sample: the same scene and parameters at 1/scale of the resolution."""
@@ -309,6 +337,7 @@ def run_crisb(args):
     e_ms = sharding.max_over_ranks(e_start.elapsed_time(e_end), dist, "cuda")
     e2e_value = sharding.whole_job_rate(ppp * W * H, e_steps, world, e_ms)
     img_mean = float(host.mean())
+    tone = tonemap_timing(out, W, H, stream)
 
     # ---- roofline of the resampling kernels; traversal in rays/s -----------------
     peak, peak_kind = measured_peaks()
@@ -367,7 +396,7 @@ def run_crisb(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 48, "d2h_bytes_per_step": W * H * 12},
             "roofline": roofline, "traversal": traversal, "phases_ms": phases, "pass_ms": pass_ms,
             "cpu_baseline": cb, "clocks": clk,
-            "gpu_launches": launches_per_frame * args.steps, "image_mean": img_mean}
+            "gpu_launches": launches_per_frame * args.steps, "image_mean": img_mean, "tonemap": tone}
     if qual is not None:
         line["quality"] = qual
     print(json.dumps(line), flush=True)

@@ -185,6 +185,8 @@ ENTRY_POINTS = {
     "crisb_batch_create": (c_i32, [ctypes.POINTER(c_vp), c_u32, ctypes.POINTER(c_vp)]),
     "crisb_batch_destroy": (c_i32, [c_vp]),
     "crisb_batch_render": (c_i32, [c_vp, c_vp, ctypes.POINTER(c_vp), c_vp]),
+    "crisb_tonemap_srgb8": (c_i32, [c_vp, c_vp, c_u32, c_vp]),
+    "crisb_srgb8_thresholds": (c_i32, [c_vp, c_vp]),
     "crisb_set_trace_grid": (c_i32, [c_vp, c_u32]),
     "crisb_autotune": (c_i32, [c_vp, ctypes.POINTER(Camera), c_u32, ctypes.POINTER(c_u32)]),
     "crisb_set_graph": (c_i32, [c_vp, c_i32]),

@@ -1111,6 +1111,21 @@ int crisb_render_frame(crisb_renderer* r, const crisb_camera* cam, float* out_rg
     });
 }
 
+int crisb_tonemap_srgb8(const float* rgb_dev, uint8_t* srgb_dev, uint32_t num_pixels, void* stream) {
+    return guarded([&] {
+        if (num_pixels == 0) return;  // nothing is read or written
+        require(rgb_dev && srgb_dev, "null argument");
+        check(launch_tonemap_srgb8(rgb_dev, srgb_dev, num_pixels, static_cast<cudaStream_t>(stream)), "tonemap");
+    });
+}
+
+int crisb_srgb8_thresholds(float* thresholds, float* c_max) {
+    return guarded([&] {
+        require(thresholds && c_max, "null argument");
+        srgb8_thresholds(thresholds, c_max);
+    });
+}
+
 int crisb_set_trace_grid(crisb_renderer* r, uint32_t blocks_per_resident_block) {
     return guarded([&] {
         require(r != nullptr, "null renderer");

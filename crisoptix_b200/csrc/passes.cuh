@@ -134,6 +134,10 @@ void adjoint_forward(const SceneView& eval, const crisb_material* sample_mats, u
                      const FrameParams& fp, float* out, cudaStream_t st);
 void adjoint_backward(const SceneView& eval, const crisb_material* sample_mats, uint32_t num_mats,
                       const FrameParams& fp, const float* d_img, float* g_mat, float* g_em, cudaStream_t st);
+// sRGB tone mapping of n float RGB pixels to bytes (tonemap.cu)
+cudaError_t launch_tonemap_srgb8(const float* rgb, uint8_t* out, uint32_t n, cudaStream_t st);
+// the kernel's step table: t256[k] smallest float with byte >= k, and c_max
+void srgb8_thresholds(float* t256, float* c_max);
 // generic LBVH stages over `cap` primitives (count in w.n)
 void launch_lbvh_hierarchy(const lbvh::Work& w, uint32_t cap, int leaf_max, cudaStream_t st);
 

@@ -7,10 +7,12 @@
 // makes discrete decisions (hits, selections, neighbours) reproducible bit
 // for bit.  Transcendentals the reference takes from glm are replaced by
 // deterministic definitions: sin/cos via Cody-Waite reduction plus Taylor
-// polynomials, pow(x, 5) via repeated squaring.
+// polynomials, pow(x, 5) via repeated squaring, the sRGB curve's x^(1/2.4)
+// via double-precision series.
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 #include <cuda_runtime.h>
 
 #include "crisb.h"
@@ -87,6 +89,80 @@ RT_HD void sincos_reduced(float phi, float& s, float& c) {
     const int quadrant = static_cast<int>(q) & 3;
     s = quadrant == 0 ? sn : (quadrant == 1 ? cs : (quadrant == 2 ? -sn : -cs));
     c = quadrant == 0 ? cs : (quadrant == 1 ? -sn : (quadrant == 2 ? -cs : sn));
+}
+
+RT_HD uint64_t dbits(double x) {
+#ifdef __CUDA_ARCH__
+    return static_cast<uint64_t>(__double_as_longlong(x));
+#else
+    uint64_t b;
+    memcpy(&b, &x, sizeof b);
+    return b;
+#endif
+}
+RT_HD double dfrom(uint64_t b) {
+#ifdef __CUDA_ARCH__
+    return __longlong_as_double(static_cast<long long>(b));
+#else
+    double x;
+    memcpy(&x, &b, sizeof x);
+    return x;
+#endif
+}
+
+// x^(1/2.4) of the sRGB transfer curve for a float x, evaluated in double:
+// ln x = e ln 2 + 2 atanh((m - 1) / (m + 1)) with the mantissa m in
+// [sqrt(1/2), sqrt(2)) (series to s^19), then exp(ln x / 2.4) = 2^k e^r with
+// r in [0, ln 2) (Taylor series to r^17).  Relative error below 1e-14, so the
+// float result is the correctly rounded power except within 1e-14 of a
+// rounding midpoint.  NaN and negative x give NaN, +-0 gives 0, +inf gives
+// +inf, as pow does.
+RT_HD float srgb_root(float xf) {
+    if (isnan(xf) || xf < 0.0f) return static_cast<float>(dfrom(0x7ff8000000000000ULL));
+    if (xf == 0.0f) return 0.0f;
+    if (isinf(xf)) return xf;
+    const uint64_t b = dbits(static_cast<double>(xf));
+    int e = static_cast<int>((b >> 52) & 0x7ff) - 1023;
+    double m = dfrom((b & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL);
+    if (m > 1.4142135623730951) {
+        m = m * 0.5;
+        e = e + 1;
+    }
+    const double s = (m - 1.0) / (m + 1.0);
+    const double s2 = s * s;
+    double p = 1.0 / 19.0;
+    p = p * s2 + 1.0 / 17.0;
+    p = p * s2 + 1.0 / 15.0;
+    p = p * s2 + 1.0 / 13.0;
+    p = p * s2 + 1.0 / 11.0;
+    p = p * s2 + 1.0 / 9.0;
+    p = p * s2 + 1.0 / 7.0;
+    p = p * s2 + 1.0 / 5.0;
+    p = p * s2 + 1.0 / 3.0;
+    p = p * s2 + 1.0;
+    const double ln2 = 0.6931471805599453;
+    const double z = (static_cast<double>(e) * ln2 + 2.0 * s * p) / 2.4;
+    const double k = floor(z / ln2);
+    const double r = z - k * ln2;
+    double t = 1.0;
+    for (int i = 17; i >= 1; --i) t = 1.0 + r * t / static_cast<double>(i);
+    const double scale = dfrom(static_cast<uint64_t>(static_cast<int>(k) + 1023) << 52);
+    return static_cast<float>(t * scale);
+}
+
+// LinearToSrgb (src/kernel/tonemap.cu:7-21) for one channel, in the
+// reference's arithmetic: both branches of the curve evaluated and blended
+// by glm::lerp(if_false, if_true, cond) = if_false * (1 - cond) + if_true *
+// cond, glm's clamp (NaN passes through), times 255, truncated.  So negative
+// and NaN channels, +inf, and channels above FLT_MAX / 12.92 (where
+// 12.92 c overflows and inf * 0 is NaN) all give 0, as in the reference.
+RT_HD uint8_t srgb8(float c) {
+    const float cond = c < 0.0031308f ? 1.0f : 0.0f;
+    const float if_true = 12.92f * c;
+    const float if_false = 1.055f * srgb_root(c) - 0.055f;
+    const float g = if_false * (1.0f - cond) + if_true * cond;
+    const float v = gclamp(g, 0.0f, 1.0f) * 255.0f;
+    return isnan(v) ? uint8_t{0} : static_cast<uint8_t>(v);
 }
 
 // ---------------------------------------------------------------------------

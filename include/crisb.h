@@ -465,6 +465,21 @@ int crisb_batch_create(crisb_renderer* const* renderers, uint32_t n, crisb_batch
 int crisb_batch_destroy(crisb_batch* b);
 int crisb_batch_render(crisb_batch* b, const crisb_camera* cams, float* const* outs, void* stream);
 
+/* ToneMapping (src/kernel/tonemap.cu:7-39, called from src/main.cpp:127): the
+ * sRGB transfer curve per channel, clamped to [0, 1] and truncated to 8 bits,
+ * from num_pixels float RGB triples to num_pixels byte triples, both on the
+ * device, stream-ordered.  The reference then draws the bytes with OpenGL;
+ * here the caller keeps them (crisoptix_b200.image writes PNG files).
+ * num_pixels = 0 is a no-op (the pointers may then be null). */
+int crisb_tonemap_srgb8(const float* rgb_dev, uint8_t* srgb_dev, uint32_t num_pixels, void* stream);
+
+/* The step table crisb_tonemap_srgb8 searches (host memory, no GPU needed):
+ * thresholds[k] (k = 1..255) is the smallest float c >= 0 whose byte is at
+ * least k, thresholds[0] = 0; *c_max is the largest float with a finite
+ * 12.92 c.  A channel's byte is the count of k >= 1 with thresholds[k] <= c
+ * for 0 <= c <= c_max, and 0 otherwise (negative, NaN, larger). */
+int crisb_srgb8_thresholds(float* thresholds /* 256 */, float* c_max);
+
 /* Launch shape of the traversal kernels: blocks per block resident at once
  * (default 8; results do not depend on it).  crisb_autotune renders `frames`
  * frames of `cam` for each candidate (1, 2, 4, 8, 16) on a scratch renderer of

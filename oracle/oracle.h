@@ -62,6 +62,11 @@ uint64_t oracle_tea64(uint32_t v0, uint32_t v1);
 /* FP16 storage codecs (test hooks): binary16 bits and their value; octahedral
  * codes and their decoded unit vectors (dirs: n x 3 floats). */
 void oracle_half(const float* in, uint32_t n, uint16_t* bits, float* back);
+void oracle_srgb_root(const float* in, uint32_t n, float* out);
+int oracle_tonemap_srgb8(const float* rgb, uint8_t* out, uint32_t num_pixels);
+/* first float bit pattern b in (lo_bits, hi_bits] whose sRGB byte is below
+ * that of b - 1, or 0 when the bytes never decrease there */
+uint32_t oracle_srgb8_first_decrease(uint32_t lo_bits, uint32_t hi_bits);
 void oracle_oct(const float* dirs, uint32_t n, uint32_t* codes, float* decoded);
 void oracle_sincos(const float* phi, uint32_t n, float* s, float* c);
 int oracle_camera_data(const crisb_camera* cam, crisb_camera_data* out);

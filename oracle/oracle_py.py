@@ -57,6 +57,9 @@ def load():
         "oracle_tea64": (u64, [u32, u32]),
         "oracle_sincos": (None, [vp, u32, vp, vp]),
         "oracle_half": (None, [vp, u32, vp, vp]),
+        "oracle_srgb_root": (None, [vp, u32, vp]),
+        "oracle_tonemap_srgb8": (i32, [vp, vp, u32]),
+        "oracle_srgb8_first_decrease": (u32, [u32, u32]),
         "oracle_oct": (None, [vp, u32, vp, vp]),
         "oracle_camera_data": (i32, [ctypes.POINTER(_abi.Camera), ctypes.POINTER(_abi.CameraData)]),
         "oracle_frame_random_for": (u32, [u64, u64]),
@@ -195,6 +198,31 @@ def half(x: np.ndarray):
     back = np.zeros_like(x)
     load().oracle_half(_ptr(x), x.size, _ptr(bits), _ptr(back))
     return bits, back
+
+
+def srgb_root(x: np.ndarray) -> np.ndarray:
+    """x^(1/2.4) as the sRGB curve computes it (float in, float out)."""
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.zeros_like(x)
+    load().oracle_srgb_root(_ptr(x), x.size, _ptr(out))
+    return out
+
+
+def tonemap_srgb8(rgb: np.ndarray) -> np.ndarray:
+    """ToneMapping of (..., 3) linear float RGB to sRGB bytes."""
+    x = np.ascontiguousarray(rgb, np.float32)
+    assert x.shape[-1] == 3
+    out = np.zeros(x.shape, np.uint8)
+    assert load().oracle_tonemap_srgb8(_ptr(x), _ptr(out), x.size // 3) == 0
+    return out
+
+
+def srgb8_first_decrease(lo: float, hi: float) -> int:
+    """First float bit pattern in (lo, hi] whose byte is below its
+    predecessor's (0: the bytes never decrease on [lo, hi])."""
+    lo_b = int(np.float32(lo).view(np.uint32))
+    hi_b = int(np.float32(hi).view(np.uint32))
+    return int(load().oracle_srgb8_first_decrease(lo_b, hi_b))
 
 
 def oct(dirs: np.ndarray):

@@ -96,6 +96,47 @@ inline bool anyNanInf(vec3 v) {
            std::isinf(v.y) || std::isinf(v.z);
 }
 
+// DEFINED: x^(1/2.4) for the sRGB curve, in double.  ln x = e ln 2 +
+// 2 atanh(s), s = (m - 1) / (m + 1), mantissa m in [sqrt(1/2), sqrt(2))
+// (odd series to s^19); exp(ln x / 2.4) = 2^k e^r, r = z - k ln 2 (Taylor
+// series to r^17, Horner).  The reference calls glm::pow (powf); this stays
+// within 1e-14 relative of the exact power.
+inline float SrgbRoot(float xf) {
+    if (std::isnan(xf) || xf < 0.0f) return std::numeric_limits<float>::quiet_NaN();
+    if (xf == 0.0f) return 0.0f;
+    if (std::isinf(xf)) return xf;
+    int e = 0;
+    double m = 2.0 * std::frexp(static_cast<double>(xf), &e);  // [1, 2)
+    e -= 1;
+    if (m > 1.4142135623730951) {
+        m *= 0.5;
+        e += 1;
+    }
+    const double s = (m - 1.0) / (m + 1.0), s2 = s * s;
+    double p = 0.0;
+    for (int k = 19; k >= 1; k -= 2) p = (k == 19) ? 1.0 / 19.0 : p * s2 + 1.0 / k;
+    const double ln2 = 0.6931471805599453;
+    const double z = (static_cast<double>(e) * ln2 + 2.0 * s * p) / 2.4;
+    const double k = std::floor(z / ln2);
+    const double r = z - k * ln2;
+    double t = 1.0;
+    for (int i = 17; i >= 1; --i) t = 1.0 + r * t / static_cast<double>(i);
+    return static_cast<float>(t * std::ldexp(1.0, static_cast<int>(k)));
+}
+
+// LinearToSrgb / ApplySrgbGamma, src/kernel/tonemap.cu:7-21, one channel:
+// both branches, glm::lerp(if_false, if_true, cond) = if_false * (1 - cond) +
+// if_true * cond, glm::clamp (ternary min/max), * 255, truncation (NaN -> 0).
+inline uint8_t LinearToSrgb8(float c) {
+    const float cond = c < 0.0031308f ? 1.0f : 0.0f;
+    const float if_true = 12.92f * c;
+    const float if_false = 1.055f * SrgbRoot(c) - 0.055f;
+    const float g = if_false * (1.0f - cond) + if_true * cond;
+    const float lo = (g < 0.0f) ? 0.0f : g;
+    const float v = ((1.0f < lo) ? 1.0f : lo) * 255.0f;
+    return std::isnan(v) ? 0 : static_cast<uint8_t>(v);
+}
+
 // GetLuminance, include/graph/luminance.h:6-9
 inline float GetLuminance(vec3 c) { return dot(c, vec3(0.2126f, 0.7152f, 0.0722f)); }
 
@@ -2305,6 +2346,35 @@ void oracle_pcg32(uint64_t initstate, uint64_t initseq, uint32_t n, uint32_t* ou
 }
 
 uint64_t oracle_tea64(uint32_t v0, uint32_t v1) { return SampleTEA64(v0, v1); }
+
+void oracle_srgb_root(const float* in, uint32_t n, float* out) {
+    for (uint32_t i = 0; i < n; ++i) out[i] = SrgbRoot(in[i]);
+}
+
+uint32_t oracle_srgb8_first_decrease(uint32_t lo_bits, uint32_t hi_bits) {
+    uint32_t first = 0;
+#pragma omp parallel for schedule(static) reduction(min : first)
+    for (int64_t chunk = 0; chunk < (static_cast<int64_t>(hi_bits) - lo_bits + 65535) / 65536; ++chunk) {
+        const uint32_t b0 = lo_bits + static_cast<uint32_t>(chunk) * 65536u;
+        const uint32_t b1 = std::min<uint64_t>(static_cast<uint64_t>(b0) + 65536u, hi_bits);
+        float f;
+        memcpy(&f, &b0, sizeof f);
+        uint8_t prev = LinearToSrgb8(f);
+        for (uint32_t b = b0 + 1; b <= b1; ++b) {
+            memcpy(&f, &b, sizeof f);
+            const uint8_t cur = LinearToSrgb8(f);
+            if (cur < prev && (first == 0 || b < first)) first = b;
+            prev = cur;
+        }
+    }
+    return first;
+}
+
+int oracle_tonemap_srgb8(const float* rgb, uint8_t* out, uint32_t num_pixels) {
+    if ((!rgb || !out) && num_pixels) return CRISB_ERR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < 3 * num_pixels; ++i) out[i] = LinearToSrgb8(rgb[i]);
+    return CRISB_OK;
+}
 
 void oracle_half(const float* in, uint32_t n, uint16_t* bits, float* back) {
     for (uint32_t i = 0; i < n; ++i) {
