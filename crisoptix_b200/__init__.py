@@ -209,6 +209,14 @@ class Renderer:
         check(load().crisb_autotune(self.handle, ctypes.byref(camera_struct(camera)), int(frames), ctypes.byref(v)))
         return v.value
 
+    def set_motion_vectors(self, motion_dev_ptr: int):
+        """width * height float pairs on the device for MOTION_VECTORS (0 clears)."""
+        check(load().crisb_set_motion_vectors(self.handle, motion_dev_ptr or None))
+
+    def set_srgb_output(self, srgb_dev_ptr: int):
+        """Tone-map each frame into width * height * 3 device bytes (0 stops)."""
+        check(load().crisb_set_srgb_output(self.handle, srgb_dev_ptr or None))
+
     def set_graph(self, enable: bool):
         """Run frames as one CUDA graph of the pass chain (default) or launch
         the kernels directly; the results are identical."""

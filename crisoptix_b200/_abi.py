@@ -29,6 +29,9 @@ RADIUS_CONSTANT = 0
 RADIUS_PATH_LENGTH = 1
 STORAGE_FP32 = 0
 STORAGE_FP16 = 1
+MOTION_NONE = 0
+MOTION_VECTORS = 1
+MOTION_REPROJECT = 2
 INVALID_PRIM = 0xFFFFFFFF
 
 BUF_PREFIX_RES_FRONT = 0
@@ -82,7 +85,7 @@ class Params(ctypes.Structure):
                 ("prefix_spatial_rounds", c_i32), ("suffix_enable_temporal", c_i32), ("suffix_enable_spatial", c_i32),
                 ("suffix_spatial_count", c_i32), ("suffix_spatial_rounds", c_i32), ("gather_n", c_i32),
                 ("gather_m", c_i32), ("gather_radius", c_f), ("gather_radius_type", c_i32), ("window_radius", c_i32),
-                ("storage", c_i32), ("reserved", c_i32), ("seed", c_u64)]
+                ("storage", c_i32), ("motion_mode", c_i32), ("seed", c_u64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -187,6 +190,8 @@ ENTRY_POINTS = {
     "crisb_batch_render": (c_i32, [c_vp, c_vp, ctypes.POINTER(c_vp), c_vp]),
     "crisb_tonemap_srgb8": (c_i32, [c_vp, c_vp, c_u32, c_vp]),
     "crisb_srgb8_thresholds": (c_i32, [c_vp, c_vp]),
+    "crisb_set_srgb_output": (c_i32, [c_vp, c_vp]),
+    "crisb_set_motion_vectors": (c_i32, [c_vp, c_vp]),
     "crisb_set_trace_grid": (c_i32, [c_vp, c_u32]),
     "crisb_autotune": (c_i32, [c_vp, ctypes.POINTER(Camera), c_u32, ctypes.POINTER(c_u32)]),
     "crisb_set_graph": (c_i32, [c_vp, c_i32]),

@@ -415,6 +415,7 @@ void validate_params(const crisb_params& p) {
     require(p.window_radius >= 0 && p.window_radius < 32768, "params: window_radius");
     require(p.storage == CRISB_STORAGE_FP32 || p.storage == CRISB_STORAGE_FP16, "params: unknown storage");
     require(p.nee_prob >= 0.0f && p.nee_prob <= 1.0f, "params: nee_prob must be in [0, 1]");
+    require(p.motion_mode >= CRISB_MOTION_NONE && p.motion_mode <= CRISB_MOTION_REPROJECT, "params: motion_mode");
 }
 
 }  // namespace
@@ -600,6 +601,13 @@ struct crisb_renderer {
     // out the tail (8 measured best on the 1080p workload; crisb_autotune
     // picks it per workload)
     uint32_t trace_grid = 8;
+    // optional sRGB bytes of each frame (ToneMapping after LaunchFrame,
+    // src/main.cpp:122-127), written by a last kernel of the frame
+    uint8_t* srgb_out = nullptr;
+    // temporal reprojection: caller motion vectors, the previous frame's camera
+    const float2* motion = nullptr;
+    crisb_camera_data prev_cam{};
+    bool has_prev_cam = false;
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
 
@@ -667,6 +675,13 @@ struct crisb_renderer {
         fp.back = back;
         fp.k = K();
         fp.trace_grid = trace_grid;
+        require(params.motion_mode != CRISB_MOTION_VECTORS || motion != nullptr,
+                "render_frame: CRISB_MOTION_VECTORS without motion vectors");
+        fp.motion = motion;
+        fp.prev_cam = prev_cam;
+        fp.has_prev_cam = has_prev_cam ? 1u : 0u;
+        prev_cam = fp.cam;
+        has_prev_cam = true;
         SceneView s = scene->view(err.p);
         last_stream = st;
         ktimer.n = 0;
@@ -679,10 +694,13 @@ struct crisb_renderer {
         record(0, st);
         launch_prefix_gen_temp_split(s, fp, bufs(), out, st, m);
         const uint32_t sj = shift_launches_per_phase();
-        launches += params.renderer_type == CRISB_RENDERER_PATH_TRACER ? 1 : 2 + sj + wf_launches_per_pass(fp, 0);
+        launches += params.renderer_type == CRISB_RENDERER_PATH_TRACER
+                        ? 1
+                        : 2 + sj + wf_launches_per_pass(fp, 0) + prefix_pass_extra_launches(fp);
         record(1, st);
         const int type = params.renderer_type;
         if (type == CRISB_RENDERER_PATH_TRACER) {
+            tonemap_epilogue(out, st, m);
             for (int i = 2; i < 7; ++i) record(i, st);
             check(cudaGetLastError(), "launch");
             return;
@@ -698,6 +716,7 @@ struct crisb_renderer {
         record(2, st);
         if (type == CRISB_RENDERER_CONDITIONAL_RESTIR) {
             launch_suffix_gen_temp(s, fp, bufs(), st, m);
+            scur ^= 1;
             launches += 2 + sj + wf_launches_per_pass(fp, 1);
             record(3, st);
             if (params.suffix_enable_spatial && params.suffix_spatial_count > 0) {
@@ -731,8 +750,16 @@ struct crisb_renderer {
             record(4, st);
             record(5, st);
         }
+        tonemap_epilogue(out, st, m);
         record(6, st);
         check(cudaGetLastError(), "launch");
+    }
+
+    void tonemap_epilogue(const float* out, cudaStream_t st, Marker* m) {
+        if (!srgb_out) return;
+        check(launch_tonemap_srgb8(out, srgb_out, width * height, st), "tonemap");
+        if (m) m->mark(kClsOther, st);
+        ++launches;
     }
 };
 
@@ -1116,6 +1143,21 @@ int crisb_tonemap_srgb8(const float* rgb_dev, uint8_t* srgb_dev, uint32_t num_pi
         if (num_pixels == 0) return;  // nothing is read or written
         require(rgb_dev && srgb_dev, "null argument");
         check(launch_tonemap_srgb8(rgb_dev, srgb_dev, num_pixels, static_cast<cudaStream_t>(stream)), "tonemap");
+    });
+}
+
+int crisb_set_motion_vectors(crisb_renderer* r, const float* motion_dev) {
+    return guarded([&] {
+        require(r != nullptr, "null renderer");
+        require(reinterpret_cast<uintptr_t>(motion_dev) % alignof(float2) == 0, "motion vectors: 8-byte alignment");
+        r->motion = reinterpret_cast<const float2*>(motion_dev);
+    });
+}
+
+int crisb_set_srgb_output(crisb_renderer* r, uint8_t* srgb_dev) {
+    return guarded([&] {
+        require(r != nullptr, "null renderer");
+        r->srgb_out = srgb_dev;
     });
 }
 

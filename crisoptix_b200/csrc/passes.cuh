@@ -37,7 +37,8 @@ struct SresBuf {
 // Device buffers of one renderer.  Prefix reservoirs keep the reference's
 // front/back pair; suffix reservoirs live in two physical buffers where
 // `sres_cur` holds the state every logical copy front -> back has made equal
-// and spatial rounds write `sres_next` (then the roles swap).
+// and the temporal pass and each spatial round write `sres_next` (then the
+// roles swap), so every read sees the pass-start state.
 struct Bufs {
     PresBuf pres[2];
     crisb_prefix_rec* canon_prefix;
@@ -122,6 +123,8 @@ void launch_wf_gather(const SceneView& s, const FrameParams& fp, const Bufs& b, 
 uint32_t wf_launches_per_pass(const FrameParams& fp, int flow);
 // kernels of one shift-job phase (begin + rounds of closest / shadow / step)
 uint32_t shift_launches_per_phase();
+// kernels the prefix pass adds after its combine (the reprojection back copy)
+uint32_t prefix_pass_extra_launches(const FrameParams& fp);
 // prefix entries, endpoint bounds/count and Morton keys (w.keys_in); the
 // caller then sorts w.keys_in into w.keys and calls launch_knn_finish
 void launch_store_entries(const SceneView& s, const FrameParams& fp, const Bufs& b, const lbvh::Work& w,

@@ -96,23 +96,30 @@ struct ShiftSrc {
 RT_D ShiftSrc shift_src(const Suffix& S) { return ShiftSrc{S.rng, S.flags, S.last_prefix, S.recon, S.prf, S.rod}; }
 RT_D ShiftSrc shift_src(const Prefix& P) { return ShiftSrc{P.rng, P.flags, P.primary, P.recon, P.prf, P.rod}; }
 
+// the previous pixel of pixel i (its G-buffer entry; i itself without
+// reprojection); only called for pixels whose previous pixel exists
+RT_D uint32_t prev_pixel(const FrameParams& fp, const Bufs& b, uint32_t i) {
+    return fp.p.motion_mode == CRISB_MOTION_NONE ? i : prev_index(b.gbuf[i].prev_xy, fp.width);
+}
+
 // the job's source path and, when `dst` is given, its destination vertex
 RT_D ShiftSrc resolve_job(const FrameParams& fp, const Bufs& b, int mode, uint32_t code, Hit* dst) {
     const uint32_t i = code >> kSlotBits, slot = code & ((1u << kSlotBits) - 1), n = slot >> 1;
     if (mode == kModePrefix) {
         // slot 0: the previous prefix onto the canonical one; slot 1: back
+        const uint32_t pi = prev_pixel(fp, b, i);
         if (slot == 0) {
             if (dst) *dst = ld_hit(b.canon_prefix[i].primary);
-            return shift_src(ld_pres(b.pres[fp.back], i).s);
+            return shift_src(ld_pres(b.pres[fp.back], pi).s);
         }
-        if (dst) *dst = pres_primary(b.pres[fp.back], i);
+        if (dst) *dst = pres_primary(b.pres[fp.back], pi);
         return shift_src(ld_prefix(b.canon_prefix[i]));
     }
     const bool onto_own = (slot & 1u) == 0;
     SufRef own, other;
     if (mode == kModeTemporal) {
         own = SufRef{b.canon_suffix, b.sres_cur, i};  // canonical; "other" is the previous sample
-        other = SufRef{nullptr, b.sres_cur, i};
+        other = SufRef{nullptr, b.sres_cur, prev_pixel(fp, b, i)};
     } else if (mode == kModeSpatial) {
         own = SufRef{nullptr, b.sres_cur, i};
         other = SufRef{nullptr, b.sres_cur, b.spatial_nbr[static_cast<size_t>(i) * (b.slots >> 1) + n]};
@@ -296,15 +303,21 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_temp_finish(FrameParams f
         uint32_t st = kStFinal;
         if (b.pass_status[i] == kWfPath) {  // else the init kernel invalidated the reservoir
             b.gbuf[i].rng = b.wf[i].rng;
-            Res<Suffix> cur = ld_sres(b.sres_cur, i);
+            const uint32_t prev_xy = b.gbuf[i].prev_xy;
             if (!fl_valid(b.canon_suffix[i].sample.flags)) {
+                Res<Suffix> cur = ld_sres(b.sres_cur, i);
                 invalidate(cur);
-                st_sres(b.sres_cur, i, cur);
-            } else if (!fp.p.suffix_enable_temporal || cur.w_sum <= 0.0f || !fl_valid(cur.s.flags)) {
-                st = kStCanonOnly;  // prevPixelCoord == pixelCoord is always inside the image
+                st_sres(b.sres_next, i, cur);
+            } else if (!fp.p.suffix_enable_temporal || prev_xy == kPrevNone) {
+                st = kStCanonOnly;
             } else {
-                st = kStReuse;
-                mask = 3;
+                const uint32_t pi = prev_pixel(fp, b, i);
+                if (sres_wsum(b.sres_cur, pi) <= 0.0f || !fl_valid(sres_flags(b.sres_cur, pi))) {
+                    st = kStCanonOnly;
+                } else {
+                    st = kStReuse;
+                    mask = 3;
+                }
             }
         }
         b.pass_status[i] = st;
@@ -321,7 +334,9 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_temp_combine(FrameParams 
     const Suffix canon = ld_suffix(b.canon_suffix[i].sample);
     Rng rng{b.gbuf[i].rng};
     const float canon_phat = luminance(canon.f);
-    const Res<Suffix> prev = cur;  // back[prevPixelIdx] == front[i] content before the pass
+    // suffixReservoirs[back][prevPixelIdx]: the previous frame's reservoirs are
+    // the pass-start state sres_cur; this pass writes sres_next
+    const Res<Suffix> prev = st == kStReuse ? ld_sres(b.sres_cur, prev_pixel(fp, b, i)) : cur;
     cur.w_sum = 0.0f;
     cur.conf = 0.0f;
     if (st == kStCanonOnly) {
@@ -348,7 +363,7 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_temp_combine(FrameParams 
         }
     }
     b.gbuf[i].rng = rng.state;
-    st_sres(b.sres_cur, i, cur);
+    st_sres(b.sres_next, i, cur);
 }
 
 // ---- suffix spatial reuse (shader/suffix_spatial_reuse.cu:16-167) -----------------
@@ -565,14 +580,22 @@ __global__ void __launch_bounds__(kPassBlock) k_gather_combine(FrameParams fp, B
 
 
 // ---- prefix generation + temporal reuse (shader/prefix_gen_temp_reuse.cu) -----------
+// the pass leaves back = front (prefix_gen_temp_reuse.cu:159-164)
+RT_HD bool prefix_back_copy(const FrameParams& fp) {
+    const int type = fp.p.renderer_type;
+    return (type == CRISB_RENDERER_RESTIR_PT && fp.p.prefix_enable_spatial) ||
+           (type == CRISB_RENDERER_CONDITIONAL_RESTIR && fp.p.suffix_enable_spatial);
+}
+
 RT_D void prefix_tail(const FrameParams& fp, const Bufs& b, float* out, uint32_t i, const Res<Prefix>& cur,
                       bool valid) {
     const int type = fp.p.renderer_type;
     if (type == CRISB_RENDERER_RESTIR_PT && !fp.p.prefix_enable_spatial)
         store_output(fp, out, i, valid ? cur.w_sum * cur.s.f : splat(0.0f));
-    if ((type == CRISB_RENDERER_RESTIR_PT && fp.p.prefix_enable_spatial) ||
-        (type == CRISB_RENDERER_CONDITIONAL_RESTIR && fp.p.suffix_enable_spatial))
-        st_pres(b.pres[fp.back], i, cur);
+    // front -> back copy for the spatial passes; with reprojection other
+    // pixels still read back[prevPixelIdx] in this pass, so the copy runs as a
+    // kernel of its own after it (prefix_back_copy)
+    if (prefix_back_copy(fp) && fp.p.motion_mode == CRISB_MOTION_NONE) st_pres(b.pres[fp.back], i, cur);
 }
 
 // PathTracer mode: TraceCompletePath per pixel (prefix_gen_temp_reuse.cu:175-192)
@@ -588,21 +611,34 @@ __global__ void __launch_bounds__(kPassBlock) k_path_tracer(SceneView s, FramePa
 
 // per pixel after the canonical prefixes (wavefront.cu, prefix flow) finished:
 // the temporal-reuse decision, its shift jobs and the G-buffer
-__global__ void __launch_bounds__(kPassBlock) k_prefix_finish(FrameParams fp, Bufs b, float* out) {
+__global__ void __launch_bounds__(kPassBlock) k_prefix_finish(SceneView s, FrameParams fp, Bufs b, float* out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     uint64_t mask = 0;
     if (i < pixel_count(fp)) {
         const uint32_t x = i % fp.width, y = i / fp.width;
         const bool valid = fl_valid(b.canon_prefix[i].flags);
+        // prevPixelCoord (prefix_gen_temp_reuse.cu:130-136)
+        uint32_t prev_xy = x | (y << 16);
+        if (fp.p.motion_mode == CRISB_MOTION_VECTORS) {
+            const float2 mv = fp.motion[i];
+            prev_xy = prev_from_motion(x, y, mv.x, mv.y, fp.width, fp.height);
+        } else if (fp.p.motion_mode == CRISB_MOTION_REPROJECT) {
+            prev_xy = kPrevNone;
+            if (valid && fp.has_prev_cam) {
+                const Isect it = unpack(s, ld_hit(b.canon_prefix[i].primary));
+                if (it.valid) prev_xy = reproject(fp.prev_cam, it.pos, fp.width, fp.height);
+            }
+        }
         uint32_t st = kStFinal;
         if (!valid) {
             prefix_tail(fp, b, out, i, ld_pres(b.pres[fp.front], i), false);
-        } else if (!fp.p.prefix_enable_temporal) {
+        } else if (!fp.p.prefix_enable_temporal || prev_xy == kPrevNone) {
             st = kStCanonOnly;
         } else {
-            const uint32_t pf = pres_flags(b.pres[fp.back], i);
+            const uint32_t pi = fp.p.motion_mode == CRISB_MOTION_NONE ? i : prev_index(prev_xy, fp.width);
+            const uint32_t pf = pres_flags(b.pres[fp.back], pi);
             const bool skip_nee = fp.p.renderer_type == CRISB_RENDERER_CONDITIONAL_RESTIR && fl_nee(pf);
-            if (pres_wsum(b.pres[fp.back], i) <= 0.0f || !fl_valid(pf) || skip_nee) {
+            if (pres_wsum(b.pres[fp.back], pi) <= 0.0f || !fl_valid(pf) || skip_nee) {
                 st = kStCanonOnly;
             } else {
                 st = kStReuse;
@@ -611,7 +647,7 @@ __global__ void __launch_bounds__(kPassBlock) k_prefix_finish(FrameParams fp, Bu
         }
         crisb_gbuffer_rec g;
         g.rng = b.wf[i].rng;
-        g.prev_xy = x | (y << 16);
+        g.prev_xy = prev_xy;
         g.flags = valid ? 1u : 0u;
         b.gbuf[i] = g;
         b.pass_status[i] = st;
@@ -636,11 +672,12 @@ __global__ void __launch_bounds__(kPassBlock) k_prefix_combine(FrameParams fp, B
     cur.conf = 0.0f;
     int sel = 0;
     V3 f_canon_of_prev = splat(0.0f);
+    const uint32_t pi = prev_pixel(fp, b, i);
     if (st == kStCanonOnly) {
         if (res_choose(cur.w_sum, cur.conf, canon_phat / canon.p, rng, 1.0f)) sel = 1;
     } else {
-        const V3 prev_f = pres_f(b.pres[fp.back], i);
-        const float prev_conf = pres_conf(b.pres[fp.back], i), prev_wsum = pres_wsum(b.pres[fp.back], i);
+        const V3 prev_f = pres_f(b.pres[fp.back], pi);
+        const float prev_conf = pres_conf(b.pres[fp.back], pi), prev_wsum = pres_wsum(b.pres[fp.back], pi);
         const float4 o0 = b.shift_out[static_cast<size_t>(i) * b.slots];
         const float4 o1 = b.shift_out[static_cast<size_t>(i) * b.slots + 1];
         f_canon_of_prev = xyz(o0);
@@ -659,7 +696,7 @@ __global__ void __launch_bounds__(kPassBlock) k_prefix_combine(FrameParams fp, B
     } else if (sel == 1) {
         cur.s = canon;
     } else {
-        cur.s = ld_pres(b.pres[fp.back], i).s;  // PrefixPath(prev, f, canon.primaryInt)
+        cur.s = ld_pres(b.pres[fp.back], pi).s;  // PrefixPath(prev, f, canon.primaryInt)
         cur.s.f = f_canon_of_prev;
         cur.s.primary = canon.primary;
     }
@@ -731,11 +768,19 @@ void launch_prefix_gen_temp_split(const SceneView& s, const FrameParams& fp, con
     }
     launch_wf_prefix(s, fp, b, st, m);
     cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
-    k_prefix_finish<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, out);
+    k_prefix_finish<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b, out);
     MARK(kClsShade);
     run_shift_jobs(s, fp, b, kModePrefix, st, m);
     k_prefix_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, out);
     MARK(kClsResample);
+    if (prefix_back_copy(fp) && fp.p.motion_mode != CRISB_MOTION_NONE) {
+        launch_prefix_copy_front_back(fp, b, st);
+        MARK(kClsOther);
+    }
+}
+
+uint32_t prefix_pass_extra_launches(const FrameParams& fp) {
+    return prefix_back_copy(fp) && fp.p.motion_mode != CRISB_MOTION_NONE ? 1u : 0u;
 }
 
 void launch_suffix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m) {

@@ -21,7 +21,55 @@ struct FrameParams {
     int front, back;     // 0/1 buffer selection
     uint32_t k;          // gatherM - 1
     uint32_t trace_grid; // traversal launches: blocks per resident block (host side only)
+    const float2* motion = nullptr;  // CRISB_MOTION_VECTORS: per-pixel motion vectors
+    crisb_camera_data prev_cam{};    // CRISB_MOTION_REPROJECT: the previous frame's camera
+    uint32_t has_prev_cam = 0;
 };
+
+// ---- temporal reprojection (prevPixelCoord) ---------------------------------------
+// G-buffer prev_xy: x | y << 16, or kPrevNone when the pixel has no previous
+// pixel (IsPixelValid false); resolutions stay below 65535 so no valid pixel
+// packs to it.
+constexpr uint32_t kPrevNone = 0xffffffffu;
+
+RT_HD uint32_t pack_prev(uint32_t px, uint32_t py, uint32_t w, uint32_t h) {
+    return (px < w && py < h) ? (px | (py << 16)) : kPrevNone;
+}
+
+// glm::uvec2(vec2) as it compiles on the GPU (cvt.rzi.u32.f32): truncation
+// toward zero, saturating at 0 and 2^32 - 1, NaN to 0
+RT_HD uint32_t f2u_sat(float v) {
+    if (!(v > 0.0f)) return 0u;
+    if (v >= 4294967296.0f) return 0xffffffffu;
+    return static_cast<uint32_t>(v);
+}
+
+// prevPixelCoord = uvec2(vec2(pixelCoord) + vec2(0.5) + motionVector)
+// (prefix_gen_temp_reuse.cu:136, the commented-out form)
+RT_HD uint32_t prev_from_motion(uint32_t x, uint32_t y, float mx, float my, uint32_t w, uint32_t h) {
+    const float fx = (static_cast<float>(x) + 0.5f) + mx;
+    const float fy = (static_cast<float>(y) + 0.5f) + my;
+    return pack_prev(f2u_sat(fx), f2u_sat(fy), w, h);
+}
+
+// The pixel of camera `c` whose footprint holds world point p: the inverse of
+// camera_dir (d = U ux + V uy + W with U, V, W orthogonal), ux = 2 x / width -
+// 1 over the pixel's footprint [x, x + 1).  None behind the camera or off
+// screen.
+RT_HD uint32_t reproject(const crisb_camera_data& c, V3 p, uint32_t w, uint32_t h) {
+    const V3 U = ld3(c.u), V = ld3(c.v), W = ld3(c.w);
+    const V3 d = p - ld3(c.pos);
+    const float t = dot(d, W) / dot(W, W);
+    if (!(t > 0.0f)) return kPrevNone;
+    const float ux = dot(d, U) / (t * dot(U, U));
+    const float uy = dot(d, V) / (t * dot(V, V));
+    const float xc = (ux + 1.0f) * 0.5f * static_cast<float>(w);
+    const float yc = (uy + 1.0f) * 0.5f * static_cast<float>(h);
+    if (!(xc >= 0.0f && xc < static_cast<float>(w) && yc >= 0.0f && yc < static_cast<float>(h))) return kPrevNone;
+    return pack_prev(static_cast<uint32_t>(xc), static_cast<uint32_t>(yc), w, h);
+}
+
+RT_HD uint32_t prev_index(uint32_t prev_xy, uint32_t w) { return (prev_xy & 0xffffu) + (prev_xy >> 16) * w; }
 
 // ---- reservoir (include/graph/restir/Reservoir.h:28-50) ------------------------
 template <typename T>

@@ -139,6 +139,24 @@ typedef struct crisb_camera_data {
 } crisb_camera_data;
 
 /* ---- parameters (RestirParams + LaunchParams knobs) --------------------- */
+/* Temporal reprojection: where the temporal passes find a pixel's previous
+ * reservoirs (prevPixelCoord, shader/prefix_gen_temp_reuse.cu:130-136).
+ * NONE is the reference as it runs: prevPixelCoord = pixelCoord.  VECTORS is
+ * the reference's commented-out form, prevPixelCoord = uvec2(pixelCoord + 0.5
+ * + motionVectors[pixel]) with caller-supplied vectors
+ * (crisb_set_motion_vectors; LaunchParams::motionVectors,
+ * include/graph/LaunchParams.h:28), the float -> uint conversion saturating at
+ * 0 as on the GPU.  REPROJECT projects the pixel's primary hit through the
+ * previous frame's camera (Camera::GetData keeps prevW2V,
+ * src/Camera.cpp:22): the pixel whose footprint holds it, none when it is
+ * behind that camera or off screen.  In VECTORS and REPROJECT both temporal
+ * passes read the previous reservoirs at prevPixelCoord (the reference's
+ * prefix pass reads them at pixelCoord, prefix_gen_temp_reuse.cu:41-42,
+ * which is the same pixel only under NONE). */
+#define CRISB_MOTION_NONE 0
+#define CRISB_MOTION_VECTORS 1
+#define CRISB_MOTION_REPROJECT 2
+
 typedef struct crisb_params {
     int32_t renderer_type;
     float nee_prob;
@@ -161,7 +179,7 @@ typedef struct crisb_params {
     int32_t gather_radius_type;
     int32_t window_radius; /* WINDOW_RADIUS, include/graph/restir/path_gen.h:12 */
     int32_t storage;       /* CRISB_STORAGE_* */
-    int32_t reserved;
+    int32_t motion_mode;   /* CRISB_MOTION_* (temporal reprojection) */
     uint64_t seed;         /* replaces std::random_device (src/Renderer.cpp:9-11) */
 } crisb_params;
 
@@ -472,6 +490,17 @@ int crisb_batch_render(crisb_batch* b, const crisb_camera* cams, float* const* o
  * here the caller keeps them (crisoptix_b200.image writes PNG files).
  * num_pixels = 0 is a no-op (the pointers may then be null). */
 int crisb_tonemap_srgb8(const float* rgb_dev, uint8_t* srgb_dev, uint32_t num_pixels, void* stream);
+
+/* Per-pixel motion vectors for CRISB_MOTION_VECTORS: width * height float
+ * pairs on the device, read during each crisb_render_frame (NULL clears). */
+int crisb_set_motion_vectors(crisb_renderer* r, const float* motion_dev);
+
+/* Tone-map every frame of `r` into srgb_dev (width * height * 3 bytes on the
+ * device; NULL stops it): the same kernel as crisb_tonemap_srgb8, run as the
+ * last kernel of each crisb_render_frame / crisb_batch_render frame on the
+ * frame's stream (inside the frame's CUDA graph).  This is the reference's
+ * frame loop, LaunchFrame then ToneMapping (src/main.cpp:122-127). */
+int crisb_set_srgb_output(crisb_renderer* r, uint8_t* srgb_dev);
 
 /* The step table crisb_tonemap_srgb8 searches (host memory, no GPU needed):
  * thresholds[k] (k = 1..255) is the smallest float c >= 0 whose byte is at

@@ -39,6 +39,9 @@ int oracle_render_frame(oracle_ctx* ctx, const crisb_camera* cam, float* out_rgb
 /* Same, with per-pass wall times (ms) written to pass_ms[6]. */
 int oracle_render_frame_timed(oracle_ctx* ctx, const crisb_camera* cam,
                               float* out_rgb, double* pass_ms);
+/* CRISB_MOTION_VECTORS input: num_pixels (= width * height) float pairs on the
+ * host, copied; NULL clears */
+int oracle_set_motion_vectors(oracle_ctx* ctx, const float* motion, uint32_t num_pixels);
 uint64_t oracle_frame_index(const oracle_ctx* ctx);
 uint32_t oracle_frame_random(const oracle_ctx* ctx);
 /* Copy internal state in the crisb_*_rec layout (CRISB_BUF_* ids). */

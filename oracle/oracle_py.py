@@ -46,6 +46,7 @@ def load():
         "oracle_scene_size": (f32, [vp]),
         "oracle_render_frame": (i32, [vp, ctypes.POINTER(_abi.Camera), vp]),
         "oracle_render_frame_timed": (i32, [vp, ctypes.POINTER(_abi.Camera), vp, vp]),
+        "oracle_set_motion_vectors": (i32, [vp, vp, u32]),
         "oracle_frame_index": (u64, [vp]),
         "oracle_frame_random": (u32, [vp]),
         "oracle_dump": (i32, [vp, i32, vp, ctypes.c_size_t]),
@@ -134,6 +135,15 @@ class Oracle:
     def scene_size(self) -> float:
         return load().oracle_scene_size(self.h)
 
+    def set_motion_vectors(self, motion):
+        """(H, W, 2) float motion vectors for MOTION_VECTORS (None clears)."""
+        if motion is None:
+            assert load().oracle_set_motion_vectors(self.h, None, 0) == 0
+            return
+        m = np.ascontiguousarray(motion, np.float32)
+        assert m.size == 2 * self.width * self.height
+        assert load().oracle_set_motion_vectors(self.h, _ptr(m), self.width * self.height) == 0
+
     def render_frame(self, cam, out: np.ndarray, timed: bool = False):
         from crisoptix_b200 import camera_struct
         assert out.dtype == np.float32 and out.size == self.width * self.height * 3 and out.flags.c_contiguous
@@ -142,7 +152,8 @@ class Oracle:
             ms = np.zeros(6, np.float64)
             load().oracle_render_frame_timed(self.h, ctypes.byref(c), _ptr(out), _ptr(ms))
             return ms
-        load().oracle_render_frame(self.h, ctypes.byref(c), _ptr(out))
+        if load().oracle_render_frame(self.h, ctypes.byref(c), _ptr(out)) != 0:
+            raise ValueError("oracle rejected the frame (motion vectors missing?)")
         return None
 
     def frame_index(self) -> int:

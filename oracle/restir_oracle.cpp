@@ -946,6 +946,11 @@ struct oracle_ctx {
     uint32_t random = 0;
     int front = 0, back = 0;
     CameraData cam;
+    CameraData prevCam;       // this frame's previous camera (REPROJECT)
+    bool hasPrevCam = false;
+    CameraData lastCam;       // the last RenderFrame's camera
+    bool hasLastCam = false;
+    std::vector<float> motion;  // 2 per pixel (VECTORS)
 
     std::vector<Reservoir<PrefixPath>> prefixRes[2];
     std::vector<PrefixPath> canonPrefix;
@@ -1031,6 +1036,42 @@ struct oracle_ctx {
     }
 
     bool IsPixelValid(uint32_t x, uint32_t y) const { return x < width && y < height; }
+
+    // ---- prevPixelCoord, prefix_gen_temp_reuse.cu:130-136 -----------------
+    // DEFINED (CRISB_MOTION_*): NONE keeps pixelCoord; VECTORS is the
+    // commented-out uvec2(vec2(pixelCoord) + vec2(0.5) + motionVector) with
+    // the GPU's saturating float -> uint conversion; REPROJECT takes the
+    // pixel of the previous frame's camera whose footprint [x, x + 1) holds
+    // the primary hit.  No previous pixel is stored as (0xffff, 0xffff).
+    static constexpr uint32_t kNoPrev = 0xffffu;
+    static uint32_t ToUintSat(float v) {
+        if (!(v > 0.0f)) return 0u;
+        if (v >= 4294967296.0f) return 0xffffffffu;
+        return static_cast<uint32_t>(v);
+    }
+    void SetPrev(uint32_t px, uint32_t py, uint32_t& prevX, uint32_t& prevY) const {
+        const bool ok = IsPixelValid(px, py);
+        prevX = ok ? px : kNoPrev;
+        prevY = ok ? py : kNoPrev;
+    }
+    void PrevFromMotion(uint32_t x, uint32_t y, uint32_t& prevX, uint32_t& prevY) const {
+        const size_t i = static_cast<size_t>(y) * width + x;
+        const float fx = (static_cast<float>(x) + 0.5f) + motion[2 * i];
+        const float fy = (static_cast<float>(y) + 0.5f) + motion[2 * i + 1];
+        SetPrev(ToUintSat(fx), ToUintSat(fy), prevX, prevY);
+    }
+    void PrevFromReprojection(vec3 p, uint32_t& prevX, uint32_t& prevY) const {
+        prevX = prevY = kNoPrev;
+        const vec3 d = p - prevCam.pos;
+        const float t = dot(d, prevCam.W) / dot(prevCam.W, prevCam.W);
+        if (!(t > 0.0f)) return;
+        const float ux = dot(d, prevCam.U) / (t * dot(prevCam.U, prevCam.U));
+        const float uy = dot(d, prevCam.V) / (t * dot(prevCam.V, prevCam.V));
+        const float xc = (ux + 1.0f) * 0.5f * static_cast<float>(width);
+        const float yc = (uy + 1.0f) * 0.5f * static_cast<float>(height);
+        if (!(xc >= 0.0f && xc < static_cast<float>(width) && yc >= 0.0f && yc < static_cast<float>(height))) return;
+        SetPrev(static_cast<uint32_t>(xc), static_cast<uint32_t>(yc), prevX, prevY);
+    }
 
     // ---- path generation, include/graph/restir/path_gen.h -----------------
     // ComputeCanonicalPairwiseMISWeight, path_gen.h:15-31
@@ -1405,9 +1446,16 @@ struct oracle_ctx {
     }
 
     // PrefixGenTempReuse, shader/prefix_gen_temp_reuse.cu:11-98
-    bool PrefixGenTempReuse(size_t pixelIdx, uint32_t prevX, uint32_t prevY, vec3 origin, vec3 dir, PCG32& rng) {
+    bool PrefixGenTempReuse(size_t pixelIdx, uint32_t& prevX, uint32_t& prevY, vec3 origin, vec3 dir, PCG32& rng) {
         TracePrefix(canonPrefix[pixelIdx], origin, dir, rng);
         const PrefixPath& canon = canonPrefix[pixelIdx];
+        if (params.motion_mode == CRISB_MOTION_REPROJECT) {
+            prevX = prevY = kNoPrev;
+            if (canon.IsValid() && hasPrevCam) {
+                const Interaction it = Unpack(canon.primaryInt);
+                if (it.valid) PrevFromReprojection(it.pos, prevX, prevY);
+            }
+        }
         if (!canon.IsValid()) return false;
         const float canonPHat = GetLuminance(canon.f);
         Reservoir<PrefixPath>& currRes = prefixRes[front][pixelIdx];
@@ -1417,7 +1465,10 @@ struct oracle_ctx {
             currRes.FinalizeGRIS();
             return true;
         }
-        const Reservoir<PrefixPath>& prevRes = prefixRes[back][pixelIdx];
+        // the reference reads back[pixelIdx] (prefix_gen_temp_reuse.cu:42), the
+        // same pixel as prevPixelIdx under CRISB_MOTION_NONE
+        const size_t prevPixelIdx = static_cast<size_t>(prevY) * width + prevX;
+        const Reservoir<PrefixPath>& prevRes = prefixRes[back][prevPixelIdx];
         const PrefixPath& prevPrefix = prevRes.sample;
         const bool skipBecauseOfNee = params.renderer_type == CRISB_RENDERER_CONDITIONAL_RESTIR && prevPrefix.IsNee();
         if (prevRes.wSum <= 0.0f || !prevPrefix.IsValid() || skipBecauseOfNee) {
@@ -1459,7 +1510,8 @@ struct oracle_ctx {
             const vec3 origin = cam.pos;
             const int type = params.renderer_type;
             if (type == CRISB_RENDERER_CONDITIONAL_RESTIR || type == CRISB_RENDERER_RESTIR_PT) {
-                const uint32_t prevX = x, prevY = y;
+                uint32_t prevX = x, prevY = y;
+                if (params.motion_mode == CRISB_MOTION_VECTORS) PrevFromMotion(x, y, prevX, prevY);
                 const bool validPrimaryInt = PrefixGenTempReuse(pixelIdx, prevX, prevY, origin, dir, rng);
                 if (type == CRISB_RENDERER_RESTIR_PT && !params.prefix_enable_spatial) {
                     if (validPrimaryInt) {
@@ -1467,10 +1519,6 @@ struct oracle_ctx {
                         outputRadiance = r.wSum * r.sample.f;
                     }
                     StoreOutput(out, pixelIdx, outputRadiance);
-                }
-                if ((type == CRISB_RENDERER_RESTIR_PT && params.prefix_enable_spatial) ||
-                    (type == CRISB_RENDERER_CONDITIONAL_RESTIR && params.suffix_enable_spatial)) {
-                    prefixRes[back][pixelIdx] = prefixRes[front][pixelIdx];
                 }
                 GBuffer& g = gbuf[pixelIdx];
                 g.rng = rng;
@@ -1482,6 +1530,15 @@ struct oracle_ctx {
                 if (anyNanInf(outputRadiance)) outputRadiance = vec3(0.0f);
                 StoreOutput(out, pixelIdx, outputRadiance);
             }
+        }
+        // Copy front to back reservoir for spatial reuse
+        // (prefix_gen_temp_reuse.cu:159-164), after every pixel's temporal
+        // reuse: other pixels read back[prevPixelIdx] during the pass
+        const int type = params.renderer_type;
+        if ((type == CRISB_RENDERER_RESTIR_PT && params.prefix_enable_spatial) ||
+            (type == CRISB_RENDERER_CONDITIONAL_RESTIR && params.suffix_enable_spatial)) {
+#pragma omp parallel for schedule(static)
+            for (int64_t pi = 0; pi < P; ++pi) prefixRes[back][pi] = prefixRes[front][pi];
         }
     }
 
@@ -1623,10 +1680,11 @@ struct oracle_ctx {
     void PassSuffixGenTempReuse() {
         const int64_t P = static_cast<int64_t>(width) * height;
 #pragma omp parallel for schedule(dynamic, 64)
-        for (int64_t pi = 0; pi < P; ++pi) {
-            SuffixGenTempReuse(static_cast<size_t>(pi));
-            suffixRes[back][pi] = suffixRes[front][pi];
-        }
+        for (int64_t pi = 0; pi < P; ++pi) SuffixGenTempReuse(static_cast<size_t>(pi));
+        // "Swap buffers" (suffix_gen_temp_reuse.cu:129-133) after every pixel:
+        // other pixels read back[prevPixelIdx] during the pass
+#pragma omp parallel for schedule(static)
+        for (int64_t pi = 0; pi < P; ++pi) suffixRes[back][pi] = suffixRes[front][pi];
     }
 
     // SuffixSpatialReuse, shader/suffix_spatial_reuse.cu:16-145 (neighbours
@@ -1957,6 +2015,10 @@ struct oracle_ctx {
         random = FrameRandom(params.seed, frameCounter);
         ++frameCounter;
         cam = GetCameraData(c);
+        prevCam = lastCam;
+        hasPrevCam = hasLastCam;
+        lastCam = cam;
+        hasLastCam = true;
         if (front == 0) {
             front = 1;
             back = 0;
@@ -2142,7 +2204,7 @@ int oracle_set_params(oracle_ctx* ctx, const crisb_params* p) {
     if (p->prefix_spatial_count < 0 || p->prefix_spatial_count > CRISB_MAX_SPATIAL_NEIGH ||
         p->suffix_spatial_count < 0 || p->suffix_spatial_count > CRISB_MAX_SPATIAL_NEIGH || p->gather_m < 1 ||
         p->gather_m > CRISB_MAX_GATHER_M || p->gather_n < 1 || p->max_path_len < 1 || p->prefix_len < 1 ||
-        p->window_radius < 0)
+        p->window_radius < 0 || p->motion_mode < CRISB_MOTION_NONE || p->motion_mode > CRISB_MOTION_REPROJECT)
         return CRISB_ERR_INVALID_ARGUMENT;
     const uint32_t oldK = ctx->K();
     ctx->params = *p;
@@ -2159,15 +2221,33 @@ int oracle_set_threads(int n) {
 
 float oracle_scene_size(const oracle_ctx* ctx) { return ctx ? ctx->scene.sceneSize : 0.0f; }
 
+namespace {
+bool MotionReady(const oracle_ctx* ctx) {
+    return ctx->params.motion_mode != CRISB_MOTION_VECTORS ||
+           ctx->motion.size() == 2 * static_cast<size_t>(ctx->width) * ctx->height;
+}
+}  // namespace
+
 int oracle_render_frame(oracle_ctx* ctx, const crisb_camera* cam, float* out_rgb) {
-    if (!ctx || !cam || !out_rgb) return CRISB_ERR_INVALID_ARGUMENT;
+    if (!ctx || !cam || !out_rgb || !MotionReady(ctx)) return CRISB_ERR_INVALID_ARGUMENT;
     ctx->RenderFrame(*cam, out_rgb, nullptr);
     return CRISB_OK;
 }
 
 int oracle_render_frame_timed(oracle_ctx* ctx, const crisb_camera* cam, float* out_rgb, double* pass_ms) {
-    if (!ctx || !cam || !out_rgb) return CRISB_ERR_INVALID_ARGUMENT;
+    if (!ctx || !cam || !out_rgb || !MotionReady(ctx)) return CRISB_ERR_INVALID_ARGUMENT;
     ctx->RenderFrame(*cam, out_rgb, pass_ms);
+    return CRISB_OK;
+}
+
+int oracle_set_motion_vectors(oracle_ctx* ctx, const float* motion, uint32_t num_pixels) {
+    if (!ctx) return CRISB_ERR_INVALID_ARGUMENT;
+    if (!motion) {
+        ctx->motion.clear();
+        return CRISB_OK;
+    }
+    if (num_pixels != ctx->width * ctx->height) return CRISB_ERR_INVALID_ARGUMENT;
+    ctx->motion.assign(motion, motion + 2 * static_cast<size_t>(num_pixels));
     return CRISB_OK;
 }
 

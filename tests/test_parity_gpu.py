@@ -53,12 +53,17 @@ def test_flattened_instances_match_float64_reference(cuda_device):
     assert (mat == rm).all()
 
 
-def run_parity(desc, cam, params, W, H, frames, cam_fn, change_params=None, timing=0, graph=lambda f: True):
+def run_parity(desc, cam, params, W, H, frames, cam_fn, change_params=None, timing=0, graph=lambda f: True,
+               motion=None):
     sc = Scene(desc)
     tri = sc.read_triangles()
     o = op.Oracle.from_scene(desc, W, H, params, triangles=tri)
     r = Renderer(W, H, sc, params)
     r.set_timing(timing)
+    if motion is not None:  # (H, W, 2) motion vectors for MOTION_VECTORS
+        mv_d = torch.from_numpy(np.ascontiguousarray(motion, np.float32)).cuda()
+        r.set_motion_vectors(mv_d.data_ptr())
+        o.set_motion_vectors(motion)
     out_d = torch.zeros(H * W * 3, dtype=torch.float32, device="cuda")
     out_h = np.zeros((H, W, 3), np.float32)
     for f in range(frames):

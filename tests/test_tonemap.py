@@ -238,3 +238,41 @@ def test_tonemap_rendered_frame(cuda_device, tmp_path):
     assert (srgb == op.tonemap_srgb8(hdr.cpu().numpy())).all()
     assert (image.decode_png(open(p, "rb").read()) == srgb[::-1]).all()
     assert srgb.mean() > 20
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("graph", [True, False])
+@pytest.mark.parametrize("rtype", [_abi.CONDITIONAL_RESTIR, _abi.RESTIR_PT, _abi.PATH_TRACER])
+def test_frame_srgb_output(cuda_device, graph, rtype):
+    """The frame loop with the sRGB epilogue (LaunchFrame then ToneMapping):
+    float frame and bytes both bit-exact with the oracle, every frame, in and
+    out of the frame graph; turning the output off stops the writes."""
+    import torch
+
+    from crisoptix_b200 import Renderer, Scene, scenes
+    from helpers import scene_size_of, small_config_params
+
+    desc, cam = scenes.cornell_box()
+    W, H = 48, 40
+    p = small_config_params(scene_size_of(desc), renderer_type=rtype)
+    sc = Scene(desc)
+    o = op.Oracle.from_scene(desc, W, H, p, triangles=sc.read_triangles())
+    r = Renderer(W, H, sc, p)
+    r.set_graph(graph)
+    hdr = torch.zeros(H * W * 3, dtype=torch.float32, device="cuda")
+    srgb = torch.zeros(H * W * 3, dtype=torch.uint8, device="cuda")
+    r.set_srgb_output(srgb.data_ptr())
+    out_h = np.zeros((H, W, 3), np.float32)
+    for _ in range(3):
+        r.launch_frame(cam, hdr.data_ptr())
+        o.render_frame(cam, out_h)
+        torch.cuda.synchronize()
+        r.check_device_errors()
+        assert hdr.cpu().numpy().tobytes() == out_h.tobytes()
+        assert (srgb.cpu().numpy() == op.tonemap_srgb8(out_h).ravel()).all()
+    assert int(srgb.sum()) > 0
+    r.set_srgb_output(0)
+    srgb.zero_()
+    r.launch_frame(cam, hdr.data_ptr())
+    torch.cuda.synchronize()
+    assert int(srgb.sum()) == 0
