@@ -75,7 +75,8 @@ def config_for(name: str, W: int, H: int, n_tris: int, p, ppp: int, world: int, 
     """The `config` object of both arms' JSON lines."""
     return {"workload": f"{name}: {W}x{H} conditional ReSTIR PT, {n_tris} triangles, k={p.gather_m - 1}, "
                         f"{p.suffix_spatial_rounds}x{p.suffix_spatial_count} spatial, max depth {p.max_path_len}, "
-                        f"{'FP16' if p.storage == 1 else 'FP32'} storage",
+                        f"{'FP16' if p.storage == 1 else 'FP32'} storage"
+                        + (", reprojected temporal reuse" if p.motion_mode == 2 else ""),
             "paths_per_pixel": ppp, "l2": "working set (reservoirs, BVH) larger than L2",
             "parallelism": f"view-sharded replicas x{world}", "frame_as_cuda_graph": graph}
 
@@ -264,6 +265,7 @@ def run_crisb(args):
     sc = Scene(desc)
     p = params_for(args.workload, sc.scene_size)
     p.storage = _abi.STORAGE_FP16 if args.storage == "fp16" else _abi.STORAGE_FP32
+    p.motion_mode = _abi.MOTION_REPROJECT if args.motion == "reproject" else _abi.MOTION_NONE
     r = Renderer(W, H, sc, p)
     r.set_graph(not args.no_graph)
     tuned = r.autotune(cam, 3) if args.autotune else None
@@ -380,9 +382,12 @@ def run_crisb(args):
         cam_of = lambda f: scenes.orbit_camera(cam, f, 60)  # noqa: E731
         ref = quality.reference_image(sc, W, H, cam_of(30), p, args.relmse)
         qual = {"reference_spp": args.relmse, "frame": 30}
-        for name, storage in (("fp32", _abi.STORAGE_FP32), ("fp16", _abi.STORAGE_FP16)):
+        for name, storage, motion in (("fp32", _abi.STORAGE_FP32, _abi.MOTION_NONE),
+                                      ("fp16", _abi.STORAGE_FP16, _abi.MOTION_NONE),
+                                      ("fp32_reproject", _abi.STORAGE_FP32, _abi.MOTION_REPROJECT)):
             q = copy.copy(p)
             q.storage = storage
+            q.motion_mode = motion
             qual[name] = quality.score(sc, W, H, cam_of, q, 31, args.relmse, ref=ref)
     cb = None
     if not args.no_cpu_baseline and world == 1:
@@ -417,6 +422,7 @@ def run_multiview(args):
     p = params_for("large", sc.scene_size)
     p.seed = 2
     p.storage = _abi.STORAGE_FP16 if args.storage == "fp16" else _abi.STORAGE_FP32
+    p.motion_mode = _abi.MOTION_REPROJECT if args.motion == "reproject" else _abi.MOTION_NONE
     views = scenes.multiview_cameras(seed=2)
     rs = [Renderer(w, h, sc, p) for _, w, h in views]
     outs = [torch.zeros(w * h * 3, dtype=torch.float32, device="cuda") for _, w, h in views]
@@ -496,6 +502,8 @@ def main():
                          "SPP-sample FP64-accumulated path-traced reference")
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"],
                     help="reservoir storage between passes and frames (fp16: packed binary16 / octahedral records)")
+    ap.add_argument("--motion", default="none", choices=["none", "reproject"],
+                    help="temporal reprojection of the previous reservoirs (off in the reference)")
     ap.add_argument("--autotune", action="store_true", help="pick the traversal launch shape by timing candidates")
     ap.add_argument("--no-graph", action="store_true", help="launch kernels directly instead of one CUDA graph per frame")
     ap.add_argument("--cpu-scale", type=int, default=2)

@@ -4,10 +4,11 @@ files on the host.
 The reference tone-maps the HDR frame into an OpenGL pixel buffer and draws
 it (src/main.cpp:110-135, src/kernel/tonemap.cu:23-39).  Here the same
 tone-mapping kernel writes a device byte buffer, which the caller keeps or
-writes to a file.  Row 0 of a frame buffer is the BOTTOM row of the image
-(the camera maps launch row 0 to -V, and OpenGL's texture origin is the
-bottom-left corner), so the PNG writer emits rows last to first, and the PFM
-writer, whose format is bottom-up, emits them in order.
+writes to a file.  Row 0 of a frame buffer is the TOP row of the image: launch
+row 0 maps to uv.y = -1, and the camera's V axis points down (Camera::GetData
+negates the up vector, src/Camera.cpp:28), so that ray looks up.  The PNG
+writer emits rows in order; the PFM writer, whose format stores the bottom row
+first, emits them last to first.
 """
 import struct
 import zlib
@@ -41,7 +42,7 @@ def _chunk(kind: bytes, data: bytes) -> bytes:
     return struct.pack(">I", len(data)) + body + struct.pack(">I", zlib.crc32(body) & 0xFFFFFFFF)
 
 
-def encode_png(srgb8: np.ndarray, bottom_up: bool = True) -> bytes:
+def encode_png(srgb8: np.ndarray, bottom_up: bool = False) -> bytes:
     """8-bit RGB PNG of an (H, W, 3) uint8 array (filter 0 on every row)."""
     a = np.ascontiguousarray(srgb8)
     if a.dtype != np.uint8 or a.ndim != 3 or a.shape[2] != 3:
@@ -80,34 +81,34 @@ def decode_png(data: bytes) -> np.ndarray:
     return raw[:, 1:].reshape(h, w, 3).copy()
 
 
-def write_png(path: str, srgb8: np.ndarray, bottom_up: bool = True) -> None:
+def write_png(path: str, srgb8: np.ndarray, bottom_up: bool = False) -> None:
     """Write an (H, W, 3) uint8 frame as PNG; `bottom_up` says row 0 is the
-    bottom of the image (the frame buffer convention)."""
+    bottom of the image (frame buffers have it at the top)."""
     with open(path, "wb") as f:
         f.write(encode_png(srgb8, bottom_up))
 
 
 def write_pfm(path: str, rgb: np.ndarray) -> None:
-    """Write an (H, W, 3) float frame as a little-endian PFM (rows bottom to
-    top, which is the frame buffer's own order)."""
+    """Write an (H, W, 3) float frame (row 0 the top) as a little-endian PFM,
+    which stores rows bottom to top."""
     a = np.ascontiguousarray(rgb, dtype="<f4")
     if a.ndim != 3 or a.shape[2] != 3:
         raise ValueError("expected an (H, W, 3) array")
     h, w, _ = a.shape
     with open(path, "wb") as f:
         f.write(f"PF\n{w} {h}\n-1.0\n".encode("ascii"))
-        f.write(a.tobytes())
+        f.write(np.ascontiguousarray(a[::-1]).tobytes())
 
 
 def read_pfm(path: str) -> np.ndarray:
-    """(H, W, 3) float32 array of a colour PFM file, row 0 the bottom row."""
+    """(H, W, 3) float32 array of a colour PFM file, row 0 the top row."""
     with open(path, "rb") as f:
         if f.readline().strip() != b"PF":
             raise ValueError("not a colour PFM file")
         w, h = (int(v) for v in f.readline().split())
         scale = float(f.readline())
         a = np.frombuffer(f.read(w * h * 12), "<f4" if scale < 0 else ">f4")
-    return a.reshape(h, w, 3).astype(np.float32)
+    return np.ascontiguousarray(a.reshape(h, w, 3)[::-1]).astype(np.float32)
 
 
 def save_frame(path: str, hdr, stream: int = 0) -> np.ndarray:

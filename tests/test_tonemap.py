@@ -105,8 +105,8 @@ def test_png_round_trip_and_orientation(tmp_path):
     data = open(p, "rb").read()
     assert data[:8] == b"\x89PNG\r\n\x1a\n" and data[12:16] == b"IHDR"
     back = image.decode_png(data)
-    assert (back == a[::-1]).all()  # row 0 of the frame is the bottom of the file
-    assert (image.decode_png(image.encode_png(a, bottom_up=False)) == a).all()
+    assert (back == a).all()  # row 0 of a frame is the top row of the file
+    assert (image.decode_png(image.encode_png(a, bottom_up=True)) == a[::-1]).all()
     with pytest.raises(ValueError):
         image.encode_png(a.astype(np.float32))
 
@@ -118,6 +118,8 @@ def test_pfm_round_trip(tmp_path):
     assert open(p, "rb").read(3) == b"PF\n"
     assert os.path.getsize(p) == len(b"PF\n24 17\n-1.0\n") + a.nbytes
     assert (image.read_pfm(p) == a).all()
+    raw = np.frombuffer(open(p, "rb").read()[len(b"PF\n24 17\n-1.0\n"):], "<f4").reshape(17, 24, 3)
+    assert (raw[0] == a[-1]).all()  # PFM stores the bottom row first
 
 
 def _thresholds():
@@ -236,7 +238,7 @@ def test_tonemap_rendered_frame(cuda_device, tmp_path):
     p = str(tmp_path / "frame.png")
     srgb = image.save_frame(p, hdr)
     assert (srgb == op.tonemap_srgb8(hdr.cpu().numpy())).all()
-    assert (image.decode_png(open(p, "rb").read()) == srgb[::-1]).all()
+    assert (image.decode_png(open(p, "rb").read()) == srgb).all()
     assert srgb.mean() > 20
 
 
