@@ -108,6 +108,23 @@ class Scene:
         d.num_emitters = len(desc.emitters)
         d.emitter_faces = arr(desc.emitter_faces, np.float32)
         d.num_emitter_faces = len(desc.emitter_faces)
+        if desc.material_textures is not None:
+            mt = np.ascontiguousarray(desc.material_textures, np.int32)
+            if mt.shape != (len(desc.materials), 3):
+                raise ValueError("material_textures must be (num_materials, 3)")
+            d.material_textures = arr(mt, np.int32)
+            if desc.uvs is not None:
+                d.uvs = arr(desc.uvs, np.float32)
+            tex = (_abi.Texture * max(len(desc.textures), 1))()
+            for i, t in enumerate(desc.textures):
+                t = np.ascontiguousarray(t, np.uint8)
+                if t.ndim != 3 or t.shape[2] != 4:
+                    raise ValueError("textures must be (H, W, 4) uint8")
+                tex[i].rgba = arr(t, np.uint8)
+                tex[i].height, tex[i].width = int(t.shape[0]), int(t.shape[1])
+            self._keep.append(tex)
+            d.textures = ctypes.cast(tex, ctypes.c_void_p)
+            d.num_textures = len(desc.textures)
         h = ctypes.c_void_p()
         check(lib.crisb_scene_create(ctypes.byref(d), ctypes.byref(h)))
         self.handle = h

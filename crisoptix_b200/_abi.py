@@ -29,6 +29,8 @@ RADIUS_CONSTANT = 0
 RADIUS_PATH_LENGTH = 1
 STORAGE_FP32 = 0
 STORAGE_FP16 = 1
+SPEC_COLOR = 0
+SPEC_OCC_ROUGH_METAL = 1
 MOTION_NONE = 0
 MOTION_VECTORS = 1
 MOTION_REPROJECT = 2
@@ -66,7 +68,12 @@ class SceneDesc(ctypes.Structure):
     _fields_ = [("positions", c_vp), ("normals", c_vp), ("num_vertices", c_u32), ("indices", c_vp),
                 ("triangle_material", c_vp), ("num_triangles", c_u32), ("materials", c_vp), ("num_materials", c_u32),
                 ("meshes", c_vp), ("num_meshes", c_u32), ("instances", c_vp), ("num_instances", c_u32),
-                ("emitters", c_vp), ("num_emitters", c_u32), ("emitter_faces", c_vp), ("num_emitter_faces", c_u32)]
+                ("emitters", c_vp), ("num_emitters", c_u32), ("emitter_faces", c_vp), ("num_emitter_faces", c_u32),
+                ("uvs", c_vp), ("textures", c_vp), ("num_textures", c_u32), ("material_textures", c_vp)]
+
+
+class Texture(ctypes.Structure):
+    _fields_ = [("rgba", c_vp), ("width", c_u32), ("height", c_u32)]
 
 
 class Camera(ctypes.Structure):

@@ -219,6 +219,7 @@ struct crisb_scene {
     float scene_size = 0.0f;
     std::vector<float> h_pos, h_nrm;
     std::vector<uint32_t> h_mat;
+    std::vector<float> h_uv;  // 6 per triangle when the scene has uvs
     DevBuf<Bvh4Node> nodes;
     int bvh_max_stack = 0, bvh_max_depth = 0;
     DevBuf<float4> tris;
@@ -227,6 +228,11 @@ struct crisb_scene {
     DevBuf<crisb_emitter> emitters;
     DevBuf<float> emitter_faces;
     uint32_t num_emitters = 0;
+    DevBuf<float2> uvs;
+    DevBuf<int4> mat_tex;
+    DevBuf<uint32_t> texels;
+    DevBuf<uint4> tex_info;
+    bool textured = false;
     DevBuf<int> err;
 
     SceneView view(int* err_word) const {
@@ -242,6 +248,12 @@ struct crisb_scene {
         v.err = err_word;
         v.ray_count = nullptr;
         v.trav_count = nullptr;
+        if (textured) {
+            v.uvs = uvs.p;
+            v.mat_tex = mat_tex.p;
+            v.texels = texels.p;
+            v.tex_info = tex_info.p;
+        }
         return v;
     }
 };
@@ -318,6 +330,12 @@ void flatten(const crisb_scene_desc& d, crisb_scene& s) {
             s.h_pos.insert(s.h_pos.end(), p, p + 9);
             s.h_nrm.insert(s.h_nrm.end(), n, n + 9);
             s.h_mat.push_back(override_mat >= 0 ? static_cast<uint32_t>(override_mat) : d.triangle_material[t]);
+            if (d.uvs)
+                for (int c = 0; c < 3; ++c) {
+                    const float* uv = d.uvs + 2 * static_cast<size_t>(d.indices[3 * t + c]);
+                    s.h_uv.push_back(uv[0]);
+                    s.h_uv.push_back(uv[1]);
+                }
         }
     };
     if (d.num_instances == 0) {
@@ -347,6 +365,48 @@ void flatten(const crisb_scene_desc& d, crisb_scene& s) {
     s.scene_size = distance(V3{lo[0], lo[1], lo[2]}, V3{hi[0], hi[1], hi[2]});
 }
 
+// Textures, their per-material assignment and the corner uvs (only when a
+// material uses a texture).  Texels are packed RGBA8 words, one texture after
+// the other.
+void upload_textures(const crisb_scene_desc& d, crisb_scene& s) {
+    if (!d.material_textures) return;
+    std::vector<int4> mt(d.num_materials);
+    bool any = false;
+    for (uint32_t m = 0; m < d.num_materials; ++m) {
+        int t[3];
+        for (int k = 0; k < 3; ++k) {
+            t[k] = d.material_textures[3 * m + k];
+            require(t[k] >= -1 && t[k] < static_cast<int64_t>(d.num_textures), "scene: texture index out of range");
+            any = any || t[k] >= 0;
+        }
+        mt[m] = make_int4(t[0], t[1], t[2], -1);
+    }
+    if (!any) return;
+    require(d.uvs != nullptr, "scene: textured materials need uvs");
+    require(d.textures != nullptr, "scene: null texture array");
+    std::vector<uint4> info(d.num_textures);
+    size_t words = 0;
+    for (uint32_t t = 0; t < d.num_textures; ++t) {
+        const crisb_texture& tx = d.textures[t];
+        require(tx.rgba && tx.width > 0 && tx.height > 0 && tx.width < 65536 && tx.height < 65536,
+                "scene: bad texture");
+        require(words + static_cast<size_t>(tx.width) * tx.height < 0xffffffffu, "scene: textures too large");
+        info[t] = make_uint4(static_cast<uint32_t>(words), tx.width, tx.height, 0);
+        words += static_cast<size_t>(tx.width) * tx.height;
+    }
+    std::vector<uint32_t> texels(std::max<size_t>(words, 1));
+    for (uint32_t t = 0; t < d.num_textures; ++t)
+        std::memcpy(texels.data() + info[t].x, d.textures[t].rgba,
+                    4 * static_cast<size_t>(d.textures[t].width) * d.textures[t].height);
+    std::vector<float2> uv(3 * static_cast<size_t>(std::max<uint32_t>(s.num_tris, 1)), make_float2(0, 0));
+    for (size_t k = 0; k < 3 * static_cast<size_t>(s.num_tris); ++k) uv[k] = make_float2(s.h_uv[2 * k], s.h_uv[2 * k + 1]);
+    s.uvs.upload(uv.data(), uv.size());
+    s.mat_tex.upload(mt.data(), mt.size());
+    s.texels.upload(texels.data(), texels.size());
+    s.tex_info.upload(info.data(), info.size());
+    s.textured = true;
+}
+
 void build_scene(const crisb_scene_desc& d, crisb_scene& s) {
     check(cudaGetDevice(&s.device), "cudaGetDevice");
     flatten(d, s);
@@ -369,6 +429,7 @@ void build_scene(const crisb_scene_desc& d, crisb_scene& s) {
     s.emitters.upload(d.emitters, d.num_emitters);
     s.emitter_faces.upload(d.emitter_faces, 9 * static_cast<size_t>(d.num_emitter_faces));
     s.num_emitters = d.num_emitters;
+    upload_textures(d, s);
     s.err.alloc(1);
     check(cudaMemset(s.err.p, 0, sizeof(int)), "memset");
     // 4-wide SAH BVH built on the host; triangles stored in leaf order
@@ -1049,6 +1110,7 @@ int crisb_adjoint_create(crisb_scene* scene, uint32_t width, uint32_t height, co
         validate_params(*params);
         require(params->max_path_len <= 16, "adjoint: max_path_len must be <= 16");
         require(scene->num_emitters > 0, "adjoint: the scene has no emitters");
+        require(!scene->textured, "adjoint: textured materials are not differentiated");
         auto a = std::make_unique<crisb_adjoint>();
         a->scene = scene;
         a->width = width;

@@ -139,12 +139,13 @@ RT_D void job_out(const Bufs& b, uint32_t code, float4 v) {
 // Runs the job from vertex `cur` with `left` replays to go: queues its next
 // ray (returned request) or, when `inline_rays`, traces the remaining rays in
 // place; a finished job writes its result.
+template <bool kTex>
 RT_D int shift_advance(const SceneView& s, const Bufs& b, bool prefix, const ShiftSrc& src, ShiftJob& j, Isect cur,
                        Rng& srng, V3 tp, uint32_t left, bool inline_rays) {
     const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     while (left > 0) {
         srng.next_float();
-        const BrdfSample bs = brdf_sample(s, cur, srng);
+        const BrdfSample bs = brdf_sample<kTex>(s, cur, srng);
         if (bs.pdf <= 0.0f) {
             job_out(b, j.code, zero);
             return kReqDone;
@@ -176,7 +177,7 @@ RT_D int shift_advance(const SceneView& s, const Bufs& b, bool prefix, const Shi
         job_out(b, j.code, zero);
         return kReqDone;
     }
-    const BrdfEval b1 = brdf_eval(s, cur, rdir);
+    const BrdfEval b1 = brdf_eval<kTex>(s, cur, rdir);
     float4 res = zero;
     if (b1.pdf > 0.0f) {
         tp = tp * b1.brdf;
@@ -185,7 +186,7 @@ RT_D int shift_advance(const SceneView& s, const Bufs& b, bool prefix, const Shi
             src_recon.dir = rdir;
             if (!prefix && is_zero(src.rod)) ok = false;
             if (ok) {
-                const BrdfEval b2 = brdf_eval(s, src_recon, src.rod);
+                const BrdfEval b2 = brdf_eval<kTex>(s, src_recon, src.rod);
                 if (b2.pdf <= 0.0f) ok = false;
                 else tp = tp * b2.brdf;
             }
@@ -217,6 +218,8 @@ RT_D void job_push(const Bufs& b, int round, int req, uint32_t t) {
 
 // first step of every job of the list: the checks of the reference function,
 // then the first ray
+// kTex: the scene has textured materials
+template <bool kTex>
 __global__ void __launch_bounds__(kPassBlock) k_shift_begin(SceneView s, FrameParams fp, Bufs b, int mode) {
     const uint32_t total = *b.job_count;
     count_jobs(s, total);
@@ -240,7 +243,7 @@ __global__ void __launch_bounds__(kPassBlock) k_shift_begin(SceneView s, FramePa
                 const int skip = prefix ? 2 : 1;
                 const uint32_t left = static_cast<uint32_t>(max(static_cast<int>(fl_recon(src.flags)) - skip, 0));
                 Rng srng{src.rng};
-                req = shift_advance(s, b, prefix, src, j, cur, srng, splat(1.0f), left, false);
+                req = shift_advance<kTex>(s, b, prefix, src, j, cur, srng, splat(1.0f), left, false);
                 if (req != kReqDone) b.jobs[t] = j;
             }
         }
@@ -250,7 +253,7 @@ __global__ void __launch_bounds__(kPassBlock) k_shift_begin(SceneView s, FramePa
 
 // resume every job whose ray of round `cur` finished; in the last round jobs
 // with replays left finish inline
-template <bool kLast>
+template <bool kLast, bool kTex>
 __global__ void __launch_bounds__(kPassBlock) k_shift_step(SceneView s, FrameParams fp, Bufs b, int mode, int cur) {
     const uint32_t nc = b.job_qcount[2 * cur], ns = b.job_qcount[2 * cur + 1];
     const uint32_t total = nc + ns;
@@ -284,7 +287,7 @@ __global__ void __launch_bounds__(kPassBlock) k_shift_step(SceneView s, FramePar
                     it.nrm = normalize(interp(it.bu, it.bv, tri.n0, tri.n1, tri.n2));
                     const ShiftSrc src = resolve_job(fp, b, mode, j.code, nullptr);
                     Rng srng{j.rng};
-                    req = shift_advance(s, b, prefix, src, j, it, srng, f3(j.acc), j.ctr, kLast);
+                    req = shift_advance<kTex>(s, b, prefix, src, j, it, srng, f3(j.acc), j.ctr, kLast);
                     if (req != kReqDone) b.jobs[t] = j;
                 }
             }
@@ -712,18 +715,23 @@ __global__ void __launch_bounds__(kPassBlock) k_prefix_combine(FrameParams fp, B
 }
 
 struct ShiftGrids {
-    unsigned begin, step, step_last, trace;
+    unsigned begin, step, step_last;
 };
 
+template <bool kTex>
 const ShiftGrids& shift_grids() {
     static std::once_flag once;
     static ShiftGrids g{};
     std::call_once(once, [] {
-        g.begin = persistent_grid(reinterpret_cast<const void*>(k_shift_begin));
-        g.step = persistent_grid(reinterpret_cast<const void*>(k_shift_step<false>));
-        g.step_last = persistent_grid(reinterpret_cast<const void*>(k_shift_step<true>));
-        g.trace = persistent_grid(reinterpret_cast<const void*>(k_q_trace<ShiftJob>));
+        g.begin = persistent_grid(reinterpret_cast<const void*>(k_shift_begin<kTex>));
+        g.step = persistent_grid(reinterpret_cast<const void*>(k_shift_step<false, kTex>));
+        g.step_last = persistent_grid(reinterpret_cast<const void*>(k_shift_step<true, kTex>));
     });
+    return g;
+}
+
+unsigned shift_trace_grid() {
+    static const unsigned g = persistent_grid(reinterpret_cast<const void*>(k_q_trace<ShiftJob>));
     return g;
 }
 
@@ -733,26 +741,38 @@ const ShiftGrids& shift_grids() {
     } while (0)
 
 // the shift jobs of the list: begin, then rounds of trace / step
-void run_shift_jobs(const SceneView& s0, const FrameParams& fp, const Bufs& b, int mode, cudaStream_t st, Marker* m) {
-    const ShiftGrids& g = shift_grids();
-    const SceneView s = shift_view(s0);
+template <bool kTex>
+void run_shift_jobs_as(const SceneView& s, const FrameParams& fp, const Bufs& b, int mode, cudaStream_t st,
+                       Marker* m) {
+    const ShiftGrids& g = shift_grids<kTex>();
     cudaMemsetAsync(b.job_qcount, 0, 2 * sizeof(uint32_t), st);
-    k_shift_begin<<<g.begin, kPassBlock, 0, st>>>(s, fp, b, mode);
+    k_shift_begin<kTex><<<g.begin, kPassBlock, 0, st>>>(s, fp, b, mode);
     MARK(kClsShift);
     for (int r = 0; r < kShiftRounds; ++r) {
         const int cur = r & 1, nxt = cur ^ 1;
-        k_q_trace<ShiftJob><<<g.trace * std::max(fp.trace_grid, 1u), kPassBlock, 0, st>>>(s, b.job_queue[2 * cur], b.job_qcount + 2 * cur,
-                                                            b.job_queue[2 * cur + 1], b.job_qcount + 2 * cur + 1,
-                                                            b.jobs);
+        k_q_trace<ShiftJob><<<shift_trace_grid() * std::max(fp.trace_grid, 1u), kPassBlock, 0, st>>>(
+            s, b.job_queue[2 * cur], b.job_qcount + 2 * cur, b.job_queue[2 * cur + 1], b.job_qcount + 2 * cur + 1,
+            b.jobs);
         MARK(kClsTrace);
         if (r + 1 < kShiftRounds) {
             cudaMemsetAsync(b.job_qcount + 2 * nxt, 0, 2 * sizeof(uint32_t), st);
-            k_shift_step<false><<<g.step, kPassBlock, 0, st>>>(s, fp, b, mode, cur);
+            k_shift_step<false, kTex><<<g.step, kPassBlock, 0, st>>>(s, fp, b, mode, cur);
         } else {
-            k_shift_step<true><<<g.step_last, kPassBlock, 0, st>>>(s, fp, b, mode, cur);
+            k_shift_step<true, kTex><<<g.step_last, kPassBlock, 0, st>>>(s, fp, b, mode, cur);
         }
         MARK(kClsShift);
     }
+}
+
+// the shift kernels come in two builds: with the texture lookup, for scenes
+// with textured materials, and without it (20 registers fewer, 7 instead of
+// 5 resident blocks per SM)
+void run_shift_jobs(const SceneView& s0, const FrameParams& fp, const Bufs& b, int mode, cudaStream_t st, Marker* m) {
+    const SceneView s = shift_view(s0);
+    if (s.mat_tex)
+        run_shift_jobs_as<true>(s, fp, b, mode, st, m);
+    else
+        run_shift_jobs_as<false>(s, fp, b, mode, st, m);
 }
 
 }  // namespace

@@ -51,6 +51,13 @@ struct SceneView {
     // their rays land in [2, 3] and their job count in [4]
     unsigned long long* ray_count;
     unsigned long long* trav_count;  // [node visits, triangle tests] or null
+    // textures (null without): per-triangle corner uvs in scene order, per
+    // material (diffuse, specular, roughness, -) texture or -1, texel words
+    // (RGBA8, first row first) and per texture (first word, width, height, -)
+    const float2* uvs = nullptr;
+    const int4* mat_tex = nullptr;
+    const uint32_t* texels = nullptr;
+    const uint4* tex_info = nullptr;
 };
 
 struct RayPre {
@@ -504,11 +511,81 @@ struct MatVals {
     float rough;
 };
 
-RT_D MatVals mat_vals(const crisb_material& m) {
+// tex2D<float4> of the reference's texture objects (src/Texture.cpp:44-72:
+// normalised coordinates, cudaAddressModeWrap, cudaFilterModeLinear,
+// cudaReadModeNormalizedFloat on uchar4 texels), DEFINED in software after the
+// CUDA programming guide's linear-filtering formula: the coordinate's
+// fraction scaled to texels, x_B = x - 0.5, i = floor(x_B), alpha = frac(x_B)
+// held with 8 fractional bits (rounded here), neighbours i and i + 1 wrapped,
+// result = (1-a)(1-b) T[i,j] + a(1-b) T[i+1,j] + (1-a) b T[i,j+1] + a b
+// T[i+1,j+1] in that order, texel channels c / 255.  Non-finite
+// coordinates read as 0.
+RT_HD float tex_frac_weight(float a) { return floorf(a * 256.0f + 0.5f) * (1.0f / 256.0f); }
+
+RT_D float4 texel_rgba(uint32_t w) {
+    return make_float4(static_cast<float>(w & 0xffu) / 255.0f, static_cast<float>((w >> 8) & 0xffu) / 255.0f,
+                       static_cast<float>((w >> 16) & 0xffu) / 255.0f, static_cast<float>(w >> 24) / 255.0f);
+}
+
+RT_D float4 tex_sample(const uint32_t* texels, const uint4* tex_info, int tex, float u, float v) {
+    const uint4 info = tex_info[tex];
+    const int W = static_cast<int>(info.y), H = static_cast<int>(info.z);
+    if (!(u - u == 0.0f)) u = 0.0f;  // NaN or infinite
+    if (!(v - v == 0.0f)) v = 0.0f;
+    const float x = (u - floorf(u)) * static_cast<float>(W) - 0.5f;
+    const float y = (v - floorf(v)) * static_cast<float>(H) - 0.5f;
+    const float xf = floorf(x), yf = floorf(y);
+    const float a = tex_frac_weight(x - xf), b = tex_frac_weight(y - yf);
+    int i0 = static_cast<int>(xf) % W, j0 = static_cast<int>(yf) % H;
+    if (i0 < 0) i0 += W;
+    if (j0 < 0) j0 += H;
+    const int i1 = i0 + 1 == W ? 0 : i0 + 1, j1 = j0 + 1 == H ? 0 : j0 + 1;
+    const uint32_t* t = texels + info.x;
+    // ((w00 T00 + w10 T10) + w01 T01) + w11 T11, one texel live at a time
+    float4 acc;
+    auto add = [&](uint32_t word, float w, bool first) {
+        const float4 c = texel_rgba(word);
+        acc = first ? make_float4(w * c.x, w * c.y, w * c.z, w * c.w)
+                    : make_float4(acc.x + w * c.x, acc.y + w * c.y, acc.z + w * c.z, acc.w + w * c.w);
+    };
+    add(__ldg(t + static_cast<size_t>(j0) * W + i0), (1.0f - a) * (1.0f - b), true);
+    add(__ldg(t + static_cast<size_t>(j0) * W + i1), a * (1.0f - b), false);
+    add(__ldg(t + static_cast<size_t>(j1) * W + i0), (1.0f - a) * b, false);
+    add(__ldg(t + static_cast<size_t>(j1) * W + i1), a * b, false);
+    return acc;
+}
+
+struct TexVals {
+    V3 diff, f0;
+    float rough;
+};
+
+// GetFromTexIfPossible for a textured material (mt: diffuse, specular,
+// roughness texture or -1) at uv = InterpolateBary of the corner uvs
+// (include/graph/Interaction.h:171).  Inlined: a non-inlined form raised
+// the shading kernel from 128 to 156 registers (the call's saved registers).
+RT_D TexVals textured_vals(const float2* uvs, const uint32_t* texels, const uint4* tex_info,
+                                              int4 mt, uint32_t prim, float bu, float bv, TexVals v) {
+    const float2 a = uvs[3 * static_cast<size_t>(prim)], b = uvs[3 * static_cast<size_t>(prim) + 1],
+                 c = uvs[3 * static_cast<size_t>(prim) + 2];
+    const float w = 1.0f - bu - bv;
+    const float u = (w * a.x + bu * b.x) + bv * c.x, t = (w * a.y + bu * b.y) + bv * c.y;
+    if (mt.x >= 0) {
+        const float4 q = tex_sample(texels, tex_info, mt.x, u, t);
+        v.diff = V3{q.x, q.y, q.z};
+    }
+    if (mt.y >= 0) {
+        const float4 q = tex_sample(texels, tex_info, mt.y, u, t);
+        v.f0 = V3{q.x, q.y, q.z};
+    }
+    if (mt.z >= 0) v.rough = tex_sample(texels, tex_info, mt.z, u, t).x;
+    return v;
+}
+
+// the metal workflow and mix of shader/brdf.cu:129-138 over looked-up values
+RT_D MatVals finish_mat(const crisb_material& m, V3 diff, V3 f0, float rough) {
     MatVals v;
-    v.diff = V3{m.diffuse[0], m.diffuse[1], m.diffuse[2]};
-    V3 f0 = V3{m.specular[0], m.specular[1], m.specular[2]};
-    float rough = m.roughness;
+    v.diff = diff;
     float metal = 0.0f;
     if (m.spec_usage == CRISB_SPEC_OCC_ROUGH_METAL) {
         rough = f0.y;
@@ -519,6 +596,30 @@ RT_D MatVals mat_vals(const crisb_material& m) {
     v.emission = V3{m.emission[0], m.emission[1], m.emission[2]};
     v.rough = rough;
     return v;
+}
+
+// material values at an interaction: GetFromTexIfPossible for the diffuse
+// colour, specF0 and roughness (shader/brdf.cu:64-97,120-138)
+// kTex = false compiles the texture lookup out (kernels instantiated for
+// untextured scenes keep their register budget).
+template <bool kTex = true>
+RT_D MatVals mat_vals(const SceneView& s, const Isect& it) {
+    const uint32_t mi = material_of(s, it.prim);
+    const crisb_material& m = s.mats[mi];
+    TexVals v{V3{m.diffuse[0], m.diffuse[1], m.diffuse[2]}, V3{m.specular[0], m.specular[1], m.specular[2]},
+              m.roughness};
+    if (kTex && s.mat_tex) {
+        const int4 mt = s.mat_tex[mi];
+        if (mt.x >= 0 || mt.y >= 0 || mt.z >= 0)
+            v = textured_vals(s.uvs, s.texels, s.tex_info, mt, it.prim, it.bu, it.bv, v);
+    }
+    return finish_mat(m, v.diff, v.f0, v.rough);
+}
+
+// the material without its textures (constant values)
+RT_D MatVals mat_vals(const crisb_material& m) {
+    return finish_mat(m, V3{m.diffuse[0], m.diffuse[1], m.diffuse[2]}, V3{m.specular[0], m.specular[1], m.specular[2]},
+                      m.roughness);
 }
 
 RT_D float pow5(float x) {
@@ -561,13 +662,14 @@ RT_D void brdf_value(const MatVals& m, V3 nrm, V3 view, V3 light, float ndotl, f
 }
 
 // __direct_callable__ggx_eval, shader/brdf.cu:115-190
+template <bool kTex = true>
 RT_D BrdfEval brdf_eval(const SceneView& s, const Isect& it, V3 out_dir) {
     BrdfEval r;
     r.brdf = splat(0.0f);
     r.pdf = 0.0f;
     r.emission = splat(0.0f);
     r.roughness = 0.0f;
-    const MatVals m = mat_vals(s.mats[material_of(s, it.prim)]);
+    const MatVals m = mat_vals<kTex>(s, it);
     const V3 view = -it.dir;
     const float ndotv = dot(it.nrm, view);
     const float ndotl = dot(it.nrm, out_dir);
@@ -592,8 +694,9 @@ RT_D V3 local_to_world(V3 z, V3 v) {
 }
 
 // __direct_callable__ggx_sample, shader/brdf.cu:214-337
+template <bool kTex = true>
 RT_D BrdfSample brdf_sample(const SceneView& s, const Isect& it, Rng& rng) {
-    const MatVals m = mat_vals(s.mats[material_of(s, it.prim)]);
+    const MatVals m = mat_vals<kTex>(s, it);
     BrdfSample r;
     r.roughness = m.rough;
     r.dir = splat(0.0f);

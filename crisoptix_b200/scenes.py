@@ -25,7 +25,7 @@ from __future__ import annotations
 
 import dataclasses
 import math
-from typing import List, Tuple
+from typing import Optional, List, Tuple
 
 import numpy as np
 
@@ -77,6 +77,24 @@ class Scene:
     emitters: list
     emitter_faces: np.ndarray
     name: str = "scene"
+    # textured materials: (V, 2) vertex uvs, (H, W, 4) uint8 RGBA textures
+    # (first row first) and (M, 3) int32 diffuse / specular / roughness
+    # texture per material (-1: the material's constant)
+    uvs: Optional[np.ndarray] = None
+    textures: list = dataclasses.field(default_factory=list)
+    material_textures: Optional[np.ndarray] = None
+
+    @property
+    def textured(self) -> bool:
+        return self.material_textures is not None and bool((np.asarray(self.material_textures) >= 0).any())
+
+    def flatten_uvs(self) -> np.ndarray:
+        """(T, 6) corner uvs of the world-space triangles, in flatten() order."""
+        UV = np.asarray(self.uvs, np.float32)[self.indices].reshape(-1, 6)
+        if not self.instances:
+            return UV.copy()
+        return np.concatenate([UV[int(self.meshes[m][0]):int(self.meshes[m][0]) + int(self.meshes[m][1])]
+                               for m, _, _ in self.instances]).astype(np.float32)
 
     @property
     def num_world_triangles(self) -> int:
@@ -197,6 +215,53 @@ def cornell_box() -> Tuple[Scene, Camera]:
                   [((17.0, 12.0, 4.0), 0, 2)], faces.astype(np.float32), name="cornell")
     cam = Camera((0.0, 0.5, 1.35), (0.0, 0.0, -1.0), (0.0, 1.0, 0.0), 1.0, math.radians(60.0))
     return scene, cam
+
+
+def _checker(h: int, w: int, a, b, cell: int = 1) -> np.ndarray:
+    yy, xx = np.mgrid[0:h, 0:w]
+    on = ((yy // cell + xx // cell) % 2 == 0)[..., None]
+    return np.where(on, np.asarray(a, np.uint8), np.asarray(b, np.uint8)).astype(np.uint8)
+
+
+def textured_cornell_box() -> Tuple[Scene, Camera]:
+    """The Cornell box with textured materials: a checkered diffuse floor and
+    back wall (8 x 8 texels, uvs running over [-1.5, 1.5] so the wrap is
+    exercised), a 5 x 3 diffuse gradient on the short box, an
+    occlusion-roughness-metal texture (g = roughness, b = metal, 4 x 4) on the
+    tall box's specular input with SpecTexUsage::OccRoughMetal, and a 6 x 6
+    roughness texture on the red wall, which gets a specular colour.  uvs are
+    planar projections of the vertex positions."""
+    desc, cam = cornell_box()
+    mats = desc.materials.copy()
+    mats[1]["specular"] = (0.9, 0.9, 0.9)
+    mats[4]["spec_usage"] = 1  # CRISB_SPEC_OCC_ROUGH_METAL
+    P, N = desc.positions, desc.normals
+    ax = np.argmax(np.abs(N), axis=1)
+    u = np.where(ax == 0, P[:, 2], P[:, 0])
+    v = np.where(ax == 1, P[:, 2], P[:, 1])
+    uvs = (np.stack([u, v], axis=1) * 3.0).astype(np.float32)
+    rng = np.random.default_rng(3)
+    gradient = np.zeros((3, 5, 4), np.uint8)
+    gradient[..., 0] = np.linspace(40, 250, 5, dtype=np.uint8)[None, :]
+    gradient[..., 1] = np.linspace(200, 30, 3, dtype=np.uint8)[:, None]
+    gradient[..., 2] = 90
+    gradient[..., 3] = 255
+    orm = np.zeros((4, 4, 4), np.uint8)
+    orm[..., 0] = 255
+    orm[..., 1] = rng.integers(50, 230, (4, 4))
+    orm[..., 2] = rng.integers(0, 256, (4, 4))
+    orm[..., 3] = 255
+    rough = np.zeros((6, 6, 4), np.uint8)
+    rough[..., 0] = rng.integers(40, 255, (6, 6))
+    rough[..., 3] = 255
+    textures = [_checker(8, 8, (230, 230, 220, 255), (40, 60, 160, 255), 2), gradient, orm, rough]
+    mt = np.full((len(mats), 3), -1, np.int32)
+    mt[0, 0] = 0  # floor, ceiling and back wall: checker diffuse
+    mt[3, 0] = 1  # short box: gradient diffuse
+    mt[4, 1] = 2  # tall box: ORM specular input
+    mt[1, 2] = 3  # red wall: roughness texture
+    return dataclasses.replace(desc, materials=mats, uvs=uvs, textures=textures, material_textures=mt,
+                               name="cornell_textured"), cam
 
 
 def _icosphere(subdiv: int):

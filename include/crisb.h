@@ -64,7 +64,8 @@ extern "C" {
 #define CRISB_INVALID_PRIM 0xFFFFFFFFu
 
 /* ---- scene description ------------------------------------------------- */
-/* MaterialSbtData without textures (include/model/Material.h:15-32).
+/* MaterialSbtData (include/model/Material.h:15-32); its textures are in
+ * crisb_scene_desc.material_textures.
  * specular is the reference's specF0 input; with spec_usage == COLOR the
  * reference replaces it by mix(diffuse, specular, 0) = diffuse
  * (shader/brdf.cu:124-138), and this library does the same. */
@@ -101,6 +102,16 @@ typedef struct crisb_emitter {
     uint32_t num_faces;
 } crisb_emitter;
 
+/* Texture (src/Texture.cpp:8-75): width * height RGBA8 texels in the order
+ * stbi_load(..., STBI_rgb_alpha) returns them (first row first).  Sampled as
+ * the reference's texture objects are set up: normalised coordinates, wrap
+ * addressing, linear filtering, texels read as c / 255. */
+typedef struct crisb_texture {
+    const uint8_t* rgba;
+    uint32_t width;
+    uint32_t height;
+} crisb_texture;
+
 typedef struct crisb_scene_desc {
     const float* positions;         /* num_vertices * 3 */
     const float* normals;           /* num_vertices * 3, or NULL (face normals) */
@@ -118,6 +129,14 @@ typedef struct crisb_scene_desc {
     uint32_t num_emitters;
     const float* emitter_faces;     /* num_emitter_faces * 9 (v0,v1,v2) */
     uint32_t num_emitter_faces;
+    /* Textured materials (MaterialSbtData::{diff,spec,rough}Tex,
+     * include/model/Material.h:23-30; sampled in shader/brdf.cu:64-97).  All
+     * may be NULL / 0: no textures. */
+    const float* uvs;               /* num_vertices * 2 (Vertex::uv), or NULL */
+    const crisb_texture* textures;
+    uint32_t num_textures;
+    const int32_t* material_textures; /* num_materials * 3: diffuse, specular,
+                                         roughness texture index or -1 */
 } crisb_scene_desc;
 
 /* ---- camera (Camera, include/graph/Camera.h:24-79) --------------------- */

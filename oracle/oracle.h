@@ -42,6 +42,13 @@ int oracle_render_frame_timed(oracle_ctx* ctx, const crisb_camera* cam,
 /* CRISB_MOTION_VECTORS input: num_pixels (= width * height) float pairs on the
  * host, copied; NULL clears */
 int oracle_set_motion_vectors(oracle_ctx* ctx, const float* motion, uint32_t num_pixels);
+/* textured materials: 6 corner uvs per oracle triangle, the textures and per
+ * material (diffuse, specular, roughness) texture indices or -1 (NULL: none) */
+int oracle_set_textures(oracle_ctx* ctx, const float* tri_uvs, uint32_t num_tris, const crisb_texture* textures,
+                        uint32_t num_textures, const int32_t* material_textures);
+/* the texture fetch alone: n (u, v) pairs -> n RGBA floats */
+void oracle_tex_sample(const uint8_t* rgba, uint32_t width, uint32_t height, const float* uv, uint32_t n,
+                       float* out);
 uint64_t oracle_frame_index(const oracle_ctx* ctx);
 uint32_t oracle_frame_random(const oracle_ctx* ctx);
 /* Copy internal state in the crisb_*_rec layout (CRISB_BUF_* ids). */

@@ -47,6 +47,8 @@ def load():
         "oracle_render_frame": (i32, [vp, ctypes.POINTER(_abi.Camera), vp]),
         "oracle_render_frame_timed": (i32, [vp, ctypes.POINTER(_abi.Camera), vp, vp]),
         "oracle_set_motion_vectors": (i32, [vp, vp, u32]),
+        "oracle_set_textures": (i32, [vp, vp, u32, vp, u32, vp]),
+        "oracle_tex_sample": (None, [vp, u32, u32, vp, u32, vp]),
         "oracle_frame_index": (u64, [vp]),
         "oracle_frame_random": (u32, [vp]),
         "oracle_dump": (i32, [vp, i32, vp, ctypes.c_size_t]),
@@ -118,8 +120,24 @@ class Oracle:
         """Oracle over a scene description; `triangles` = (pos, nrm, mat) soup
         (defaults to the scene's own float64 flattening)."""
         pos, nrm, mat = triangles if triangles is not None else scene_desc.flatten()
-        return cls(pos, nrm, mat, scene_desc.materials, scene_desc.emitters, scene_desc.emitter_faces, width,
-                   height, params)
+        o = cls(pos, nrm, mat, scene_desc.materials, scene_desc.emitters, scene_desc.emitter_faces, width, height,
+                params)
+        if getattr(scene_desc, "textured", False):
+            o.set_textures(scene_desc.flatten_uvs(), scene_desc.textures, scene_desc.material_textures)
+        return o
+
+    def set_textures(self, tri_uvs, textures, material_textures):
+        """(T, 6) corner uvs, (H, W, 4) uint8 textures, (M, 3) texture indices."""
+        uv = np.ascontiguousarray(tri_uvs, np.float32)
+        keep = [np.ascontiguousarray(t, np.uint8) for t in textures]
+        tex = (_abi.Texture * max(len(keep), 1))()
+        for i, t in enumerate(keep):
+            tex[i].rgba = t.ctypes.data_as(ctypes.c_void_p)
+            tex[i].height, tex[i].width = int(t.shape[0]), int(t.shape[1])
+        mt = np.ascontiguousarray(material_textures, np.int32)
+        if load().oracle_set_textures(self.h, _ptr(uv), len(uv), ctypes.cast(tex, ctypes.c_void_p), len(keep),
+                                      _ptr(mt)) != 0:
+            raise ValueError("oracle rejected the textures")
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -234,6 +252,16 @@ def srgb8_first_decrease(lo: float, hi: float) -> int:
     lo_b = int(np.float32(lo).view(np.uint32))
     hi_b = int(np.float32(hi).view(np.uint32))
     return int(load().oracle_srgb8_first_decrease(lo_b, hi_b))
+
+
+def tex_sample(rgba: np.ndarray, uv: np.ndarray) -> np.ndarray:
+    """The oracle's texture fetch of an (H, W, 4) uint8 texture at (n, 2)
+    normalised coordinates: (n, 4) floats."""
+    t = np.ascontiguousarray(rgba, np.uint8)
+    q = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
+    out = np.zeros((len(q), 4), np.float32)
+    load().oracle_tex_sample(_ptr(t), t.shape[1], t.shape[0], _ptr(q), len(q), _ptr(out))
+    return out
 
 
 def oct(dirs: np.ndarray):

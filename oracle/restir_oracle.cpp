@@ -36,6 +36,7 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -742,12 +743,11 @@ struct MatVals {
     float roughness;
 };
 
-// material fetch of brdf.cu:120-138 / 219-237 without textures
-inline MatVals GetMat(const crisb_material& m) {
+// material fetch of brdf.cu:120-138 / 219-237 over looked-up values (the
+// material's constants, or texture samples where it has textures)
+inline MatVals FinishMat(const crisb_material& m, vec3 diff, vec3 specF0, float roughness) {
     MatVals v;
-    v.diff = vec3(m.diffuse[0], m.diffuse[1], m.diffuse[2]);
-    vec3 specF0(m.specular[0], m.specular[1], m.specular[2]);
-    float roughness = m.roughness;
+    v.diff = diff;
     float metal = 0.0f;
     if (m.spec_usage == CRISB_SPEC_OCC_ROUGH_METAL) {
         roughness = specF0.y;
@@ -761,9 +761,13 @@ inline MatVals GetMat(const crisb_material& m) {
     return v;
 }
 
+inline MatVals GetMat(const crisb_material& m) {
+    return FinishMat(m, vec3(m.diffuse[0], m.diffuse[1], m.diffuse[2]),
+                     vec3(m.specular[0], m.specular[1], m.specular[2]), m.roughness);
+}
+
 // __direct_callable__ggx_eval, brdf.cu:115-190
-inline BrdfEvalResult GgxEval(const crisb_material& mat, const Interaction& interaction, vec3 outDir) {
-    const MatVals m = GetMat(mat);
+inline BrdfEvalResult GgxEval(const MatVals& m, const Interaction& interaction, vec3 outDir) {
     BrdfEvalResult result;
     const vec3 lightDir = outDir;
     const vec3 viewDir = -interaction.inRayDir;
@@ -814,8 +818,7 @@ inline Frame3 ComputeLocalFrame(vec3 localZ) {
 }
 
 // __direct_callable__ggx_sample, brdf.cu:214-337
-inline BrdfSampleResult GgxSample(const crisb_material& mat, const Interaction& interaction, PCG32& rng) {
-    const MatVals m = GetMat(mat);
+inline BrdfSampleResult GgxSample(const MatVals& m, const Interaction& interaction, PCG32& rng) {
     const vec3 normal = interaction.normal;
     const vec3 viewDir = -interaction.inRayDir;
     BrdfSampleResult result;
@@ -1011,8 +1014,79 @@ struct oracle_ctx {
         return it;
     }
     const crisb_material& MatOf(const Interaction& it) const { return scene.mats[scene.tris[it.prim].mat]; }
-    BrdfEvalResult Eval(const Interaction& it, vec3 dir) const { return GgxEval(MatOf(it), it, dir); }
-    BrdfSampleResult Sample(const Interaction& it, PCG32& rng) const { return GgxSample(MatOf(it), it, rng); }
+    BrdfEvalResult Eval(const Interaction& it, vec3 dir) const { return GgxEval(MatValsAt(it), it, dir); }
+    BrdfSampleResult Sample(const Interaction& it, PCG32& rng) const { return GgxSample(MatValsAt(it), it, rng); }
+
+    // ---- textures: tex2D of src/Texture.cpp:44-72 and GetFromTexIfPossible,
+    // shader/brdf.cu:64-97 ----------------------------------------------------
+    struct Texture {
+        uint32_t width = 0, height = 0;
+        std::vector<uint32_t> texels;  // RGBA8 words, first row first
+    };
+    std::vector<float> triUv;                   // 6 per triangle (corner uvs)
+    std::vector<Texture> textures;
+    std::vector<std::array<int32_t, 3>> matTex;  // diffuse, specular, roughness
+
+    struct Rgba {
+        float r, g, b, a;
+    };
+    static Rgba Texel(uint32_t w) {
+        return Rgba{static_cast<float>(w & 0xffu) / 255.0f, static_cast<float>((w >> 8) & 0xffu) / 255.0f,
+                    static_cast<float>((w >> 16) & 0xffu) / 255.0f, static_cast<float>(w >> 24) / 255.0f};
+    }
+    // DEFINED after the CUDA programming guide's linear filtering of
+    // normalised, wrapped coordinates: x_B = frac(u) * width - 0.5, i =
+    // floor(x_B), alpha = frac(x_B) with 8 fractional bits (rounded), texels
+    // i and i + 1 wrapped; (1-a)(1-b) T00 + a(1-b) T10 + (1-a) b T01 + a b T11.
+    Rgba TexSample(int t, float u, float v) const {
+        const Texture& tx = textures[static_cast<size_t>(t)];
+        const int W = static_cast<int>(tx.width), H = static_cast<int>(tx.height);
+        if (!std::isfinite(u)) u = 0.0f;
+        if (!std::isfinite(v)) v = 0.0f;
+        const float x = (u - std::floor(u)) * static_cast<float>(W) - 0.5f;
+        const float y = (v - std::floor(v)) * static_cast<float>(H) - 0.5f;
+        const float xf = std::floor(x), yf = std::floor(y);
+        const float a = std::floor((x - xf) * 256.0f + 0.5f) * (1.0f / 256.0f);
+        const float b = std::floor((y - yf) * 256.0f + 0.5f) * (1.0f / 256.0f);
+        const int i0 = ((static_cast<int>(xf) % W) + W) % W, j0 = ((static_cast<int>(yf) % H) + H) % H;
+        const int i1 = (i0 + 1) % W, j1 = (j0 + 1) % H;
+        const Rgba t00 = Texel(tx.texels[static_cast<size_t>(j0) * W + i0]);
+        const Rgba t10 = Texel(tx.texels[static_cast<size_t>(j0) * W + i1]);
+        const Rgba t01 = Texel(tx.texels[static_cast<size_t>(j1) * W + i0]);
+        const Rgba t11 = Texel(tx.texels[static_cast<size_t>(j1) * W + i1]);
+        const float w00 = (1.0f - a) * (1.0f - b), w10 = a * (1.0f - b), w01 = (1.0f - a) * b, w11 = a * b;
+        auto mix = [&](float c00, float c10, float c01, float c11) {
+            return ((w00 * c00 + w10 * c10) + w01 * c01) + w11 * c11;
+        };
+        return Rgba{mix(t00.r, t10.r, t01.r, t11.r), mix(t00.g, t10.g, t01.g, t11.g),
+                    mix(t00.b, t10.b, t01.b, t11.b), mix(t00.a, t10.a, t01.a, t11.a)};
+    }
+    MatVals MatValsAt(const Interaction& it) const {
+        const crisb_material& m = MatOf(it);
+        vec3 diff(m.diffuse[0], m.diffuse[1], m.diffuse[2]);
+        vec3 f0(m.specular[0], m.specular[1], m.specular[2]);
+        float rough = m.roughness;
+        if (!matTex.empty()) {
+            const std::array<int32_t, 3>& t = matTex[scene.tris[it.prim].mat];
+            if (t[0] >= 0 || t[1] >= 0 || t[2] >= 0) {
+                // Interaction::uv = InterpolateBary of the corner uvs (Interaction.h:171)
+                const float* c = &triUv[6 * static_cast<size_t>(it.prim)];
+                const float w = 1.0f - it.bary.x - it.bary.y;
+                const float u = (w * c[0] + it.bary.x * c[2]) + it.bary.y * c[4];
+                const float v = (w * c[1] + it.bary.x * c[3]) + it.bary.y * c[5];
+                if (t[0] >= 0) {
+                    const Rgba s = TexSample(t[0], u, v);
+                    diff = vec3(s.r, s.g, s.b);
+                }
+                if (t[1] >= 0) {
+                    const Rgba s = TexSample(t[1], u, v);
+                    f0 = vec3(s.r, s.g, s.b);
+                }
+                if (t[2] >= 0) rough = TexSample(t[2], u, v).r;
+            }
+        }
+        return FinishMat(m, diff, f0, rough);
+    }
 
     // SampleEmitter, sample_emitter.h:3-12 + EmitterData::SamplePoint, Emitter.h:21-54
     EmitterSample SampleEmitter(PCG32& rng) const {
@@ -2238,6 +2312,54 @@ int oracle_render_frame_timed(oracle_ctx* ctx, const crisb_camera* cam, float* o
     if (!ctx || !cam || !out_rgb || !MotionReady(ctx)) return CRISB_ERR_INVALID_ARGUMENT;
     ctx->RenderFrame(*cam, out_rgb, pass_ms);
     return CRISB_OK;
+}
+
+int oracle_set_textures(oracle_ctx* ctx, const float* tri_uvs, uint32_t num_tris, const crisb_texture* textures,
+                        uint32_t num_textures, const int32_t* material_textures) {
+    if (!ctx || num_tris != ctx->scene.tris.size()) return CRISB_ERR_INVALID_ARGUMENT;
+    if (!material_textures) {
+        ctx->matTex.clear();
+        return CRISB_OK;
+    }
+    const size_t M = ctx->scene.mats.size();
+    std::vector<std::array<int32_t, 3>> mt(M);
+    for (size_t m = 0; m < M; ++m)
+        for (int k = 0; k < 3; ++k) {
+            const int32_t t = material_textures[3 * m + k];
+            if (t < -1 || t >= static_cast<int64_t>(num_textures)) return CRISB_ERR_INVALID_ARGUMENT;
+            mt[m][k] = t;
+        }
+    if (!tri_uvs || (num_textures && !textures)) return CRISB_ERR_INVALID_ARGUMENT;
+    std::vector<oracle_ctx::Texture> tx(num_textures);
+    for (uint32_t t = 0; t < num_textures; ++t) {
+        if (!textures[t].rgba || textures[t].width == 0 || textures[t].height == 0) return CRISB_ERR_INVALID_ARGUMENT;
+        tx[t].width = textures[t].width;
+        tx[t].height = textures[t].height;
+        tx[t].texels.resize(static_cast<size_t>(tx[t].width) * tx[t].height);
+        std::memcpy(tx[t].texels.data(), textures[t].rgba, 4 * tx[t].texels.size());
+    }
+    ctx->triUv.assign(tri_uvs, tri_uvs + 6 * static_cast<size_t>(num_tris));
+    ctx->textures = std::move(tx);
+    ctx->matTex = std::move(mt);
+    return CRISB_OK;
+}
+
+void oracle_tex_sample(const uint8_t* rgba, uint32_t width, uint32_t height, const float* uv, uint32_t n,
+                       float* out) {
+    oracle_ctx::Texture t;
+    t.width = width;
+    t.height = height;
+    t.texels.resize(static_cast<size_t>(width) * height);
+    std::memcpy(t.texels.data(), rgba, 4 * t.texels.size());
+    oracle_ctx probe;
+    probe.textures.push_back(std::move(t));
+    for (uint32_t i = 0; i < n; ++i) {
+        const oracle_ctx::Rgba c = probe.TexSample(0, uv[2 * i], uv[2 * i + 1]);
+        out[4 * i] = c.r;
+        out[4 * i + 1] = c.g;
+        out[4 * i + 2] = c.b;
+        out[4 * i + 3] = c.a;
+    }
 }
 
 int oracle_set_motion_vectors(oracle_ctx* ctx, const float* motion, uint32_t num_pixels) {

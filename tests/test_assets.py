@@ -1,0 +1,195 @@
+"""Textured materials and the OBJ / MTL / PNG asset path.
+
+CPU: the PNG reader on every row filter and colour type, an OBJ + MTL + PNG
+round trip of the textured Cornell box to the same arrays and the same oracle
+frames, the oracle's texture fetch against a numpy restatement of its
+definition, and textures against constant materials.  GPU: the library
+against the oracle on textured scenes (FP32 and FP16 storage, the three
+renderer types) and on the scene read back from OBJ."""
+import struct
+import zlib
+
+import numpy as np
+import pytest
+
+import oracle_py as op
+from crisoptix_b200 import _abi, assets, scenes
+from helpers import scene_size_of, small_config_params, static
+
+W, H = 48, 40
+
+
+def _png(rows: np.ndarray, color: int) -> bytes:
+    """Filter-0 PNG of (H, W, C) uint8 rows with colour type `color`."""
+    h, w = rows.shape[:2]
+    raw = np.concatenate([np.zeros((h, 1), np.uint8), rows.reshape(h, -1)], axis=1)
+
+    def chunk(k, b):
+        return struct.pack(">I", len(b)) + k + b + struct.pack(">I", zlib.crc32(k + b) & 0xFFFFFFFF)
+
+    return (b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, color, 0, 0, 0)) +
+            chunk(b"IDAT", zlib.compress(raw.tobytes())) + chunk(b"IEND", b""))
+
+
+@pytest.mark.parametrize("filter_type", [0, 1, 2, 3, 4])
+def test_png_filters_round_trip(filter_type):
+    rng = np.random.default_rng(filter_type)
+    a = rng.integers(0, 256, (9, 13, 4), dtype=np.uint8)
+    a[3:5] = a[2]  # repeated rows and smooth runs exercise the predictors
+    a[:, 4:8] = np.arange(4, dtype=np.uint8)[None, :, None] * 40
+    assert (assets.decode_png_rgba(assets.encode_png_rgba(a, filter_type)) == a).all()
+
+
+def test_png_colour_types_expand_like_stbi_rgba():
+    rng = np.random.default_rng(1)
+    g = rng.integers(0, 256, (5, 7, 1), dtype=np.uint8)
+    ga = rng.integers(0, 256, (5, 7, 2), dtype=np.uint8)
+    rgb = rng.integers(0, 256, (5, 7, 3), dtype=np.uint8)
+    out = assets.decode_png_rgba(_png(g, 0))
+    assert (out[..., :3] == g).all() and (out[..., 3] == 255).all()
+    out = assets.decode_png_rgba(_png(ga, 4))
+    assert (out[..., :3] == ga[..., :1]).all() and (out[..., 3] == ga[..., 1]).all()
+    out = assets.decode_png_rgba(_png(rgb, 2))
+    assert (out[..., :3] == rgb).all() and (out[..., 3] == 255).all()
+    with pytest.raises(ValueError):
+        assets.decode_png_rgba(b"not a png")
+
+
+def _tex_np(rgba, uv):
+    """numpy float32 restatement of the texture fetch's definition."""
+    t = rgba.astype(np.float32) / np.float32(255.0)
+    h, w = rgba.shape[:2]
+    f = np.float32
+    u, v = uv[:, 0].astype(f), uv[:, 1].astype(f)
+    u = np.where(np.isfinite(u), u, f(0))
+    v = np.where(np.isfinite(v), v, f(0))
+    x = (u - np.floor(u)) * f(w) - f(0.5)
+    y = (v - np.floor(v)) * f(h) - f(0.5)
+    xf, yf = np.floor(x), np.floor(y)
+    a = np.floor((x - xf) * f(256) + f(0.5)) * f(1 / 256)
+    b = np.floor((y - yf) * f(256) + f(0.5)) * f(1 / 256)
+    i0, j0 = xf.astype(np.int64) % w, yf.astype(np.int64) % h
+    i1, j1 = (i0 + 1) % w, (j0 + 1) % h
+    w00, w10, w01, w11 = (f(1) - a) * (f(1) - b), a * (f(1) - b), (f(1) - a) * b, a * b
+    return (((w00[:, None] * t[j0, i0] + w10[:, None] * t[j0, i1]) + w01[:, None] * t[j1, i0]) +
+            w11[:, None] * t[j1, i1]).astype(f)
+
+
+def test_oracle_texture_fetch_matches_its_definition():
+    rng = np.random.default_rng(2)
+    for h, w in ((1, 1), (3, 5), (8, 8), (17, 2)):
+        tex = rng.integers(0, 256, (h, w, 4), dtype=np.uint8)
+        uv = np.concatenate([rng.uniform(-3, 3, (4000, 2)), rng.normal(0, 1e-7, (200, 2)),
+                             [[np.nan, 0.2], [np.inf, -np.inf], [0.5 / w, 0.5 / h], [1.0, 1.0], [-1.0, 2.0]]])
+        uv = uv.astype(np.float32)
+        got = op.tex_sample(tex, uv)
+        assert (got == _tex_np(tex, uv)).all()
+    # at texel centres the fetch is the texel itself
+    tex = rng.integers(0, 256, (4, 6, 4), dtype=np.uint8)
+    jj, ii = np.mgrid[0:4, 0:6]
+    uv = np.stack([(ii.ravel() + 0.5) / 6, (jj.ravel() + 0.5) / 4], axis=1).astype(np.float32)
+    assert np.allclose(op.tex_sample(tex, uv), tex.reshape(-1, 4) / 255.0, atol=1e-6)
+
+
+def test_obj_round_trip(tmp_path):
+    desc, cam = scenes.textured_cornell_box()
+    path = str(tmp_path / "box.obj")
+    assets.save_obj(path, desc)
+    back = assets.load_obj(path)
+    for name in ("positions", "normals", "uvs", "indices", "triangle_material", "emitter_faces"):
+        assert (np.asarray(getattr(back, name)) == np.asarray(getattr(desc, name))).all(), name
+    # SpecTexUsage is a per-model argument (src/Model.cpp:9), not in the MTL
+    assert (back.materials["spec_usage"] == 0).all()
+    back.materials["spec_usage"] = desc.materials["spec_usage"]
+    assert back.materials.tobytes() == desc.materials.tobytes()
+    # textures are numbered in order of first use; every slot reads the same texels
+    assert ((back.material_textures >= 0) == (desc.material_textures >= 0)).all()
+    assert len(back.textures) == len(desc.textures)
+    for tb, td in zip(back.material_textures.ravel(), desc.material_textures.ravel()):
+        if td >= 0:
+            assert (back.textures[tb] == desc.textures[td]).all()
+    assert [(tuple(np.float32(c)), f, n) for c, f, n in back.emitters] == \
+           [(tuple(np.float32(c)), f, n) for c, f, n in desc.emitters]
+    p = small_config_params(scene_size_of(desc))
+    a, b = op.Oracle.from_scene(desc, W, H, p), op.Oracle.from_scene(back, W, H, p)
+    oa, ob = np.zeros((H, W, 3), np.float32), np.zeros((H, W, 3), np.float32)
+    for f in range(2):
+        a.render_frame(cam, oa)
+        b.render_frame(cam, ob)
+        assert oa.tobytes() == ob.tobytes()
+
+
+def test_obj_flip_uv_fan_and_defaults(tmp_path):
+    (tmp_path / "q.mtl").write_text("newmtl lit\nKe 5 5 5\nnewmtl plain\n")
+    (tmp_path / "q.obj").write_text(
+        "mtllib q.mtl\nv 0 0 0\nv 1 0 0\nv 1 1 0\nv 0 1 0\nvt 0 0.25\nvt 1 0.25\nvt 1 1\nvt 0 1\n"
+        "usemtl plain\nf 1/1 2/2 3/3 4/4\nusemtl lit\nf -4/-4 -2/-2 -1/-1\n")
+    d = assets.load_obj(str(tmp_path / "q.obj"), flip_uv=True)
+    assert d.indices.shape == (3, 3)  # quad fanned into two, plus one
+    assert len(d.positions) == 9  # corners without vn get the face normal: a vertex each
+    assert np.allclose(d.uvs[:3, 1], [0.75, 0.75, 0.0])
+    assert np.allclose(d.normals[:6], [0, 0, 1])  # generated face normals
+    plain, lit = d.materials
+    assert tuple(plain["diffuse"]) == (1, 1, 1) and plain["roughness"] == 1.0
+    assert tuple(lit["emission"]) == (5, 5, 5) and d.emitters[0][1:] == (0, 1)
+    assert d.material_textures is None
+
+
+def test_textures_change_the_oracle_frame_and_match_constants():
+    """A 1 x 1 texture of value c reads c / 255 (to rounding), so the frame
+    matches the untextured scene with that constant; the textured box does
+    not."""
+    desc, cam = scenes.cornell_box()
+    p = small_config_params(scene_size_of(desc))
+    mats = desc.materials.copy()
+    mats[0]["diffuse"] = (200 / 255, 100 / 255, 50 / 255)
+    const = scenes.Scene(**{**desc.__dict__, "materials": mats})
+    mt = np.full((len(mats), 3), -1, np.int32)
+    mt[0, 0] = 0
+    tex = scenes.Scene(**{**desc.__dict__, "uvs": np.zeros((len(desc.positions), 2), np.float32),
+                          "textures": [np.array([[[200, 100, 50, 255]]], np.uint8)], "material_textures": mt})
+    a, b = op.Oracle.from_scene(const, W, H, p), op.Oracle.from_scene(tex, W, H, p)
+    oa, ob = np.zeros((H, W, 3), np.float32), np.zeros((H, W, 3), np.float32)
+    a.render_frame(cam, oa)
+    b.render_frame(cam, ob)
+    assert np.abs(oa - ob).max() <= 1e-4 * max(1.0, float(np.abs(oa).max()))
+    t, _ = scenes.textured_cornell_box()
+    c = op.Oracle.from_scene(t, W, H, p)
+    oc = np.zeros((H, W, 3), np.float32)
+    c.render_frame(cam, oc)
+    assert np.isfinite(oc).all() and np.abs(oc - oa).mean() > 0.05
+
+
+# ---- GPU parity -----------------------------------------------------------------
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage", [_abi.STORAGE_FP32, _abi.STORAGE_FP16])
+@pytest.mark.parametrize("rtype", [_abi.CONDITIONAL_RESTIR, _abi.RESTIR_PT, _abi.PATH_TRACER])
+def test_textured_parity(cuda_device, rtype, storage):
+    from helpers import orbit
+    from test_parity_gpu import run_parity
+
+    desc, cam = scenes.textured_cornell_box()
+    p = small_config_params(scene_size_of(desc), renderer_type=rtype, storage=storage)
+    run_parity(desc, cam, p, W, H, 3, lambda c, f: orbit(c, f, 30))
+
+
+@pytest.mark.gpu
+def test_obj_scene_parity(cuda_device, tmp_path):
+    from test_parity_gpu import run_parity
+
+    desc, cam = scenes.textured_cornell_box()
+    path = str(tmp_path / "box.obj")
+    assets.save_obj(path, desc)
+    back = assets.load_obj(path, spec_usage=_abi.SPEC_OCC_ROUGH_METAL)  # every material: the ORM workflow
+    run_parity(back, cam, small_config_params(scene_size_of(back)), W, H, 3, static)
+
+
+@pytest.mark.gpu
+def test_adjoint_rejects_textures(cuda_device):
+    from crisoptix_b200 import CrisbError, Scene
+    from crisoptix_b200.adjoint import PtAdjoint
+
+    desc, cam = scenes.textured_cornell_box()
+    with pytest.raises(CrisbError):
+        PtAdjoint(Scene(desc), W, H, small_config_params(scene_size_of(desc), renderer_type=_abi.PATH_TRACER))
