@@ -11,6 +11,7 @@
 //   gather: TracePrefix, then TraceSuffix when the prefix ends without NEE,
 //           into fresh records (final gather, FinalGatherCanon).
 #include <algorithm>
+#include <cstddef>
 #include <mutex>
 
 #include "queues.cuh"
@@ -175,6 +176,52 @@ RT_D void wf_trace_inline(const SceneView& s, WfPath& w, int req) {
 // with kInline (the last wavefront round) trace the path's remaining rays in
 // place until it ends, so the few long paths left do not cost a trace and a
 // shade launch per bounce.
+// Path records move between rounds field group by field group.  A step after
+// a closest hit reads the header (rng, phase, ctr), the ray and the hit; a
+// shadow or reconnection step reads the whole record.  A step writes the
+// header and the groups of the phase it leaves the path in: the next ray
+// (hit phases), the interaction and light (shadow phases), the ray and the
+// NEE BRDF (reconnection); a finished path only its header.  Fields a later
+// step reads are therefore always current in memory, and the hit / occluded
+// words written by the traversal kernels are never overwritten.
+static_assert(offsetof(WfPath, ray_o) == 16, "WfPath header is one 16-byte chunk");
+
+RT_D WfPath wf_load(const WfPath* rec, uint32_t i) {
+    const WfPath* r = rec + i;
+    const uint4 h = *reinterpret_cast<const uint4*>(r);
+    const uint32_t phase = h.z;
+    if (phase != kPhPreHit && phase != kPhSufHit) return *r;
+    WfPath w;
+    w.rng = static_cast<uint64_t>(h.x) | (static_cast<uint64_t>(h.y) << 32);
+    w.phase = h.z;
+    w.ctr = h.w;
+    w.ray_o = r->ray_o;
+    w.ray_d = r->ray_d;
+    w.hit = r->hit;
+    w.occluded = 0u;
+    return w;
+}
+
+RT_D void wf_store(WfPath* rec, uint32_t i, const WfPath& w) {
+    WfPath* r = rec + i;
+    *reinterpret_cast<uint4*>(r) =
+        make_uint4(static_cast<uint32_t>(w.rng), static_cast<uint32_t>(w.rng >> 32), w.phase, w.ctr);
+    if (w.phase == kPhPreHit || w.phase == kPhSufHit) {
+        r->ray_o = w.ray_o;
+        r->ray_d = w.ray_d;
+    } else if (w.phase == kPhPreShadow || w.phase == kPhSufShadow) {
+        r->it_pos = w.it_pos;
+        r->it_nrm = w.it_nrm;
+        r->it_dir = w.it_dir;
+        r->nee_dir = w.nee_dir;
+        r->nee_col = w.nee_col;
+    } else if (w.phase == kPhSufRecon) {
+        r->ray_o = w.ray_o;
+        r->ray_d = w.ray_d;
+        r->nee_brdf = w.nee_brdf;
+    }
+}
+
 template <bool kInline>
 __global__ void __launch_bounds__(kPassBlock) k_wf_shade(SceneView s, FrameParams fp, Bufs b, int flow, int cur) {
     const uint32_t nc = b.wf_count[2 * cur], ns = b.wf_count[2 * cur + 1];
@@ -190,7 +237,7 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_shade(SceneView s, FrameParam
         uint32_t i = 0;
         if (t < total) {
             i = t < nc ? qc[t] : qs[t - nc];
-            WfPath w = b.wf[i];
+            WfPath w = wf_load(b.wf, i);
             Rng rng{w.rng};
             req = wf_step(s, fp, b, flow, i, w, rng);
             if (kInline) {
@@ -205,7 +252,7 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_shade(SceneView s, FrameParam
                 req = kReqDone;
             }
             w.rng = rng.state;
-            b.wf[i] = w;
+            wf_store(b.wf, i, w);
         }
         if (!kInline) wf_push(b, nxt, req, i);
     }
