@@ -58,6 +58,49 @@ RT_D Prefix fresh_prefix() {
     return cp;
 }
 
+// A machine step's record: the running values (flags, f, postReconF, p, path
+// length, reconOutDir) move every step, the vertex fields only when the step
+// set them (kSet*); the rng and first-vertex fields are written when the
+// record is started, by a whole-record store.
+RT_D Prefix ld_prefix_run(const crisb_prefix_rec& r) {
+    Prefix p;
+    p.flags = r.flags;
+    p.f = ld3(r.f);
+    p.prf = ld3(r.post_recon_f);
+    p.p = r.p;
+    p.path_len = r.path_len;
+    p.rod = ld3(r.recon_out_dir);
+    return p;
+}
+RT_D void st_prefix_step(crisb_prefix_rec& r, const Prefix& p, uint32_t set) {
+    if (set & kSetPrimary) st_hit(r.primary, p.primary);
+    if (set & kSetRecon) st_hit(r.recon, p.recon);
+    if (set & kSetLast) st_hit(r.last, p.last);
+    r.flags = p.flags;
+    st3(r.f, p.f);
+    st3(r.post_recon_f, p.prf);
+    r.p = p.p;
+    r.path_len = p.path_len;
+    st3(r.recon_out_dir, p.rod);
+}
+RT_D Suffix ld_suffix_run(const crisb_suffix_rec& r) {
+    Suffix s;
+    s.flags = r.flags;
+    s.f = ld3(r.f);
+    s.prf = ld3(r.post_recon_f);
+    s.p = r.p;
+    s.rod = ld3(r.recon_out_dir);
+    return s;
+}
+RT_D void st_suffix_step(crisb_suffix_rec& r, const Suffix& s, uint32_t set) {
+    if (set & kSetRecon) st_hit(r.recon, s.recon);
+    r.flags = s.flags;
+    st3(r.f, s.f);
+    st3(r.post_recon_f, s.prf);
+    r.p = s.p;
+    st3(r.recon_out_dir, s.rod);
+}
+
 RT_D void st_suffix_slot(crisb_suffix_res_rec& slot, const Suffix& sfx) {
     crisb_suffix_res_rec o;
     st_suffix(o.sample, sfx);
@@ -136,9 +179,10 @@ RT_D int wf_step(const SceneView& s, const FrameParams& fp, const Bufs& b, int f
                  Rng& rng) {
     if (w.phase == kPhPreHit || w.phase == kPhPreShadow) {
         crisb_prefix_rec& rec = flow == 0 ? b.canon_prefix[i] : b.gather_cp[i];
-        Prefix pre = ld_prefix(rec);
-        int req = w.phase == kPhPreHit ? pre_on_hit(s, fp, pre, w, rng) : pre_on_shadow(s, pre, w);
-        st_prefix(rec, pre);
+        Prefix pre = ld_prefix_run(rec);
+        uint32_t set = 0;
+        int req = w.phase == kPhPreHit ? pre_on_hit(s, fp, pre, w, rng, set) : pre_on_shadow(s, pre, w, set);
+        st_prefix_step(rec, pre, set);
         if (req == kReqDone && flow == 2 && fl_valid(pre.flags) && !fl_nee(pre.flags)) {
             // FinalGatherCanon: the canonical suffix continues the canonical prefix
             Suffix cs = fresh_suffix();
@@ -148,12 +192,13 @@ RT_D int wf_step(const SceneView& s, const FrameParams& fp, const Bufs& b, int f
         return req;
     }
     crisb_suffix_res_rec& slot = flow == 1 ? b.canon_suffix[i] : b.gather_cs[i];
-    Suffix suf = ld_suffix(slot.sample);
+    Suffix suf = ld_suffix_run(slot.sample);
+    uint32_t set = 0;
     int req = kReqDone;
-    if (w.phase == kPhSufHit) req = suf_on_hit(s, fp, suf, w, rng);
+    if (w.phase == kPhSufHit) req = suf_on_hit(s, fp, suf, w, rng, set);
     else if (w.phase == kPhSufShadow) req = suf_on_shadow(s, suf, w);
-    else if (w.phase == kPhSufRecon) req = suf_on_recon(s, suf, w);
-    st_suffix_slot(slot, suf);
+    else if (w.phase == kPhSufRecon) req = suf_on_recon(s, suf, w, set);
+    st_suffix_step(slot.sample, suf, set);
     return req;
 }
 

@@ -112,12 +112,16 @@ RT_D int pre_begin(const FrameParams& fp, Prefix& pre, WfPath& w, V3 origin, V3 
     return kReqClosest;
 }
 
+// Vertex fields a machine step wrote (the steps never read them: a step's
+// record moves as its running values plus the vertex fields it set)
+enum : uint32_t { kSetPrimary = 1u, kSetRecon = 2u, kSetLast = 4u };
+
 RT_D int pre_invalid(Prefix& pre, WfPath& w) {
     pre.flags = fl_set_valid(pre.flags, false);
     return wf_done(w);
 }
 
-RT_D int pre_on_hit(const SceneView& s, const FrameParams& fp, Prefix& pre, WfPath& w, Rng& rng) {
+RT_D int pre_on_hit(const SceneView& s, const FrameParams& fp, Prefix& pre, WfPath& w, Rng& rng, uint32_t& set) {
     Isect it;
     if (!wf_hit_isect(s, w, it)) return pre_invalid(pre, w);
     const V3 cur_pos = f3(w.ray_o);
@@ -127,15 +131,20 @@ RT_D int pre_on_hit(const SceneView& s, const FrameParams& fp, Prefix& pre, WfPa
     const float nee = fp.p.nee_prob;
     pre.path_len += distance(cur_pos, it.pos);
     pre.flags = fl_set_len(pre.flags, fl_len(pre.flags) + 1);
-    if (fl_len(pre.flags) == 1) pre.primary = it.pack();
+    if (fl_len(pre.flags) == 1) {
+        pre.primary = it.pack();
+        set |= kSetPrimary;
+    }
     if (type == CRISB_RENDERER_CONDITIONAL_RESTIR && ti == max_len - 1) {
         if (!post) {
             pre.recon = it.pack();
             pre.flags = fl_set_recon(pre.flags, fl_len(pre.flags));
             pre.rod = splat(0.0f);
+            set |= kSetRecon;
         }
         pre.flags = fl_set_valid(pre.flags, true);
         pre.last = it.pack();
+        set |= kSetLast;
         return wf_done(w);
     }
     const bool force_nee = type == CRISB_RENDERER_RESTIR_PT && ti == max_len - 1;
@@ -160,6 +169,7 @@ RT_D int pre_on_hit(const SceneView& s, const FrameParams& fp, Prefix& pre, WfPa
         pre.flags = fl_set_recon(pre.flags, fl_len(pre.flags));
         pre.rod = bs.dir;
         post = true;
+        set |= kSetRecon;
     }
     pre.f = pre.f * bs.brdf;
     pre.p *= bs.pdf * (1.0f - nee);
@@ -172,10 +182,11 @@ RT_D int pre_on_hit(const SceneView& s, const FrameParams& fp, Prefix& pre, WfPa
         return kReqClosest;
     }
     pre.last = it.pack();
+    set |= kSetLast;
     return wf_done(w);
 }
 
-RT_D int pre_on_shadow(const SceneView& s, Prefix& pre, WfPath& w) {
+RT_D int pre_on_shadow(const SceneView& s, Prefix& pre, WfPath& w, uint32_t& set) {
     if (w.occluded) return pre_invalid(pre, w);
     const Isect it = wf_it(w);
     if (!wf_post(w)) {
@@ -183,6 +194,7 @@ RT_D int pre_on_shadow(const SceneView& s, Prefix& pre, WfPath& w) {
         pre.recon = it.pack();
         pre.flags = fl_set_recon(pre.flags, fl_len(pre.flags));
         pre.rod = f3(w.ray_d);
+        set |= kSetRecon;
     }
     const bool post = true;
     const V3 light_dir = f3(w.nee_dir), color = f3(w.nee_col);
@@ -196,6 +208,7 @@ RT_D int pre_on_shadow(const SceneView& s, Prefix& pre, WfPath& w) {
     pre.flags = fl_set_nee(pre.flags, true);
     pre.flags = fl_set_valid(pre.flags, true);
     pre.last = it.pack();
+    set |= kSetLast;
     return wf_done(w);
 }
 
@@ -214,7 +227,7 @@ RT_D int suf_finish_nee(Suffix& suf, WfPath& w, V3 brdf) {
 // loop body at vertex index wf_idx(w) with interaction `it`; last_pos is the
 // position the vertex was traced from (lastPos)
 RT_D int suf_vertex(const SceneView& s, const FrameParams& fp, Suffix& suf, WfPath& w, const Isect& it, V3 last_pos,
-                    Rng& rng) {
+                    Rng& rng, uint32_t& set) {
     const uint32_t vi = wf_idx(w), max_len = wf_maxlen(w), pre_len = wf_prelen(w);
     bool post = wf_post(w);
     const float nee = fp.p.nee_prob;
@@ -245,6 +258,7 @@ RT_D int suf_vertex(const SceneView& s, const FrameParams& fp, Suffix& suf, WfPa
         suf.flags = fl_set_recon(suf.flags, pre_len);
         suf.rod = bs.dir;
         post = true;
+        set |= kSetRecon;
     }
     suf.flags = fl_set_len(suf.flags, fl_len(suf.flags) + 1);
     if (vi + 1 < max_len) {
@@ -272,13 +286,14 @@ RT_D int suf_begin(const SceneView& s, const FrameParams& fp, Suffix& suf, WfPat
     const Isect it = unpack(s, pre_last);
     if (!it.valid || max_len == 0) return wf_done(w);
     wf_set(w, 0, false, max_len, fl_len(pre_flags));
-    return suf_vertex(s, fp, suf, w, it, it.pos, rng);
+    uint32_t set = 0;  // suf_begin's callers store the whole record
+    return suf_vertex(s, fp, suf, w, it, it.pos, rng, set);
 }
 
-RT_D int suf_on_hit(const SceneView& s, const FrameParams& fp, Suffix& suf, WfPath& w, Rng& rng) {
+RT_D int suf_on_hit(const SceneView& s, const FrameParams& fp, Suffix& suf, WfPath& w, Rng& rng, uint32_t& set) {
     Isect it;
     if (!wf_hit_isect(s, w, it)) return wf_done(w);
-    return suf_vertex(s, fp, suf, w, it, f3(w.ray_o), rng);
+    return suf_vertex(s, fp, suf, w, it, f3(w.ray_o), rng, set);
 }
 
 RT_D int suf_on_shadow(const SceneView& s, Suffix& suf, WfPath& w) {
@@ -298,9 +313,10 @@ RT_D int suf_on_shadow(const SceneView& s, Suffix& suf, WfPath& w) {
     return suf_finish_nee(suf, w, be.brdf);
 }
 
-RT_D int suf_on_recon(const SceneView& s, Suffix& suf, WfPath& w) {
+RT_D int suf_on_recon(const SceneView& s, Suffix& suf, WfPath& w, uint32_t& set) {
     Isect rc;
     if (!wf_hit_isect(s, w, rc)) return wf_done(w);
+    set |= kSetRecon;
     suf.recon = rc.pack();
     suf.flags = fl_set_recon(suf.flags, fl_len(suf.flags));
     suf.rod = splat(0.0f);
