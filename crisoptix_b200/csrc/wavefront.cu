@@ -109,6 +109,52 @@ RT_D void st_suffix_slot(crisb_suffix_res_rec& slot, const Suffix& sfx) {
     slot = o;
 }
 
+// Path records move between rounds field group by field group.  A step after
+// a closest hit reads the header (rng, phase, ctr), the ray and the hit; a
+// shadow or reconnection step reads the whole record.  A step writes the
+// header and the groups of the phase it leaves the path in: the next ray
+// (hit phases), the interaction and light (shadow phases), the ray and the
+// NEE BRDF (reconnection); a finished path only its header.  Fields a later
+// step reads are therefore always current in memory, and the hit / occluded
+// words written by the traversal kernels are never overwritten.
+static_assert(offsetof(WfPath, ray_o) == 16, "WfPath header is one 16-byte chunk");
+
+RT_D WfPath wf_load(const WfPath* rec, uint32_t i) {
+    const WfPath* r = rec + i;
+    const uint4 h = *reinterpret_cast<const uint4*>(r);
+    const uint32_t phase = h.z;
+    if (phase != kPhPreHit && phase != kPhSufHit) return *r;
+    WfPath w;
+    w.rng = static_cast<uint64_t>(h.x) | (static_cast<uint64_t>(h.y) << 32);
+    w.phase = h.z;
+    w.ctr = h.w;
+    w.ray_o = r->ray_o;
+    w.ray_d = r->ray_d;
+    w.hit = r->hit;
+    w.occluded = 0u;
+    return w;
+}
+
+RT_D void wf_store(WfPath* rec, uint32_t i, const WfPath& w) {
+    WfPath* r = rec + i;
+    *reinterpret_cast<uint4*>(r) =
+        make_uint4(static_cast<uint32_t>(w.rng), static_cast<uint32_t>(w.rng >> 32), w.phase, w.ctr);
+    if (w.phase == kPhPreHit || w.phase == kPhSufHit) {
+        r->ray_o = w.ray_o;
+        r->ray_d = w.ray_d;
+    } else if (w.phase == kPhPreShadow || w.phase == kPhSufShadow) {
+        r->it_pos = w.it_pos;
+        r->it_nrm = w.it_nrm;
+        r->it_dir = w.it_dir;
+        r->nee_dir = w.nee_dir;
+        r->nee_col = w.nee_col;
+    } else if (w.phase == kPhSufRecon) {
+        r->ray_o = w.ray_o;
+        r->ray_d = w.ray_d;
+        r->nee_brdf = w.nee_brdf;
+    }
+}
+
 // ---- init kernels (round 0 requests) ----------------------------------------------
 __global__ void __launch_bounds__(kPassBlock) k_wf_init_prefix(FrameParams fp, Bufs b) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -122,7 +168,7 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_prefix(FrameParams fp, B
         req = pre_begin(fp, pre, w, ld3(fp.cam.pos), dir, rng);
         st_prefix(b.canon_prefix[i], pre);
         w.rng = rng.state;
-        b.wf[i] = w;
+        wf_store(b.wf, i, w);
         b.pass_status[i] = kWfPath;
     }
     wf_push(b, 0, req, i);
@@ -145,7 +191,7 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_suffix(SceneView s, Fram
             req = suf_begin(s, fp, suf, w, pflags, pres_last(b.pres[fp.front], i), rng);
             st_suffix_slot(b.canon_suffix[i], suf);
             w.rng = rng.state;
-            b.wf[i] = w;
+            wf_store(b.wf, i, w);
             b.pass_status[i] = kWfPath;
         }
     }
@@ -167,7 +213,7 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_gather(FrameParams fp, B
             req = pre_begin(fp, cp, w, ld3(fp.cam.pos), dir, rng);
             st_prefix(b.gather_cp[i], cp);
             w.rng = rng.state;
-            b.wf[i] = w;
+            wf_store(b.wf, i, w);
             b.pass_status[i] = kWfPath;
         }
     }
@@ -221,52 +267,6 @@ RT_D void wf_trace_inline(const SceneView& s, WfPath& w, int req) {
 // with kInline (the last wavefront round) trace the path's remaining rays in
 // place until it ends, so the few long paths left do not cost a trace and a
 // shade launch per bounce.
-// Path records move between rounds field group by field group.  A step after
-// a closest hit reads the header (rng, phase, ctr), the ray and the hit; a
-// shadow or reconnection step reads the whole record.  A step writes the
-// header and the groups of the phase it leaves the path in: the next ray
-// (hit phases), the interaction and light (shadow phases), the ray and the
-// NEE BRDF (reconnection); a finished path only its header.  Fields a later
-// step reads are therefore always current in memory, and the hit / occluded
-// words written by the traversal kernels are never overwritten.
-static_assert(offsetof(WfPath, ray_o) == 16, "WfPath header is one 16-byte chunk");
-
-RT_D WfPath wf_load(const WfPath* rec, uint32_t i) {
-    const WfPath* r = rec + i;
-    const uint4 h = *reinterpret_cast<const uint4*>(r);
-    const uint32_t phase = h.z;
-    if (phase != kPhPreHit && phase != kPhSufHit) return *r;
-    WfPath w;
-    w.rng = static_cast<uint64_t>(h.x) | (static_cast<uint64_t>(h.y) << 32);
-    w.phase = h.z;
-    w.ctr = h.w;
-    w.ray_o = r->ray_o;
-    w.ray_d = r->ray_d;
-    w.hit = r->hit;
-    w.occluded = 0u;
-    return w;
-}
-
-RT_D void wf_store(WfPath* rec, uint32_t i, const WfPath& w) {
-    WfPath* r = rec + i;
-    *reinterpret_cast<uint4*>(r) =
-        make_uint4(static_cast<uint32_t>(w.rng), static_cast<uint32_t>(w.rng >> 32), w.phase, w.ctr);
-    if (w.phase == kPhPreHit || w.phase == kPhSufHit) {
-        r->ray_o = w.ray_o;
-        r->ray_d = w.ray_d;
-    } else if (w.phase == kPhPreShadow || w.phase == kPhSufShadow) {
-        r->it_pos = w.it_pos;
-        r->it_nrm = w.it_nrm;
-        r->it_dir = w.it_dir;
-        r->nee_dir = w.nee_dir;
-        r->nee_col = w.nee_col;
-    } else if (w.phase == kPhSufRecon) {
-        r->ray_o = w.ray_o;
-        r->ray_d = w.ray_d;
-        r->nee_brdf = w.nee_brdf;
-    }
-}
-
 template <bool kInline>
 __global__ void __launch_bounds__(kPassBlock) k_wf_shade(SceneView s, FrameParams fp, Bufs b, int flow, int cur) {
     const uint32_t nc = b.wf_count[2 * cur], ns = b.wf_count[2 * cur + 1];
