@@ -211,6 +211,17 @@ RT_D int shift_advance(const SceneView& s, const Bufs& b, bool prefix, const Shi
     return kReqShadow;
 }
 
+// a job waiting for its ray: everything but the hit word, which the traversal
+// kernels write
+RT_D void job_store(ShiftJob* r, const ShiftJob& j) {
+    r->o = j.o;
+    r->d = j.d;
+    r->acc = j.acc;
+    r->rng = j.rng;
+    r->code = j.code;
+    r->ctr = j.ctr;
+}
+
 RT_D void job_push(const Bufs& b, int round, int req, uint32_t t) {
     q_append(b.job_queue[2 * round], &b.job_qcount[2 * round], req == kReqClosest, t);
     q_append(b.job_queue[2 * round + 1], &b.job_qcount[2 * round + 1], req == kReqShadow, t);
@@ -244,7 +255,7 @@ __global__ void __launch_bounds__(kPassBlock) k_shift_begin(SceneView s, FramePa
                 const uint32_t left = static_cast<uint32_t>(max(static_cast<int>(fl_recon(src.flags)) - skip, 0));
                 Rng srng{src.rng};
                 req = shift_advance<kTex>(s, b, prefix, src, j, cur, srng, splat(1.0f), left, false);
-                if (req != kReqDone) b.jobs[t] = j;
+                if (req != kReqDone) job_store(b.jobs + t, j);
             }
         }
         job_push(b, 0, req, t);
@@ -267,10 +278,18 @@ __global__ void __launch_bounds__(kPassBlock) k_shift_step(SceneView s, FramePar
         uint32_t t = 0;
         if (u < total) {
             t = u < nc ? qc[u] : qs[u - nc];
-            ShiftJob j = b.jobs[t];
+            const ShiftJob* jr = b.jobs + t;
             if (u >= nc) {
-                job_out(b, j.code, __float_as_uint(j.hit.x) ? zero : j.acc);
+                // the shadow ray's result: occluded flag, prepared value, job code
+                job_out(b, jr->code, __float_as_uint(jr->hit.x) ? zero : jr->acc);
             } else {
+                ShiftJob j;  // o is written before it is read
+                j.d = jr->d;
+                j.hit = jr->hit;
+                j.acc = jr->acc;
+                j.rng = jr->rng;
+                j.code = jr->code;
+                j.ctr = jr->ctr;
                 // trace_closest semantics: interpolated, normalised normal
                 Isect it;
                 const uint32_t prim = __float_as_uint(j.hit.x);
@@ -288,7 +307,7 @@ __global__ void __launch_bounds__(kPassBlock) k_shift_step(SceneView s, FramePar
                     const ShiftSrc src = resolve_job(fp, b, mode, j.code, nullptr);
                     Rng srng{j.rng};
                     req = shift_advance<kTex>(s, b, prefix, src, j, it, srng, f3(j.acc), j.ctr, kLast);
-                    if (req != kReqDone) b.jobs[t] = j;
+                    if (req != kReqDone) job_store(b.jobs + t, j);
                 }
             }
         }
