@@ -54,15 +54,16 @@ def _unfilter(raw: np.ndarray, h: int, stride: int, bpp: int) -> np.ndarray:
             cur = line.copy()
         elif ft == 2:
             cur = (line.astype(np.uint16) + prev).astype(np.uint8)
-        elif ft in (1, 3, 4):
+        elif ft == 1:
+            # Sub: a running sum per channel, modulo 256
+            cur = np.cumsum(line.reshape(-1, bpp), axis=0, dtype=np.uint8).reshape(-1)
+        elif ft in (3, 4):
             cur = np.zeros(stride, np.uint8)
             for x in range(stride):  # left neighbour dependency: sequential
                 a = int(cur[x - bpp]) if x >= bpp else 0
                 b = int(prev[x])
                 c = int(prev[x - bpp]) if x >= bpp else 0
-                if ft == 1:
-                    pred = a
-                elif ft == 3:
+                if ft == 3:
                     pred = (a + b) >> 1
                 else:
                     p = a + b - c
