@@ -493,6 +493,7 @@ struct crisb_renderer {
     DevBuf<uint4> pres[2];
     DevBuf<crisb_prefix_rec> canon_prefix;
     DevBuf<uint4> sres[2];
+    DevBuf<uint8_t> nval[2];  // per pixel: usable as a spatial neighbour (same ping-pong as sres)
     DevBuf<crisb_suffix_res_rec> canon_suffix;
     DevBuf<crisb_gbuffer_rec> gbuf;
     DevBuf<crisb_neighbor_rec> neighbors;
@@ -547,6 +548,8 @@ struct crisb_renderer {
         b.canon_prefix = canon_prefix.p;
         b.sres_cur = SresBuf{sres[scur].p, f16};
         b.sres_next = SresBuf{sres[scur ^ 1].p, f16};
+        b.nval_cur = nval[scur].p;
+        b.nval_next = nval[scur ^ 1].p;
         b.canon_suffix = canon_suffix.p;
         b.gbuf = gbuf.p;
         b.neighbors = neighbors.p;
@@ -620,6 +623,8 @@ struct crisb_renderer {
         for (int i = 0; i < 2; ++i) {
             pres[i].alloc(static_cast<size_t>(p) * (pres_bytes() / 16));
             sres[i].alloc(static_cast<size_t>(p) * (sres_bytes() / 16));
+            nval[i].alloc(p);
+            check(cudaMemset(nval[i].p, 0, nval[i].bytes()), "memset");
         }
         canon_prefix.alloc(p);
         canon_suffix.alloc(p);

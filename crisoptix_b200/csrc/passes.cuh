@@ -44,6 +44,11 @@ struct Bufs {
     crisb_prefix_rec* canon_prefix;
     SresBuf sres_cur;
     SresBuf sres_next;
+    // per pixel, beside each suffix reservoir buffer: 1 when the pixel can be a
+    // spatial neighbour (valid primary interaction and valid reservoir sample),
+    // written with the reservoir so the neighbour test reads one byte
+    uint8_t* nval_cur;
+    uint8_t* nval_next;
     crisb_suffix_res_rec* canon_suffix;  // 112-byte slots, w_sum/confidence unused
     crisb_gbuffer_rec* gbuf;
     crisb_neighbor_rec* neighbors;  // P * k

@@ -330,6 +330,7 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_temp_finish(FrameParams f
                 Res<Suffix> cur = ld_sres(b.sres_cur, i);
                 invalidate(cur);
                 st_sres(b.sres_next, i, cur);
+                b.nval_next[i] = 0;
             } else if (!fp.p.suffix_enable_temporal || prev_xy == kPrevNone) {
                 st = kStCanonOnly;
             } else {
@@ -386,6 +387,7 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_temp_combine(FrameParams 
     }
     b.gbuf[i].rng = rng.state;
     st_sres(b.sres_next, i, cur);
+    b.nval_next[i] = (b.gbuf[i].flags & 1u) && fl_valid(cur.s.flags) ? 1 : 0;
 }
 
 // ---- suffix spatial reuse (shader/suffix_spatial_reuse.cu:16-167) -----------------
@@ -409,8 +411,7 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_select(FrameParam
                 select_spatial_neighbor(x, y, static_cast<uint32_t>(fp.p.window_radius), rng, nx, ny);
                 if (!(nx < fp.width && ny < fp.height)) continue;
                 const uint32_t ni = ny * fp.width + nx;
-                if (!(b.gbuf[ni].flags & 1u)) continue;
-                if (!fl_valid(sres_flags(b.sres_cur, ni))) continue;
+                if (!b.nval_cur[ni]) continue;  // primary valid && reservoir sample valid
                 nbr[n] = ni;
                 vflags |= 1u << n;
                 mask |= 3ull << (2 * n);
@@ -430,6 +431,7 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_combine(FramePara
     if (b.pass_status[i] == kStFinal) {
         invalidate(cur);
         st_sres(b.sres_next, i, cur);
+        b.nval_next[i] = 0;
         return;
     }
     Rng rng{b.gbuf[i].rng};
@@ -485,6 +487,7 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_combine(FramePara
     }
     b.gbuf[i].rng = rng.state;
     st_sres(b.sres_next, i, cur);
+    b.nval_next[i] = (b.gbuf[i].flags & 1u) && fl_valid(cur.s.flags) ? 1 : 0;
 }
 
 // ---- final gather with gatherN == 1 (shader/final_gather.cu:69-188, 290-356) -----

@@ -183,6 +183,7 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_suffix(SceneView s, Fram
             Res<Suffix> cur = ld_sres(b.sres_cur, i);
             invalidate(cur);
             st_sres(b.sres_next, i, cur);  // the temporal pass writes sres_next
+            b.nval_next[i] = 0;
             b.pass_status[i] = kWfIdle;
         } else {
             Rng rng{b.gbuf[i].rng};
