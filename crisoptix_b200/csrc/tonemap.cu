@@ -162,7 +162,9 @@ __global__ void __launch_bounds__(kToneBlock) k_tonemap_srgb8(const float* __res
     }
 }
 
-// the bucket table in device memory, uploaded once per device
+// the bucket table in device memory, uploaded once per device (13 KB) and
+// kept for the life of the process: no handle owns it, and a table freed while
+// a caller's stream still runs a tone-mapping kernel would be read after free
 const uint2* device_table(int dev) {
     static std::mutex mu;
     static const uint2* tables[64] = {};
