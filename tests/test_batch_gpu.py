@@ -47,3 +47,37 @@ def test_batch_rejects_bad_input(cuda_device):
     b = Batch([r])
     with pytest.raises(Exception):
         b.render([cam], [0])
+
+
+@pytest.mark.gpu
+def test_batch_with_srgb_output_and_reprojection(cuda_device):
+    """Batched views with the sRGB epilogue and temporal reprojection on: each
+    view's bytes and state equal the same view rendered alone."""
+    desc, cam = small_sphere_room()
+    sc = Scene(desc)
+    size = scene_size_of(desc)
+    views = [(48, 40, large_config_params(size, gather_radius=0.3, motion_mode=_abi.MOTION_REPROJECT)),
+             (33, 17, large_config_params(size, gather_radius=0.3))]
+    batched = [Renderer(w, h, sc, p) for w, h, p in views]
+    single = [Renderer(w, h, sc, p) for w, h, p in views]
+    batch = Batch(batched)
+    hdr_b = [torch.zeros(w * h * 3, dtype=torch.float32, device="cuda") for w, h, _ in views]
+    hdr_s = [torch.zeros(w * h * 3, dtype=torch.float32, device="cuda") for w, h, _ in views]
+    srgb_b = [torch.zeros(w * h * 3, dtype=torch.uint8, device="cuda") for w, h, _ in views]
+    srgb_s = [torch.zeros(w * h * 3, dtype=torch.uint8, device="cuda") for w, h, _ in views]
+    for r, o in zip(batched, srgb_b):
+        r.set_srgb_output(o.data_ptr())
+    for r, o in zip(single, srgb_s):
+        r.set_srgb_output(o.data_ptr())
+    for f in range(3):
+        cams = [orbit(cam, f + 11 * k, 120) for k in range(len(views))]
+        batch.render(cams, [o.data_ptr() for o in hdr_b])
+        for r, c, o in zip(single, cams, hdr_s):
+            r.launch_frame(c, o.data_ptr())
+        torch.cuda.synchronize()
+        for k in range(len(views)):
+            assert hdr_b[k].cpu().numpy().tobytes() == hdr_s[k].cpu().numpy().tobytes(), (f, k)
+            assert (srgb_b[k].cpu() == srgb_s[k].cpu()).all(), (f, k)
+            assert int(srgb_b[k].sum()) > 0
+            for b in STATE_BUFS:
+                assert batched[k].debug_read(b).tobytes() == single[k].debug_read(b).tobytes(), (f, k, b)
