@@ -129,9 +129,11 @@ def flat_scene(desc: Scene) -> Scene:
     """The same scene as a non-instanced triangle soup (float64 flattening)."""
     pos, nrm, mat = desc.flatten()
     T = len(mat)
+    uvs = desc.flatten_uvs().reshape(-1, 2) if desc.uvs is not None else None
     return Scene(pos.reshape(-1, 3).copy(), nrm.reshape(-1, 3).copy(), np.arange(3 * T, dtype=np.uint32).reshape(T, 3),
                  mat.astype(np.uint32), desc.materials, np.zeros((0, 2), np.uint32), [], desc.emitters,
-                 desc.emitter_faces, name=desc.name + "_flat")
+                 desc.emitter_faces, name=desc.name + "_flat", uvs=uvs, textures=desc.textures,
+                 material_textures=desc.material_textures)
 
 
 def _material(diffuse, roughness=1.0, emission=(0.0, 0.0, 0.0), specular=None):

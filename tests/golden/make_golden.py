@@ -31,6 +31,12 @@ CASES = {
                                                    prefix_enable_spatial=1, prefix_spatial_count=2))),
     "spheres_large_params": dict(scene="spheres", W=24, H=24, frames=3, cam="orbit",
                                  params=("large", dict(gather_radius=0.3))),
+    "cornell_textured": dict(scene="cornell_textured", W=24, H=20, frames=3, cam="orbit",
+                             params=("small", dict(gather_m=5, gather_radius=0.4))),
+    "cornell_reproject": dict(scene="cornell", W=24, H=20, frames=4, cam="orbit",
+                              params=("small", dict(motion_mode=_abi.MOTION_REPROJECT))),
+    "spheres_fp16": dict(scene="spheres", W=24, H=24, frames=3, cam="orbit",
+                         params=("large", dict(gather_radius=0.3, storage=_abi.STORAGE_FP16))),
 }
 
 STATE = [_abi.BUF_PREFIX_RES_FRONT, _abi.BUF_CANON_PREFIX, _abi.BUF_SUFFIX_RES_FRONT, _abi.BUF_CANON_SUFFIX,
@@ -38,7 +44,8 @@ STATE = [_abi.BUF_PREFIX_RES_FRONT, _abi.BUF_CANON_PREFIX, _abi.BUF_SUFFIX_RES_F
 
 
 def case_inputs(case):
-    desc, cam = scenes.cornell_box() if case["scene"] == "cornell" else small_sphere_room()
+    desc, cam = {"cornell": scenes.cornell_box, "cornell_textured": scenes.textured_cornell_box,
+                 "spheres": small_sphere_room}[case["scene"]]()
     kind, kw = case["params"]
     size = scene_size_of(desc)
     p = {"small": small_config_params, "large": large_config_params, "plain": make_params}[kind](size, **kw)
@@ -55,8 +62,10 @@ def run_oracle(case, triangles=None):
     return out, {str(b): o.dump(b) for b in STATE}
 
 
-def main():
+def main(names=None):
     for name, case in CASES.items():
+        if names and name not in names:
+            continue
         img, state = run_oracle(case)
         np.savez_compressed(os.path.join(HERE, name + ".npz"), image=img,
                             **{"buf" + k: v.view(np.uint8) for k, v in state.items()})
@@ -64,4 +73,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])
