@@ -193,3 +193,18 @@ def test_adjoint_rejects_textures(cuda_device):
     desc, cam = scenes.textured_cornell_box()
     with pytest.raises(CrisbError):
         PtAdjoint(Scene(desc), W, H, small_config_params(scene_size_of(desc), renderer_type=_abi.PATH_TRACER))
+
+
+def test_flat_scene_keeps_textures():
+    """The flattened soup of a textured scene reads the same texels at the
+    same corners, so the oracle renders it identically."""
+    desc, cam = scenes.textured_cornell_box()
+    flat = scenes.flat_scene(desc)
+    assert flat.textured and len(flat.textures) == len(desc.textures)
+    assert (flat.flatten_uvs() == desc.flatten_uvs()).all()
+    p = small_config_params(scene_size_of(desc))
+    a, b = op.Oracle.from_scene(desc, W, H, p), op.Oracle.from_scene(flat, W, H, p)
+    oa, ob = np.zeros((H, W, 3), np.float32), np.zeros((H, W, 3), np.float32)
+    a.render_frame(cam, oa)
+    b.render_frame(cam, ob)
+    assert oa.tobytes() == ob.tobytes()
