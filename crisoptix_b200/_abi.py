@@ -212,6 +212,8 @@ ENTRY_POINTS = {
     "crisb_abi_sizes": (c_i32, [ctypes.POINTER(c_u32), c_u32]),
     "crisb_endpoint_search": (c_i32, [c_vp, c_u32, c_vp, c_u32, c_u32, c_vp, c_vp, c_vp]),
     "crisb_endpoint_search_noalloc": (c_i32, [c_vp, c_u32, c_vp, c_u32, c_u32, c_vp, c_vp, c_vp]),
+    "crisb_endpoint_search_status": (c_i32, [c_vp]),
+    "crisb_endpoint_search_set_visit_cap": (c_i32, [c_u32]),
 }
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libcrisb.so")

@@ -14,7 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libcrisb.so")
-SOURCES = ["api.cu", "passes.cu", "search.cu", "reuse_passes.cu", "wavefront.cu", "bvh_build.cpp", "adjoint.cu", "tonemap.cu"]
+SOURCES = ["api.cu", "passes.cu", "search.cu", "reuse_passes.cu", "wavefront.cu", "bvh_build.cpp", "adjoint.cu", "tonemap.cu",
+           "context.cpp"]
 
 
 def nvcc_path() -> str:
@@ -37,24 +38,50 @@ def needs_build() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not needs_build():
-        return OUT
-    cmd = [
-        nvcc_path(), "-ccbin", host_cxx(), "-std=c++17", "-O3", "-lineinfo",
+def _flags() -> list:
+    return [
+        "-ccbin", host_cxx(), "-std=c++17", "-O3", "-lineinfo",
         "-gencode", "arch=compute_100a,code=sm_100a",
         "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
         "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",
-        "-Xptxas", "-v" if verbose else "-O3",
-        "-shared", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
-        "-o", OUT + ".tmp",
-    ] + [os.path.join(CSRC, s) for s in SOURCES]
-    r = subprocess.run(cmd, capture_output=True, text=True)
+        "-I", os.path.join(ROOT, "include"), "-I", CSRC,
+    ]
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every source to an object in parallel, then link the shared
+    library.  Objects go to a build folder beside the sources."""
+    if not force and not needs_build():
+        return OUT
+    from concurrent.futures import ThreadPoolExecutor
+
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    nvcc = nvcc_path()
+
+    def compile_one(src: str):
+        obj = os.path.join(objdir, src + ".o")
+        cmd = [nvcc] + _flags() + ["-Xptxas", "-v" if verbose else "-O3", "-c", os.path.join(CSRC, src),
+                                   "-o", obj]
+        return subprocess.run(cmd, capture_output=True, text=True), obj
+
+    with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 4)) as ex:
+        results = list(ex.map(compile_one, SOURCES))
+    failed = False
+    for r, _ in results:
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            failed = True
+        elif verbose:
+            sys.stderr.write(r.stderr)
+    if failed:
+        raise RuntimeError("nvcc failed")
+    link = [nvcc, "-ccbin", host_cxx(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
+            "-o", OUT + ".tmp"] + [o for _, o in results]
+    r = subprocess.run(link, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed")
-    if verbose:
-        sys.stderr.write(r.stderr)
+        raise RuntimeError("nvcc link failed")
     os.replace(OUT + ".tmp", OUT)
     return OUT
 

@@ -56,8 +56,11 @@ RT_D void knn_error(int* err, int code) {
     if (err) atomicOr(err, code);
 }
 
-// The k (<= CRISB_MAX_GATHER_M) nearest entries whose radius covers q.
-RT_D void knn_query(const KnnView& v, int* err, V3 q, uint32_t k, NeighborList& nl) {
+// The k (<= CRISB_MAX_GATHER_M) nearest entries whose radius covers q.  A
+// query that visits more than max_visits nodes stops with the neighbours found
+// so far and sets kDevErrKnn in *err.
+RT_D void knn_query(const KnnView& v, int* err, V3 q, uint32_t k, NeighborList& nl,
+                    uint32_t max_visits = kKnnMaxVisits) {
     nl.count = 0;
     const uint32_t n = *v.n;
     if (n == 0 || k == 0 || nonfinite(q)) return;
@@ -66,7 +69,7 @@ RT_D void knn_query(const KnnView& v, int* err, V3 q, uint32_t k, NeighborList& 
     int cur = 0;
     uint32_t visits = 0;
     while (true) {
-        if (++visits > kKnnMaxVisits) {
+        if (++visits > max_visits) {
             knn_error(err, kDevErrKnn);
             return;
         }

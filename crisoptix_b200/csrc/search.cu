@@ -4,10 +4,14 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <utility>
+#include <vector>
 
+#include "context.h"
 #include "knn.cuh"
 
 namespace crisb {
@@ -164,12 +168,20 @@ __global__ void k_leaves(const float4* entries, lbvh::Work w, float4* leaf) {
     w.leaf_box[i] = entry_box(e);
 }
 
-__global__ void k_query(KnnView v, int* err, const float* queries, uint32_t n_queries, uint32_t k,
+// Device error word of the standalone searches: the kDevErr* bits of every
+// query that stopped early since the word was last read.  Each CUDA context
+// that loads the library has its own copy, zero at load.
+__device__ int g_search_err;
+
+// visit cap per query; 0 selects kKnnMaxVisits (set only by tests)
+std::atomic<uint32_t> g_visit_cap{0};
+
+__global__ void k_query(KnnView v, const float* queries, uint32_t n_queries, uint32_t k, uint32_t max_visits,
                         crisb_neighbor_rec* out, uint32_t* count) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n_queries) return;
     NeighborList nl;
-    knn_query(v, err, V3{queries[3 * q], queries[3 * q + 1], queries[3 * q + 2]}, k, nl);
+    knn_query(v, &g_search_err, V3{queries[3 * q], queries[3 * q + 1], queries[3 * q + 2]}, k, nl, max_visits);
     for (uint32_t j = 0; j < k; ++j) {
         crisb_neighbor_rec r;
         r.pixel = j < nl.count ? nl.pix[j] : 0u;
@@ -195,7 +207,9 @@ inline cudaError_t run(const Scratch& s, const float4* entries, uint32_t n_entri
     launch_lbvh_hierarchy(s.w, std::max<uint32_t>(n_entries, 1), kLeafMax, st);
     if (n_queries > 0) {
         const KnnView v{s.w.nodes, s.leaf, s.w.order, s.w.n};
-        k_query<<<grid(n_queries), kBlock, 0, st>>>(v, s.w.err, queries, n_queries, k, out, count);
+        const uint32_t cap = g_visit_cap.load(std::memory_order_relaxed);
+        k_query<<<grid(n_queries), kBlock, 0, st>>>(v, queries, n_queries, k, cap ? cap : kKnnMaxVisits, out,
+                                                    count);
     }
     return cudaGetLastError();
 }
@@ -213,6 +227,10 @@ inline int validate(const float* entries, uint32_t n_entries, const float* queri
     if (n_entries >= (1u << 31)) return fail(CRISB_ERR_INVALID_ARGUMENT, "endpoint search: too many entries");
     if (reinterpret_cast<uintptr_t>(entries) % 16 != 0)
         return fail(CRISB_ERR_INVALID_ARGUMENT, "endpoint search: entries must be 16-byte aligned");
+    if (reinterpret_cast<uintptr_t>(out) % alignof(crisb_neighbor_rec) != 0 ||
+        reinterpret_cast<uintptr_t>(count) % alignof(uint32_t) != 0 ||
+        reinterpret_cast<uintptr_t>(queries) % alignof(float) != 0)
+        return fail(CRISB_ERR_INVALID_ARGUMENT, "endpoint search: misaligned queries, out or count array");
     return CRISB_OK;
 }
 
@@ -249,38 +267,42 @@ extern "C" int crisb_endpoint_search(const float* entries_dev, uint32_t n_entrie
 // Scratch for crisb_endpoint_search_noalloc: one static device array that
 // every GPU loading this library holds until the process exits.  Host code
 // only sees a stand-in symbol for it; its device address comes from
-// cudaGetSymbolAddress, looked up once per device.
+// cudaGetSymbolAddress, looked up once per CUDA context (an address is only
+// valid in the context it was looked up in).
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = 8u << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mutex;
-void* g_noalloc_base[kMaxDevices] = {};
+std::vector<std::pair<unsigned long long, void*>> g_noalloc_base;  // (context id, address)
 
-// device address of the scratch array on the current device (first call per
-// device does the lookup and checks that the largest accepted search fits)
+// device address of the scratch array in the current context (the first call
+// in a context does the lookup and checks that the largest accepted search
+// fits)
 int noalloc_scratch(void** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return search::fail(CRISB_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxDevices) return search::fail(CRISB_ERR_NOT_SUPPORTED, "device ordinal out of range");
+    unsigned long long ctx = 0;
+    cudaError_t e = current_context_id(&ctx);
+    if (e != cudaSuccess)
+        return search::fail(CRISB_ERR_CUDA, std::string("endpoint search (no-alloc): no current context: ") +
+                                                cudaGetErrorString(e));
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_base[dev]) {
-        const size_t need = search::layout(CRISB_NOALLOC_MAX_ENTRIES,
-                                           search::sort_temp_bytes(CRISB_NOALLOC_MAX_ENTRIES), nullptr, nullptr);
-        if (need > kNoAllocScratchBytes)
-            return search::fail(CRISB_ERR_NOT_SUPPORTED, "endpoint search (no-alloc): scratch array too small");
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return search::fail(CRISB_ERR_CUDA,
-                                std::string("endpoint search (no-alloc): cudaGetSymbolAddress: ") +
-                                    cudaGetErrorString(e));
-        g_noalloc_base[dev] = p;
-    }
-    *out = g_noalloc_base[dev];
+    for (const auto& b : g_noalloc_base)
+        if (b.first == ctx) {
+            *out = b.second;
+            return CRISB_OK;
+        }
+    const size_t need = search::layout(CRISB_NOALLOC_MAX_ENTRIES, search::sort_temp_bytes(CRISB_NOALLOC_MAX_ENTRIES),
+                                       nullptr, nullptr);
+    if (need > kNoAllocScratchBytes)
+        return search::fail(CRISB_ERR_NOT_SUPPORTED, "endpoint search (no-alloc): scratch array too small");
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return search::fail(CRISB_ERR_CUDA,
+                            std::string("endpoint search (no-alloc): cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_noalloc_base.emplace_back(ctx, p);
+    *out = p;
     return CRISB_OK;
 }
 
@@ -307,5 +329,29 @@ extern "C" int crisb_endpoint_search_noalloc(const float* entries_dev, uint32_t 
                                       n_queries, k, out_dev, count_dev, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess)
         return search::fail(CRISB_ERR_CUDA, std::string("endpoint search (no-alloc): ") + cudaGetErrorString(e));
+    return CRISB_OK;
+}
+
+extern "C" int crisb_endpoint_search_status(void* stream) {
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int word = 0;
+    static const int zero = 0;
+    cudaError_t e = cudaMemcpyFromSymbolAsync(&word, search::g_search_err, sizeof word, 0, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbolAsync(search::g_search_err, &zero, sizeof zero, 0,
+                                                      cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+        return search::fail(CRISB_ERR_CUDA, std::string("endpoint search status: ") + cudaGetErrorString(e));
+    if (word != 0)
+        return search::fail(CRISB_ERR_DEVICE_FAULT,
+                            std::string("endpoint search: a query stopped early (") +
+                                ((word & kDevErrKnn) ? "visit cap" : "") +
+                                ((word & kDevErrKnn) && (word & kDevErrStack) ? ", " : "") +
+                                ((word & kDevErrStack) ? "stack depth" : "") + "); its neighbour list is incomplete");
+    return CRISB_OK;
+}
+
+extern "C" int crisb_endpoint_search_set_visit_cap(uint32_t max_visits) {
+    search::g_visit_cap.store(max_visits, std::memory_order_relaxed);
     return CRISB_OK;
 }

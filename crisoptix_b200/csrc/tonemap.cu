@@ -12,9 +12,12 @@
 // operations per channel and would make this copy-shaped kernel FP64-bound.
 // The host finds, once, the smallest float T[k] with srgb8(T[k]) >= k for
 // k = 1..255 by bisection over float bit patterns, checks both sides of every
-// step, and the kernel finds the count of thresholds at or below c from a
-// fast single-precision guess corrected against a shared-memory copy of the
-// table (srgb8_lookup).  The bytes are the formula's by construction.
+// step, and files the steps into 1665 buckets of float bit patterns (one
+// exponent and 7 leading mantissa bits each) so that no bucket holds more
+// than one step.  A bucket stores the byte at its start and the bit pattern of
+// its step; the kernel copies the buckets to shared memory and finds a
+// channel's byte with one bucket load and one integer compare
+// (srgb8_lookup).  The bytes are the formula's by construction.
 //
 // Memory: 12 bytes read and 3 written per pixel.  Each thread takes four
 // pixels (three 16-byte loads, three 4-byte stores) when both pointers are
@@ -24,7 +27,10 @@
 #include <cstring>
 #include <mutex>
 #include <stdexcept>
+#include <utility>
+#include <vector>
 
+#include "context.h"
 #include "passes.cuh"
 
 namespace crisb {
@@ -162,25 +168,28 @@ __global__ void __launch_bounds__(kToneBlock) k_tonemap_srgb8(const float* __res
     }
 }
 
-// the bucket table in device memory, uploaded once per device (13 KB) and
-// kept for the life of the process: no handle owns it, and a table freed while
-// a caller's stream still runs a tone-mapping kernel would be read after free
-const uint2* device_table(int dev) {
+// the bucket table in device memory, uploaded once per CUDA context (13 KB)
+// and kept for the life of that context: no handle owns it, and a table freed
+// while a caller's stream still runs a tone-mapping kernel would be read after
+// free.  Keyed by context id (context.h), so a context created after a
+// cudaDeviceReset, or a caller's own context, gets a table of its own.
+const uint2* device_table() {
     static std::mutex mu;
-    static const uint2* tables[64] = {};
+    static std::vector<std::pair<unsigned long long, const uint2*>> tables;
+    unsigned long long ctx = 0;
+    if (current_context_id(&ctx) != cudaSuccess) throw std::runtime_error("no current CUDA context");
     std::lock_guard<std::mutex> lock(mu);
-    if (dev < 0 || dev >= 64) throw std::runtime_error("device index out of range");
-    if (!tables[dev]) {
-        void* p = nullptr;
-        const SrgbTable& tab = srgb_table();
-        if (cudaMalloc(&p, sizeof tab.bucket) != cudaSuccess) throw std::runtime_error("sRGB table allocation");
-        if (cudaMemcpy(p, tab.bucket, sizeof tab.bucket, cudaMemcpyHostToDevice) != cudaSuccess) {
-            cudaFree(p);
-            throw std::runtime_error("sRGB table upload");
-        }
-        tables[dev] = static_cast<const uint2*>(p);
+    for (const auto& t : tables)
+        if (t.first == ctx) return t.second;
+    void* p = nullptr;
+    const SrgbTable& tab = srgb_table();
+    if (cudaMalloc(&p, sizeof tab.bucket) != cudaSuccess) throw std::runtime_error("sRGB table allocation");
+    if (cudaMemcpy(p, tab.bucket, sizeof tab.bucket, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(p);
+        throw std::runtime_error("sRGB table upload");
     }
-    return tables[dev];
+    tables.emplace_back(ctx, static_cast<const uint2*>(p));
+    return tables.back().second;
 }
 
 // blocks of the kernel resident on the whole device at once
@@ -209,10 +218,7 @@ cudaError_t launch_tonemap_srgb8(const float* rgb, uint8_t* out, uint32_t n, cud
     const uint32_t work = quads + (n - 4 * quads);
     static const unsigned cap = tone_grid_cap();
     const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((work + kToneBlock - 1) / kToneBlock, cap));
-    int dev = 0;
-    const cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    k_tonemap_srgb8<<<grid, kToneBlock, 0, st>>>(rgb, out, n, quads, device_table(dev),
+    k_tonemap_srgb8<<<grid, kToneBlock, 0, st>>>(rgb, out, n, quads, device_table(),
                                                  float_bits(srgb_table().c_max));
     return cudaGetLastError();
 }

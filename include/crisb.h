@@ -410,12 +410,28 @@ int crisb_trace_rays(const crisb_scene* scene, const float* rays_dev,
  * queries_dev: n_queries float triples.  For query q, out_dev[q*k .. q*k+k)
  * receives the k nearest entries j with |p_j - q| <= radius_j, ordered by
  * (distance, entry index), unused slots zeroed; count_dev[q] their number.
- * k in [1, 31].  Scratch comes from the stream-ordered allocator
- * (cudaMallocAsync / cudaFreeAsync on `stream`); the call is asynchronous. */
+ * k in [1, 31].  out_dev must be 8-byte and count_dev 4-byte aligned.
+ * Scratch comes from the stream-ordered allocator (cudaMallocAsync /
+ * cudaFreeAsync on `stream`); the call is asynchronous.  A query that hits
+ * the traversal's visit cap or stack depth keeps the neighbours found so far
+ * and marks the search error word, which crisb_endpoint_search_status reads
+ * (the reference's OptiX query has no such cap and reports nothing). */
 int crisb_endpoint_search(const float* entries_dev, uint32_t n_entries,
                           const float* queries_dev, uint32_t n_queries,
                           uint32_t k, crisb_neighbor_rec* out_dev,
                           uint32_t* count_dev, void* stream);
+
+/* Reads and clears the error word of crisb_endpoint_search and
+ * crisb_endpoint_search_noalloc for the current CUDA context: synchronises
+ * `stream`, then returns CRISB_OK when no query stopped early since the last
+ * read, else CRISB_ERR_DEVICE_FAULT (message via crisb_last_error).  Calls no
+ * allocator.  The renderer's own searches report through
+ * crisb_check_device_errors instead. */
+int crisb_endpoint_search_status(void* stream);
+
+/* Test hook: caps the node visits of each standalone search query at
+ * max_visits (0 restores the default cap of 2^21).  Process-wide. */
+int crisb_endpoint_search_set_visit_cap(uint32_t max_visits);
 
 /* Largest n_entries crisb_endpoint_search_noalloc accepts. */
 #define CRISB_NOALLOC_MAX_ENTRIES 32768u
@@ -432,9 +448,11 @@ int crisb_endpoint_search(const float* entries_dev, uint32_t n_entries,
  * share that array (it keeps the last call's contents; each call clears what
  * it needs), so calls that overlap on the GPU -- on different streams, or
  * from different host threads -- race and corrupt each other's results:
- * serialise them.  The first call on each device looks up the array's device
- * address (cudaGetSymbolAddress); make that first call before any stream
- * capture. */
+ * serialise them.  The first call in each CUDA context looks up the array's
+ * device address there (cudaGetSymbolAddress) and keeps it for that context
+ * (keyed by the context's id, so a context made after cudaDeviceReset, or a
+ * caller's own context, does its own lookup); make that first call before
+ * any stream capture. */
 int crisb_endpoint_search_noalloc(const float* entries_dev, uint32_t n_entries,
                                   const float* queries_dev, uint32_t n_queries,
                                   uint32_t k, crisb_neighbor_rec* out_dev,

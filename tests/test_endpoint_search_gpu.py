@@ -67,6 +67,47 @@ def test_endpoint_search_matches_brute_force(cuda_device, k):
     assert (gc == rc).all()
     assert got.tobytes() == ref.tobytes()
     assert rc.max() == k and (rc == 0).any()
+    assert _abi.load().crisb_endpoint_search_status(None) == _abi.OK
+
+
+@pytest.mark.parametrize("fn", ["crisb_endpoint_search", "crisb_endpoint_search_noalloc"])
+def test_capped_query_reports_device_error(cuda_device, fn):
+    """A query that runs out of node visits keeps a partial list and the
+    status call reports it (a bounded loop that gives up, not a fault); the
+    word is cleared by reading it."""
+    lib = _abi.load()
+    entries, queries = make_case(7, n_entries=6000, n_queries=500)
+    try:
+        lib.crisb_endpoint_search_set_visit_cap(3)
+        got, gc = gpu_search(entries, queries, 8, fn)
+        rc = lib.crisb_endpoint_search_status(None)
+        buf = ctypes.create_string_buffer(256)
+        lib.crisb_last_error(buf, 256)
+    finally:
+        lib.crisb_endpoint_search_set_visit_cap(0)
+    assert rc == _abi.ERR_DEVICE_FAULT and b"visit cap" in buf.value
+    assert lib.crisb_endpoint_search_status(None) == _abi.OK  # read clears it
+    ref, refc = brute_force(entries, queries, 8)
+    assert (gc <= refc).all() and gc.sum() < refc.sum()
+    got2, gc2 = gpu_search(entries, queries, 8, fn)
+    assert lib.crisb_endpoint_search_status(None) == _abi.OK
+    assert (gc2 == refc).all() and got2.tobytes() == ref.tobytes()
+
+
+def test_misaligned_outputs_rejected(cuda_device):
+    lib = _abi.load()
+    e = torch.zeros((4, 4), dtype=torch.float32, device="cuda")
+    q = torch.zeros((2, 3), dtype=torch.float32, device="cuda")
+    out = torch.zeros(64, dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(8, dtype=torch.int32, device="cuda")
+    for fn in ("crisb_endpoint_search", "crisb_endpoint_search_noalloc"):
+        f = getattr(lib, fn)
+        rc = f(ctypes.c_void_p(e.data_ptr()), 4, ctypes.c_void_p(q.data_ptr()), 2, 4,
+               ctypes.c_void_p(out.data_ptr() + 4), ctypes.c_void_p(cnt.data_ptr()), None)
+        assert rc == _abi.ERR_INVALID_ARGUMENT
+        rc = f(ctypes.c_void_p(e.data_ptr()), 4, ctypes.c_void_p(q.data_ptr()), 2, 4,
+               ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(cnt.data_ptr() + 2), None)
+        assert rc == _abi.ERR_INVALID_ARGUMENT
 
 
 def test_endpoint_search_edge_cases(cuda_device):
