@@ -214,6 +214,7 @@ ENTRY_POINTS = {
     "crisb_endpoint_search_noalloc": (c_i32, [c_vp, c_u32, c_vp, c_u32, c_u32, c_vp, c_vp, c_vp]),
     "crisb_endpoint_search_status": (c_i32, [c_vp]),
     "crisb_endpoint_search_set_visit_cap": (c_i32, [c_u32]),
+    "crisb_selftest_kat": (c_i32, [c_i32, c_vp, c_u32, c_vp, c_vp]),
 }
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libcrisb.so")

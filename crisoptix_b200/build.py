@@ -15,7 +15,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libcrisb.so")
 SOURCES = ["api.cu", "passes.cu", "search.cu", "reuse_passes.cu", "wavefront.cu", "bvh_build.cpp", "adjoint.cu", "tonemap.cu",
-           "context.cpp"]
+           "context.cpp", "selftest.cu"]
 
 
 def nvcc_path() -> str:

@@ -444,6 +444,10 @@ RT_D V3 shift_suffix(const SceneView& s, const Suffix& src, const Suffix& dst, f
     return shift_suffix(s, src, dst_last, jac);
 }
 
+// SpawnCameraRay's direction (include/graph/Camera.h:14-22) at viewport
+// coordinates (ux, uy)
+RT_D V3 spawn_camera_dir(V3 U, V3 V, V3 W, float ux, float uy) { return normalize(U * ux + V * uy + W); }
+
 // jittered camera ray of the pixel (prefix_gen_temp_reuse.cu:124-126); the x
 // jitter is drawn before the y jitter.
 RT_D V3 camera_dir(const FrameParams& fp, uint32_t x, uint32_t y, Rng& rng) {
@@ -453,8 +457,7 @@ RT_D V3 camera_dir(const FrameParams& fp, uint32_t x, uint32_t y, Rng& rng) {
     float uy = (static_cast<float>(y) + jy) / static_cast<float>(fp.height);
     ux = 2.0f * ux - 1.0f;
     uy = 2.0f * uy - 1.0f;
-    const V3 U = ld3(fp.cam.u), V = ld3(fp.cam.v), W = ld3(fp.cam.w);
-    return normalize(U * ux + V * uy + W);
+    return spawn_camera_dir(ld3(fp.cam.u), ld3(fp.cam.v), ld3(fp.cam.w), ux, uy);
 }
 
 }  // namespace crisb

@@ -590,6 +590,19 @@ int crisb_debug_size(const crisb_renderer* r, int buffer_id, size_t* out);
  * Writes up to n values; returns the number of structs. */
 int crisb_abi_sizes(uint32_t* out, uint32_t n);
 
+/* Test hook: evaluates the library's device implementation of one unit-level
+ * function of the reference on n packed records in device memory (record
+ * layouts and function ids as in the project's oracle/kat.h: SampleTEA64,
+ * PCG32 seeding and draws, GetLuminance, the two pairwise MIS weights,
+ * SelectSpatialNeighbor, CalcReconnectionJacobian, Reservoir::Update +
+ * FinalizeGRIS, D_GGX / V_SmithJointGGX / FresnelSchlick, SpawnCameraRay),
+ * so tests can hold them to known answers of the reference's own code.
+ * PCG32 records outside the default stream are answered with all words set
+ * (the library's generator runs the default stream only, as the reference
+ * uses it).  Asynchronous on `stream`. */
+int crisb_selftest_kat(int fn, const void* in_dev, uint32_t n, void* out_dev,
+                       void* stream);
+
 #ifdef __cplusplus
 }
 #endif

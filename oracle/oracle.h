@@ -82,6 +82,12 @@ void oracle_sincos(const float* phi, uint32_t n, float* s, float* c);
 int oracle_camera_data(const crisb_camera* cam, crisb_camera_data* out);
 uint32_t oracle_frame_random_for(uint64_t seed, uint64_t frame_counter);
 
+/* known-answer-test hooks: function `fn` of kat.h on n packed records, and
+ * SampleEmitter over the given emitters (out: point, colour per draw) */
+int oracle_kat(int fn, const void* in, uint32_t n, void* out);
+int oracle_kat_emitter(const crisb_emitter* ems, uint32_t num_emitters, const float* faces,
+                       const uint64_t* states, uint32_t n, float* out, uint64_t* state_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,7 +24,7 @@ _lib = None
 
 
 def build(force: bool = False) -> str:
-    srcs = [os.path.join(HERE, f) for f in ("restir_oracle.cpp", "oracle.h", "Makefile")]
+    srcs = [os.path.join(HERE, f) for f in ("restir_oracle.cpp", "oracle.h", "kat.h", "Makefile")]
     srcs.append(os.path.join(ROOT, "include", "crisb.h"))
     if force or not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs):
         subprocess.run(["make", "-s", "-B" if force else "-s", "-C", HERE], check=True)
@@ -58,6 +58,8 @@ def load():
         "oracle_pt_accumulate": (i32, [vp, ctypes.POINTER(_abi.Camera), u32, u64, vp]),
         "oracle_pcg32": (None, [u64, u64, u32, vp]),
         "oracle_tea64": (u64, [u32, u32]),
+        "oracle_kat": (i32, [i32, vp, u32, vp]),
+        "oracle_kat_emitter": (i32, [vp, u32, vp, vp, u32, vp, vp]),
         "oracle_sincos": (None, [vp, u32, vp, vp]),
         "oracle_half": (None, [vp, u32, vp, vp]),
         "oracle_srgb_root": (None, [vp, u32, vp]),

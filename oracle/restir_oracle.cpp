@@ -7,14 +7,21 @@
  * the product never links it, and only tests/, __graft_entry__.smoke() and
  * bench.py's CPU-baseline leg load it.
  *
- * Parity status: the reference cannot be built or run here (it needs the
- * OptiX SDK and glm, neither is installed, and ships no tests or golden
- * vectors), so this restatement is NOT pinned against reference outputs
- * ("parity unpinned").  What is pinned: PCG32 against the published pcg32
- * demo sequence (tests/test_oracle_kat.py).  Everything else follows the
+ * Parity status: the reference application cannot be built or run here (it
+ * needs the OptiX SDK and an OpenGL window) and ships no tests or golden
+ * vectors.  Its unit-level device code can: oracle/Makefile `ref` compiles
+ * the reference's own headers unmodified (random.h, luminance.h,
+ * Reservoir.h, Camera.h, sample_emitter.h, and path_gen.h:12-72,
+ * Emitter.h:6-55, brdf.cu:12-37/99-112 cut from files whose rest needs OptiX)
+ * against a minimal glm (oracle/ref_shim), and tests/golden/ref_kat.npz
+ * records its answers.  This restatement matches them bit for bit (TEA,
+ * PCG32 seeding and draws, luminance, both pairwise MIS weights,
+ * SelectSpatialNeighbor, the reconnection Jacobian, Reservoir::Update /
+ * FinalizeGRIS sequences, D_GGX, V_SmithJointGGX, SpawnCameraRay, emitter
+ * sampling), FresnelSchlick within 4 ulp (pow below); tests/test_ref_kat.py.
+ * Above that level (traversal, the pass chain) the restatement follows the
  * cited reference lines; where the reference is non-deterministic or leans on
- * OptiX internals the restatement fixes a deterministic definition, marked
- * DEFINED below:
+ * OptiX internals it fixes a deterministic definition, marked DEFINED below:
  *   - optixTrace: own BVH + watertight ray/triangle test (Woop, Benthin &
  *     Wald 2013), closest hit = smallest t, ties -> lower triangle index;
  *     a hit counts when tmin < t < tmax.
@@ -32,6 +39,7 @@
  *     the interaction already in hand, so it is not re-traced.
  */
 #include "oracle.h"
+#include "kat.h"
 
 #include <omp.h>
 
@@ -922,6 +930,42 @@ inline void SpawnCameraRay(const CameraData& cam, vec2 vp, vec3& origin, vec3& d
     dir = normalize(cam.U * vp.x + cam.V * vp.y + cam.W);
 }
 
+// SampleEmitter, sample_emitter.h:3-12 + EmitterData::SamplePoint, Emitter.h:21-54
+inline EmitterSample SampleEmitterFrom(const std::vector<EmitterData>& emitters, PCG32& rng) {
+    const size_t emitterCount = emitters.size();
+    const size_t emitterIdx = rng.NextUint64() % emitterCount;
+    const EmitterData& e = emitters[emitterIdx];
+    const size_t faceCount = e.faces.size() / 3;
+    const size_t faceIdx = rng.NextUint64() % faceCount;
+    const vec3 v0 = e.faces[faceIdx * 3 + 0];
+    const vec3 v1 = e.faces[faceIdx * 3 + 1];
+    const vec3 v2 = e.faces[faceIdx * 3 + 2];
+    float r0 = rng.NextFloat();
+    float r1 = rng.NextFloat();
+    float r2 = rng.NextFloat();
+    const float rSum = r0 + r1 + r2;
+    r0 /= rSum;
+    r1 /= rSum;
+    r2 /= rSum;
+    const vec3 point = r0 * v0 + r1 * v1 + r2 * v2;
+    return {point, e.color, 1.0f};
+}
+
+// SelectSpatialNeighbor, path_gen.h:50-57, with the window radius R as a
+// parameter (the reference's WINDOW_RADIUS = 10, path_gen.h:12)
+inline void SelectSpatialNeighborR(uint32_t px, uint32_t py, uint32_t R, PCG32& rng, uint32_t& nx, uint32_t& ny) {
+    const uint32_t WS = 2 * R + 1;
+    const uint32_t x = (px + R) - (rng.NextUint32() % WS);
+    const uint32_t y = (py + R) - (rng.NextUint32() % WS);
+    if (x == px && y == py) {
+        nx = px + 1;
+        ny = py + 1;
+        return;
+    }
+    nx = x;
+    ny = y;
+}
+
 // ---------------------------------------------------------------------------
 // The renderer state and passes
 // ---------------------------------------------------------------------------
@@ -1088,26 +1132,7 @@ struct oracle_ctx {
         return FinishMat(m, diff, f0, rough);
     }
 
-    // SampleEmitter, sample_emitter.h:3-12 + EmitterData::SamplePoint, Emitter.h:21-54
-    EmitterSample SampleEmitter(PCG32& rng) const {
-        const size_t emitterCount = scene.emitters.size();
-        const size_t emitterIdx = rng.NextUint64() % emitterCount;
-        const EmitterData& e = scene.emitters[emitterIdx];
-        const size_t faceCount = e.faces.size() / 3;
-        const size_t faceIdx = rng.NextUint64() % faceCount;
-        const vec3 v0 = e.faces[faceIdx * 3 + 0];
-        const vec3 v1 = e.faces[faceIdx * 3 + 1];
-        const vec3 v2 = e.faces[faceIdx * 3 + 2];
-        float r0 = rng.NextFloat();
-        float r1 = rng.NextFloat();
-        float r2 = rng.NextFloat();
-        const float rSum = r0 + r1 + r2;
-        r0 /= rSum;
-        r1 /= rSum;
-        r2 /= rSum;
-        const vec3 point = r0 * v0 + r1 * v1 + r2 * v2;
-        return {point, e.color, 1.0f};
-    }
+    EmitterSample SampleEmitter(PCG32& rng) const { return SampleEmitterFrom(scene.emitters, rng); }
 
     bool IsPixelValid(uint32_t x, uint32_t y) const { return x < width && y < height; }
 
@@ -1165,19 +1190,8 @@ struct oracle_ctx {
         }
         return w;
     }
-    // SelectSpatialNeighbor, path_gen.h:50-57 (radius from params)
     void SelectSpatialNeighbor(uint32_t px, uint32_t py, PCG32& rng, uint32_t& nx, uint32_t& ny) const {
-        const uint32_t R = static_cast<uint32_t>(params.window_radius);
-        const uint32_t WS = 2 * R + 1;
-        const uint32_t x = (px + R) - (rng.NextUint32() % WS);
-        const uint32_t y = (py + R) - (rng.NextUint32() % WS);
-        if (x == px && y == py) {
-            nx = px + 1;
-            ny = py + 1;
-            return;
-        }
-        nx = x;
-        ny = y;
+        SelectSpatialNeighborR(px, py, static_cast<uint32_t>(params.window_radius), rng, nx, ny);
     }
     // CalcReconnectionJacobian, path_gen.h:59-72
     static float ReconJacobian(vec3 oldXi, vec3 newXi, vec3 targetPos, vec3 targetNormal) {
@@ -2610,5 +2624,157 @@ int oracle_camera_data(const crisb_camera* cam, crisb_camera_data* out) {
 }
 
 uint32_t oracle_frame_random_for(uint64_t seed, uint64_t frame_counter) { return FrameRandom(seed, frame_counter); }
+
+/* known-answer-test hooks (kat.h): the oracle's own unit-level functions */
+namespace {
+uint64_t KatGet64(const uint32_t* w) { return static_cast<uint64_t>(w[0]) | (static_cast<uint64_t>(w[1]) << 32); }
+void KatPut64(uint32_t* w, uint64_t v) {
+    w[0] = static_cast<uint32_t>(v);
+    w[1] = static_cast<uint32_t>(v >> 32);
+}
+float KatGetF(const uint32_t* w) {
+    float f;
+    std::memcpy(&f, w, 4);
+    return f;
+}
+void KatPutF(uint32_t* w, float f) { std::memcpy(w, &f, 4); }
+vec3 KatGet3(const uint32_t* w) { return vec3(KatGetF(w), KatGetF(w + 1), KatGetF(w + 2)); }
+void KatPut3(uint32_t* w, vec3 v) {
+    KatPutF(w, v.x);
+    KatPutF(w + 1, v.y);
+    KatPutF(w + 2, v.z);
+}
+PCG32 KatRng(const uint32_t* w) {
+    PCG32 r;
+    r.state = KatGet64(w);
+    r.inc = KatGet64(w + 2);
+    return r;
+}
+struct KatSample {
+    vec3 f;
+    uint32_t id = 0;
+};
+
+void KatEval(int fn, const uint32_t* in, uint32_t* out) {
+    switch (fn) {
+        case KAT_TEA64:
+            KatPut64(out, SampleTEA64(in[0], in[1]));
+            break;
+        case KAT_PCG_SEED: {
+            const PCG32 r(KatGet64(in), KatGet64(in + 2));
+            KatPut64(out, r.state);
+            KatPut64(out + 2, r.inc);
+            break;
+        }
+        case KAT_PCG_DRAWS: {
+            PCG32 r = KatRng(in);
+            out[0] = r.NextUint32();
+            KatPutF(out + 1, r.NextFloat());
+            KatPut64(out + 2, r.NextUint64());
+            KatPut64(out + 4, r.state);
+            break;
+        }
+        case KAT_LUMINANCE:
+            KatPutF(out, GetLuminance(KatGet3(in)));
+            break;
+        case KAT_MIS_CANON:
+            KatPutF(out, oracle_ctx::CanonMis(KatGet3(in), KatGet3(in + 3), KatGetF(in + 6), KatGetF(in + 7),
+                                              KatGetF(in + 8), KatGetF(in + 9)));
+            break;
+        case KAT_MIS_NEIGH:
+            KatPutF(out, oracle_ctx::NeighMis(KatGet3(in), KatGet3(in + 3), KatGetF(in + 6), KatGetF(in + 7),
+                                              KatGetF(in + 8), KatGetF(in + 9)));
+            break;
+        case KAT_SELECT_NEIGHBOR: {
+            PCG32 r = KatRng(in + 2);
+            SelectSpatialNeighborR(in[0], in[1], 10u, r, out[0], out[1]);
+            KatPut64(out + 2, r.state);
+            break;
+        }
+        case KAT_JACOBIAN:
+            KatPutF(out, oracle_ctx::ReconJacobian(KatGet3(in), KatGet3(in + 3), KatGet3(in + 6), KatGet3(in + 9)));
+            break;
+        case KAT_RESERVOIR: {
+            PCG32 r = KatRng(in);
+            Reservoir<KatSample> res;
+            res.wSum = KatGetF(in + 4);
+            res.confidence = KatGetF(in + 5);
+            res.sample.f = KatGet3(in + 6);
+            res.sample.id = KAT_RES_STEPS;
+            const uint32_t* c = in + 9;
+            for (uint32_t st = 0; st < KAT_RES_STEPS; ++st, c += 5) {
+                KatSample k;
+                k.f = KatGet3(c + 2);
+                k.id = st;
+                out[3 * st] = res.Update(k, KatGetF(c), r, KatGetF(c + 1)) ? 1u : 0u;
+                KatPutF(out + 3 * st + 1, res.wSum);
+                KatPutF(out + 3 * st + 2, res.confidence);
+            }
+            res.FinalizeGRIS();
+            uint32_t* o = out + 3 * KAT_RES_STEPS;
+            o[0] = res.sample.id;
+            KatPutF(o + 1, res.wSum);
+            KatPut64(o + 2, r.state);
+            break;
+        }
+        case KAT_GGX:
+            KatPutF(out, D_GGX(KatGetF(in), KatGetF(in + 3)));
+            KatPutF(out + 1, V_SmithJointGGX(KatGetF(in + 1), KatGetF(in + 2), KatGetF(in + 3)));
+            KatPut3(out + 2, FresnelSchlick(KatGet3(in + 5), KatGetF(in + 4)));
+            break;
+        case KAT_CAMERA_RAY: {
+            CameraData cd;
+            cd.pos = KatGet3(in);
+            cd.U = KatGet3(in + 3);
+            cd.V = KatGet3(in + 6);
+            cd.W = KatGet3(in + 9);
+            vec3 o, d;
+            vec2 vp;
+            vp.x = KatGetF(in + 12);
+            vp.y = KatGetF(in + 13);
+            SpawnCameraRay(cd, vp, o, d);
+            KatPut3(out, d);
+            break;
+        }
+        default:
+            break;
+    }
+}
+}  // namespace
+
+int oracle_kat(int fn, const void* in, uint32_t n, void* out) {
+    static const int kIn[] = KAT_IN_WORDS;
+    static const int kOut[] = KAT_OUT_WORDS;
+    if (fn < 1 || fn > KAT_NUM_FN) return CRISB_ERR_INVALID_ARGUMENT;
+    const uint32_t* i = static_cast<const uint32_t*>(in);
+    uint32_t* o = static_cast<uint32_t*>(out);
+    for (uint32_t k = 0; k < n; ++k)
+        KatEval(fn, i + static_cast<size_t>(k) * kIn[fn], o + static_cast<size_t>(k) * kOut[fn]);
+    return CRISB_OK;
+}
+
+int oracle_kat_emitter(const crisb_emitter* ems, uint32_t num_emitters, const float* faces, const uint64_t* states,
+                       uint32_t n, float* out, uint64_t* state_out) {
+    if (!ems || num_emitters == 0) return CRISB_ERR_INVALID_ARGUMENT;
+    std::vector<EmitterData> table(num_emitters);
+    for (uint32_t e = 0; e < num_emitters; ++e) {
+        table[e].color = vec3(ems[e].color[0], ems[e].color[1], ems[e].color[2]);
+        for (uint32_t f = 0; f < ems[e].num_faces; ++f)
+            for (int c = 0; c < 3; ++c) {
+                const float* v = faces + 9 * (static_cast<size_t>(ems[e].first_face) + f) + 3 * c;
+                table[e].faces.push_back(vec3(v[0], v[1], v[2]));
+            }
+    }
+    for (uint32_t k = 0; k < n; ++k) {
+        PCG32 r;
+        r.state = states[2 * k];
+        r.inc = states[2 * k + 1];
+        const EmitterSample s = SampleEmitterFrom(table, r);
+        const float v[6] = {s.pos.x, s.pos.y, s.pos.z, s.color.x, s.color.y, s.color.z};
+        std::memcpy(out + 6 * static_cast<size_t>(k), v, sizeof v);
+        state_out[k] = r.state;
+    }
+    return CRISB_OK;
+}
 
 }  // extern "C"
