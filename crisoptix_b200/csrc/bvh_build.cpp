@@ -212,6 +212,7 @@ struct Builder {
 struct Collapser {
     const std::vector<BinNode>& bin;
     std::vector<Bvh4Node>& out;
+    float margin;  // widening of every emitted child box (box_margin)
     int max_stack = 0;
 
     bool is_leaf(int i) const { return bin[i].left < 0; }
@@ -244,6 +245,7 @@ struct Collapser {
     int emit(int i, uint32_t w) {
         int ch[kBvhWidth], k;
         gather(i, ch, k);
+        const float m = margin;
         Bvh4Node nd;
         int inner = 0;
         for (int c = 0; c < kBvhWidth; ++c) {
@@ -254,12 +256,12 @@ struct Collapser {
         }
         for (int c = 0; c < k; ++c) {
             const Box& bx = bin[ch[c]].box;
-            nd.lo_x[c] = bx.lo[0];
-            nd.lo_y[c] = bx.lo[1];
-            nd.lo_z[c] = bx.lo[2];
-            nd.hi_x[c] = bx.hi[0];
-            nd.hi_y[c] = bx.hi[1];
-            nd.hi_z[c] = bx.hi[2];
+            nd.lo_x[c] = bx.lo[0] - m;
+            nd.lo_y[c] = bx.lo[1] - m;
+            nd.lo_z[c] = bx.lo[2] - m;
+            nd.hi_x[c] = bx.hi[0] + m;
+            nd.hi_y[c] = bx.hi[1] + m;
+            nd.hi_z[c] = bx.hi[2] + m;
             if (is_leaf(ch[c])) {
                 nd.link[c] = -1 - static_cast<int>(bin[ch[c]].first);
                 nd.count[c] = static_cast<int>(bin[ch[c]].count);
@@ -311,7 +313,10 @@ WideBvh build_wide_bvh(const float* pos, uint32_t n, int leaf_max, int median_de
     const uint32_t root = bld.alloc();
     bld.build(root, 0, n, 0);
     r.max_depth = bld.max_depth.load();
-    Collapser col{bin, r.nodes};
+    float max_abs = 0.0f;
+    for (size_t i = 0; i < 9 * static_cast<size_t>(n); ++i) max_abs = std::max(max_abs, std::fabs(pos[i]));
+    const float margin = box_margin(max_abs);
+    Collapser col{bin, r.nodes, margin};
     r.nodes.reserve(bld.next.load() / 2 + 1);
     r.nodes.emplace_back();
     if (bin[root].left < 0) {
@@ -320,12 +325,12 @@ WideBvh build_wide_bvh(const float* pos, uint32_t n, int leaf_max, int median_de
         std::memset(&nd, 0, sizeof(nd));
         for (int c = 0; c < kBvhWidth; ++c) nd.link[c] = kNoChild;
         const Box& bx = bin[root].box;
-        nd.lo_x[0] = bx.lo[0];
-        nd.lo_y[0] = bx.lo[1];
-        nd.lo_z[0] = bx.lo[2];
-        nd.hi_x[0] = bx.hi[0];
-        nd.hi_y[0] = bx.hi[1];
-        nd.hi_z[0] = bx.hi[2];
+        nd.lo_x[0] = bx.lo[0] - margin;
+        nd.lo_y[0] = bx.lo[1] - margin;
+        nd.lo_z[0] = bx.lo[2] - margin;
+        nd.hi_x[0] = bx.hi[0] + margin;
+        nd.hi_y[0] = bx.hi[1] + margin;
+        nd.hi_z[0] = bx.hi[2] + margin;
         nd.link[0] = -1;
         nd.count[0] = static_cast<int>(n);
         r.nodes[0] = nd;

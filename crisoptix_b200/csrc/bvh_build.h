@@ -3,10 +3,16 @@
 // Stands in for the OptiX GAS/IAS build of the reference
 // (src/Scene.cpp:73-160, src/Mesh.cpp:54-120): a binned-SAH binary
 // tree over the flattened triangles, collapsed greedily (largest surface area
-// first) into 4-wide nodes.  Any conservative tree gives the same closest and
-// any hit, so the tree shape only changes speed.
+// first) into 4-wide nodes.  Every child box is widened by box_margin(): the
+// watertight triangle test accepts rays a few ulp of the origin-vertex
+// distance outside the exact triangle (and t to a few ulp), and the slab test
+// cuts a ray lying in a box face plane off at t = 0, so exact boxes can reject
+// a ray the triangle test accepts.  With the margin, the box test is at least
+// an order of magnitude more generous than those errors, every tree gives the
+// hits of testing all triangles, and the tree shape only changes speed.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <vector>
 
@@ -33,6 +39,10 @@ struct alignas(128) Bvh4Node {
 static_assert(sizeof(Bvh4Node) == 32 * kBvhWidth, "node size");
 
 constexpr int kNoChild = 0x7fffffff;
+
+// box widening for a scene whose largest coordinate magnitude is max_abs:
+// 2^-17 x max_abs (rays are taken to start within twice that magnitude)
+inline float box_margin(float max_abs) { return std::ldexp(max_abs > 1e-20f ? max_abs : 1e-20f, -17); }
 
 struct WideBvh {
     std::vector<Bvh4Node> nodes;  // root at 0

@@ -410,7 +410,7 @@ int crisb_trace_rays(const crisb_scene* scene, const float* rays_dev,
  * queries_dev: n_queries float triples.  For query q, out_dev[q*k .. q*k+k)
  * receives the k nearest entries j with |p_j - q| <= radius_j, ordered by
  * (distance, entry index), unused slots zeroed; count_dev[q] their number.
- * k in [1, 31].  out_dev must be 8-byte and count_dev 4-byte aligned.
+ * k in [1, 31].  out_dev and count_dev must be 4-byte aligned.
  * Scratch comes from the stream-ordered allocator (cudaMallocAsync /
  * cudaFreeAsync on `stream`); the call is asynchronous.  A query that hits
  * the traversal's visit cap or stack depth keeps the neighbours found so far

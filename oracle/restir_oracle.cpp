@@ -24,7 +24,9 @@
  * OptiX internals it fixes a deterministic definition, marked DEFINED below:
  *   - optixTrace: own BVH + watertight ray/triangle test (Woop, Benthin &
  *     Wald 2013), closest hit = smallest t, ties -> lower triangle index;
- *     a hit counts when tmin < t < tmax.
+ *     a hit counts when tmin < t < tmax.  Boxes are widened by a margin
+ *     (BoxMargin) so the hits are those of testing every triangle, whatever
+ *     the tree.
  *   - prefix-endpoint neighbour search: the k nearest in-radius endpoints
  *     ordered by (distance, pixel index) instead of OptiX traversal order.
  *   - spatial reuse reads neighbours from the snapshot taken at pass start
@@ -563,6 +565,18 @@ struct HitResult {
 // Robust slab test (Ize 2013, "Robust BVH Ray Traversal"): tfar *= 1 + 2*gamma(3).
 constexpr float kSlabFarScale = 1.0000003576f;
 
+// DEFINED: box margin.  The watertight triangle test translates vertices to
+// the ray origin and shears them in float, so it accepts rays up to a few ulp
+// of the origin-vertex distance outside the exact triangle, and t to a few
+// ulp; a ray lying in a box face plane (a zero direction component, common
+// between points of one axis-aligned face) is also cut off at t = 0 by the
+// slab test.  Widening every box by 2^-17 x the scene's largest coordinate
+// magnitude keeps each box test at least an order of magnitude more generous
+// than those errors for rays starting within twice that magnitude, so the box
+// test never rejects a ray the triangle test accepts and any tree yields the
+// brute-force hits.
+inline float BoxMargin(float maxAbsCoord) { return std::ldexp(std::max(maxAbsCoord, 1e-20f), -17); }
+
 inline bool SlabHit(const RayPre& r, const BvhNode& n, float tmin, float tmax) {
     float tn = tmin, tf = tmax;
     for (int a = 0; a < 3; ++a) {
@@ -590,6 +604,14 @@ class Bvh {
                                  (t.p[0].y + t.p[1].y + t.p[2].y) / 3.0f,
                                  (t.p[0].z + t.p[1].z + t.p[2].z) / 3.0f);
         }
+        // DEFINED: every node box is widened by kBoxMargin x the largest
+        // coordinate magnitude of the scene (BoxMargin), so that the box test
+        // never rejects a ray the triangle test would accept
+        float maxAbs = 0.0f;
+        for (const Triangle& t : tris)
+            for (int c = 0; c < 3; ++c)
+                for (int a = 0; a < 3; ++a) maxAbs = std::max(maxAbs, std::fabs(t.p[c][a]));
+        margin_ = BoxMargin(maxAbs);
         nodes_.clear();
         nodes_.reserve(2 * n + 1);
         if (n > 0) BuildRec(0, n);
@@ -674,6 +696,10 @@ class Bvh {
                 chi[a] = std::max(chi[a], centroids_[order_[i]][a]);
             }
         }
+        for (int a = 0; a < 3; ++a) {
+            nd.lo[a] -= margin_;
+            nd.hi[a] += margin_;
+        }
         if (count <= 4) {
             nd.first = first;
             nd.count = count;
@@ -698,6 +724,7 @@ class Bvh {
     }
 
     const std::vector<Triangle>* tris_ = nullptr;
+    float margin_ = 0.0f;
     std::vector<uint32_t> order_;
     std::vector<vec3> centroids_;
     std::vector<BvhNode> nodes_;

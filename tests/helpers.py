@@ -128,3 +128,37 @@ def static(cam, frame):
 
 
 TWO_PI = 2.0 * math.pi
+
+
+def surface_rays(desc, n: int, seed: int) -> np.ndarray:
+    """Rays between points on the scene's triangles, as shadow and
+    reconnection rays run them: from a surface point (tmin 1e-3) to another
+    surface point at tmax = their distance.  A sixth of the endpoints sit on a
+    triangle edge and a sixth on a vertex, so on axis-aligned geometry many
+    rays lie in a face plane (a zero direction component) and end on an edge:
+    the configurations where a box test can disagree with the triangle test."""
+    rng = np.random.default_rng(seed)
+    pos, _, _ = desc.flatten()
+    tri = pos.reshape(-1, 3, 3).astype(np.float32)
+
+    def points(m):
+        t = rng.integers(0, len(tri), m)
+        r = rng.random((m, 3)).astype(np.float32)
+        k = rng.integers(0, 6, m)
+        r[k == 0, 0] = 0.0
+        r[k == 1] = [1.0, 0.0, 0.0]
+        r /= r.sum(1, keepdims=True)
+        return (r[:, 0:1] * tri[t, 0] + r[:, 1:2] * tri[t, 1] + r[:, 2:3] * tri[t, 2]).astype(np.float32)
+
+    a, b = points(n), points(n)
+    d = (b - a).astype(np.float32)
+    ln = np.sqrt((d * d).sum(1)).astype(np.float32)
+    keep = ln > 1e-3
+    a, d, ln = a[keep], d[keep], ln[keep]
+    d = (d / ln[:, None]).astype(np.float32)
+    rays = np.zeros((len(a), 8), np.float32)
+    rays[:, 0:3] = a
+    rays[:, 3] = 1e-3
+    rays[:, 4:7] = d
+    rays[:, 7] = ln
+    return rays

@@ -103,7 +103,7 @@ def test_misaligned_outputs_rejected(cuda_device):
     for fn in ("crisb_endpoint_search", "crisb_endpoint_search_noalloc"):
         f = getattr(lib, fn)
         rc = f(ctypes.c_void_p(e.data_ptr()), 4, ctypes.c_void_p(q.data_ptr()), 2, 4,
-               ctypes.c_void_p(out.data_ptr() + 4), ctypes.c_void_p(cnt.data_ptr()), None)
+               ctypes.c_void_p(out.data_ptr() + 2), ctypes.c_void_p(cnt.data_ptr()), None)
         assert rc == _abi.ERR_INVALID_ARGUMENT
         rc = f(ctypes.c_void_p(e.data_ptr()), 4, ctypes.c_void_p(q.data_ptr()), 2, 4,
                ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(cnt.data_ptr() + 2), None)
