@@ -107,7 +107,7 @@ def resample_bytes(k: int, spatial_count: int, spatial_rounds: int, copy_prefix_
 # at 960x540 (518,400 px, caches flushed before each launch), per reservoir
 # storage, with the pixel count it was taken at; scaled by pixels to the bench
 # resolution.
-PROFILED_TRAFFIC = {"resampling": (867.04e6, 960 * 540), "resampling_fp16": (610.73e6, 960 * 540)}
+PROFILED_TRAFFIC = {"resampling": (469.79e6, 960 * 540), "resampling_fp16": (333.55e6, 960 * 540)}
 
 
 class ClockSampler:
@@ -247,6 +247,63 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def comparison_arms(sc, cam, W: int, H: int, p, ppp: int, value: float, ms_per_frame: float, args) -> dict:
+    """The comparison the benchmark metric names, measured on the same GPU
+    right after the main loop:
+      - single view: FP32 storage (the main `value`) and FP16 storage, each
+        with the relMSE of orbit frame 30 against one FP64-accumulated
+        path-traced reference of that frame (`arm_ref_spp` samples per pixel,
+        fewer than the 4096 of the full quality run, to stay within the
+        benchmark's time; stated in the line);
+      - 16 uneven views: the plain form (FP32 storage, views one after another)
+        against the batched form (FP16 storage, one CUDA graph per frame with
+        a branch per view), and their ratio of resampled paths/s."""
+    import torch
+
+    from crisoptix_b200 import Renderer, _abi, quality, scenes
+
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    q = copy.copy(p)
+    q.storage = _abi.STORAGE_FP16
+    r16 = Renderer(W, H, sc, q)
+    out = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
+    cams = [scenes.orbit_camera(cam, f, 60) for f in range(60)]
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            r16.launch_frame(cams[i], out.data_ptr(), sptr)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for i in range(args.arm_steps):
+        r16.launch_frame(cams[(args.warmup + i) % 60], out.data_ptr(), sptr)
+    b.record(stream)
+    torch.cuda.synchronize()
+    r16.check_device_errors()
+    ms16 = a.elapsed_time(b) / args.arm_steps
+    del r16
+    cam_of = lambda f: scenes.orbit_camera(cam, f, 60)  # noqa: E731
+    ref = quality.reference_image(sc, W, H, cam_of(30), p, args.arm_ref_spp)
+    q32 = quality.score(sc, W, H, cam_of, p, 31, args.arm_ref_spp, ref=ref)
+    q16 = quality.score(sc, W, H, cam_of, q, 31, args.arm_ref_spp, ref=ref)
+    mv_plain = multiview_time(_abi.STORAGE_FP32, False, args.arm_mv_steps, 2)
+    mv_batch = multiview_time(_abi.STORAGE_FP16, True, args.arm_mv_steps, 2)
+    keep = ("relmse", "relmse_trimmed_0.1pct")
+    return {
+        "single_view_fp32": {"value": value, "ms_per_frame": ms_per_frame,
+                             "relmse": {k: q32[k] for k in keep}},
+        "single_view_fp16": {"value": ppp * W * H * 1000.0 / ms16, "ms_per_frame": ms16, "steps": args.arm_steps,
+                             "relmse": {k: q16[k] for k in keep}},
+        "fp16_over_fp32": ms_per_frame / ms16,
+        "relmse_reference": {"kind": "path tracer (TraceCompletePath), FP64 accumulation", "spp": args.arm_ref_spp,
+                             "frame": 30},
+        "multiview_plain_fp32": dict(mv_plain, steps=args.arm_mv_steps),
+        "multiview_batched_fp16": dict(mv_batch, steps=args.arm_mv_steps),
+        "batched_fp16_over_plain_fp32": mv_batch["value"] / mv_plain["value"],
+        "unit": UNIT,
+    }
+
+
 def run_crisb(args):
     import torch
 
@@ -361,11 +418,18 @@ def run_crisb(args):
     img_mean = float(host.mean())
     tone = tonemap_timing(out, W, H, stream)
 
+    # ---- the north star's comparison arms (same box, same run) -----------------
+    arms = None
+    if not args.no_arms and world == 1 and args.workload == "large" and not args.res:
+        arms = comparison_arms(sc, cam, W, H, p, ppp, value, ms_per_frame, args)
+
     # ---- roofline of the resampling kernels; traversal in rays/s -----------------
     peak, peak_kind = measured_peaks()
-    rb = resample_bytes(p.gather_m - 1, p.suffix_spatial_count, p.suffix_spatial_rounds, bool(p.suffix_enable_spatial),
-                        p.storage == _abi.STORAGE_FP16)
-    res_bytes = sum(rb.values()) * W * H
+    # algorithmic bytes: what the resampling kernels read and write for the
+    # work present in this frame (valid neighbours, chosen records), counted
+    # on the device at statistics level 2 (crisb_stats.resample_bytes)
+    tally = rays["resample_bytes"]
+    res_bytes = sum(tally.values())
     achieved = res_bytes / (passes["resample_ms"] / 1000.0) / 1e9
     traffic = None
     key = "resampling_fp16" if p.storage == _abi.STORAGE_FP16 else "resampling"
@@ -373,9 +437,13 @@ def run_crisb(args):
         tb, tpx = PROFILED_TRAFFIC[key]
         traffic = tb * (W * H) / tpx
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "resampling kernels (reuse-pass combine / select)",
+                "traffic": traffic,
+                "traffic_frac": traffic / (passes["resample_ms"] / 1000.0) / 1e9 / peak if traffic else None,
+                "kernel": "resampling kernels (reuse-pass combine / select)",
                 "peak_kind": f"{peak_kind} copy bandwidth", "algorithmic_bytes_per_launch": res_bytes,
-                "bytes_per_pixel": rb, "ms": passes["resample_ms"]}
+                "algorithmic_bytes_per_pixel": {k: v / (W * H) for k, v in tally.items()},
+                "algorithmic_bytes": "counted on the device for the frame's actual work (statistics level 2)",
+                "ms": passes["resample_ms"]}
     n_rays = rays["closest_rays"] + rays["shadow_rays"]
     traversal = {"closest_rays_per_frame": rays["closest_rays"], "shadow_rays_per_frame": rays["shadow_rays"],
                  "shift_closest_rays_per_frame": rays["shift_closest_rays"],
@@ -426,7 +494,57 @@ def run_crisb(args):
             "gpu_launches": launches_per_frame * args.steps, "image_mean": img_mean, "tonemap": tone}
     if qual is not None:
         line["quality"] = qual
+    if arms is not None:
+        line["arms"] = arms
     print(json.dumps(line), flush=True)
+
+
+def multiview_time(storage: int, batched: bool, steps: int, warmup: int, motion: int = 0) -> dict:
+    """Device-resident frames of the 16-view workload (seed 2): ms per frame
+    and resampled paths/s.  Renderers are freed on return."""
+    import torch
+
+    from crisoptix_b200 import Batch, Renderer, Scene, scenes
+
+    desc, _, _, _, ppp = workload("large")
+    sc = Scene(desc)
+    p = params_for("large", sc.scene_size)
+    p.seed = 2
+    p.storage = storage
+    p.motion_mode = motion
+    views = scenes.multiview_cameras(seed=2)
+    rs = [Renderer(w, h, sc, p) for _, w, h in views]
+    outs = [torch.zeros(w * h * 3, dtype=torch.float32, device="cuda") for _, w, h in views]
+    ptrs = [o.data_ptr() for o in outs]
+    px = sum(w * h for _, w, h in views)
+    stream = torch.cuda.Stream()
+    batch = Batch(rs) if batched else None
+
+    def frame(f):
+        cs = [scenes.orbit_camera(c, f % 30, 60) for c, _, _ in views]
+        if batch is not None:
+            batch.render(cs, ptrs, stream.cuda_stream)
+        else:
+            for r, c, o in zip(rs, cs, ptrs):
+                r.launch_frame(c, o, stream.cuda_stream)
+
+    with torch.cuda.stream(stream):
+        for f in range(warmup):
+            frame(f)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for f in range(steps):
+        frame(warmup + f)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    for r in rs:
+        r.check_device_errors()
+    ms = t0.elapsed_time(t1) / steps
+    del batch, rs, outs
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return {"ms_per_frame": ms, "value": ppp * px * 1000.0 / ms, "pixels": px}
 
 
 def run_multiview(args):
@@ -556,6 +674,12 @@ def main():
     ap.add_argument("--no-graph", action="store_true", help="launch kernels directly instead of one CUDA graph per frame")
     ap.add_argument("--cpu-scale", type=int, default=2)
     ap.add_argument("--res", default=None, help="WxH override of the workload resolution (profiling runs)")
+    ap.add_argument("--no-arms", action="store_true",
+                    help="skip the comparison arms (FP16 storage, multiview plain vs batched, relMSE)")
+    ap.add_argument("--arm-steps", type=int, default=10, help="timed frames of the FP16 single-view arm")
+    ap.add_argument("--arm-mv-steps", type=int, default=4, help="timed frames of each multiview arm")
+    ap.add_argument("--arm-ref-spp", type=int, default=256,
+                    help="samples per pixel of the path-traced relMSE reference of the arms")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -246,7 +246,9 @@ class Renderer:
     def stats(self) -> dict:
         s = _abi.Stats()
         check(load().crisb_get_stats(self.handle, ctypes.byref(s)))
-        return {k: getattr(s, k) for k, _ in s._fields_}
+        d = {k: getattr(s, k) for k, _ in s._fields_ if k != "resample_bytes"}
+        d["resample_bytes"] = dict(zip(_abi.RESAMPLE_KERNELS, (int(v) for v in s.resample_bytes)))
+        return d
 
     def check_device_errors(self):
         check(load().crisb_check_device_errors(self.handle))

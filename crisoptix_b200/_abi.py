@@ -108,7 +108,9 @@ class Stats(ctypes.Structure):
                 ("kernel_launches", c_u32), ("trace_ms", c_f), ("shift_ms", c_f), ("resample_ms", c_f),
                 ("search_ms", c_f), ("shade_ms", c_f), ("other_ms", c_f), ("closest_rays", c_u64), ("shadow_rays", c_u64),
                 ("shift_closest_rays", c_u64), ("shift_shadow_rays", c_u64), ("shift_jobs", c_u64),
-                ("node_visits", c_u64), ("tri_tests", c_u64)]
+                ("node_visits", c_u64), ("tri_tests", c_u64), ("resample_bytes", c_u64 * 5)]
+
+RESAMPLE_KERNELS = ("prefix_combine", "temporal_combine", "spatial_select", "spatial_combine", "gather_combine")
 
 
 HIT_DTYPE = np.dtype([("prim", "<u4"), ("bary", "<f4", 2), ("in_dir", "<f4", 3)])

@@ -48,21 +48,23 @@ def _flags() -> list:
     ]
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
+def build(force: bool = False, verbose: bool = False, out: str = OUT, defines=()) -> str:
     """Compile every source to an object in parallel, then link the shared
-    library.  Objects go to a build folder beside the sources."""
-    if not force and not needs_build():
+    library.  Objects go to a build folder beside the sources.  `defines`
+    (NAME=VALUE strings) select compile-time variants, built into `out`."""
+    if out == OUT and not defines and not force and not needs_build():
         return OUT
     from concurrent.futures import ThreadPoolExecutor
 
-    objdir = os.path.join(HERE, "_build")
+    tag = "_".join(d.replace("=", "") for d in defines)
+    objdir = os.path.join(HERE, "_build" + ("_" + tag if tag else ""))
     os.makedirs(objdir, exist_ok=True)
     nvcc = nvcc_path()
 
     def compile_one(src: str):
         obj = os.path.join(objdir, src + ".o")
-        cmd = [nvcc] + _flags() + ["-Xptxas", "-v" if verbose else "-O3", "-c", os.path.join(CSRC, src),
-                                   "-o", obj]
+        cmd = [nvcc] + _flags() + [f"-D{d}" for d in defines] + [
+            "-Xptxas", "-v" if verbose else "-O3", "-c", os.path.join(CSRC, src), "-o", obj]
         return subprocess.run(cmd, capture_output=True, text=True), obj
 
     with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 4)) as ex:
@@ -77,13 +79,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if failed:
         raise RuntimeError("nvcc failed")
     link = [nvcc, "-ccbin", host_cxx(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
-            "-o", OUT + ".tmp"] + [o for _, o in results]
+            "-o", out + ".tmp"] + [o for _, o in results]
     r = subprocess.run(link, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("nvcc link failed")
-    os.replace(OUT + ".tmp", OUT)
-    return OUT
+    os.replace(out + ".tmp", out)
+    return out
 
 
 if __name__ == "__main__":

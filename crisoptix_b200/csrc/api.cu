@@ -516,6 +516,9 @@ struct crisb_renderer {
     int timing = 0;
     cudaEvent_t ev[7] = {};
     uint32_t launches = 0;
+    // statistics level 2: ray, job, node-visit and triangle-test counters,
+    // then the resampling kernels' byte tallies
+    static constexpr int kRayCounters = 7;
     DevBuf<unsigned long long> ray_count;
 
     // per-kernel timing: an event after each kernel, tagged with its class
@@ -568,6 +571,7 @@ struct crisb_renderer {
         b.gather_cs = gather_cs.p;
         b.gather_state = gather_state.p;
         b.slots = slots;
+        b.tally = timing >= 2 && ray_count.p ? ray_count.p + kRayCounters : nullptr;
         b.wf = wf.p;
         for (int q = 0; q < 4; ++q) b.wf_queue[q] = wf_queue[q].p;
         b.wf_count = wf_count.p;
@@ -752,7 +756,8 @@ struct crisb_renderer {
         last_stream = st;
         ktimer.n = 0;
         if (timing >= 2) {
-            check(cudaMemsetAsync(ray_count.p, 0, 7 * sizeof(unsigned long long), st), "memset");
+            check(cudaMemsetAsync(ray_count.p, 0, (kRayCounters + kTallyKernels) * sizeof(unsigned long long), st),
+                  "memset");
             s.ray_count = ray_count.p;
             s.trav_count = ray_count.p + 5;
         }
@@ -1326,7 +1331,7 @@ int crisb_set_timing(crisb_renderer* r, int enable) {
             for (auto& e : r->ev) check(cudaEventCreate(&e), "event create");
             for (auto& e : r->ktimer.ev) check(cudaEventCreate(&e), "event create");
         }
-        if (enable >= 2 && !r->ray_count.p) r->ray_count.alloc(7);
+        if (enable >= 2 && !r->ray_count.p) r->ray_count.alloc(crisb_renderer::kRayCounters + kTallyKernels);
         r->timing = enable;
     });
 }
@@ -1362,8 +1367,10 @@ int crisb_get_stats(crisb_renderer* r, crisb_stats* out) {
         out->shade_ms = cls_ms[kClsShade];
         out->other_ms = cls_ms[kClsOther];
         if (r->timing >= 2) {
-            unsigned long long rc[7] = {0, 0, 0, 0, 0, 0, 0};
+            constexpr int kRayCounters = crisb_renderer::kRayCounters;
+            unsigned long long rc[kRayCounters + kTallyKernels] = {};
             check(cudaMemcpy(rc, r->ray_count.p, sizeof(rc), cudaMemcpyDeviceToHost), "ray counters");
+            for (int k = 0; k < kTallyKernels; ++k) out->resample_bytes[k] = rc[kRayCounters + k];
             out->closest_rays = rc[0] + rc[2];
             out->shadow_rays = rc[1] + rc[3];
             out->shift_closest_rays = rc[2];

@@ -8,8 +8,12 @@
 //   octahedral: the zero vector -> CRISB_OCT_ZERO; otherwise p = n.xy / |n|_1,
 //     folded for n.z < 0, each coordinate clamped to [-1, 1] and rounded to
 //     nearest even of v * 32767 as int16; decoded by the inverse fold and a
-//     normalisation.  Decoding and re-encoding a code gives the code back, so
-//     storing a loaded record again does not move it.
+//     normalisation.  The fold's sign is the sign bit (-0 folds negative):
+//     decoding a code on the fold's edge (|x| or |y| = 1) unfolds the other
+//     coordinate to a signed zero, and a sign test of v >= 0 would flip it on
+//     re-encoding.  With the sign bit, decoding and re-encoding every code the
+//     encoder produces gives the code back, so storing a loaded record again
+//     does not move it.
 #pragma once
 
 #include <cuda_fp16.h>
@@ -25,7 +29,7 @@ RT_D uint16_t h16(float x) {
 }
 RT_D float f16(uint16_t h) { return __half2float(__ushort_as_half(h)); }
 
-RT_D float oct_sign(float v) { return v >= 0.0f ? 1.0f : -1.0f; }
+RT_D float oct_sign(float v) { return signbit(v) ? -1.0f : 1.0f; }
 
 RT_D uint32_t oct_encode(V3 n) {
     if (n.x == 0.0f && n.y == 0.0f && n.z == 0.0f) return CRISB_OCT_ZERO;

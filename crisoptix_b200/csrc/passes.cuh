@@ -39,14 +39,20 @@ struct SresBuf {
 // `sres_cur` holds the state every logical copy front -> back has made equal
 // and the temporal pass and each spatial round write `sres_next` (then the
 // roles swap), so every read sees the pass-start state.
+// bits of the per-pixel byte beside each suffix reservoir buffer
+constexpr uint8_t kNvalNeighbor = 1;  // usable as a spatial neighbour: valid primary hit and sample
+constexpr uint8_t kNvalSpatial = 2;   // takes part in the next spatial round: valid prefix (not NEE),
+                                      // canonical suffix and sample
+constexpr uint8_t kNvalSample = 4;    // valid reservoir sample
+
 struct Bufs {
     PresBuf pres[2];
     crisb_prefix_rec* canon_prefix;
     SresBuf sres_cur;
     SresBuf sres_next;
-    // per pixel, beside each suffix reservoir buffer: 1 when the pixel can be a
-    // spatial neighbour (valid primary interaction and valid reservoir sample),
-    // written with the reservoir so the neighbour test reads one byte
+    // per pixel, beside each suffix reservoir buffer, written with the
+    // reservoir: kNval* bits, so that the spatial selection and the gather
+    // query test one dense byte instead of flag words of large records
     uint8_t* nval_cur;
     uint8_t* nval_next;
     crisb_suffix_res_rec* canon_suffix;  // 112-byte slots, w_sum/confidence unused
@@ -70,6 +76,9 @@ struct Bufs {
     crisb_suffix_res_rec* gather_cs;  // P: canonical suffix of the final gather
     float4* gather_state;   // P * 3: prefix f / p, canonical contribution, direct result
     uint32_t slots;         // job slots per pixel (>= 2 * max(k, spatial count, 1))
+    // statistics level 2 only (else null): bytes read and written by each
+    // resampling kernel for the work present in the frame (kTally*)
+    unsigned long long* tally;
     // wavefront path tracing: one path state per pixel, ray queues of two
     // rounds (closest, shadow) x 2 and their counts
     WfPath* wf;

@@ -66,8 +66,11 @@ RT_D void set_occluded(ShiftJob& j, uint32_t v) { j.hit.x = __uint_as_float(v); 
 // (the last, slowest rays) overlap instead of running back to back.
 // 9 resident blocks per SM (56 registers): 13.40 -> 13.25 ms of traversal per
 // 1080p frame against 8 blocks (64 registers), despite a few more spills
+#ifndef CRISB_TRACE_MIN_BLOCKS
+#define CRISB_TRACE_MIN_BLOCKS 9
+#endif
 template <class R>
-__global__ void __launch_bounds__(kPassBlock, 9) k_q_trace(SceneView s, const uint32_t* qc, const uint32_t* ccnt,
+__global__ void __launch_bounds__(kPassBlock, CRISB_TRACE_MIN_BLOCKS) k_q_trace(SceneView s, const uint32_t* qc, const uint32_t* ccnt,
                                                         const uint32_t* qs, const uint32_t* scnt, R* rec) {
     const uint32_t nc = *ccnt, ns = *scnt;
     const uint32_t n = nc + ns;

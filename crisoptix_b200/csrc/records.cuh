@@ -131,6 +131,51 @@ RT_D void store_output(const FrameParams& fp, float* out, uint32_t i, V3 radianc
     out[3 * i + 2] = v.z;
 }
 
+// the per-pixel byte beside a suffix reservoir (kNval*): primary hit valid,
+// prefix and canonical suffix valid for spatial reuse, sample valid
+RT_D uint8_t nval_bits(bool primary_valid, bool spatial_ok, bool sample_valid) {
+    if (!sample_valid) return 0;
+    return static_cast<uint8_t>(kNvalSample | (primary_valid ? kNvalNeighbor : 0) | (spatial_ok ? kNvalSpatial : 0));
+}
+
+// ---- byte tally of the resampling kernels (statistics level 2) ----------------
+// Each kernel adds the bytes of every field it reads or writes, at the size
+// it is stored in, for the work actually present (valid neighbours, the
+// chosen record); the sum over a frame is the roofline's algorithmic byte
+// count.  A thread's count is added to its kernel's counter when the tally
+// goes out of scope (one warp-aggregated atomic per exit point).
+enum TallyKernel : int {
+    kTallyPrefixCombine = 0,
+    kTallyTemporalCombine = 1,
+    kTallySpatialSelect = 2,
+    kTallySpatialCombine = 3,
+    kTallyGatherCombine = 4,
+    kTallyKernels = 5
+};
+
+struct ByteTally {
+    unsigned long long* counter;
+    uint32_t n;
+    RT_D ByteTally(const Bufs& b, int kernel) : counter(b.tally ? b.tally + kernel : nullptr), n(0) {}
+    RT_D void add(uint32_t bytes) { n += bytes; }
+    RT_D ~ByteTally() {
+        if (!counter) return;
+        const unsigned m = __activemask();
+        const uint32_t sum = __reduce_add_sync(m, n);
+        if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(counter, static_cast<unsigned long long>(sum));
+    }
+};
+
+// stored sizes of reservoir records and of their weight fields (f, w_sum,
+// confidence) in either storage layout
+RT_D uint32_t pres_bytes(const PresBuf& b) {
+    return b.f16 ? sizeof(crisb_prefix_res16_rec) : sizeof(crisb_prefix_res_rec);
+}
+RT_D uint32_t sres_bytes(const SresBuf& b) {
+    return b.f16 ? sizeof(crisb_suffix_res16_rec) : sizeof(crisb_suffix_res_rec);
+}
+RT_D uint32_t weight_bytes(bool f16) { return (f16 ? 6u : 12u) + 8u; }
+
 RT_D void invalidate(Res<Suffix>& r) {
     r.w_sum = 0.0f;
     r.conf = 0.0f;

@@ -351,43 +351,73 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_temp_finish(FrameParams f
 __global__ void __launch_bounds__(kPassBlock) k_suffix_temp_combine(FrameParams fp, Bufs b) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pixel_count(fp)) return;
+    ByteTally bt(b, kTallyTemporalCombine);
     const uint32_t st = b.pass_status[i];
+    bt.add(4);
     if (st == kStFinal) return;
-    Res<Suffix> cur = ld_sres(b.sres_cur, i);
-    const Suffix canon = ld_suffix(b.canon_suffix[i].sample);
+    // Reservoir::Update's arithmetic with the chosen sample tracked by index
+    // (0: the sample the reset reservoir still holds, 1: the canonical suffix,
+    // 2: the previous sample shifted onto it); the candidates contribute their
+    // weight fields and the chosen record is read once at the end.
+    const crisb_suffix_rec& cs = b.canon_suffix[i].sample;
+    const V3 canon_f = ld3(cs.f);
+    const float canon_p = cs.p;
     Rng rng{b.gbuf[i].rng};
-    const float canon_phat = luminance(canon.f);
+    bt.add(12 + 4 + 8);  // canonical f and p, RNG
+    const float canon_phat = luminance(canon_f);
+    float w_sum = 0.0f, conf = 0.0f;
+    int sel = 0;
+    V3 f_canon_of_prev = splat(0.0f);
     // suffixReservoirs[back][prevPixelIdx]: the previous frame's reservoirs are
     // the pass-start state sres_cur; this pass writes sres_next
-    const Res<Suffix> prev = st == kStReuse ? ld_sres(b.sres_cur, prev_pixel(fp, b, i)) : cur;
-    cur.w_sum = 0.0f;
-    cur.conf = 0.0f;
+    uint32_t pi = i;
+    const float K = 1.0f;
     if (st == kStCanonOnly) {
-        res_update(cur, canon, canon_phat / canon.p, rng, 1.0f);
-        res_finalize(cur);
+        if (res_choose(w_sum, conf, canon_phat / canon_p, rng, 1.0f)) sel = 1;
     } else {
+        pi = prev_pixel(fp, b, i);
+        const V3 prev_f = sres_f(b.sres_cur, pi);
+        const float prev_conf = sres_conf(b.sres_cur, pi), prev_wsum = sres_wsum(b.sres_cur, pi);
         const float4 o0 = b.shift_out[static_cast<size_t>(i) * b.slots];
         const float4 o1 = b.shift_out[static_cast<size_t>(i) * b.slots + 1];
-        const V3 f_canon_of_prev = xyz(o0), f_prev_of_canon = xyz(o1);
+        bt.add(weight_bytes(b.sres_cur.f16) + 32);
+        f_canon_of_prev = xyz(o0);
+        const V3 f_prev_of_canon = xyz(o1);
         const float jac_prev_to_canon = o0.w, jac_canon_to_prev = o1.w;
         const float p_canon_of_prev = luminance(f_canon_of_prev) * jac_prev_to_canon;
-        const float K = 1.0f;
-        const float prev_mis = mis_neighbor(f_canon_of_prev, prev.s.f, jac_prev_to_canon, K, 1.0f, prev.conf);
+        const float prev_mis = mis_neighbor(f_canon_of_prev, prev_f, jac_prev_to_canon, K, 1.0f, prev_conf);
         const float canon_mis =
-            1.0f + mis_canonical(canon.f, f_prev_of_canon, jac_canon_to_prev, K, 1.0f, prev.conf);
-        res_update(cur, canon, canon_mis * canon_phat / canon.p, rng, 1.0f);
-        Suffix shifted = prev.s;  // SuffixPath(prev, canon.lastPrefixInt, f)
-        shifted.last_prefix = canon.last_prefix;
-        shifted.f = f_canon_of_prev;
-        res_update(cur, shifted, prev_mis * p_canon_of_prev * prev.w_sum, rng, prev.conf);
-        if (cur.w_sum > 0.0f) {
-            cur.w_sum /= K + 1.0f;
-            res_finalize(cur);
-        }
+            1.0f + mis_canonical(canon_f, f_prev_of_canon, jac_canon_to_prev, K, 1.0f, prev_conf);
+        if (res_choose(w_sum, conf, canon_mis * canon_phat / canon_p, rng, 1.0f)) sel = 1;
+        if (res_choose(w_sum, conf, prev_mis * p_canon_of_prev * prev_wsum, rng, prev_conf)) sel = 2;
+    }
+    Res<Suffix> cur;
+    if (sel == 0) {
+        cur.s = ld_sres(b.sres_cur, i).s;
+        bt.add(sres_bytes(b.sres_cur));
+    } else if (sel == 1) {
+        cur.s = ld_suffix(cs);
+        bt.add(sizeof(crisb_suffix_rec));
+    } else {
+        // SuffixPath(prev, canon.lastPrefixInt, fFromCanonOfPrev)
+        cur.s = ld_sres(b.sres_cur, pi).s;
+        cur.s.last_prefix = ld_hit(cs.last_prefix);
+        cur.s.f = f_canon_of_prev;
+        bt.add(sres_bytes(b.sres_cur) + sizeof(crisb_hit_rec));
+    }
+    cur.w_sum = w_sum;
+    cur.conf = conf;
+    if (st == kStCanonOnly) {
+        res_finalize(cur);
+    } else if (cur.w_sum > 0.0f) {
+        cur.w_sum /= K + 1.0f;
+        res_finalize(cur);
     }
     b.gbuf[i].rng = rng.state;
     st_sres(b.sres_next, i, cur);
-    b.nval_next[i] = (b.gbuf[i].flags & 1u) && fl_valid(cur.s.flags) ? 1 : 0;
+    // this combine runs only for a valid prefix (not NEE) and canonical suffix
+    b.nval_next[i] = nval_bits(b.gbuf[i].flags & 1u, true, fl_valid(cur.s.flags));
+    bt.add(8 + sres_bytes(b.sres_next) + 1 + 4);  // RNG, reservoir and byte out, primary-valid flag
 }
 
 // ---- suffix spatial reuse (shader/suffix_spatial_reuse.cu:16-167) -----------------
@@ -396,12 +426,14 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_select(FrameParam
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     uint64_t mask = 0;
     if (i < pixel_count(fp)) {
+        ByteTally bt(b, kTallySpatialSelect);
+        // the pixel's byte in, the status word out
+        bt.add(1 + 4);
         const uint32_t x = i % fp.width, y = i / fp.width;
-        const uint32_t cur_flags = sres_flags(b.sres_cur, i);
-        const uint32_t prefix_flags = pres_flags(b.pres[fp.front], i);
-        const uint32_t canon_flags = b.canon_suffix[i].sample.flags;
         uint32_t st = kStFinal;
-        if (fl_valid(prefix_flags) && !fl_nee(prefix_flags) && fl_valid(cur_flags) && fl_valid(canon_flags)) {
+        // valid prefix (not NEE), valid reservoir sample and canonical suffix
+        // (suffix_spatial_reuse.cu:18-35), as recorded by the previous combine
+        if (b.nval_cur[i] & kNvalSpatial) {
             st = kStReuse;
             Rng rng{b.gbuf[i].rng};
             uint32_t vflags = 0;
@@ -411,13 +443,16 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_select(FrameParam
                 select_spatial_neighbor(x, y, static_cast<uint32_t>(fp.p.window_radius), rng, nx, ny);
                 if (!(nx < fp.width && ny < fp.height)) continue;
                 const uint32_t ni = ny * fp.width + nx;
-                if (!b.nval_cur[ni]) continue;  // primary valid && reservoir sample valid
+                bt.add(1);
+                if (!(b.nval_cur[ni] & kNvalNeighbor)) continue;  // primary valid && reservoir sample valid
                 nbr[n] = ni;
+                bt.add(4);
                 vflags |= 1u << n;
                 mask |= 3ull << (2 * n);
             }
             b.gbuf[i].rng = rng.state;
             b.pass_flags[i] = vflags;
+            bt.add(8 + 8 + 4);
         }
         b.pass_status[i] = st;
     }
@@ -427,19 +462,23 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_select(FrameParam
 __global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_combine(FrameParams fp, Bufs b) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pixel_count(fp)) return;
-    Res<Suffix> cur = ld_sres(b.sres_cur, i);
+    ByteTally bt(b, kTallySpatialCombine);
+    bt.add(4);
     if (b.pass_status[i] == kStFinal) {
+        Res<Suffix> cur = ld_sres(b.sres_cur, i);
         invalidate(cur);
         st_sres(b.sres_next, i, cur);
         b.nval_next[i] = 0;
+        bt.add(sres_bytes(b.sres_cur) + sres_bytes(b.sres_next) + 1);
         return;
     }
     Rng rng{b.gbuf[i].rng};
-    const Suffix cur_suffix = cur.s;
-    const float cur_wsum = cur.w_sum, cur_conf = cur.conf;
-    cur.w_sum = 0.0f;
-    cur.conf = 0.0f;
+    // the pixel's own sample: its weight fields now, its record at the end
+    const V3 own_f = sres_f(b.sres_cur, i);
+    const float cur_wsum = sres_wsum(b.sres_cur, i), cur_conf = sres_conf(b.sres_cur, i);
     const uint32_t vflags = b.pass_flags[i];
+    bt.add(8 + weight_bytes(b.sres_cur.f16) + 4);  // RNG, own weight fields, neighbour flags
+    float w_sum = 0.0f, conf = 0.0f;
     const float K = static_cast<float>(__popc(vflags));
     const uint32_t* nbr = b.spatial_nbr + static_cast<size_t>(i) * (b.slots >> 1);
     const float4* sh = b.shift_out + static_cast<size_t>(i) * b.slots;
@@ -449,7 +488,7 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_combine(FramePara
     // with the chosen sample tracked by index: -1 is the pixel's own sample,
     // which the reset reservoir also still holds).
     int sel = -1;
-    V3 sel_f = cur_suffix.f;
+    V3 sel_f = own_f;
     float canon_mis = 1.0f;
     for (int n = 0; n < fp.p.suffix_spatial_count; ++n) {
         if (!((vflags >> n) & 1u)) continue;
@@ -457,37 +496,45 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_combine(FramePara
         const V3 nf = sres_f(b.sres_cur, ni);
         const float nconf = sres_conf(b.sres_cur, ni), nwsum = sres_wsum(b.sres_cur, ni);
         const float4 o0 = sh[2 * n], o1 = sh[2 * n + 1];
+        bt.add(4 + weight_bytes(b.sres_cur.f16) + 32);  // index, weight fields, two shift results
         const V3 f_c_of_n = xyz(o0), f_n_of_c = xyz(o1);
         const float jac_n2c = o0.w, jac_c2n = o1.w;
         const float p_c_of_n = luminance(f_c_of_n) * jac_n2c;
         float nmis = mis_neighbor(f_c_of_n, nf, jac_n2c, K, cur_conf, nconf);
         if (nonfinite(nmis)) nmis = 0.0f;
-        if (res_choose(cur.w_sum, cur.conf, nmis * p_c_of_n * nwsum, rng, nconf)) {
+        if (res_choose(w_sum, conf, nmis * p_c_of_n * nwsum, rng, nconf)) {
             sel = n;
             sel_f = f_c_of_n;
         }
-        canon_mis += mis_canonical(cur_suffix.f, f_n_of_c, jac_c2n, K, cur_conf, nconf);
+        canon_mis += mis_canonical(own_f, f_n_of_c, jac_c2n, K, cur_conf, nconf);
     }
     if (nonfinite(canon_mis)) canon_mis = 0.0f;
-    if (res_choose(cur.w_sum, cur.conf, canon_mis * cur_wsum * luminance(cur_suffix.f), rng, cur_conf)) {
+    if (res_choose(w_sum, conf, canon_mis * cur_wsum * luminance(own_f), rng, cur_conf)) {
         sel = -1;
-        sel_f = cur_suffix.f;
+        sel_f = own_f;
     }
+    Res<Suffix> cur;
     if (sel >= 0) {
         // SuffixPath(neighbour, currSuffix.lastPrefixInt, fFromCanonOfNeigh)
         cur.s = ld_sres(b.sres_cur, nbr[sel]).s;
-        cur.s.last_prefix = cur_suffix.last_prefix;
+        cur.s.last_prefix = sres_last_prefix(b.sres_cur, i);
         cur.s.f = sel_f;
+        bt.add(sres_bytes(b.sres_cur) + (b.sres_cur.f16 ? sizeof(crisb_hit16_rec) : sizeof(crisb_hit_rec)));
     } else {
-        cur.s = cur_suffix;
+        cur.s = ld_sres(b.sres_cur, i).s;
+        bt.add(sres_bytes(b.sres_cur));
     }
+    cur.w_sum = w_sum;
+    cur.conf = conf;
     if (cur.w_sum > 0.0f) {
         cur.w_sum /= K + 1.0f;
         res_finalize(cur);
     }
     b.gbuf[i].rng = rng.state;
     st_sres(b.sres_next, i, cur);
-    b.nval_next[i] = (b.gbuf[i].flags & 1u) && fl_valid(cur.s.flags) ? 1 : 0;
+    // the pixel took part in this round: its prefix and canonical suffix are valid
+    b.nval_next[i] = nval_bits(b.gbuf[i].flags & 1u, true, fl_valid(cur.s.flags));
+    bt.add(8 + sres_bytes(b.sres_next) + 1 + 4);  // RNG, reservoir and byte out, primary-valid flag
 }
 
 // ---- final gather with gatherN == 1 (shader/final_gather.cu:69-188, 290-356) -----
@@ -544,7 +591,7 @@ __global__ void __launch_bounds__(kPassBlock) k_gather_query(SceneView s, FrameP
             knn_query(b.knn(), s.err, last.pos, k, nl);
             uint32_t vflags = 0;
             for (uint32_t n = 0; n < nl.count; ++n) {
-                if (!fl_valid(sres_flags(b.sres_cur, nl.pix[n]))) continue;
+                if (!(b.nval_cur[nl.pix[n]] & kNvalSample)) continue;
                 vflags |= 1u << n;
                 mask |= 3ull << (2 * n);
             }
@@ -566,7 +613,12 @@ __global__ void __launch_bounds__(kPassBlock) k_gather_query(SceneView s, FrameP
 
 __global__ void __launch_bounds__(kPassBlock) k_gather_combine(FrameParams fp, Bufs b, float* out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= pixel_count(fp) || b.pass_status[i] != kStReuse) return;
+    if (i >= pixel_count(fp)) return;
+    ByteTally bt(b, kTallyGatherCombine);
+    bt.add(4);
+    if (b.pass_status[i] != kStReuse) return;
+    // count, flags, canonical suffix f, gather state, the output RGB
+    bt.add(4 + 4 + 12 + 32 + (fp.p.enable_accum ? 24 : 12));
     const uint32_t k = fp.k;
     const uint32_t count = b.neigh_count[i];
     const uint32_t vflags = b.pass_flags[i];
@@ -582,6 +634,7 @@ __global__ void __launch_bounds__(kPassBlock) k_gather_combine(FrameParams fp, B
     for (uint32_t n = 0; n < count; ++n) {
         if (!(vflags & (1u << n))) continue;
         const uint32_t np_ = b.neighbors[static_cast<size_t>(i) * k + n].pixel;
+        bt.add(4 + weight_bytes(b.sres_cur.f16) + 32);  // neighbour pixel, weight fields, two shift results
         const V3 nf = sres_f(b.sres_cur, np_);
         const float nconf = sres_conf(b.sres_cur, np_), nwsum = sres_wsum(b.sres_cur, np_);
         const float4 o0 = sh[2 * n], o1 = sh[2 * n + 1];
@@ -684,11 +737,19 @@ __global__ void __launch_bounds__(kPassBlock) k_prefix_finish(SceneView s, Frame
 __global__ void __launch_bounds__(kPassBlock) k_prefix_combine(FrameParams fp, Bufs b, float* out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pixel_count(fp) || fp.p.renderer_type == CRISB_RENDERER_PATH_TRACER) return;
+    ByteTally bt(b, kTallyPrefixCombine);
     const uint32_t st = b.pass_status[i];
+    bt.add(4);
     if (st == kStFinal) return;
-    const Prefix canon = ld_prefix(b.canon_prefix[i]);
+    const crisb_prefix_rec& cp = b.canon_prefix[i];
+    const V3 canon_f = ld3(cp.f);
+    const float canon_p = cp.p;
     Rng rng{b.gbuf[i].rng};
-    const float canon_phat = luminance(canon.f);
+    // canonical f and p, RNG in and out, the front reservoir out (and its back
+    // copy for the spatial passes)
+    bt.add(12 + 4 + 8 + 8 + pres_bytes(b.pres[fp.front]) +
+           (prefix_back_copy(fp) && fp.p.motion_mode == CRISB_MOTION_NONE ? pres_bytes(b.pres[fp.back]) : 0));
+    const float canon_phat = luminance(canon_f);
     // Reservoir::Update's arithmetic with the chosen sample tracked by index
     // (0: the sample the reset front reservoir still holds, 1: canonical,
     // 2: the shifted previous sample); the chosen record is read at the end.
@@ -699,8 +760,9 @@ __global__ void __launch_bounds__(kPassBlock) k_prefix_combine(FrameParams fp, B
     V3 f_canon_of_prev = splat(0.0f);
     const uint32_t pi = prev_pixel(fp, b, i);
     if (st == kStCanonOnly) {
-        if (res_choose(cur.w_sum, cur.conf, canon_phat / canon.p, rng, 1.0f)) sel = 1;
+        if (res_choose(cur.w_sum, cur.conf, canon_phat / canon_p, rng, 1.0f)) sel = 1;
     } else {
+        bt.add(weight_bytes(b.pres[fp.back].f16) + 32);  // previous weight fields, two shift results
         const V3 prev_f = pres_f(b.pres[fp.back], pi);
         const float prev_conf = pres_conf(b.pres[fp.back], pi), prev_wsum = pres_wsum(b.pres[fp.back], pi);
         const float4 o0 = b.shift_out[static_cast<size_t>(i) * b.slots];
@@ -712,18 +774,21 @@ __global__ void __launch_bounds__(kPassBlock) k_prefix_combine(FrameParams fp, B
         const float K = 1.0f;
         const float prev_mis = mis_neighbor(f_canon_of_prev, prev_f, jac_prev_to_canon, K, 1.0f, prev_conf);
         const float canon_mis =
-            1.0f + mis_canonical(canon.f, f_prev_of_canon, jac_canon_to_prev, K, 1.0f, prev_conf);
-        if (res_choose(cur.w_sum, cur.conf, canon_mis * canon_phat / canon.p, rng, 1.0f)) sel = 1;
+            1.0f + mis_canonical(canon_f, f_prev_of_canon, jac_canon_to_prev, K, 1.0f, prev_conf);
+        if (res_choose(cur.w_sum, cur.conf, canon_mis * canon_phat / canon_p, rng, 1.0f)) sel = 1;
         if (res_choose(cur.w_sum, cur.conf, prev_mis * p_canon_of_prev * prev_wsum, rng, prev_conf)) sel = 2;
     }
     if (sel == 0) {
+        bt.add(pres_bytes(b.pres[fp.front]));
         cur.s = ld_pres(b.pres[fp.front], i).s;
     } else if (sel == 1) {
-        cur.s = canon;
+        bt.add(sizeof(crisb_prefix_rec));
+        cur.s = ld_prefix(cp);
     } else {
+        bt.add(pres_bytes(b.pres[fp.back]) + sizeof(crisb_hit_rec));
         cur.s = ld_pres(b.pres[fp.back], pi).s;  // PrefixPath(prev, f, canon.primaryInt)
         cur.s.f = f_canon_of_prev;
-        cur.s.primary = canon.primary;
+        cur.s.primary = ld_hit(cp.primary);
     }
     if (st == kStCanonOnly) {
         res_finalize(cur);

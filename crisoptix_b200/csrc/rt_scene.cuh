@@ -206,7 +206,9 @@ struct Trav {
     // slab() with the near / far plane of each axis chosen by the sign of the
     // inverse direction: the same values as the min / max form, since
     // (lo - o) * inv <= (hi - o) * inv exactly when inv > 0 (rounding is
-    // monotonic) and the inverse direction is never zero or NaN
+    // monotonic) and the inverse direction is never zero or NaN.  (One FMA per
+    // plane against a per-ray org * inv measured no faster: 13.67 against
+    // 13.59 ms of traversal per 1080p frame; the traversal is latency-bound.)
     RT_D bool slab_nf(float nx, float fx, float ny, float fy, float nz, float fz, float tmax_, float& tnear) const {
         float tn = (nx - r.org.x) * r.inv.x, tf = (fx - r.org.x) * r.inv.x;
         tn = fmaxf(tn, (ny - r.org.y) * r.inv.y);

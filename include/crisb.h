@@ -350,6 +350,11 @@ typedef struct crisb_stats {
      * ray/triangle tests (level 2 only) */
     uint64_t node_visits;
     uint64_t tri_tests;
+    /* bytes read and written by the resampling kernels for the work present
+     * in the frame, at the stored size of every field they touch (level 2
+     * only): prefix combine, suffix temporal combine, suffix spatial
+     * selection, suffix spatial combine, final-gather combine (all rounds) */
+    uint64_t resample_bytes[5];
 } crisb_stats;
 
 /* debug buffer ids for crisb_debug_read */

@@ -79,6 +79,10 @@ int oracle_tonemap_srgb8(const float* rgb, uint8_t* out, uint32_t num_pixels);
 uint32_t oracle_srgb8_first_decrease(uint32_t lo_bits, uint32_t hi_bits);
 void oracle_oct(const float* dirs, uint32_t n, uint32_t* codes, float* decoded);
 void oracle_sincos(const float* phi, uint32_t n, float* s, float* c);
+/* codes c whose re-encoded code c1 = encode(decode(c)) is not stable
+ * (encode(decode(c1)) != c1); 0 means storing a loaded direction again never
+ * moves its code */
+uint64_t oracle_oct_unstable(const uint32_t* codes, uint32_t n);
 int oracle_camera_data(const crisb_camera* cam, crisb_camera_data* out);
 uint32_t oracle_frame_random_for(uint64_t seed, uint64_t frame_counter);
 

@@ -59,6 +59,7 @@ def load():
         "oracle_pcg32": (None, [u64, u64, u32, vp]),
         "oracle_tea64": (u64, [u32, u32]),
         "oracle_kat": (i32, [i32, vp, u32, vp]),
+        "oracle_oct_unstable": (u64, [vp, u32]),
         "oracle_kat_emitter": (i32, [vp, u32, vp, vp, u32, vp, vp]),
         "oracle_sincos": (None, [vp, u32, vp, vp]),
         "oracle_half": (None, [vp, u32, vp, vp]),

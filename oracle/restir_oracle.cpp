@@ -405,7 +405,9 @@ float HalfValue(uint16_t h) {
 
 float Quant16(float f) { return HalfValue(HalfBits(f)); }
 
-float OctSign(float v) { return v >= 0.0f ? 1.0f : -1.0f; }
+// the fold's sign is the sign bit (-0 folds negative), which keeps every code
+// the encoder produces stable under decode + re-encode
+float OctSign(float v) { return std::signbit(v) ? -1.0f : 1.0f; }
 
 uint32_t OctEncode(vec3 n) {
     if (n.x == 0.0f && n.y == 0.0f && n.z == 0.0f) return CRISB_OCT_ZERO;
@@ -2634,6 +2636,16 @@ void oracle_oct(const float* dirs, uint32_t n, uint32_t* codes, float* decoded) 
         decoded[3 * i + 1] = d.y;
         decoded[3 * i + 2] = d.z;
     }
+}
+
+uint64_t oracle_oct_unstable(const uint32_t* codes, uint32_t n) {
+    uint64_t bad = 0;
+#pragma omp parallel for reduction(+ : bad)
+    for (int64_t i = 0; i < static_cast<int64_t>(n); ++i) {
+        const uint32_t c1 = OctEncode(OctDecode(codes[i]));
+        if (OctEncode(OctDecode(c1)) != c1) ++bad;
+    }
+    return bad;
 }
 
 void oracle_sincos(const float* phi, uint32_t n, float* s, float* c) {
