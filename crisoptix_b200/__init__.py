@@ -53,10 +53,11 @@ def default_params(scene_size: float, **overrides) -> _abi.Params:
 
 
 class Scene:
-    """Scene(instances, emitters): flattens instances and builds the device
-    BVH on the current CUDA device."""
+    """Scene(instances, emitters): flattens instances and builds the BVH of
+    the current CUDA device (on the device by default; builder=BVH_HOST builds
+    it on the host)."""
 
-    def __init__(self, desc: SceneDesc):
+    def __init__(self, desc: SceneDesc, builder: int = _abi.BVH_DEVICE):
         lib = load()
         self.desc = desc
         self._keep = []
@@ -108,6 +109,7 @@ class Scene:
         d.num_emitters = len(desc.emitters)
         d.emitter_faces = arr(desc.emitter_faces, np.float32)
         d.num_emitter_faces = len(desc.emitter_faces)
+        d.bvh_builder = int(builder)
         if desc.material_textures is not None:
             mt = np.ascontiguousarray(desc.material_textures, np.int32)
             if mt.shape != (len(desc.materials), 3):

@@ -27,6 +27,8 @@ RESTIR_PT = 1
 CONDITIONAL_RESTIR = 2
 RADIUS_CONSTANT = 0
 RADIUS_PATH_LENGTH = 1
+BVH_DEVICE = 0
+BVH_HOST = 1
 STORAGE_FP32 = 0
 STORAGE_FP16 = 1
 SPEC_COLOR = 0
@@ -69,7 +71,8 @@ class SceneDesc(ctypes.Structure):
                 ("triangle_material", c_vp), ("num_triangles", c_u32), ("materials", c_vp), ("num_materials", c_u32),
                 ("meshes", c_vp), ("num_meshes", c_u32), ("instances", c_vp), ("num_instances", c_u32),
                 ("emitters", c_vp), ("num_emitters", c_u32), ("emitter_faces", c_vp), ("num_emitter_faces", c_u32),
-                ("uvs", c_vp), ("textures", c_vp), ("num_textures", c_u32), ("material_textures", c_vp)]
+                ("uvs", c_vp), ("textures", c_vp), ("num_textures", c_u32), ("material_textures", c_vp),
+                ("bvh_builder", c_u32)]
 
 
 class Texture(ctypes.Structure):
@@ -217,6 +220,8 @@ ENTRY_POINTS = {
     "crisb_endpoint_search_status": (c_i32, [c_vp]),
     "crisb_endpoint_search_set_visit_cap": (c_i32, [c_u32]),
     "crisb_selftest_kat": (c_i32, [c_i32, c_vp, c_u32, c_vp, c_vp]),
+    "crisb_selftest_sort": (c_i32, [c_vp, c_vp, c_u32, c_vp, ctypes.c_size_t, c_vp]),
+    "crisb_selftest_sort_temp_bytes": (ctypes.c_size_t, [c_u32]),
 }
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libcrisb.so")

@@ -15,7 +15,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libcrisb.so")
 SOURCES = ["api.cu", "passes.cu", "search.cu", "reuse_passes.cu", "wavefront.cu", "bvh_build.cpp", "adjoint.cu", "tonemap.cu",
-           "context.cpp", "selftest.cu"]
+           "context.cpp", "selftest.cu", "radix_sort.cu",
+           "bvh_device.cu"]
 
 
 def nvcc_path() -> str:

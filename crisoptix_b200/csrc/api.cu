@@ -4,7 +4,6 @@
 // Mirrors Scene (src/Scene.cpp), Camera::GetData (src/Camera.cpp:20-32) and
 // Renderer (src/Renderer.cpp).  No call throws across the ABI; failures are
 // status codes with a per-thread message (crisb_last_error).
-#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -14,7 +13,9 @@
 #include <string>
 #include <vector>
 
+#include "bvh_device.h"
 #include "passes.cuh"
+#include "radix_sort.h"
 #include "records.cuh"
 
 namespace crisb {
@@ -222,6 +223,7 @@ struct crisb_scene {
     std::vector<float> h_uv;  // 6 per triangle when the scene has uvs
     DevBuf<Bvh4Node> nodes;
     int bvh_max_stack = 0, bvh_max_depth = 0;
+    bool bvh_on_device = false;  // built by build_wide_bvh_device
     DevBuf<float4> tris;
     DevBuf<float4> shade;
     DevBuf<crisb_material> mats;
@@ -407,6 +409,58 @@ void upload_textures(const crisb_scene_desc& d, crisb_scene& s) {
     s.textured = true;
 }
 
+// The scene BVH built on the device (bvh_device.h), then copied back once for
+// the same structural check as a host-built tree (every triangle in one leaf,
+// boxes containing their subtrees, the traversal stack bound).  Returns false
+// when the tree would need a deeper traversal stack than the kernels have
+// (the host builder's median fallback then bounds the depth).
+bool build_bvh_on_device(crisb_scene& s) {
+    const uint32_t n = s.num_tris;
+    float max_abs = 0.0f;
+    for (float v : s.h_pos) max_abs = std::max(max_abs, std::fabs(v));
+    DevBuf<float> pos;
+    pos.upload(s.h_pos.data(), std::max<size_t>(s.h_pos.size(), 1));
+    DeviceWideBvh db;
+    check(build_wide_bvh_device(pos.p, n, kTriLeafMax, box_margin(max_abs), nullptr, &db), "device BVH build");
+    WideBvh hb;
+    hb.nodes.resize(db.num_nodes);
+    std::vector<float4> t3(3 * static_cast<size_t>(std::max<uint32_t>(n, 1)));
+    cudaError_t e = cudaMemcpy(hb.nodes.data(), db.nodes, db.num_nodes * sizeof(Bvh4Node), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(t3.data(), db.tris, t3.size() * sizeof(float4), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        cudaFree(db.nodes);
+        cudaFree(db.tris);
+        check(e, "device BVH copy");
+    }
+    hb.order.resize(n);
+    for (uint32_t i = 0; i < n; ++i) std::memcpy(&hb.order[i], &t3[3 * i + 2].w, 4);
+    hb.max_stack = 1 << 30;
+    int stack = 0;
+    try {
+        stack = validate_wide_bvh(hb, s.h_pos.data(), n, kTriLeafMax);
+    } catch (const std::runtime_error& ex) {
+        cudaFree(db.nodes);
+        cudaFree(db.tris);
+        throw Error(CRISB_ERR_INVALID_ARGUMENT, std::string("device scene build: ") + ex.what());
+    }
+    if (stack > kTraversalStack) {
+        cudaFree(db.nodes);
+        cudaFree(db.tris);
+        return false;
+    }
+    s.nodes.release();
+    s.nodes.p = db.nodes;
+    s.nodes.n = db.num_nodes;
+    s.tris.release();
+    s.tris.p = db.tris;
+    s.tris.n = 3 * static_cast<size_t>(std::max<uint32_t>(n, 1));
+    s.bvh_max_stack = stack;
+    s.bvh_max_depth = db.binary_depth;
+    s.bvh_on_device = true;
+    check(cudaDeviceSynchronize(), "scene build");
+    return true;
+}
+
 void build_scene(const crisb_scene_desc& d, crisb_scene& s) {
     check(cudaGetDevice(&s.device), "cudaGetDevice");
     flatten(d, s);
@@ -432,6 +486,8 @@ void build_scene(const crisb_scene_desc& d, crisb_scene& s) {
     upload_textures(d, s);
     s.err.alloc(1);
     check(cudaMemset(s.err.p, 0, sizeof(int)), "memset");
+    require(d.bvh_builder == CRISB_BVH_DEVICE || d.bvh_builder == CRISB_BVH_HOST, "scene: unknown bvh_builder");
+    if (d.bvh_builder == CRISB_BVH_DEVICE && build_bvh_on_device(s)) return;
     // 4-wide SAH BVH built on the host; triangles stored in leaf order
     WideBvh bvh = build_wide_bvh(s.h_pos.data(), n, kTriLeafMax, kMedianDepth);
     if (bvh.max_stack > kTraversalStack) {
@@ -447,6 +503,7 @@ void build_scene(const crisb_scene_desc& d, crisb_scene& s) {
     }
     s.bvh_max_stack = bvh.max_stack;
     s.bvh_max_depth = bvh.max_depth;
+    s.bvh_on_device = false;
     std::vector<float4> tris(3 * static_cast<size_t>(std::max<uint32_t>(n, 1)), make_float4(0, 0, 0, 0));
     for (uint32_t i = 0; i < n; ++i) {
         const uint32_t prim = bvh.order[i];
@@ -648,10 +705,7 @@ struct crisb_renderer {
                                                                          b0.sres_cur, b0.sres_next, canon_suffix.p,
                                                                          gbuf.p, p);
         check(cudaGetLastError(), "init records");
-        size_t need = 0;
-        check(cub::DeviceRadixSort::SortKeys(nullptr, need, knn.keys_in.p, knn.keys.p, static_cast<int>(p), 0, 64),
-              "sort size");
-        sort_temp.alloc(need);
+        sort_temp.alloc(rsort::temp_bytes(p));
         check(cudaDeviceSynchronize(), "renderer init");
     }
 
@@ -800,13 +854,11 @@ struct crisb_renderer {
             record(4, st);
             lbvh::Work w = knn.work(err.p);
             launch_store_entries(s, fp, bufs(), w, bounds.p, st);
-            size_t have = sort_temp.bytes();
-            check(cub::DeviceRadixSort::SortKeys(sort_temp.p, have, knn.keys_in.p, knn.keys.p, static_cast<int>(P()),
-                                                 0, 64, st),
+            check(rsort::sort_high32(knn.keys_in.p, knn.keys.p, sort_temp.p, sort_temp.bytes(), P(), st),
                   "radix sort");
             launch_knn_finish(fp, bufs(), w, knn_leaf.p, st);
             if (m) m->mark(kClsSearch, st);
-            launches += 3 + 4;  // own kernels; the radix sort's library kernels are not counted
+            launches += 3 + 4 + rsort::kLaunches;
             record(5, st);
             if (params.gather_n == 1) {
                 launch_final_gather_split(s, fp, bufs(), out, st, m);

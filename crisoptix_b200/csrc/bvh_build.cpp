@@ -340,7 +340,7 @@ WideBvh build_wide_bvh(const float* pos, uint32_t n, int leaf_max, int median_de
     return r;
 }
 
-void validate_wide_bvh(const WideBvh& bvh, const float* pos, uint32_t n, int leaf_max) {
+int validate_wide_bvh(const WideBvh& bvh, const float* pos, uint32_t n, int leaf_max) {
     auto fail = [](const char* what) { throw std::runtime_error(std::string("bvh check: ") + what); };
     const size_t nn = bvh.nodes.size();
     if (nn == 0) fail("no root");
@@ -408,6 +408,7 @@ void validate_wide_bvh(const WideBvh& bvh, const float* pos, uint32_t n, int lea
     for (size_t i = 0; i < nn; ++i)
         if (!seen_node[i]) fail("unreachable node");
     if (max_stack > bvh.max_stack) fail("stack bound");
+    return max_stack;
 }
 
 }  // namespace crisb

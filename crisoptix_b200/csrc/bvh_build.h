@@ -59,7 +59,8 @@ WideBvh build_wide_bvh(const float* pos, uint32_t num_tris, int leaf_max, int me
 // Structural check before the tree goes to the device: links in range, every
 // triangle in exactly one leaf, leaves of at most `leaf_max` triangles, child
 // boxes containing their subtrees, each inner node reached once, and the
-// traversal stack bound recomputed.  Throws std::runtime_error on a failure.
-void validate_wide_bvh(const WideBvh& bvh, const float* pos, uint32_t num_tris, int leaf_max);
+// traversal stack bound recomputed (it must not exceed bvh.max_stack, and is
+// returned).  Throws std::runtime_error on a failure.
+int validate_wide_bvh(const WideBvh& bvh, const float* pos, uint32_t num_tris, int leaf_max);
 
 }  // namespace crisb

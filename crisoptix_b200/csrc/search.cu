@@ -1,8 +1,6 @@
 // search.cu -- the prefix-endpoint neighbour search as a standalone operation:
 // build the search structure over caller-given entries, then answer a batch
 // of query points.  The renderer runs the same query inside its final gather.
-#include <cub/device/device_radix_sort.cuh>
-
 #include <algorithm>
 #include <atomic>
 #include <cstring>
@@ -13,6 +11,7 @@
 
 #include "context.h"
 #include "knn.cuh"
+#include "radix_sort.h"
 
 namespace crisb {
 
@@ -90,13 +89,7 @@ inline size_t layout(uint32_t cap, size_t sort_bytes, char* base, Scratch* s) {
     return off;
 }
 
-inline size_t sort_temp_bytes(uint32_t cap) {
-    size_t need = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, need, static_cast<const uint64_t*>(nullptr),
-                                   static_cast<uint64_t*>(nullptr), static_cast<int>(std::max<uint32_t>(cap, 2)), 0,
-                                   64);
-    return need;
-}
+inline size_t sort_temp_bytes(uint32_t cap) { return rsort::temp_bytes(std::max<uint32_t>(cap, 2)); }
 
 __global__ void k_init(unsigned int* ob, uint32_t* n, int* err) {
     if (threadIdx.x < 3) ob[threadIdx.x] = float_to_ordered(INFINITY);
@@ -198,9 +191,7 @@ inline cudaError_t run(const Scratch& s, const float4* entries, uint32_t n_entri
     if (n_entries > 0) {
         k_bounds<<<grid(n_entries), kBlock, 0, st>>>(entries, n_entries, s.bounds, s.w.n);
         k_keys<<<grid(n_entries), kBlock, 0, st>>>(entries, n_entries, s.bounds, s.w.keys_in);
-        size_t bytes = s.sort_bytes;
-        const cudaError_t e = cub::DeviceRadixSort::SortKeys(s.sort_temp, bytes, s.w.keys_in, s.w.keys,
-                                                             static_cast<int>(n_entries), 0, 64, st);
+        const cudaError_t e = rsort::sort_high32(s.w.keys_in, s.w.keys, s.sort_temp, s.sort_bytes, n_entries, st);
         if (e != cudaSuccess) return e;
         k_leaves<<<grid(n_entries), kBlock, 0, st>>>(entries, s.w, s.leaf);
     }

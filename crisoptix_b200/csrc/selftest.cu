@@ -4,6 +4,7 @@
 // rendering path calls this.
 #include <string>
 
+#include "radix_sort.h"
 #include "rt_restir.cuh"
 
 namespace crisb {
@@ -148,3 +149,20 @@ extern "C" int crisb_selftest_kat(int fn, const void* in_dev, uint32_t n, void* 
     }
     return CRISB_OK;
 }
+
+extern "C" int crisb_selftest_sort(const uint64_t* in_dev, uint64_t* out_dev, uint32_t n, void* temp_dev,
+                                   size_t temp_bytes, void* stream) {
+    if (n > 0 && (!in_dev || !out_dev || !temp_dev || temp_bytes < crisb::rsort::temp_bytes(n))) {
+        crisb::set_last_error("selftest sort: null array or scratch too small");
+        return CRISB_ERR_INVALID_ARGUMENT;
+    }
+    const cudaError_t e =
+        crisb::rsort::sort_high32(in_dev, out_dev, temp_dev, temp_bytes, n, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) {
+        crisb::set_last_error(std::string("selftest sort: ") + cudaGetErrorString(e));
+        return CRISB_ERR_CUDA;
+    }
+    return CRISB_OK;
+}
+
+extern "C" size_t crisb_selftest_sort_temp_bytes(uint32_t n) { return crisb::rsort::temp_bytes(n); }

@@ -137,7 +137,16 @@ typedef struct crisb_scene_desc {
     uint32_t num_textures;
     const int32_t* material_textures; /* num_materials * 3: diffuse, specular,
                                          roughness texture index or -1 */
+    /* Builder of the scene BVH (the OptiX GAS/IAS build of src/Scene.cpp:73-160
+     * and src/Mesh.cpp:54-120): CRISB_BVH_DEVICE (0) or CRISB_BVH_HOST.  Any
+     * builder gives the same hits; only traversal speed differs. */
+    uint32_t bvh_builder;
 } crisb_scene_desc;
+
+/* crisb_scene_desc.bvh_builder */
+#define CRISB_BVH_DEVICE 0 /* on the GPU: Morton order, PLOC clustering, SAH
+                              collapse into 4-wide nodes */
+#define CRISB_BVH_HOST 1   /* on the host: binned SAH, collapsed into 4-wide nodes */
 
 /* ---- camera (Camera, include/graph/Camera.h:24-79) --------------------- */
 typedef struct crisb_camera {
@@ -607,6 +616,15 @@ int crisb_abi_sizes(uint32_t* out, uint32_t n);
  * uses it).  Asynchronous on `stream`. */
 int crisb_selftest_kat(int fn, const void* in_dev, uint32_t n, void* out_dev,
                        void* stream);
+
+/* Test hook: the library's radix sort of the prefix-endpoint keys on its own
+ * (the per-frame structure rebuild uses it, replacing the OptiX GAS rebuild of
+ * src/PrefixAccelStruct.cpp:66-221): out_dev = in_dev's n keys sorted stably
+ * by their high 32 bits; temp_dev holds crisb_selftest_sort_temp_bytes(n)
+ * bytes.  Asynchronous on `stream`. */
+int crisb_selftest_sort(const uint64_t* in_dev, uint64_t* out_dev, uint32_t n,
+                        void* temp_dev, size_t temp_bytes, void* stream);
+size_t crisb_selftest_sort_temp_bytes(uint32_t n);
 
 #ifdef __cplusplus
 }
