@@ -327,7 +327,10 @@ def run_crisb(args):
     p = params_for(args.workload, sc.scene_size)
     p.storage = _abi.STORAGE_FP16 if args.storage == "fp16" else _abi.STORAGE_FP32
     p.motion_mode = _abi.MOTION_REPROJECT if args.motion == "reproject" else _abi.MOTION_NONE
+    free0 = torch.cuda.mem_get_info()[0]
     r = Renderer(W, H, sc, p)
+    torch.cuda.synchronize()
+    renderer_bytes = free0 - torch.cuda.mem_get_info()[0]
     r.set_graph(not args.no_graph)
     tuned = r.autotune(cam, 3) if args.autotune else None
     stream = torch.cuda.Stream()
@@ -485,13 +488,16 @@ def run_crisb(args):
             "warmup": args.warmup, "ms_per_step": ms_per_frame, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": dict(config_for(args.workload, W, H, sc.num_triangles, p, ppp, world, not args.no_graph),
-                           trace_grid=tuned if tuned is not None else 8),
+                           launch=tuned if tuned is not None else {"trace_block": 128, "trace_grid": 8,
+                                                                  "jobs_per_pixel": r.job_capacity()}),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 48, "d2h_bytes_per_step": W * H * 12,
                     "copies": "each frame's RGB copied to pinned host memory on a copy stream, overlapping the "
                               "next frame (two output buffers)"},
             "roofline": roofline, "traversal": traversal, "phases_ms": phases, "pass_ms": pass_ms,
             "cpu_baseline": cb, "clocks": clk,
-            "gpu_launches": launches_per_frame * args.steps, "image_mean": img_mean, "tonemap": tone}
+            "gpu_launches": launches_per_frame * args.steps, "image_mean": img_mean, "tonemap": tone,
+            "memory": {"renderer_bytes": renderer_bytes, "bytes_per_pixel": renderer_bytes / (W * H),
+                       "note": "device memory the renderer allocates (free memory before and after creating it)"}}
     if qual is not None:
         line["quality"] = qual
     if arms is not None:
@@ -513,7 +519,11 @@ def multiview_time(storage: int, batched: bool, steps: int, warmup: int, motion:
     p.storage = storage
     p.motion_mode = motion
     views = scenes.multiview_cameras(seed=2)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
     rs = [Renderer(w, h, sc, p) for _, w, h in views]
+    torch.cuda.synchronize()
+    mem = free0 - torch.cuda.mem_get_info()[0]
     outs = [torch.zeros(w * h * 3, dtype=torch.float32, device="cuda") for _, w, h in views]
     ptrs = [o.data_ptr() for o in outs]
     px = sum(w * h for _, w, h in views)
@@ -544,7 +554,7 @@ def multiview_time(storage: int, batched: bool, steps: int, warmup: int, motion:
     del batch, rs, outs
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
-    return {"ms_per_frame": ms, "value": ppp * px * 1000.0 / ms, "pixels": px}
+    return {"ms_per_frame": ms, "value": ppp * px * 1000.0 / ms, "pixels": px, "renderer_bytes": mem}
 
 
 def run_multiview(args):

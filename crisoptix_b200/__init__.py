@@ -221,12 +221,16 @@ class Renderer:
     def set_trace_grid(self, blocks_per_resident_block: int):
         check(load().crisb_set_trace_grid(self.handle, int(blocks_per_resident_block)))
 
-    def autotune(self, camera: CameraDesc, frames: int = 3) -> int:
-        """Pick the traversal launch shape by timing candidates on a scratch
-        renderer (this renderer's state is untouched); returns the choice."""
-        v = ctypes.c_uint32()
-        check(load().crisb_autotune(self.handle, ctypes.byref(camera_struct(camera)), int(frames), ctypes.byref(v)))
-        return v.value
+    def autotune(self, camera: CameraDesc, frames: int = 3) -> dict:
+        """Pick the launch settings (traversal block size and grid, job
+        capacity) by timing candidates on a scratch renderer (this renderer's
+        state is untouched); applies and returns the choices."""
+        t = _abi.Tuning()
+        check(load().crisb_autotune_ex(self.handle, ctypes.byref(camera_struct(camera)), int(frames), ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in t._fields_}
+
+    def set_trace_block(self, threads: int):
+        check(load().crisb_set_trace_block(self.handle, int(threads)))
 
     def set_motion_vectors(self, motion_dev_ptr: int):
         """width * height float pairs on the device for MOTION_VECTORS (0 clears)."""
@@ -235,6 +239,16 @@ class Renderer:
     def set_srgb_output(self, srgb_dev_ptr: int):
         """Tone-map each frame into width * height * 3 device bytes (0 stops)."""
         check(load().crisb_set_srgb_output(self.handle, srgb_dev_ptr or None))
+
+    def set_job_capacity(self, jobs_per_pixel: int):
+        """Shift-machine job records per pixel (memory against speed; results
+        do not depend on it)."""
+        check(load().crisb_set_job_capacity(self.handle, int(jobs_per_pixel)))
+
+    def job_capacity(self) -> int:
+        v = ctypes.c_uint32()
+        check(load().crisb_get_job_capacity(self.handle, ctypes.byref(v)))
+        return v.value
 
     def set_graph(self, enable: bool):
         """Run frames as one CUDA graph of the pass chain (default) or launch

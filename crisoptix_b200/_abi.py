@@ -75,6 +75,10 @@ class SceneDesc(ctypes.Structure):
                 ("bvh_builder", c_u32)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("trace_block", c_u32), ("trace_grid", c_u32), ("jobs_per_pixel", c_u32), ("frame_ms", c_f)]
+
+
 class Texture(ctypes.Structure):
     _fields_ = [("rgba", c_vp), ("width", c_u32), ("height", c_u32)]
 
@@ -207,6 +211,10 @@ ENTRY_POINTS = {
     "crisb_set_trace_grid": (c_i32, [c_vp, c_u32]),
     "crisb_autotune": (c_i32, [c_vp, ctypes.POINTER(Camera), c_u32, ctypes.POINTER(c_u32)]),
     "crisb_set_graph": (c_i32, [c_vp, c_i32]),
+    "crisb_set_job_capacity": (c_i32, [c_vp, c_u32]),
+    "crisb_set_trace_block": (c_i32, [c_vp, c_u32]),
+    "crisb_autotune_ex": (c_i32, [c_vp, ctypes.POINTER(Camera), c_u32, ctypes.POINTER(Tuning)]),
+    "crisb_get_job_capacity": (c_i32, [c_vp, ctypes.POINTER(c_u32)]),
     "crisb_frame_index": (c_i32, [c_vp, ctypes.POINTER(c_u64)]),
     "crisb_frame_random": (c_i32, [c_vp, ctypes.POINTER(c_u32)]),
     "crisb_set_timing": (c_i32, [c_vp, c_i32]),

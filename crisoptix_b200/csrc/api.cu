@@ -560,10 +560,14 @@ struct crisb_renderer {
     DevBuf<float4> shift_out, gather_state;
     DevBuf<crisb_suffix_res_rec> gather_cs;
     DevBuf<crisb_prefix_rec> gather_cp;
-    DevBuf<WfPath> wf;
-    DevBuf<uint32_t> wf_queue[4], wf_count;
-    DevBuf<ShiftJob> jobs;
-    DevBuf<uint32_t> job_queue[4], job_qcount;
+    // The path machines' states and ray queues and the shift machines' job
+    // records and ray queues share one allocation: within a pass the path
+    // machines finish (the pass's finish kernel reads the last path field, the
+    // RNG state) before its shift jobs begin, and the next pass's path
+    // machines start after them.
+    DevBuf<char> machine_state;
+    DevBuf<uint32_t> machine_queue[4];
+    DevBuf<uint32_t> wf_count, job_qcount;
     uint32_t slots = 0;
     DevBuf<unsigned int> bounds;
     DevBuf<char> sort_temp;
@@ -628,13 +632,14 @@ struct crisb_renderer {
         b.gather_cs = gather_cs.p;
         b.gather_state = gather_state.p;
         b.slots = slots;
+        b.job_cap = static_cast<uint32_t>(std::min<size_t>(job_capacity(), 0xFFFFFFFFu));
         b.tally = timing >= 2 && ray_count.p ? ray_count.p + kRayCounters : nullptr;
-        b.wf = wf.p;
-        for (int q = 0; q < 4; ++q) b.wf_queue[q] = wf_queue[q].p;
+        b.wf = reinterpret_cast<WfPath*>(machine_state.p);
+        for (int q = 0; q < 4; ++q) b.wf_queue[q] = machine_queue[q].p;
         b.wf_count = wf_count.p;
         b.gather_cp = gather_cp.p;
-        b.jobs = jobs.p;
-        for (int q = 0; q < 4; ++q) b.job_queue[q] = job_queue[q].p;
+        b.jobs = reinterpret_cast<ShiftJob*>(machine_state.p);
+        for (int q = 0; q < 4; ++q) b.job_queue[q] = machine_queue[q].p;
         b.job_qcount = job_qcount.p;
         return b;
     }
@@ -656,14 +661,27 @@ struct crisb_renderer {
         return 2 * m;
     }
 
+    // Shift jobs: the list and the results have a slot for every possible
+    // job (4 + 16 bytes); the machines' job records and ray queues (96 bytes
+    // a job) hold jobs_per_pixel x P jobs, and a pass's jobs beyond them run
+    // in the overflow kernel -- the same results, traced in place.  A 1080p
+    // frame of the large workload runs about 2.5 jobs per pixel over all its
+    // passes, against 16 slots; a capacity of 1 to 4 jobs per pixel renders
+    // it within 1% of the same time.
+    static constexpr uint32_t kDefaultJobsPerPixel = 2;
+    uint32_t jobs_per_pixel = kDefaultJobsPerPixel;
+
+    size_t job_capacity() const { return P() * static_cast<size_t>(std::min(jobs_per_pixel, slots)); }
+
     void allocate_jobs() {
         const size_t p = P();
         slots = slots_for(params);
         spatial_nbr.alloc(p * (slots / 2));
         job_items.alloc(p * slots);
         shift_out.alloc(p * slots);
-        jobs.alloc(p * slots);
-        for (int q = 0; q < 4; ++q) job_queue[q].alloc(p * slots);
+        const size_t state = std::max(p * sizeof(WfPath), job_capacity() * sizeof(ShiftJob));
+        machine_state.alloc((state + 255) & ~static_cast<size_t>(255));
+        for (int q = 0; q < 4; ++q) machine_queue[q].alloc(std::max(p, job_capacity()));
     }
 
     void allocate() {
@@ -674,8 +692,6 @@ struct crisb_renderer {
         gather_cs.alloc(p);
         gather_state.alloc(2 * static_cast<size_t>(p));
         gather_cp.alloc(p);
-        wf.alloc(p);
-        for (int q = 0; q < 4; ++q) wf_queue[q].alloc(p);
         wf_count.alloc(4);
         check(cudaMemset(wf_count.p, 0, wf_count.bytes()), "memset");
         job_qcount.alloc(4);
@@ -725,6 +741,7 @@ struct crisb_renderer {
     // out the tail (8 measured best on the 1080p workload; crisb_autotune
     // picks it per workload)
     uint32_t trace_grid = 8;
+    uint32_t trace_block = 128;  // threads per traversal block
     // optional sRGB bytes of each frame (ToneMapping after LaunchFrame,
     // src/main.cpp:122-127), written by a last kernel of the frame
     uint8_t* srgb_out = nullptr;
@@ -799,6 +816,7 @@ struct crisb_renderer {
         fp.back = back;
         fp.k = K();
         fp.trace_grid = trace_grid;
+        fp.trace_block = trace_block;
         require(params.motion_mode != CRISB_MOTION_VECTORS || motion != nullptr,
                 "render_frame: CRISB_MOTION_VECTORS without motion vectors");
         fp.motion = motion;
@@ -885,6 +903,44 @@ struct crisb_renderer {
         ++launches;
     }
 };
+
+namespace {
+
+// Times candidate settings of one knob on renderer t: every candidate renders
+// `frames` frames of `cam`, interleaved frame by frame so that drift hits all
+// of them alike, after one untimed frame each (graph instantiation per shape).
+// Returns the per-candidate total milliseconds.
+template <class Apply>
+std::vector<float> time_candidates(crisb_renderer& t, const crisb_camera& cam, float* out, cudaStream_t st,
+                                   uint32_t frames, size_t count, Apply apply) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    check(cudaEventCreate(&e0), "event");
+    check(cudaEventCreate(&e1), "event");
+    std::vector<float> total(count, 0.0f);
+    for (size_t k = 0; k < count; ++k) {
+        apply(k);
+        t.render(cam, out, st);
+    }
+    for (uint32_t f = 0; f < std::max<uint32_t>(frames, 3); ++f) {
+        for (size_t k = 0; k < count; ++k) {
+            apply(k);
+            check(cudaEventRecord(e0, st), "event");
+            t.render(cam, out, st);
+            check(cudaEventRecord(e1, st), "event");
+            check(cudaEventSynchronize(e1), "sync");
+            float ms = 0.0f;
+            check(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+            total[k] += ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return total;
+}
+
+size_t fastest(const std::vector<float>& v) { return static_cast<size_t>(std::min_element(v.begin(), v.end()) - v.begin()); }
+
+}  // namespace
 
 extern "C" {
 
@@ -1300,7 +1356,7 @@ int crisb_set_trace_grid(crisb_renderer* r, uint32_t blocks_per_resident_block) 
     });
 }
 
-int crisb_autotune(crisb_renderer* r, const crisb_camera* cam, uint32_t frames, uint32_t* chosen) {
+int crisb_autotune_ex(crisb_renderer* r, const crisb_camera* cam, uint32_t frames, crisb_tuning* out) {
     return guarded([&] {
         require(r && cam && frames > 0, "autotune: null argument or no frames");
         // a scratch renderer of the same scene, size and parameters: the
@@ -1309,48 +1365,72 @@ int crisb_autotune(crisb_renderer* r, const crisb_camera* cam, uint32_t frames, 
         if (crisb_renderer_create(r->scene, r->width, r->height, &r->params, &t) != CRISB_OK)
             throw Error(CRISB_ERR_CUDA, g_last_error);
         std::unique_ptr<crisb_renderer> tmp(t);
-        DevBuf<float> out;
-        out.alloc(static_cast<size_t>(r->P()) * 3);
+        DevBuf<float> buf;
+        buf.alloc(static_cast<size_t>(r->P()) * 3);
         cudaStream_t st = nullptr;
-        cudaEvent_t e0 = nullptr, e1 = nullptr;
         check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
-        check(cudaEventCreate(&e0), "event");
-        check(cudaEventCreate(&e1), "event");
-        const uint32_t cand[] = {1, 2, 4, 8, 16};
-        constexpr int kCand = 5;
         // warm up until the reservoirs carry history (the per-frame cost of a
-        // fresh renderer's first frames is lower), then time the candidates
-        // interleaved frame by frame so that drift hits all of them alike
-        for (int f = 0; f < 4; ++f) tmp->render(*cam, out.p, st);
-        for (int k = 0; k < kCand; ++k) {  // graph instantiation per shape
-            tmp->trace_grid = cand[k];
-            tmp->render(*cam, out.p, st);
-        }
-        float total[kCand] = {};
-        for (uint32_t f = 0; f < std::max<uint32_t>(frames, 3); ++f) {
-            for (int k = 0; k < kCand; ++k) {
-                tmp->trace_grid = cand[k];
-                check(cudaEventRecord(e0, st), "event");
-                tmp->render(*cam, out.p, st);
-                check(cudaEventRecord(e1, st), "event");
-                check(cudaEventSynchronize(e1), "sync");
-                float ms = 0.0f;
-                check(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
-                total[k] += ms;
+        // fresh renderer's first frames is lower)
+        for (int f = 0; f < 4; ++f) tmp->render(*cam, buf.p, st);
+        // coordinate descent: traversal block size, traversal grid, then the
+        // shift machines' job capacity (the smallest within 1% of the fastest:
+        // capacity costs memory, 96 bytes per job)
+        const uint32_t blocks[] = {64, 128, 256};
+        auto tb = time_candidates(*tmp, *cam, buf.p, st, frames, 3, [&](size_t k) { tmp->trace_block = blocks[k]; });
+        tmp->trace_block = blocks[fastest(tb)];
+        const uint32_t grids[] = {1, 2, 4, 8, 16};
+        auto tg = time_candidates(*tmp, *cam, buf.p, st, frames, 5, [&](size_t k) { tmp->trace_grid = grids[k]; });
+        tmp->trace_grid = grids[fastest(tg)];
+        std::vector<uint32_t> caps;
+        for (uint32_t c : {1u, 2u, 4u, 8u})
+            if (c <= tmp->slots) caps.push_back(c);
+        if (caps.empty() || caps.back() != tmp->slots) caps.push_back(tmp->slots);
+        const uint32_t base_cap = tmp->jobs_per_pixel;
+        auto tc = time_candidates(*tmp, *cam, buf.p, st, frames, caps.size(), [&](size_t k) {
+            if (tmp->jobs_per_pixel == caps[k]) return;
+            check(cudaStreamSynchronize(st), "sync");
+            tmp->jobs_per_pixel = caps[k];
+            tmp->allocate_jobs();
+        });
+        const float best_cap_ms = tc[fastest(tc)];
+        uint32_t cap = caps.back();
+        for (size_t k = 0; k < caps.size(); ++k)
+            if (tc[k] <= 1.01f * best_cap_ms) {
+                cap = caps[k];
+                break;
             }
-        }
-        uint32_t best = r->trace_grid;
-        float best_ms = INFINITY;
-        for (int k = 0; k < kCand; ++k)
-            if (total[k] < best_ms) {
-                best_ms = total[k];
-                best = cand[k];
-            }
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
+        (void)base_cap;
+        check(cudaStreamSynchronize(st), "sync");
         cudaStreamDestroy(st);
-        r->trace_grid = best;
-        if (chosen) *chosen = best;
+        r->trace_block = tmp->trace_block;
+        r->trace_grid = tmp->trace_grid;
+        if (r->jobs_per_pixel != cap) {
+            check(cudaDeviceSynchronize(), "job capacity");
+            r->jobs_per_pixel = cap;
+            r->allocate_jobs();
+        }
+        if (out) {
+            out->trace_block = r->trace_block;
+            out->trace_grid = r->trace_grid;
+            out->jobs_per_pixel = std::min(cap, r->slots);
+            out->frame_ms = std::min(tb[fastest(tb)], std::min(tg[fastest(tg)], best_cap_ms)) /
+                            static_cast<float>(std::max<uint32_t>(frames, 3));
+        }
+    });
+}
+
+int crisb_autotune(crisb_renderer* r, const crisb_camera* cam, uint32_t frames, uint32_t* chosen) {
+    crisb_tuning t{};
+    const int rc = crisb_autotune_ex(r, cam, frames, &t);
+    if (rc == CRISB_OK && chosen) *chosen = t.trace_grid;
+    return rc;
+}
+
+int crisb_set_trace_block(crisb_renderer* r, uint32_t threads) {
+    return guarded([&] {
+        require(r != nullptr, "null renderer");
+        require(threads == 64 || threads == 128 || threads == 256, "trace block: 64, 128 or 256 threads");
+        r->trace_block = threads;
     });
 }
 
@@ -1372,6 +1452,24 @@ int crisb_frame_random(const crisb_renderer* r, uint32_t* out) {
     return guarded([&] {
         require(r && out, "null argument");
         *out = r->random;
+    });
+}
+
+int crisb_set_job_capacity(crisb_renderer* r, uint32_t jobs_per_pixel) {
+    return guarded([&] {
+        require(r != nullptr, "null renderer");
+        require(jobs_per_pixel <= CRISB_MAX_GATHER_M * 2, "job capacity: at most 64 jobs per pixel");
+        if (jobs_per_pixel == r->jobs_per_pixel) return;
+        check(cudaDeviceSynchronize(), "job capacity");
+        r->jobs_per_pixel = jobs_per_pixel;
+        r->allocate_jobs();
+    });
+}
+
+int crisb_get_job_capacity(const crisb_renderer* r, uint32_t* jobs_per_pixel) {
+    return guarded([&] {
+        require(r && jobs_per_pixel, "null argument");
+        *jobs_per_pixel = std::min(r->jobs_per_pixel, r->slots);
     });
 }
 

@@ -76,6 +76,9 @@ struct Bufs {
     crisb_suffix_res_rec* gather_cs;  // P: canonical suffix of the final gather
     float4* gather_state;   // P * 3: prefix f / p, canonical contribution, direct result
     uint32_t slots;         // job slots per pixel (>= 2 * max(k, spatial count, 1))
+    // capacity of the shift machines' job records and queues; list entries
+    // beyond it run in k_shift_overflow, tracing their rays in place
+    uint32_t job_cap;
     // statistics level 2 only (else null): bytes read and written by each
     // resampling kernel for the work present in the frame (kTally*)
     unsigned long long* tally;

@@ -7,6 +7,8 @@
 // and results, so one traversal kernel serves every kind of machine.
 #pragma once
 
+#include <algorithm>
+
 #include "passes.cuh"
 
 namespace crisb {
@@ -66,12 +68,30 @@ RT_D void set_occluded(ShiftJob& j, uint32_t v) { j.hit.x = __uint_as_float(v); 
 // (the last, slowest rays) overlap instead of running back to back.
 // 9 resident blocks per SM (56 registers): 13.40 -> 13.25 ms of traversal per
 // 1080p frame against 8 blocks (64 registers), despite a few more spills
-#ifndef CRISB_TRACE_MIN_BLOCKS
-#define CRISB_TRACE_MIN_BLOCKS 9
-#endif
-template <class R>
-__global__ void __launch_bounds__(kPassBlock, CRISB_TRACE_MIN_BLOCKS) k_q_trace(SceneView s, const uint32_t* qc, const uint32_t* ccnt,
-                                                        const uint32_t* qs, const uint32_t* scnt, R* rec) {
+// Block sizes of the traversal kernel (crisb_set_trace_block, tuned by
+// crisb_autotune): resident blocks per SM chosen so every size keeps the
+// register budget of 9 x 128 threads (56 registers; 64 at 256 threads).
+// 9 resident 128-thread blocks per SM: 13.40 -> 13.25 ms of traversal per
+// 1080p frame against 8 blocks (64 registers), despite a few more spills.
+template <int kB>
+struct TraceShape;
+template <>
+struct TraceShape<64> {
+    static constexpr int kMinBlocks = 18;
+};
+template <>
+struct TraceShape<128> {
+    static constexpr int kMinBlocks = 9;
+};
+template <>
+struct TraceShape<256> {
+    static constexpr int kMinBlocks = 4;
+};
+
+template <class R, int kB>
+__global__ void __launch_bounds__(kB, TraceShape<kB>::kMinBlocks) k_q_trace(SceneView s, const uint32_t* qc,
+                                                                          const uint32_t* ccnt, const uint32_t* qs,
+                                                                          const uint32_t* scnt, R* rec) {
     const uint32_t nc = *ccnt, ns = *scnt;
     const uint32_t n = nc + ns;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
@@ -103,6 +123,37 @@ inline unsigned persistent_grid(const void* kernel) {
 }
 
 inline unsigned grid_for(uint32_t n) { return (n + kPassBlock - 1) / kPassBlock; }
+
+// all blocks of `kernel` at `block` threads resident on the device at once
+inline unsigned persistent_grid_at(const void* kernel, int block) {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) == cudaSuccess && sms > 0 &&
+        per_sm > 0)
+        return static_cast<unsigned>(sms * per_sm);
+    return 148u * 4u;
+}
+
+template <class R, int kB>
+unsigned trace_grid_of() {
+    static const unsigned g = persistent_grid_at(reinterpret_cast<const void*>(k_q_trace<R, kB>), kB);
+    return g;
+}
+
+// one traversal launch over a closest-hit and a shadow queue: `block`
+// threads (64, 128 or 256) and `mult` x the blocks resident at once
+template <class R>
+void launch_trace(uint32_t block, uint32_t mult, cudaStream_t st, const SceneView& s, const uint32_t* qc,
+                  const uint32_t* ccnt, const uint32_t* qs, const uint32_t* scnt, R* rec) {
+    const uint32_t m = std::max(mult, 1u);
+    if (block == 64)
+        k_q_trace<R, 64><<<trace_grid_of<R, 64>() * m, 64, 0, st>>>(s, qc, ccnt, qs, scnt, rec);
+    else if (block == 256)
+        k_q_trace<R, 256><<<trace_grid_of<R, 256>() * m, 256, 0, st>>>(s, qc, ccnt, qs, scnt, rec);
+    else
+        k_q_trace<R, 128><<<trace_grid_of<R, 128>() * m, 128, 0, st>>>(s, qc, ccnt, qs, scnt, rec);
+}
 
 }  // namespace
 }  // namespace crisb

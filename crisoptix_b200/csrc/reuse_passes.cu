@@ -232,8 +232,9 @@ RT_D void job_push(const Bufs& b, int round, int req, uint32_t t) {
 // kTex: the scene has textured materials
 template <bool kTex>
 __global__ void __launch_bounds__(kPassBlock) k_shift_begin(SceneView s, FrameParams fp, Bufs b, int mode) {
-    const uint32_t total = *b.job_count;
-    count_jobs(s, total);
+    const uint32_t all = *b.job_count;
+    count_jobs(s, all);
+    const uint32_t total = min(all, b.job_cap);
     const bool prefix = mode == kModePrefix;
     const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
@@ -259,6 +260,33 @@ __global__ void __launch_bounds__(kPassBlock) k_shift_begin(SceneView s, FramePa
             }
         }
         job_push(b, 0, req, t);
+    }
+}
+
+// list entries beyond the machines' capacity: the same job, every ray traced
+// in place (shift_advance with inline rays is the machine's own step)
+template <bool kTex>
+__global__ void __launch_bounds__(kPassBlock) k_shift_overflow(SceneView s, FrameParams fp, Bufs b, int mode) {
+    const uint32_t total = *b.job_count;
+    const bool prefix = mode == kModePrefix;
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (uint32_t t = b.job_cap + blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        ShiftJob j;
+        j.code = b.job_items[t];
+        Hit dh;
+        const ShiftSrc src = resolve_job(fp, b, mode, j.code, &dh);
+        const Isect cur = unpack(s, dh);
+        bool ok = fl_valid(src.flags) && cur.valid;
+        if (prefix) ok = ok && fl_recon(src.flags) >= 2;
+        ok = ok && unpack(s, src.anchor).valid && unpack(s, src.recon).valid;
+        if (!ok) {
+            job_out(b, j.code, zero);
+            continue;
+        }
+        const int skip = prefix ? 2 : 1;
+        const uint32_t left = static_cast<uint32_t>(max(static_cast<int>(fl_recon(src.flags)) - skip, 0));
+        Rng srng{src.rng};
+        shift_advance<kTex>(s, b, prefix, src, j, cur, srng, splat(1.0f), left, true);
     }
 }
 
@@ -802,7 +830,7 @@ __global__ void __launch_bounds__(kPassBlock) k_prefix_combine(FrameParams fp, B
 }
 
 struct ShiftGrids {
-    unsigned begin, step, step_last;
+    unsigned begin, step, step_last, overflow;
 };
 
 template <bool kTex>
@@ -813,14 +841,11 @@ const ShiftGrids& shift_grids() {
         g.begin = persistent_grid(reinterpret_cast<const void*>(k_shift_begin<kTex>));
         g.step = persistent_grid(reinterpret_cast<const void*>(k_shift_step<false, kTex>));
         g.step_last = persistent_grid(reinterpret_cast<const void*>(k_shift_step<true, kTex>));
+        g.overflow = persistent_grid(reinterpret_cast<const void*>(k_shift_overflow<kTex>));
     });
     return g;
 }
 
-unsigned shift_trace_grid() {
-    static const unsigned g = persistent_grid(reinterpret_cast<const void*>(k_q_trace<ShiftJob>));
-    return g;
-}
 
 #define MARK(cls)          \
     do {                   \
@@ -835,11 +860,12 @@ void run_shift_jobs_as(const SceneView& s, const FrameParams& fp, const Bufs& b,
     cudaMemsetAsync(b.job_qcount, 0, 2 * sizeof(uint32_t), st);
     k_shift_begin<kTex><<<g.begin, kPassBlock, 0, st>>>(s, fp, b, mode);
     MARK(kClsShift);
+    k_shift_overflow<kTex><<<g.overflow, kPassBlock, 0, st>>>(s, fp, b, mode);
+    MARK(kClsShift);
     for (int r = 0; r < kShiftRounds; ++r) {
         const int cur = r & 1, nxt = cur ^ 1;
-        k_q_trace<ShiftJob><<<shift_trace_grid() * std::max(fp.trace_grid, 1u), kPassBlock, 0, st>>>(
-            s, b.job_queue[2 * cur], b.job_qcount + 2 * cur, b.job_queue[2 * cur + 1], b.job_qcount + 2 * cur + 1,
-            b.jobs);
+        launch_trace<ShiftJob>(fp.trace_block, fp.trace_grid, st, s, b.job_queue[2 * cur], b.job_qcount + 2 * cur,
+                               b.job_queue[2 * cur + 1], b.job_qcount + 2 * cur + 1, b.jobs);
         MARK(kClsTrace);
         if (r + 1 < kShiftRounds) {
             cudaMemsetAsync(b.job_qcount + 2 * nxt, 0, 2 * sizeof(uint32_t), st);
@@ -864,7 +890,7 @@ void run_shift_jobs(const SceneView& s0, const FrameParams& fp, const Bufs& b, i
 
 }  // namespace
 
-uint32_t shift_launches_per_phase() { return 1 + 2 * kShiftRounds; }
+uint32_t shift_launches_per_phase() { return 2 + 2 * kShiftRounds; }
 
 void launch_prefix_gen_temp_split(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out,
                                   cudaStream_t st, Marker* m) {

@@ -21,6 +21,7 @@ struct FrameParams {
     int front, back;     // 0/1 buffer selection
     uint32_t k;          // gatherM - 1
     uint32_t trace_grid; // traversal launches: blocks per resident block (host side only)
+    uint32_t trace_block; // traversal launches: threads per block, 64 / 128 / 256 (host side only)
     const float2* motion = nullptr;  // CRISB_MOTION_VECTORS: per-pixel motion vectors
     crisb_camera_data prev_cam{};    // CRISB_MOTION_REPROJECT: the previous frame's camera
     uint32_t has_prev_cam = 0;

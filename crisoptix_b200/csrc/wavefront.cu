@@ -305,14 +305,13 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_shade(SceneView s, FrameParam
 }
 
 struct WfGrids {
-    unsigned trace, shade, shade_inline;
+    unsigned shade, shade_inline;
 };
 
 const WfGrids& wf_grids() {
     static std::once_flag once;
     static WfGrids g{};
     std::call_once(once, [] {
-        g.trace = persistent_grid(reinterpret_cast<const void*>(k_q_trace<WfPath>));
         g.shade = persistent_grid(reinterpret_cast<const void*>(k_wf_shade<false>));
         g.shade_inline = persistent_grid(reinterpret_cast<const void*>(k_wf_shade<true>));
     });
@@ -338,8 +337,8 @@ void wf_rounds(const SceneView& s, const FrameParams& fp, const Bufs& b, int flo
     const int rounds = wf_round_count(fp, flow);
     for (int r = 0; r < rounds; ++r) {
         const int cur = r & 1, nxt = cur ^ 1;
-        k_q_trace<WfPath><<<g.trace * std::max(fp.trace_grid, 1u), kPassBlock, 0, st>>>(s, b.wf_queue[2 * cur], b.wf_count + 2 * cur,
-                                                          b.wf_queue[2 * cur + 1], b.wf_count + 2 * cur + 1, b.wf);
+        launch_trace<WfPath>(fp.trace_block, fp.trace_grid, st, s, b.wf_queue[2 * cur], b.wf_count + 2 * cur,
+                             b.wf_queue[2 * cur + 1], b.wf_count + 2 * cur + 1, b.wf);
         if (m) m->mark(kClsTrace, st);
         if (r + 1 < rounds) {
             cudaMemsetAsync(b.wf_count + 2 * nxt, 0, 2 * sizeof(uint32_t), st);

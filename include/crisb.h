@@ -487,6 +487,15 @@ int crisb_renderer_get_params(const crisb_renderer* r, crisb_params* out);
 int crisb_render_frame(crisb_renderer* r, const crisb_camera* cam,
                        float* out_rgb_dev, void* stream);
 
+/* Capacity of the shift machines' job records, in jobs per pixel (default
+ * 2; at most the pass's job slots, 2 x max(k, spatial neighbours)).  A pass
+ * whose jobs exceed it runs the rest with their rays traced in place: results
+ * do not depend on the capacity, only speed and memory do (96 bytes per job
+ * of capacity).  Synchronises the device; call between frames.  No
+ * counterpart in the reference (its OptiX launches trace in place). */
+int crisb_set_job_capacity(crisb_renderer* r, uint32_t jobs_per_pixel);
+int crisb_get_job_capacity(const crisb_renderer* r, uint32_t* jobs_per_pixel);
+
 /* Renderer::GetFrameIdx (src/Renderer.cpp:408-411). */
 /* Scene material and emitter tables after creation (for parameter updates of
  * inverse rendering; counts must equal those given at creation).  Renderers
@@ -568,6 +577,29 @@ int crisb_srgb8_thresholds(float* thresholds /* 256 */, float* c_max);
  * reference. */
 int crisb_set_trace_grid(crisb_renderer* r, uint32_t blocks_per_resident_block);
 int crisb_autotune(crisb_renderer* r, const crisb_camera* cam, uint32_t frames, uint32_t* chosen);
+
+/* Threads per block of the traversal kernels: 64, 128 (default) or 256; each
+ * size keeps the same register budget.  Results do not depend on it. */
+int crisb_set_trace_block(crisb_renderer* r, uint32_t threads);
+
+/* Launch settings chosen by crisb_autotune_ex, and the frame time they gave. */
+typedef struct crisb_tuning {
+    uint32_t trace_block;    /* threads per traversal block */
+    uint32_t trace_grid;     /* traversal blocks per resident block */
+    uint32_t jobs_per_pixel; /* shift-machine job capacity (crisb_set_job_capacity) */
+    float frame_ms;          /* the fastest candidate's frame time */
+} crisb_tuning;
+
+/* Coordinate descent over the launch settings on a scratch renderer of the
+ * same scene, size and parameters (the given renderer's frames are left
+ * alone): traversal block size (64, 128, 256), traversal grid (1, 2, 4, 8, 16
+ * x the resident blocks), then the job capacity (1, 2, 4, 8 jobs per pixel
+ * or every slot: the smallest within 1% of the fastest, as capacity costs
+ * memory).  Each candidate renders `frames` frames of `cam`, interleaved with
+ * the others.  The choices are applied to the renderer and returned in *out
+ * (may be NULL).  Results do not depend on any of them.  No counterpart in
+ * the reference. */
+int crisb_autotune_ex(crisb_renderer* r, const crisb_camera* cam, uint32_t frames, crisb_tuning* out);
 
 /* Frames run as one CUDA graph of the pass chain by default (captured, updated in
  * place and launched on the caller's stream); 0 launches the kernels directly.

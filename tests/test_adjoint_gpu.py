@@ -64,3 +64,28 @@ def test_autograd_function_matches_direct_call(cuda_device):
     np.testing.assert_allclose(diffuse.grad.numpy(), g_mat[:, 0:3].cpu().numpy(), rtol=1e-6)
     np.testing.assert_allclose(rgb.grad.numpy(), g_em.cpu().numpy(), rtol=1e-6)
     assert np.abs(rgb.grad.numpy()).sum() > 0 and np.abs(diffuse.grad.numpy()).sum() > 0
+
+
+@pytest.mark.gpu
+def test_adjoint_at_the_inverse_rendering_config(cuda_device):
+    """The inverse-rendering config at its stated size: the large scene
+    (1,310,988 triangles; its 64 sphere materials give 64 x 3 albedos and 32
+    GGX roughnesses, its 256 emitters 256 x 3 radiances -- 992 parameters), 8
+    views of 512 x 512, L2 loss against images at the ground-truth
+    parameters, start perturbed by N(0, 0.1) relative, 20 parameters drawn
+    with seed 3, central differences with eps 1e-3 summed in float64."""
+    from crisoptix_b200 import default_params
+
+    desc, _ = scenes.sphere_room(num_spheres=64, subdiv=5, num_emitters=256, seed=1)
+    sc = Scene(desc)
+    assert sc.num_triangles == 1310988
+    p = default_params(sc.scene_size, max_path_len=8, nee_prob=0.3, seed=3)
+    cams = [c for c, _, _ in scenes.multiview_cameras([(512, 512)] * 8, seed=3)]
+    tm, trgb, sm, srgb = adjoint.perturbed_start(desc, seed=3)
+    params = adjoint.inverse_config_params(desc, 20, 3)
+    pool = 64 * 3 + int((tm["roughness"][1:65] < 1.0).sum()) + 256 * 3
+    assert pool == 992
+    r = adjoint.fd_check(sc, desc, cams, 512, 512, p, tm, trgb, sm, srgb, params, eps=1e-3)
+    big = np.abs(r["fd"]) > 1e-3 * np.abs(r["fd"]).max()
+    assert big.sum() >= 10, r
+    assert r["rel_err"][big].max() < 1e-2, (r["rel_err"], r["adjoint"], r["fd"])

@@ -54,11 +54,14 @@ def test_flattened_instances_match_float64_reference(cuda_device):
 
 
 def run_parity(desc, cam, params, W, H, frames, cam_fn, change_params=None, timing=0, graph=lambda f: True,
-               motion=None):
-    sc = Scene(desc)
+               motion=None, jobs_per_pixel=None, builder=_abi.BVH_DEVICE):
+    sc = Scene(desc, builder=builder)
     tri = sc.read_triangles()
     o = op.Oracle.from_scene(desc, W, H, params, triangles=tri)
     r = Renderer(W, H, sc, params)
+    if jobs_per_pixel is not None:
+        r.set_job_capacity(jobs_per_pixel)
+        assert r.job_capacity() == jobs_per_pixel
     r.set_timing(timing)
     if motion is not None:  # (H, W, 2) motion vectors for MOTION_VECTORS
         mv_d = torch.from_numpy(np.ascontiguousarray(motion, np.float32)).cuda()
@@ -148,3 +151,19 @@ def test_graph_and_direct_frames_interleaved(cuda_device):
     p0 = small_config_params(scene_size_of(desc))
     p1 = small_config_params(scene_size_of(desc), gather_m=4, gather_radius=0.4, suffix_spatial_rounds=2)
     run_parity(desc, cam, p0, 32, 32, 6, static, change_params={3: p1}, graph=lambda f: f % 3 != 1)
+
+
+@pytest.mark.parametrize("jobs_per_pixel", [0, 1])
+def test_shift_jobs_beyond_capacity_give_the_same_results(cuda_device, jobs_per_pixel):
+    """With no machine capacity every shift job runs in the overflow kernel,
+    with one job per pixel most passes overflow part of their list: the
+    frames must not change."""
+    desc, cam = small_sphere_room()
+    p = large_config_params(scene_size_of(desc), gather_radius=0.3)
+    run_parity(desc, cam, p, 48, 40, 3, lambda c, f: orbit(c, f, 120), jobs_per_pixel=jobs_per_pixel)
+
+
+def test_host_built_tree_gives_the_same_frames(cuda_device):
+    desc, cam = small_sphere_room()
+    p = large_config_params(scene_size_of(desc), gather_radius=0.3)
+    run_parity(desc, cam, p, 48, 40, 2, lambda c, f: orbit(c, f, 120), builder=_abi.BVH_HOST)

@@ -1,5 +1,6 @@
-"""Launch-shape tuning: the traversal grid changes no result, and autotuning
-leaves the renderer's own frame sequence untouched."""
+"""Launch-shape tuning: traversal grid, traversal block size and job capacity
+change no result, and autotuning leaves the renderer's own frame sequence
+untouched."""
 import pytest
 import torch
 
@@ -23,10 +24,30 @@ def test_trace_grid_and_autotune_do_not_change_results(cuda_device):
         c = orbit(cam, f, 120)
         if f == 1:
             chosen = tuned.autotune(c, frames=1)
-            assert chosen in (1, 2, 4, 8, 16)
+            assert chosen["trace_grid"] in (1, 2, 4, 8, 16)
+            assert chosen["trace_block"] in (64, 128, 256)
+            assert 1 <= chosen["jobs_per_pixel"] <= 16 and chosen["frame_ms"] > 0
+            assert tuned.job_capacity() == chosen["jobs_per_pixel"]
         ref.launch_frame(c, out_r.data_ptr())
         tuned.launch_frame(c, out_t.data_ptr())
         torch.cuda.synchronize()
         assert out_r.cpu().numpy().tobytes() == out_t.cpu().numpy().tobytes(), f
         for b in BUFS:
             assert ref.debug_read(b).tobytes() == tuned.debug_read(b).tobytes(), (f, b)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("threads", [64, 256])
+def test_trace_block_sizes_do_not_change_results(cuda_device, threads):
+    desc, cam = small_sphere_room()
+    sc = Scene(desc)
+    p = large_config_params(scene_size_of(desc), gather_radius=0.3)
+    a, b = Renderer(48, 40, sc, p), Renderer(48, 40, sc, p)
+    b.set_trace_block(threads)
+    oa, ob = torch.zeros(48 * 40 * 3, device="cuda"), torch.zeros(48 * 40 * 3, device="cuda")
+    for f in range(3):
+        c = orbit(cam, f, 120)
+        a.launch_frame(c, oa.data_ptr())
+        b.launch_frame(c, ob.data_ptr())
+        torch.cuda.synchronize()
+        assert oa.cpu().numpy().tobytes() == ob.cpu().numpy().tobytes(), f
