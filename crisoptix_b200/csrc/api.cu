@@ -657,7 +657,8 @@ struct crisb_renderer {
 
     // job slots per pixel of the split suffix passes: two shifts per neighbour
     static uint32_t slots_for(const crisb_params& q) {
-        const uint32_t m = static_cast<uint32_t>(std::max(std::max(q.gather_m - 1, q.suffix_spatial_count), 1));
+        const int spatial = std::max(q.suffix_spatial_count, q.prefix_enable_spatial ? q.prefix_spatial_count : 0);
+        const uint32_t m = static_cast<uint32_t>(std::max(std::max(q.gather_m - 1, spatial), 1));
         return 2 * m;
     }
 
@@ -668,10 +669,20 @@ struct crisb_renderer {
     // frame of the large workload runs about 2.5 jobs per pixel over all its
     // passes, against 16 slots; a capacity of 1 to 4 jobs per pixel renders
     // it within 1% of the same time.
+    // The default (until crisb_set_job_capacity) follows the parameters: 2
+    // jobs per pixel, or the prefix spatial pass's 2 per neighbour when that
+    // pass runs (RestirPt's spatial reuse lists nearly every neighbour).
     static constexpr uint32_t kDefaultJobsPerPixel = 2;
     uint32_t jobs_per_pixel = kDefaultJobsPerPixel;
+    bool jobs_per_pixel_set = false;
 
-    size_t job_capacity() const { return P() * static_cast<size_t>(std::min(jobs_per_pixel, slots)); }
+    uint32_t effective_jobs_per_pixel() const {
+        uint32_t j = jobs_per_pixel;
+        if (!jobs_per_pixel_set && params.prefix_enable_spatial)
+            j = std::max(j, 2u * static_cast<uint32_t>(std::max(params.prefix_spatial_count, 0)));
+        return std::min(j, slots);
+    }
+    size_t job_capacity() const { return P() * static_cast<size_t>(effective_jobs_per_pixel()); }
 
     void allocate_jobs() {
         const size_t p = P();
@@ -850,10 +861,10 @@ struct crisb_renderer {
         }
         if (params.prefix_enable_spatial) {
             for (int r = 0; r < params.prefix_spatial_rounds; ++r) {
-                launch_prefix_spatial(s, fp, bufs(), out, r, st);
+                launch_prefix_spatial(s, fp, bufs(), out, r, st, m);
                 launch_prefix_copy_front_back(fp, bufs(), st);
                 if (m) m->mark(kClsOther, st);
-                launches += 2;
+                launches += 3 + shift_launches_per_phase();
             }
         }
         record(2, st);
@@ -1293,8 +1304,12 @@ int crisb_renderer_set_params(crisb_renderer* r, const crisb_params* params) {
         validate_params(*params);
         require(params->storage == r->params.storage, "params: storage is fixed when the renderer is created");
         const bool realloc_neighbors = params->gather_m != r->params.gather_m;
-        const bool realloc_jobs = crisb_renderer::slots_for(*params) != r->slots;
+        const size_t cap_before = r->job_capacity();
+        const uint32_t slots_before = r->slots;
         r->params = *params;
+        r->slots = crisb_renderer::slots_for(*params);
+        const bool realloc_jobs = r->slots != slots_before || r->job_capacity() != cap_before;
+        r->slots = slots_before;
         if (realloc_neighbors || realloc_jobs) check(cudaDeviceSynchronize(), "sync");
         if (realloc_neighbors) {
             r->neighbors.alloc(static_cast<size_t>(r->P()) * std::max<uint32_t>(r->K(), 1));
@@ -1390,6 +1405,7 @@ int crisb_autotune_ex(crisb_renderer* r, const crisb_camera* cam, uint32_t frame
             if (tmp->jobs_per_pixel == caps[k]) return;
             check(cudaStreamSynchronize(st), "sync");
             tmp->jobs_per_pixel = caps[k];
+            tmp->jobs_per_pixel_set = true;
             tmp->allocate_jobs();
         });
         const float best_cap_ms = tc[fastest(tc)];
@@ -1404,9 +1420,10 @@ int crisb_autotune_ex(crisb_renderer* r, const crisb_camera* cam, uint32_t frame
         cudaStreamDestroy(st);
         r->trace_block = tmp->trace_block;
         r->trace_grid = tmp->trace_grid;
-        if (r->jobs_per_pixel != cap) {
+        if (r->effective_jobs_per_pixel() != std::min(cap, r->slots) || !r->jobs_per_pixel_set) {
             check(cudaDeviceSynchronize(), "job capacity");
             r->jobs_per_pixel = cap;
+            r->jobs_per_pixel_set = true;
             r->allocate_jobs();
         }
         if (out) {
@@ -1459,7 +1476,10 @@ int crisb_set_job_capacity(crisb_renderer* r, uint32_t jobs_per_pixel) {
     return guarded([&] {
         require(r != nullptr, "null renderer");
         require(jobs_per_pixel <= CRISB_MAX_GATHER_M * 2, "job capacity: at most 64 jobs per pixel");
-        if (jobs_per_pixel == r->jobs_per_pixel) return;
+        r->jobs_per_pixel_set = true;
+        if (jobs_per_pixel == r->jobs_per_pixel && r->job_capacity() == r->P() * static_cast<size_t>(
+                                                                                std::min(jobs_per_pixel, r->slots)))
+            return;
         check(cudaDeviceSynchronize(), "job capacity");
         r->jobs_per_pixel = jobs_per_pixel;
         r->allocate_jobs();
@@ -1469,7 +1489,7 @@ int crisb_set_job_capacity(crisb_renderer* r, uint32_t jobs_per_pixel) {
 int crisb_get_job_capacity(const crisb_renderer* r, uint32_t* jobs_per_pixel) {
     return guarded([&] {
         require(r && jobs_per_pixel, "null argument");
-        *jobs_per_pixel = std::min(r->jobs_per_pixel, r->slots);
+        *jobs_per_pixel = r->effective_jobs_per_pixel();
     });
 }
 

@@ -1,78 +1,16 @@
 // passes.cu -- the per-frame pass kernels of Conditional ReSTIR PT.
 //
-// Prefix spatial reuse, the prefix-endpoint entries and search structure, and
-// the final gather for gatherN > 1: one thread per pixel, records loaded
-// whole, updated with the reference's in-place field semantics, stored whole.
-// (Prefix / suffix temporal, suffix spatial and the gatherN == 1 final gather
-// are split into shift jobs in reuse_passes.cu.)
+// The prefix-endpoint entries and search structure, the front -> back prefix
+// copy, and the final gather for gatherN > 1: one thread per pixel, records
+// loaded whole, updated with the reference's in-place field semantics, stored
+// whole.  (Prefix temporal and spatial, suffix temporal and spatial, and the
+// gatherN == 1 final gather are split into shift jobs in reuse_passes.cu.)
 #define CRISB_LBVH_KERNELS 1
 #include "records.cuh"
 
 namespace crisb {
 
 namespace {
-
-// PrefixSpatialReuse, shader/prefix_spatial_reuse.cu:11-134.  Neighbours come
-// from the back buffer, which equals the front buffer at pass start.
-__global__ void __launch_bounds__(kPassBlock)
-    k_prefix_spatial(SceneView s, FrameParams fp, Bufs b, float* out, int round) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= pixel_count(fp)) return;
-    const uint32_t x = i % fp.width, y = i / fp.width;
-    Res<Prefix> cur = ld_pres(b.pres[fp.front], i);
-    bool ok = false;
-    const Prefix cur_prefix = cur.s;
-    const crisb_prefix_rec& canon = b.canon_prefix[i];
-    if (fl_valid(cur_prefix.flags) && fl_valid(canon.flags) && canon.primary.prim != CRISB_INVALID_PRIM) {
-        ok = true;
-        Rng rng{b.gbuf[i].rng};
-        const float cur_wsum = cur.w_sum, cur_conf = cur.conf;
-        cur.w_sum = 0.0f;
-        cur.conf = 0.0f;
-        const int count = fp.p.prefix_spatial_count;
-        float canon_mis = 1.0f;
-        uint32_t nvalid = 0, vflags = 0;
-        uint32_t nx[CRISB_MAX_SPATIAL_NEIGH], ny[CRISB_MAX_SPATIAL_NEIGH];
-        for (int n = 0; n < count; ++n) {
-            select_spatial_neighbor(x, y, static_cast<uint32_t>(fp.p.window_radius), rng, nx[n], ny[n]);
-            if (!(nx[n] < fp.width && ny[n] < fp.height)) continue;
-            const uint32_t ni = ny[n] * fp.width + nx[n];
-            if (!(b.gbuf[ni].flags & 1u)) continue;
-            const uint32_t nflags = pres_flags(b.pres[fp.back], ni);
-            const bool skip_nee = fp.p.renderer_type == CRISB_RENDERER_CONDITIONAL_RESTIR && fl_nee(nflags);
-            if (!fl_valid(nflags) || skip_nee) continue;
-            ++nvalid;
-            vflags |= 1u << n;
-        }
-        const float K = static_cast<float>(nvalid);
-        for (int n = 0; n < count; ++n) {
-            if (!((vflags >> n) & 1u)) continue;
-            const uint32_t ni = ny[n] * fp.width + nx[n];
-            const Res<Prefix> nr = ld_pres(b.pres[fp.back], ni);
-            float jac_n2c = 0.0f, jac_c2n = 0.0f;
-            const V3 f_c_of_n = shift_prefix(s, nr.s, cur_prefix, jac_n2c);
-            const float p_c_of_n = luminance(f_c_of_n) * jac_n2c;
-            const V3 f_n_of_c = shift_prefix(s, cur_prefix, nr.s, jac_c2n);
-            float nmis = mis_neighbor(f_c_of_n, nr.s.f, jac_n2c, K, cur_conf, nr.conf);
-            if (nonfinite(nmis)) nmis = 0.0f;
-            Prefix shifted = nr.s;
-            shifted.f = f_c_of_n;
-            shifted.primary = cur_prefix.primary;
-            res_update(cur, shifted, nmis * p_c_of_n * nr.w_sum, rng, nr.conf);
-            canon_mis += mis_canonical(cur_prefix.f, f_n_of_c, jac_c2n, K, cur_conf, nr.conf);
-        }
-        if (nonfinite(canon_mis)) canon_mis = 0.0f;
-        res_update(cur, cur_prefix, canon_mis * cur_wsum * luminance(cur_prefix.f), rng, cur_conf);
-        if (cur.w_sum > 0.0f) {
-            cur.w_sum /= K + 1.0f;
-            res_finalize(cur);
-        }
-        b.gbuf[i].rng = rng.state;
-        st_pres(b.pres[fp.front], i, cur);
-    }
-    if (fp.p.renderer_type == CRISB_RENDERER_RESTIR_PT && round == fp.p.prefix_spatial_rounds - 1)
-        store_output(fp, out, i, ok ? cur.w_sum * cur.s.f : splat(0.0f));
-}
 
 __global__ void k_prefix_copy(FrameParams fp, Bufs b) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -296,10 +234,6 @@ inline unsigned grid_for(uint32_t n) { return (n + kPassBlock - 1) / kPassBlock;
 
 }  // namespace
 
-void launch_prefix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, int round,
-                           cudaStream_t st) {
-    k_prefix_spatial<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b, out, round);
-}
 void launch_prefix_copy_front_back(const FrameParams& fp, const Bufs& b, cudaStream_t st) {
     k_prefix_copy<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
 }

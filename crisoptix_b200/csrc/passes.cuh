@@ -123,7 +123,7 @@ constexpr int kTriLeafMax = 4;
 constexpr int kMedianDepth = 40;
 
 void launch_prefix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, int round,
-                           cudaStream_t st);
+                           cudaStream_t st, Marker* m);
 void launch_prefix_copy_front_back(const FrameParams& fp, const Bufs& b, cudaStream_t st);
 // reuse passes as per-pixel kernel -> compacted shift jobs -> per-pixel combine
 void launch_prefix_gen_temp_split(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out,

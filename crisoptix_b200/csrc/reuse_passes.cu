@@ -83,6 +83,11 @@ RT_D void count_jobs(const SceneView& s, uint32_t total) {
 // occluded.  Jobs that still need a replay in the last round finish inline.
 constexpr int kShiftRounds = 3;
 constexpr int kModePrefix = 3;  // prefix temporal reuse (slot 0: previous onto canonical)
+// prefix spatial reuse (slot 2n: neighbour n onto the pixel's prefix; 2n + 1:
+// the pixel's prefix onto neighbour n's)
+constexpr int kModePrefixSpatial = 4;
+
+RT_HD bool prefix_mode(int mode) { return mode == kModePrefix || mode == kModePrefixSpatial; }
 
 // source path of a job
 struct ShiftSrc {
@@ -105,6 +110,17 @@ RT_D uint32_t prev_pixel(const FrameParams& fp, const Bufs& b, uint32_t i) {
 // the job's source path and, when `dst` is given, its destination vertex
 RT_D ShiftSrc resolve_job(const FrameParams& fp, const Bufs& b, int mode, uint32_t code, Hit* dst) {
     const uint32_t i = code >> kSlotBits, slot = code & ((1u << kSlotBits) - 1), n = slot >> 1;
+    if (mode == kModePrefixSpatial) {
+        // neighbours from the back buffer (equal to the front at pass start),
+        // the pixel's own prefix from the front buffer
+        const uint32_t ni = b.spatial_nbr[static_cast<size_t>(i) * (b.slots >> 1) + n];
+        if ((slot & 1u) == 0) {
+            if (dst) *dst = pres_primary(b.pres[fp.front], i);
+            return shift_src(ld_pres(b.pres[fp.back], ni).s);
+        }
+        if (dst) *dst = pres_primary(b.pres[fp.back], ni);
+        return shift_src(ld_pres(b.pres[fp.front], i).s);
+    }
     if (mode == kModePrefix) {
         // slot 0: the previous prefix onto the canonical one; slot 1: back
         const uint32_t pi = prev_pixel(fp, b, i);
@@ -235,7 +251,7 @@ __global__ void __launch_bounds__(kPassBlock) k_shift_begin(SceneView s, FramePa
     const uint32_t all = *b.job_count;
     count_jobs(s, all);
     const uint32_t total = min(all, b.job_cap);
-    const bool prefix = mode == kModePrefix;
+    const bool prefix = prefix_mode(mode);
     const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
         const uint32_t t = base + threadIdx.x;
@@ -268,7 +284,7 @@ __global__ void __launch_bounds__(kPassBlock) k_shift_begin(SceneView s, FramePa
 template <bool kTex>
 __global__ void __launch_bounds__(kPassBlock) k_shift_overflow(SceneView s, FrameParams fp, Bufs b, int mode) {
     const uint32_t total = *b.job_count;
-    const bool prefix = mode == kModePrefix;
+    const bool prefix = prefix_mode(mode);
     const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     for (uint32_t t = b.job_cap + blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         ShiftJob j;
@@ -298,7 +314,7 @@ __global__ void __launch_bounds__(kPassBlock) k_shift_step(SceneView s, FramePar
     const uint32_t total = nc + ns;
     const uint32_t* qc = b.job_queue[2 * cur];
     const uint32_t* qs = b.job_queue[2 * cur + 1];
-    const bool prefix = mode == kModePrefix;
+    const bool prefix = prefix_mode(mode);
     const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
         const uint32_t u = base + threadIdx.x;
@@ -685,6 +701,109 @@ __global__ void __launch_bounds__(kPassBlock) k_gather_combine(FrameParams fp, B
 }
 
 
+// ---- prefix spatial reuse (shader/prefix_spatial_reuse.cu:11-134) -----------------
+// Neighbours are read from the back buffer, which equals the front buffer at
+// pass start (the front -> back copy follows every round); the pass writes the
+// front buffer.  Split like the suffix spatial pass: selection, shift jobs,
+// combine.
+__global__ void __launch_bounds__(kPassBlock) k_prefix_spatial_select(FrameParams fp, Bufs b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t mask = 0;
+    if (i < pixel_count(fp)) {
+        const uint32_t x = i % fp.width, y = i / fp.width;
+        const crisb_prefix_rec& canon = b.canon_prefix[i];
+        uint32_t st = kStFinal;
+        if (fl_valid(pres_flags(b.pres[fp.front], i)) && fl_valid(canon.flags) &&
+            canon.primary.prim != CRISB_INVALID_PRIM) {
+            st = kStReuse;
+            Rng rng{b.gbuf[i].rng};
+            uint32_t vflags = 0;
+            uint32_t* nbr = b.spatial_nbr + static_cast<size_t>(i) * (b.slots >> 1);
+            for (int n = 0; n < fp.p.prefix_spatial_count; ++n) {
+                uint32_t nx, ny;
+                select_spatial_neighbor(x, y, static_cast<uint32_t>(fp.p.window_radius), rng, nx, ny);
+                if (!(nx < fp.width && ny < fp.height)) continue;
+                const uint32_t ni = ny * fp.width + nx;
+                if (!(b.gbuf[ni].flags & 1u)) continue;
+                const uint32_t nflags = pres_flags(b.pres[fp.back], ni);
+                const bool skip_nee = fp.p.renderer_type == CRISB_RENDERER_CONDITIONAL_RESTIR && fl_nee(nflags);
+                if (!fl_valid(nflags) || skip_nee) continue;
+                nbr[n] = ni;
+                vflags |= 1u << n;
+                mask |= 3ull << (2 * n);
+            }
+            b.gbuf[i].rng = rng.state;
+            b.pass_flags[i] = vflags;
+        }
+        b.pass_status[i] = st;
+    }
+    push_jobs(b, i, mask);
+}
+
+__global__ void __launch_bounds__(kPassBlock) k_prefix_spatial_combine(FrameParams fp, Bufs b, float* out,
+                                                                      int round) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixel_count(fp)) return;
+    const bool output = fp.p.renderer_type == CRISB_RENDERER_RESTIR_PT && round == fp.p.prefix_spatial_rounds - 1;
+    if (b.pass_status[i] == kStFinal) {
+        if (output) store_output(fp, out, i, splat(0.0f));
+        return;
+    }
+    Rng rng{b.gbuf[i].rng};
+    const V3 own_f = pres_f(b.pres[fp.front], i);
+    const float cur_wsum = pres_wsum(b.pres[fp.front], i), cur_conf = pres_conf(b.pres[fp.front], i);
+    const uint32_t vflags = b.pass_flags[i];
+    const float K = static_cast<float>(__popc(vflags));
+    const uint32_t* nbr = b.spatial_nbr + static_cast<size_t>(i) * (b.slots >> 1);
+    const float4* sh = b.shift_out + static_cast<size_t>(i) * b.slots;
+    // Reservoir::Update's arithmetic with the chosen sample tracked by index
+    // (-1: the pixel's own prefix, which the reset reservoir still holds)
+    float w_sum = 0.0f, conf = 0.0f;
+    int sel = -1;
+    V3 sel_f = own_f;
+    float canon_mis = 1.0f;
+    for (int n = 0; n < fp.p.prefix_spatial_count; ++n) {
+        if (!((vflags >> n) & 1u)) continue;
+        const uint32_t ni = nbr[n];
+        const V3 nf = pres_f(b.pres[fp.back], ni);
+        const float nconf = pres_conf(b.pres[fp.back], ni), nwsum = pres_wsum(b.pres[fp.back], ni);
+        const float4 o0 = sh[2 * n], o1 = sh[2 * n + 1];
+        const V3 f_c_of_n = xyz(o0), f_n_of_c = xyz(o1);
+        const float jac_n2c = o0.w, jac_c2n = o1.w;
+        const float p_c_of_n = luminance(f_c_of_n) * jac_n2c;
+        float nmis = mis_neighbor(f_c_of_n, nf, jac_n2c, K, cur_conf, nconf);
+        if (nonfinite(nmis)) nmis = 0.0f;
+        if (res_choose(w_sum, conf, nmis * p_c_of_n * nwsum, rng, nconf)) {
+            sel = n;
+            sel_f = f_c_of_n;
+        }
+        canon_mis += mis_canonical(own_f, f_n_of_c, jac_c2n, K, cur_conf, nconf);
+    }
+    if (nonfinite(canon_mis)) canon_mis = 0.0f;
+    if (res_choose(w_sum, conf, canon_mis * cur_wsum * luminance(own_f), rng, cur_conf)) {
+        sel = -1;
+        sel_f = own_f;
+    }
+    Res<Prefix> cur;
+    if (sel >= 0) {
+        // the neighbour's prefix with f shifted onto this pixel and its primary hit
+        cur.s = ld_pres(b.pres[fp.back], nbr[sel]).s;
+        cur.s.f = sel_f;
+        cur.s.primary = pres_primary(b.pres[fp.front], i);
+    } else {
+        cur.s = ld_pres(b.pres[fp.front], i).s;
+    }
+    cur.w_sum = w_sum;
+    cur.conf = conf;
+    if (cur.w_sum > 0.0f) {
+        cur.w_sum /= K + 1.0f;
+        res_finalize(cur);
+    }
+    b.gbuf[i].rng = rng.state;
+    st_pres(b.pres[fp.front], i, cur);
+    if (output) store_output(fp, out, i, cur.w_sum * cur.s.f);
+}
+
 // ---- prefix generation + temporal reuse (shader/prefix_gen_temp_reuse.cu) -----------
 // the pass leaves back = front (prefix_gen_temp_reuse.cu:159-164)
 RT_HD bool prefix_back_copy(const FrameParams& fp) {
@@ -914,6 +1033,16 @@ void launch_prefix_gen_temp_split(const SceneView& s, const FrameParams& fp, con
 
 uint32_t prefix_pass_extra_launches(const FrameParams& fp) {
     return prefix_back_copy(fp) && fp.p.motion_mode != CRISB_MOTION_NONE ? 1u : 0u;
+}
+
+void launch_prefix_spatial(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, int round,
+                           cudaStream_t st, Marker* m) {
+    cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
+    k_prefix_spatial_select<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
+    MARK(kClsResample);
+    run_shift_jobs(s, fp, b, kModePrefixSpatial, st, m);
+    k_prefix_spatial_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, out, round);
+    MARK(kClsResample);
 }
 
 void launch_suffix_gen_temp(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m) {
