@@ -560,6 +560,8 @@ struct crisb_renderer {
     DevBuf<float4> shift_out, gather_state;
     DevBuf<crisb_suffix_res_rec> gather_cs;
     DevBuf<crisb_prefix_rec> gather_cp;
+    DevBuf<float4> gather_ext;          // gatherN > 1 only
+    DevBuf<crisb_hit_rec> gather_last;  // gatherN > 1 only
     // The path machines' states and ray queues and the shift machines' job
     // records and ray queues share one allocation: within a pass the path
     // machines finish (the pass's finish kernel reads the last path field, the
@@ -631,6 +633,8 @@ struct crisb_renderer {
         b.shift_out = shift_out.p;
         b.gather_cs = gather_cs.p;
         b.gather_state = gather_state.p;
+        b.gather_ext = params.gather_n > 1 ? gather_ext.p : nullptr;
+        b.gather_last = params.gather_n > 1 ? gather_last.p : nullptr;
         b.slots = slots;
         b.job_cap = static_cast<uint32_t>(std::min<size_t>(job_capacity(), 0xFFFFFFFFu));
         b.tally = timing >= 2 && ray_count.p ? ray_count.p + kRayCounters : nullptr;
@@ -889,14 +893,14 @@ struct crisb_renderer {
             if (m) m->mark(kClsSearch, st);
             launches += 3 + 4 + rsort::kLaunches;
             record(5, st);
-            if (params.gather_n == 1) {
-                launch_final_gather_split(s, fp, bufs(), out, st, m);
-                launches += 3 + sj + wf_launches_per_pass(fp, 2);
-            } else {
-                launch_final_gather(s, fp, bufs(), out, st);
-                if (m) m->mark(kClsOther, st);
-                ++launches;
+            if (params.gather_n > 1 && !gather_ext.p) {
+                gather_ext.alloc(3 * static_cast<size_t>(P()));
+                gather_last.alloc(P());
             }
+            launch_final_gather_split(s, fp, bufs(), out, st, m);
+            launches += 3 + sj + wf_launches_per_pass(fp, 2);
+            if (params.gather_n > 1)
+                launches += 1 + static_cast<uint32_t>(params.gather_n - 1) * (3 + sj);
         } else {
             record(3, st);
             record(4, st);

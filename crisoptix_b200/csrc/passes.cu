@@ -1,10 +1,8 @@
 // passes.cu -- the per-frame pass kernels of Conditional ReSTIR PT.
 //
-// The prefix-endpoint entries and search structure, the front -> back prefix
-// copy, and the final gather for gatherN > 1: one thread per pixel, records
-// loaded whole, updated with the reference's in-place field semantics, stored
-// whole.  (Prefix temporal and spatial, suffix temporal and spatial, and the
-// gatherN == 1 final gather are split into shift jobs in reuse_passes.cu.)
+// The prefix-endpoint entries and search structure and the front -> back
+// prefix copy: one thread per pixel.  (The reuse passes and the final gather
+// are split into shift jobs in reuse_passes.cu.)
 #define CRISB_LBVH_KERNELS 1
 #include "records.cuh"
 
@@ -102,134 +100,6 @@ __global__ void k_knn_leaves(FrameParams fp, Bufs b, lbvh::Work w, float4* leaf_
 }
 
 // ---- final gather -----------------------------------------------------------------------
-RT_D void write_neighbors(const FrameParams& fp, const Bufs& b, uint32_t i, const NeighborList& nl) {
-    const uint32_t k = fp.k;
-    for (uint32_t n = 0; n < k; ++n) {
-        crisb_neighbor_rec r;
-        r.pixel = n < nl.count ? nl.pix[n] : 0u;
-        r.dist = n < nl.count ? nl.dist[n] : 0.0f;
-        b.neighbors[static_cast<size_t>(i) * k + n] = r;
-    }
-    b.neigh_count[i] = nl.count;
-}
-
-// FinalGatherCanon, shader/final_gather.cu:69-188
-RT_D V3 final_gather_canon(const SceneView& s, const FrameParams& fp, const Bufs& b, uint32_t i, V3 origin, V3 dir,
-                           Rng& rng, NeighborList& nl, bool& queried) {
-    Prefix cp;
-    cp.rng = 0;
-    cp.primary = cp.recon = cp.last = Hit{CRISB_INVALID_PRIM, 0.0f, 0.0f, splat(0.0f)};
-    cp.flags = 0;
-    cp.f = cp.prf = cp.rod = splat(0.0f);
-    cp.p = cp.path_len = 0.0f;
-    trace_prefix(s, fp, cp, origin, dir, rng);
-    if (!fl_valid(cp.flags)) return splat(0.0f);
-    if (fl_nee(cp.flags)) return cp.f / cp.p;
-    Suffix cs;
-    cs.rng = 0;
-    cs.recon = cs.last_prefix = Hit{CRISB_INVALID_PRIM, 0.0f, 0.0f, splat(0.0f)};
-    cs.flags = 0;
-    cs.f = cs.prf = cs.rod = splat(0.0f);
-    cs.p = 0.0f;
-    trace_suffix(s, fp, cs, cp, rng);
-    if (!fl_valid(cs.flags)) return splat(0.0f);
-    const V3 canon_contrib = cp.f * cs.f / (cp.p * cs.p);
-    const uint32_t k = fp.k;
-    if (k == 0) return canon_contrib;
-    const Isect last = unpack(s, cs.last_prefix);
-    knn_query(b.knn(), s.err, last.pos, k, nl);
-    queried = true;
-    uint32_t nvalid = 0, vflags = 0;
-    for (uint32_t n = 0; n < nl.count; ++n) {
-        if (!fl_valid(sres_flags(b.sres_cur, nl.pix[n]))) continue;
-        ++nvalid;
-        vflags |= 1u << n;
-    }
-    V3 suffix_contrib = splat(0.0f);
-    const float K = static_cast<float>(nvalid);
-    float canon_mis = 1.0f;
-    for (uint32_t n = 0; n < nl.count; ++n) {
-        if (!(vflags & (1u << n))) continue;
-        const Res<Suffix> nr = ld_sres(b.sres_cur, nl.pix[n]);
-        float jac_n2c = 0.0f, jac_c2n = 0.0f;
-        const V3 f_c_of_n = shift_suffix(s, nr.s, cs, jac_n2c);
-        const V3 f_n_of_c = shift_suffix(s, cs, nr.s, jac_c2n);
-        float nmis = mis_neighbor(f_c_of_n, nr.s.f, jac_n2c, K, 1.0f, nr.conf);
-        if (nonfinite(nmis)) nmis = 0.0f;
-        const V3 contrib = nmis * f_c_of_n * nr.w_sum * jac_n2c;
-        if (!nonfinite(contrib)) suffix_contrib = suffix_contrib + contrib;
-        canon_mis += mis_canonical(cs.f, f_n_of_c, jac_c2n, K, 1.0f, nr.conf);
-    }
-    V3 gather = suffix_contrib * cp.f / cp.p;
-    gather = gather / static_cast<float>(nvalid + 1);
-    V3 result = gather + (canon_contrib * canon_mis);
-    result = result / (K + 1.0f);
-    if (nonfinite(result)) return splat(0.0f);
-    return result;
-}
-
-// FinalGatherNotCanon, shader/final_gather.cu:190-288
-RT_D V3 final_gather_not_canon(const SceneView& s, const FrameParams& fp, const Bufs& b, V3 origin, V3 dir, Rng& rng,
-                               NeighborList& nl, bool& queried) {
-    const uint32_t k = fp.k;
-    if (k == 0) return splat(0.0f);
-    Isect last;
-    last.valid = false;
-    V3 tp;
-    float pp;
-    if (!trace_prefix_for_gather(s, tp, pp, last, origin, dir, static_cast<uint32_t>(fp.p.prefix_len), rng))
-        return splat(0.0f);
-    knn_query(b.knn(), s.err, last.pos, k, nl);
-    queried = true;
-    uint32_t nvalid = 0, vflags = 0;
-    for (uint32_t n = 0; n < nl.count; ++n) {
-        if (!fl_valid(sres_flags(b.sres_cur, nl.pix[n]))) continue;
-        ++nvalid;
-        vflags |= 1u << n;
-    }
-    V3 suffix_contrib = splat(0.0f);
-    const float K = static_cast<float>(nvalid);
-    for (uint32_t n = 0; n < nl.count; ++n) {
-        if (!(vflags & (1u << n))) continue;
-        const Res<Suffix> nr = ld_sres(b.sres_cur, nl.pix[n]);
-        float jac_n2c = 0.0f;
-        const V3 f_c_of_n = shift_suffix(s, nr.s, last, jac_n2c);
-        float nmis = mis_neighbor(f_c_of_n, nr.s.f, jac_n2c, K, 1.0f, nr.conf);
-        if (nonfinite(nmis)) nmis = 0.0f;
-        const V3 contrib = nmis * f_c_of_n * nr.w_sum * jac_n2c;
-        if (!nonfinite(contrib)) suffix_contrib = suffix_contrib + contrib;
-    }
-    V3 result = suffix_contrib * tp / pp;
-    result = result / static_cast<float>(fp.p.gather_n);
-    result = result / (K + 1.0f);
-    if (nonfinite(result)) return splat(0.0f);
-    return result;
-}
-
-// GetRadiance + __raygen__final_gather, shader/final_gather.cu:290-356
-__global__ void __launch_bounds__(kPassBlock) k_final_gather(SceneView s, FrameParams fp, Bufs b, float* out) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= pixel_count(fp)) return;
-    const uint32_t x = i % fp.width, y = i / fp.width;
-    NeighborList nl;
-    nl.count = 0;
-    bool queried = false;
-    V3 L = splat(0.0f);
-    if (b.canon_prefix[i].primary.prim != CRISB_INVALID_PRIM) {
-        Rng rng{b.gbuf[i].rng};
-        const V3 dir = camera_dir(fp, x, y, rng);
-        const V3 origin = ld3(fp.cam.pos);
-        L = L + final_gather_canon(s, fp, b, i, origin, dir, rng, nl, queried);
-        for (int g = 1; g < fp.p.gather_n; ++g) L = L + final_gather_not_canon(s, fp, b, origin, dir, rng, nl, queried);
-        if (nonfinite(L)) L = splat(0.0f);
-        b.gbuf[i].rng = rng.state;
-    }
-    if (!queried) nl.count = 0;
-    if (fp.k > 0) write_neighbors(fp, b, i, nl);
-    else b.neigh_count[i] = 0;
-    store_output(fp, out, i, L);
-}
-
 inline unsigned grid_for(uint32_t n) { return (n + kPassBlock - 1) / kPassBlock; }
 
 }  // namespace
@@ -254,9 +124,6 @@ void launch_lbvh_hierarchy(const lbvh::Work& w, uint32_t cap, int leaf_max, cuda
     lbvh::k_karras<<<g, kPassBlock, 0, st>>>(w);
     lbvh::k_refit<<<g, kPassBlock, 0, st>>>(w);
     lbvh::k_emit<<<g, kPassBlock, 0, st>>>(w, leaf_max);
-}
-void launch_final_gather(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, cudaStream_t st) {
-    k_final_gather<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b, out);
 }
 
 }  // namespace crisb

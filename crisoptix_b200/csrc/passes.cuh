@@ -74,6 +74,11 @@ struct Bufs {
     uint32_t* job_count;    // 1
     float4* shift_out;      // P * slots: shifted f (xyz) and Jacobian (w)
     crisb_suffix_res_rec* gather_cs;  // P: canonical suffix of the final gather
+    // gatherN > 1 only (else null): per pixel the camera ray direction (xyz, w
+    // = 1 when the gather ran), the radiance accumulated over the gathers, and
+    // the current extra prefix's throughput and pdf; its last vertex
+    float4* gather_ext;     // P * 3
+    crisb_hit_rec* gather_last;  // P
     float4* gather_state;   // P * 3: prefix f / p, canonical contribution, direct result
     uint32_t slots;         // job slots per pixel (>= 2 * max(k, spatial count, 1))
     // capacity of the shift machines' job records and queues; list entries
@@ -148,7 +153,7 @@ void launch_store_entries(const SceneView& s, const FrameParams& fp, const Bufs&
                           unsigned int* bounds, cudaStream_t st);
 void launch_knn_finish(const FrameParams& fp, const Bufs& b, const lbvh::Work& w, float4* leaf_entries,
                        cudaStream_t st);
-void launch_final_gather(const SceneView& s, const FrameParams& fp, const Bufs& b, float* out, cudaStream_t st);
+
 // path-replay adjoint of the frozen-sampling path tracer (adjoint.cu)
 void adjoint_forward(const SceneView& eval, const crisb_material* sample_mats, uint32_t num_mats,
                      const FrameParams& fp, float* out, cudaStream_t st);

@@ -86,6 +86,9 @@ constexpr int kModePrefix = 3;  // prefix temporal reuse (slot 0: previous onto 
 // prefix spatial reuse (slot 2n: neighbour n onto the pixel's prefix; 2n + 1:
 // the pixel's prefix onto neighbour n's)
 constexpr int kModePrefixSpatial = 4;
+// the final gather's extra prefixes (slot 2n: neighbour n's suffix onto the
+// extra prefix's last vertex)
+constexpr int kModeGatherExtra = 5;
 
 RT_HD bool prefix_mode(int mode) { return mode == kModePrefix || mode == kModePrefixSpatial; }
 
@@ -131,6 +134,10 @@ RT_D ShiftSrc resolve_job(const FrameParams& fp, const Bufs& b, int mode, uint32
         if (dst) *dst = pres_primary(b.pres[fp.back], pi);
         return shift_src(ld_prefix(b.canon_prefix[i]));
     }
+    if (mode == kModeGatherExtra) {
+        if (dst) *dst = ld_hit(b.gather_last[i]);
+        return shift_src(ld_sres(b.sres_cur, b.neighbors[static_cast<size_t>(i) * fp.k + n].pixel).s);
+    }
     const bool onto_own = (slot & 1u) == 0;
     SufRef own, other;
     if (mode == kModeTemporal) {
@@ -145,6 +152,16 @@ RT_D ShiftSrc resolve_job(const FrameParams& fp, const Bufs& b, int mode, uint32
     }
     if (dst) *dst = ld_suf_last(onto_own ? own : other);
     return shift_src(ld_suf(onto_own ? other : own));
+}
+
+// the job's destination vertex as an interaction: a stored hit re-derived as
+// the reference unpacks it (interpolated, unnormalised normal), except the
+// extra gather prefix's last vertex, which the reference hands over straight
+// from the trace (normalised normal, trace_closest)
+RT_D Isect job_dst(const SceneView& s, int mode, const Hit& h) {
+    Isect it = unpack(s, h);
+    if (mode == kModeGatherExtra && it.valid) it.nrm = normalize(it.nrm);
+    return it;
 }
 
 RT_D void job_out(const Bufs& b, uint32_t code, float4 v) {
@@ -261,7 +278,7 @@ __global__ void __launch_bounds__(kPassBlock) k_shift_begin(SceneView s, FramePa
             j.code = b.job_items[t];
             Hit dh;
             const ShiftSrc src = resolve_job(fp, b, mode, j.code, &dh);
-            const Isect cur = unpack(s, dh);
+            const Isect cur = job_dst(s, mode, dh);
             bool ok = fl_valid(src.flags) && cur.valid;
             if (prefix) ok = ok && fl_recon(src.flags) >= 2;
             ok = ok && unpack(s, src.anchor).valid && unpack(s, src.recon).valid;
@@ -291,7 +308,7 @@ __global__ void __launch_bounds__(kPassBlock) k_shift_overflow(SceneView s, Fram
         j.code = b.job_items[t];
         Hit dh;
         const ShiftSrc src = resolve_job(fp, b, mode, j.code, &dh);
-        const Isect cur = unpack(s, dh);
+        const Isect cur = job_dst(s, mode, dh);
         bool ok = fl_valid(src.flags) && cur.valid;
         if (prefix) ok = ok && fl_recon(src.flags) >= 2;
         ok = ok && unpack(s, src.anchor).valid && unpack(s, src.recon).valid;
@@ -617,8 +634,14 @@ __global__ void __launch_bounds__(kPassBlock) k_gather_finish(FrameParams fp, Bu
     }
     if (st == kStFinal) {
         V3 L = splat(0.0f) + direct;
-        if (nonfinite(L)) L = splat(0.0f);
-        store_output(fp, out, i, L);
+        if (b.gather_ext) {
+            // gatherN > 1: the canonical gather's share; the extra gathers add
+            // theirs and k_gather_output stores the sum
+            b.gather_ext[3 * static_cast<size_t>(i) + 1] = make_float4(L.x, L.y, L.z, 0.0f);
+        } else {
+            if (nonfinite(L)) L = splat(0.0f);
+            store_output(fp, out, i, L);
+        }
     }
     b.pass_status[i] = st;
 }
@@ -696,6 +719,116 @@ __global__ void __launch_bounds__(kPassBlock) k_gather_combine(FrameParams fp, B
     result = result / (K + 1.0f);
     if (nonfinite(result)) result = splat(0.0f);
     V3 L = splat(0.0f) + result;
+    if (b.gather_ext) {
+        b.gather_ext[3 * static_cast<size_t>(i) + 1] = make_float4(L.x, L.y, L.z, 0.0f);
+        return;
+    }
+    if (nonfinite(L)) L = splat(0.0f);
+    store_output(fp, out, i, L);
+}
+
+// ---- the final gather's extra prefixes, gatherN > 1 (shader/final_gather.cu:190-288,
+// FinalGatherNotCanon, summed by GetRadiance, :290-321) ------------------------------------
+constexpr uint32_t kStNoGather = 6;  // the pixel ran no gather (invalid primary hit)
+
+// TracePrefixForFinalGather along the gather's camera ray, continuing the
+// pixel's random stream; at most prefix_len closest-hit rays, traced in place
+__global__ void __launch_bounds__(kPassBlock) k_gather_extra_prefix(SceneView s, FrameParams fp, Bufs b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixel_count(fp)) return;
+    const float4 e = b.gather_ext[3 * static_cast<size_t>(i)];
+    uint32_t st = kStFinal;  // contributes zero
+    if (e.w == 0.0f) {
+        st = kStNoGather;
+    } else if (fp.k > 0) {
+        Rng rng{b.gbuf[i].rng};
+        V3 tp;
+        float pp;
+        Isect last;
+        if (trace_prefix_for_gather(s, tp, pp, last, ld3(fp.cam.pos), V3{e.x, e.y, e.z},
+                                    static_cast<uint32_t>(fp.p.prefix_len), rng)) {
+            b.gather_ext[3 * static_cast<size_t>(i) + 2] = make_float4(tp.x, tp.y, tp.z, pp);
+            st_hit(b.gather_last[i], last.pack());
+            st = kStQuery;
+        }
+        b.gbuf[i].rng = rng.state;
+    }
+    b.pass_status[i] = st;
+}
+
+// neighbour search at the extra prefix's last vertex; one job per valid
+// neighbour (slot 2n: its suffix shifted onto that vertex)
+__global__ void __launch_bounds__(kPassBlock) k_gather_extra_query(SceneView s, FrameParams fp, Bufs b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t mask = 0;
+    if (i < pixel_count(fp) && b.pass_status[i] == kStQuery) {
+        const uint32_t k = fp.k;
+        NeighborList nl;
+        const Isect last = unpack(s, ld_hit(b.gather_last[i]));
+        knn_query(b.knn(), s.err, last.pos, k, nl);
+        uint32_t vflags = 0;
+        for (uint32_t n = 0; n < nl.count; ++n) {
+            if (!(b.nval_cur[nl.pix[n]] & kNvalSample)) continue;
+            vflags |= 1u << n;
+            mask |= 1ull << (2 * n);
+        }
+        for (uint32_t n = 0; n < k; ++n) {
+            crisb_neighbor_rec r;
+            r.pixel = n < nl.count ? nl.pix[n] : 0u;
+            r.dist = n < nl.count ? nl.dist[n] : 0.0f;
+            b.neighbors[static_cast<size_t>(i) * k + n] = r;
+        }
+        b.neigh_count[i] = nl.count;
+        b.pass_flags[i] = vflags;
+        b.pass_status[i] = kStReuse;
+    }
+    push_jobs(b, i, mask);
+}
+
+__global__ void __launch_bounds__(kPassBlock) k_gather_extra_combine(FrameParams fp, Bufs b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixel_count(fp)) return;
+    const uint32_t st = b.pass_status[i];
+    if (st == kStNoGather) return;
+    V3 result = splat(0.0f);
+    if (st == kStReuse) {
+        const uint32_t k = fp.k;
+        const uint32_t vflags = b.pass_flags[i];
+        const float K = static_cast<float>(__popc(vflags));
+        const uint32_t count = b.neigh_count[i];
+        const float4* sh = b.shift_out + static_cast<size_t>(i) * b.slots;
+        V3 suffix_contrib = splat(0.0f);
+        for (uint32_t n = 0; n < count; ++n) {
+            if (!(vflags & (1u << n))) continue;
+            const uint32_t np_ = b.neighbors[static_cast<size_t>(i) * k + n].pixel;
+            const V3 nf = sres_f(b.sres_cur, np_);
+            const float nconf = sres_conf(b.sres_cur, np_), nwsum = sres_wsum(b.sres_cur, np_);
+            const float4 o0 = sh[2 * n];
+            const V3 f_c_of_n = xyz(o0);
+            const float jac_n2c = o0.w;
+            float nmis = mis_neighbor(f_c_of_n, nf, jac_n2c, K, 1.0f, nconf);
+            if (nonfinite(nmis)) nmis = 0.0f;
+            const V3 contrib = nmis * f_c_of_n * nwsum * jac_n2c;
+            if (!nonfinite(contrib)) suffix_contrib = suffix_contrib + contrib;
+        }
+        const float4 t = b.gather_ext[3 * static_cast<size_t>(i) + 2];
+        const V3 tp = V3{t.x, t.y, t.z};
+        result = suffix_contrib * tp / t.w;
+        result = result / static_cast<float>(fp.p.gather_n);
+        result = result / (K + 1.0f);
+        if (nonfinite(result)) result = splat(0.0f);
+    }
+    float4& acc = b.gather_ext[3 * static_cast<size_t>(i) + 1];
+    const V3 sum = V3{acc.x, acc.y, acc.z} + result;
+    acc = make_float4(sum.x, sum.y, sum.z, 0.0f);
+}
+
+// GetRadiance's sum over the gathers, stored
+__global__ void __launch_bounds__(kPassBlock) k_gather_output(FrameParams fp, Bufs b, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixel_count(fp)) return;
+    const float4 a = b.gather_ext[3 * static_cast<size_t>(i) + 1];
+    V3 L = V3{a.x, a.y, a.z};
     if (nonfinite(L)) L = splat(0.0f);
     store_output(fp, out, i, L);
 }
@@ -1075,6 +1208,20 @@ void launch_final_gather_split(const SceneView& s, const FrameParams& fp, const 
     run_shift_jobs(s, fp, b, kModeGather, st, m);
     k_gather_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, out);
     MARK(kClsResample);
+    if (fp.p.gather_n > 1) {
+        for (int g = 1; g < fp.p.gather_n; ++g) {
+            cudaMemsetAsync(b.job_count, 0, sizeof(uint32_t), st);
+            k_gather_extra_prefix<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b);
+            MARK(kClsShade);
+            k_gather_extra_query<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b);
+            MARK(kClsSearch);
+            run_shift_jobs(s, fp, b, kModeGatherExtra, st, m);
+            k_gather_extra_combine<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
+            MARK(kClsResample);
+        }
+        k_gather_output<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, out);
+        MARK(kClsOther);
+    }
 }
 
 #undef MARK

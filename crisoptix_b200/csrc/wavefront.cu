@@ -205,10 +205,13 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_gather(FrameParams fp, B
     if (i < pixel_count(fp)) {
         if (b.canon_prefix[i].primary.prim == CRISB_INVALID_PRIM) {
             b.pass_status[i] = kWfIdle;
+            if (b.gather_ext) b.gather_ext[3 * static_cast<size_t>(i)] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         } else {
             const uint32_t x = i % fp.width, y = i / fp.width;
             Rng rng{b.gbuf[i].rng};
             const V3 dir = camera_dir(fp, x, y, rng);
+            // gatherN > 1: the extra prefixes start along the same ray
+            if (b.gather_ext) b.gather_ext[3 * static_cast<size_t>(i)] = make_float4(dir.x, dir.y, dir.z, 1.0f);
             Prefix cp = fresh_prefix();
             WfPath w = wf_blank();
             req = pre_begin(fp, cp, w, ld3(fp.cam.pos), dir, rng);

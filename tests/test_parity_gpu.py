@@ -167,3 +167,16 @@ def test_host_built_tree_gives_the_same_frames(cuda_device):
     desc, cam = small_sphere_room()
     p = large_config_params(scene_size_of(desc), gather_radius=0.3)
     run_parity(desc, cam, p, 48, 40, 2, lambda c, f: orbit(c, f, 120), builder=_abi.BVH_HOST)
+
+
+@pytest.mark.parametrize("gather_n,gather_m,storage", [(2, 9, _abi.STORAGE_FP32), (3, 5, _abi.STORAGE_FP16),
+                                                       (2, 1, _abi.STORAGE_FP32)])
+def test_final_gather_with_extra_prefixes(cuda_device, gather_n, gather_m, storage):
+    """gatherN > 1 (shader/final_gather.cu:190-321) on the shift machines:
+    the extra prefixes continue each pixel's random stream, search at their
+    last vertex and add their neighbours' shifted suffixes; with k = 0
+    (gatherM = 1) they draw nothing and add zero."""
+    desc, cam = small_sphere_room()
+    p = large_config_params(scene_size_of(desc), gather_radius=0.3, gather_n=gather_n, gather_m=gather_m,
+                            storage=storage, enable_accum=1)
+    run_parity(desc, cam, p, 48, 40, 3, lambda c, f: orbit(c, f, 120))
