@@ -487,9 +487,9 @@ def run_crisb(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_frame, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": dict(config_for(args.workload, W, H, sc.num_triangles, p, ppp, world, not args.no_graph),
-                           launch=tuned if tuned is not None else {"trace_block": 128, "trace_grid": 8,
-                                                                  "jobs_per_pixel": r.job_capacity()}),
+            "config": config_for(args.workload, W, H, sc.num_triangles, p, ppp, world, not args.no_graph),
+            "launch": tuned if tuned is not None else {"trace_block": 128, "trace_grid": 8,
+                                                       "jobs_per_pixel": r.job_capacity()},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 48, "d2h_bytes_per_step": W * H * 12,
                     "copies": "each frame's RGB copied to pinned host memory on a copy stream, overlapping the "
                               "next frame (two output buffers)"},

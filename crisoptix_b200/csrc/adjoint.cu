@@ -91,7 +91,30 @@ struct Touched {
     V3 d_rough;  // d T_c / d roughness of this material
 };
 
-// shared-memory gradient block (materials, then emitters) or global fallback
+// Warp-aggregated add: the lanes adding to the same address at this call
+// combine their values (__match_any_sync on the address, shuffles to the
+// group's lowest lane), which issues one atomic for the group.  Paths of
+// neighbouring pixels mostly meet the same materials and emitters, so a warp
+// issues a few atomics per vertex instead of up to 32 on one address.
+RT_D void warp_add(float* addr, float v) {
+    const unsigned active = __activemask();
+    const unsigned peers = __match_any_sync(active, reinterpret_cast<unsigned long long>(addr));
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    float sum = v;
+    unsigned rest = peers & ~(1u << leader);
+    while (rest) {
+        const int src = __ffs(rest) - 1;
+        rest &= rest - 1u;
+        const float t = __shfl_sync(peers, v, src);
+        if (lane == leader) sum += t;
+    }
+    if (lane == leader) atomicAdd(addr, sum);
+}
+
+// gradient sink: a shared-memory block of all parameters (materials, then
+// emitters) flushed once per block, or the global arrays directly when the
+// block does not fit; either way behind a warp-aggregated add
 struct GradSink {
     float* sh;  // null: add to global directly
     float* g_mat;
@@ -99,13 +122,11 @@ struct GradSink {
     uint32_t num_mats;
     RT_D void add_mat(uint32_t m, int k, float v) {
         if (v == 0.0f || !isfinite(v)) return;
-        if (sh) atomicAdd(&sh[m * kMatGrad + k], v);
-        else atomicAdd(&g_mat[m * kMatGrad + k], v);
+        warp_add(sh ? &sh[m * kMatGrad + k] : &g_mat[m * kMatGrad + k], v);
     }
     RT_D void add_em(uint32_t e, int k, float v) {
         if (v == 0.0f || !isfinite(v)) return;
-        if (sh) atomicAdd(&sh[num_mats * kMatGrad + e * kEmGrad + k], v);
-        else atomicAdd(&g_em[e * kEmGrad + k], v);
+        warp_add(sh ? &sh[num_mats * kMatGrad + e * kEmGrad + k] : &g_em[e * kEmGrad + k], v);
     }
 };
 
