@@ -99,7 +99,6 @@ __global__ void k_knn_leaves(FrameParams fp, Bufs b, lbvh::Work w, float4* leaf_
     w.leaf_box[i] = entry_box(e);
 }
 
-// ---- final gather -----------------------------------------------------------------------
 inline unsigned grid_for(uint32_t n) { return (n + kPassBlock - 1) / kPassBlock; }
 
 }  // namespace
