@@ -456,6 +456,7 @@ def run_crisb(args):
                  "tri_tests_per_ray": rays["tri_tests"] / max(n_rays, 1),
                  "trace_ms": passes["trace_ms"],
                  "rays_per_s": n_rays / (passes["trace_ms"] / 1000.0) if passes["trace_ms"] > 0 else None,
+                 "bvh": sc.bvh_info(),
                  "note": "closest / shadow queue traversal kernels of the path and shift machines; rays of shift "
                          "jobs left for the last shift round are traced inside the step kernel"}
     phases = {k: passes[k] for k in ("trace_ms", "shade_ms", "shift_ms", "resample_ms", "search_ms", "other_ms")}

@@ -54,8 +54,9 @@ def default_params(scene_size: float, **overrides) -> _abi.Params:
 
 class Scene:
     """Scene(instances, emitters): flattens instances and builds the BVH of
-    the current CUDA device (on the device by default; builder=BVH_HOST builds
-    it on the host)."""
+    the current CUDA device (on the device into compressed 8-wide nodes by
+    default; builder=BVH_DEVICE_WIDE4 builds 4-wide nodes on the device,
+    BVH_HOST 4-wide nodes on the host)."""
 
     def __init__(self, desc: SceneDesc, builder: int = _abi.BVH_DEVICE):
         lib = load()
@@ -152,6 +153,13 @@ class Scene:
         v = ctypes.c_uint32()
         check(load().crisb_scene_num_triangles(self.handle, ctypes.byref(v)))
         return v.value
+
+    def bvh_info(self) -> dict:
+        """The BVH as built: format (BVH_FORMAT_*), on_device, num_nodes,
+        node_bytes, stack_bound, depth."""
+        v = _abi.BvhInfo()
+        check(load().crisb_scene_bvh_info(self.handle, ctypes.byref(v)))
+        return {k: getattr(v, k) for k, _ in _abi.BvhInfo._fields_}
 
     def read_triangles(self):
         """World-space triangle soup: (T, 9) positions, (T, 9) normals, (T,)

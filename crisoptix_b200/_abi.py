@@ -29,6 +29,9 @@ RADIUS_CONSTANT = 0
 RADIUS_PATH_LENGTH = 1
 BVH_DEVICE = 0
 BVH_HOST = 1
+BVH_DEVICE_WIDE4 = 2
+BVH_FORMAT_WIDE4 = 0
+BVH_FORMAT_COMPRESSED8 = 1
 STORAGE_FP32 = 0
 STORAGE_FP16 = 1
 SPEC_COLOR = 0
@@ -77,6 +80,11 @@ class SceneDesc(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("trace_block", c_u32), ("trace_grid", c_u32), ("jobs_per_pixel", c_u32), ("frame_ms", c_f)]
+
+
+class BvhInfo(ctypes.Structure):
+    _fields_ = [("format", c_u32), ("on_device", c_u32), ("num_nodes", c_u32), ("node_bytes", c_u32),
+                ("stack_bound", c_i32), ("depth", c_i32)]
 
 
 class Texture(ctypes.Structure):
@@ -169,7 +177,7 @@ def buffer_dtype(buffer_id: int, storage: int = STORAGE_FP32) -> np.dtype:
 # sizeof order of crisb_abi_sizes
 ABI_STRUCTS = [Material, Mesh, Instance, Emitter, SceneDesc, Camera, CameraData, Params, HIT_DTYPE, PREFIX_DTYPE,
                PREFIX_RES_DTYPE, SUFFIX_DTYPE, SUFFIX_RES_DTYPE, GBUFFER_DTYPE, NEIGHBOR_DTYPE, TraceHit, Stats,
-               HIT16_DTYPE, PREFIX_RES16_DTYPE, SUFFIX_RES16_DTYPE]
+               HIT16_DTYPE, PREFIX_RES16_DTYPE, SUFFIX_RES16_DTYPE, Tuning, BvhInfo]
 
 
 def abi_size(t) -> int:
@@ -186,6 +194,7 @@ ENTRY_POINTS = {
     "crisb_scene_destroy": (c_i32, [c_vp]),
     "crisb_scene_size": (c_i32, [c_vp, ctypes.POINTER(c_f)]),
     "crisb_scene_num_triangles": (c_i32, [c_vp, ctypes.POINTER(c_u32)]),
+    "crisb_scene_bvh_info": (c_i32, [c_vp, ctypes.POINTER(BvhInfo)]),
     "crisb_scene_read_triangles": (c_i32, [c_vp, c_vp, c_vp, c_vp]),
     "crisb_trace_rays": (c_i32, [c_vp, c_vp, c_vp, c_u32, c_i32, c_vp]),
     "crisb_renderer_create": (c_i32, [c_vp, c_u32, c_u32, ctypes.POINTER(Params), ctypes.POINTER(c_vp)]),

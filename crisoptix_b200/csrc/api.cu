@@ -222,6 +222,7 @@ struct crisb_scene {
     std::vector<uint32_t> h_mat;
     std::vector<float> h_uv;  // 6 per triangle when the scene has uvs
     DevBuf<Bvh4Node> nodes;
+    DevBuf<Bvh8QNode> qnodes;  // the compressed tree, when built (then `nodes` is empty)
     int bvh_max_stack = 0, bvh_max_depth = 0;
     bool bvh_on_device = false;  // built by build_wide_bvh_device
     DevBuf<float4> tris;
@@ -240,6 +241,7 @@ struct crisb_scene {
     SceneView view(int* err_word) const {
         SceneView v;
         v.nodes = nodes.p;
+        v.qnodes = qnodes.p;
         v.tris = tris.p;
         v.shade = shade.p;
         v.mats = mats.p;
@@ -414,6 +416,57 @@ void upload_textures(const crisb_scene_desc& d, crisb_scene& s) {
 // boxes containing their subtrees, the traversal stack bound).  Returns false
 // when the tree would need a deeper traversal stack than the kernels have
 // (the host builder's median fallback then bounds the depth).
+// the compressed 8-wide tree on the device, validated on the host; false
+// when the scene does not qualify (coordinates too large, tree deeper than
+// the group stack)
+bool build_qbvh_on_device(crisb_scene& s, float max_abs) {
+    if (!(max_abs < kQMaxCoord)) return false;
+    const uint32_t n = s.num_tris;
+    DevBuf<float> pos;
+    pos.upload(s.h_pos.data(), std::max<size_t>(s.h_pos.size(), 1));
+    DeviceWideBvh db;
+    const float margin = box_margin(max_abs);
+    check(build_wide_bvh_device(pos.p, n, kQLeafMax, margin, true, nullptr, &db), "device BVH build");
+    std::vector<Bvh8QNode> hn(db.num_nodes);
+    std::vector<float4> t3(3 * static_cast<size_t>(std::max<uint32_t>(n, 1)));
+    cudaError_t e = cudaMemcpy(hn.data(), db.qnodes, db.num_nodes * sizeof(Bvh8QNode), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(t3.data(), db.tris, t3.size() * sizeof(float4), cudaMemcpyDeviceToHost);
+    auto drop = [&]() {
+        cudaFree(db.qnodes);
+        cudaFree(db.tris);
+    };
+    if (e != cudaSuccess) {
+        drop();
+        check(e, "device BVH copy");
+    }
+    std::vector<uint32_t> order(n);
+    for (uint32_t i = 0; i < n; ++i) std::memcpy(&order[i], &t3[3 * i + 2].w, 4);
+    int depth = 0;
+    try {
+        depth = validate_qbvh(hn, order, s.h_pos.data(), n, margin);
+    } catch (const std::runtime_error& ex) {
+        drop();
+        throw Error(CRISB_ERR_INVALID_ARGUMENT, std::string("device scene build: ") + ex.what());
+    }
+    // at most one waiting group per level above the deepest node
+    if (depth > kQStack) {
+        drop();
+        return false;
+    }
+    s.nodes.release();
+    s.qnodes.release();
+    s.qnodes.p = db.qnodes;
+    s.qnodes.n = db.num_nodes;
+    s.tris.release();
+    s.tris.p = db.tris;
+    s.tris.n = 3 * static_cast<size_t>(std::max<uint32_t>(n, 1));
+    s.bvh_max_stack = depth;
+    s.bvh_max_depth = db.binary_depth;
+    s.bvh_on_device = true;
+    check(cudaDeviceSynchronize(), "scene build");
+    return true;
+}
+
 bool build_bvh_on_device(crisb_scene& s) {
     const uint32_t n = s.num_tris;
     float max_abs = 0.0f;
@@ -421,7 +474,8 @@ bool build_bvh_on_device(crisb_scene& s) {
     DevBuf<float> pos;
     pos.upload(s.h_pos.data(), std::max<size_t>(s.h_pos.size(), 1));
     DeviceWideBvh db;
-    check(build_wide_bvh_device(pos.p, n, kTriLeafMax, box_margin(max_abs), nullptr, &db), "device BVH build");
+    check(build_wide_bvh_device(pos.p, n, kTriLeafMax, box_margin(max_abs), false, nullptr, &db),
+          "device BVH build");
     WideBvh hb;
     hb.nodes.resize(db.num_nodes);
     std::vector<float4> t3(3 * static_cast<size_t>(std::max<uint32_t>(n, 1)));
@@ -486,8 +540,15 @@ void build_scene(const crisb_scene_desc& d, crisb_scene& s) {
     upload_textures(d, s);
     s.err.alloc(1);
     check(cudaMemset(s.err.p, 0, sizeof(int)), "memset");
-    require(d.bvh_builder == CRISB_BVH_DEVICE || d.bvh_builder == CRISB_BVH_HOST, "scene: unknown bvh_builder");
-    if (d.bvh_builder == CRISB_BVH_DEVICE && build_bvh_on_device(s)) return;
+    require(d.bvh_builder == CRISB_BVH_DEVICE || d.bvh_builder == CRISB_BVH_HOST ||
+                d.bvh_builder == CRISB_BVH_DEVICE_WIDE4,
+            "scene: unknown bvh_builder");
+    if (d.bvh_builder == CRISB_BVH_DEVICE) {
+        float max_abs = 0.0f;
+        for (float v : s.h_pos) max_abs = std::max(max_abs, std::fabs(v));
+        if (build_qbvh_on_device(s, max_abs)) return;
+    }
+    if (d.bvh_builder != CRISB_BVH_HOST && build_bvh_on_device(s)) return;
     // 4-wide SAH BVH built on the host; triangles stored in leaf order
     WideBvh bvh = build_wide_bvh(s.h_pos.data(), n, kTriLeafMax, kMedianDepth);
     if (bvh.max_stack > kTraversalStack) {
@@ -1031,6 +1092,19 @@ int crisb_scene_num_triangles(const crisb_scene* scene, uint32_t* out) {
     return guarded([&] {
         require(scene && out, "null argument");
         *out = scene->num_tris;
+    });
+}
+
+int crisb_scene_bvh_info(const crisb_scene* scene, crisb_bvh_info* out) {
+    return guarded([&] {
+        require(scene && out, "null argument");
+        const bool q = scene->qnodes.p != nullptr;
+        out->format = q ? CRISB_BVH_FORMAT_COMPRESSED8 : CRISB_BVH_FORMAT_WIDE4;
+        out->on_device = scene->bvh_on_device ? 1u : 0u;
+        out->num_nodes = static_cast<uint32_t>(q ? scene->qnodes.n : scene->nodes.n);
+        out->node_bytes = q ? static_cast<uint32_t>(sizeof(Bvh8QNode)) : static_cast<uint32_t>(sizeof(Bvh4Node));
+        out->stack_bound = scene->bvh_max_stack;
+        out->depth = scene->bvh_max_depth;
     });
 }
 
@@ -1644,7 +1718,8 @@ int crisb_abi_sizes(uint32_t* out, uint32_t n) {
         sizeof(crisb_scene_desc),  sizeof(crisb_camera),       sizeof(crisb_camera_data),  sizeof(crisb_params),
         sizeof(crisb_hit_rec),     sizeof(crisb_prefix_rec),   sizeof(crisb_prefix_res_rec), sizeof(crisb_suffix_rec),
         sizeof(crisb_suffix_res_rec), sizeof(crisb_gbuffer_rec), sizeof(crisb_neighbor_rec), sizeof(crisb_trace_hit),
-        sizeof(crisb_stats), sizeof(crisb_hit16_rec), sizeof(crisb_prefix_res16_rec), sizeof(crisb_suffix_res16_rec)};
+        sizeof(crisb_stats), sizeof(crisb_hit16_rec), sizeof(crisb_prefix_res16_rec), sizeof(crisb_suffix_res16_rec),
+        sizeof(crisb_tuning), sizeof(crisb_bvh_info)};
     const uint32_t count = sizeof(sizes) / sizeof(sizes[0]);
     if (!out) return static_cast<int>(count);
     for (uint32_t i = 0; i < n && i < count; ++i) out[i] = sizes[i];

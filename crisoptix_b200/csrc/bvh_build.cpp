@@ -411,4 +411,106 @@ int validate_wide_bvh(const WideBvh& bvh, const float* pos, uint32_t n, int leaf
     return max_stack;
 }
 
+int validate_qbvh(const std::vector<Bvh8QNode>& nodes, const std::vector<uint32_t>& order, const float* pos,
+                  uint32_t n, float margin) {
+    auto fail = [](const char* what) { throw std::runtime_error(std::string("compressed bvh check: ") + what); };
+    const size_t nn = nodes.size();
+    if (nn == 0) fail("no root");
+    if (order.size() != n) fail("leaf order size");
+    std::vector<uint8_t> seen_tri(n, 0), seen_node(nn, 0);
+    std::vector<int> depth(nn, 0);
+    // top-down: links, leaves, depth; children always lie after their parent
+    std::vector<uint32_t> todo{0};
+    seen_node[0] = 1;
+    depth[0] = 1;
+    int max_depth = 1;
+    while (!todo.empty()) {
+        const uint32_t v = todo.back();
+        todo.pop_back();
+        const Bvh8QNode& nd = nodes[v];
+        max_depth = std::max(max_depth, depth[v]);
+        for (int a = 0; a < 3; ++a) {
+            const int e = a == 0 ? nd.ex : a == 1 ? nd.ey : nd.ez;
+            if (e < -126 || e > 100) fail("grid exponent out of range");
+        }
+        int rank = 0;
+        for (int c = 0; c < 8; ++c) {
+            const uint32_t m = nd.meta[c];
+            const bool inner_bit = (nd.imask >> c) & 1u;
+            if (m == 0) {
+                if (inner_bit) fail("empty slot marked inner");
+                continue;
+            }
+            if (nd.qlo_x[c] > nd.qhi_x[c] || nd.qlo_y[c] > nd.qhi_y[c] || nd.qlo_z[c] > nd.qhi_z[c])
+                fail("inverted child box");
+            if ((m & 0x18u) == 0x18u) {
+                if (m != (0x38u | static_cast<uint32_t>(c)) || !inner_bit) fail("inner slot meta");
+                const uint64_t ch = static_cast<uint64_t>(nd.child_base) + static_cast<uint64_t>(rank++);
+                if (ch >= nn || ch <= v) fail("inner link out of range");
+                if (seen_node[ch]) fail("inner node reached twice");
+                seen_node[ch] = 1;
+                depth[ch] = depth[v] + 1;
+                todo.push_back(static_cast<uint32_t>(ch));
+                continue;
+            }
+            if (inner_bit) fail("leaf slot marked inner");
+            const uint32_t cb = m >> 5, off = m & 31u;
+            const uint32_t cnt = cb == 1u ? 1u : cb == 3u ? 2u : cb == 7u ? 3u : 0u;
+            if (cnt == 0 || off + cnt > static_cast<uint32_t>(kQTrisPerNode)) fail("leaf meta");
+            for (uint32_t k = 0; k < cnt; ++k) {
+                const uint64_t slot = static_cast<uint64_t>(nd.tri_base) + off + k;
+                if (slot >= n) fail("leaf range");
+                if (seen_tri[slot]) fail("triangle in two leaves");
+                seen_tri[slot] = 1;
+                if (order[slot] >= n) fail("leaf order entry");
+            }
+        }
+    }
+    for (uint32_t i = 0; i < n; ++i)
+        if (!seen_tri[i]) fail("triangle in no leaf");
+    for (size_t i = 0; i < nn; ++i)
+        if (!seen_node[i]) fail("unreachable node");
+    // bottom-up: subtree bounds against the decoded child boxes
+    std::vector<double> sub(6 * nn);
+    const double half = 0.5 * static_cast<double>(margin);
+    for (size_t v = nn; v-- > 0;) {
+        const Bvh8QNode& nd = nodes[v];
+        double box[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+        const double p[3] = {nd.px, nd.py, nd.pz};
+        const int e[3] = {nd.ex, nd.ey, nd.ez};
+        const uint8_t* qlo[3] = {nd.qlo_x, nd.qlo_y, nd.qlo_z};
+        const uint8_t* qhi[3] = {nd.qhi_x, nd.qhi_y, nd.qhi_z};
+        int rank = 0;
+        for (int c = 0; c < 8; ++c) {
+            const uint32_t m = nd.meta[c];
+            if (m == 0) continue;
+            double cb[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+            if ((m & 0x18u) == 0x18u) {
+                const size_t ch = nd.child_base + static_cast<size_t>(rank++);
+                for (int a = 0; a < 6; ++a) cb[a] = sub[6 * ch + a];
+            } else {
+                const uint32_t cbits = m >> 5, off = m & 31u;
+                const uint32_t cnt = cbits == 1u ? 1u : cbits == 3u ? 2u : 3u;
+                for (uint32_t k = 0; k < cnt; ++k) {
+                    const float* t = pos + 9 * static_cast<size_t>(order[nd.tri_base + off + k]);
+                    for (int vtx = 0; vtx < 3; ++vtx)
+                        for (int a = 0; a < 3; ++a) {
+                            cb[a] = std::min(cb[a], static_cast<double>(t[3 * vtx + a]));
+                            cb[3 + a] = std::max(cb[3 + a], static_cast<double>(t[3 * vtx + a]));
+                        }
+                }
+            }
+            for (int a = 0; a < 3; ++a) {
+                const double lo = p[a] + std::ldexp(static_cast<double>(qlo[a][c]), e[a]);
+                const double hi = p[a] + std::ldexp(static_cast<double>(qhi[a][c]), e[a]);
+                if (lo > cb[a] - half || hi < cb[3 + a] + half) fail("child box does not contain its subtree");
+                box[a] = std::min(box[a], cb[a]);
+                box[3 + a] = std::max(box[3 + a], cb[3 + a]);
+            }
+        }
+        for (int a = 0; a < 6; ++a) sub[6 * v + a] = box[a];
+    }
+    return max_depth;
+}
+
 }  // namespace crisb

@@ -51,6 +51,46 @@ struct WideBvh {
     int max_depth = 0;            // depth of the binary tree
 };
 
+// Compressed 8-wide node (80 bytes, five 16-byte loads), after Ylitie, Karras
+// & Laine 2017 ("Efficient Incoherent Ray Traversal on GPUs Through
+// Compressed Wide BVHs").  Per axis the child boxes lie on the grid
+// p + 2^e * q, q in [0, 255], rounded outward from boxes already widened by
+// box_margin().  Inner children are stored contiguously from child_base in
+// slot order, leaf triangles contiguously (leaf order) from tri_base.  Per
+// slot, meta is
+//   0                   an empty slot,
+//   0b001'11sss         an inner child (sss = the slot),
+//   0b ccc'ooooo        a leaf: ccc = 1, 3 or 7 for 1-3 triangles at
+//                       tri_base + ooooo (ooooo < 24).
+// Children are placed in slots by the octant of their centroid relative to
+// the node's (slot bit a set: toward +a), so a ray whose direction signs give
+// octant o (bit a set: negative along a) meets the child in slot o ^ k
+// roughly k-th.
+struct alignas(16) Bvh8QNode {
+    float px, py, pz;
+    int8_t ex, ey, ez;
+    uint8_t imask;  // bit s: slot s holds an inner child
+    uint32_t child_base, tri_base;
+    uint8_t meta[8];
+    uint8_t qlo_x[8], qlo_y[8], qlo_z[8], qhi_x[8], qhi_y[8], qhi_z[8];
+};
+static_assert(sizeof(Bvh8QNode) == 80, "compressed node size");
+constexpr int kQLeafMax = 3;      // triangles per leaf child of a compressed node
+constexpr int kQTrisPerNode = 24;  // triangles per compressed node
+// the compressed format needs |coordinates| below this (the slab test's
+// per-node terms stay finite for every ray direction; larger scenes use
+// 4-wide nodes)
+constexpr float kQMaxCoord = 1.6e7f;
+
+// Structural check of a compressed tree: node links in range and each node
+// reached once, leaves of 1-3 triangles inside the node's 24, every triangle
+// in exactly one leaf, every decoded child box containing its subtree's
+// triangles widened by half the margin (compared in double precision), grid
+// exponents in range.  `order`: leaf order -> triangle.  Returns the depth of
+// the tree (the traversal's group-stack bound).  Throws std::runtime_error.
+int validate_qbvh(const std::vector<Bvh8QNode>& nodes, const std::vector<uint32_t>& order, const float* pos,
+                  uint32_t num_tris, float margin);
+
 // `pos`: 9 floats per triangle (three vertices).  Leaves hold at most
 // `leaf_max` triangles; below `median_depth` binary levels the SAH split is
 // replaced by object-median splits so the depth stays logarithmic.

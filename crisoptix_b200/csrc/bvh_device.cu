@@ -203,8 +203,9 @@ __device__ bool is_leaf_child(const BNode& b, uint32_t n_tris, int id) {
 }
 
 // children of the wide node standing for binary node b: open the inner child
-// with the largest surface area until there are four
-__device__ int gather_children(const BNode* nodes, uint32_t n_tris, int b, int ch[4]) {
+// with the largest surface area until there are kW
+template <int kW>
+__device__ int gather_children(const BNode* nodes, uint32_t n_tris, int b, int ch[kW]) {
     const BNode& root = nodes[b];
     if (static_cast<uint32_t>(b) < n_tris || (root.meta & kLeafyBit)) {
         ch[0] = b;  // a single leaf (only the root can be one)
@@ -213,7 +214,7 @@ __device__ int gather_children(const BNode* nodes, uint32_t n_tris, int b, int c
     int k = 2;
     ch[0] = root.left;
     ch[1] = root.right;
-    while (k < 4) {
+    while (k < kW) {
         int best = -1;
         float best_area = -1.0f;
         for (int c = 0; c < k; ++c) {
@@ -235,12 +236,13 @@ __device__ int gather_children(const BNode* nodes, uint32_t n_tris, int b, int c
     return k;
 }
 
+template <int kW>
 __global__ void k_collapse_count(const int* __restrict__ level, uint32_t nl, const BNode* __restrict__ nodes,
                                  uint32_t n_tris, uint32_t* inner_cnt, uint32_t* tri_cnt) {
     const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nl) return;
-    int ch[4];
-    const int k = gather_children(nodes, n_tris, level[e], ch);
+    int ch[kW];
+    const int k = gather_children<kW>(nodes, n_tris, level[e], ch);
     uint32_t ni = 0, nt = 0;
     for (int c = 0; c < k; ++c) {
         const BNode& nd = nodes[ch[c]];
@@ -251,6 +253,30 @@ __global__ void k_collapse_count(const int* __restrict__ level, uint32_t nl, con
     tri_cnt[e] = nt;
 }
 
+// the triangles of leafy subtree `root`, left to right, from position `tri`
+// of the leaf order; returns the position after them
+__device__ uint32_t write_leaf_tris(const BNode* __restrict__ nodes, uint32_t n_tris, const uint32_t* __restrict__ order,
+                                    const float* __restrict__ pos, int root, uint32_t tri, float4* tris) {
+    int stack[2 * 8];
+    int sp = 0;
+    stack[sp++] = root;
+    while (sp > 0) {
+        const int id = stack[--sp];
+        if (static_cast<uint32_t>(id) < n_tris) {
+            const uint32_t t = order[id];
+            const float* p = pos + 9 * static_cast<size_t>(t);
+            tris[3 * tri + 0] = make_float4(p[0], p[1], p[2], 0.0f);
+            tris[3 * tri + 1] = make_float4(p[3], p[4], p[5], 0.0f);
+            tris[3 * tri + 2] = make_float4(p[6], p[7], p[8], __uint_as_float(t));
+            ++tri;
+        } else if (sp + 2 <= 2 * 8) {
+            stack[sp++] = nodes[id].right;
+            stack[sp++] = nodes[id].left;
+        }
+    }
+    return tri;
+}
+
 __global__ void k_collapse_write(const int* __restrict__ level, uint32_t nl, const BNode* __restrict__ nodes,
                                  uint32_t n_tris, const uint32_t* __restrict__ order, const float* __restrict__ pos,
                                  const uint32_t* __restrict__ inner_off, const uint32_t* __restrict__ tri_off,
@@ -259,7 +285,7 @@ __global__ void k_collapse_write(const int* __restrict__ level, uint32_t nl, con
     const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nl) return;
     int ch[4];
-    const int k = gather_children(nodes, n_tris, level[e], ch);
+    const int k = gather_children<4>(nodes, n_tris, level[e], ch);
     Bvh4Node w;
     for (int c = 0; c < kBvhWidth; ++c) {
         w.link[c] = kNoChild;
@@ -277,31 +303,120 @@ __global__ void k_collapse_write(const int* __restrict__ level, uint32_t nl, con
         w.hi_y[c] = nd.hi[1] + margin;
         w.hi_z[c] = nd.hi[2] + margin;
         if (is_leaf_child(nd, n_tris, ch[c])) {
-            // the subtree's triangles, left to right
             const uint32_t first = tri;
-            int stack[2 * 8];
-            int sp = 0;
-            stack[sp++] = ch[c];
-            while (sp > 0) {
-                const int id = stack[--sp];
-                if (static_cast<uint32_t>(id) < n_tris) {
-                    const uint32_t t = order[id];
-                    const float* p = pos + 9 * static_cast<size_t>(t);
-                    tris[3 * tri + 0] = make_float4(p[0], p[1], p[2], 0.0f);
-                    tris[3 * tri + 1] = make_float4(p[3], p[4], p[5], 0.0f);
-                    tris[3 * tri + 2] = make_float4(p[6], p[7], p[8], __uint_as_float(t));
-                    ++tri;
-                } else if (sp + 2 <= 2 * 8) {
-                    stack[sp++] = nodes[id].right;
-                    stack[sp++] = nodes[id].left;
-                }
-            }
+            tri = write_leaf_tris(nodes, n_tris, order, pos, ch[c], tri, tris);
             w.link[c] = -1 - static_cast<int>(first);
             w.count[c] = static_cast<int>(tri - first);
         } else {
             w.link[c] = static_cast<int>(child_base + inner);
             next_level[inner] = ch[c];
             ++inner;
+        }
+    }
+    out[node_base + e] = w;
+}
+
+// one compressed node per binary node of the level: up to eight children
+// placed in octant slots (greedy: the cheapest remaining (child, slot) pair
+// first, cost = centroid offset from the node's centre along the slot's
+// diagonal, ties to the lower child then slot), boxes widened by `margin`
+// then quantised outward in double precision
+__global__ void k_qcollapse_write(const int* __restrict__ level, uint32_t nl, const BNode* __restrict__ nodes,
+                                  uint32_t n_tris, const uint32_t* __restrict__ order, const float* __restrict__ pos,
+                                  const uint32_t* __restrict__ inner_off, const uint32_t* __restrict__ tri_off,
+                                  uint32_t node_base, uint32_t child_base, uint32_t tri_base, float margin,
+                                  Bvh8QNode* out, float4* tris, int* next_level) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nl) return;
+    int ch[8];
+    const int k = gather_children<8>(nodes, n_tris, level[e], ch);
+    float lo[8][3], hi[8][3], plo[3], phi[3];
+    for (int a = 0; a < 3; ++a) {
+        plo[a] = FLT_MAX;
+        phi[a] = -FLT_MAX;
+    }
+    for (int c = 0; c < k; ++c) {
+        const BNode& nd = nodes[ch[c]];
+        for (int a = 0; a < 3; ++a) {
+            lo[c][a] = nd.lo[a] - margin;
+            hi[c][a] = nd.hi[a] + margin;
+            plo[a] = fminf(plo[a], lo[c][a]);
+            phi[a] = fmaxf(phi[a], hi[c][a]);
+        }
+    }
+    int slot_child[8];
+    for (int t = 0; t < 8; ++t) slot_child[t] = -1;
+    uint32_t used_c = 0, used_s = 0;
+    for (int r = 0; r < k; ++r) {
+        float best = FLT_MAX;
+        int bc = -1, bs = -1;
+        for (int c = 0; c < k; ++c) {
+            if ((used_c >> c) & 1u) continue;
+            float off[3];
+            for (int a = 0; a < 3; ++a) off[a] = (lo[c][a] + hi[c][a]) - (plo[a] + phi[a]);
+            for (int t = 0; t < 8; ++t) {
+                if ((used_s >> t) & 1u) continue;
+                const float cost = ((t & 1) ? -off[0] : off[0]) + ((t & 2) ? -off[1] : off[1]) +
+                                   ((t & 4) ? -off[2] : off[2]);
+                if (bc < 0 || cost < best) {
+                    best = cost;
+                    bc = c;
+                    bs = t;
+                }
+            }
+        }
+        used_c |= 1u << bc;
+        used_s |= 1u << bs;
+        slot_child[bs] = bc;
+    }
+    Bvh8QNode w;
+    memset(&w, 0, sizeof(w));
+    int ex[3];
+    double scale[3];
+    float porg[3];
+    for (int a = 0; a < 3; ++a) {
+        const double ext = k > 0 ? static_cast<double>(phi[a]) - static_cast<double>(plo[a]) : 0.0;
+        int x = -126;
+        if (ext > 0.0) {
+            frexp(ext / 255.0, &x);  // ext / 255 < 2^x
+            x = max(x, -126);
+        }
+        porg[a] = k > 0 ? plo[a] : 0.0f;
+        ex[a] = x;
+        scale[a] = ldexp(1.0, x);
+    }
+    w.px = porg[0];
+    w.py = porg[1];
+    w.pz = porg[2];
+    w.ex = static_cast<int8_t>(ex[0]);
+    w.ey = static_cast<int8_t>(ex[1]);
+    w.ez = static_cast<int8_t>(ex[2]);
+    w.child_base = child_base + inner_off[e];
+    w.tri_base = tri_base + tri_off[e];
+    uint8_t* qlo[3] = {w.qlo_x, w.qlo_y, w.qlo_z};
+    uint8_t* qhi[3] = {w.qhi_x, w.qhi_y, w.qhi_z};
+    uint32_t cursor = 0, rank = 0;
+    for (int t = 0; t < 8; ++t) {
+        const int c = slot_child[t];
+        if (c < 0) continue;
+        for (int a = 0; a < 3; ++a) {
+            const double p = static_cast<double>(porg[a]);
+            const double l = floor((static_cast<double>(lo[c][a]) - p) / scale[a]);
+            const double h = ceil((static_cast<double>(hi[c][a]) - p) / scale[a]);
+            qlo[a][t] = static_cast<uint8_t>(fmin(fmax(l, 0.0), 255.0));
+            qhi[a][t] = static_cast<uint8_t>(fmin(fmax(h, 0.0), 255.0));
+        }
+        const BNode& nd = nodes[ch[c]];
+        if (is_leaf_child(nd, n_tris, ch[c])) {
+            const uint32_t first = w.tri_base + cursor;
+            const uint32_t cnt = write_leaf_tris(nodes, n_tris, order, pos, ch[c], first, tris) - first;
+            w.meta[t] = static_cast<uint8_t>((((1u << cnt) - 1u) << 5) | cursor);
+            cursor += cnt;
+        } else {
+            w.meta[t] = static_cast<uint8_t>(0x38u | static_cast<uint32_t>(t));
+            w.imask |= static_cast<uint8_t>(1u << t);
+            next_level[inner_off[e] + rank] = ch[c];
+            ++rank;
         }
     }
     out[node_base + e] = w;
@@ -314,8 +429,9 @@ cudaError_t dev_alloc(T** p, size_t count) {
 
 }  // namespace
 
-cudaError_t build_wide_bvh_device(const float* pos, uint32_t n, int leaf_max, float margin, cudaStream_t st,
-                                  DeviceWideBvh* out) {
+cudaError_t build_wide_bvh_device(const float* pos, uint32_t n, int leaf_max, float margin, bool compressed,
+                                  cudaStream_t st, DeviceWideBvh* out) {
+    if (compressed) leaf_max = std::min(leaf_max, kQLeafMax);
     *out = DeviceWideBvh{};
     cudaError_t e = cudaSuccess;
     // scratch
@@ -349,6 +465,7 @@ cudaError_t build_wide_bvh_device(const float* pos, uint32_t n, int leaf_max, fl
         cudaFree(level[1]);
         if (err != cudaSuccess) {
             cudaFree(out->nodes);
+            cudaFree(out->qnodes);
             cudaFree(out->tris);
             *out = DeviceWideBvh{};
         }
@@ -380,7 +497,8 @@ cudaError_t build_wide_bvh_device(const float* pos, uint32_t n, int leaf_max, fl
     };
     TRY(dev_alloc(&level[0], m));
     TRY(dev_alloc(&level[1], m));
-    TRY(dev_alloc(&out->nodes, m));
+    if (compressed) TRY(dev_alloc(&out->qnodes, m));
+    else TRY(dev_alloc(&out->nodes, m));
     TRY(dev_alloc(&out->tris, 3 * static_cast<size_t>(m)));
     TRY(cudaMemsetAsync(out->tris, 0, 3 * static_cast<size_t>(m) * sizeof(float4), st));
 
@@ -425,10 +543,17 @@ cudaError_t build_wide_bvh_device(const float* pos, uint32_t n, int leaf_max, fl
 
     // 4. collapse level by level; the root wide node at 0
     if (n == 0) {
-        Bvh4Node w;
-        std::memset(&w, 0, sizeof(w));
-        for (int c = 0; c < kBvhWidth; ++c) w.link[c] = kNoChild;
-        TRY(cudaMemcpyAsync(out->nodes, &w, sizeof(w), cudaMemcpyHostToDevice, st));
+        if (compressed) {
+            Bvh8QNode q;
+            std::memset(&q, 0, sizeof(q));
+            q.ex = q.ey = q.ez = -126;
+            TRY(cudaMemcpyAsync(out->qnodes, &q, sizeof(q), cudaMemcpyHostToDevice, st));
+        } else {
+            Bvh4Node w;
+            std::memset(&w, 0, sizeof(w));
+            for (int c = 0; c < kBvhWidth; ++c) w.link[c] = kNoChild;
+            TRY(cudaMemcpyAsync(out->nodes, &w, sizeof(w), cudaMemcpyHostToDevice, st));
+        }
         out->num_nodes = 1;
         TRY(cudaStreamSynchronize(st));
         return fail(cudaSuccess);
@@ -438,16 +563,22 @@ cudaError_t build_wide_bvh_device(const float* pos, uint32_t n, int leaf_max, fl
     int lv = 0, depth = 0;
     while (nl > 0) {
         const uint32_t child_base = node_base + nl;
-        k_collapse_count<<<blocks(nl), kBlock, 0, st>>>(level[lv], nl, nodes, n, mflag, kflag);
+        if (compressed) k_collapse_count<8><<<blocks(nl), kBlock, 0, st>>>(level[lv], nl, nodes, n, mflag, kflag);
+        else k_collapse_count<4><<<blocks(nl), kBlock, 0, st>>>(level[lv], nl, nodes, n, mflag, kflag);
         TRY(scan(mflag, mpos, nl, totals));
         TRY(scan(kflag, kpos, nl, totals + 1));
         uint32_t tot[2] = {0, 0};
         TRY(cudaMemcpyAsync(tot, totals, sizeof(tot), cudaMemcpyDeviceToHost, st));
         TRY(cudaStreamSynchronize(st));
         if (child_base + tot[0] > m || tri_base + tot[1] > n) return fail(cudaErrorUnknown);
-        k_collapse_write<<<blocks(nl), kBlock, 0, st>>>(level[lv], nl, nodes, n, order, pos, mpos, kpos, node_base,
-                                                        child_base, tri_base, margin, out->nodes, out->tris,
-                                                        level[lv ^ 1]);
+        if (compressed)
+            k_qcollapse_write<<<blocks(nl), kBlock, 0, st>>>(level[lv], nl, nodes, n, order, pos, mpos, kpos,
+                                                             node_base, child_base, tri_base, margin, out->qnodes,
+                                                             out->tris, level[lv ^ 1]);
+        else
+            k_collapse_write<<<blocks(nl), kBlock, 0, st>>>(level[lv], nl, nodes, n, order, pos, mpos, kpos,
+                                                            node_base, child_base, tri_base, margin, out->nodes,
+                                                            out->tris, level[lv ^ 1]);
         TRY(cudaGetLastError());
         node_base = child_base;
         tri_base += tot[1];

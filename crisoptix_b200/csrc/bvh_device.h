@@ -16,7 +16,9 @@
 //   4. a top-down collapse into the 4-wide nodes of bvh_build.h, level by
 //      level: a wide node opens its children largest surface area first until
 //      it has four; leaf children store their triangles contiguously in leaf
-//      order; child boxes are widened by box_margin().
+//      order; child boxes are widened by box_margin().  Or the same collapse
+//      to eight children into compressed nodes (Bvh8QNode): children placed
+//      in octant slots, boxes quantised outward on the node's grid.
 // The tree lands in the same node and triangle layouts the host builder
 // (bvh_build.h) produces, so traversal is shared.
 #pragma once
@@ -31,17 +33,20 @@
 namespace crisb {
 
 struct DeviceWideBvh {
-    Bvh4Node* nodes = nullptr;  // device, root at 0
+    Bvh4Node* nodes = nullptr;    // device, root at 0 (4-wide build)
+    Bvh8QNode* qnodes = nullptr;  // device, root at 0 (compressed 8-wide build)
     uint32_t num_nodes = 0;
     float4* tris = nullptr;     // device, 3 per triangle in leaf order, triangle id bits in tris[3i+2].w
     int binary_depth = 0;       // levels of the collapse
 };
 
 // Builds from world-space positions on the device (pos_dev: 9 floats per
-// triangle).  Allocates nodes and tris with cudaMalloc (free them with
+// triangle).  `compressed`: the collapse makes compressed 8-wide nodes
+// (Bvh8QNode, leaves of at most kQLeafMax triangles) instead of 4-wide ones.
+// Allocates nodes (or qnodes) and tris with cudaMalloc (free them with
 // cudaFree); synchronises `st` between clustering and collapse steps.
 // Returns cudaSuccess or the first CUDA error.
-cudaError_t build_wide_bvh_device(const float* pos_dev, uint32_t n, int leaf_max, float margin, cudaStream_t st,
-                                  DeviceWideBvh* out);
+cudaError_t build_wide_bvh_device(const float* pos_dev, uint32_t n, int leaf_max, float margin, bool compressed,
+                                  cudaStream_t st, DeviceWideBvh* out);
 
 }  // namespace crisb

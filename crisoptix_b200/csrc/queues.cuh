@@ -88,7 +88,7 @@ struct TraceShape<256> {
     static constexpr int kMinBlocks = 4;
 };
 
-template <class R, int kB>
+template <class R, int kB, int kFmt>
 __global__ void __launch_bounds__(kB, TraceShape<kB>::kMinBlocks) k_q_trace(SceneView s, const uint32_t* qc,
                                                                           const uint32_t* ccnt, const uint32_t* qs,
                                                                           const uint32_t* scnt, R* rec) {
@@ -100,13 +100,15 @@ __global__ void __launch_bounds__(kB, TraceShape<kB>::kMinBlocks) k_q_trace(Scen
             const uint32_t i = qc[t];
             closest_ray(rec[i], o, d);
             count_ray(s, 0);
-            const TraceResult h = traverse<false>(s, make_ray(o, d), 1e-3f, 1e16f);
+            const TraceResult h = traverse_fmt<kFmt, false>(s, make_ray(o, d), 1e-3f, 1e16f);
             set_hit(rec[i], make_float4(__uint_as_float(h.prim), h.t, h.u, h.v));
         } else {
             const uint32_t i = qs[t - nc];
             float tmax;
             shadow_ray(rec[i], o, d, tmax);
-            set_occluded(rec[i], occluded(s, o, d, 1e-3f, tmax) ? 1u : 0u);
+            count_ray(s, 1);
+            const bool occ = traverse_fmt<kFmt, true>(s, make_ray(o, d), 1e-3f, tmax).prim != CRISB_INVALID_PRIM;
+            set_occluded(rec[i], occ ? 1u : 0u);
         }
     }
 }
@@ -135,24 +137,32 @@ inline unsigned persistent_grid_at(const void* kernel, int block) {
     return 148u * 4u;
 }
 
-template <class R, int kB>
+template <class R, int kB, int kFmt>
 unsigned trace_grid_of() {
-    static const unsigned g = persistent_grid_at(reinterpret_cast<const void*>(k_q_trace<R, kB>), kB);
+    static const unsigned g = persistent_grid_at(reinterpret_cast<const void*>(k_q_trace<R, kB, kFmt>), kB);
     return g;
 }
 
+template <class R, int kFmt>
+void launch_trace_fmt(uint32_t block, uint32_t m, cudaStream_t st, const SceneView& s, const uint32_t* qc,
+                      const uint32_t* ccnt, const uint32_t* qs, const uint32_t* scnt, R* rec) {
+    if (block == 64)
+        k_q_trace<R, 64, kFmt><<<trace_grid_of<R, 64, kFmt>() * m, 64, 0, st>>>(s, qc, ccnt, qs, scnt, rec);
+    else if (block == 256)
+        k_q_trace<R, 256, kFmt><<<trace_grid_of<R, 256, kFmt>() * m, 256, 0, st>>>(s, qc, ccnt, qs, scnt, rec);
+    else
+        k_q_trace<R, 128, kFmt><<<trace_grid_of<R, 128, kFmt>() * m, 128, 0, st>>>(s, qc, ccnt, qs, scnt, rec);
+}
+
 // one traversal launch over a closest-hit and a shadow queue: `block`
-// threads (64, 128 or 256) and `mult` x the blocks resident at once
+// threads (64, 128 or 256) and `mult` x the blocks resident at once, the
+// kernel instance of the scene tree's node format
 template <class R>
 void launch_trace(uint32_t block, uint32_t mult, cudaStream_t st, const SceneView& s, const uint32_t* qc,
                   const uint32_t* ccnt, const uint32_t* qs, const uint32_t* scnt, R* rec) {
     const uint32_t m = std::max(mult, 1u);
-    if (block == 64)
-        k_q_trace<R, 64><<<trace_grid_of<R, 64>() * m, 64, 0, st>>>(s, qc, ccnt, qs, scnt, rec);
-    else if (block == 256)
-        k_q_trace<R, 256><<<trace_grid_of<R, 256>() * m, 256, 0, st>>>(s, qc, ccnt, qs, scnt, rec);
-    else
-        k_q_trace<R, 128><<<trace_grid_of<R, 128>() * m, 128, 0, st>>>(s, qc, ccnt, qs, scnt, rec);
+    if (s.qnodes) launch_trace_fmt<R, kFmtCompressed8>(block, m, st, s, qc, ccnt, qs, scnt, rec);
+    else launch_trace_fmt<R, kFmtWide4>(block, m, st, s, qc, ccnt, qs, scnt, rec);
 }
 
 }  // namespace

@@ -38,7 +38,8 @@ struct BvhNode {
 };
 
 struct SceneView {
-    const Bvh4Node* nodes;  // 4-wide scene BVH, root at 0
+    const Bvh4Node* nodes;  // 4-wide scene BVH, root at 0 (when qnodes is null)
+    const Bvh8QNode* qnodes = nullptr;  // compressed 8-wide scene BVH, root at 0, or null
     const float4* tris;   // 3 per triangle in leaf order; tris[3i+2].w = triangle index bits
     const float4* shade;  // 5 per triangle in scene order: p0 p1 p2 n0 n1 n2 material
     const crisb_material* mats;
@@ -407,9 +408,156 @@ RT_D void count_trav(const SceneView& s, uint32_t visits, uint32_t tris) {
     }
 }
 
-// Closest hit (any_hit == false) or first hit (any_hit == true) over the BVH.
+// ---- compressed 8-wide tree ------------------------------------------------------
+constexpr int kQStack = 32;
+
+// one leaf triangle of the compressed tree; true when an any-hit query is
+// answered
 template <bool kAnyHit>
-RT_D TraceResult traverse(const SceneView& s, const RayPre& r, float tmin, float tmax) {
+RT_D bool q_triangle(const SceneView& s, const RayPre& r, uint32_t slot, float tmin, float tmax, TraceResult& best) {
+    const float4 q0 = __ldg(&s.tris[3 * slot + 0]);
+    const float4 q1 = __ldg(&s.tris[3 * slot + 1]);
+    const float4 q2 = __ldg(&s.tris[3 * slot + 2]);
+    const uint32_t prim = __float_as_uint(q2.w);
+    float t, u, v;
+    if (!intersect_tri(r, V3{q0.x, q0.y, q0.z}, V3{q1.x, q1.y, q1.z}, V3{q2.x, q2.y, q2.z}, tmin, tmax, t, u, v))
+        return false;
+    if (kAnyHit) {
+        best.prim = prim;
+        best.t = t;
+        return true;
+    }
+    if (best.prim == CRISB_INVALID_PRIM || t < best.t || (t == best.t && prim < best.prim)) {
+        best.prim = prim;
+        best.t = t;
+        best.u = u;
+        best.v = v;
+    }
+    return false;
+}
+
+// 2^e for a grid exponent e in [-126, 127]
+RT_D float exp2_int(int e) { return __int_as_float((e + 127) << 23); }
+
+// Closest or first hit over the compressed tree (Bvh8QNode).  A child plane
+// at grid step q is met at t = q * (2^e * inv) + (p - o) * inv, one FMA per
+// plane on two per-node terms per axis; against the subtract-and-multiply
+// form on the decoded plane this adds roundings of |p - o| and |X - o| size,
+// far inside the box margin, so the test stays conservative and the hits are
+// those of testing every triangle (the tree only changes the speed).  Hit
+// children go into one mask: inner children at bit 24 + (slot ^ octant), leaf
+// triangles at their bits 0-23.  Inner children are taken lowest bit first
+// (near to far in the octant order); the rest of a node's hit inner children
+// wait on the stack as one group (child base, bits, inner mask, the least
+// entry t of the group, which culls the group once a closer hit is known).
+template <bool kAnyHit>
+RT_D TraceResult traverse_q(const SceneView& s, const RayPre& r, float tmin, float tmax) {
+    TraceResult best{CRISB_INVALID_PRIM, tmax, 0.0f, 0.0f};
+    if (s.num_tris == 0) return best;
+    const uint32_t ox = signbit(r.inv.x) ? 1u : 0u, oy = signbit(r.inv.y) ? 1u : 0u, oz = signbit(r.inv.z) ? 1u : 0u;
+    const uint32_t oct = ox | (oy << 1) | (oz << 2);
+    uint4 stk[kQStack];
+    int sp = 0;
+    uint32_t node = 0, visits = 0, ntris = 0;
+    for (;;) {
+        if (++visits > kMaxNodeVisits) {
+            dev_error(s, kDevErrIterations);
+            break;
+        }
+        const float4* np = reinterpret_cast<const float4*>(s.qnodes + node);
+        const float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
+        const uint32_t ew = __float_as_uint(n0.w);
+        const float sx = exp2_int(static_cast<int>(static_cast<int8_t>(ew & 0xffu))) * r.inv.x;
+        const float sy = exp2_int(static_cast<int>(static_cast<int8_t>((ew >> 8) & 0xffu))) * r.inv.y;
+        const float sz = exp2_int(static_cast<int>(static_cast<int8_t>((ew >> 16) & 0xffu))) * r.inv.z;
+        const float bx = (n0.x - r.org.x) * r.inv.x;
+        const float by = (n0.y - r.org.y) * r.inv.y;
+        const float bz = (n0.z - r.org.z) * r.inv.z;
+        const float bnd = best.t;
+        uint32_t hits = 0;
+        float gmin = INFINITY;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint32_t meta = __float_as_uint(h ? n1.w : n1.z);
+            const uint32_t lx = __float_as_uint(h ? n2.y : n2.x), hx = __float_as_uint(h ? n3.w : n3.z);
+            const uint32_t ly = __float_as_uint(h ? n2.w : n2.z), hy = __float_as_uint(h ? n4.y : n4.x);
+            const uint32_t lz = __float_as_uint(h ? n3.y : n3.x), hz = __float_as_uint(h ? n4.w : n4.z);
+            const uint32_t nx = ox ? hx : lx, fx = ox ? lx : hx;
+            const uint32_t ny = oy ? hy : ly, fy = oy ? ly : hy;
+            const uint32_t nz = oz ? hz : lz, fz = oz ? lz : hz;
+            // per byte: inner children have meta bits 4 and 3 set
+            const uint32_t inner4 = (meta & (meta << 1)) & 0x10101010u;
+            const uint32_t bit4 = (meta ^ ((inner4 >> 4) * oct)) & 0x1f1f1f1fu;
+            const uint32_t cnt4 = (meta >> 5) & 0x07070707u;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                // byte j as the float 2^23 + q, minus 2^23 (exact)
+                const uint32_t sel = 0x7440u + static_cast<uint32_t>(j);
+                const float qnx = __uint_as_float(__byte_perm(nx, 0x4B000000u, sel)) - 8388608.0f;
+                const float qfx = __uint_as_float(__byte_perm(fx, 0x4B000000u, sel)) - 8388608.0f;
+                const float qny = __uint_as_float(__byte_perm(ny, 0x4B000000u, sel)) - 8388608.0f;
+                const float qfy = __uint_as_float(__byte_perm(fy, 0x4B000000u, sel)) - 8388608.0f;
+                const float qnz = __uint_as_float(__byte_perm(nz, 0x4B000000u, sel)) - 8388608.0f;
+                const float qfz = __uint_as_float(__byte_perm(fz, 0x4B000000u, sel)) - 8388608.0f;
+                const float tn = fmaxf(fmaxf(fmaf(qnx, sx, bx), fmaf(qny, sy, by)), fmaxf(fmaf(qnz, sz, bz), tmin));
+                const float tf = fminf(fminf(fmaf(qfx, sx, bx), fmaf(qfy, sy, by)), fminf(fmaf(qfz, sz, bz), bnd));
+                if (tn <= tf * kSlabFarScale) {
+                    const uint32_t sh = 8u * static_cast<uint32_t>(j);
+                    hits |= ((cnt4 >> sh) & 7u) << ((bit4 >> sh) & 31u);
+                    if ((inner4 >> (sh + 4u)) & 1u) gmin = fminf(gmin, tn);
+                }
+            }
+        }
+        // the node's leaf triangles
+        const uint32_t tbase = __float_as_uint(n1.y);
+        uint32_t tmask = hits & 0x00ffffffu;
+        bool answered = false;
+        while (tmask) {
+            const uint32_t k = static_cast<uint32_t>(__ffs(tmask) - 1);
+            tmask &= tmask - 1u;
+            ++ntris;
+            if (q_triangle<kAnyHit>(s, r, tbase + k, tmin, tmax, best)) {
+                answered = true;
+                break;
+            }
+        }
+        if (answered) break;
+        // next node: this node's nearest inner child, else a group from the stack
+        uint32_t gbase = __float_as_uint(n1.x), gbits = hits >> 24, gim = ew >> 24;
+        float gt = gmin;
+        if (!kAnyHit && gt > best.t * kSlabFarScale) gbits = 0;
+        if (gbits == 0) {
+            while (sp > 0) {
+                const uint4 e = stk[--sp];
+                if (kAnyHit || __uint_as_float(e.z) <= best.t * kSlabFarScale) {
+                    gbase = e.x;
+                    gbits = e.y & 0xffu;
+                    gim = e.y >> 8;
+                    gt = __uint_as_float(e.z);
+                    break;
+                }
+            }
+            if (gbits == 0) break;
+        }
+        const uint32_t b = static_cast<uint32_t>(__ffs(gbits) - 1);
+        gbits &= gbits - 1u;
+        const uint32_t slot = b ^ oct;
+        node = gbase + static_cast<uint32_t>(__popc(gim & ((1u << slot) - 1u)));
+        if (gbits) {
+            if (sp >= kQStack) {
+                dev_error(s, kDevErrStack);
+                break;
+            }
+            stk[sp++] = make_uint4(gbase, gbits | (gim << 8), __float_as_uint(gt), 0u);
+        }
+    }
+    count_trav(s, visits, ntris);
+    return best;
+}
+
+// closest or first hit over the 4-wide tree
+template <bool kAnyHit>
+RT_D TraceResult traverse_wide4(const SceneView& s, const RayPre& r, float tmin, float tmax) {
     Trav<kAnyHit> t;
     TravStack st;
     t.init(r, tmin, tmax);
@@ -417,6 +565,26 @@ RT_D TraceResult traverse(const SceneView& s, const RayPre& r, float tmin, float
     }
     count_trav(s, t.visits, t.tris);
     return t.best;
+}
+
+// node formats of the scene tree
+constexpr int kFmtWide4 = 0;
+constexpr int kFmtCompressed8 = 1;
+
+// traversal for a format fixed at compile time (the queue traversal kernel
+// is instantiated per format, so it carries only one traversal)
+template <int kFmt, bool kAnyHit>
+RT_D TraceResult traverse_fmt(const SceneView& s, const RayPre& r, float tmin, float tmax) {
+    if (kFmt == kFmtCompressed8) return traverse_q<kAnyHit>(s, r, tmin, tmax);
+    return traverse_wide4<kAnyHit>(s, r, tmin, tmax);
+}
+
+// Closest hit (any_hit == false) or first hit (any_hit == true) over the
+// scene tree, whichever format it has.
+template <bool kAnyHit>
+RT_D TraceResult traverse(const SceneView& s, const RayPre& r, float tmin, float tmax) {
+    if (s.qnodes) return traverse_q<kAnyHit>(s, r, tmin, tmax);
+    return traverse_wide4<kAnyHit>(s, r, tmin, tmax);
 }
 
 // ---- interactions -------------------------------------------------------------

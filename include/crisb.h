@@ -138,15 +138,21 @@ typedef struct crisb_scene_desc {
     const int32_t* material_textures; /* num_materials * 3: diffuse, specular,
                                          roughness texture index or -1 */
     /* Builder of the scene BVH (the OptiX GAS/IAS build of src/Scene.cpp:73-160
-     * and src/Mesh.cpp:54-120): CRISB_BVH_DEVICE (0) or CRISB_BVH_HOST.  Any
-     * builder gives the same hits; only traversal speed differs. */
+     * and src/Mesh.cpp:54-120): CRISB_BVH_DEVICE (0), CRISB_BVH_HOST or
+     * CRISB_BVH_DEVICE_WIDE4.  Any builder gives the same hits; only
+     * traversal speed differs. */
     uint32_t bvh_builder;
 } crisb_scene_desc;
 
 /* crisb_scene_desc.bvh_builder */
 #define CRISB_BVH_DEVICE 0 /* on the GPU: Morton order, PLOC clustering, SAH
-                              collapse into 4-wide nodes */
+                              collapse into compressed 8-wide nodes (8-bit child
+                              boxes on a per-node grid, 80 bytes); scenes with
+                              coordinates of 1.6e7 or more, or a tree deeper than
+                              the traversal stack, get CRISB_BVH_DEVICE_WIDE4 */
 #define CRISB_BVH_HOST 1   /* on the host: binned SAH, collapsed into 4-wide nodes */
+#define CRISB_BVH_DEVICE_WIDE4 2 /* on the GPU as CRISB_BVH_DEVICE, collapsed into
+                              4-wide nodes (128 bytes) */
 
 /* ---- camera (Camera, include/graph/Camera.h:24-79) --------------------- */
 typedef struct crisb_camera {
@@ -402,6 +408,19 @@ int crisb_scene_destroy(crisb_scene* scene);
 int crisb_scene_size(const crisb_scene* scene, float* out);
 /* number of world-space triangles after flattening */
 int crisb_scene_num_triangles(const crisb_scene* scene, uint32_t* out);
+
+/* The scene BVH as built (a compressed build can fall back to 4-wide nodes). */
+typedef struct crisb_bvh_info {
+    uint32_t format;     /* CRISB_BVH_FORMAT_* */
+    uint32_t on_device;  /* 1: built on the GPU */
+    uint32_t num_nodes;
+    uint32_t node_bytes; /* 128 (4-wide) or 80 (compressed 8-wide) */
+    int32_t stack_bound; /* traversal stack entries the tree needs */
+    int32_t depth;       /* collapse levels (device) or binary depth (host) */
+} crisb_bvh_info;
+#define CRISB_BVH_FORMAT_WIDE4 0
+#define CRISB_BVH_FORMAT_COMPRESSED8 1
+int crisb_scene_bvh_info(const crisb_scene* scene, crisb_bvh_info* out);
 /* read back flattened world-space positions (ntri*9), normals (ntri*9) and
  * materials (ntri) in original triangle order; any pointer may be NULL. */
 int crisb_scene_read_triangles(const crisb_scene* scene, float* positions,

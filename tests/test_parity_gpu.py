@@ -30,10 +30,26 @@ def gpu_trace(scene: Scene, rays: np.ndarray, any_hit: bool) -> np.ndarray:
     return h.cpu().numpy().view(_abi.TRACE_HIT_DTYPE).reshape(-1)
 
 
+BUILDERS = [_abi.BVH_DEVICE, _abi.BVH_DEVICE_WIDE4]
+
+
+def make_scene(desc, builder):
+    """Scene built by `builder`; the default build of these scenes must give
+    compressed nodes, the others 4-wide ones."""
+    sc = Scene(desc, builder=builder)
+    info = sc.bvh_info()
+    if builder == _abi.BVH_DEVICE:
+        assert info["format"] == _abi.BVH_FORMAT_COMPRESSED8 and info["node_bytes"] == 80, info
+    else:
+        assert info["format"] == _abi.BVH_FORMAT_WIDE4 and info["node_bytes"] == 128, info
+    return sc
+
+
+@pytest.mark.parametrize("builder", BUILDERS)
 @pytest.mark.parametrize("which", ["cornell", "spheres"])
-def test_traversal_hits_bit_exact(cuda_device, which):
+def test_traversal_hits_bit_exact(cuda_device, which, builder):
     desc = scenes.cornell_box()[0] if which == "cornell" else small_sphere_room()[0]
-    sc = Scene(desc)
+    sc = make_scene(desc, builder)
     tri = sc.read_triangles()
     o = op.Oracle.from_scene(desc, 4, 4, make_params(sc.scene_size), triangles=tri)
     rays = random_rays(desc, 1 << 15, seed=3)
@@ -55,7 +71,7 @@ def test_flattened_instances_match_float64_reference(cuda_device):
 
 def run_parity(desc, cam, params, W, H, frames, cam_fn, change_params=None, timing=0, graph=lambda f: True,
                motion=None, jobs_per_pixel=None, builder=_abi.BVH_DEVICE):
-    sc = Scene(desc, builder=builder)
+    sc = make_scene(desc, builder)
     tri = sc.read_triangles()
     o = op.Oracle.from_scene(desc, W, H, params, triangles=tri)
     r = Renderer(W, H, sc, params)
@@ -163,10 +179,36 @@ def test_shift_jobs_beyond_capacity_give_the_same_results(cuda_device, jobs_per_
     run_parity(desc, cam, p, 48, 40, 3, lambda c, f: orbit(c, f, 120), jobs_per_pixel=jobs_per_pixel)
 
 
-def test_host_built_tree_gives_the_same_frames(cuda_device):
+@pytest.mark.parametrize("builder", [_abi.BVH_HOST, _abi.BVH_DEVICE_WIDE4])
+def test_other_trees_give_the_same_frames(cuda_device, builder):
     desc, cam = small_sphere_room()
     p = large_config_params(scene_size_of(desc), gather_radius=0.3)
-    run_parity(desc, cam, p, 48, 40, 2, lambda c, f: orbit(c, f, 120), builder=_abi.BVH_HOST)
+    run_parity(desc, cam, p, 48, 40, 2, lambda c, f: orbit(c, f, 120), builder=builder)
+
+
+def test_compressed_tree_layout(cuda_device):
+    """The compressed build makes 80-byte nodes, fewer of them than the
+    4-wide build of the same scene."""
+    desc, _ = small_sphere_room()
+    wide = make_scene(desc, _abi.BVH_DEVICE_WIDE4).bvh_info()
+    comp = make_scene(desc, _abi.BVH_DEVICE).bvh_info()
+    assert comp["on_device"] == 1 and wide["on_device"] == 1 and comp["num_nodes"] < wide["num_nodes"]
+    assert 1 <= comp["stack_bound"] <= 32
+
+
+def test_large_coordinates_fall_back_to_four_wide_nodes(cuda_device):
+    """Coordinates of 1.6e7 and more get 4-wide nodes from the default
+    builder, with the same hits as the oracle."""
+    desc = scenes.cornell_box()[0]
+    desc.positions = (np.asarray(desc.positions, np.float64) * 1e6 + 5e7).astype(np.float32)
+    desc.emitter_faces = (np.asarray(desc.emitter_faces, np.float64) * 1e6 + 5e7).astype(np.float32)
+    sc = Scene(desc)
+    assert sc.bvh_info()["format"] == _abi.BVH_FORMAT_WIDE4
+    o = op.Oracle.from_scene(desc, 4, 4, make_params(sc.scene_size), triangles=sc.read_triangles())
+    rays = random_rays(desc, 1 << 14, seed=5)
+    g, c = gpu_trace(sc, rays, False), o.trace(rays)
+    assert (g["prim"] != _abi.INVALID_PRIM).mean() > 0.5
+    assert first_mismatch(g, c) is None, first_mismatch(g, c)
 
 
 @pytest.mark.parametrize("gather_n,gather_m,storage", [(2, 9, _abi.STORAGE_FP32), (3, 5, _abi.STORAGE_FP16),

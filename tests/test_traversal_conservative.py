@@ -31,13 +31,15 @@ def test_oracle_tree_equals_brute_force_on_grazing_rays(which):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("builder", [0, 2])
 @pytest.mark.parametrize("which", list(SCENES))
-def test_library_tree_equals_brute_force_on_grazing_rays(cuda_device, which):
-    from crisoptix_b200 import Scene
-    from test_parity_gpu import gpu_trace
+def test_library_tree_equals_brute_force_on_grazing_rays(cuda_device, which, builder):
+    """Both device trees: compressed 8-wide nodes, whose boxes are quantised
+    outward (builder 0), and 4-wide nodes (builder 2)."""
+    from test_parity_gpu import gpu_trace, make_scene
 
     desc = SCENES[which]()
-    sc = Scene(desc)
+    sc = make_scene(desc, builder)
     o = op.Oracle.from_scene(desc, 4, 4, make_params(sc.scene_size), triangles=sc.read_triangles())
     rays = surface_rays(desc, 1 << 20, seed=22)
     for any_hit in (True, False):
