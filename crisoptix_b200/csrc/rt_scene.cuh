@@ -439,6 +439,35 @@ RT_D bool q_triangle(const SceneView& s, const RayPre& r, uint32_t slot, float t
 // 2^e for a grid exponent e in [-126, 127]
 RT_D float exp2_int(int e) { return __int_as_float((e + 127) << 23); }
 
+// packed pairs of floats (sm_100 f32x2 arithmetic: two IEEE round-to-nearest
+// operations per instruction) and three-input min / max
+RT_D uint64_t pk2(float lo, float hi) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+RT_D void upk2(uint64_t v, float& lo, float& hi) { asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v)); }
+RT_D uint64_t add2(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+RT_D uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+RT_D float max3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+RT_D float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // Closest or first hit over the compressed tree (Bvh8QNode).  A child plane
 // at grid step q is met at t = q * (2^e * inv) + (p - o) * inv, one FMA per
 // plane on two per-node terms per axis; against the subtract-and-multiply
@@ -473,6 +502,10 @@ RT_D TraceResult traverse_q(const SceneView& s, const RayPre& r, float tmin, flo
         const float bx = (n0.x - r.org.x) * r.inv.x;
         const float by = (n0.y - r.org.y) * r.inv.y;
         const float bz = (n0.z - r.org.z) * r.inv.z;
+        // per axis (near, far) pairs share the scale and the offset
+        const uint64_t sx2 = pk2(sx, sx), sy2 = pk2(sy, sy), sz2 = pk2(sz, sz);
+        const uint64_t bx2 = pk2(bx, bx), by2 = pk2(by, by), bz2 = pk2(bz, bz);
+        const uint64_t m23 = pk2(-8388608.0f, -8388608.0f);
         const float bnd = best.t;
         uint32_t hits = 0;
         float gmin = INFINITY;
@@ -491,16 +524,21 @@ RT_D TraceResult traverse_q(const SceneView& s, const RayPre& r, float tmin, flo
             const uint32_t cnt4 = (meta >> 5) & 0x07070707u;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                // byte j as the float 2^23 + q, minus 2^23 (exact)
+                // byte j of the near and far words as the floats 2^23 + q,
+                // minus 2^23 (exact), then t = q * s + b per plane
                 const uint32_t sel = 0x7440u + static_cast<uint32_t>(j);
-                const float qnx = __uint_as_float(__byte_perm(nx, 0x4B000000u, sel)) - 8388608.0f;
-                const float qfx = __uint_as_float(__byte_perm(fx, 0x4B000000u, sel)) - 8388608.0f;
-                const float qny = __uint_as_float(__byte_perm(ny, 0x4B000000u, sel)) - 8388608.0f;
-                const float qfy = __uint_as_float(__byte_perm(fy, 0x4B000000u, sel)) - 8388608.0f;
-                const float qnz = __uint_as_float(__byte_perm(nz, 0x4B000000u, sel)) - 8388608.0f;
-                const float qfz = __uint_as_float(__byte_perm(fz, 0x4B000000u, sel)) - 8388608.0f;
-                const float tn = fmaxf(fmaxf(fmaf(qnx, sx, bx), fmaf(qny, sy, by)), fmaxf(fmaf(qnz, sz, bz), tmin));
-                const float tf = fminf(fminf(fmaf(qfx, sx, bx), fmaf(qfy, sy, by)), fminf(fmaf(qfz, sz, bz), bnd));
+                const uint64_t qx = add2(pk2(__uint_as_float(__byte_perm(nx, 0x4B000000u, sel)),
+                                             __uint_as_float(__byte_perm(fx, 0x4B000000u, sel))), m23);
+                const uint64_t qy = add2(pk2(__uint_as_float(__byte_perm(ny, 0x4B000000u, sel)),
+                                             __uint_as_float(__byte_perm(fy, 0x4B000000u, sel))), m23);
+                const uint64_t qz = add2(pk2(__uint_as_float(__byte_perm(nz, 0x4B000000u, sel)),
+                                             __uint_as_float(__byte_perm(fz, 0x4B000000u, sel))), m23);
+                float tnx, tfx, tny, tfy, tnz, tfz;
+                upk2(fma2(qx, sx2, bx2), tnx, tfx);
+                upk2(fma2(qy, sy2, by2), tny, tfy);
+                upk2(fma2(qz, sz2, bz2), tnz, tfz);
+                const float tn = max3f(tnx, tny, fmaxf(tnz, tmin));
+                const float tf = min3f(tfx, tfy, fminf(tfz, bnd));
                 if (tn <= tf * kSlabFarScale) {
                     const uint32_t sh = 8u * static_cast<uint32_t>(j);
                     hits |= ((cnt4 >> sh) & 7u) << ((bit4 >> sh) & 31u);
