@@ -1,4 +1,4 @@
-// bvh_build.h -- host builder of the scene's 4-wide BVH.
+// bvh_build.h -- node formats of the scene BVH and its host builder and validators.
 //
 // Stands in for the OptiX GAS/IAS build of the reference
 // (src/Scene.cpp:73-160, src/Mesh.cpp:54-120): a binned-SAH binary

@@ -1,4 +1,4 @@
-// bvh_device.h -- the scene's 4-wide BVH built on the device.
+// bvh_device.h -- the scene BVH built on the device (compressed 8-wide or 4-wide nodes).
 //
 // Stands in for the OptiX GAS/IAS build of the reference (src/Scene.cpp:73-160,
 // src/Mesh.cpp:54-120) on the GPU:
@@ -19,8 +19,9 @@
 //      order; child boxes are widened by box_margin().  Or the same collapse
 //      to eight children into compressed nodes (Bvh8QNode): children placed
 //      in octant slots, boxes quantised outward on the node's grid.
-// The tree lands in the same node and triangle layouts the host builder
-// (bvh_build.h) produces, so traversal is shared.
+// The 4-wide tree lands in the same node and triangle layouts the host
+// builder (bvh_build.h) produces, so its traversal is shared; the compressed
+// tree keeps the same leaf-ordered triangle layout.
 #pragma once
 
 #include <cuda_runtime.h>

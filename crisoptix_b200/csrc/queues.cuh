@@ -58,16 +58,18 @@ RT_D void shadow_ray(const ShiftJob& j, V3& o, V3& d, float& tmax) {
 }
 RT_D void set_occluded(ShiftJob& j, uint32_t v) { j.hit.x = __uint_as_float(v); }
 
-// Grid-stride loops over the queue.  A warp-synchronous variant with dynamic
-// ray fetching (refill idle lanes from per-warp batches) measured slower on
-// the 1080p workload (31 ms against 20 ms of trace per frame) at every refill
-// threshold: the per-step convergence removes the latency hiding between the
-// diverged inner-node and leaf lanes.
+// Grid-stride loops over the queue, each lane walking its ray to the end.
+// Warps lose most of their lanes to that (a warp runs 2.4x the node visits
+// its rays need on the 1080p workload), but refilling finished lanes measured
+// slower every time: with 4-wide nodes (per-warp batches, 31 ms against 20 ms
+// of trace per frame: the per-step convergence removes the latency hiding
+// between diverged inner-node and leaf lanes) and with compressed nodes
+// (per-warp chunks of the queue, every idle lane refilled at once when at most
+// 8-31 lanes are busy: 19.1-19.8 against 12.1 ms: lanes on different rays and
+// depths no longer load the same nodes in the same instruction).
 // One launch per round over both queues: entries [0, nc) of the closest-hit
 // queue, then [nc, nc + ns) of the shadow queue, so the two queues' tails
 // (the last, slowest rays) overlap instead of running back to back.
-// 9 resident blocks per SM (56 registers): 13.40 -> 13.25 ms of traversal per
-// 1080p frame against 8 blocks (64 registers), despite a few more spills
 // Block sizes of the traversal kernel (crisb_set_trace_block, tuned by
 // crisb_autotune): resident blocks per SM chosen so every size keeps the
 // register budget of 9 x 128 threads (56 registers; 64 at 256 threads).

@@ -411,31 +411,6 @@ RT_D void count_trav(const SceneView& s, uint32_t visits, uint32_t tris) {
 // ---- compressed 8-wide tree ------------------------------------------------------
 constexpr int kQStack = 32;
 
-// one leaf triangle of the compressed tree; true when an any-hit query is
-// answered
-template <bool kAnyHit>
-RT_D bool q_triangle(const SceneView& s, const RayPre& r, uint32_t slot, float tmin, float tmax, TraceResult& best) {
-    const float4 q0 = __ldg(&s.tris[3 * slot + 0]);
-    const float4 q1 = __ldg(&s.tris[3 * slot + 1]);
-    const float4 q2 = __ldg(&s.tris[3 * slot + 2]);
-    const uint32_t prim = __float_as_uint(q2.w);
-    float t, u, v;
-    if (!intersect_tri(r, V3{q0.x, q0.y, q0.z}, V3{q1.x, q1.y, q1.z}, V3{q2.x, q2.y, q2.z}, tmin, tmax, t, u, v))
-        return false;
-    if (kAnyHit) {
-        best.prim = prim;
-        best.t = t;
-        return true;
-    }
-    if (best.prim == CRISB_INVALID_PRIM || t < best.t || (t == best.t && prim < best.prim)) {
-        best.prim = prim;
-        best.t = t;
-        best.u = u;
-        best.v = v;
-    }
-    return false;
-}
-
 // 2^e for a grid exponent e in [-126, 127]
 RT_D float exp2_int(int e) { return __int_as_float((e + 127) << 23); }
 
@@ -479,20 +454,40 @@ RT_D float min3f(float a, float b, float c) {
 // (near to far in the octant order); the rest of a node's hit inner children
 // wait on the stack as one group (child base, bits, inner mask, the least
 // entry t of the group, which culls the group once a closer hit is known).
-template <bool kAnyHit>
-RT_D TraceResult traverse_q(const SceneView& s, const RayPre& r, float tmin, float tmax) {
-    TraceResult best{CRISB_INVALID_PRIM, tmax, 0.0f, 0.0f};
-    if (s.num_tris == 0) return best;
-    const uint32_t ox = signbit(r.inv.x) ? 1u : 0u, oy = signbit(r.inv.y) ? 1u : 0u, oz = signbit(r.inv.z) ? 1u : 0u;
-    const uint32_t oct = ox | (oy << 1) | (oz << 2);
-    uint4 stk[kQStack];
-    int sp = 0;
-    uint32_t node = 0, visits = 0, ntris = 0;
-    for (;;) {
+// Traversal state of one ray over the compressed tree; step() visits one
+// node (its eight child boxes, then the triangles of its hit leaf children)
+// and picks the next, reporting when the ray is finished.  `any`: first hit
+// (occlusion) instead of the closest.  The group stack is kept apart so the
+// scalar state stays in registers.
+struct QTrav {
+    RayPre r;
+    float tmin, tmax0;
+    TraceResult best;
+    uint32_t node, visits, ntris;
+    int sp;
+    uint32_t oct;
+    bool any;
+
+    RT_D void init(const RayPre& ray, float t0, float t1, bool any_hit) {
+        r = ray;
+        tmin = t0;
+        tmax0 = t1;
+        best = TraceResult{CRISB_INVALID_PRIM, t1, 0.0f, 0.0f};
+        node = 0;
+        visits = 0;
+        ntris = 0;
+        sp = 0;
+        oct = (signbit(r.inv.x) ? 1u : 0u) | (signbit(r.inv.y) ? 2u : 0u) | (signbit(r.inv.z) ? 4u : 0u);
+        any = any_hit;
+    }
+
+    RT_D bool step(const SceneView& s, uint4* stk) {
+        if (s.num_tris == 0) return true;
         if (++visits > kMaxNodeVisits) {
             dev_error(s, kDevErrIterations);
-            break;
+            return true;
         }
+        const uint32_t ox = oct & 1u, oy = (oct >> 1) & 1u, oz = oct >> 2;
         const float4* np = reinterpret_cast<const float4*>(s.qnodes + node);
         const float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
         const uint32_t ew = __float_as_uint(n0.w);
@@ -549,25 +544,20 @@ RT_D TraceResult traverse_q(const SceneView& s, const RayPre& r, float tmin, flo
         // the node's leaf triangles
         const uint32_t tbase = __float_as_uint(n1.y);
         uint32_t tmask = hits & 0x00ffffffu;
-        bool answered = false;
         while (tmask) {
             const uint32_t k = static_cast<uint32_t>(__ffs(tmask) - 1);
             tmask &= tmask - 1u;
             ++ntris;
-            if (q_triangle<kAnyHit>(s, r, tbase + k, tmin, tmax, best)) {
-                answered = true;
-                break;
-            }
+            if (triangle(s, tbase + k)) return true;
         }
-        if (answered) break;
         // next node: this node's nearest inner child, else a group from the stack
         uint32_t gbase = __float_as_uint(n1.x), gbits = hits >> 24, gim = ew >> 24;
         float gt = gmin;
-        if (!kAnyHit && gt > best.t * kSlabFarScale) gbits = 0;
+        if (!any && gt > best.t * kSlabFarScale) gbits = 0;
         if (gbits == 0) {
             while (sp > 0) {
                 const uint4 e = stk[--sp];
-                if (kAnyHit || __uint_as_float(e.z) <= best.t * kSlabFarScale) {
+                if (any || __uint_as_float(e.z) <= best.t * kSlabFarScale) {
                     gbase = e.x;
                     gbits = e.y & 0xffu;
                     gim = e.y >> 8;
@@ -575,7 +565,7 @@ RT_D TraceResult traverse_q(const SceneView& s, const RayPre& r, float tmin, flo
                     break;
                 }
             }
-            if (gbits == 0) break;
+            if (gbits == 0) return true;
         }
         const uint32_t b = static_cast<uint32_t>(__ffs(gbits) - 1);
         gbits &= gbits - 1u;
@@ -584,13 +574,47 @@ RT_D TraceResult traverse_q(const SceneView& s, const RayPre& r, float tmin, flo
         if (gbits) {
             if (sp >= kQStack) {
                 dev_error(s, kDevErrStack);
-                break;
+                return true;
             }
             stk[sp++] = make_uint4(gbase, gbits | (gim << 8), __float_as_uint(gt), 0u);
         }
+        return false;
     }
-    count_trav(s, visits, ntris);
-    return best;
+
+    // one leaf triangle; true when a first-hit query is answered
+    RT_D bool triangle(const SceneView& s, uint32_t slot) {
+        const float4 q0 = __ldg(&s.tris[3 * slot + 0]);
+        const float4 q1 = __ldg(&s.tris[3 * slot + 1]);
+        const float4 q2 = __ldg(&s.tris[3 * slot + 2]);
+        const uint32_t prim = __float_as_uint(q2.w);
+        float t, u, v;
+        if (!intersect_tri(r, V3{q0.x, q0.y, q0.z}, V3{q1.x, q1.y, q1.z}, V3{q2.x, q2.y, q2.z}, tmin, tmax0, t,
+                           u, v))
+            return false;
+        if (any) {
+            best.prim = prim;
+            best.t = t;
+            return true;
+        }
+        if (best.prim == CRISB_INVALID_PRIM || t < best.t || (t == best.t && prim < best.prim)) {
+            best.prim = prim;
+            best.t = t;
+            best.u = u;
+            best.v = v;
+        }
+        return false;
+    }
+};
+
+template <bool kAnyHit>
+RT_D TraceResult traverse_q(const SceneView& s, const RayPre& r, float tmin, float tmax) {
+    QTrav t;
+    uint4 stk[kQStack];
+    t.init(r, tmin, tmax, kAnyHit);
+    while (!t.step(s, stk)) {
+    }
+    count_trav(s, t.visits, t.ntris);
+    return t.best;
 }
 
 // closest or first hit over the 4-wide tree
