@@ -274,13 +274,16 @@ def comparison_arms(sc, cam, W: int, H: int, p, ppp: int, value: float, ms_per_f
             r16.launch_frame(cams[i], out.data_ptr(), sptr)
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # the frames of the orbit the main (FP32) loop timed: early frames cost
+    # more than later ones, so both arms average the same stretch
+    arm_steps = args.arm_steps or args.steps
     a.record(stream)
-    for i in range(args.arm_steps):
+    for i in range(arm_steps):
         r16.launch_frame(cams[(args.warmup + i) % 60], out.data_ptr(), sptr)
     b.record(stream)
     torch.cuda.synchronize()
     r16.check_device_errors()
-    ms16 = a.elapsed_time(b) / args.arm_steps
+    ms16 = a.elapsed_time(b) / arm_steps
     del r16
     cam_of = lambda f: scenes.orbit_camera(cam, f, 60)  # noqa: E731
     ref = quality.reference_image(sc, W, H, cam_of(30), p, args.arm_ref_spp)
@@ -292,7 +295,7 @@ def comparison_arms(sc, cam, W: int, H: int, p, ppp: int, value: float, ms_per_f
     return {
         "single_view_fp32": {"value": value, "ms_per_frame": ms_per_frame,
                              "relmse": {k: q32[k] for k in keep}},
-        "single_view_fp16": {"value": ppp * W * H * 1000.0 / ms16, "ms_per_frame": ms16, "steps": args.arm_steps,
+        "single_view_fp16": {"value": ppp * W * H * 1000.0 / ms16, "ms_per_frame": ms16, "steps": arm_steps,
                              "relmse": {k: q16[k] for k in keep}},
         "fp16_over_fp32": ms_per_frame / ms16,
         "relmse_reference": {"kind": "path tracer (TraceCompletePath), FP64 accumulation", "spp": args.arm_ref_spp,
@@ -687,7 +690,8 @@ def main():
     ap.add_argument("--res", default=None, help="WxH override of the workload resolution (profiling runs)")
     ap.add_argument("--no-arms", action="store_true",
                     help="skip the comparison arms (FP16 storage, multiview plain vs batched, relMSE)")
-    ap.add_argument("--arm-steps", type=int, default=10, help="timed frames of the FP16 single-view arm")
+    ap.add_argument("--arm-steps", type=int, default=0,
+                    help="timed frames of the FP16 single-view arm (0: the main loop's --steps, same frames)")
     ap.add_argument("--arm-mv-steps", type=int, default=4, help="timed frames of each multiview arm")
     ap.add_argument("--arm-ref-spp", type=int, default=256,
                     help="samples per pixel of the path-traced relMSE reference of the arms")
