@@ -156,7 +156,7 @@ class Scene:
 
     def bvh_info(self) -> dict:
         """The BVH as built: format (BVH_FORMAT_*), on_device, num_nodes,
-        node_bytes, stack_bound, depth."""
+        node_bytes, stack_bound, depth, inner_children, leaf_children."""
         v = _abi.BvhInfo()
         check(load().crisb_scene_bvh_info(self.handle, ctypes.byref(v)))
         return {k: getattr(v, k) for k, _ in _abi.BvhInfo._fields_}

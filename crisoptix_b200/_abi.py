@@ -84,7 +84,7 @@ class Tuning(ctypes.Structure):
 
 class BvhInfo(ctypes.Structure):
     _fields_ = [("format", c_u32), ("on_device", c_u32), ("num_nodes", c_u32), ("node_bytes", c_u32),
-                ("stack_bound", c_i32), ("depth", c_i32)]
+                ("stack_bound", c_i32), ("depth", c_i32), ("inner_children", c_u32), ("leaf_children", c_u32)]
 
 
 class Texture(ctypes.Structure):

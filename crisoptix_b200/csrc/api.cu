@@ -224,6 +224,7 @@ struct crisb_scene {
     DevBuf<Bvh4Node> nodes;
     DevBuf<Bvh8QNode> qnodes;  // the compressed tree, when built (then `nodes` is empty)
     int bvh_max_stack = 0, bvh_max_depth = 0;
+    uint32_t bvh_inner_children = 0, bvh_leaf_children = 0;
     bool bvh_on_device = false;  // built by build_wide_bvh_device
     DevBuf<float4> tris;
     DevBuf<float4> shade;
@@ -416,6 +417,26 @@ void upload_textures(const crisb_scene_desc& d, crisb_scene& s) {
 // boxes containing their subtrees, the traversal stack bound).  Returns false
 // when the tree would need a deeper traversal stack than the kernels have
 // (the host builder's median fallback then bounds the depth).
+// child slots holding a node / triangles
+void count_children(const std::vector<Bvh8QNode>& nodes, crisb_scene& s) {
+    s.bvh_inner_children = s.bvh_leaf_children = 0;
+    for (const Bvh8QNode& nd : nodes)
+        for (int c = 0; c < 8; ++c) {
+            if (nd.meta[c] == 0) continue;
+            if ((nd.meta[c] & 0x18u) == 0x18u) ++s.bvh_inner_children;
+            else ++s.bvh_leaf_children;
+        }
+}
+void count_children(const std::vector<Bvh4Node>& nodes, crisb_scene& s) {
+    s.bvh_inner_children = s.bvh_leaf_children = 0;
+    for (const Bvh4Node& nd : nodes)
+        for (int c = 0; c < kBvhWidth; ++c) {
+            if (nd.link[c] == kNoChild) continue;
+            if (nd.link[c] >= 0) ++s.bvh_inner_children;
+            else ++s.bvh_leaf_children;
+        }
+}
+
 // the compressed 8-wide tree on the device, validated on the host; false
 // when the scene does not qualify (coordinates too large, tree deeper than
 // the group stack)
@@ -461,6 +482,7 @@ bool build_qbvh_on_device(crisb_scene& s, float max_abs) {
     s.tris.p = db.tris;
     s.tris.n = 3 * static_cast<size_t>(std::max<uint32_t>(n, 1));
     s.bvh_max_stack = depth;
+    count_children(hn, s);
     s.bvh_max_depth = db.binary_depth;
     s.bvh_on_device = true;
     check(cudaDeviceSynchronize(), "scene build");
@@ -509,6 +531,7 @@ bool build_bvh_on_device(crisb_scene& s) {
     s.tris.p = db.tris;
     s.tris.n = 3 * static_cast<size_t>(std::max<uint32_t>(n, 1));
     s.bvh_max_stack = stack;
+    count_children(hb.nodes, s);
     s.bvh_max_depth = db.binary_depth;
     s.bvh_on_device = true;
     check(cudaDeviceSynchronize(), "scene build");
@@ -563,6 +586,7 @@ void build_scene(const crisb_scene_desc& d, crisb_scene& s) {
         throw Error(CRISB_ERR_INVALID_ARGUMENT, std::string("scene build: ") + e.what());
     }
     s.bvh_max_stack = bvh.max_stack;
+    count_children(bvh.nodes, s);
     s.bvh_max_depth = bvh.max_depth;
     s.bvh_on_device = false;
     std::vector<float4> tris(3 * static_cast<size_t>(std::max<uint32_t>(n, 1)), make_float4(0, 0, 0, 0));
@@ -1105,6 +1129,8 @@ int crisb_scene_bvh_info(const crisb_scene* scene, crisb_bvh_info* out) {
         out->node_bytes = q ? static_cast<uint32_t>(sizeof(Bvh8QNode)) : static_cast<uint32_t>(sizeof(Bvh4Node));
         out->stack_bound = scene->bvh_max_stack;
         out->depth = scene->bvh_max_depth;
+        out->inner_children = scene->bvh_inner_children;
+        out->leaf_children = scene->bvh_leaf_children;
     });
 }
 

@@ -16,9 +16,12 @@
 //   4. a top-down collapse into the 4-wide nodes of bvh_build.h, level by
 //      level: a wide node opens its children largest surface area first until
 //      it has four; leaf children store their triangles contiguously in leaf
-//      order; child boxes are widened by box_margin().  Or the same collapse
-//      to eight children into compressed nodes (Bvh8QNode): children placed
-//      in octant slots, boxes quantised outward on the node's grid.
+//      order; child boxes are widened by box_margin().  Or, for compressed
+//      nodes (Bvh8QNode), the SAH-optimal distribution of every subtree over
+//      eight child slots (leaves of up to kQLeafMax triangles; after Ylitie,
+//      Karras & Laine 2017), found bottom-up in PLOC merge order and taken
+//      top-down level by level; children placed in octant slots, boxes
+//      quantised outward on the node's grid.
 // The 4-wide tree lands in the same node and triangle layouts the host
 // builder (bvh_build.h) produces, so its traversal is shared; the compressed
 // tree keeps the same leaf-ordered triangle layout.

@@ -417,6 +417,8 @@ typedef struct crisb_bvh_info {
     uint32_t node_bytes; /* 128 (4-wide) or 80 (compressed 8-wide) */
     int32_t stack_bound; /* traversal stack entries the tree needs */
     int32_t depth;       /* collapse levels (device) or binary depth (host) */
+    uint32_t inner_children; /* child slots holding a node */
+    uint32_t leaf_children;  /* child slots holding triangles */
 } crisb_bvh_info;
 #define CRISB_BVH_FORMAT_WIDE4 0
 #define CRISB_BVH_FORMAT_COMPRESSED8 1

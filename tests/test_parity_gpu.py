@@ -188,12 +188,15 @@ def test_other_trees_give_the_same_frames(cuda_device, builder):
 
 def test_compressed_tree_layout(cuda_device):
     """The compressed build makes 80-byte nodes, fewer of them than the
-    4-wide build of the same scene."""
+    4-wide build of the same scene, and its SAH distribution fills most of
+    their eight child slots."""
     desc, _ = small_sphere_room()
     wide = make_scene(desc, _abi.BVH_DEVICE_WIDE4).bvh_info()
     comp = make_scene(desc, _abi.BVH_DEVICE).bvh_info()
     assert comp["on_device"] == 1 and wide["on_device"] == 1 and comp["num_nodes"] < wide["num_nodes"]
     assert 1 <= comp["stack_bound"] <= 32
+    assert comp["inner_children"] == comp["num_nodes"] - 1
+    assert (comp["inner_children"] + comp["leaf_children"]) / comp["num_nodes"] > 5.0, comp
 
 
 def test_large_coordinates_fall_back_to_four_wide_nodes(cuda_device):
