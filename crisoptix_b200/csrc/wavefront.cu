@@ -270,7 +270,9 @@ RT_D void wf_trace_inline(const SceneView& s, WfPath& w, int req) {
 // Resume every path whose ray of round `cur` finished and queue its next ray;
 // with kInline (the last wavefront round) trace the path's remaining rays in
 // place until it ends, so the few long paths left do not cost a trace and a
-// shade launch per bounce.
+// shade launch per bounce.  One launch over both queues: a separate instance
+// for the shadow-ray results (94 against 126 registers) cost more in launches
+// than it gained in occupancy (shading 3.85 -> 3.98 ms per 1080p frame).
 template <bool kInline>
 __global__ void __launch_bounds__(kPassBlock) k_wf_shade(SceneView s, FrameParams fp, Bufs b, int flow, int cur) {
     const uint32_t nc = b.wf_count[2 * cur], ns = b.wf_count[2 * cur + 1];
