@@ -409,7 +409,13 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_temp_finish(FrameParams f
     push_jobs(b, i, mask);
 }
 
-__global__ void __launch_bounds__(kPassBlock) k_suffix_temp_combine(FrameParams fp, Bufs b) {
+// resampling kernels (selection and combines) at 10 resident 128-thread
+// blocks per SM (48 registers, a few spills): their candidate chains are
+// latency-bound, and more warps in flight beat the spills (0.935 -> 0.902 ms
+// per 1080p frame; 12 and 16 blocks spill more: 0.995 and 1.23 ms)
+constexpr int kResampleMinBlocks = 10;
+
+__global__ void __launch_bounds__(kPassBlock, kResampleMinBlocks) k_suffix_temp_combine(FrameParams fp, Bufs b) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pixel_count(fp)) return;
     ByteTally bt(b, kTallyTemporalCombine);
@@ -483,7 +489,7 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_temp_combine(FrameParams 
 
 // ---- suffix spatial reuse (shader/suffix_spatial_reuse.cu:16-167) -----------------
 // Reads the pass-start state sres_cur (own and neighbours), writes sres_next.
-__global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_select(FrameParams fp, Bufs b) {
+__global__ void __launch_bounds__(kPassBlock, kResampleMinBlocks) k_suffix_spatial_select(FrameParams fp, Bufs b) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     uint64_t mask = 0;
     if (i < pixel_count(fp)) {
@@ -520,7 +526,7 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_select(FrameParam
     push_jobs(b, i, mask);
 }
 
-__global__ void __launch_bounds__(kPassBlock) k_suffix_spatial_combine(FrameParams fp, Bufs b) {
+__global__ void __launch_bounds__(kPassBlock, kResampleMinBlocks) k_suffix_spatial_combine(FrameParams fp, Bufs b) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pixel_count(fp)) return;
     ByteTally bt(b, kTallySpatialCombine);
@@ -678,7 +684,7 @@ __global__ void __launch_bounds__(kPassBlock) k_gather_query(SceneView s, FrameP
     push_jobs(b, i, mask);
 }
 
-__global__ void __launch_bounds__(kPassBlock) k_gather_combine(FrameParams fp, Bufs b, float* out) {
+__global__ void __launch_bounds__(kPassBlock, kResampleMinBlocks) k_gather_combine(FrameParams fp, Bufs b, float* out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pixel_count(fp)) return;
     ByteTally bt(b, kTallyGatherCombine);
@@ -1014,7 +1020,7 @@ __global__ void __launch_bounds__(kPassBlock) k_prefix_finish(SceneView s, Frame
 }
 
 // slot 0: previous prefix shifted onto the canonical one; slot 1: the reverse
-__global__ void __launch_bounds__(kPassBlock) k_prefix_combine(FrameParams fp, Bufs b, float* out) {
+__global__ void __launch_bounds__(kPassBlock, kResampleMinBlocks) k_prefix_combine(FrameParams fp, Bufs b, float* out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pixel_count(fp) || fp.p.renderer_type == CRISB_RENDERER_PATH_TRACER) return;
     ByteTally bt(b, kTallyPrefixCombine);
