@@ -254,7 +254,10 @@ def comparison_arms(sc, cam, W: int, H: int, p, ppp: int, value: float, ms_per_f
         with the relMSE of orbit frame 30 against one FP64-accumulated
         path-traced reference of that frame (`arm_ref_spp` samples per pixel,
         fewer than the 4096 of the full quality run, to stay within the
-        benchmark's time; stated in the line);
+        benchmark's time; stated in the line), beside the plain path tracer
+        at equal time (the samples of frame 30's camera that fit in one FP32
+        ReSTIR frame's time) and the FP32 form with reprojected temporal
+        reuse, scored against the same reference;
       - 16 uneven views: the plain form (FP32 storage, views one after another)
         against the batched form (FP16 storage, one CUDA graph per frame with
         a branch per view), and their ratio of resampled paths/s."""
@@ -289,6 +292,10 @@ def comparison_arms(sc, cam, W: int, H: int, p, ppp: int, value: float, ms_per_f
     ref = quality.reference_image(sc, W, H, cam_of(30), p, args.arm_ref_spp)
     q32 = quality.score(sc, W, H, cam_of, p, 31, args.arm_ref_spp, ref=ref)
     q16 = quality.score(sc, W, H, cam_of, q, 31, args.arm_ref_spp, ref=ref)
+    qpt = quality.pt_equal_time(sc, W, H, cam_of(30), p, ms_per_frame, ref)
+    qrp = copy.copy(p)
+    qrp.motion_mode = _abi.MOTION_REPROJECT
+    q32rp = quality.score(sc, W, H, cam_of, qrp, 31, args.arm_ref_spp, ref=ref)
     mv_plain = multiview_time(_abi.STORAGE_FP32, False, args.arm_mv_steps, 2)
     mv_batch = multiview_time(_abi.STORAGE_FP16, True, args.arm_mv_steps, 2)
     keep = ("relmse", "relmse_trimmed_0.1pct")
@@ -300,6 +307,14 @@ def comparison_arms(sc, cam, W: int, H: int, p, ppp: int, value: float, ms_per_f
         "fp16_over_fp32": ms_per_frame / ms16,
         "relmse_reference": {"kind": "path tracer (TraceCompletePath), FP64 accumulation", "spp": args.arm_ref_spp,
                              "frame": 30},
+        "single_view_fp32_reprojected": {"relmse": {k: q32rp[k] for k in keep},
+                                         "note": "temporal reuse from the primary hit reprojected into the previous "
+                                                 "camera (CRISB_MOTION_REPROJECT) instead of the same pixel"},
+        "plain_pt_equal_time": {"equal_time_spp": qpt["equal_time_spp"], "ms_per_spp": qpt["ms_per_spp"],
+                                "relmse_by_spp": qpt["scores"],
+                                "note": "the path tracer at frame 30's camera, one sample per frame, scored at "
+                                        "the whole sample counts either side of one ReSTIR FP32 frame's time; "
+                                        "its own random stream"},
         "multiview_plain_fp32": dict(mv_plain, steps=args.arm_mv_steps),
         "multiview_batched_fp16": dict(mv_batch, steps=args.arm_mv_steps),
         "batched_fp16_over_plain_fp32": mv_batch["value"] / mv_plain["value"],

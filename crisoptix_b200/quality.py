@@ -87,6 +87,49 @@ def restir_frame(scene, W: int, H: int, cam_of: Callable[[int], Camera], params,
     return out.cpu().numpy().reshape(H, W, 3)
 
 
+def pt_equal_time(scene, W: int, H: int, cam: Camera, params, ms_budget: float, ref: np.ndarray,
+                  seed_offset: int = 7919) -> dict:
+    """The plain path tracer at equal time: one-sample frames of `cam` are
+    timed here, `equal_time_spp` = ms_budget / ms per sample, and the mean of
+    the first floor(equal_time_spp) samples (at least one) and of one sample
+    more are scored against `ref`, so a budget near a whole number of samples
+    shows both sides.  Its random stream differs from the reference's (seed +
+    seed_offset), so the samples are not the reference's own."""
+    import torch
+
+    from . import Renderer
+
+    p = copy.copy(params)
+    p.renderer_type = _abi.PATH_TRACER
+    p.enable_accum = 0
+    p.seed = int(p.seed) + seed_offset
+    r = Renderer(W, H, scene, p)
+    out = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
+    c = copy.copy(cam)
+    c.changed = False
+    for _ in range(3):  # warm-up frames (not part of the image)
+        r.launch_frame(c, out.data_ptr())
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(5):
+        r.launch_frame(c, out.data_ptr())
+    t1.record()
+    torch.cuda.synchronize()
+    ms_spp = t0.elapsed_time(t1) / 5
+    lo = max(1, int(ms_budget // ms_spp))
+    acc = torch.zeros(W * H * 3, dtype=torch.float64, device="cuda")
+    scores = {}
+    for n in range(1, lo + 2):
+        r.launch_frame(c, out.data_ptr())
+        acc += out.double()
+        if n >= lo:
+            img = (acc / n).cpu().numpy().reshape(H, W, 3)
+            scores[str(n)] = {"relmse": relmse(img, ref), "relmse_trimmed_0.1pct": relmse_trimmed(img, ref)}
+    r.check_device_errors()
+    return {"ms_per_spp": ms_spp, "equal_time_spp": ms_budget / ms_spp, "scores": scores}
+
+
 def score(scene, W: int, H: int, cam_of: Callable[[int], Camera], params, frames: int, spp: int,
           ref: Optional[np.ndarray] = None) -> dict:
     """relMSE of frame `frames - 1` against the `spp` path-traced reference of

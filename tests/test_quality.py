@@ -40,3 +40,24 @@ def test_restir_beats_one_sample_path_tracing(cuda_device):
     e_pt = quality.relmse(one, ref)
     assert np.isfinite(s["relmse"])
     assert s["relmse"] < e_pt, (s["relmse"], e_pt)
+
+
+@pytest.mark.gpu
+def test_equal_time_path_tracer_scores(cuda_device):
+    """The equal-time path tracer arm: whole sample counts either side of the
+    budget, each scored, and its samples are not the reference's own (a
+    reference made of them would score exactly zero)."""
+    from crisoptix_b200 import Scene
+
+    desc, cam = scenes.cornell_box()
+    sc = Scene(desc)
+    p = small_config_params(scene_size_of(desc))
+    W = H = 48
+    ref = quality.reference_image(sc, W, H, cam, p, 64)
+    r = quality.pt_equal_time(sc, W, H, cam, p, 0.0, ref)
+    assert r["ms_per_spp"] > 0.0 and r["equal_time_spp"] == 0.0
+    assert sorted(r["scores"]) == ["1", "2"]
+    for v in r["scores"].values():
+        assert np.isfinite(v["relmse"]) and v["relmse"] > 0.0
+    # two samples are closer to the 64-sample reference than one
+    assert r["scores"]["2"]["relmse"] < r["scores"]["1"]["relmse"]
