@@ -135,7 +135,7 @@ RT_D ShiftSrc resolve_job(const FrameParams& fp, const Bufs& b, int mode, uint32
             return shift_src(ld_pres(b.pres[fp.back], pi).s);
         }
         if (dst) *dst = pres_primary(b.pres[fp.back], pi);
-        return shift_src(ld_prefix(b.canon_prefix[i]));
+        return shift_src(ld_prefix_v(b.canon_prefix[i]));
     }
     if (mode == kModeGatherExtra) {
         if (dst) *dst = ld_hit(b.gather_last[i]);
@@ -621,7 +621,7 @@ __global__ void __launch_bounds__(kPassBlock) k_gather_finish(FrameParams fp, Bu
     V3 direct = splat(0.0f);
     if (b.pass_status[i] == kWfPath) {
         b.gbuf[i].rng = b.wf[i].rng;
-        const Prefix cp = ld_prefix(b.gather_cp[i]);
+        const Prefix cp = ld_prefix_v(b.gather_cp[i]);
         if (fl_valid(cp.flags)) {
             if (fl_nee(cp.flags)) {
                 direct = cp.f / cp.p;
@@ -1072,7 +1072,7 @@ __global__ void __launch_bounds__(kPassBlock, kResampleMinBlocks) k_prefix_combi
         cur.s = ld_pres(b.pres[fp.front], i).s;
     } else if (sel == 1) {
         bt.add(sizeof(crisb_prefix_rec));
-        cur.s = ld_prefix(cp);
+        cur.s = ld_prefix_v(cp);
     } else {
         bt.add(pres_bytes(b.pres[fp.back]) + sizeof(crisb_hit_rec));
         cur.s = ld_pres(b.pres[fp.back], pi).s;  // PrefixPath(prev, f, canon.primaryInt)

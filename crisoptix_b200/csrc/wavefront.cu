@@ -64,24 +64,14 @@ RT_D Prefix fresh_prefix() {
 // record is started, by a whole-record store.
 RT_D Prefix ld_prefix_run(const crisb_prefix_rec& r) {
     Prefix p;
-    p.flags = r.flags;
-    p.f = ld3(r.f);
-    p.prf = ld3(r.post_recon_f);
-    p.p = r.p;
-    p.path_len = r.path_len;
-    p.rod = ld3(r.recon_out_dir);
+    ld_prefix_tail_v(r, p);
     return p;
 }
 RT_D void st_prefix_step(crisb_prefix_rec& r, const Prefix& p, uint32_t set) {
     if (set & kSetPrimary) st_hit(r.primary, p.primary);
     if (set & kSetRecon) st_hit(r.recon, p.recon);
     if (set & kSetLast) st_hit(r.last, p.last);
-    r.flags = p.flags;
-    st3(r.f, p.f);
-    st3(r.post_recon_f, p.prf);
-    r.p = p.p;
-    r.path_len = p.path_len;
-    st3(r.recon_out_dir, p.rod);
+    st_prefix_tail_v(r, p);
 }
 RT_D Suffix ld_suffix_run(const crisb_suffix_rec& r) {
     Suffix s;
@@ -101,12 +91,14 @@ RT_D void st_suffix_step(crisb_suffix_rec& r, const Suffix& s, uint32_t set) {
     st3(r.recon_out_dir, s.rod);
 }
 
+// a whole reservoir slot (112 bytes) as seven 16-byte stores
 RT_D void st_suffix_slot(crisb_suffix_res_rec& slot, const Suffix& sfx) {
     crisb_suffix_res_rec o;
     st_suffix(o.sample, sfx);
+    o.sample.pad = 0u;
     o.w_sum = 0.0f;
     o.confidence = 0.0f;
-    slot = o;
+    st_rec(&slot, 0, o);
 }
 
 // Path records move between rounds field group by field group.  A step after
@@ -163,10 +155,10 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_prefix(FrameParams fp, B
         const uint32_t x = i % fp.width, y = i / fp.width;
         Rng rng = rng_seeded(tea64(i, fp.random));
         const V3 dir = camera_dir(fp, x, y, rng);
-        Prefix pre = ld_prefix(b.canon_prefix[i]);
+        Prefix pre = ld_prefix_v(b.canon_prefix[i]);
         WfPath w = wf_blank();
         req = pre_begin(fp, pre, w, ld3(fp.cam.pos), dir, rng);
-        st_prefix(b.canon_prefix[i], pre);
+        st_prefix_v(b.canon_prefix[i], pre);
         w.rng = rng.state;
         wf_store(b.wf, i, w);
         b.pass_status[i] = kWfPath;
@@ -187,7 +179,7 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_suffix(SceneView s, Fram
             b.pass_status[i] = kWfIdle;
         } else {
             Rng rng{b.gbuf[i].rng};
-            Suffix suf = ld_suffix(b.canon_suffix[i].sample);
+            Suffix suf = ld_suffix(ld_rec<crisb_suffix_res_rec>(b.canon_suffix, i).sample);
             WfPath w = wf_blank();
             req = suf_begin(s, fp, suf, w, pflags, pres_last(b.pres[fp.front], i), rng);
             st_suffix_slot(b.canon_suffix[i], suf);
@@ -215,7 +207,7 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_gather(FrameParams fp, B
             Prefix cp = fresh_prefix();
             WfPath w = wf_blank();
             req = pre_begin(fp, cp, w, ld3(fp.cam.pos), dir, rng);
-            st_prefix(b.gather_cp[i], cp);
+            st_prefix_v(b.gather_cp[i], cp);
             w.rng = rng.state;
             wf_store(b.wf, i, w);
             b.pass_status[i] = kWfPath;
