@@ -347,26 +347,46 @@ __device__ inline void st_prefix_tail_v(crisb_prefix_rec& r, const Prefix& p) {
     w[6] = make_uint4(fbits(p.prf.x), fbits(p.prf.y), fbits(p.prf.z), fbits(p.p));
     w[7] = make_uint4(fbits(p.path_len), fbits(p.rod.x), fbits(p.rod.y), fbits(p.rod.z));
 }
-__device__ inline Prefix ld_prefix_v(const crisb_prefix_rec& r) {
-    const uint4* w = reinterpret_cast<const uint4*>(&r);
-    const uint4 a = w[0], b = w[1], c = w[2], d = w[3], e = w[4];
+// the record's eight words from / to the fields
+__device__ inline Prefix prefix_of_words(const uint4 (&w)[8]) {
+    const uint4 a = w[0], b = w[1], c = w[2], d = w[3], e = w[4], f = w[5], g = w[6], h = w[7];
     Prefix p;
     p.rng = static_cast<uint64_t>(a.x) | (static_cast<uint64_t>(a.y) << 32);
     p.primary = Hit{a.z, bitsf(a.w), bitsf(b.x), V3{bitsf(b.y), bitsf(b.z), bitsf(b.w)}};
     p.recon = Hit{c.x, bitsf(c.y), bitsf(c.z), V3{bitsf(c.w), bitsf(d.x), bitsf(d.y)}};
     p.last = Hit{d.z, bitsf(d.w), bitsf(e.x), V3{bitsf(e.y), bitsf(e.z), bitsf(e.w)}};
-    ld_prefix_tail_v(r, p);
+    p.flags = f.x;
+    p.f = V3{bitsf(f.y), bitsf(f.z), bitsf(f.w)};
+    p.prf = V3{bitsf(g.x), bitsf(g.y), bitsf(g.z)};
+    p.p = bitsf(g.w);
+    p.path_len = bitsf(h.x);
+    p.rod = V3{bitsf(h.y), bitsf(h.z), bitsf(h.w)};
     return p;
 }
-__device__ inline void st_prefix_v(crisb_prefix_rec& r, const Prefix& p) {
-    uint4* w = reinterpret_cast<uint4*>(&r);
+__device__ inline void words_of_prefix(const Prefix& p, uint4 (&w)[8]) {
     w[0] = make_uint4(static_cast<uint32_t>(p.rng), static_cast<uint32_t>(p.rng >> 32), p.primary.prim,
                       fbits(p.primary.bu));
     w[1] = make_uint4(fbits(p.primary.bv), fbits(p.primary.dir.x), fbits(p.primary.dir.y), fbits(p.primary.dir.z));
     w[2] = make_uint4(p.recon.prim, fbits(p.recon.bu), fbits(p.recon.bv), fbits(p.recon.dir.x));
     w[3] = make_uint4(fbits(p.recon.dir.y), fbits(p.recon.dir.z), p.last.prim, fbits(p.last.bu));
     w[4] = make_uint4(fbits(p.last.bv), fbits(p.last.dir.x), fbits(p.last.dir.y), fbits(p.last.dir.z));
-    st_prefix_tail_v(r, p);
+    w[5] = make_uint4(p.flags, fbits(p.f.x), fbits(p.f.y), fbits(p.f.z));
+    w[6] = make_uint4(fbits(p.prf.x), fbits(p.prf.y), fbits(p.prf.z), fbits(p.p));
+    w[7] = make_uint4(fbits(p.path_len), fbits(p.rod.x), fbits(p.rod.y), fbits(p.rod.z));
+}
+__device__ inline Prefix ld_prefix_v(const crisb_prefix_rec& r) {
+    const uint4* s = reinterpret_cast<const uint4*>(&r);
+    uint4 w[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) w[k] = s[k];
+    return prefix_of_words(w);
+}
+__device__ inline void st_prefix_v(crisb_prefix_rec& r, const Prefix& p) {
+    uint4 w[8];
+    words_of_prefix(p, w);
+    uint4* d = reinterpret_cast<uint4*>(&r);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) d[k] = w[k];
 }
 #endif
 

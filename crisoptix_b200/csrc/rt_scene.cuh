@@ -774,7 +774,7 @@ RT_D float4 tex_sample(const uint32_t* texels, const uint4* tex_info, int tex, f
     const int i1 = i0 + 1 == W ? 0 : i0 + 1, j1 = j0 + 1 == H ? 0 : j0 + 1;
     const uint32_t* t = texels + info.x;
     // ((w00 T00 + w10 T10) + w01 T01) + w11 T11, one texel live at a time
-    float4 acc;
+    float4 acc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // set by the first add
     auto add = [&](uint32_t word, float w, bool first) {
         const float4 c = texel_rgba(word);
         acc = first ? make_float4(w * c.x, w * c.y, w * c.z, w * c.w)

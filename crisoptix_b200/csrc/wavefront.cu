@@ -14,6 +14,7 @@
 #include <cstddef>
 #include <mutex>
 
+#include "coalesce.cuh"
 #include "queues.cuh"
 #include "records.cuh"
 
@@ -148,21 +149,28 @@ RT_D void wf_store(WfPath* rec, uint32_t i, const WfPath& w) {
 }
 
 // ---- init kernels (round 0 requests) ----------------------------------------------
+// The canonical prefix records of a warp's 32 pixels are one contiguous 4 KB
+// run: they move through shared memory (warp_load_rows / warp_store_rows).
 __global__ void __launch_bounds__(kPassBlock) k_wf_init_prefix(FrameParams fp, Bufs b) {
+    __shared__ uint4 stage[kPassBlock / 32][WarpRows<8>::kStage];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in = i < pixel_count(fp);
+    uint4 rec[8];
+    warp_load_rows<8>(reinterpret_cast<const uint4*>(b.canon_prefix), i, rec, in, stage[threadIdx.x >> 5]);
     int req = kReqDone;
-    if (i < pixel_count(fp)) {
+    if (in) {
         const uint32_t x = i % fp.width, y = i / fp.width;
         Rng rng = rng_seeded(tea64(i, fp.random));
         const V3 dir = camera_dir(fp, x, y, rng);
-        Prefix pre = ld_prefix_v(b.canon_prefix[i]);
+        Prefix pre = prefix_of_words(rec);
         WfPath w = wf_blank();
         req = pre_begin(fp, pre, w, ld3(fp.cam.pos), dir, rng);
-        st_prefix_v(b.canon_prefix[i], pre);
+        words_of_prefix(pre, rec);
         w.rng = rng.state;
         wf_store(b.wf, i, w);
         b.pass_status[i] = kWfPath;
     }
+    warp_store_rows<8>(reinterpret_cast<uint4*>(b.canon_prefix), i, rec, in, stage[threadIdx.x >> 5]);
     wf_push(b, 0, req, i);
 }
 
@@ -192,8 +200,11 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_suffix(SceneView s, Fram
 }
 
 __global__ void __launch_bounds__(kPassBlock) k_wf_init_gather(FrameParams fp, Bufs b) {
+    __shared__ uint4 stage[kPassBlock / 32][WarpRows<8>::kStage];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     int req = kReqDone;
+    uint4 rec[8];
+    bool started = false;
     if (i < pixel_count(fp)) {
         if (b.canon_prefix[i].primary.prim == CRISB_INVALID_PRIM) {
             b.pass_status[i] = kWfIdle;
@@ -207,12 +218,14 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_gather(FrameParams fp, B
             Prefix cp = fresh_prefix();
             WfPath w = wf_blank();
             req = pre_begin(fp, cp, w, ld3(fp.cam.pos), dir, rng);
-            st_prefix_v(b.gather_cp[i], cp);
+            words_of_prefix(cp, rec);
+            started = true;
             w.rng = rng.state;
             wf_store(b.wf, i, w);
             b.pass_status[i] = kWfPath;
         }
     }
+    warp_store_rows<8>(reinterpret_cast<uint4*>(b.gather_cp), i, rec, started, stage[threadIdx.x >> 5]);
     wf_push(b, 0, req, i);
 }
 
