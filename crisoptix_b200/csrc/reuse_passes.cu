@@ -415,7 +415,10 @@ __global__ void __launch_bounds__(kPassBlock) k_suffix_temp_finish(FrameParams f
 // resampling kernels (selection and combines) at 10 resident 128-thread
 // blocks per SM (48 registers, a few spills): their candidate chains are
 // latency-bound, and more warps in flight beat the spills (0.935 -> 0.902 ms
-// per 1080p frame; 12 and 16 blocks spill more: 0.995 and 1.23 ms)
+// per 1080p frame; 12 and 16 blocks spill more: 0.995 and 1.23 ms).  Their
+// reservoir stores stay per thread: storing a warp's records as one run
+// through shared memory (as the path-machine init kernels do) took 0.895 ->
+// 1.09 ms, the kernels having to reach the store with every lane.
 constexpr int kResampleMinBlocks = 10;
 
 __global__ void __launch_bounds__(kPassBlock, kResampleMinBlocks) k_suffix_temp_combine(FrameParams fp, Bufs b) {
