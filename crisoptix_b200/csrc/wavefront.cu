@@ -174,6 +174,7 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_prefix(FrameParams fp, B
     wf_push(b, 0, req, i);
 }
 
+template <bool kTex>
 __global__ void __launch_bounds__(kPassBlock) k_wf_init_suffix(SceneView s, FrameParams fp, Bufs b) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     int req = kReqDone;
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_suffix(SceneView s, Fram
             Rng rng{b.gbuf[i].rng};
             Suffix suf = ld_suffix(ld_rec<crisb_suffix_res_rec>(b.canon_suffix, i).sample);
             WfPath w = wf_blank();
-            req = suf_begin(s, fp, suf, w, pflags, pres_last(b.pres[fp.front], i), rng);
+            req = suf_begin<kTex>(s, fp, suf, w, pflags, pres_last(b.pres[fp.front], i), rng);
             st_suffix_slot(b.canon_suffix[i], suf);
             w.rng = rng.state;
             wf_store(b.wf, i, w);
@@ -230,18 +231,19 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_gather(FrameParams fp, B
 }
 
 // ---- shading: resume every path whose ray of round `cur` finished ---------------------
+template <bool kTex>
 RT_D int wf_step(const SceneView& s, const FrameParams& fp, const Bufs& b, int flow, uint32_t i, WfPath& w,
                  Rng& rng) {
     if (w.phase == kPhPreHit || w.phase == kPhPreShadow) {
         crisb_prefix_rec& rec = flow == 0 ? b.canon_prefix[i] : b.gather_cp[i];
         Prefix pre = ld_prefix_run(rec);
         uint32_t set = 0;
-        int req = w.phase == kPhPreHit ? pre_on_hit(s, fp, pre, w, rng, set) : pre_on_shadow(s, pre, w, set);
+        int req = w.phase == kPhPreHit ? pre_on_hit<kTex>(s, fp, pre, w, rng, set) : pre_on_shadow<kTex>(s, pre, w, set);
         st_prefix_step(rec, pre, set);
         if (req == kReqDone && flow == 2 && fl_valid(pre.flags) && !fl_nee(pre.flags)) {
             // FinalGatherCanon: the canonical suffix continues the canonical prefix
             Suffix cs = fresh_suffix();
-            req = suf_begin(s, fp, cs, w, pre.flags, pre.last, rng);
+            req = suf_begin<kTex>(s, fp, cs, w, pre.flags, pre.last, rng);
             st_suffix_slot(b.gather_cs[i], cs);
         }
         return req;
@@ -250,8 +252,8 @@ RT_D int wf_step(const SceneView& s, const FrameParams& fp, const Bufs& b, int f
     Suffix suf = ld_suffix_run(slot.sample);
     uint32_t set = 0;
     int req = kReqDone;
-    if (w.phase == kPhSufHit) req = suf_on_hit(s, fp, suf, w, rng, set);
-    else if (w.phase == kPhSufShadow) req = suf_on_shadow(s, suf, w);
+    if (w.phase == kPhSufHit) req = suf_on_hit<kTex>(s, fp, suf, w, rng, set);
+    else if (w.phase == kPhSufShadow) req = suf_on_shadow<kTex>(s, suf, w);
     else if (w.phase == kPhSufRecon) req = suf_on_recon(s, suf, w, set);
     st_suffix_step(slot.sample, suf, set);
     return req;
@@ -278,8 +280,11 @@ RT_D void wf_trace_inline(const SceneView& s, WfPath& w, int req) {
 // shade launch per bounce.  One launch over both queues: a separate instance
 // for the shadow-ray results (94 against 126 registers) cost more in launches
 // than it gained in occupancy (shading 3.85 -> 3.98 ms per 1080p frame).
-template <bool kInline>
-__global__ void __launch_bounds__(kPassBlock) k_wf_shade(SceneView s, FrameParams fp, Bufs b, int flow, int cur) {
+// kTex: the scene has textured materials.  The untextured step kernel runs
+// at 5 resident blocks per SM (96 registers; shading 3.86 -> 3.78 ms per
+// 1080p frame against one kernel for both), the textured one at 4.
+template <bool kInline, bool kTex>
+__global__ void __launch_bounds__(kPassBlock, kInline ? 1 : (kTex ? 4 : 5)) k_wf_shade(SceneView s, FrameParams fp, Bufs b, int flow, int cur) {
     const uint32_t nc = b.wf_count[2 * cur], ns = b.wf_count[2 * cur + 1];
     const uint32_t total = nc + ns;
     const uint32_t* qc = b.wf_queue[2 * cur];
@@ -295,7 +300,7 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_shade(SceneView s, FrameParam
             i = t < nc ? qc[t] : qs[t - nc];
             WfPath w = wf_load(b.wf, i);
             Rng rng{w.rng};
-            req = wf_step(s, fp, b, flow, i, w, rng);
+            req = wf_step<kTex>(s, fp, b, flow, i, w, rng);
             if (kInline) {
                 for (int k = 0; req != kReqDone; ++k) {
                     if (k >= max_steps) {
@@ -303,7 +308,7 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_shade(SceneView s, FrameParam
                         break;
                     }
                     wf_trace_inline(s, w, req);
-                    req = wf_step(s, fp, b, flow, i, w, rng);
+                    req = wf_step<kTex>(s, fp, b, flow, i, w, rng);
                 }
                 req = kReqDone;
             }
@@ -318,12 +323,13 @@ struct WfGrids {
     unsigned shade, shade_inline;
 };
 
+template <bool kTex>
 const WfGrids& wf_grids() {
     static std::once_flag once;
     static WfGrids g{};
     std::call_once(once, [] {
-        g.shade = persistent_grid(reinterpret_cast<const void*>(k_wf_shade<false>));
-        g.shade_inline = persistent_grid(reinterpret_cast<const void*>(k_wf_shade<true>));
+        g.shade = persistent_grid(reinterpret_cast<const void*>(k_wf_shade<false, kTex>));
+        g.shade_inline = persistent_grid(reinterpret_cast<const void*>(k_wf_shade<true, kTex>));
     });
     return g;
 }
@@ -342,8 +348,9 @@ int wf_round_count(const FrameParams& fp, int flow) {
 }
 
 // rounds after the init kernel
-void wf_rounds(const SceneView& s, const FrameParams& fp, const Bufs& b, int flow, cudaStream_t st, Marker* m) {
-    const WfGrids& g = wf_grids();
+template <bool kTex>
+void wf_rounds_t(const SceneView& s, const FrameParams& fp, const Bufs& b, int flow, cudaStream_t st, Marker* m) {
+    const WfGrids& g = wf_grids<kTex>();
     const int rounds = wf_round_count(fp, flow);
     for (int r = 0; r < rounds; ++r) {
         const int cur = r & 1, nxt = cur ^ 1;
@@ -352,12 +359,17 @@ void wf_rounds(const SceneView& s, const FrameParams& fp, const Bufs& b, int flo
         if (m) m->mark(kClsTrace, st);
         if (r + 1 < rounds) {
             cudaMemsetAsync(b.wf_count + 2 * nxt, 0, 2 * sizeof(uint32_t), st);
-            k_wf_shade<false><<<g.shade, kPassBlock, 0, st>>>(s, fp, b, flow, cur);
+            k_wf_shade<false, kTex><<<g.shade, kPassBlock, 0, st>>>(s, fp, b, flow, cur);
         } else {
-            k_wf_shade<true><<<g.shade_inline, kPassBlock, 0, st>>>(s, fp, b, flow, cur);
+            k_wf_shade<true, kTex><<<g.shade_inline, kPassBlock, 0, st>>>(s, fp, b, flow, cur);
         }
         if (m) m->mark(kClsShade, st);
     }
+}
+
+void wf_rounds(const SceneView& s, const FrameParams& fp, const Bufs& b, int flow, cudaStream_t st, Marker* m) {
+    if (s.mat_tex) wf_rounds_t<true>(s, fp, b, flow, st, m);
+    else wf_rounds_t<false>(s, fp, b, flow, st, m);
 }
 
 }  // namespace
@@ -375,7 +387,8 @@ void launch_wf_prefix(const SceneView& s, const FrameParams& fp, const Bufs& b, 
 
 void launch_wf_suffix(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m) {
     cudaMemsetAsync(b.wf_count, 0, 2 * sizeof(uint32_t), st);
-    k_wf_init_suffix<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b);
+    if (s.mat_tex) k_wf_init_suffix<true><<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b);
+    else k_wf_init_suffix<false><<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(s, fp, b);
     if (m) m->mark(kClsShade, st);
     wf_rounds(s, fp, b, 1, st, m);
 }

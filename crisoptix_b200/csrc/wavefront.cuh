@@ -121,6 +121,7 @@ RT_D int pre_invalid(Prefix& pre, WfPath& w) {
     return wf_done(w);
 }
 
+template <bool kTex>
 RT_D int pre_on_hit(const SceneView& s, const FrameParams& fp, Prefix& pre, WfPath& w, Rng& rng, uint32_t& set) {
     Isect it;
     if (!wf_hit_isect(s, w, it)) return pre_invalid(pre, w);
@@ -159,7 +160,7 @@ RT_D int pre_on_hit(const SceneView& s, const FrameParams& fp, Prefix& pre, WfPa
         w.phase = kPhPreShadow;
         return kReqShadow;
     }
-    const BrdfSample bs = brdf_sample(s, it, rng);
+    const BrdfSample bs = brdf_sample<kTex>(s, it, rng);
     if (bs.pdf <= 0.0f) return pre_invalid(pre, w);
     const float recon_dist = distance(cur_pos, it.pos);
     const bool can_recon = recon_dist > fp.p.recon_min_distance && bs.roughness > fp.p.recon_min_roughness &&
@@ -186,6 +187,7 @@ RT_D int pre_on_hit(const SceneView& s, const FrameParams& fp, Prefix& pre, WfPa
     return wf_done(w);
 }
 
+template <bool kTex>
 RT_D int pre_on_shadow(const SceneView& s, Prefix& pre, WfPath& w, uint32_t& set) {
     if (w.occluded) return pre_invalid(pre, w);
     const Isect it = wf_it(w);
@@ -199,7 +201,7 @@ RT_D int pre_on_shadow(const SceneView& s, Prefix& pre, WfPath& w, uint32_t& set
     const bool post = true;
     const V3 light_dir = f3(w.nee_dir), color = f3(w.nee_col);
     const float dist = w.nee_dir.w;
-    const BrdfEval be = brdf_eval(s, it, light_dir);
+    const BrdfEval be = brdf_eval<kTex>(s, it, light_dir);
     if (be.pdf <= 0.0f) return pre_invalid(pre, w);
     const float dist_factor = 1.0f / (dist * dist);
     pre.f = pre.f * (be.brdf * color * dist_factor);
@@ -226,6 +228,7 @@ RT_D int suf_finish_nee(Suffix& suf, WfPath& w, V3 brdf) {
 
 // loop body at vertex index wf_idx(w) with interaction `it`; last_pos is the
 // position the vertex was traced from (lastPos)
+template <bool kTex>
 RT_D int suf_vertex(const SceneView& s, const FrameParams& fp, Suffix& suf, WfPath& w, const Isect& it, V3 last_pos,
                     Rng& rng, uint32_t& set) {
     const uint32_t vi = wf_idx(w), max_len = wf_maxlen(w), pre_len = wf_prelen(w);
@@ -245,7 +248,7 @@ RT_D int suf_vertex(const SceneView& s, const FrameParams& fp, Suffix& suf, WfPa
         w.phase = kPhSufShadow;
         return kReqShadow;
     }
-    const BrdfSample bs = brdf_sample(s, it, rng);
+    const BrdfSample bs = brdf_sample<kTex>(s, it, rng);
     if (bs.pdf <= 0.0f) return wf_done(w);
     suf.p *= bs.pdf * (1.0f - nee);
     suf.f = suf.f * bs.brdf;
@@ -273,6 +276,7 @@ RT_D int suf_vertex(const SceneView& s, const FrameParams& fp, Suffix& suf, WfPa
 
 // suffix from the prefix with flags `pre_flags` ending at `pre_last`; `suf`
 // holds the previous record content
+template <bool kTex>
 RT_D int suf_begin(const SceneView& s, const FrameParams& fp, Suffix& suf, WfPath& w, uint32_t pre_flags,
                    const Hit& pre_last, Rng& rng) {
     suf.f = splat(1.0f);
@@ -287,20 +291,22 @@ RT_D int suf_begin(const SceneView& s, const FrameParams& fp, Suffix& suf, WfPat
     if (!it.valid || max_len == 0) return wf_done(w);
     wf_set(w, 0, false, max_len, fl_len(pre_flags));
     uint32_t set = 0;  // suf_begin's callers store the whole record
-    return suf_vertex(s, fp, suf, w, it, it.pos, rng, set);
+    return suf_vertex<kTex>(s, fp, suf, w, it, it.pos, rng, set);
 }
 
+template <bool kTex>
 RT_D int suf_on_hit(const SceneView& s, const FrameParams& fp, Suffix& suf, WfPath& w, Rng& rng, uint32_t& set) {
     Isect it;
     if (!wf_hit_isect(s, w, it)) return wf_done(w);
-    return suf_vertex(s, fp, suf, w, it, f3(w.ray_o), rng, set);
+    return suf_vertex<kTex>(s, fp, suf, w, it, f3(w.ray_o), rng, set);
 }
 
+template <bool kTex>
 RT_D int suf_on_shadow(const SceneView& s, Suffix& suf, WfPath& w) {
     if (w.occluded) return wf_done(w);
     const Isect it = wf_it(w);
     const V3 light_dir = f3(w.nee_dir);
-    const BrdfEval be = brdf_eval(s, it, light_dir);
+    const BrdfEval be = brdf_eval<kTex>(s, it, light_dir);
     if (be.pdf <= 0.0f) return wf_done(w);
     suf.flags = fl_set_len(suf.flags, fl_len(suf.flags) + 1);
     if (!wf_post(w)) {
