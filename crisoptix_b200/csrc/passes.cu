@@ -4,6 +4,7 @@
 // prefix copy: one thread per pixel.  (The reuse passes and the final gather
 // are split into shift jobs in reuse_passes.cu.)
 #define CRISB_LBVH_KERNELS 1
+#include "coalesce.cuh"
 #include "records.cuh"
 
 namespace crisb {
@@ -25,18 +26,42 @@ __global__ void k_bounds_init(unsigned int* ob, uint32_t* n) {
 // __raygen__prefix_store_entries, shader/prefix_store_entries.cu:9-53: the
 // endpoint of the front prefix and the radius the search tests against,
 // (aabb.maxX - aabb.minX) / 2 (shader/prefix_search_hit.cu:42).
+// The front prefix reservoirs of a warp's 32 pixels are one contiguous run:
+// they are loaded through shared memory (coalesce.cuh), and the flags, last
+// vertex and path length taken from the words.
 __global__ void k_store_entries(FrameParams fp, Bufs b, const SceneView s, unsigned int* ob, uint32_t* count) {
+    __shared__ uint4 stage[kPassBlock / 32][WarpRows<9>::kStage];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t P = pixel_count(fp);
     float4 e = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
     bool valid = false;
+    uint32_t pflags = 0;
+    Hit plast{};
+    float plen = 0.0f;
+    if (b.pres[fp.front].f16) {
+        static_assert(sizeof(crisb_prefix_res16_rec) == 5 * 16, "FP16 prefix reservoir size");
+        uint4 w[5];
+        warp_load_rows<5>(static_cast<const uint4*>(b.pres[fp.front].p), i, w, i < P, stage[threadIdx.x >> 5]);
+        crisb_prefix_res16_rec o;
+        memcpy(&o, w, sizeof(o));
+        pflags = o.flags;
+        plast = unpack_hit16(o.last);
+        plen = o.path_len;
+    } else {
+        static_assert(sizeof(crisb_prefix_res_rec) == 9 * 16, "FP32 prefix reservoir size");
+        uint4 w[9];
+        warp_load_rows<9>(static_cast<const uint4*>(b.pres[fp.front].p), i, w, i < P, stage[threadIdx.x >> 5]);
+        const Prefix pr = prefix_of_words(reinterpret_cast<const uint4 (&)[8]>(w));
+        pflags = pr.flags;
+        plast = pr.last;
+        plen = pr.path_len;
+    }
     if (i < P) {
-        const uint32_t pflags = pres_flags(b.pres[fp.front], i);
         const uint32_t sflags = sres_flags(b.sres_cur, i);
-        const Isect last = unpack(s, pres_last(b.pres[fp.front], i));
+        const Isect last = unpack(s, plast);
         if (fl_valid(pflags) && fl_valid(sflags) && last.valid) {
             float radius = fp.p.gather_radius;
-            if (fp.p.gather_radius_type == CRISB_RADIUS_PATH_LENGTH) radius *= pres_path_len(b.pres[fp.front], i) / 4.5f;
+            if (fp.p.gather_radius_type == CRISB_RADIUS_PATH_LENGTH) radius *= plen / 4.5f;
             const float minx = last.pos.x - radius, maxx = last.pos.x + radius;
             e = make_float4(last.pos.x, last.pos.y, last.pos.z, (maxx - minx) / 2.0f);
             valid = true;

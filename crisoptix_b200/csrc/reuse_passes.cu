@@ -677,7 +677,15 @@ __global__ void __launch_bounds__(kPassBlock) k_gather_query(SceneView s, FrameP
             b.pass_flags[i] = vflags;
             b.pass_status[i] = kStReuse;
         }
-        if (k > 0) {
+        if (k > 0 && (k & 1u) == 0u) {
+            // an even count: the pixel's list starts 16-byte aligned, two records a store
+            uint4* d = reinterpret_cast<uint4*>(b.neighbors + static_cast<size_t>(i) * k);
+            for (uint32_t n = 0; n < k; n += 2) {
+                const bool a0 = n < nl.count, a1 = n + 1 < nl.count;
+                d[n >> 1] = make_uint4(a0 ? nl.pix[n] : 0u, __float_as_uint(a0 ? nl.dist[n] : 0.0f),
+                                       a1 ? nl.pix[n + 1] : 0u, __float_as_uint(a1 ? nl.dist[n + 1] : 0.0f));
+            }
+        } else if (k > 0) {
             for (uint32_t n = 0; n < k; ++n) {
                 crisb_neighbor_rec r;
                 r.pixel = n < nl.count ? nl.pix[n] : 0u;
