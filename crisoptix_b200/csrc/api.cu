@@ -921,6 +921,10 @@ struct crisb_renderer {
         fp.back = back;
         fp.k = K();
         fp.trace_grid = std::max(1u, trace_grid / std::max(1u, concurrent_views));
+        // views rendering at once keep shared memory out of their init kernels:
+        // the 16-view batch ran 100.7 ms per frame with the staged instances
+        // beside 95.7 without, while a single 1080p view gains 0.17 ms from them
+        fp.shared_stage = concurrent_views > 1 ? 0u : 1u;
         fp.trace_block = trace_block;
         require(params.motion_mode != CRISB_MOTION_VECTORS || motion != nullptr,
                 "render_frame: CRISB_MOTION_VECTORS without motion vectors");

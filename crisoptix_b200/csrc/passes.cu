@@ -26,11 +26,14 @@ __global__ void k_bounds_init(unsigned int* ob, uint32_t* n) {
 // __raygen__prefix_store_entries, shader/prefix_store_entries.cu:9-53: the
 // endpoint of the front prefix and the radius the search tests against,
 // (aabb.maxX - aabb.minX) / 2 (shader/prefix_search_hit.cu:42).
-// The front prefix reservoirs of a warp's 32 pixels are one contiguous run:
-// they are loaded through shared memory (coalesce.cuh), and the flags, last
-// vertex and path length taken from the words.
+// kStage: the front prefix reservoirs of a warp's 32 pixels are one
+// contiguous run, loaded through shared memory (coalesce.cuh; 20 KB per
+// block), and the flags, last vertex and path length taken from the words.
+// Otherwise each thread reads its own reservoir's three fields: the instance
+// for views rendering at once, whose kernels stay clear of large shared
+// memory blocks.
+template <bool kStage>
 __global__ void k_store_entries(FrameParams fp, Bufs b, const SceneView s, unsigned int* ob, uint32_t* count) {
-    __shared__ uint4 stage[kPassBlock / 32][WarpRows<9>::kStage];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t P = pixel_count(fp);
     float4 e = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
@@ -38,23 +41,32 @@ __global__ void k_store_entries(FrameParams fp, Bufs b, const SceneView s, unsig
     uint32_t pflags = 0;
     Hit plast{};
     float plen = 0.0f;
-    if (b.pres[fp.front].f16) {
-        static_assert(sizeof(crisb_prefix_res16_rec) == 5 * 16, "FP16 prefix reservoir size");
-        uint4 w[5];
-        warp_load_rows<5>(static_cast<const uint4*>(b.pres[fp.front].p), i, w, i < P, stage[threadIdx.x >> 5]);
-        crisb_prefix_res16_rec o;
-        memcpy(&o, w, sizeof(o));
-        pflags = o.flags;
-        plast = unpack_hit16(o.last);
-        plen = o.path_len;
+    if constexpr (!kStage) {
+        if (i < P) {
+            pflags = pres_flags(b.pres[fp.front], i);
+            plast = pres_last(b.pres[fp.front], i);
+            plen = pres_path_len(b.pres[fp.front], i);
+        }
     } else {
-        static_assert(sizeof(crisb_prefix_res_rec) == 9 * 16, "FP32 prefix reservoir size");
-        uint4 w[9];
-        warp_load_rows<9>(static_cast<const uint4*>(b.pres[fp.front].p), i, w, i < P, stage[threadIdx.x >> 5]);
-        const Prefix pr = prefix_of_words(reinterpret_cast<const uint4 (&)[8]>(w));
-        pflags = pr.flags;
-        plast = pr.last;
-        plen = pr.path_len;
+        __shared__ uint4 stage[kPassBlock / 32][WarpRows<9>::kStage];
+        if (b.pres[fp.front].f16) {
+            static_assert(sizeof(crisb_prefix_res16_rec) == 5 * 16, "FP16 prefix reservoir size");
+            uint4 w[5];
+            warp_load_rows<5>(static_cast<const uint4*>(b.pres[fp.front].p), i, w, i < P, stage[threadIdx.x >> 5]);
+            crisb_prefix_res16_rec o;
+            memcpy(&o, w, sizeof(o));
+            pflags = o.flags;
+            plast = unpack_hit16(o.last);
+            plen = o.path_len;
+        } else {
+            static_assert(sizeof(crisb_prefix_res_rec) == 9 * 16, "FP32 prefix reservoir size");
+            uint4 w[9];
+            warp_load_rows<9>(static_cast<const uint4*>(b.pres[fp.front].p), i, w, i < P, stage[threadIdx.x >> 5]);
+            const Prefix pr = prefix_of_words(reinterpret_cast<const uint4 (&)[8]>(w));
+            pflags = pr.flags;
+            plast = pr.last;
+            plen = pr.path_len;
+        }
     }
     if (i < P) {
         const uint32_t sflags = sres_flags(b.sres_cur, i);
@@ -134,7 +146,8 @@ void launch_prefix_copy_front_back(const FrameParams& fp, const Bufs& b, cudaStr
 void launch_store_entries(const SceneView& s, const FrameParams& fp, const Bufs& b, const lbvh::Work& w,
                           unsigned int* bounds, cudaStream_t st) {
     k_bounds_init<<<1, 32, 0, st>>>(bounds, w.n);
-    k_store_entries<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, s, bounds, w.n);
+    if (fp.shared_stage) k_store_entries<true><<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, s, bounds, w.n);
+    else k_store_entries<false><<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, s, bounds, w.n);
     k_knn_keys<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b, w, bounds);
 }
 void launch_knn_finish(const FrameParams& fp, const Bufs& b, const lbvh::Work& w, float4* leaf_entries,

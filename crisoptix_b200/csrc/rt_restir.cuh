@@ -22,6 +22,7 @@ struct FrameParams {
     uint32_t k;          // gatherM - 1
     uint32_t trace_grid; // traversal launches: blocks per resident block (host side only)
     uint32_t trace_block; // traversal launches: threads per block, 64 / 128 / 256 (host side only)
+    uint32_t shared_stage = 1;  // init kernels stage record runs in shared memory (host side only)
     const float2* motion = nullptr;  // CRISB_MOTION_VECTORS: per-pixel motion vectors
     crisb_camera_data prev_cam{};    // CRISB_MOTION_REPROJECT: the previous frame's camera
     uint32_t has_prev_cam = 0;

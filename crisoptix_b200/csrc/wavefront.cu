@@ -150,13 +150,47 @@ RT_D void wf_store(WfPath* rec, uint32_t i, const WfPath& w) {
 
 // ---- init kernels (round 0 requests) ----------------------------------------------
 // The canonical prefix records of a warp's 32 pixels are one contiguous 4 KB
-// run: they move through shared memory (warp_load_rows / warp_store_rows).
+// run.  kStage: they move through shared memory (warp_load_rows /
+// warp_store_rows; 18 KB per block).  Otherwise each thread moves its own
+// record's eight 16-byte words and the kernel uses no shared memory, which is
+// the instance for views rendering at once (the staged one slowed a 16-view
+// batch by 5%).  Every lane calls both; lanes with `valid` false are untouched.
+template <bool kStage>
+struct PrefixRows {
+    uint4* stage = nullptr;
+    RT_D PrefixRows() {
+        if constexpr (kStage) {
+            __shared__ uint4 rows[kPassBlock / 32][WarpRows<8>::kStage];
+            stage = rows[threadIdx.x >> 5];
+        }
+    }
+    RT_D void load(const crisb_prefix_rec* base, uint32_t i, uint4 (&w)[8], bool valid) const {
+        if constexpr (kStage) {
+            warp_load_rows<8>(reinterpret_cast<const uint4*>(base), i, w, valid, stage);
+        } else if (valid) {
+            const uint4* s = reinterpret_cast<const uint4*>(base + i);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) w[k] = s[k];
+        }
+    }
+    RT_D void store(crisb_prefix_rec* base, uint32_t i, const uint4 (&w)[8], bool valid) const {
+        if constexpr (kStage) {
+            warp_store_rows<8>(reinterpret_cast<uint4*>(base), i, w, valid, stage);
+        } else if (valid) {
+            uint4* d = reinterpret_cast<uint4*>(base + i);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) d[k] = w[k];
+        }
+    }
+};
+
+template <bool kStage>
 __global__ void __launch_bounds__(kPassBlock) k_wf_init_prefix(FrameParams fp, Bufs b) {
-    __shared__ uint4 stage[kPassBlock / 32][WarpRows<8>::kStage];
+    const PrefixRows<kStage> rows;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool in = i < pixel_count(fp);
     uint4 rec[8];
-    warp_load_rows<8>(reinterpret_cast<const uint4*>(b.canon_prefix), i, rec, in, stage[threadIdx.x >> 5]);
+    rows.load(b.canon_prefix, i, rec, in);
     int req = kReqDone;
     if (in) {
         const uint32_t x = i % fp.width, y = i / fp.width;
@@ -170,7 +204,7 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_prefix(FrameParams fp, B
         wf_store(b.wf, i, w);
         b.pass_status[i] = kWfPath;
     }
-    warp_store_rows<8>(reinterpret_cast<uint4*>(b.canon_prefix), i, rec, in, stage[threadIdx.x >> 5]);
+    rows.store(b.canon_prefix, i, rec, in);
     wf_push(b, 0, req, i);
 }
 
@@ -200,8 +234,9 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_suffix(SceneView s, Fram
     wf_push(b, 0, req, i);
 }
 
+template <bool kStage>
 __global__ void __launch_bounds__(kPassBlock) k_wf_init_gather(FrameParams fp, Bufs b) {
-    __shared__ uint4 stage[kPassBlock / 32][WarpRows<8>::kStage];
+    const PrefixRows<kStage> rows;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     int req = kReqDone;
     uint4 rec[8];
@@ -226,7 +261,7 @@ __global__ void __launch_bounds__(kPassBlock) k_wf_init_gather(FrameParams fp, B
             b.pass_status[i] = kWfPath;
         }
     }
-    warp_store_rows<8>(reinterpret_cast<uint4*>(b.gather_cp), i, rec, started, stage[threadIdx.x >> 5]);
+    rows.store(b.gather_cp, i, rec, started);
     wf_push(b, 0, req, i);
 }
 
@@ -380,7 +415,8 @@ uint32_t wf_launches_per_pass(const FrameParams& fp, int flow) {
 
 void launch_wf_prefix(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m) {
     cudaMemsetAsync(b.wf_count, 0, 2 * sizeof(uint32_t), st);
-    k_wf_init_prefix<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
+    if (fp.shared_stage) k_wf_init_prefix<true><<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
+    else k_wf_init_prefix<false><<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
     if (m) m->mark(kClsShade, st);
     wf_rounds(s, fp, b, 0, st, m);
 }
@@ -395,7 +431,8 @@ void launch_wf_suffix(const SceneView& s, const FrameParams& fp, const Bufs& b, 
 
 void launch_wf_gather(const SceneView& s, const FrameParams& fp, const Bufs& b, cudaStream_t st, Marker* m) {
     cudaMemsetAsync(b.wf_count, 0, 2 * sizeof(uint32_t), st);
-    k_wf_init_gather<<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
+    if (fp.shared_stage) k_wf_init_gather<true><<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
+    else k_wf_init_gather<false><<<grid_for(fp.width * fp.height), kPassBlock, 0, st>>>(fp, b);
     if (m) m->mark(kClsShade, st);
     wf_rounds(s, fp, b, 2, st, m);
 }
