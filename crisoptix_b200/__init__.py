@@ -216,6 +216,22 @@ class Renderer:
         check(load().crisb_render_frame(self.handle, ctypes.byref(camera_struct(camera)), ctypes.c_void_p(out_dev_ptr),
                                         ctypes.c_void_p(stream)))
 
+    def restir_adjoint_enable(self, on: bool = True):
+        """From the next frame on, keep what the resampled-path adjoint reads
+        (crisb_restir_adjoint_enable)."""
+        check(load().crisb_restir_adjoint_enable(self.handle, 1 if on else 0))
+
+    def restir_adjoint_forward(self, out_dev_ptr: int, stream: int = 0):
+        """The last frame's final-gather estimator at the scene's current
+        tables, frozen at the frame's (width*height*3 floats)."""
+        check(load().crisb_restir_adjoint_forward(self.handle, ctypes.c_void_p(out_dev_ptr), ctypes.c_void_p(stream)))
+
+    def restir_adjoint_backward(self, d_img_ptr: int, d_mats_ptr: int, d_em_ptr: int, stream: int = 0):
+        """Adds dLoss/dparameter of the last frame's final-gather estimator
+        (7 floats per material, 3 per emitter) for d_img = dLoss/dimage."""
+        check(load().crisb_restir_adjoint_backward(self.handle, ctypes.c_void_p(d_img_ptr), ctypes.c_void_p(d_mats_ptr),
+                                                   ctypes.c_void_p(d_em_ptr), ctypes.c_void_p(stream)))
+
     def get_frame_idx(self) -> int:
         v = ctypes.c_uint64()
         check(load().crisb_frame_index(self.handle, ctypes.byref(v)))

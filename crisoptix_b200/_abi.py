@@ -210,6 +210,9 @@ ENTRY_POINTS = {
     "crisb_adjoint_refreeze": (c_i32, [c_vp]),
     "crisb_adjoint_forward": (c_i32, [c_vp, ctypes.POINTER(Camera), c_u64, c_vp, c_vp]),
     "crisb_adjoint_backward": (c_i32, [c_vp, ctypes.POINTER(Camera), c_u64, c_vp, c_vp, c_vp, c_vp]),
+    "crisb_restir_adjoint_enable": (c_i32, [c_vp, c_i32]),
+    "crisb_restir_adjoint_forward": (c_i32, [c_vp, c_vp, c_vp]),
+    "crisb_restir_adjoint_backward": (c_i32, [c_vp, c_vp, c_vp, c_vp, c_vp]),
     "crisb_batch_create": (c_i32, [ctypes.POINTER(c_vp), c_u32, ctypes.POINTER(c_vp)]),
     "crisb_batch_destroy": (c_i32, [c_vp]),
     "crisb_batch_render": (c_i32, [c_vp, c_vp, ctypes.POINTER(c_vp), c_vp]),

@@ -1,9 +1,12 @@
-"""Path-replay adjoint of the path tracer (include/crisb.h, crisb_adjoint_*).
+"""Path-replay adjoints (include/crisb.h): of the path tracer
+(crisb_adjoint_*) and of the final gather's resampled estimator
+(crisb_restir_adjoint_*).
 
-``PtAdjoint`` wraps the C ABI; ``PtImage`` is a ``torch.autograd.Function``
-over it, for checking only (the library itself needs no torch); ``fd_check``
-compares the adjoint's gradient of an L2 image loss with central differences
-of the same frozen-sampling estimator, summed in float64.
+``PtAdjoint`` and ``RestirAdjoint`` wrap the C ABI; ``PtImage`` and
+``RestirImage`` are ``torch.autograd.Function`` classes over them, for checking
+only (the library itself needs no torch); ``fd_check`` and
+``restir_fd_check`` compare an adjoint's gradient of an L2 image loss with
+central differences of the same frozen estimator, summed in float64.
 
 Parameters as the inverse-rendering config names them: per material the
 diffuse albedo (3) and roughness (1); per emitter its radiance (3), which the
@@ -139,6 +142,86 @@ def pt_image_function():
     return PtImage
 
 
+class RestirAdjoint:
+    """Path-replay adjoint of the resampled estimator over one Conditional
+    ReSTIR renderer per view (FP32 storage, gather_n 1, no accumulation).
+    ``prepare`` renders `frames` frames of every view at the scene's current
+    tables (temporal and spatial reuse fill the reservoirs); ``render`` and
+    ``gradient`` then evaluate and differentiate each view's last frame."""
+
+    def __init__(self, scene, width: int, height: int, params: _abi.Params, num_views: int):
+        from . import Renderer
+
+        self.scene, self.width, self.height = scene, width, height
+        self.num_mats = len(scene.desc.materials)
+        self.num_emitters = len(scene.desc.emitters)
+        self.views = [Renderer(width, height, scene, params) for _ in range(num_views)]
+        for r in self.views:
+            r.restir_adjoint_enable(True)
+        self.frame_images = None
+
+    def prepare(self, cams: Sequence[Camera], frames: int = 3):
+        """Renders the frames; returns the last frame's (V, H, W, 3) images."""
+        import torch
+
+        out = torch.zeros(len(cams), self.height * self.width * 3, dtype=torch.float32, device="cuda")
+        for f in range(frames):
+            for r, c, o in zip(self.views, cams, out):
+                r.launch_frame(c, o.data_ptr())
+        torch.cuda.synchronize()
+        self.frame_images = out.view(len(cams), self.height, self.width, 3)
+        return self.frame_images
+
+    def render(self):
+        """(V, H, W, 3) float32 device tensor: each view's frozen estimator at
+        the scene's current tables."""
+        import torch
+
+        out = torch.zeros(len(self.views), self.height * self.width * 3, dtype=torch.float32, device="cuda")
+        for r, o in zip(self.views, out):
+            r.restir_adjoint_forward(o.data_ptr())
+        return out.view(len(self.views), self.height, self.width, 3)
+
+    def gradient(self, d_img):
+        """(materials x 7, emitters x 3) float32 device tensors of dLoss/dparameter
+        for d_img = dLoss/dimage of shape (V, H, W, 3)."""
+        import torch
+
+        d_img = d_img.contiguous().view(len(self.views), -1).float()
+        g_mat = torch.zeros(self.num_mats * MAT_GRAD, dtype=torch.float32, device="cuda")
+        g_em = torch.zeros(self.num_emitters * EM_GRAD, dtype=torch.float32, device="cuda")
+        for v, r in enumerate(self.views):
+            r.restir_adjoint_backward(d_img[v].data_ptr(), g_mat.data_ptr(), g_em.data_ptr())
+        return g_mat.view(self.num_mats, MAT_GRAD), g_em.view(self.num_emitters, EM_GRAD)
+
+
+def restir_image_function():
+    """The torch.autograd.Function class of the resampled estimator (built
+    lazily so importing this module needs no torch)."""
+    import torch
+
+    class RestirImage(torch.autograd.Function):
+        """images = RestirImage.apply(diffuse (M,3), roughness (M,), emission
+        (M,3), emitter_rgb (E,3), adjoint, base_materials): the frozen
+        estimator of the adjoint's prepared frames at these parameters"""
+
+        @staticmethod
+        def forward(ctx, diffuse, roughness, emission, emitter_rgb, adj, base):
+            _apply(adj.scene, base, diffuse.detach().cpu().numpy(), roughness.detach().cpu().numpy(),
+                   emission.detach().cpu().numpy(), emitter_rgb.detach().cpu().numpy())
+            ctx.adj = adj
+            ctx.like = (diffuse, roughness, emission, emitter_rgb)
+            return adj.render()
+
+        @staticmethod
+        def backward(ctx, grad_img):
+            g_mat, g_em = ctx.adj.gradient(grad_img)
+            grads = (g_mat[:, 0:3], g_mat[:, 3], g_mat[:, 4:7], g_em)
+            return tuple(g.to(device=t.device, dtype=t.dtype) for g, t in zip(grads, ctx.like)) + (None,) * 2
+
+    return RestirImage
+
+
 @dataclass
 class Param:
     kind: str   # "diffuse", "roughness" or "radiance"
@@ -234,6 +317,77 @@ def fd_check(scene, desc, cams: Sequence[Camera], width: int, height: int, param
     return {"adjoint": grad, "fd": fd, "rel_err": rel, "loss": loss(start_mats, start_rgb)}
 
 
+def restir_fd_check(scene, desc, cams: Sequence[Camera], width: int, height: int, params: _abi.Params,
+                    target_mats: np.ndarray, target_rgb: np.ndarray, start_mats: np.ndarray, start_rgb: np.ndarray,
+                    check_params: Sequence[Param], eps: float = 1e-3, frames: int = 3) -> dict:
+    """As ``fd_check`` for the resampled estimator: `frames` Conditional ReSTIR
+    frames per view at the start parameters, then the adjoint gradient of loss
+    = sum of (image - target)^2 (target: the frozen estimator at the target
+    parameters) against central differences of the frozen estimator.  Also
+    the largest difference between the frozen estimator at the start
+    parameters and the frames' own images."""
+    em_mats = emitter_materials(desc)
+    set_materials(scene, start_mats)
+    set_emitter_colors(scene, start_rgb)
+    adj = RestirAdjoint(scene, width, height, params, len(cams))
+    frame_img = adj.prepare(cams, frames).double()
+    start_img = adj.render()
+    frame_diff = float((start_img.double() - frame_img).abs().max())
+    frame_scale = float(frame_img.abs().max())
+    set_materials(scene, target_mats)
+    set_emitter_colors(scene, target_rgb)
+    target = adj.render().double()
+    set_materials(scene, start_mats)
+    set_emitter_colors(scene, start_rgb)
+    img = adj.render()
+    d_img = 2.0 * (img.double() - target)
+    g_mat, g_em = adj.gradient(d_img.float())
+    grad = gather(g_mat.cpu().numpy().astype(np.float64), g_em.cpu().numpy().astype(np.float64), check_params,
+                  em_mats)
+
+    def loss(mats, rgb):
+        set_materials(scene, mats)
+        set_emitter_colors(scene, rgb)
+        return float(((adj.render().double() - target) ** 2).sum())
+
+    fd = np.zeros(len(check_params))
+    for k, p in enumerate(check_params):
+        h = eps * max(abs(value_of(start_mats, start_rgb, p)), 1e-2)
+        mp, rp = perturb(start_mats, start_rgb, p, h, em_mats)
+        mm, rm = perturb(start_mats, start_rgb, p, -h, em_mats)
+        fd[k] = (loss(mp, rp) - loss(mm, rm)) / (2.0 * h)
+    set_materials(scene, start_mats)
+    set_emitter_colors(scene, start_rgb)
+    scale = np.maximum(np.abs(fd), 1e-12)
+    rel = np.abs(grad - fd) / scale
+    return {"adjoint": grad, "fd": fd, "rel_err": rel, "loss": loss(start_mats, start_rgb),
+            "frame_max_abs_diff": frame_diff, "frame_max_abs": frame_scale,
+            "frame_equal": bool(torch_equal(start_img, frame_img))}
+
+
+def restir_params(scene_size: float, seed: int = 3, **overrides) -> _abi.Params:
+    """Conditional ReSTIR with the large workload's reuse (depth 8, prefix
+    length 2, NEE probability 0.3, temporal reuse, 2 suffix spatial rounds of
+    5 neighbours, final gather with k = 8 neighbours in a path-length radius)
+    and what the adjoint needs: FP32 storage, one final-gather prefix, no
+    accumulation."""
+    from . import default_params
+
+    kw = dict(renderer_type=_abi.CONDITIONAL_RESTIR, max_path_len=8, nee_prob=0.3, seed=seed, enable_accum=0,
+              recon_min_distance=0.01 * scene_size, recon_min_roughness=0.2, prefix_len=2, prefix_enable_temporal=1,
+              prefix_enable_spatial=0, suffix_enable_temporal=1, suffix_enable_spatial=1, suffix_spatial_count=5,
+              suffix_spatial_rounds=2, gather_n=1, gather_m=9, gather_radius=0.01,
+              gather_radius_type=_abi.RADIUS_PATH_LENGTH, window_radius=10, storage=_abi.STORAGE_FP32)
+    kw.update(overrides)
+    return default_params(scene_size, **kw)
+
+
+def torch_equal(a, b) -> bool:
+    import torch
+
+    return bool(torch.equal(a.double(), b.double()))
+
+
 def inverse_config_params(desc, num_params: int = 20, seed: int = 3, min_roughness: int = 0) -> List[Param]:
     """`num_params` random parameters of the inverse-rendering config: sphere
     albedos (materials 1..64, 3 channels), GGX roughnesses (odd spheres) and
@@ -298,6 +452,9 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--min-roughness", type=int, default=4, help="at least this many roughness parameters")
     ap.add_argument("--small", action="store_true", help="a 12-sphere room instead of the large scene")
+    ap.add_argument("--estimator", default="pt", choices=["pt", "restir"],
+                    help="pt: the path tracer; restir: the final gather's resampled estimator")
+    ap.add_argument("--frames", type=int, default=3, help="restir: frames rendered before the check")
     a = ap.parse_args(argv)
     if a.small:
         desc, _ = scenes.sphere_room(num_spheres=12, subdiv=2, num_emitters=12, seed=4)
@@ -310,12 +467,19 @@ def main(argv=None):
     tm, trgb, sm, srgb = perturbed_start(desc, seed=a.seed)
     chk = inverse_config_params(desc, a.params, a.seed, a.min_roughness)
     t0 = time.time()
-    r = fd_check(sc, desc, cams, a.res, a.res, p, tm, trgb, sm, srgb, chk, eps=a.eps)
+    if a.estimator == "restir":
+        p = restir_params(sc.scene_size, a.seed)
+        r = restir_fd_check(sc, desc, cams, a.res, a.res, p, tm, trgb, sm, srgb, chk, eps=a.eps, frames=a.frames)
+    else:
+        r = fd_check(sc, desc, cams, a.res, a.res, p, tm, trgb, sm, srgb, chk, eps=a.eps)
     torch.cuda.synchronize()
     big = np.abs(r["fd"]) > 1e-3 * np.abs(r["fd"]).max()
+    extra = {k: r[k] for k in ("frame_max_abs_diff", "frame_max_abs", "frame_equal") if k in r}
     print(json.dumps({"config": f"inverse rendering: {a.views} views {a.res}x{a.res}, {len(desc.materials)} materials, "
                                 f"{len(desc.emitters)} emitters, {len(chk)} parameters, eps {a.eps}, seed {a.seed}",
+                      "estimator": a.estimator, **extra,
                       "max_rel_err": float(r["rel_err"][big].max()) if big.any() else None,
+                      "max_rel_err_all": float(r["rel_err"].max()),
                       "params_checked": int(big.sum()), "loss": r["loss"],
                       "params": [f"{q.kind}[{q.index}].{q.channel}" for q in chk],
                       "adjoint": [float(v) for v in r["adjoint"]], "fd": [float(v) for v in r["fd"]],

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libcrisb.so")
-SOURCES = ["api.cu", "passes.cu", "search.cu", "reuse_passes.cu", "wavefront.cu", "bvh_build.cpp", "adjoint.cu", "tonemap.cu",
+SOURCES = ["api.cu", "passes.cu", "search.cu", "reuse_passes.cu", "wavefront.cu", "bvh_build.cpp", "adjoint.cu", "restir_adjoint.cu", "tonemap.cu",
            "context.cpp", "selftest.cu", "radix_sort.cu",
            "bvh_device.cu"]
 

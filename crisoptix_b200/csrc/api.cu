@@ -847,6 +847,13 @@ struct crisb_renderer {
     // (at least 1) x the resident blocks (16 views of the multiview workload:
     // 98.6 against 100.0 ms per frame at the full multiplier)
     uint32_t concurrent_views = 1;
+    // resampled-path adjoint (crisb_restir_adjoint_*): while enabled, each
+    // frame copies the material and emitter tables it renders with (the
+    // adjoint's frozen sampling); the last frame's parameters
+    bool adjoint_on = false, adjoint_frame = false, has_frame = false;
+    DevBuf<crisb_material> frame_mats;
+    DevBuf<crisb_emitter> frame_emitters;
+    FrameParams last_fp{};
     // optional sRGB bytes of each frame (ToneMapping after LaunchFrame,
     // src/main.cpp:122-127), written by a last kernel of the frame
     uint8_t* srgb_out = nullptr;
@@ -933,6 +940,16 @@ struct crisb_renderer {
         fp.has_prev_cam = has_prev_cam ? 1u : 0u;
         prev_cam = fp.cam;
         has_prev_cam = true;
+        if (adjoint_on) {
+            check(cudaMemcpyAsync(frame_mats.p, scene->mats.p, scene->mats.bytes(), cudaMemcpyDeviceToDevice, st),
+                  "adjoint tables");
+            check(cudaMemcpyAsync(frame_emitters.p, scene->emitters.p, scene->emitters.bytes(),
+                                  cudaMemcpyDeviceToDevice, st),
+                  "adjoint tables");
+        }
+        adjoint_frame = adjoint_on;
+        last_fp = fp;
+        has_frame = true;
         SceneView s = scene->view(err.p);
         last_stream = st;
         ktimer.n = 0;
@@ -1446,6 +1463,54 @@ int crisb_render_frame(crisb_renderer* r, const crisb_camera* cam, float* out_rg
     return guarded([&] {
         require(r && cam, "null argument");
         r->render(*cam, out_rgb_dev, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int crisb_restir_adjoint_enable(crisb_renderer* r, int on) {
+    return guarded([&] {
+        require(r != nullptr, "null renderer");
+        if (on && r->frame_mats.n != r->scene->mats.n) r->frame_mats.alloc(r->scene->mats.n);
+        if (on && r->frame_emitters.n != r->scene->emitters.n) r->frame_emitters.alloc(r->scene->emitters.n);
+        r->adjoint_on = on != 0;
+    });
+}
+
+namespace {
+void restir_adjoint_check(const crisb_renderer* r) {
+    require(r->has_frame && r->adjoint_frame,
+            "restir adjoint: enable it (crisb_restir_adjoint_enable) before rendering the frame");
+    const crisb_params& p = r->params;
+    require(p.renderer_type == CRISB_RENDERER_CONDITIONAL_RESTIR, "restir adjoint: Conditional ReSTIR only");
+    require(p.gather_n == 1, "restir adjoint: gather_n must be 1");
+    require(p.storage == CRISB_STORAGE_FP32, "restir adjoint: FP32 reservoir storage only");
+    require(p.max_path_len <= 16, "restir adjoint: max_path_len must be <= 16");
+    require(!r->scene->textured, "restir adjoint: textured materials are not differentiated");
+    require(r->scene->num_emitters > 0, "restir adjoint: the scene has no emitters");
+    require(r->frame_mats.n == r->scene->mats.n && r->frame_emitters.n == r->scene->emitters.n,
+            "restir adjoint: table sizes changed");
+}
+}  // namespace
+
+int crisb_restir_adjoint_forward(crisb_renderer* r, float* out_rgb_dev, void* stream) {
+    return guarded([&] {
+        require(r && out_rgb_dev, "null argument");
+        restir_adjoint_check(r);
+        restir_adjoint_forward(r->scene->view(r->err.p), r->frame_mats.p, r->frame_emitters.p,
+                               static_cast<uint32_t>(r->scene->mats.n), r->last_fp, r->bufs(), out_rgb_dev,
+                               static_cast<cudaStream_t>(stream));
+        check(cudaGetLastError(), "restir adjoint forward");
+    });
+}
+
+int crisb_restir_adjoint_backward(crisb_renderer* r, const float* d_image_dev, float* d_materials_dev,
+                                  float* d_emitters_dev, void* stream) {
+    return guarded([&] {
+        require(r && d_image_dev && d_materials_dev && d_emitters_dev, "null argument");
+        restir_adjoint_check(r);
+        restir_adjoint_backward(r->scene->view(r->err.p), r->frame_mats.p, r->frame_emitters.p,
+                                static_cast<uint32_t>(r->scene->mats.n), r->last_fp, r->bufs(), d_image_dev,
+                                d_materials_dev, d_emitters_dev, static_cast<cudaStream_t>(stream));
+        check(cudaGetLastError(), "restir adjoint backward");
     });
 }
 

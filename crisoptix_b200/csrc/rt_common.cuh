@@ -253,6 +253,14 @@ RT_HD bool fl_valid(uint32_t f) { return (f & kFlagValid) != 0; }
 RT_HD bool fl_nee(uint32_t f) { return (f & kFlagNee) != 0; }
 RT_HD uint32_t fl_set_valid(uint32_t f, bool v) { return v ? (f | kFlagValid) : (f & ~kFlagValid); }
 RT_HD uint32_t fl_set_nee(uint32_t f, bool v) { return v ? (f | kFlagNee) : (f & ~kFlagNee); }
+// Suffix flags bits 24-31: the loop index of the suffix vertex at which the
+// reconnection vertex was chosen (the vertex itself, or the NEE vertex whose
+// light ray found it).  The reference's records have no such field (its
+// reconIdx of a suffix holds the prefix length); with it the path after the
+// reconnection vertex can be re-traced from the suffix's seed, since every
+// suffix vertex before it took one NEE draw and three BRDF-sampling draws.
+RT_HD uint32_t fl_recon_vert(uint32_t f) { return f >> 24; }
+RT_HD uint32_t fl_set_recon_vert(uint32_t f, uint32_t v) { return (f & 0x00FFFFFFu) | ((v & 0xFFu) << 24); }
 
 struct Prefix {
     uint64_t rng;

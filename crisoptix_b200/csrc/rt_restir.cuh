@@ -276,6 +276,7 @@ RT_D void trace_suffix(const SceneView& s, const FrameParams& fp, Suffix& suffix
                 if (!rc.valid) return;
                 suffix.recon = rc.pack();
                 suffix.flags = fl_set_recon(suffix.flags, fl_len(suffix.flags));
+                suffix.flags = fl_set_recon_vert(suffix.flags, vi);
                 suffix.rod = splat(0.0f);
                 post = true;
             }
@@ -297,6 +298,7 @@ RT_D void trace_suffix(const SceneView& s, const FrameParams& fp, Suffix& suffix
         if (!post && can_recon) {
             suffix.recon = it.pack();
             suffix.flags = fl_set_recon(suffix.flags, fl_len(prefix.flags));
+            suffix.flags = fl_set_recon_vert(suffix.flags, vi);
             suffix.rod = bs.dir;
             post = true;
         }

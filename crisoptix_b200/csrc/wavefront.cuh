@@ -259,6 +259,7 @@ RT_D int suf_vertex(const SceneView& s, const FrameParams& fp, Suffix& suf, WfPa
     if (!post && can_recon) {
         suf.recon = it.pack();
         suf.flags = fl_set_recon(suf.flags, pre_len);
+        suf.flags = fl_set_recon_vert(suf.flags, fl_len(suf.flags));  // the loop index vi
         suf.rod = bs.dir;
         post = true;
         set |= kSetRecon;
@@ -325,6 +326,7 @@ RT_D int suf_on_recon(const SceneView& s, Suffix& suf, WfPath& w, uint32_t& set)
     set |= kSetRecon;
     suf.recon = rc.pack();
     suf.flags = fl_set_recon(suf.flags, fl_len(suf.flags));
+    suf.flags = fl_set_recon_vert(suf.flags, fl_len(suf.flags) - 1);  // the NEE vertex
     suf.rod = splat(0.0f);
     return suf_finish_nee(suf, w, f3(w.nee_brdf));
 }

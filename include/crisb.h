@@ -254,7 +254,9 @@ typedef struct crisb_suffix_rec {
     uint64_t rng;
     crisb_hit_rec recon;
     crisb_hit_rec last_prefix;
-    uint32_t flags; /* 0:8 length, 8:16 reconIdx, bit16 valid */
+    uint32_t flags; /* 0:8 length, 8:16 reconIdx, bit16 valid; 24:32 loop index of the
+                       suffix vertex that chose the reconnection vertex (not in the
+                       reference's SuffixPath; read by the resampled-path adjoint) */
     float f[3];
     float post_recon_f[3];
     float p;
@@ -300,7 +302,7 @@ typedef struct crisb_prefix_res16_rec { /* 80 bytes */
 
 typedef struct crisb_suffix_res16_rec { /* 64 bytes */
     uint64_t rng;
-    uint32_t flags;
+    uint32_t flags; /* as crisb_suffix_rec.flags */
     float p;
     crisb_hit16_rec recon;
     crisb_hit16_rec last_prefix;
@@ -548,6 +550,38 @@ int crisb_adjoint_forward(crisb_adjoint* a, const crisb_camera* cam, uint64_t fr
                           void* stream);
 int crisb_adjoint_backward(crisb_adjoint* a, const crisb_camera* cam, uint64_t frame, const float* d_image_dev,
                            float* d_materials_dev, float* d_emitters_dev, void* stream);
+
+/* Path-replay adjoint of the resampled estimator (survey config INV, north
+ * star "re-trace each pixel's selected resampled paths from their stored
+ * seeds").  The estimator is the final gather of the frame `r` rendered last
+ * (FinalGatherCanon, shader/final_gather.cu:69-188): per pixel the canonical
+ * path and each valid neighbour's suffix shifted onto the canonical prefix,
+ * combined with pairwise MIS.  Frozen at the material and emitter tables that
+ * frame was rendered with: random decisions, sampled directions, sampling
+ * pdfs, path and shift validity, neighbour lists, MIS weights, the
+ * neighbours' unbiased contribution weights and the reconnection Jacobians.
+ * Evaluated at the scene's current tables: every BRDF value along the paths,
+ * emitter colours and emissions.  Each factor is re-traced from stored state
+ * (the gather's canonical prefix and suffix, each neighbour sample's seed), no
+ * tape.  At the frame's tables it equals the frame's gather value; for any
+ * tables it is unbiased for the expected image at those tables as far as the
+ * frame's estimator is, so its gradient is an unbiased gradient estimate.
+ * crisb_restir_adjoint_enable(r, 1) must precede the frame (each frame then
+ * copies the tables it uses: 48 bytes per material, 20 per emitter).
+ * crisb_restir_adjoint_forward writes the estimator at the current tables into
+ * out_rgb_dev (W*H*3 floats, before any accumulation blend);
+ * crisb_restir_adjoint_backward ADDS dLoss/dparameter at the frame's tables,
+ * given d_image_dev = dLoss/dimage (W*H*3), into d_materials_dev (7 floats per
+ * material: diffuse rgb, roughness, emission rgb) and d_emitters_dev (3 floats
+ * per emitter: colour).  Both read the frame's buffers: run them on the
+ * frame's stream (or after it) and before the next frame.  Requires
+ * CRISB_RENDERER_CONDITIONAL_RESTIR, gather_n 1, FP32 storage, an untextured
+ * scene and max_path_len <= 16.  No counterpart in the reference, which has no
+ * differentiable renderer. */
+int crisb_restir_adjoint_enable(crisb_renderer* r, int on);
+int crisb_restir_adjoint_forward(crisb_renderer* r, float* out_rgb_dev, void* stream);
+int crisb_restir_adjoint_backward(crisb_renderer* r, const float* d_image_dev, float* d_materials_dev,
+                                  float* d_emitters_dev, void* stream);
 
 /* Batched views (survey config MV: many cameras of uneven resolution).  A
  * batch holds renderers of one device -- one per view, each with its own

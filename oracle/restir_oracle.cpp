@@ -324,6 +324,11 @@ struct SuffixPath {
     void SetReconIdx(uint32_t r) { flags &= ~0xFF00u; flags |= (r & 0xFFu) << 8u; }
     bool IsValid() const { return (flags & (1u << 16u)) != 0; }
     void SetValid(bool v) { flags &= ~(1u << 16u); if (v) flags |= 1u << 16u; }
+    // bits 24-31 (not in the reference's SuffixPath.h): the loop index of the
+    // suffix vertex at which the reconnection vertex was chosen, so that the
+    // path after it can be re-traced from `rng` by a path-replay adjoint
+    uint32_t GetReconVert() const { return flags >> 24u; }
+    void SetReconVert(uint32_t v) { flags &= 0x00FFFFFFu; flags |= (v & 0xFFu) << 24u; }
 };
 
 // Reservoir, include/graph/restir/Reservoir.h:8-51
@@ -1360,6 +1365,7 @@ struct oracle_ctx {
                     if (!reconInt.valid) return;
                     suffix.reconInt = reconInt.Pack();
                     suffix.SetReconIdx(suffix.GetLength());
+                    suffix.SetReconVert(vertIdx);
                     suffix.reconOutDir = vec3(0.0f);
                     postRecon = true;
                 }
@@ -1382,6 +1388,7 @@ struct oracle_ctx {
             if (!postRecon && intCanRecon) {
                 suffix.reconInt = interaction.Pack();
                 suffix.SetReconIdx(prefix.GetLength());
+                suffix.SetReconVert(vertIdx);
                 suffix.reconOutDir = brdfSampleResult.outDir;
                 postRecon = true;
             }
