@@ -260,7 +260,10 @@ def comparison_arms(sc, cam, W: int, H: int, p, ppp: int, value: float, ms_per_f
         reuse, scored against the same reference;
       - 16 uneven views: the plain form (FP32 storage, views one after another)
         against the batched form (FP16 storage, one CUDA graph per frame with
-        a branch per view), and their ratio of resampled paths/s."""
+        a branch per view), and their ratio of resampled paths/s;
+      - the path-replay adjoint of the resampled estimator on the same
+        workload: one backward pass (dLoss/dimage = 1 everywhere) and one
+        evaluation of the frozen estimator, beside the frame time."""
     import torch
 
     from crisoptix_b200 import Renderer, _abi, quality, scenes
@@ -296,6 +299,7 @@ def comparison_arms(sc, cam, W: int, H: int, p, ppp: int, value: float, ms_per_f
     qrp = copy.copy(p)
     qrp.motion_mode = _abi.MOTION_REPROJECT
     q32rp = quality.score(sc, W, H, cam_of, qrp, 31, args.arm_ref_spp, ref=ref)
+    adj = adjoint_time(sc, cam, W, H, p, args.warmup, 3)
     mv_plain = multiview_time(_abi.STORAGE_FP32, False, args.arm_mv_steps, 2)
     mv_batch = multiview_time(_abi.STORAGE_FP16, True, args.arm_mv_steps, 2)
     keep = ("relmse", "relmse_trimmed_0.1pct")
@@ -318,6 +322,7 @@ def comparison_arms(sc, cam, W: int, H: int, p, ppp: int, value: float, ms_per_f
         "multiview_plain_fp32": dict(mv_plain, steps=args.arm_mv_steps),
         "multiview_batched_fp16": dict(mv_batch, steps=args.arm_mv_steps),
         "batched_fp16_over_plain_fp32": mv_batch["value"] / mv_plain["value"],
+        "adjoint_fp32": adj,
         "unit": UNIT,
     }
 
@@ -522,6 +527,52 @@ def run_crisb(args):
     if arms is not None:
         line["arms"] = arms
     print(json.dumps(line), flush=True)
+
+
+def adjoint_time(sc, cam, W: int, H: int, p, warmup: int, steps: int) -> dict:
+    """Device time of the resampled estimator's adjoint (crisb_restir_adjoint_*)
+    on the workload's last frame: the backward pass for dLoss/dimage = 1 and
+    the frozen estimator's evaluation, each averaged over `steps` calls after
+    a frame of the orbit, beside that frame's time."""
+    import torch
+
+    from crisoptix_b200 import Renderer, scenes
+
+    r = Renderer(W, H, sc, p)
+    r.restir_adjoint_enable(True)
+    out = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
+    ones = torch.ones(W * H * 3, dtype=torch.float32, device="cuda")
+    g_mat = torch.zeros(len(sc.desc.materials) * 7, dtype=torch.float32, device="cuda")
+    g_em = torch.zeros(len(sc.desc.emitters) * 3, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    with torch.cuda.stream(stream):
+        for f in range(warmup):
+            r.launch_frame(scenes.orbit_camera(cam, f, 60), out.data_ptr(), sptr)
+        ev[0].record(stream)
+        r.launch_frame(scenes.orbit_camera(cam, warmup, 60), out.data_ptr(), sptr)
+        ev[1].record(stream)
+        r.restir_adjoint_backward(ones.data_ptr(), g_mat.data_ptr(), g_em.data_ptr(), sptr)  # warm-up call
+        ev[2].record(stream)
+        for _ in range(steps):
+            r.restir_adjoint_backward(ones.data_ptr(), g_mat.data_ptr(), g_em.data_ptr(), sptr)
+        ev[3].record(stream)
+        ev[4].record(stream)
+        for _ in range(steps):
+            r.restir_adjoint_forward(out.data_ptr(), sptr)
+        ev[5].record(stream)
+    torch.cuda.synchronize()
+    r.check_device_errors()
+    frame_ms = ev[0].elapsed_time(ev[1])
+    back_ms = ev[2].elapsed_time(ev[3]) / steps
+    fwd_ms = ev[4].elapsed_time(ev[5]) / steps
+    nonzero = int((g_mat != 0).sum()) + int((g_em != 0).sum())
+    del r
+    return {"ms_backward": back_ms, "ms_forward": fwd_ms, "ms_frame": frame_ms,
+            "backward_over_frame": back_ms / frame_ms, "gradient_entries_nonzero": nonzero,
+            "note": "crisb_restir_adjoint_backward with dLoss/dimage = 1 (7 floats per material, 3 per emitter) "
+                    "and crisb_restir_adjoint_forward on the last frame of the orbit, FP32 storage"}
 
 
 def multiview_time(storage: int, batched: bool, steps: int, warmup: int, motion: int = 0) -> dict:

@@ -215,9 +215,11 @@ RT_D void seg_suffix(const RAdjView& a, const FrameParams& fp, const Suffix& cs,
 // T_n: the throughput of the shift of `src` onto the vertex `dst_last`
 // (suffix CalcCurrContribInOtherDomain, suffix_reuse.h:10-108) before its
 // postReconF; false where the frame's shift failed (its value was zero).
-// Validity uses the frozen tables, as the frame did.
+// Validity uses the frozen tables, as the frame did; `passed`: the frame's
+// shift value was nonzero, so its occlusion and pdf checks passed and are not
+// repeated (a zero value may be a failure: those shifts run every check).
 template <bool kGrad>
-RT_D bool seg_shift(const RAdjView& a, const Suffix& src, const Isect& dst_last, Seg<kGrad>& sg) {
+RT_D bool seg_shift(const RAdjView& a, const Suffix& src, const Isect& dst_last, bool passed, Seg<kGrad>& sg) {
     sg.init();
     if (!fl_valid(src.flags) || !dst_last.valid) return false;
     if (!unpack(a.eval, src.last_prefix).valid) return false;
@@ -229,7 +231,7 @@ RT_D bool seg_shift(const RAdjView& a, const Suffix& src, const Isect& dst_last,
     for (int i = 0; i < nrep; ++i) {
         srng.next_float();
         const BrdfSample bs = brdf_sample(a.samp, cur, srng);
-        if (bs.pdf <= 0.0f) return false;
+        if (!passed && bs.pdf <= 0.0f) return false;
         uint32_t mi;
         sg.mul_brdf(grad_at(a, cur, bs.dir, mi), mi);
         const V3 pos = cur.pos;
@@ -239,15 +241,16 @@ RT_D bool seg_shift(const RAdjView& a, const Suffix& src, const Isect& dst_last,
     const V3 rv = src_recon.pos - cur.pos;
     const float rlen = length(rv);
     const V3 rdir = normalize(rv);
-    if (nonfinite(rdir)) return false;
-    if (occluded(a.eval, cur.pos, rdir, 1e-3f, rlen)) return false;
-    if (brdf_eval(a.samp, cur, rdir).pdf <= 0.0f) return false;
+    if (!passed) {
+        if (nonfinite(rdir)) return false;
+        if (occluded(a.eval, cur.pos, rdir, 1e-3f, rlen)) return false;
+        if (brdf_eval(a.samp, cur, rdir).pdf <= 0.0f) return false;
+    }
     uint32_t m1;
     sg.mul_brdf(grad_at(a, cur, rdir, m1), m1);
     if (fl_recon(src.flags) < fl_len(src.flags)) {
         src_recon.dir = rdir;
-        if (is_zero(src.rod)) return false;
-        if (brdf_eval(a.samp, src_recon, src.rod).pdf <= 0.0f) return false;
+        if (!passed && (is_zero(src.rod) || brdf_eval(a.samp, src_recon, src.rod).pdf <= 0.0f)) return false;
         uint32_t m2;
         sg.mul_brdf(grad_at(a, src_recon, src.rod, m2), m2);
     }
@@ -393,8 +396,9 @@ RT_D V3 gather_pixel(const RAdjView& a, const FrameParams& fp, const Bufs& b, ui
             const float4 o0 = sh[2 * n];
             float nmis = mis_neighbor(xyz(o0), ns.f, o0.w, K, 1.0f, nconf);
             if (nonfinite(nmis)) nmis = 0.0f;
+            if (nmis * nwsum * o0.w == 0.0f) continue;  // no weight, no gradient
             const V3 wn = dl * cp.f * (nmis * nwsum * o0.w / (pp * E * D));
-            if (!seg_shift(a, ns, dst_last, sg)) continue;
+            if (!seg_shift(a, ns, dst_last, !is_zero(xyz(o0)), sg)) continue;
             sg.emit(wn * ns.prf, sink);
             const V3 tn = sg.val;
             seg_post(a, fp, ns, sg);
@@ -416,7 +420,7 @@ RT_D V3 gather_pixel(const RAdjView& a, const FrameParams& fp, const Bufs& b, ui
         float nmis = mis_neighbor(xyz(o0), ns.f, o0.w, K, 1.0f, nconf);
         if (nonfinite(nmis)) nmis = 0.0f;
         V3 fshift = splat(0.0f);
-        if (seg_shift(a, ns, dst_last, sg)) {
+        if (seg_shift(a, ns, dst_last, !is_zero(xyz(o0)), sg)) {
             const V3 tn = sg.val;
             seg_post(a, fp, ns, sg);
             fshift = tn * sg.val;
