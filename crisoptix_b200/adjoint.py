@@ -388,6 +388,123 @@ def torch_equal(a, b) -> bool:
     return bool(torch.equal(a.double(), b.double()))
 
 
+def inverse_steps(scene, desc, cams: Sequence[Camera], width: int, height: int, params: _abi.Params,
+                  target_mats: np.ndarray, target_rgb: np.ndarray, start_mats: np.ndarray, start_rgb: np.ndarray,
+                  steps: int = 10, lr: float = 0.02, estimator: str = "pt", frames: int = 3,
+                  free=("diffuse", "roughness", "radiance")) -> dict:
+    """Inverse-rendering steps: gradient descent with a backtracking line
+    search (steps preconditioned by each parameter's size; the first trial
+    moves the steepest parameter by `lr`) on the groups `free` of the parameters the
+    adjoints differentiate (every material's diffuse albedo and GGX roughness,
+    every emitter's radiance; the other groups stay at the target's values),
+    minimising sum of (image - target)^2 over the views.  The
+    estimator is frozen at the start parameters -- the path tracer's sampling
+    (``PtAdjoint``) or the resampled estimator's prepared frames
+    (``RestirAdjoint``, `frames` Conditional ReSTIR frames) -- and the target
+    is the same frozen estimator at the target parameters, so the loss is a
+    smooth function of the parameters.  Returns the loss before each step and
+    after the last, and the parameters' mean absolute relative error to the
+    target before and after: over all of them, and over the quarter with the
+    largest first gradients (scaled to the parameter), the ones the images
+    determine most."""
+    em_mats = emitter_materials(desc)
+    set_materials(scene, start_mats)
+    set_emitter_colors(scene, start_rgb)
+    if estimator == "restir":
+        adj = RestirAdjoint(scene, width, height, params, len(cams))
+        adj.prepare(cams, frames)
+        render, grad = adj.render, adj.gradient
+    else:
+        adj = PtAdjoint(scene, width, height, params)
+
+        def render():
+            return adj.render(cams)
+
+        def grad(d):
+            return adj.gradient(cams, d)
+
+    set_materials(scene, target_mats)
+    set_emitter_colors(scene, target_rgb)
+    target = render().double()
+    em = np.array([m for m in em_mats], np.int64)
+    surf = np.array([m for m in range(len(start_mats)) if m not in set(em_mats)], np.int64)  # not emitters
+    ggx = surf[start_mats["roughness"][surf] < 1.0]
+
+    def pack(mats, rgb):
+        return np.concatenate([mats["diffuse"][surf].reshape(-1), mats["roughness"][ggx], rgb.reshape(-1)])
+
+    def unpack(x):
+        mats, rgb = start_mats.copy(), start_rgb.copy()
+        nd, nr = 3 * len(surf), len(ggx)
+        mats["diffuse"][surf] = np.clip(x[:nd].reshape(-1, 3), 0.01, 0.99)
+        mats["roughness"][ggx] = np.clip(x[nd:nd + nr], 0.02, 1.0)
+        rgb = np.maximum(x[nd + nr:].reshape(-1, 3), 0.0).astype(np.float32)
+        for e, m in enumerate(em):
+            if m >= 0:
+                mats["emission"][m] = rgb[e]
+        return mats, rgb
+
+    # groups not optimised start (and stay) at the target's values
+    sel = np.concatenate([np.full(3 * len(surf), "diffuse" in free), np.full(len(ggx), "roughness" in free),
+                          np.full(3 * len(em), "radiance" in free)])
+    x_target = pack(target_mats, target_rgb).astype(np.float64)
+    x = np.where(sel, pack(start_mats, start_rgb), x_target)
+    scale = np.maximum(np.abs(x), 1e-2)  # steps relative to each parameter's size
+    losses = []
+    rel_err = lambda v: np.abs(v - x_target) / np.maximum(np.abs(x_target), 1e-2)  # noqa: E731
+    err0 = rel_err(x)
+    observed = None
+
+    def loss_at(v):
+        mats, rgb = unpack(v)
+        set_materials(scene, mats)
+        set_emitter_colors(scene, rgb)
+        img = render().double()
+        return float(((img - target) ** 2).sum()), img
+
+    cur, img = loss_at(x)
+    losses.append(cur)
+    alpha = None
+    for it in range(steps):
+        g_mat, g_em = grad((2.0 * (img - target)).float())
+        g_mat = g_mat.double().cpu().numpy()
+        g_em = g_em.double().cpu().numpy()
+        g_rad = g_em.copy()
+        for e, m in enumerate(em):
+            if m >= 0:
+                g_rad[e] += g_mat[m, 4:7]
+        g = np.concatenate([g_mat[surf, 0:3].reshape(-1), g_mat[ggx, 3], g_rad.reshape(-1)]) * scale * sel
+        if observed is None:
+            observed = sel & (np.abs(g) >= np.quantile(np.abs(g[sel]), 0.75))
+        gg = float((g * g).sum())
+        if gg == 0.0:
+            break
+        if alpha is None:
+            alpha = lr / float(np.abs(g).max())  # the first trial moves the steepest parameter by lr
+        else:
+            alpha *= 2.0
+        # backtracking (Armijo) along the preconditioned gradient
+        for _ in range(20):
+            trial = pack(*unpack(x - alpha * scale * g))
+            val, timg = loss_at(trial)
+            if val <= cur - 1e-4 * alpha * gg:
+                break
+            alpha *= 0.5
+        else:
+            break
+        x, cur, img = trial, val, timg
+        losses.append(cur)
+    set_materials(scene, start_mats)
+    set_emitter_colors(scene, start_rgb)
+    err1 = rel_err(x)
+    if observed is None:
+        observed = sel
+    return {"losses": losses, "param_rel_err_start": float(err0[sel].mean()),
+            "param_rel_err_end": float(err1[sel].mean()), "free": list(free), "num_free": int(sel.sum()),
+            "observed_rel_err_start": float(err0[observed].mean()), "observed_rel_err_end": float(err1[observed].mean()),
+            "num_params": int(len(x)), "num_observed": int(observed.sum()), "estimator": estimator}
+
+
 def inverse_config_params(desc, num_params: int = 20, seed: int = 3, min_roughness: int = 0) -> List[Param]:
     """`num_params` random parameters of the inverse-rendering config: sphere
     albedos (materials 1..64, 3 channels), GGX roughnesses (odd spheres) and
@@ -455,6 +572,11 @@ def main(argv=None):
     ap.add_argument("--estimator", default="pt", choices=["pt", "restir"],
                     help="pt: the path tracer; restir: the final gather's resampled estimator")
     ap.add_argument("--frames", type=int, default=3, help="restir: frames rendered before the check")
+    ap.add_argument("--inverse-steps", type=int, default=0,
+                    help="instead of the check, run this many Adam steps on all parameters and print the losses")
+    ap.add_argument("--lr", type=float, default=0.02, help="Adam step, relative to each parameter")
+    ap.add_argument("--free", default="diffuse,roughness,radiance",
+                    help="inverse steps: the parameter groups optimised (the rest stay at the target)")
     a = ap.parse_args(argv)
     if a.small:
         desc, _ = scenes.sphere_room(num_spheres=12, subdiv=2, num_emitters=12, seed=4)
@@ -467,6 +589,15 @@ def main(argv=None):
     tm, trgb, sm, srgb = perturbed_start(desc, seed=a.seed)
     chk = inverse_config_params(desc, a.params, a.seed, a.min_roughness)
     t0 = time.time()
+    if a.inverse_steps:
+        q = restir_params(sc.scene_size, a.seed) if a.estimator == "restir" else p
+        r = inverse_steps(sc, desc, cams, a.res, a.res, q, tm, trgb, sm, srgb, steps=a.inverse_steps, lr=a.lr,
+                          estimator=a.estimator, frames=a.frames, free=tuple(a.free.split(",")))
+        torch.cuda.synchronize()
+        print(json.dumps({"config": f"inverse rendering: {a.views} views {a.res}x{a.res}, {len(desc.materials)} "
+                                    f"materials, {len(desc.emitters)} emitters, Adam lr {a.lr}, seed {a.seed}",
+                          **r, "seconds": time.time() - t0}))
+        return
     if a.estimator == "restir":
         p = restir_params(sc.scene_size, a.seed)
         r = restir_fd_check(sc, desc, cams, a.res, a.res, p, tm, trgb, sm, srgb, chk, eps=a.eps, frames=a.frames)

@@ -160,3 +160,22 @@ def test_canonical_gradient_matches_the_path_tracer_gradient(cuda_device):
     tight = np.sqrt(sp[top] ** 2 + sr[top] ** 2) < 0.02 * np.abs(mp[top])
     assert tight.sum() >= 6, (mp[top], sp[top], sr[top])
     assert np.all(np.abs(mr[top][tight] / mp[top][tight] - 1.0) < 0.08), (mp[top], mr[top])
+
+
+@pytest.mark.parametrize("estimator", ["pt", "restir"])
+def test_inverse_rendering_steps_reduce_the_loss(cuda_device, estimator):
+    """Adam on every diffuse albedo of the 12-sphere room (start perturbed by
+    N(0, 0.1) relative; roughness and radiance at the target, which removes
+    the albedo-radiance scale ambiguity), each step one adjoint backward
+    pass: the loss against the target images falls, and the albedos the
+    images determine (the quarter with the largest first gradients) move
+    toward the target."""
+    desc, cam = _room()
+    sc = Scene(desc)
+    tm, trgb, sm, srgb = adjoint.perturbed_start(desc, seed=3)
+    cams = [cam, scenes.orbit_camera(cam, 15, 60)]
+    p = _params(desc) if estimator == "restir" else large_config_params(scene_size_of(desc), max_path_len=6)
+    r = adjoint.inverse_steps(sc, desc, cams, 96, 64, p, tm, trgb, sm, srgb, steps=15, lr=0.02,
+                              estimator=estimator, free=("diffuse",))
+    assert r["losses"][-1] < 0.5 * r["losses"][0], r
+    assert r["observed_rel_err_end"] < r["observed_rel_err_start"], r
