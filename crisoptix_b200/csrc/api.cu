@@ -853,6 +853,7 @@ struct crisb_renderer {
     bool adjoint_on = false, adjoint_frame = false, has_frame = false;
     DevBuf<crisb_material> frame_mats;
     DevBuf<crisb_emitter> frame_emitters;
+    DevBuf<float4> adj_pairs;  // the adjoint's per (pixel, neighbour) scratch
     FrameParams last_fp{};
     // optional sRGB bytes of each frame (ToneMapping after LaunchFrame,
     // src/main.cpp:122-127), written by a last kernel of the frame
@@ -1489,6 +1490,11 @@ void restir_adjoint_check(const crisb_renderer* r) {
     require(r->frame_mats.n == r->scene->mats.n && r->frame_emitters.n == r->scene->emitters.n,
             "restir adjoint: table sizes changed");
 }
+float4* restir_adjoint_pairs(crisb_renderer* r) {
+    const size_t need = static_cast<size_t>(r->last_fp.width) * r->last_fp.height * std::max(1u, r->last_fp.k);
+    if (r->adj_pairs.n < need) r->adj_pairs.alloc(need);
+    return r->adj_pairs.p;
+}
 }  // namespace
 
 int crisb_restir_adjoint_forward(crisb_renderer* r, float* out_rgb_dev, void* stream) {
@@ -1496,8 +1502,8 @@ int crisb_restir_adjoint_forward(crisb_renderer* r, float* out_rgb_dev, void* st
         require(r && out_rgb_dev, "null argument");
         restir_adjoint_check(r);
         restir_adjoint_forward(r->scene->view(r->err.p), r->frame_mats.p, r->frame_emitters.p,
-                               static_cast<uint32_t>(r->scene->mats.n), r->last_fp, r->bufs(), out_rgb_dev,
-                               static_cast<cudaStream_t>(stream));
+                               static_cast<uint32_t>(r->scene->mats.n), r->last_fp, r->bufs(), restir_adjoint_pairs(r),
+                               out_rgb_dev, static_cast<cudaStream_t>(stream));
         check(cudaGetLastError(), "restir adjoint forward");
     });
 }
@@ -1508,8 +1514,8 @@ int crisb_restir_adjoint_backward(crisb_renderer* r, const float* d_image_dev, f
         require(r && d_image_dev && d_materials_dev && d_emitters_dev, "null argument");
         restir_adjoint_check(r);
         restir_adjoint_backward(r->scene->view(r->err.p), r->frame_mats.p, r->frame_emitters.p,
-                                static_cast<uint32_t>(r->scene->mats.n), r->last_fp, r->bufs(), d_image_dev,
-                                d_materials_dev, d_emitters_dev, static_cast<cudaStream_t>(stream));
+                                static_cast<uint32_t>(r->scene->mats.n), r->last_fp, r->bufs(), restir_adjoint_pairs(r),
+                                d_image_dev, d_materials_dev, d_emitters_dev, static_cast<cudaStream_t>(stream));
         check(cudaGetLastError(), "restir adjoint backward");
     });
 }

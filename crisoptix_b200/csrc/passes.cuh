@@ -161,13 +161,15 @@ void adjoint_backward(const SceneView& eval, const crisb_material* sample_mats, 
                       const FrameParams& fp, const float* d_img, float* g_mat, float* g_em, cudaStream_t st);
 // path-replay adjoint of the final gather's resampled estimator of the last
 // frame (restir_adjoint.cu): `b` holds that frame's state, frame_mats and
-// frame_emitters the tables it was rendered with
+// frame_emitters the tables it was rendered with; `pairs` is scratch of
+// width * height * k float4 (one per pixel and final-gather neighbour)
 void restir_adjoint_forward(const SceneView& eval, const crisb_material* frame_mats,
                             const crisb_emitter* frame_emitters, uint32_t num_mats, const FrameParams& fp,
-                            const Bufs& b, float* out, cudaStream_t st);
+                            const Bufs& b, float4* pairs, float* out, cudaStream_t st);
 void restir_adjoint_backward(const SceneView& eval, const crisb_material* frame_mats,
                              const crisb_emitter* frame_emitters, uint32_t num_mats, const FrameParams& fp,
-                             const Bufs& b, const float* d_img, float* g_mat, float* g_em, cudaStream_t st);
+                             const Bufs& b, float4* pairs, const float* d_img, float* g_mat, float* g_em,
+                             cudaStream_t st);
 // sRGB tone mapping of n float RGB pixels to bytes (tonemap.cu)
 cudaError_t launch_tonemap_srgb8(const float* rgb, uint8_t* out, uint32_t n, cudaStream_t st);
 // the kernel's step table: t256[k] smallest float with byte >= k, and c_max

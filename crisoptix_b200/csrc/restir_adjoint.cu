@@ -319,10 +319,44 @@ RT_D void seg_post(const RAdjView& a, const FrameParams& fp, const Suffix& src, 
     }
 }
 
-// One pixel: kGrad false returns the frozen estimator's value at theta;
-// kGrad true adds dl . dL/dtheta at theta0 to the sink and returns zero.
+// Neighbour terms run as threads of their own, one per (pixel, neighbour
+// slot), neighbour-major (thread t = n * P + i): a warp replays the n-th
+// neighbours of 32 adjacent pixels instead of one thread replaying all of a
+// pixel's neighbours in turn (3 of 32 lanes busy).  The pair buffer holds per
+// (pixel, neighbour) the term's value at theta (forward: the pair kernel runs
+// first, the pixel kernel adds the terms in the frame's order) or its weight
+// dLoss/d(shifted throughput) (backward: the pixel kernel runs first), with
+// w = 1 where the frame added the term and 0 elsewhere.
+
+// what the frame's gather read for neighbour n of pixel i (K valid neighbours)
+struct NeighTerm {
+    uint32_t np;
+    float nmis, nwsum, jac;
+    V3 f0;      // the shifted value at theta0
+    bool used;  // the frame added the term (finite)
+};
+
+RT_D NeighTerm neigh_term(const FrameParams& fp, const Bufs& b, uint32_t i, uint32_t n, float K) {
+    NeighTerm t;
+    t.np = b.neighbors[static_cast<size_t>(i) * fp.k + n].pixel;
+    const float4 o0 = b.shift_out[static_cast<size_t>(i) * b.slots + 2 * n];
+    t.f0 = xyz(o0);
+    t.jac = o0.w;
+    t.nwsum = sres_wsum(b.sres_cur, t.np);
+    float nmis = mis_neighbor(t.f0, sres_f(b.sres_cur, t.np), t.jac, K, 1.0f, sres_conf(b.sres_cur, t.np));
+    if (nonfinite(nmis)) nmis = 0.0f;
+    t.nmis = nmis;
+    t.used = !nonfinite(nmis * t.f0 * t.nwsum * t.jac);
+    return t;
+}
+
+// One pixel: kGrad false returns the frozen estimator's value at theta, its
+// neighbour terms read from `pairs`; kGrad true adds dl . dL/dtheta of the
+// canonical factors at theta0 to the sink, writes the neighbour terms'
+// weights into `pairs` and returns zero.
 template <bool kGrad>
-RT_D V3 gather_pixel(const RAdjView& a, const FrameParams& fp, const Bufs& b, uint32_t i, V3 dl, GradSink* sink) {
+RT_D V3 gather_pixel(const RAdjView& a, const FrameParams& fp, const Bufs& b, uint32_t i, V3 dl, GradSink* sink,
+                     float4* pairs) {
     if (b.canon_prefix[i].primary.prim == CRISB_INVALID_PRIM) return splat(0.0f);  // no gather ran
     const Prefix cp = ld_prefix_v(b.gather_cp[i]);
     if (!fl_valid(cp.flags)) return splat(0.0f);
@@ -351,7 +385,7 @@ RT_D V3 gather_pixel(const RAdjView& a, const FrameParams& fp, const Bufs& b, ui
         return fpv * sg.val / (pp * ps);
     }
     // the frozen weights, from what k_gather_combine read
-    const uint32_t k = fp.k;
+    const uint32_t P = pixel_count(fp);
     const uint32_t count = b.neigh_count[i];
     const uint32_t vflags = b.pass_flags[i];
     const uint32_t nvalid = __popc(vflags);
@@ -360,21 +394,12 @@ RT_D V3 gather_pixel(const RAdjView& a, const FrameParams& fp, const Bufs& b, ui
     const float4* sh = b.shift_out + static_cast<size_t>(i) * b.slots;
     V3 s0 = splat(0.0f);
     float canon_mis = 1.0f;
-    uint32_t use = 0;  // terms the frame added
     for (uint32_t n = 0; n < count; ++n) {
         if (!(vflags & (1u << n))) continue;
-        const uint32_t np_ = b.neighbors[static_cast<size_t>(i) * k + n].pixel;
-        const V3 nf = sres_f(b.sres_cur, np_);
-        const float nconf = sres_conf(b.sres_cur, np_), nwsum = sres_wsum(b.sres_cur, np_);
-        const float4 o0 = sh[2 * n], o1 = sh[2 * n + 1];
-        float nmis = mis_neighbor(xyz(o0), nf, o0.w, K, 1.0f, nconf);
-        if (nonfinite(nmis)) nmis = 0.0f;
-        const V3 contrib = nmis * xyz(o0) * nwsum * o0.w;
-        if (!nonfinite(contrib)) {
-            s0 = s0 + contrib;
-            use |= 1u << n;
-        }
-        canon_mis += mis_canonical(cs.f, xyz(o1), o1.w, K, 1.0f, nconf);
+        const NeighTerm t = neigh_term(fp, b, i, n, K);
+        if (t.used) s0 = s0 + t.nmis * t.f0 * t.nwsum * t.jac;
+        const float4 o1 = sh[2 * n + 1];
+        canon_mis += mis_canonical(cs.f, xyz(o1), o1.w, K, 1.0f, sres_conf(b.sres_cur, t.np));
     }
     {
         V3 g0 = s0 * cp.f / pp;
@@ -382,27 +407,18 @@ RT_D V3 gather_pixel(const RAdjView& a, const FrameParams& fp, const Bufs& b, ui
         const V3 r0 = (g0 + (cp.f * cs.f / (pp * ps)) * canon_mis) / D;
         if (nonfinite(r0)) return splat(0.0f);  // the frame stored zero
     }
-    const Isect dst_last = unpack(a.eval, cs.last_prefix);
     if (kGrad) {
         seg_prefix(a, fp, cp, sg);
         sg.emit(dl * ((s0 / pp) / E + (cs.f / (pp * ps)) * canon_mis) / D, sink);
         seg_suffix(a, fp, cs, sg);
         sg.emit(dl * (cp.f / (pp * ps)) * canon_mis / D, sink);
         for (uint32_t n = 0; n < count; ++n) {
-            if (!(use & (1u << n))) continue;
-            const uint32_t np_ = b.neighbors[static_cast<size_t>(i) * k + n].pixel;
-            const Suffix ns = ld_sres(b.sres_cur, np_).s;
-            const float nconf = sres_conf(b.sres_cur, np_), nwsum = sres_wsum(b.sres_cur, np_);
-            const float4 o0 = sh[2 * n];
-            float nmis = mis_neighbor(xyz(o0), ns.f, o0.w, K, 1.0f, nconf);
-            if (nonfinite(nmis)) nmis = 0.0f;
-            if (nmis * nwsum * o0.w == 0.0f) continue;  // no weight, no gradient
-            const V3 wn = dl * cp.f * (nmis * nwsum * o0.w / (pp * E * D));
-            if (!seg_shift(a, ns, dst_last, !is_zero(xyz(o0)), sg)) continue;
-            sg.emit(wn * ns.prf, sink);
-            const V3 tn = sg.val;
-            seg_post(a, fp, ns, sg);
-            sg.emit(wn * tn, sink);
+            if (!(vflags & (1u << n))) continue;
+            const NeighTerm t = neigh_term(fp, b, i, n, K);
+            const float wa = t.nmis * t.nwsum * t.jac;
+            if (!t.used || wa == 0.0f) continue;  // no term, or no weight: no gradient
+            const V3 wn = dl * cp.f * (wa / (pp * E * D));
+            pairs[static_cast<size_t>(n) * P + i] = make_float4(wn.x, wn.y, wn.z, 1.0f);
         }
         return splat(0.0f);
     }
@@ -412,20 +428,8 @@ RT_D V3 gather_pixel(const RAdjView& a, const FrameParams& fp, const Bufs& b, ui
     const V3 canon = fpv * sg.val / (pp * ps);
     V3 suffix_contrib = splat(0.0f);
     for (uint32_t n = 0; n < count; ++n) {
-        if (!(use & (1u << n))) continue;
-        const uint32_t np_ = b.neighbors[static_cast<size_t>(i) * k + n].pixel;
-        const Suffix ns = ld_sres(b.sres_cur, np_).s;
-        const float nconf = sres_conf(b.sres_cur, np_), nwsum = sres_wsum(b.sres_cur, np_);
-        const float4 o0 = sh[2 * n];
-        float nmis = mis_neighbor(xyz(o0), ns.f, o0.w, K, 1.0f, nconf);
-        if (nonfinite(nmis)) nmis = 0.0f;
-        V3 fshift = splat(0.0f);
-        if (seg_shift(a, ns, dst_last, !is_zero(xyz(o0)), sg)) {
-            const V3 tn = sg.val;
-            seg_post(a, fp, ns, sg);
-            fshift = tn * sg.val;
-        }
-        suffix_contrib = suffix_contrib + nmis * fshift * nwsum * o0.w;
+        const float4 c = pairs[static_cast<size_t>(n) * P + i];
+        if (c.w != 0.0f) suffix_contrib = suffix_contrib + xyz(c);
     }
     V3 gather = suffix_contrib * fpv / pp;
     gather = gather / E;
@@ -433,38 +437,109 @@ RT_D V3 gather_pixel(const RAdjView& a, const FrameParams& fp, const Bufs& b, ui
     return result / D;
 }
 
+// the gradient sink of a block: all parameters in shared memory when they fit
+struct BlockSink {
+    GradSink sink;
+    float* sh;
+    uint32_t n_sh;
+    RT_D void begin() {
+        if (sh) {
+            for (uint32_t k = threadIdx.x; k < n_sh; k += blockDim.x) sh[k] = 0.0f;
+            __syncthreads();
+        }
+    }
+    RT_D void end() {
+        if (sh) {
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < n_sh; k += blockDim.x) {
+                const float v = sh[k];
+                if (v == 0.0f) continue;
+                if (k < sink.num_mats * kMatGrad) atomicAdd(&sink.g_mat[k], v);
+                else atomicAdd(&sink.g_em[k - sink.num_mats * kMatGrad], v);
+            }
+        }
+    }
+};
+
 template <bool kGrad>
 __global__ void __launch_bounds__(kPassBlock) k_restir_adjoint(RAdjView a, FrameParams fp, Bufs b, const float* d_img,
-                                                               float* out, float* g_mat, float* g_em, int use_shared) {
-    extern __shared__ float sh[];
-    const uint32_t n_sh = a.num_mats * kMatGrad + a.eval.num_emitters * kEmGrad;
-    if (kGrad && use_shared) {
-        for (uint32_t k = threadIdx.x; k < n_sh; k += blockDim.x) sh[k] = 0.0f;
-        __syncthreads();
-    }
-    GradSink sink{kGrad && use_shared ? sh : nullptr, g_mat, g_em, a.num_mats};
+                                                               float* out, float4* pairs, float* g_mat, float* g_em,
+                                                               int use_shared) {
+    extern __shared__ float shm[];
+    BlockSink bs{GradSink{kGrad && use_shared ? shm : nullptr, g_mat, g_em, a.num_mats},
+                 kGrad && use_shared ? shm : nullptr, a.num_mats * kMatGrad + a.eval.num_emitters * kEmGrad};
+    bs.begin();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < pixel_count(fp)) {
+    const uint32_t P = pixel_count(fp);
+    if (i < P) {
         if (kGrad) {
+            for (uint32_t n = 0; n < fp.k; ++n) pairs[static_cast<size_t>(n) * P + i] = make_float4(0.f, 0.f, 0.f, 0.f);
             const V3 dl = V3{d_img[3 * i], d_img[3 * i + 1], d_img[3 * i + 2]};
-            if (!nonfinite(dl) && !is_zero(dl)) gather_pixel<true>(a, fp, b, i, dl, &sink);
+            if (!nonfinite(dl) && !is_zero(dl)) gather_pixel<true>(a, fp, b, i, dl, &bs.sink, pairs);
         } else {
-            V3 L = splat(0.0f) + gather_pixel<false>(a, fp, b, i, splat(0.0f), nullptr);
+            V3 L = splat(0.0f) + gather_pixel<false>(a, fp, b, i, splat(0.0f), nullptr, pairs);
             if (nonfinite(L)) L = splat(0.0f);
             out[3 * i] = L.x;
             out[3 * i + 1] = L.y;
             out[3 * i + 2] = L.z;
         }
     }
-    if (kGrad && use_shared) {
-        __syncthreads();
-        for (uint32_t k = threadIdx.x; k < n_sh; k += blockDim.x) {
-            const float v = sh[k];
-            if (v == 0.0f) continue;
-            if (k < a.num_mats * kMatGrad) atomicAdd(&g_mat[k], v);
-            else atomicAdd(&g_em[k - a.num_mats * kMatGrad], v);
+    bs.end();
+}
+
+// one neighbour term per thread: forward, its value at theta; backward, the
+// gradient of its shifted throughput T_n (.) R_n under the weight the pixel
+// kernel wrote.  Only slots below the pixel's neighbour count (written by the
+// frame's query for every pixel) are read.
+template <bool kGrad>
+__global__ void __launch_bounds__(kPassBlock) k_restir_pairs(RAdjView a, FrameParams fp, Bufs b, float4* pairs,
+                                                             float* g_mat, float* g_em, int use_shared) {
+    extern __shared__ float shm[];
+    BlockSink bs{GradSink{kGrad && use_shared ? shm : nullptr, g_mat, g_em, a.num_mats},
+                 kGrad && use_shared ? shm : nullptr, a.num_mats * kMatGrad + a.eval.num_emitters * kEmGrad};
+    bs.begin();
+    const uint32_t P = pixel_count(fp);
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < P * fp.k) {
+        const uint32_t n = t / P, i = t - n * P;
+        Seg<kGrad> sg;
+        if (kGrad) {
+            const float4 w4 = pairs[t];
+            if (w4.w != 0.0f) {
+                const V3 wn = xyz(w4);
+                const uint32_t np_ = b.neighbors[static_cast<size_t>(i) * fp.k + n].pixel;
+                const Suffix ns = ld_sres(b.sres_cur, np_).s;
+                const float4 o0 = b.shift_out[static_cast<size_t>(i) * b.slots + 2 * n];
+                const Isect dst_last = unpack(a.eval, ld_hit(b.gather_cs[i].sample.last_prefix));
+                if (seg_shift(a, ns, dst_last, !is_zero(xyz(o0)), sg)) {
+                    sg.emit(wn * ns.prf, &bs.sink);
+                    const V3 tn = sg.val;
+                    seg_post(a, fp, ns, sg);
+                    sg.emit(wn * tn, &bs.sink);
+                }
+            }
+        } else {
+            float4 res = make_float4(0.f, 0.f, 0.f, 0.f);
+            const uint32_t vflags = b.pass_flags[i];
+            if (n < b.neigh_count[i] && ((vflags >> n) & 1u)) {
+                const NeighTerm tm = neigh_term(fp, b, i, n, static_cast<float>(__popc(vflags)));
+                if (tm.used) {
+                    const Suffix ns = ld_sres(b.sres_cur, tm.np).s;
+                    const Isect dst_last = unpack(a.eval, ld_hit(b.gather_cs[i].sample.last_prefix));
+                    V3 fshift = splat(0.0f);
+                    if (seg_shift(a, ns, dst_last, !is_zero(tm.f0), sg)) {
+                        const V3 tn = sg.val;
+                        seg_post(a, fp, ns, sg);
+                        fshift = tn * sg.val;
+                    }
+                    const V3 c = tm.nmis * fshift * tm.nwsum * tm.jac;
+                    res = make_float4(c.x, c.y, c.z, 1.0f);
+                }
+            }
+            pairs[t] = res;
         }
     }
+    bs.end();
 }
 
 RAdjView make_view(const SceneView& eval, const crisb_material* frame_mats, const crisb_emitter* frame_emitters,
@@ -482,22 +557,30 @@ RAdjView make_view(const SceneView& eval, const crisb_material* frame_mats, cons
 
 void restir_adjoint_forward(const SceneView& eval, const crisb_material* frame_mats,
                             const crisb_emitter* frame_emitters, uint32_t num_mats, const FrameParams& fp,
-                            const Bufs& b, float* out, cudaStream_t st) {
+                            const Bufs& b, float4* pairs, float* out, cudaStream_t st) {
     const RAdjView a = make_view(eval, frame_mats, frame_emitters, num_mats);
     const uint32_t P = fp.width * fp.height;
-    k_restir_adjoint<false><<<(P + kPassBlock - 1) / kPassBlock, kPassBlock, 0, st>>>(a, fp, b, nullptr, out,
+    if (fp.k > 0)
+        k_restir_pairs<false><<<(P * fp.k + kPassBlock - 1) / kPassBlock, kPassBlock, 0, st>>>(a, fp, b, pairs, nullptr,
+                                                                                              nullptr, 0);
+    k_restir_adjoint<false><<<(P + kPassBlock - 1) / kPassBlock, kPassBlock, 0, st>>>(a, fp, b, nullptr, out, pairs,
                                                                                        nullptr, nullptr, 0);
 }
 
 void restir_adjoint_backward(const SceneView& eval, const crisb_material* frame_mats,
                              const crisb_emitter* frame_emitters, uint32_t num_mats, const FrameParams& fp,
-                             const Bufs& b, const float* d_img, float* g_mat, float* g_em, cudaStream_t st) {
+                             const Bufs& b, float4* pairs, const float* d_img, float* g_mat, float* g_em,
+                             cudaStream_t st) {
     const RAdjView a = make_view(eval, frame_mats, frame_emitters, num_mats);
     const uint32_t P = fp.width * fp.height;
     const size_t sh_bytes = (static_cast<size_t>(num_mats) * kMatGrad + eval.num_emitters * kEmGrad) * sizeof(float);
     const int use_shared = sh_bytes <= 48u * 1024u ? 1 : 0;
-    k_restir_adjoint<true><<<(P + kPassBlock - 1) / kPassBlock, kPassBlock, use_shared ? sh_bytes : 0, st>>>(
-        a, fp, b, d_img, nullptr, g_mat, g_em, use_shared);
+    const size_t shb = use_shared ? sh_bytes : 0;
+    k_restir_adjoint<true><<<(P + kPassBlock - 1) / kPassBlock, kPassBlock, shb, st>>>(a, fp, b, d_img, nullptr, pairs,
+                                                                                       g_mat, g_em, use_shared);
+    if (fp.k > 0)
+        k_restir_pairs<true><<<(P * fp.k + kPassBlock - 1) / kPassBlock, kPassBlock, shb, st>>>(a, fp, b, pairs, g_mat,
+                                                                                               g_em, use_shared);
 }
 
 }  // namespace crisb
