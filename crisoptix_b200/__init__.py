@@ -253,6 +253,15 @@ class Renderer:
         check(load().crisb_autotune_ex(self.handle, ctypes.byref(camera_struct(camera)), int(frames), ctypes.byref(t)))
         return {k: getattr(t, k) for k, _ in t._fields_}
 
+    def autotune_spatial(self, camera: CameraDesc, budget_ms: float, frames: int = 3) -> dict:
+        """Pick suffix_spatial_count for a frame budget (crisb_autotune_spatial):
+        the largest candidate count whose frame time fits; applies it and
+        returns {"count", "frame_ms"}.  Changes the estimator."""
+        c, ms = ctypes.c_uint32(), ctypes.c_float()
+        check(load().crisb_autotune_spatial(self.handle, ctypes.byref(camera_struct(camera)), int(frames),
+                                            ctypes.c_float(budget_ms), ctypes.byref(c), ctypes.byref(ms)))
+        return {"count": c.value, "frame_ms": ms.value}
+
     def set_trace_block(self, threads: int):
         check(load().crisb_set_trace_block(self.handle, int(threads)))
 

@@ -210,6 +210,8 @@ ENTRY_POINTS = {
     "crisb_adjoint_refreeze": (c_i32, [c_vp]),
     "crisb_adjoint_forward": (c_i32, [c_vp, ctypes.POINTER(Camera), c_u64, c_vp, c_vp]),
     "crisb_adjoint_backward": (c_i32, [c_vp, ctypes.POINTER(Camera), c_u64, c_vp, c_vp, c_vp, c_vp]),
+    "crisb_autotune_spatial": (c_i32, [c_vp, ctypes.POINTER(Camera), c_u32, c_f, ctypes.POINTER(c_u32),
+                                       ctypes.POINTER(c_f)]),
     "crisb_restir_adjoint_enable": (c_i32, [c_vp, c_i32]),
     "crisb_restir_adjoint_forward": (c_i32, [c_vp, c_vp, c_vp]),
     "crisb_restir_adjoint_backward": (c_i32, [c_vp, c_vp, c_vp, c_vp, c_vp]),

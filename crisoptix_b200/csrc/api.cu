@@ -1623,6 +1623,71 @@ int crisb_autotune_ex(crisb_renderer* r, const crisb_camera* cam, uint32_t frame
     });
 }
 
+int crisb_autotune_spatial(crisb_renderer* r, const crisb_camera* cam, uint32_t frames, float budget_ms,
+                           uint32_t* chosen, float* chosen_ms) {
+    return guarded([&] {
+        require(r && cam && frames > 0 && budget_ms > 0.0f, "autotune spatial: null argument, no frames or no budget");
+        require(r->params.renderer_type == CRISB_RENDERER_CONDITIONAL_RESTIR && r->params.suffix_enable_spatial &&
+                    r->params.suffix_spatial_rounds > 0,
+                "autotune spatial: Conditional ReSTIR with suffix spatial reuse only");
+        DevBuf<float> buf;
+        buf.alloc(static_cast<size_t>(r->P()) * 3);
+        cudaStream_t st = nullptr;
+        check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        check(cudaEventCreate(&e0), "event");
+        check(cudaEventCreate(&e1), "event");
+        // ascending: the frame time grows with the count, so the first count
+        // over the budget ends the search
+        const uint32_t counts[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16};
+        uint32_t best = 0;
+        float best_ms = 0.0f, first_ms = 0.0f;
+        for (uint32_t c : counts) {
+            if (c > CRISB_MAX_SPATIAL_NEIGH) break;
+            crisb_params p = r->params;
+            p.suffix_spatial_count = static_cast<int>(c);
+            // a scratch renderer with the caller's launch settings; the
+            // caller's reservoirs are left alone
+            crisb_renderer* t = nullptr;
+            if (crisb_renderer_create(r->scene, r->width, r->height, &p, &t) != CRISB_OK)
+                throw Error(CRISB_ERR_CUDA, g_last_error);
+            std::unique_ptr<crisb_renderer> tmp(t);
+            tmp->trace_block = r->trace_block;
+            tmp->trace_grid = r->trace_grid;
+            if (r->jobs_per_pixel_set) {
+                tmp->jobs_per_pixel = r->jobs_per_pixel;
+                tmp->jobs_per_pixel_set = true;
+                tmp->allocate_jobs();
+            }
+            for (int f = 0; f < 4; ++f) tmp->render(*cam, buf.p, st);  // reservoirs with history
+            check(cudaEventRecord(e0, st), "event");
+            for (uint32_t f = 0; f < frames; ++f) tmp->render(*cam, buf.p, st);
+            check(cudaEventRecord(e1, st), "event");
+            check(cudaEventSynchronize(e1), "sync");
+            float ms = 0.0f;
+            check(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+            ms /= static_cast<float>(frames);
+            if (c == counts[0]) first_ms = ms;
+            if (ms > budget_ms) break;
+            best = c;
+            best_ms = ms;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        check(cudaStreamSynchronize(st), "sync");
+        cudaStreamDestroy(st);
+        if (best == 0) {  // nothing fits: the cheapest
+            best = counts[0];
+            best_ms = first_ms;
+        }
+        crisb_params p = r->params;
+        p.suffix_spatial_count = static_cast<int>(best);
+        if (crisb_renderer_set_params(r, &p) != CRISB_OK) throw Error(CRISB_ERR_INVALID_ARGUMENT, g_last_error);
+        if (chosen) *chosen = best;
+        if (chosen_ms) *chosen_ms = best_ms;
+    });
+}
+
 int crisb_autotune(crisb_renderer* r, const crisb_camera* cam, uint32_t frames, uint32_t* chosen) {
     crisb_tuning t{};
     const int rc = crisb_autotune_ex(r, cam, frames, &t);

@@ -657,6 +657,20 @@ typedef struct crisb_tuning {
  * the reference. */
 int crisb_autotune_ex(crisb_renderer* r, const crisb_camera* cam, uint32_t frames, crisb_tuning* out);
 
+/* The spatial-neighbour count of suffix spatial reuse (suffix_spatial_count,
+ * the reference's ImGui knob in src/Renderer.cpp:413-470) picked for a frame
+ * budget: candidates 1, 2, 3, 4, 5, 6, 8, 10, 12, 16 in turn, each on a
+ * scratch renderer of the same scene, size, parameters and launch settings
+ * (4 warm-up frames, then `frames` timed frames of `cam`), until one's mean
+ * frame time exceeds budget_ms; the largest count within the budget (the
+ * cheapest when none fits) is set on `r` through crisb_renderer_set_params
+ * and returned in *chosen, its frame time in *chosen_ms (either may be
+ * NULL).  Unlike the launch settings this changes the estimator: more
+ * neighbours give lower variance per frame for more time.  Conditional ReSTIR
+ * with suffix spatial reuse on only.  No counterpart in the reference. */
+int crisb_autotune_spatial(crisb_renderer* r, const crisb_camera* cam, uint32_t frames, float budget_ms,
+                           uint32_t* chosen, float* chosen_ms);
+
 /* Frames run as one CUDA graph of the pass chain by default (captured, updated in
  * place and launched on the caller's stream); 0 launches the kernels directly.
  * Frames with per-kernel timing on (crisb_set_timing) always launch directly.
