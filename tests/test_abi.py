@@ -65,3 +65,8 @@ def test_null_arguments_are_rejected_without_a_gpu():
     assert lib.crisb_last_error(buf, 256) == 0 and b"null" in buf.value
     assert lib.crisb_renderer_create(None, 8, 8, None, ctypes.byref(h)) == _abi.ERR_INVALID_ARGUMENT
     assert lib.crisb_render_frame(None, None, None, None) == _abi.ERR_INVALID_ARGUMENT
+    # the resampled-path adjoint and the spatial-count tuner
+    assert lib.crisb_restir_adjoint_enable(None, 1) == _abi.ERR_INVALID_ARGUMENT
+    assert lib.crisb_restir_adjoint_forward(None, None, None) == _abi.ERR_INVALID_ARGUMENT
+    assert lib.crisb_restir_adjoint_backward(None, None, None, None, None) == _abi.ERR_INVALID_ARGUMENT
+    assert lib.crisb_autotune_spatial(None, None, 1, 1.0, None, None) == _abi.ERR_INVALID_ARGUMENT
