@@ -53,6 +53,11 @@ uint64_t oracle_frame_index(const oracle_ctx* ctx);
 uint32_t oracle_frame_random(const oracle_ctx* ctx);
 /* Copy internal state in the crisb_*_rec layout (CRISB_BUF_* ids). */
 int oracle_dump(const oracle_ctx* ctx, int buffer_id, void* dst, size_t bytes);
+/* Every valid sample of the front suffix reservoirs re-traced past its
+ * reconnection vertex from its seed (the loop index in flags bits 24-31):
+ * *checked samples compared, *mismatched whose postReconF differs in any bit,
+ * *nee_recon reconnected at their NEE vertex (not re-traceable, not compared). */
+int oracle_check_post_recon(const oracle_ctx* ctx, uint32_t* checked, uint32_t* mismatched, uint32_t* nee_recon);
 size_t oracle_dump_size(const oracle_ctx* ctx, int buffer_id);
 
 /* ray k = rays[8k..8k+7] = (ox, oy, oz, tmin, dx, dy, dz, tmax) */

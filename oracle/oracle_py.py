@@ -52,6 +52,7 @@ def load():
         "oracle_frame_index": (u64, [vp]),
         "oracle_frame_random": (u32, [vp]),
         "oracle_dump": (i32, [vp, i32, vp, ctypes.c_size_t]),
+        "oracle_check_post_recon": (i32, [vp, ctypes.POINTER(u32), ctypes.POINTER(u32), ctypes.POINTER(u32)]),
         "oracle_dump_size": (ctypes.c_size_t, [vp, i32]),
         "oracle_trace": (i32, [vp, vp, vp, u32, i32]),
         "oracle_trace_bruteforce": (i32, [vp, vp, vp, u32, i32]),
@@ -190,6 +191,15 @@ class Oracle:
         if n and load().oracle_dump(self.h, buffer_id, _ptr(out), n) != 0:
             raise RuntimeError("oracle_dump failed")
         return out
+
+    def check_post_recon(self) -> dict:
+        """oracle_check_post_recon: the front suffix samples re-traced past
+        their reconnection vertex from their seeds against their stored
+        postReconF (test infrastructure for the resampled-path adjoint)."""
+        c, m, n = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        if load().oracle_check_post_recon(self.h, ctypes.byref(c), ctypes.byref(m), ctypes.byref(n)) != 0:
+            raise RuntimeError("oracle_check_post_recon failed")
+        return {"checked": c.value, "mismatched": m.value, "nee_recon": n.value}
 
     def trace(self, rays: np.ndarray, any_hit: bool = False, brute: bool = False) -> np.ndarray:
         rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)

@@ -1542,6 +1542,46 @@ struct oracle_ctx {
         return ShiftSuffix(srcSuffix, dstLastPrefixInt, jacobian);
     }
 
+    // Test infrastructure (not in the reference): the postReconF of a valid
+    // suffix sample re-traced from its seed past its reconnection vertex, as
+    // the resampled-path adjoint re-traces it -- the random state advanced
+    // four draws per suffix vertex up to and including the one whose loop
+    // index the flags carry (GetReconVert), then TraceSuffix's loop from the
+    // next vertex along reconOutDir.  `checkable` is false for samples that
+    // reconnected at their NEE vertex (postReconF = colour * 1/d^2 of a light
+    // sample whose vertex is not stored).
+    vec3 ReplayPostRecon(const SuffixPath& s, bool& checkable) const {
+        const uint32_t len = s.GetLength(), r = s.GetReconVert();
+        checkable = r + 1 < len;
+        if (!checkable) return vec3(0.0f);
+        const uint32_t maxLen = static_cast<uint32_t>(params.max_path_len - params.prefix_len);
+        PCG32 rng = s.rng;
+        for (uint32_t k = 0; k < 4 * (r + 1); ++k) rng.NextFloat();
+        vec3 pos = Unpack(s.reconInt).pos, dir = s.reconOutDir;
+        vec3 prf(1.0f);
+        for (uint32_t vertIdx = r + 1; vertIdx < maxLen; ++vertIdx) {
+            Interaction it;
+            TraceClosest(pos, dir, 1e-3f, 1e16f, it);
+            if (!it.valid) return vec3(NAN);
+            const bool forceNee = vertIdx == maxLen - 1;
+            if (rng.NextFloat() < params.nee_prob || forceNee) {
+                const EmitterSample emitter = SampleEmitter(rng);
+                const vec3 lightVec = emitter.pos - it.pos;
+                const float lightLen = length(lightVec);
+                const BrdfEvalResult e = Eval(it, normalize(lightVec));
+                const float distFactor = 1.0f / (lightLen * lightLen);
+                prf *= emitter.color * distFactor;
+                if (s.GetReconIdx() < len) prf *= e.brdfResult;
+                return prf;
+            }
+            const BrdfSampleResult b = Sample(it, rng);
+            prf *= b.brdfVal;
+            pos = it.pos;
+            dir = b.outDir;
+        }
+        return vec3(NAN);
+    }
+
     // ---- passes ----------------------------------------------------------------
     vec3 PixelJitterDir(uint32_t x, uint32_t y, PCG32& rng) const {
         // Next2d: x drawn first (DEFINED: left-to-right argument evaluation)
@@ -2445,6 +2485,24 @@ size_t oracle_dump_size(const oracle_ctx* ctx, int id) {
         case CRISB_BUF_NEIGHBOR_COUNT: return P * sizeof(uint32_t);
         default: return 0;
     }
+}
+
+int oracle_check_post_recon(const oracle_ctx* ctx, uint32_t* checked, uint32_t* mismatched, uint32_t* nee_recon) {
+    if (!ctx || !checked || !mismatched || !nee_recon) return CRISB_ERR_INVALID_ARGUMENT;
+    if (ctx->params.renderer_type != CRISB_RENDERER_CONDITIONAL_RESTIR) return CRISB_ERR_INVALID_ARGUMENT;
+    *checked = *mismatched = *nee_recon = 0;
+    for (const auto& res : ctx->suffixRes[ctx->front]) {
+        if (!res.sample.IsValid()) continue;
+        bool checkable = false;
+        const vec3 v = ctx->ReplayPostRecon(res.sample, checkable);
+        if (!checkable) {
+            ++*nee_recon;
+            continue;
+        }
+        ++*checked;
+        if (std::memcmp(&v, &res.sample.postReconF, sizeof(v)) != 0) ++*mismatched;
+    }
+    return CRISB_OK;
 }
 
 int oracle_dump(const oracle_ctx* ctx, int id, void* dst, size_t bytes) {
