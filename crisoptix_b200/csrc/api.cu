@@ -775,6 +775,7 @@ struct crisb_renderer {
 
     void allocate_jobs() {
         const size_t p = P();
+        adjoint_frame = false;  // the resampled-path adjoint reads the frame's shift results
         slots = slots_for(params);
         spatial_nbr.alloc(p * (slots / 2));
         job_items.alloc(p * slots);
@@ -1446,6 +1447,7 @@ int crisb_renderer_set_params(crisb_renderer* r, const crisb_params* params) {
         r->slots = slots_before;
         if (realloc_neighbors || realloc_jobs) check(cudaDeviceSynchronize(), "sync");
         if (realloc_neighbors) {
+            r->adjoint_frame = false;  // the frame's neighbour lists are gone
             r->neighbors.alloc(static_cast<size_t>(r->P()) * std::max<uint32_t>(r->K(), 1));
             check(cudaMemset(r->neighbors.p, 0, r->neighbors.bytes()), "memset");
         }
@@ -1479,8 +1481,9 @@ int crisb_restir_adjoint_enable(crisb_renderer* r, int on) {
 namespace {
 void restir_adjoint_check(const crisb_renderer* r) {
     require(r->has_frame && r->adjoint_frame,
-            "restir adjoint: enable it (crisb_restir_adjoint_enable) before rendering the frame");
-    const crisb_params& p = r->params;
+            "restir adjoint: enable it (crisb_restir_adjoint_enable) and render a frame first (a parameter or "
+            "job-capacity change that reallocated the frame's buffers ends its adjoint)");
+    const crisb_params& p = r->last_fp.p;  // the frame's parameters
     require(p.renderer_type == CRISB_RENDERER_CONDITIONAL_RESTIR, "restir adjoint: Conditional ReSTIR only");
     require(p.gather_n == 1, "restir adjoint: gather_n must be 1");
     require(p.storage == CRISB_STORAGE_FP32, "restir adjoint: FP32 reservoir storage only");

@@ -574,7 +574,10 @@ int crisb_adjoint_backward(crisb_adjoint* a, const crisb_camera* cam, uint64_t f
  * given d_image_dev = dLoss/dimage (W*H*3), into d_materials_dev (7 floats per
  * material: diffuse rgb, roughness, emission rgb) and d_emitters_dev (3 floats
  * per emitter: colour).  Both read the frame's buffers: run them on the
- * frame's stream (or after it) and before the next frame; the first call
+ * frame's stream (or after it) and before the next frame (a
+ * crisb_renderer_set_params, crisb_set_job_capacity or crisb_autotune_ex that
+ * reallocates the renderer's buffers also ends the frame's adjoint: they
+ * return CRISB_ERR_INVALID_ARGUMENT until another frame); the first call
  * allocates width*height*k*16 bytes of scratch (k = gather_m - 1).  Requires
  * CRISB_RENDERER_CONDITIONAL_RESTIR, gather_n 1, FP32 storage, an untextured
  * scene and max_path_len <= 16.  No counterpart in the reference, which has no

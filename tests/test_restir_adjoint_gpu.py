@@ -86,6 +86,11 @@ def test_restir_adjoint_rejects_unsupported_configurations(cuda_device):
         r.restir_adjoint_backward(out.data_ptr(), g_mat.data_ptr(), g_em.data_ptr())
     r.launch_frame(cam, out.data_ptr())
     r.restir_adjoint_forward(out.data_ptr())
+    r.set_job_capacity(4)  # reallocates the frame's shift results: its adjoint ends
+    with pytest.raises(RuntimeError):
+        r.restir_adjoint_forward(out.data_ptr())
+    r.launch_frame(cam, out.data_ptr())
+    r.restir_adjoint_forward(out.data_ptr())
     for kw in (dict(storage=_abi.STORAGE_FP16), dict(gather_n=2), dict(renderer_type=_abi.PATH_TRACER)):
         r = Renderer(32, 24, sc, _params(desc, **kw))
         r.restir_adjoint_enable(True)
