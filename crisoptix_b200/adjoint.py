@@ -94,16 +94,20 @@ class PtAdjoint:
             self.forward(c, frame, out[v].data_ptr())
         return out.view(len(cams), self.height, self.width, 3)
 
-    def gradient(self, cams: Sequence[Camera], d_img, frame: int = 0):
+    def gradient(self, cams: Sequence[Camera], d_img, frame: int = 0, dist=None):
         """(materials x 7, emitters x 3) float32 device tensors of dLoss/dparameter
-        for d_img = dLoss/dimage of shape (V, H, W, 3)."""
+        for d_img = dLoss/dimage of shape (V, H, W, 3); with a process group
+        `dist`, summed over the ranks (each differentiating its own views)."""
         import torch
+
+        from .sharding import sum_gradients
 
         d_img = d_img.contiguous().view(len(cams), -1).float()
         g_mat = torch.zeros(self.num_mats * MAT_GRAD, dtype=torch.float32, device="cuda")
         g_em = torch.zeros(self.num_emitters * EM_GRAD, dtype=torch.float32, device="cuda")
         for v, c in enumerate(cams):
             self.backward(c, frame, d_img[v].data_ptr(), g_mat.data_ptr(), g_em.data_ptr())
+        sum_gradients(g_mat, g_em, dist)
         return g_mat.view(self.num_mats, MAT_GRAD), g_em.view(self.num_emitters, EM_GRAD)
 
 
@@ -182,16 +186,20 @@ class RestirAdjoint:
             r.restir_adjoint_forward(o.data_ptr())
         return out.view(len(self.views), self.height, self.width, 3)
 
-    def gradient(self, d_img):
+    def gradient(self, d_img, dist=None):
         """(materials x 7, emitters x 3) float32 device tensors of dLoss/dparameter
-        for d_img = dLoss/dimage of shape (V, H, W, 3)."""
+        for d_img = dLoss/dimage of shape (V, H, W, 3); with a process group
+        `dist`, summed over the ranks (each differentiating its own views)."""
         import torch
+
+        from .sharding import sum_gradients
 
         d_img = d_img.contiguous().view(len(self.views), -1).float()
         g_mat = torch.zeros(self.num_mats * MAT_GRAD, dtype=torch.float32, device="cuda")
         g_em = torch.zeros(self.num_emitters * EM_GRAD, dtype=torch.float32, device="cuda")
         for v, r in enumerate(self.views):
             r.restir_adjoint_backward(d_img[v].data_ptr(), g_mat.data_ptr(), g_em.data_ptr())
+        sum_gradients(g_mat, g_em, dist)
         return g_mat.view(self.num_mats, MAT_GRAD), g_em.view(self.num_emitters, EM_GRAD)
 
 

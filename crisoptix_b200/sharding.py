@@ -4,8 +4,10 @@ ranks of a device time, and the whole-job rate.
 The frame loop does not shard within a view (spatial reuse needs a halo of
 reservoirs, the final-gather endpoint search is global in world space), so N
 GPUs run N independent view replicas: weak scaling, no collective on the data
-path.  The only collectives are the timing reductions here (an all-reduce of one
-float per measurement), over NCCL on GPUs or gloo on CPU.
+path.  The collectives are the timing reductions here (an all-reduce of one
+float per measurement) and, for inverse rendering over views split across
+ranks, one all-reduce of the gradient vector per step (sum_gradients), over
+NCCL on GPUs or gloo on CPU.
 """
 from __future__ import annotations
 
@@ -45,6 +47,25 @@ def max_over_ranks(value: float, dist=None, device: Optional[str] = None) -> flo
     t = torch.tensor([float(value)], dtype=torch.float64, device=device or "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def sum_gradients(g_mat, g_em, dist=None):
+    """Inverse rendering over views split across ranks (assign_views): each rank
+    adds its own views' dLoss/dparameter into g_mat (materials x 7) and g_em
+    (emitters x 3); this sums them over all ranks in place, as one all-reduce
+    of the two flattened into one buffer (992 values for the inverse-rendering
+    config's parameters, 321 x 7 + 256 x 3 floats as stored).  Identity
+    without a process group.  Every rank must call this at the same point."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return g_mat, g_em
+    import torch
+
+    flat = torch.cat([g_mat.reshape(-1), g_em.reshape(-1)])
+    dist.all_reduce(flat, op=dist.ReduceOp.SUM)
+    n = g_mat.numel()
+    g_mat.copy_(flat[:n].view_as(g_mat))
+    g_em.copy_(flat[n:].view_as(g_em))
+    return g_mat, g_em
 
 
 def whole_job_rate(units_per_rank_step: float, steps: int, world: int, ms: float) -> float:

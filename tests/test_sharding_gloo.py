@@ -1,5 +1,6 @@
-"""Multi-rank host logic of the bench on CPU: two gloo ranks reduce their
-device times to the max, split the views, and agree on the whole-job rate."""
+"""Multi-rank host logic on CPU: two gloo ranks reduce their device times to
+the max, split the views, agree on the whole-job rate, and sum the gradient
+vectors of their views for inverse rendering."""
 import os
 import socket
 
@@ -27,7 +28,14 @@ def _rank_main(rank, world, port, out):
         e2e = sharding.max_over_ranks(20.0 - rank, dist)
         rate = sharding.whole_job_rate(1000.0, 5, world, ms)
         views = sharding.assign_views([512 * 512] * 8 + [1280 * 720] * 4 + [1920 * 1080] * 4, world)
-        out[rank] = (ms, e2e, rate, sharding.orbit_offset(rank, world), views)
+        # inverse rendering: 8 views of 512^2 split across ranks, each rank's
+        # gradient from its own views (here: view index + 1 per entry), summed
+        inv = sharding.assign_views([512 * 512] * 8, world)[rank]
+        g_mat = torch.full((321, 7), float(sum(v + 1 for v in inv)))
+        g_em = torch.full((256, 3), -float(sum(v + 1 for v in inv)))
+        sharding.sum_gradients(g_mat, g_em, dist)
+        out[rank] = (ms, e2e, rate, sharding.orbit_offset(rank, world), views, inv,
+                     float(g_mat[5, 3]), float(g_em[100, 2]), float(g_mat.sum()))
     finally:
         dist.destroy_process_group()
 
@@ -38,11 +46,15 @@ def test_two_gloo_ranks_agree():
     mp.spawn(_rank_main, args=(world, _free_port(), out), nprocs=world, join=True)
     assert sorted(out.keys()) == [0, 1]
     for r in range(world):
-        ms, e2e, rate, _, views = out[r]
+        ms, e2e, rate, _, views, inv, gm, ge, gsum = out[r]
         assert ms == 11.0  # max over ranks, not the rank's own time
         assert e2e == 20.0
         assert rate == pytest.approx(1000.0 * 5 * world / 0.011)
         assert views == out[0][4]  # every rank computes the same split
+        assert len(inv) == 4  # 4 of the 8 inverse-rendering views per rank
+        # every rank holds the sum over all 8 views: 1 + 2 + ... + 8 = 36
+        assert gm == 36.0 and ge == -36.0 and gsum == 36.0 * 321 * 7
+    assert sorted(out[0][5] + out[1][5]) == list(range(8))
     assert out[0][3] == 0 and out[1][3] == 30  # distinct views of the 60-frame orbit
 
 
@@ -59,6 +71,9 @@ def test_assign_views_partitions_and_balances():
 
 def test_single_rank_identity():
     assert sharding.max_over_ranks(3.5, None) == 3.5
+    g_mat, g_em = torch.ones(3, 7), torch.ones(2, 3)
+    a, b = sharding.sum_gradients(g_mat, g_em, None)
+    assert a is g_mat and float(a.sum()) == 21.0 and float(b.sum()) == 6.0
     assert sharding.orbit_offset(0, 1) == 0
     with pytest.raises(ValueError):
         sharding.orbit_offset(2, 2)
