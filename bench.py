@@ -444,7 +444,7 @@ def run_crisb(args):
     img_mean = float(host.mean())
     tone = tonemap_timing(out, W, H, stream)
 
-    # ---- the north star's comparison arms (same box, same run) -----------------
+    # ---- the comparison arms the metric names (same box, same run) ------------
     arms = None
     if not args.no_arms and world == 1 and args.workload == "large" and not args.res:
         arms = comparison_arms(sc, cam, W, H, p, ppp, value, ms_per_frame, args)

@@ -527,7 +527,8 @@ int crisb_scene_get_materials(const crisb_scene* scene, crisb_material* out, uin
 int crisb_scene_set_materials(crisb_scene* scene, const crisb_material* mats, uint32_t n);
 int crisb_scene_set_emitter_colors(crisb_scene* scene, const float* rgb, uint32_t n);
 
-/* Path-replay adjoint (survey config INV).  The estimator is the path tracer
+/* Path-replay adjoint (inverse rendering: materials' albedo, roughness and
+ * emission, emitters' colour).  The estimator is the path tracer
  * (TraceCompletePath, include/graph/restir/path_gen.h:389-472) with frozen
  * sampling: random decisions, sampled directions and sampling pdfs use the
  * material table copied when the context is made (or at
@@ -551,9 +552,9 @@ int crisb_adjoint_forward(crisb_adjoint* a, const crisb_camera* cam, uint64_t fr
 int crisb_adjoint_backward(crisb_adjoint* a, const crisb_camera* cam, uint64_t frame, const float* d_image_dev,
                            float* d_materials_dev, float* d_emitters_dev, void* stream);
 
-/* Path-replay adjoint of the resampled estimator (survey config INV, north
- * star "re-trace each pixel's selected resampled paths from their stored
- * seeds").  The estimator is the final gather of the frame `r` rendered last
+/* Path-replay adjoint of the resampled estimator: each pixel's selected
+ * resampled paths re-traced from their stored seeds.  The estimator is the
+ * final gather of the frame `r` rendered last
  * (FinalGatherCanon, shader/final_gather.cu:69-188): per pixel the canonical
  * path and each valid neighbour's suffix shifted onto the canonical prefix,
  * combined with pairwise MIS.  Frozen at the material and emitter tables that
@@ -587,7 +588,7 @@ int crisb_restir_adjoint_forward(crisb_renderer* r, float* out_rgb_dev, void* st
 int crisb_restir_adjoint_backward(crisb_renderer* r, const float* d_image_dev, float* d_materials_dev,
                                   float* d_emitters_dev, void* stream);
 
-/* Batched views (survey config MV: many cameras of uneven resolution).  A
+/* Batched views (many cameras of uneven resolution).  A
  * batch holds renderers of one device -- one per view, each with its own
  * resolution, parameters and storage -- and crisb_batch_render runs one frame
  * of every view as parallel branches of a single CUDA graph launched on
