@@ -1,9 +1,10 @@
-"""Scene files: Wavefront OBJ + MTL with PNG textures.
+"""Scene files: Wavefront OBJ + MTL and binary FBX, with PNG textures.
 
 The reference imports models with assimp (src/Model.cpp:9-207: triangulated,
 normals generated where missing, optional uv flip) and reads textures with
 stb_image as RGBA8 (src/Texture.cpp:8-30).  Neither library is part of this
-package; this module reads the same inputs itself, for OBJ/MTL and 8-bit PNG:
+package; this module reads the same inputs itself, for OBJ/MTL, binary FBX
+(load_fbx, described with its section below) and 8-bit PNG:
 
 * geometry: `v`, `vt`, `vn`, `f` (polygons fanned into triangles, negative
   indices relative), `usemtl`, `mtllib`; every distinct v/vt/vn corner is one
@@ -318,3 +319,475 @@ def save_obj(path: str, desc: scenes.Scene) -> None:
                 f.write(f"usemtl m{int(mi)}\n")
                 cur = mi
             f.write("f " + " ".join(f"{int(v) + 1}/{int(v) + 1}/{int(v) + 1}" for v in tri) + "\n")
+
+
+# ---- FBX (binary) -------------------------------------------------------------------
+# The reference reads FBX through assimp (src/Model.cpp:9-207).  This reader
+# covers the binary format's node tree (FBX 7.x: 32-bit node records before
+# version 7500, 64-bit from it; zlib-compressed arrays) and the parts of the
+# scene graph the reference's Model uses, mapped as assimp's FBX importer maps
+# them:
+#
+# * Geometry (Mesh): `Vertices`, `PolygonVertexIndex` (a negative index ends a
+#   polygon: -(i + 1)); polygons fanned into triangles (aiProcess_Triangulate);
+#   `LayerElementNormal` / `LayerElementUV` mapped ByPolygonVertex or
+#   ByVertice, referenced Direct or IndexToDirect; `LayerElementMaterial`
+#   AllSame or ByPolygon; polygons without normals get their face normal
+#   (aiProcess_GenNormals); every polygon corner is its own vertex;
+# * Model: `Lcl Translation`, `Lcl Rotation` (degrees, XYZ order),
+#   `Lcl Scaling` through the parent chain (Connections "OO"), baked into the
+#   triangles (normals by the inverse transpose); pivots, pre/post-rotations
+#   and geometric transforms are not read;
+# * Material: DiffuseColor, SpecularColor, EmissiveColor, each times its
+#   ...Factor when present (assimp's factored colours), a Roughness or
+#   RoughnessFactor property if the file has one, with the reference's
+#   fallbacks otherwise (diffuse and specular 1, emission 0, roughness 1);
+#   Texture objects connected ("OP") to DiffuseColor / SpecularColor /
+#   Roughness (or 3ds Max's roughness_map) give the diffuse / specular /
+#   roughness textures (RelativeFilename, else FileName's base name, relative
+#   to the FBX's folder; PNG);
+# * faces of a material with non-zero emission form one emitter per material,
+#   as in load_obj.
+#
+# ASCII FBX is not read.
+
+_FBX_MAGIC = b"Kaydara FBX Binary  \x00\x1a\x00"
+
+
+class FbxNode:
+    """One node of the FBX tree: name, property values, children."""
+
+    def __init__(self, name: str, props=None, children=None):
+        self.name = name
+        self.props = list(props or [])
+        self.children = list(children or [])
+
+    def child(self, name: str) -> Optional["FbxNode"]:
+        for c in self.children:
+            if c.name == name:
+                return c
+        return None
+
+    def all(self, name: str) -> List["FbxNode"]:
+        return [c for c in self.children if c.name == name]
+
+
+_ARRAY_DTYPE = {ord("f"): "<f4", ord("d"): "<f8", ord("l"): "<i8", ord("i"): "<i4", ord("b"): "u1"}
+
+
+def _fbx_prop(buf: bytes, o: int):
+    t = buf[o]
+    o += 1
+    if t == ord("Y"):
+        return struct.unpack_from("<h", buf, o)[0], o + 2
+    if t == ord("C"):
+        return bool(buf[o]), o + 1
+    if t == ord("I"):
+        return struct.unpack_from("<i", buf, o)[0], o + 4
+    if t == ord("F"):
+        return struct.unpack_from("<f", buf, o)[0], o + 4
+    if t == ord("D"):
+        return struct.unpack_from("<d", buf, o)[0], o + 8
+    if t == ord("L"):
+        return struct.unpack_from("<q", buf, o)[0], o + 8
+    if t in _ARRAY_DTYPE:
+        n, enc, clen = struct.unpack_from("<III", buf, o)
+        o += 12
+        raw = buf[o:o + clen]
+        if enc == 1:
+            raw = zlib.decompress(raw)
+        elif enc != 0:
+            raise ValueError(f"FBX: array encoding {enc}")
+        return np.frombuffer(raw, dtype=_ARRAY_DTYPE[t], count=n).copy(), o + clen
+    if t in (ord("S"), ord("R")):
+        n = struct.unpack_from("<I", buf, o)[0]
+        o += 4
+        v = bytes(buf[o:o + n])
+        return (v.decode("utf-8", "replace") if t == ord("S") else v), o + n
+    raise ValueError(f"FBX: property type {chr(t)!r} at byte {o - 1}")
+
+
+def _fbx_node(buf: bytes, o: int, wide: bool):
+    """(node or None for a null record, offset after it)."""
+    hdr = "<QQQ" if wide else "<III"
+    end, nprops, _plen = struct.unpack_from(hdr, buf, o)
+    o += 24 if wide else 12
+    nlen = buf[o]
+    o += 1
+    if end == 0:
+        return None, o  # null record: the rest of it is zeros
+    name = bytes(buf[o:o + nlen]).decode("ascii", "replace")
+    o += nlen
+    props = []
+    for _ in range(nprops):
+        v, o = _fbx_prop(buf, o)
+        props.append(v)
+    children = []
+    while o < end:
+        c, o2 = _fbx_node(buf, o, wide)
+        if c is None:
+            o = end
+            break
+        children.append(c)
+        o = o2
+    return FbxNode(name, props, children), end
+
+
+def read_fbx_tree(data: bytes) -> Tuple[int, List[FbxNode]]:
+    """(version, top-level nodes) of a binary FBX file."""
+    if not data.startswith(_FBX_MAGIC):
+        raise ValueError("not a binary FBX file (ASCII FBX is not read)")
+    version = struct.unpack_from("<I", data, len(_FBX_MAGIC))[0]
+    wide = version >= 7500
+    o = len(_FBX_MAGIC) + 4
+    nodes = []
+    while o < len(data):
+        if o + (25 if wide else 13) > len(data):
+            break
+        node, o = _fbx_node(data, o, wide)
+        if node is None:
+            break
+        nodes.append(node)
+    return version, nodes
+
+
+def _p70(node: Optional[FbxNode]) -> Dict[str, list]:
+    """An object's Properties70: property name -> its values (after the
+    name, type, label and flags strings)."""
+    out: Dict[str, list] = {}
+    p = node.child("Properties70") if node is not None else None
+    if p is not None:
+        for q in p.all("P"):
+            if q.props:
+                out[str(q.props[0])] = list(q.props[4:])
+    return out
+
+
+def _euler_xyz(deg) -> np.ndarray:
+    """Rotation of FBX's default XYZ order: about x first, then y, then z."""
+    rx, ry, rz = np.radians(np.asarray(deg, np.float64)[:3])
+    cx, sx, cy, sy, cz, sz = np.cos(rx), np.sin(rx), np.cos(ry), np.sin(ry), np.cos(rz), np.sin(rz)
+    Rx = np.array([[1, 0, 0], [0, cx, -sx], [0, sx, cx]])
+    Ry = np.array([[cy, 0, sy], [0, 1, 0], [-sy, 0, cy]])
+    Rz = np.array([[cz, -sz, 0], [sz, cz, 0], [0, 0, 1]])
+    return Rz @ Ry @ Rx
+
+
+def _fbx_local(props: Dict[str, list]) -> np.ndarray:
+    M = np.eye(4)
+    M[:3, :3] = _euler_xyz(props.get("Lcl Rotation", [0.0, 0.0, 0.0])) @ np.diag(
+        np.asarray(props.get("Lcl Scaling", [1.0, 1.0, 1.0])[:3], np.float64))
+    M[:3, 3] = np.asarray(props.get("Lcl Translation", [0.0, 0.0, 0.0])[:3], np.float64)
+    return M
+
+
+def _fbx_layer(geom: FbxNode, layer: str, data: str, index: str, width: int, corner_vertex: np.ndarray,
+               corner_polygon: np.ndarray) -> Optional[np.ndarray]:
+    """Per-corner values of the geometry's first `layer` (or None)."""
+    el = geom.child(layer)
+    if el is None or el.child(data) is None:
+        return None
+    mapping = str(el.child("MappingInformationType").props[0]) if el.child("MappingInformationType") else "ByVertice"
+    ref = str(el.child("ReferenceInformationType").props[0]) if el.child("ReferenceInformationType") else "Direct"
+    vals = np.asarray(el.child(data).props[0], np.float64).reshape(-1, width)
+    n = len(corner_vertex)
+    if mapping == "ByPolygonVertex":
+        key = np.arange(n)
+    elif mapping in ("ByVertice", "ByVertex", "ByControlPoint"):
+        key = corner_vertex
+    elif mapping == "ByPolygon":
+        key = corner_polygon
+    elif mapping == "AllSame":
+        key = np.zeros(n, np.int64)
+    else:
+        raise ValueError(f"FBX {layer}: mapping {mapping}")
+    if ref in ("IndexToDirect", "Index"):
+        key = np.asarray(el.child(index).props[0], np.int64)[key]
+    return vals[key]
+
+
+def _factored(props: Dict[str, list], name: str, default) -> List[float]:
+    """assimp's factored colour: <name>Color times <name>Factor when present
+    (the old `<name>` key when there is no `<name>Color`)."""
+    c = props.get(name + "Color", props.get(name))
+    if c is None:
+        return list(default)
+    col = [float(x) for x in c[:3]]
+    f = props.get(name + "Factor")
+    return [x * float(f[0]) for x in col] if f else col
+
+
+def load_fbx(path: str, flip_uv: bool = False, spec_usage: int = 0) -> scenes.Scene:
+    """Scene description of a binary FBX file: every mesh model's polygons,
+    triangulated and transformed to world space, its materials and their PNG
+    textures (paths relative to the file's folder)."""
+    base = os.path.dirname(os.path.abspath(path))
+    with open(path, "rb") as f:
+        _version, top = read_fbx_tree(f.read())
+    find = {n.name: n for n in top}
+    if "Objects" not in find:
+        raise ValueError(f"{path}: no Objects")
+    objects: Dict[int, FbxNode] = {int(n.props[0]): n for n in find["Objects"].children if n.props}
+    oo, op = [], []
+    for c in (find["Connections"].all("C") if "Connections" in find else []):
+        if c.props[0] == "OO":
+            oo.append((int(c.props[1]), int(c.props[2])))
+        elif c.props[0] == "OP":
+            op.append((int(c.props[1]), int(c.props[2]), str(c.props[3]) if len(c.props) > 3 else ""))
+
+    def kind(i):
+        n = objects.get(i)
+        return n.name if n is not None else None
+
+    parent = {c: p for c, p in oo if kind(c) == "Model" and kind(p) == "Model"}
+    world_cache: Dict[int, np.ndarray] = {}
+
+    def world(m: int) -> np.ndarray:
+        if m not in world_cache:
+            local = _fbx_local(_p70(objects[m]))
+            world_cache[m] = world(parent[m]) @ local if m in parent else local
+        return world_cache[m]
+
+    mat_ids = [i for i, n in objects.items() if n.name == "Material"]
+    model_mats: Dict[int, List[int]] = {}
+    geom_models: Dict[int, List[int]] = {}
+    for c, p in oo:
+        if kind(c) == "Material" and kind(p) == "Model":
+            model_mats.setdefault(p, []).append(mat_ids.index(c))
+        elif kind(c) == "Geometry" and kind(p) == "Model":
+            geom_models.setdefault(c, []).append(p)
+    tex_of: Dict[Tuple[int, str], int] = {}
+    for c, p, prop in op:
+        if kind(c) == "Texture" and kind(p) == "Material":
+            tex_of[(mat_ids.index(p), prop)] = c
+
+    pos: List[np.ndarray] = []
+    nrm: List[np.ndarray] = []
+    uv: List[np.ndarray] = []
+    tri_mat: List[np.ndarray] = []
+    n_vert = 0
+    extra_default = False  # polygons whose model has no material for their slot
+    for gid, g in objects.items():
+        if g.name != "Geometry" or g.child("Vertices") is None or g.child("PolygonVertexIndex") is None:
+            continue
+        V = np.asarray(g.child("Vertices").props[0], np.float64).reshape(-1, 3)
+        pvi = np.asarray(g.child("PolygonVertexIndex").props[0], np.int64)
+        ends = pvi < 0
+        cv = np.where(ends, -pvi - 1, pvi)
+        cp = np.concatenate([[0], np.cumsum(ends)[:-1]]).astype(np.int64)
+        cn = _fbx_layer(g, "LayerElementNormal", "Normals", "NormalsIndex", 3, cv, cp)
+        cu = _fbx_layer(g, "LayerElementUV", "UV", "UVIndex", 2, cv, cp)
+        ml = g.child("LayerElementMaterial")
+        starts = np.concatenate([[0], np.flatnonzero(ends)[:-1] + 1])
+        npoly = len(starts)
+        if ml is not None and ml.child("Materials") is not None:
+            slots = np.asarray(ml.child("Materials").props[0], np.int64)
+            mapping = str(ml.child("MappingInformationType").props[0]) if ml.child("MappingInformationType") \
+                else "AllSame"
+            poly_slot = slots[:npoly] if mapping == "ByPolygon" else np.full(npoly, slots[0] if len(slots) else 0)
+        else:
+            poly_slot = np.zeros(npoly, np.int64)
+        # fan triangles: (first, k, k + 1) corners of each polygon
+        tri_c, tri_p = [], []
+        for p_i, (s, e) in enumerate(zip(starts, np.flatnonzero(ends))):
+            for k in range(s + 1, e):
+                tri_c.append((s, k, k + 1))
+                tri_p.append(p_i)
+        if not tri_c:
+            continue
+        tri_c = np.asarray(tri_c, np.int64)
+        tri_p = np.asarray(tri_p, np.int64)
+        for m in geom_models.get(gid, []):
+            M = world(m)
+            A, t = M[:3, :3], M[:3, 3]
+            ident = np.array_equal(M, np.eye(4))  # untransformed: values kept bit for bit
+            P = V[cv[tri_c]] if ident else V[cv[tri_c]] @ A.T + t  # (T, 3, 3) per triangle corner
+            if cn is not None:
+                Nn = cn[tri_c]
+                if not ident:
+                    Nn = Nn @ np.linalg.inv(A)  # the inverse transpose
+                    Nn = Nn / np.maximum(np.linalg.norm(Nn, axis=2, keepdims=True), 1e-30)
+            else:
+                fn = np.cross(P[:, 1] - P[:, 0], P[:, 2] - P[:, 0])
+                ln = np.linalg.norm(fn, axis=1, keepdims=True)
+                fn = np.where(ln > 0, fn / np.maximum(ln, 1e-30), np.array([[0.0, 0.0, 1.0]]))
+                Nn = np.repeat(fn[:, None, :], 3, axis=1)
+            U = cu[tri_c] if cu is not None else np.zeros((len(tri_c), 3, 2))
+            if flip_uv:
+                U = np.stack([U[..., 0], 1.0 - U[..., 1]], axis=-1)
+            slots_m = model_mats.get(m, [])
+            ts = poly_slot[tri_p]
+            gm = np.array([slots_m[s] if 0 <= s < len(slots_m) else -1 for s in ts], np.int64)
+            if (gm < 0).any():
+                extra_default = True
+                gm = np.where(gm < 0, len(mat_ids), gm)
+            pos.append(P.reshape(-1, 3))
+            nrm.append(Nn.reshape(-1, 3))
+            uv.append(U.reshape(-1, 2))
+            tri_mat.append(gm)
+            n_vert += 3 * len(tri_c)
+    if not pos:
+        raise ValueError(f"{path}: no mesh polygons")
+    textures: List[np.ndarray] = []
+    tex_index: Dict[int, int] = {}
+
+    def texture(tid: Optional[int]) -> int:
+        if tid is None:
+            return -1
+        if tid not in tex_index:
+            t = objects[tid]
+            name = None
+            for key in ("RelativeFilename", "FileName"):
+                if t.child(key) is not None and t.child(key).props and str(t.child(key).props[0]):
+                    name = str(t.child(key).props[0]).replace("\\", "/")
+                    break
+            if name is None:
+                return -1
+            fp = os.path.join(base, name)
+            if not os.path.exists(fp):
+                fp = os.path.join(base, os.path.basename(name))
+            with open(fp, "rb") as tf:
+                textures.append(decode_png_rgba(tf.read()))
+            tex_index[tid] = len(textures) - 1
+        return tex_index[tid]
+
+    mats, mt = [], []
+    for i, mid in enumerate(mat_ids + ([None] if extra_default else [])):
+        props = _p70(objects[mid]) if mid is not None else {}
+        m = np.zeros((), dtype=scenes.MATERIAL_DTYPE)
+        m["diffuse"] = _factored(props, "Diffuse", (1.0, 1.0, 1.0))
+        m["specular"] = _factored(props, "Specular", (1.0, 1.0, 1.0))
+        m["emission"] = _factored(props, "Emissive", (0.0, 0.0, 0.0))
+        r = props.get("Roughness", props.get("RoughnessFactor"))
+        m["roughness"] = float(r[0]) if r else 1.0
+        m["spec_usage"] = spec_usage
+        mats.append(m)
+        rough_tex = tex_of.get((i, "Roughness"), tex_of.get((i, "3dsMax|Parameters|roughness_map")))
+        mt.append([texture(tex_of.get((i, "DiffuseColor"))), texture(tex_of.get((i, "SpecularColor"))),
+                   texture(rough_tex)])
+    P = np.concatenate(pos).astype(np.float32)
+    T = np.arange(len(P), dtype=np.uint32).reshape(-1, 3)
+    TM = np.concatenate(tri_mat).astype(np.uint32)
+    emitters, faces = [], []
+    for i, m in enumerate(mats):
+        e = [float(x) for x in m["emission"]]
+        if any(v != 0.0 for v in e):
+            sel = np.flatnonzero(TM == i)
+            if len(sel):
+                emitters.append((tuple(e), len(faces), len(sel)))
+                faces.extend(P[T[sel]].reshape(-1, 9))
+    mt_arr = np.asarray(mt, np.int32).reshape(-1, 3)
+    return scenes.Scene(P, np.concatenate(nrm).astype(np.float32), T, TM, np.stack(mats),
+                        np.zeros((0, 2), np.uint32), [], emitters,
+                        np.asarray(faces, np.float32).reshape(-1, 9), name=os.path.basename(path),
+                        uvs=np.concatenate(uv).astype(np.float32), textures=textures,
+                        material_textures=mt_arr if (mt_arr >= 0).any() else None)
+
+
+_ARRAY_CODE = {np.dtype("<f4"): b"f", np.dtype("<f8"): b"d", np.dtype("<i8"): b"l", np.dtype("<i4"): b"i",
+               np.dtype("u1"): b"b"}
+
+
+def _fbx_prop_bytes(v) -> bytes:
+    if isinstance(v, (bool, np.bool_)):
+        return b"C" + bytes([1 if v else 0])
+    if isinstance(v, (int, np.integer)):
+        return b"L" + struct.pack("<q", int(v))
+    if isinstance(v, (float, np.floating)):
+        return b"D" + struct.pack("<d", float(v))
+    if isinstance(v, str):
+        b = v.encode("utf-8")
+        return b"S" + struct.pack("<I", len(b)) + b
+    if isinstance(v, bytes):
+        return b"R" + struct.pack("<I", len(v)) + v
+    a = np.ascontiguousarray(v)
+    dt = a.dtype.newbyteorder("<") if a.dtype.itemsize > 1 else np.dtype("u1")
+    raw = a.astype(dt).tobytes()
+    enc, data = (1, zlib.compress(raw)) if len(raw) > 64 else (0, raw)  # both encodings occur
+    return _ARRAY_CODE[dt] + struct.pack("<III", a.size, enc, len(data)) + data
+
+
+def _fbx_node_bytes(node: FbxNode, offset: int, wide: bool) -> bytes:
+    name = node.name.encode("ascii")
+    props = b"".join(_fbx_prop_bytes(v) for v in node.props)
+    head_len = (25 if wide else 13) + len(name)
+    body = b""
+    if node.children:
+        pos = offset + head_len + len(props)
+        for c in node.children:
+            cb = _fbx_node_bytes(c, pos, wide)
+            body += cb
+            pos += len(cb)
+        body += b"\x00" * (25 if wide else 13)  # null record ends the child list
+    end = offset + head_len + len(props) + len(body)
+    head = struct.pack("<QQQ" if wide else "<III", end, len(node.props), len(props)) + bytes([len(name)]) + name
+    return head + props + body
+
+
+def write_fbx_tree(path: str, nodes: List[FbxNode], version: int = 7400) -> None:
+    """Write top-level nodes as a binary FBX file of `version` (64-bit node
+    records from 7500)."""
+    wide = version >= 7500
+    out = bytearray(_FBX_MAGIC + struct.pack("<I", version))
+    for n in nodes:
+        out += _fbx_node_bytes(n, len(out), wide)
+    out += b"\x00" * (25 if wide else 13)
+    with open(path, "wb") as f:
+        f.write(bytes(out))
+
+
+def fbx_p(name: str, kind: str, *values) -> FbxNode:
+    """A Properties70 entry."""
+    return FbxNode("P", [name, kind, "", "A", *values])
+
+
+def save_fbx(path: str, desc: scenes.Scene, version: int = 7400) -> None:
+    """Write a non-instanced scene as a binary FBX that load_fbx reads back to
+    the same triangles (every corner's position, normal and uv), materials,
+    textures and emitters: one Geometry (normals and uvs by vertex, materials
+    by polygon), one Model, one Material per material (textures connected to
+    DiffuseColor, SpecularColor and Roughness)."""
+    if desc.instances:
+        raise ValueError("save_fbx writes non-instanced scenes")
+    base = os.path.dirname(os.path.abspath(path))
+    stem = os.path.splitext(os.path.basename(path))[0]
+    tex_names = []
+    for i, t in enumerate(desc.textures):
+        name = f"{stem}_tex{i}.png"
+        with open(os.path.join(base, name), "wb") as f:
+            f.write(encode_png_rgba(t))
+        tex_names.append(name)
+    idx = np.asarray(desc.indices, np.int64).reshape(-1, 3).copy()
+    idx[:, 2] = -idx[:, 2] - 1  # a negative index ends a polygon
+    layers = [FbxNode("LayerElementNormal", [0], [
+        FbxNode("MappingInformationType", ["ByVertice"]), FbxNode("ReferenceInformationType", ["Direct"]),
+        FbxNode("Normals", [np.asarray(desc.normals, np.float64).reshape(-1)])])]
+    if desc.uvs is not None:
+        layers.append(FbxNode("LayerElementUV", [0], [
+            FbxNode("MappingInformationType", ["ByVertice"]), FbxNode("ReferenceInformationType", ["Direct"]),
+            FbxNode("UV", [np.asarray(desc.uvs, np.float64).reshape(-1)])]))
+    layers.append(FbxNode("LayerElementMaterial", [0], [
+        FbxNode("MappingInformationType", ["ByPolygon"]), FbxNode("ReferenceInformationType", ["IndexToDirect"]),
+        FbxNode("Materials", [np.asarray(desc.triangle_material, np.int32)])]))
+    objs = [FbxNode("Geometry", [1000, "geometry\x00\x01Geometry", "Mesh"], [
+        FbxNode("Vertices", [np.asarray(desc.positions, np.float64).reshape(-1)]),
+        FbxNode("PolygonVertexIndex", [idx.reshape(-1).astype(np.int32)])] + layers),
+        FbxNode("Model", [2000, "model\x00\x01Model", "Mesh"], [FbxNode("Properties70")])]
+    conns = [FbxNode("C", ["OO", 2000, 0]), FbxNode("C", ["OO", 1000, 2000])]
+    for i, m in enumerate(desc.materials):
+        objs.append(FbxNode("Material", [3000 + i, f"m{i}\x00\x01Material", ""], [FbxNode("Properties70", [], [
+            fbx_p("DiffuseColor", "Color", *[float(x) for x in m["diffuse"]]),
+            fbx_p("SpecularColor", "Color", *[float(x) for x in m["specular"]]),
+            fbx_p("EmissiveColor", "Color", *[float(x) for x in m["emission"]]),
+            fbx_p("Roughness", "Number", float(m["roughness"]))])]))
+        conns.append(FbxNode("C", ["OO", 3000 + i, 2000]))
+    mt = desc.material_textures
+    for t, name in enumerate(tex_names):
+        objs.append(FbxNode("Texture", [4000 + t, f"t{t}\x00\x01Texture", ""], [FbxNode("RelativeFilename", [name])]))
+    if mt is not None:
+        for i, row in enumerate(np.asarray(mt).reshape(-1, 3)):
+            for slot, prop in enumerate(("DiffuseColor", "SpecularColor", "Roughness")):
+                if row[slot] >= 0:
+                    conns.append(FbxNode("C", ["OP", 4000 + int(row[slot]), 3000 + i, prop]))
+    write_fbx_tree(path, [FbxNode("FBXHeaderExtension", [], [FbxNode("FBXVersion", [version])]),
+                          FbxNode("Objects", [], objs), FbxNode("Connections", [], conns)], version)

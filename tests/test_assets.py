@@ -208,3 +208,110 @@ def test_flat_scene_keeps_textures():
     a.render_frame(cam, oa)
     b.render_frame(cam, ob)
     assert oa.tobytes() == ob.tobytes()
+
+
+@pytest.mark.parametrize("version", [7400, 7500])
+def test_fbx_round_trip(tmp_path, version):
+    """save_fbx -> load_fbx keeps every triangle corner's position, normal and
+    uv bit for bit, the materials, textures and emitters; the oracle renders
+    the read scene as the original (32- and 64-bit node records)."""
+    desc, cam = scenes.textured_cornell_box()
+    path = str(tmp_path / "box.fbx")
+    assets.save_fbx(path, desc, version=version)
+    back = assets.load_fbx(path)
+    ti, tb = np.asarray(desc.indices).reshape(-1, 3), np.asarray(back.indices).reshape(-1, 3)
+    for name in ("positions", "normals", "uvs"):
+        a, b = np.asarray(getattr(desc, name))[ti], np.asarray(getattr(back, name))[tb]
+        assert a.tobytes() == b.tobytes(), name
+    assert (np.asarray(back.triangle_material) == np.asarray(desc.triangle_material)).all()
+    assert (back.materials["spec_usage"] == 0).all()
+    back.materials["spec_usage"] = desc.materials["spec_usage"]
+    assert back.materials.tobytes() == desc.materials.tobytes()
+    assert ((back.material_textures >= 0) == (desc.material_textures >= 0)).all()
+    for tbk, td in zip(back.material_textures.ravel(), desc.material_textures.ravel()):
+        if td >= 0:
+            assert (back.textures[tbk] == desc.textures[td]).all()
+    assert [(tuple(np.float32(c)), f, n) for c, f, n in back.emitters] == \
+           [(tuple(np.float32(c)), f, n) for c, f, n in desc.emitters]
+    assert np.asarray(back.emitter_faces).tobytes() == np.asarray(desc.emitter_faces).tobytes()
+    p = small_config_params(scene_size_of(desc))
+    a, b = op.Oracle.from_scene(desc, W, H, p), op.Oracle.from_scene(back, W, H, p)
+    oa, ob = np.zeros((H, W, 3), np.float32), np.zeros((H, W, 3), np.float32)
+    for f in range(2):
+        a.render_frame(cam, oa)
+        b.render_frame(cam, ob)
+        assert oa.tobytes() == ob.tobytes()
+
+
+def _fbx_graph_file(path):
+    """A quad and a triangle with per-corner indexed normals and uvs, one
+    material slot, used by two models: `child` (rotated 90 degrees about z,
+    scaled 2) under `parent` (translated by (1, 2, 3)), and `other` at the
+    origin with no material."""
+    N = assets.FbxNode
+    verts = np.array([0, 0, 0, 1, 0, 0, 1, 1, 0, 0, 1, 0, 2, 0, 0], np.float64)
+    pvi = np.array([0, 1, 2, -4, 1, 4, -3], np.int32)  # quad (0 1 2 3), triangle (1 4 2)
+    normals = np.array([0, 0, 1, 0, 0, -1], np.float64)
+    nidx = np.array([0, 0, 0, 0, 1, 1, 1], np.int32)
+    uvs = np.array([0, 0, 1, 0, 1, 1, 0, 1, 0.5, 0.25], np.float64)
+    uvidx = np.array([0, 1, 2, 3, 1, 4, 2], np.int32)
+    geom = N("Geometry", [10, "g\x00\x01Geometry", "Mesh"], [
+        N("Vertices", [verts]), N("PolygonVertexIndex", [pvi]),
+        N("LayerElementNormal", [0], [N("MappingInformationType", ["ByPolygonVertex"]),
+                                      N("ReferenceInformationType", ["IndexToDirect"]),
+                                      N("Normals", [normals]), N("NormalsIndex", [nidx])]),
+        N("LayerElementUV", [0], [N("MappingInformationType", ["ByPolygonVertex"]),
+                                  N("ReferenceInformationType", ["IndexToDirect"]),
+                                  N("UV", [uvs]), N("UVIndex", [uvidx])]),
+        N("LayerElementMaterial", [0], [N("MappingInformationType", ["AllSame"]),
+                                        N("ReferenceInformationType", ["IndexToDirect"]),
+                                        N("Materials", [np.array([0], np.int32)])])])
+    parent = N("Model", [20, "parent\x00\x01Model", "Null"], [N("Properties70", [], [
+        assets.fbx_p("Lcl Translation", "Lcl Translation", 1.0, 2.0, 3.0)])])
+    child = N("Model", [21, "child\x00\x01Model", "Mesh"], [N("Properties70", [], [
+        assets.fbx_p("Lcl Rotation", "Lcl Rotation", 0.0, 0.0, 90.0),
+        assets.fbx_p("Lcl Scaling", "Lcl Scaling", 2.0, 2.0, 2.0)])])
+    other = N("Model", [22, "other\x00\x01Model", "Mesh"], [N("Properties70")])
+    mat = N("Material", [30, "red\x00\x01Material", ""], [N("Properties70", [], [
+        assets.fbx_p("DiffuseColor", "Color", 0.8, 0.4, 0.2), assets.fbx_p("DiffuseFactor", "Number", 0.5),
+        assets.fbx_p("EmissiveColor", "Color", 0.0, 0.0, 0.0)])])
+    conns = [N("C", ["OO", 20, 0]), N("C", ["OO", 21, 20]), N("C", ["OO", 22, 0]), N("C", ["OO", 10, 21]),
+             N("C", ["OO", 10, 22]), N("C", ["OO", 30, 21])]
+    assets.write_fbx_tree(str(path), [N("Objects", [], [geom, parent, child, other, mat]),
+                                      N("Connections", [], conns)], version=7400)
+
+
+def test_fbx_scene_graph_transforms_fans_and_layers(tmp_path):
+    path = tmp_path / "graph.fbx"
+    _fbx_graph_file(path)
+    d = assets.load_fbx(str(path), flip_uv=True)
+    P = np.asarray(d.positions, np.float64)[np.asarray(d.indices).reshape(-1, 3)]
+    Nn = np.asarray(d.normals, np.float64)[np.asarray(d.indices).reshape(-1, 3)]
+    U = np.asarray(d.uvs, np.float64)[np.asarray(d.indices).reshape(-1, 3)]
+    assert P.shape == (6, 3, 3)  # (quad -> 2 triangles + 1 triangle) x 2 models
+    # the child model: rotate 90 degrees about z, scale 2, then translate (1, 2, 3)
+    to_world = lambda v: np.array([-2 * v[1] + 1, 2 * v[0] + 2, 2 * v[2] + 3])  # noqa: E731
+    quad = [(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0)]
+    expect = [to_world(quad[0]), to_world(quad[1]), to_world(quad[2])]
+    np.testing.assert_allclose(P[0], expect, atol=1e-6)
+    np.testing.assert_allclose(P[1], [to_world(quad[0]), to_world(quad[2]), to_world(quad[3])], atol=1e-6)
+    np.testing.assert_allclose(P[2], [to_world((1, 0, 0)), to_world((2, 0, 0)), to_world((1, 1, 0))], atol=1e-6)
+    np.testing.assert_allclose(P[3:], np.array([[quad[0], quad[1], quad[2]], [quad[0], quad[2], quad[3]],
+                                                [(1, 0, 0), (2, 0, 0), (1, 1, 0)]], np.float64))
+    np.testing.assert_allclose(Nn[:2], np.tile([0, 0, 1.0], (2, 3, 1)), atol=1e-6)  # z normals stay z
+    np.testing.assert_allclose(Nn[2], np.tile([0, 0, -1.0], (3, 1)), atol=1e-6)
+    np.testing.assert_allclose(U[0], [[0, 1], [1, 1], [1, 0]])  # flipped v
+    np.testing.assert_allclose(U[2], [[1, 1], [0.5, 0.75], [1, 0]])
+    # the child's slot 0 is the red material, diffuse times its factor; the
+    # other model has no material: the reference's fallbacks
+    assert list(d.triangle_material) == [0, 0, 0, 1, 1, 1]
+    np.testing.assert_allclose(d.materials["diffuse"][0], [0.4, 0.2, 0.1], rtol=1e-6)
+    np.testing.assert_allclose(d.materials["diffuse"][1], [1, 1, 1])
+    assert float(d.materials["roughness"][1]) == 1.0 and d.emitters == []
+
+
+def test_fbx_rejects_ascii(tmp_path):
+    path = tmp_path / "a.fbx"
+    path.write_text("; FBX 7.4.0 project file\nFBXHeaderExtension:  {\n}\n")
+    with pytest.raises(ValueError):
+        assets.load_fbx(str(path))
