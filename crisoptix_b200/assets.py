@@ -334,10 +334,12 @@ def save_obj(path: str, desc: scenes.Scene) -> None:
 #   ByVertice, referenced Direct or IndexToDirect; `LayerElementMaterial`
 #   AllSame or ByPolygon; polygons without normals get their face normal
 #   (aiProcess_GenNormals); every polygon corner is its own vertex;
-# * Model: `Lcl Translation`, `Lcl Rotation` (degrees, XYZ order),
-#   `Lcl Scaling` through the parent chain (Connections "OO"), baked into the
-#   triangles (normals by the inverse transpose); pivots, pre/post-rotations
-#   and geometric transforms are not read;
+# * Model: the FBX SDK's transform chain -- translation, rotation offset and
+#   pivot, pre-rotation, `Lcl Rotation` in the model's RotationOrder,
+#   post-rotation, scaling offset and pivot, `Lcl Scaling` -- through the
+#   parent chain (Connections "OO"), times the model's own geometric
+#   translation / rotation / scaling, baked into the triangles (normals by
+#   the inverse transpose);
 # * Material: DiffuseColor, SpecularColor, EmissiveColor, each times its
 #   ...Factor when present (assimp's factored colours), a Roughness or
 #   RoughnessFactor property if the file has one, with the reference's
@@ -463,22 +465,57 @@ def _p70(node: Optional[FbxNode]) -> Dict[str, list]:
     return out
 
 
-def _euler_xyz(deg) -> np.ndarray:
-    """Rotation of FBX's default XYZ order: about x first, then y, then z."""
-    rx, ry, rz = np.radians(np.asarray(deg, np.float64)[:3])
-    cx, sx, cy, sy, cz, sz = np.cos(rx), np.sin(rx), np.cos(ry), np.sin(ry), np.cos(rz), np.sin(rz)
-    Rx = np.array([[1, 0, 0], [0, cx, -sx], [0, sx, cx]])
-    Ry = np.array([[cy, 0, sy], [0, 1, 0], [-sy, 0, cy]])
-    Rz = np.array([[cz, -sz, 0], [sz, cz, 0], [0, 0, 1]])
-    return Rz @ Ry @ Rx
+# FBX's RotationOrder enum: the axes in the order they are applied
+_ROT_ORDERS = ("xyz", "xzy", "yzx", "yxz", "zxy", "zyx")
+
+
+def _euler(deg, order: int = 0) -> np.ndarray:
+    """Rotation by Euler angles (degrees) applied in RotationOrder `order`
+    (0, eEulerXYZ: about x first, then y, then z)."""
+    a = np.radians(np.asarray(deg, np.float64)[:3])
+    c, s = np.cos(a), np.sin(a)
+    R = {"x": np.array([[1, 0, 0], [0, c[0], -s[0]], [0, s[0], c[0]]]),
+         "y": np.array([[c[1], 0, s[1]], [0, 1, 0], [-s[1], 0, c[1]]]),
+         "z": np.array([[c[2], -s[2], 0], [s[2], c[2], 0], [0, 0, 1]])}
+    M = np.eye(3)
+    for axis in _ROT_ORDERS[order if 0 <= order < 6 else 0]:
+        M = R[axis] @ M
+    return M
+
+
+def _m4(R=None, t=None, s=None) -> np.ndarray:
+    M = np.eye(4)
+    if R is not None:
+        M[:3, :3] = R
+    if s is not None:
+        M[:3, :3] = M[:3, :3] @ np.diag(np.asarray(s, np.float64)[:3])
+    if t is not None:
+        M[:3, 3] = np.asarray(t, np.float64)[:3]
+    return M
 
 
 def _fbx_local(props: Dict[str, list]) -> np.ndarray:
-    M = np.eye(4)
-    M[:3, :3] = _euler_xyz(props.get("Lcl Rotation", [0.0, 0.0, 0.0])) @ np.diag(
-        np.asarray(props.get("Lcl Scaling", [1.0, 1.0, 1.0])[:3], np.float64))
-    M[:3, 3] = np.asarray(props.get("Lcl Translation", [0.0, 0.0, 0.0])[:3], np.float64)
-    return M
+    """A model's local transform as the FBX SDK composes it:
+    T * Roff * Rp * Rpre * R * Rpost^-1 * Rp^-1 * Soff * Sp * S * Sp^-1
+    (pre- and post-rotations in XYZ order, R in the model's RotationOrder)."""
+    def v(name, default):
+        return props.get(name, default)[:3]
+
+    order = int(props.get("RotationOrder", [0])[0])
+    z3 = [0.0, 0.0, 0.0]
+    Rp, Sp = _m4(t=v("RotationPivot", z3)), _m4(t=v("ScalingPivot", z3))
+    Rpost = _m4(R=_euler(v("PostRotation", z3)))
+    return (_m4(t=v("Lcl Translation", z3)) @ _m4(t=v("RotationOffset", z3)) @ Rp
+            @ _m4(R=_euler(v("PreRotation", z3))) @ _m4(R=_euler(v("Lcl Rotation", z3), order))
+            @ np.linalg.inv(Rpost) @ np.linalg.inv(Rp) @ _m4(t=v("ScalingOffset", z3)) @ Sp
+            @ _m4(s=v("Lcl Scaling", [1.0, 1.0, 1.0])) @ np.linalg.inv(Sp))
+
+
+def _fbx_geometric(props: Dict[str, list]) -> np.ndarray:
+    """The geometric transform of a model's own geometry (not inherited)."""
+    z3 = [0.0, 0.0, 0.0]
+    return _m4(R=_euler(props.get("GeometricRotation", z3)[:3]), t=props.get("GeometricTranslation", z3)[:3],
+               s=props.get("GeometricScaling", [1.0, 1.0, 1.0])[:3])
 
 
 def _fbx_layer(geom: FbxNode, layer: str, data: str, index: str, width: int, corner_vertex: np.ndarray,
@@ -598,7 +635,7 @@ def load_fbx(path: str, flip_uv: bool = False, spec_usage: int = 0) -> scenes.Sc
         tri_c = np.asarray(tri_c, np.int64)
         tri_p = np.asarray(tri_p, np.int64)
         for m in geom_models.get(gid, []):
-            M = world(m)
+            M = world(m) @ _fbx_geometric(_p70(objects[m]))
             A, t = M[:3, :3], M[:3, 3]
             ident = np.array_equal(M, np.eye(4))  # untransformed: values kept bit for bit
             P = V[cv[tri_c]] if ident else V[cv[tri_c]] @ A.T + t  # (T, 3, 3) per triangle corner

@@ -315,3 +315,53 @@ def test_fbx_rejects_ascii(tmp_path):
     path.write_text("; FBX 7.4.0 project file\nFBXHeaderExtension:  {\n}\n")
     with pytest.raises(ValueError):
         assets.load_fbx(str(path))
+
+
+def test_fbx_transform_chain_pivots_orders_and_geometric(tmp_path):
+    """The FBX SDK's chain T Roff Rp Rpre R Rpost^-1 Rp^-1 Soff Sp S Sp^-1 and
+    the model's geometric transform, against the same product composed here
+    with scipy's Euler rotations (extrinsic 'xyz' is FBX's XYZ order)."""
+    from scipy.spatial.transform import Rotation
+
+    N = assets.FbxNode
+    P = assets.fbx_p
+    verts = np.array([0.3, -0.2, 0.5, 1.0, 0.1, 0.0, 0.2, 0.9, -0.4], np.float64)
+    geom = N("Geometry", [10, "g\x00\x01Geometry", "Mesh"], [
+        N("Vertices", [verts]), N("PolygonVertexIndex", [np.array([0, 1, -3], np.int32)])])
+    props = dict(T=(1.0, -2.0, 0.5), Roff=(0.1, 0.2, 0.3), Rp=(1.0, 0.0, -1.0), Rpre=(-90.0, 0.0, 0.0),
+                 R=(10.0, 20.0, 30.0), Rpost=(0.0, 15.0, 0.0), Soff=(0.0, 0.5, 0.0), Sp=(0.2, 0.2, 0.2),
+                 S=(2.0, 1.0, 0.5), Gt=(0.0, 0.0, 1.0), Gr=(0.0, 0.0, 45.0), Gs=(1.0, 2.0, 1.0))
+    model = N("Model", [21, "m\x00\x01Model", "Mesh"], [N("Properties70", [], [
+        P("Lcl Translation", "Lcl Translation", *props["T"]), P("RotationOffset", "Vector3D", *props["Roff"]),
+        P("RotationPivot", "Vector3D", *props["Rp"]), P("PreRotation", "Vector3D", *props["Rpre"]),
+        P("Lcl Rotation", "Lcl Rotation", *props["R"]), P("RotationOrder", "enum", 5),
+        P("PostRotation", "Vector3D", *props["Rpost"]), P("ScalingOffset", "Vector3D", *props["Soff"]),
+        P("ScalingPivot", "Vector3D", *props["Sp"]), P("Lcl Scaling", "Lcl Scaling", *props["S"]),
+        P("GeometricTranslation", "Vector3D", *props["Gt"]), P("GeometricRotation", "Vector3D", *props["Gr"]),
+        P("GeometricScaling", "Vector3D", *props["Gs"])])])
+    path = tmp_path / "chain.fbx"
+    assets.write_fbx_tree(str(path), [N("Objects", [], [geom, model]), N("Connections", [], [
+        N("C", ["OO", 21, 0]), N("C", ["OO", 10, 21])])], version=7500)
+    d = assets.load_fbx(str(path))
+
+    def tr(t):
+        M = np.eye(4)
+        M[:3, 3] = t
+        return M
+
+    def rot(deg, seq="xyz"):
+        M = np.eye(4)
+        angles = deg if seq == "xyz" else deg[::-1]  # 'zyx': z first, so pass (z, y, x)
+        M[:3, :3] = Rotation.from_euler(seq, angles, degrees=True).as_matrix()
+        return M
+
+    def sc(s):
+        return np.diag([*s, 1.0])
+
+    inv = np.linalg.inv
+    W = (tr(props["T"]) @ tr(props["Roff"]) @ tr(props["Rp"]) @ rot(props["Rpre"]) @ rot(props["R"], "zyx")
+         @ inv(rot(props["Rpost"])) @ inv(tr(props["Rp"])) @ tr(props["Soff"]) @ tr(props["Sp"]) @ sc(props["S"])
+         @ inv(tr(props["Sp"])) @ tr(props["Gt"]) @ rot(props["Gr"]) @ sc(props["Gs"]))
+    expect = (np.c_[verts.reshape(-1, 3), np.ones(3)] @ W.T)[:, :3]
+    got = np.asarray(d.positions, np.float64)[np.asarray(d.indices).reshape(-1)]
+    np.testing.assert_allclose(got, expect, rtol=1e-5, atol=1e-5)
