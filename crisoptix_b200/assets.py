@@ -828,3 +828,14 @@ def save_fbx(path: str, desc: scenes.Scene, version: int = 7400) -> None:
                     conns.append(FbxNode("C", ["OP", 4000 + int(row[slot]), 3000 + i, prop]))
     write_fbx_tree(path, [FbxNode("FBXHeaderExtension", [], [FbxNode("FBXVersion", [version])]),
                           FbxNode("Objects", [], objs), FbxNode("Connections", [], conns)], version)
+
+
+def load_model(path: str, flip_uv: bool = False, spec_usage: int = 0) -> scenes.Scene:
+    """Model(path, flipUv, specTexUsage) (src/Model.cpp:9-44): the scene
+    description of an OBJ or binary FBX file, by its extension."""
+    ext = os.path.splitext(path)[1].lower()
+    if ext == ".obj":
+        return load_obj(path, flip_uv, spec_usage)
+    if ext == ".fbx":
+        return load_fbx(path, flip_uv, spec_usage)
+    raise ValueError(f"{path}: only .obj and binary .fbx files are read")

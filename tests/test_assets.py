@@ -365,3 +365,16 @@ def test_fbx_transform_chain_pivots_orders_and_geometric(tmp_path):
     expect = (np.c_[verts.reshape(-1, 3), np.ones(3)] @ W.T)[:, :3]
     got = np.asarray(d.positions, np.float64)[np.asarray(d.indices).reshape(-1)]
     np.testing.assert_allclose(got, expect, rtol=1e-5, atol=1e-5)
+
+
+def test_load_model_dispatches_on_the_extension(tmp_path):
+    desc, _ = scenes.textured_cornell_box()
+    assets.save_obj(str(tmp_path / "box.obj"), desc)
+    assets.save_fbx(str(tmp_path / "box.fbx"), desc)
+    a = assets.load_model(str(tmp_path / "box.obj"), spec_usage=1)
+    b = assets.load_model(str(tmp_path / "box.fbx"), spec_usage=1)
+    ia, ib = np.asarray(a.indices).reshape(-1, 3), np.asarray(b.indices).reshape(-1, 3)
+    assert np.asarray(a.positions)[ia].tobytes() == np.asarray(b.positions)[ib].tobytes()
+    assert (a.materials["spec_usage"] == 1).all() and (b.materials["spec_usage"] == 1).all()
+    with pytest.raises(ValueError):
+        assets.load_model(str(tmp_path / "box.gltf"))
