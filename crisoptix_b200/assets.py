@@ -346,8 +346,9 @@ def save_obj(path: str, desc: scenes.Scene) -> None:
 #   fallbacks otherwise (diffuse and specular 1, emission 0, roughness 1);
 #   Texture objects connected ("OP") to DiffuseColor / SpecularColor /
 #   Roughness (or 3ds Max's roughness_map) give the diffuse / specular /
-#   roughness textures (RelativeFilename, else FileName's base name, relative
-#   to the FBX's folder; PNG);
+#   roughness textures: embedded (a Video object's Content) or the file
+#   (RelativeFilename, else FileName's base name, relative to the FBX's
+#   folder); PNG;
 # * faces of a material with non-zero emission form one emitter per material,
 #   as in load_obj.
 #
@@ -597,6 +598,8 @@ def load_fbx(path: str, flip_uv: bool = False, spec_usage: int = 0) -> scenes.Sc
     for c, p, prop in op:
         if kind(c) == "Texture" and kind(p) == "Material":
             tex_of[(mat_ids.index(p), prop)] = c
+    # embedded image bytes: a Video object connected to the texture
+    video_of = {p: c for c, p in oo if kind(c) == "Video" and kind(p) == "Texture"}
 
     pos: List[np.ndarray] = []
     nrm: List[np.ndarray] = []
@@ -673,6 +676,13 @@ def load_fbx(path: str, flip_uv: bool = False, spec_usage: int = 0) -> scenes.Sc
             return -1
         if tid not in tex_index:
             t = objects[tid]
+            v = objects.get(video_of.get(tid, -1))
+            content = v.child("Content") if v is not None else None
+            if content is not None and content.props and isinstance(content.props[0], bytes) \
+                    and content.props[0].startswith(_SIG):
+                textures.append(decode_png_rgba(content.props[0]))
+                tex_index[tid] = len(textures) - 1
+                return tex_index[tid]
             name = None
             for key in ("RelativeFilename", "FileName"):
                 if t.child(key) is not None and t.child(key).props and str(t.child(key).props[0]):

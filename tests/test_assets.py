@@ -378,3 +378,24 @@ def test_load_model_dispatches_on_the_extension(tmp_path):
     assert (a.materials["spec_usage"] == 1).all() and (b.materials["spec_usage"] == 1).all()
     with pytest.raises(ValueError):
         assets.load_model(str(tmp_path / "box.gltf"))
+
+
+def test_fbx_embedded_texture(tmp_path):
+    """A texture whose Video object embeds the PNG bytes is read from them
+    (no file beside the FBX)."""
+    N = assets.FbxNode
+    rgba = (np.arange(4 * 3 * 4) * 7 % 256).astype(np.uint8).reshape(4, 3, 4)
+    geom = N("Geometry", [10, "g\x00\x01Geometry", "Mesh"], [
+        N("Vertices", [np.array([0, 0, 0, 1, 0, 0, 0, 1, 0], np.float64)]),
+        N("PolygonVertexIndex", [np.array([0, 1, -3], np.int32)])])
+    objs = [geom, N("Model", [20, "m\x00\x01Model", "Mesh"], [N("Properties70")]),
+            N("Material", [30, "t\x00\x01Material", ""], [N("Properties70")]),
+            N("Texture", [40, "tex\x00\x01Texture", ""], [N("RelativeFilename", ["missing.png"])]),
+            N("Video", [50, "v\x00\x01Video", "Clip"], [N("Content", [assets.encode_png_rgba(rgba)])])]
+    conns = [N("C", ["OO", 20, 0]), N("C", ["OO", 10, 20]), N("C", ["OO", 30, 20]),
+             N("C", ["OP", 40, 30, "DiffuseColor"]), N("C", ["OO", 50, 40])]
+    path = tmp_path / "emb.fbx"
+    assets.write_fbx_tree(str(path), [N("Objects", [], objs), N("Connections", [], conns)])
+    d = assets.load_fbx(str(path))
+    assert d.material_textures.tolist() == [[0, -1, -1]]
+    assert (d.textures[0] == rgba).all()
