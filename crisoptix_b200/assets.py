@@ -1,9 +1,9 @@
-"""Scene files: Wavefront OBJ + MTL and binary FBX, with PNG textures.
+"""Scene files: Wavefront OBJ + MTL and FBX (binary and ASCII), with PNG textures.
 
 The reference imports models with assimp (src/Model.cpp:9-207: triangulated,
 normals generated where missing, optional uv flip) and reads textures with
 stb_image as RGBA8 (src/Texture.cpp:8-30).  Neither library is part of this
-package; this module reads the same inputs itself, for OBJ/MTL, binary FBX
+package; this module reads the same inputs itself, for OBJ/MTL, FBX
 (load_fbx, described with its section below) and 8-bit PNG:
 
 * geometry: `v`, `vt`, `vn`, `f` (polygons fanned into triangles, negative
@@ -321,7 +321,7 @@ def save_obj(path: str, desc: scenes.Scene) -> None:
             f.write("f " + " ".join(f"{int(v) + 1}/{int(v) + 1}/{int(v) + 1}" for v in tri) + "\n")
 
 
-# ---- FBX (binary) -------------------------------------------------------------------
+# ---- FBX ----------------------------------------------------------------------------
 # The reference reads FBX through assimp (src/Model.cpp:9-207).  This reader
 # covers the binary format's node tree (FBX 7.x: 32-bit node records before
 # version 7500, 64-bit from it; zlib-compressed arrays) and the parts of the
@@ -352,7 +352,8 @@ def save_obj(path: str, desc: scenes.Scene) -> None:
 # * faces of a material with non-zero emission form one emitter per material,
 #   as in load_obj.
 #
-# ASCII FBX is not read.
+# The ASCII form (`Name: values { children }`, arrays as `*N { a: ... }`) is
+# read into the same node tree; its embedded contents are not.
 
 _FBX_MAGIC = b"Kaydara FBX Binary  \x00\x1a\x00"
 
@@ -436,10 +437,81 @@ def _fbx_node(buf: bytes, o: int, wide: bool):
     return FbxNode(name, props, children), end
 
 
+_FBX_TOKEN = __import__("re").compile(
+    r'\s+|;[^\n]*|(?P<name>[A-Za-z_][\w|]*):|(?P<str>"(?:[^"\\]|\\.)*")|(?P<count>\*\d+)'
+    r'|(?P<num>[-+]?(?:\d+\.?\d*|\.\d+)(?:[eE][-+]?\d+)?)|(?P<sym>[{},])|(?P<word>[A-Za-z_][\w|]*)')
+
+
+def _fbx_ascii_tokens(text: str):
+    toks = []
+    for m in _FBX_TOKEN.finditer(text):
+        k = m.lastgroup
+        if k is None:
+            continue  # white space, comment
+        toks.append((k, m.group(k)))
+    return toks
+
+
+def _fbx_ascii_block(toks, i: int) -> Tuple[List[FbxNode], int]:
+    nodes = []
+    while i < len(toks) and toks[i] != ("sym", "}"):
+        kind, name = toks[i]
+        if kind != "name":
+            raise ValueError(f"FBX (ASCII): expected a node name, got {name!r}")
+        i += 1
+        props: list = []
+        children: List[FbxNode] = []
+        while i < len(toks) and toks[i][0] in ("str", "num", "count", "word", "sym") and toks[i] != ("sym", "}"):
+            kind, v = toks[i]
+            if (kind, v) == ("sym", "{"):
+                children, i = _fbx_ascii_block(toks, i + 1)
+                i += 1  # the closing brace
+                break
+            if kind == "sym":  # a comma
+                i += 1
+            elif kind == "count":  # *N { a: values }
+                if toks[i + 1] != ("sym", "{") or toks[i + 2] != ("name", "a"):
+                    raise ValueError("FBX (ASCII): malformed array")
+                i += 3
+                vals = []
+                while toks[i] != ("sym", "}"):
+                    if toks[i][0] == "num":
+                        vals.append(toks[i][1])
+                    i += 1
+                i += 1
+                is_float = any(("." in x) or ("e" in x) or ("E" in x) for x in vals)
+                props.append(np.array([float(x) for x in vals], np.float64) if is_float
+                             else np.array([int(x) for x in vals], np.int64))
+            elif kind == "num":
+                props.append(float(v) if any(c in v for c in ".eE") else int(v))
+                i += 1
+            elif kind == "str":
+                props.append(v[1:-1].replace("&quot;", '"'))
+                i += 1
+            else:
+                props.append(v)
+                i += 1
+        nodes.append(FbxNode(name, props, children))
+    return nodes, i
+
+
+def _read_fbx_ascii(text: str) -> Tuple[int, List[FbxNode]]:
+    nodes, _ = _fbx_ascii_block(_fbx_ascii_tokens(text), 0)
+    version = 0
+    for n in nodes:
+        if n.name == "FBXHeaderExtension" and n.child("FBXVersion") is not None:
+            version = int(n.child("FBXVersion").props[0])
+    return version, nodes
+
+
 def read_fbx_tree(data: bytes) -> Tuple[int, List[FbxNode]]:
-    """(version, top-level nodes) of a binary FBX file."""
+    """(version, top-level nodes) of a binary or ASCII FBX file."""
     if not data.startswith(_FBX_MAGIC):
-        raise ValueError("not a binary FBX file (ASCII FBX is not read)")
+        text = data.decode("utf-8", "replace").lstrip("\ufeff")
+        version, nodes = _read_fbx_ascii(text)
+        if not any(n.name == "Objects" for n in nodes) and not any(n.name == "FBXHeaderExtension" for n in nodes):
+            raise ValueError("not an FBX file")
+        return version, nodes
     version = struct.unpack_from("<I", data, len(_FBX_MAGIC))[0]
     wide = version >= 7500
     o = len(_FBX_MAGIC) + 4
@@ -556,7 +628,7 @@ def _factored(props: Dict[str, list], name: str, default) -> List[float]:
 
 
 def load_fbx(path: str, flip_uv: bool = False, spec_usage: int = 0) -> scenes.Scene:
-    """Scene description of a binary FBX file: every mesh model's polygons,
+    """Scene description of an FBX file (binary or ASCII): every mesh model's polygons,
     triangulated and transformed to world space, its materials and their PNG
     textures (paths relative to the file's folder)."""
     base = os.path.dirname(os.path.abspath(path))
@@ -783,17 +855,56 @@ def write_fbx_tree(path: str, nodes: List[FbxNode], version: int = 7400) -> None
         f.write(bytes(out))
 
 
+def _fbx_ascii_value(v) -> str:
+    if isinstance(v, (bool, np.bool_)):
+        return "T" if v else "F"
+    if isinstance(v, (int, np.integer)):
+        return str(int(v))
+    if isinstance(v, (float, np.floating)):
+        return repr(float(v))
+    if isinstance(v, bytes):
+        return '""'  # embedded content is not written in the ASCII form
+    s = str(v)
+    if "\x00\x01" in s:  # binary "name\x00\x01Class" is "Class::name" in ASCII
+        name, cls = s.split("\x00\x01", 1)
+        s = f"{cls}::{name}"
+    return '"' + s.replace('"', "&quot;") + '"'
+
+
+def _fbx_ascii_lines(node: FbxNode, indent: str) -> List[str]:
+    if len(node.props) == 1 and isinstance(node.props[0], np.ndarray):
+        a = node.props[0].reshape(-1)
+        vals = ",".join(repr(float(x)) if a.dtype.kind == "f" else str(int(x)) for x in a)
+        return [f"{indent}{node.name}: *{a.size} {{", f"{indent}\ta: {vals}", f"{indent}}}"]
+    head = f"{indent}{node.name}: " + ",".join(_fbx_ascii_value(v) for v in node.props)
+    if not node.children:
+        return [head]
+    out = [head + " {"]
+    for c in node.children:
+        out.extend(_fbx_ascii_lines(c, indent + "\t"))
+    return out + [f"{indent}}}"]
+
+
+def write_fbx_ascii_tree(path: str, nodes: List[FbxNode]) -> None:
+    """Write top-level nodes as an ASCII FBX file."""
+    lines = ["; FBX 7.4.0 project file"]
+    for n in nodes:
+        lines.extend(_fbx_ascii_lines(n, ""))
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
 def fbx_p(name: str, kind: str, *values) -> FbxNode:
     """A Properties70 entry."""
     return FbxNode("P", [name, kind, "", "A", *values])
 
 
-def save_fbx(path: str, desc: scenes.Scene, version: int = 7400) -> None:
-    """Write a non-instanced scene as a binary FBX that load_fbx reads back to
-    the same triangles (every corner's position, normal and uv), materials,
-    textures and emitters: one Geometry (normals and uvs by vertex, materials
-    by polygon), one Model, one Material per material (textures connected to
-    DiffuseColor, SpecularColor and Roughness)."""
+def save_fbx(path: str, desc: scenes.Scene, version: int = 7400, ascii: bool = False) -> None:
+    """Write a non-instanced scene as a binary (or ASCII) FBX that load_fbx
+    reads back to the same triangles (every corner's position, normal and
+    uv), materials, textures and emitters: one Geometry (normals and uvs by
+    vertex, materials by polygon), one Model, one Material per material
+    (textures connected to DiffuseColor, SpecularColor and Roughness)."""
     if desc.instances:
         raise ValueError("save_fbx writes non-instanced scenes")
     base = os.path.dirname(os.path.abspath(path))
@@ -836,16 +947,20 @@ def save_fbx(path: str, desc: scenes.Scene, version: int = 7400) -> None:
             for slot, prop in enumerate(("DiffuseColor", "SpecularColor", "Roughness")):
                 if row[slot] >= 0:
                     conns.append(FbxNode("C", ["OP", 4000 + int(row[slot]), 3000 + i, prop]))
-    write_fbx_tree(path, [FbxNode("FBXHeaderExtension", [], [FbxNode("FBXVersion", [version])]),
-                          FbxNode("Objects", [], objs), FbxNode("Connections", [], conns)], version)
+    top = [FbxNode("FBXHeaderExtension", [], [FbxNode("FBXVersion", [version])]),
+           FbxNode("Objects", [], objs), FbxNode("Connections", [], conns)]
+    if ascii:
+        write_fbx_ascii_tree(path, top)
+    else:
+        write_fbx_tree(path, top, version)
 
 
 def load_model(path: str, flip_uv: bool = False, spec_usage: int = 0) -> scenes.Scene:
     """Model(path, flipUv, specTexUsage) (src/Model.cpp:9-44): the scene
-    description of an OBJ or binary FBX file, by its extension."""
+    description of an OBJ or FBX file, by its extension."""
     ext = os.path.splitext(path)[1].lower()
     if ext == ".obj":
         return load_obj(path, flip_uv, spec_usage)
     if ext == ".fbx":
         return load_fbx(path, flip_uv, spec_usage)
-    raise ValueError(f"{path}: only .obj and binary .fbx files are read")
+    raise ValueError(f"{path}: only .obj and .fbx files are read")

@@ -243,7 +243,7 @@ def test_fbx_round_trip(tmp_path, version):
         assert oa.tobytes() == ob.tobytes()
 
 
-def _fbx_graph_file(path):
+def _fbx_graph_file(path, ascii=False):
     """A quad and a triangle with per-corner indexed normals and uvs, one
     material slot, used by two models: `child` (rotated 90 degrees about z,
     scaled 2) under `parent` (translated by (1, 2, 3)), and `other` at the
@@ -277,8 +277,11 @@ def _fbx_graph_file(path):
         assets.fbx_p("EmissiveColor", "Color", 0.0, 0.0, 0.0)])])
     conns = [N("C", ["OO", 20, 0]), N("C", ["OO", 21, 20]), N("C", ["OO", 22, 0]), N("C", ["OO", 10, 21]),
              N("C", ["OO", 10, 22]), N("C", ["OO", 30, 21])]
-    assets.write_fbx_tree(str(path), [N("Objects", [], [geom, parent, child, other, mat]),
-                                      N("Connections", [], conns)], version=7400)
+    top = [N("Objects", [], [geom, parent, child, other, mat]), N("Connections", [], conns)]
+    if ascii:
+        assets.write_fbx_ascii_tree(str(path), top)
+    else:
+        assets.write_fbx_tree(str(path), top, version=7400)
 
 
 def test_fbx_scene_graph_transforms_fans_and_layers(tmp_path):
@@ -310,11 +313,28 @@ def test_fbx_scene_graph_transforms_fans_and_layers(tmp_path):
     assert float(d.materials["roughness"][1]) == 1.0 and d.emitters == []
 
 
-def test_fbx_rejects_ascii(tmp_path):
-    path = tmp_path / "a.fbx"
-    path.write_text("; FBX 7.4.0 project file\nFBXHeaderExtension:  {\n}\n")
-    with pytest.raises(ValueError):
-        assets.load_fbx(str(path))
+def test_fbx_ascii_reads_like_binary(tmp_path):
+    """The ASCII form of the same trees gives the same scenes: the textured
+    box through save_fbx, the scene graph through the node writer."""
+    desc, _ = scenes.textured_cornell_box()
+    assets.save_fbx(str(tmp_path / "b.fbx"), desc)
+    assets.save_fbx(str(tmp_path / "a.fbx"), desc, ascii=True)
+    _fbx_graph_file(tmp_path / "gb.fbx")
+    _fbx_graph_file(tmp_path / "ga.fbx", ascii=True)
+    assert (tmp_path / "a.fbx").read_text().startswith("; FBX")
+    for bn, an in (("b.fbx", "a.fbx"), ("gb.fbx", "ga.fbx")):
+        b, a = assets.load_fbx(str(tmp_path / bn)), assets.load_fbx(str(tmp_path / an))
+        for name in ("positions", "normals", "uvs", "indices", "triangle_material", "emitter_faces"):
+            assert np.asarray(getattr(a, name)).tobytes() == np.asarray(getattr(b, name)).tobytes(), (an, name)
+        assert a.materials.tobytes() == b.materials.tobytes()
+
+
+def test_fbx_rejects_non_fbx(tmp_path):
+    (tmp_path / "h.fbx").write_text("; FBX 7.4.0 project file\nFBXHeaderExtension:  {\n}\n")
+    (tmp_path / "x.fbx").write_text("solid cube\nfacet normal 0 0 1\n")
+    for name in ("h.fbx", "x.fbx"):  # no Objects; not FBX at all
+        with pytest.raises(ValueError):
+            assets.load_fbx(str(tmp_path / name))
 
 
 def test_fbx_transform_chain_pivots_orders_and_geometric(tmp_path):
