@@ -611,7 +611,7 @@ def _fbx_layer(geom: FbxNode, layer: str, data: str, index: str, width: int, cor
         key = np.zeros(n, np.int64)
     else:
         raise ValueError(f"FBX {layer}: mapping {mapping}")
-    if ref in ("IndexToDirect", "Index"):
+    if ref in ("IndexToDirect", "Index") and el.child(index) is not None:  # without indices: direct
         key = np.asarray(el.child(index).props[0], np.int64)[key]
     return vals[key]
 
